@@ -1,0 +1,237 @@
+/* rhgpu.h - C ABI of the B200 (sm_100a) hybrid-PIC hot path for RHybrid.
+ *
+ * One time step of RHybrid's propagate() (src/user.cpp:49-158, order at
+ * :118-134) runs on one GPU behind these entry points:
+ *   1. Boris-Buneman ion push with the field gather at the particle
+ *      (src/particle_propagator_boris_buneman.h:64-194, getFields
+ *      src/hybrid_propagator.cpp:1879-1891): face-linear B, NGP Ue and Ep.
+ *   2. Cell-to-cell migration of particles that left their cell (Corsair's
+ *      particle list, not vendored; rule restated in DESIGN.md).
+ *   3. CIC charge and ion-current deposit (src/particle_accumulator.cpp:44-156)
+ *      with the finalize step /dV and rho clamp (:319-333).
+ *   4. Particle boundary conditions (src/particle_boundary_cond_hybrid.h:112-185).
+ *   5. The staggered-grid field update propagateB (src/hybrid_propagator.cpp:42-440).
+ *
+ * Conventions shared with the reference:
+ *   - cells are Corsair 1x1x1 blocks; the linear cell index is
+ *     n = i + nx*(j + ny*k), x fastest;
+ *   - vector grid arrays crossing this ABI are interleaved per cell
+ *     (component l of cell n at [3*n+l]), exactly as ParGrid stores them;
+ *   - a particle is 7 doubles {X,Y,Z,VX,VY,VZ,WEIGHT} with X,Y,Z local to
+ *     its cell, in [0,dx) (src/particle_definition.h:29-38); particle arrays
+ *     crossing this ABI are grouped by cell in linear cell order, with a
+ *     per-cell count array (the flattened form of ParGrid's per-cell lists).
+ *
+ * All entry points return 0 on success or an RHGPU_ERR_* code; the text of
+ * the last error of the calling thread is returned by rhgpu_last_error().
+ * A context is used by one host thread at a time.
+ */
+#ifndef RHGPU_H
+#define RHGPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Physical constants. Corsair's constants:: namespace is not vendored with
+ * the reference; these are the CODATA 2018 values it is expected to hold
+ * (used at src/hybrid_propagator.cpp:1505-1517, src/particle_species.cpp:67-94). */
+#define RHGPU_PERMEABILITY       1.2566370614359173e-06
+#define RHGPU_CHARGE_ELEMENTARY  1.602176634e-19
+#define RHGPU_MASS_PROTON        1.67262192369e-27
+#define RHGPU_BOLTZMANN          1.380649e-23
+#define RHGPU_GRAVITY            6.67430e-11
+
+/* status codes */
+#define RHGPU_OK              0
+#define RHGPU_ERR_ARG         1  /* bad argument */
+#define RHGPU_ERR_CUDA        2  /* CUDA runtime error */
+#define RHGPU_ERR_STATE       3  /* call out of order (e.g. step before upload) */
+#define RHGPU_ERR_DEVICE      4  /* a kernel raised its device error word (see rhgpu_device_errors) */
+#define RHGPU_ERR_NOMEM       5  /* device allocation failed */
+#define RHGPU_ERR_CAPACITY    6  /* particle storage capacity exceeded */
+
+/* device error word bits (rhgpu_device_errors) */
+#define RHGPU_DEVERR_NAN_PARTICLE   1u  /* non-finite particle coordinate after the push */
+#define RHGPU_DEVERR_FAST_PARTICLE  2u  /* particle moved more than one cell in a step */
+#define RHGPU_DEVERR_CAPACITY       4u  /* particle buffer overflow during migration */
+
+/* per-cell flag bits of the cell_flags array (user.cpp:1883-1941) */
+#define RHGPU_FLAG_INNER_FIELD     1u  /* innerFlagField: cell centre inside R_fieldObstacle */
+#define RHGPU_FLAG_INNER_NODE      2u  /* innerFlagNode: (+,+,+) node inside R_fieldObstacle */
+#define RHGPU_FLAG_INNER_PARTICLE  4u  /* innerFlagParticle: cell may hold obstacle particles */
+#define RHGPU_FLAG_INNER_CELLEP    8u  /* innerFlagCellEp: electron pressure field zeroed */
+
+/* grid arrays addressable through rhgpu_download_array / rhgpu_upload_array
+ * (names of the Hybrid:: DataIDs in src/hybrid.h:166-187) */
+enum rhgpu_array_id {
+   RHGPU_FACE_B = 0,      /* faceB,     3 per cell: component l lives on the +l face */
+   RHGPU_CELL_B,          /* cellB,     3 */
+   RHGPU_CELL_UE,         /* cellUe,    3 */
+   RHGPU_CELL_EP,         /* cellEp,    3 */
+   RHGPU_CELL_RHOQI,      /* cellRhoQi, 1 */
+   RHGPU_CELL_JI,         /* cellJi,    3 */
+   RHGPU_CELL_J,          /* cellJ,     3 */
+   RHGPU_NODE_RHOQI,      /* nodeRhoQi, 1: node at the (+,+,+) corner of the cell */
+   RHGPU_NODE_JI,         /* nodeJi,    3 */
+   RHGPU_NODE_J,          /* nodeJ,     3 */
+   RHGPU_NODE_UE,         /* nodeUe,    3 */
+   RHGPU_NODE_B,          /* nodeB,     3 */
+   RHGPU_NODE_E,          /* nodeE,     3 */
+   RHGPU_NODE_ETA,        /* nodeEta,   1 */
+   RHGPU_CELL_AVERAGE_B,  /* cellAverageB, 3 (WRITE_GRID_TEMPORAL_AVERAGES) */
+   RHGPU_NUM_ARRAYS
+};
+
+/* counters (Hybrid::logCounter*, src/hybrid.h:313-327), rhgpu_get_counters order */
+enum rhgpu_counter_id {
+   RHGPU_CNT_FIELD_MIN_CELL_RHOQI = 0, /* logCounterFieldMinCellRhoQi  (particle_accumulator.cpp:329) */
+   RHGPU_CNT_FIELD_MAX_CELL_UE,        /* logCounterFieldMaxCellUe     (hybrid_propagator.cpp:1384) */
+   RHGPU_CNT_FIELD_MAX_NODE_UE,        /* logCounterFieldMaxNodeUe     (:1581) */
+   RHGPU_CNT_FIELD_MAX_VW,             /* logCounterFieldMaxVw         (:1515) */
+   RHGPU_CNT_FIELD_MAX_E,              /* logCounterFieldMaxE          (:1442) */
+   RHGPU_CNT_FIELD_MIN_NODE_RHOQI,     /* logCounterFieldMinNodeRhoQi  (:1554) */
+   RHGPU_CNT_GRID_AVERAGE_COUNTER,     /* gridTemporalAverageCounter   (:166) */
+   RHGPU_NUM_FIELD_COUNTERS,
+   /* then per species s, 5 values at RHGPU_NUM_FIELD_COUNTERS + 5*s + {0..4}:
+    * logCounterParticleMaxVi, Escape (weight), EscapeKineticEnergy, Impact (weight),
+    * ImpactKineticEnergy (boris.h:156, particle_boundary_cond_hybrid.h:120-121,148-149) */
+   RHGPU_CNT_PER_SPECIES = 5
+};
+
+/* Simulation and Hybrid:: parameters the hot path reads. Derived values are
+ * given already converted, as userLateInitialization leaves them
+ * (src/user.cpp:356-1807): squared radii and speeds, SI resistivity table. */
+typedef struct rhgpu_params {
+   int32_t nx, ny, nz;            /* cells per axis, including exterior cells of non-periodic walls */
+   int32_t periodic[3];           /* LogicallyCartesian x/y/z_periodic */
+   double  x_min, y_min, z_min;   /* box minimum corner [m] */
+   double  dx;                    /* cube cell side [m] (Hybrid::dx) */
+   double  dt;                    /* time step [s] */
+   double  t_initial;             /* simulation time at the first step [s] */
+   int32_t use_hall;              /* Hybrid::useHallElectricField */
+   int32_t use_electron_pressure; /* Hybrid::useElectronPressure */
+   int32_t isothermal_electrons;  /* Hybrid::useIsothermalElectrons */
+   int32_t use_gravity;           /* Hybrid::useGravity */
+   int32_t use_initial_flow_through;       /* Hybrid::useInitialFlowThrough at start */
+   int32_t n_linear_smoothings_nodeE;      /* Hybrid::N_linearSmoothingsNodeE */
+   int32_t use_gaussian_smoothing_nodeE;   /* Hybrid::useGaussianSmoothingNodeE */
+   int32_t reserved0;
+   double  electron_pressure_coeff;        /* Hybrid::electronPressureCoeff */
+   double  gaussian_coeffs[4];             /* Hybrid::gaussianSmoothingCoeffsNodeE */
+   double  field_obstacle_Ue[3];           /* Hybrid::fieldObstacleUe */
+   double  GMdt;                           /* Hybrid::GMdt */
+   double  max_ion_speed2;                 /* Hybrid::maxIonSpeed2 */
+   double  max_electron_speed2;            /* Hybrid::maxElectronSpeed2 */
+   double  min_ion_charge_density;         /* Hybrid::minIonChargeDensity [C/m^3] */
+   double  max_electric_field2;            /* Hybrid::maxElectricField2 (0: off) */
+   double  max_whistler_speed;             /* Hybrid::maxWhistlerSpeed */
+   double  initial_flow_through_period;    /* Hybrid::initialFlowThroughPeriod [s] */
+   double  imf_B[3];                       /* Hybrid::IMFBx,IMFBy,IMFBz */
+   int32_t imf_boundary_cellB[6];          /* Hybrid::IMFBoundaryCellB (+x -x +y -y +z -z) */
+   int32_t imf_boundary_faceB[6];          /* Hybrid::IMFBoundaryFaceB */
+} rhgpu_params;
+
+/* One ion population (struct Species, src/particle_species.h:75-91). */
+typedef struct rhgpu_species {
+   double  q;            /* charge [C] */
+   double  m;            /* mass [kg] */
+   double  R2_obstacle;  /* squared particle obstacle radius [m^2] (negative: none) */
+   int32_t accumulate;   /* deposit this population */
+   int32_t accelerate;   /* push with the Lorentz force (else drift only) */
+} rhgpu_species;
+
+typedef struct rhgpu_ctx rhgpu_ctx;
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* rhgpu_last_error(void);
+
+/* Version string of the library build (architecture, build flags). */
+const char* rhgpu_version(void);
+
+/* Creates a context on the current CUDA device. Replaces the state that
+ * userLateInitialization (src/user.cpp:356) sets up: grid arrays are
+ * allocated and zeroed (src/user.cpp:1853-1868); particle storage holds up
+ * to capacity[s] particles of species s. The device is cudaSetDevice'd to
+ * `device` first. */
+int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_species* species,
+                 const int64_t* capacity, int32_t device, rhgpu_ctx** out);
+
+/* Frees all device memory of the context. */
+int rhgpu_destroy(rhgpu_ctx* ctx);
+
+/* Uploads one grid array (AoS, dim values per cell, nx*ny*nz cells). */
+int rhgpu_upload_array(rhgpu_ctx* ctx, int32_t array_id, const double* host);
+
+/* Downloads one grid array (AoS, dim values per cell). */
+int rhgpu_download_array(rhgpu_ctx* ctx, int32_t array_id, double* host);
+
+/* Uploads the per-cell flag bytes (RHGPU_FLAG_*). */
+int rhgpu_upload_cell_flags(rhgpu_ctx* ctx, const uint8_t* host);
+
+/* Replaces the particles of species s: counts[n] particles of cell n,
+ * records grouped by cell in linear cell order (7 doubles each). */
+int rhgpu_upload_particles(rhgpu_ctx* ctx, int32_t s, const uint32_t* counts,
+                           const double* particles, int64_t n_particles);
+
+/* Number of particles of species s currently stored. */
+int rhgpu_num_particles(rhgpu_ctx* ctx, int32_t s, int64_t* n_out);
+
+/* Downloads species s (layout as in rhgpu_upload_particles). `capacity` is the
+ * size of `particles` in records; fails with RHGPU_ERR_ARG if too small. */
+int rhgpu_download_particles(rhgpu_ctx* ctx, int32_t s, uint32_t* counts, double* particles,
+                             int64_t capacity, int64_t* n_out);
+
+/* Runs nsteps time steps of propagate() (src/user.cpp:118-134) on the
+ * device: field gather + push, migration, deposit, particle boundary
+ * conditions, propagateB. Host-resident nothing; returns after enqueueing and
+ * checking the device error word once at the end. */
+int rhgpu_step(rhgpu_ctx* ctx, int32_t nsteps);
+
+/* The constituent calls, for a Corsair-style host that drives the plugins
+ * one at a time (BorisBuneman::propagateCell, Accumulator::accumulate*,
+ * ParticleBoundaryCondHybrid::apply, propagateB). rhgpu_step == the
+ * sequence push -> accumulate -> boundary -> propagate_fields. */
+int rhgpu_push(rhgpu_ctx* ctx);              /* all species: gather, push, drift, migrate */
+int rhgpu_accumulate(rhgpu_ctx* ctx);        /* clear, deposit all species, finalize (/dV, clamp) */
+int rhgpu_apply_boundaries(rhgpu_ctx* ctx);  /* exterior-cell and obstacle removal */
+int rhgpu_propagate_fields(rhgpu_ctx* ctx);  /* propagateB */
+
+/* Synchronises and returns the accumulated device error word (RHGPU_DEVERR_*). */
+int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);
+
+/* Counters: RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*n_species doubles. */
+int rhgpu_get_counters(rhgpu_ctx* ctx, double* out, int32_t n);
+
+/* Current simulation time and time-step number (Simulation::t, ::timestep). */
+int rhgpu_get_time(rhgpu_ctx* ctx, double* t_out, int64_t* timestep_out);
+
+/* Device-side FP64 reductions for the field and population logs
+ * (diagnostics.h:187-404): out[0..] = per species {sum w, sum w*vx, sum w*vy,
+ * sum w*vz, sum w*v^2, N macroparticles}, then field {sum faceB^2 over
+ * non-exterior cells, max |cellB|, sum cellRhoQi, max cellRhoQi}. Length
+ * 6*n_species + 4. */
+int rhgpu_reduce_diagnostics(rhgpu_ctx* ctx, double* out, int32_t n);
+
+/* The CUDA stream (cudaStream_t) the context enqueues on. */
+void* rhgpu_stream(rhgpu_ctx* ctx);
+
+/* Per-kernel CUDA-event timing of the last rhgpu_step call: fills names
+ * (comma separated, up to name_cap bytes) and ms (total milliseconds per
+ * kernel class, up to n entries); returns the number of classes in *n_out.
+ * Timing is recorded only when enabled with rhgpu_set_timing(ctx, 1). */
+int rhgpu_set_timing(rhgpu_ctx* ctx, int32_t enable);
+int rhgpu_get_timing(rhgpu_ctx* ctx, char* names, int32_t name_cap, double* ms, int32_t n,
+                     int32_t* n_out);
+
+/* Number of kernel launches issued by the last rhgpu_step call. */
+int rhgpu_last_launch_count(rhgpu_ctx* ctx, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

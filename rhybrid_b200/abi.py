@@ -1,0 +1,330 @@
+"""ctypes binding of the C ABI declared in include/rhgpu.h.
+
+The same entry-point set is exported under three prefixes:
+  rhgpu_  the B200 library (rhybrid_b200/librhgpu.so, the product),
+  rho_    the C restatement of the reference algorithm (oracle, tests only),
+  rhref_  the reference's own sources built against the oracle shim (tests only).
+`Library` binds any of them; the package itself only ever loads rhgpu_.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+# rhgpu.h: status codes
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_DEVICE, ERR_NOMEM, ERR_CAPACITY = range(7)
+
+# rhgpu.h: device error bits
+DEVERR_NAN_PARTICLE = 1
+DEVERR_FAST_PARTICLE = 2
+DEVERR_CAPACITY = 4
+
+# rhgpu.h: cell flag bits
+FLAG_INNER_FIELD = 1
+FLAG_INNER_NODE = 2
+FLAG_INNER_PARTICLE = 4
+FLAG_INNER_CELLEP = 8
+
+# rhgpu.h: rhgpu_array_id
+ARRAYS = [
+    "faceB", "cellB", "cellUe", "cellEp", "cellRhoQi", "cellJi", "cellJ",
+    "nodeRhoQi", "nodeJi", "nodeJ", "nodeUe", "nodeB", "nodeE", "nodeEta", "cellAverageB",
+]
+ARRAY_ID = {n: i for i, n in enumerate(ARRAYS)}
+SCALAR_ARRAYS = {"cellRhoQi", "nodeRhoQi", "nodeEta"}
+
+# rhgpu.h: rhgpu_counter_id
+FIELD_COUNTERS = [
+    "fieldMinCellRhoQi", "fieldMaxCellUe", "fieldMaxNodeUe", "fieldMaxVw", "fieldMaxE",
+    "fieldMinNodeRhoQi", "gridTemporalAverageCounter",
+]
+SPECIES_COUNTERS = ["particleMaxVi", "particleEscape", "particleEscapeKineticEnergy",
+                    "particleImpact", "particleImpactKineticEnergy"]
+
+# rhgpu.h: physical constants
+PERMEABILITY = 1.2566370614359173e-06
+CHARGE_ELEMENTARY = 1.602176634e-19
+MASS_PROTON = 1.67262192369e-27
+BOLTZMANN = 1.380649e-23
+GRAVITY = 6.67430e-11
+
+
+class Params(C.Structure):
+    """struct rhgpu_params"""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("periodic", C.c_int32 * 3),
+        ("x_min", C.c_double), ("y_min", C.c_double), ("z_min", C.c_double),
+        ("dx", C.c_double), ("dt", C.c_double), ("t_initial", C.c_double),
+        ("use_hall", C.c_int32), ("use_electron_pressure", C.c_int32),
+        ("isothermal_electrons", C.c_int32), ("use_gravity", C.c_int32),
+        ("use_initial_flow_through", C.c_int32), ("n_linear_smoothings_nodeE", C.c_int32),
+        ("use_gaussian_smoothing_nodeE", C.c_int32), ("reserved0", C.c_int32),
+        ("electron_pressure_coeff", C.c_double),
+        ("gaussian_coeffs", C.c_double * 4),
+        ("field_obstacle_Ue", C.c_double * 3),
+        ("GMdt", C.c_double),
+        ("max_ion_speed2", C.c_double),
+        ("max_electron_speed2", C.c_double),
+        ("min_ion_charge_density", C.c_double),
+        ("max_electric_field2", C.c_double),
+        ("max_whistler_speed", C.c_double),
+        ("initial_flow_through_period", C.c_double),
+        ("imf_B", C.c_double * 3),
+        ("imf_boundary_cellB", C.c_int32 * 6),
+        ("imf_boundary_faceB", C.c_int32 * 6),
+    ]
+
+
+class Species(C.Structure):
+    """struct rhgpu_species"""
+    _fields_ = [
+        ("q", C.c_double), ("m", C.c_double), ("R2_obstacle", C.c_double),
+        ("accumulate", C.c_int32), ("accelerate", C.c_int32),
+    ]
+
+
+class RhError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_U32 = C.POINTER(C.c_uint32)
+_U8 = C.POINTER(C.c_uint8)
+_I64 = C.POINTER(C.c_int64)
+
+# entry point -> argtypes (all return int32 status unless listed in _RESTYPES)
+_SIGNATURES = {
+    "create": [C.POINTER(Params), C.c_int32, C.POINTER(Species), _I64, C.c_int32, C.POINTER(_P)],
+    "destroy": [_P],
+    "upload_array": [_P, C.c_int32, _D],
+    "download_array": [_P, C.c_int32, _D],
+    "upload_cell_flags": [_P, _U8],
+    "upload_particles": [_P, C.c_int32, _U32, _D, C.c_int64],
+    "num_particles": [_P, C.c_int32, _I64],
+    "download_particles": [_P, C.c_int32, _U32, _D, C.c_int64, _I64],
+    "step": [_P, C.c_int32],
+    "push": [_P],
+    "accumulate": [_P],
+    "apply_boundaries": [_P],
+    "propagate_fields": [_P],
+    "get_counters": [_P, _D, C.c_int32],
+    "get_time": [_P, _D, _I64],
+    "last_error": [],
+}
+_OPTIONAL = {
+    "device_errors": [_P, _U32],
+    "reduce_diagnostics": [_P, _D, C.c_int32],
+    "set_timing": [_P, C.c_int32],
+    "get_timing": [_P, C.c_char_p, C.c_int32, _D, C.c_int32, C.POINTER(C.c_int32)],
+    "last_launch_count": [_P, _I64],
+    "stream": [_P],
+    "version": [],
+    "set_deposit_order": [_P, C.c_int32],
+    "set_threads": [_P, C.c_int32],
+}
+_RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p}
+
+
+def _ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class Library:
+    """A loaded implementation of the rhgpu C ABI under some prefix."""
+
+    def __init__(self, path: str, prefix: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.prefix = prefix
+        self.dll = C.CDLL(path)
+        self.fn = {}
+        for name, argt in list(_SIGNATURES.items()) + list(_OPTIONAL.items()):
+            sym = prefix + name
+            if not hasattr(self.dll, sym):
+                if name in _SIGNATURES:
+                    raise RuntimeError(f"{path}: missing symbol {sym}")
+                continue
+            f = getattr(self.dll, sym)
+            f.argtypes = argt
+            f.restype = _RESTYPES.get(name, C.c_int32)
+            self.fn[name] = f
+
+    def has(self, name: str) -> bool:
+        return name in self.fn
+
+    def last_error(self) -> str:
+        s = self.fn["last_error"]()
+        return s.decode() if s else ""
+
+    def call(self, name: str, *args) -> int:
+        rc = self.fn[name](*args)
+        if rc != OK:
+            raise RhError(rc, f"{self.prefix}{name}: {self.last_error()}")
+        return rc
+
+
+class Context:
+    """One simulation context of a Library (rhgpu_ctx*)."""
+
+    def __init__(self, lib: Library, params: Params, species: list, capacity=None, device: int = 0):
+        self.lib = lib
+        self.params = params
+        self.nspecies = len(species)
+        self.ncells = params.nx * params.ny * params.nz
+        arr = (Species * len(species))(*species)
+        cap = np.asarray(capacity if capacity is not None else [0] * len(species), dtype=np.int64)
+        h = C.c_void_p()
+        lib.call("create", C.byref(params), len(species), arr, _ptr(cap, C.c_int64), device, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call("destroy", self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # grid arrays -----------------------------------------------------
+    def upload_array(self, name: str, data: np.ndarray):
+        dim = 1 if name in SCALAR_ARRAYS else 3
+        a = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+        if a.size != dim * self.ncells:
+            raise ValueError(f"{name}: expected {dim * self.ncells} values, got {a.size}")
+        self.lib.call("upload_array", self.h, ARRAY_ID[name], _ptr(a, C.c_double))
+
+    def download_array(self, name: str) -> np.ndarray:
+        dim = 1 if name in SCALAR_ARRAYS else 3
+        out = np.empty(dim * self.ncells, dtype=np.float64)
+        self.lib.call("download_array", self.h, ARRAY_ID[name], _ptr(out, C.c_double))
+        return out if dim == 1 else out.reshape(self.ncells, 3)
+
+    def upload_cell_flags(self, flags: np.ndarray):
+        f = np.ascontiguousarray(flags, dtype=np.uint8).reshape(-1)
+        assert f.size == self.ncells
+        self.lib.call("upload_cell_flags", self.h, _ptr(f, C.c_uint8))
+
+    # particles -------------------------------------------------------
+    def upload_particles(self, s: int, counts: np.ndarray, particles: np.ndarray):
+        cnt = np.ascontiguousarray(counts, dtype=np.uint32)
+        p = np.ascontiguousarray(particles, dtype=np.float64).reshape(-1, 7)
+        assert cnt.size == self.ncells
+        self.lib.call("upload_particles", self.h, s, _ptr(cnt, C.c_uint32), _ptr(p, C.c_double), p.shape[0])
+
+    def num_particles(self, s: int) -> int:
+        n = C.c_int64()
+        self.lib.call("num_particles", self.h, s, C.byref(n))
+        return n.value
+
+    def download_particles(self, s: int):
+        n = self.num_particles(s)
+        cnt = np.empty(self.ncells, dtype=np.uint32)
+        p = np.empty((max(n, 1), 7), dtype=np.float64)
+        nout = C.c_int64()
+        self.lib.call("download_particles", self.h, s, _ptr(cnt, C.c_uint32), _ptr(p, C.c_double), p.shape[0],
+                      C.byref(nout))
+        return cnt, p[: nout.value]
+
+    # stepping --------------------------------------------------------
+    def step(self, n: int = 1):
+        self.lib.call("step", self.h, n)
+
+    def push(self):
+        self.lib.call("push", self.h)
+
+    def accumulate(self):
+        self.lib.call("accumulate", self.h)
+
+    def apply_boundaries(self):
+        self.lib.call("apply_boundaries", self.h)
+
+    def propagate_fields(self):
+        self.lib.call("propagate_fields", self.h)
+
+    def counters(self) -> dict:
+        n = len(FIELD_COUNTERS) + len(SPECIES_COUNTERS) * self.nspecies
+        out = np.zeros(n, dtype=np.float64)
+        self.lib.call("get_counters", self.h, _ptr(out, C.c_double), n)
+        d = {k: out[i] for i, k in enumerate(FIELD_COUNTERS)}
+        for s in range(self.nspecies):
+            for j, k in enumerate(SPECIES_COUNTERS):
+                d[f"{k}[{s}]"] = out[len(FIELD_COUNTERS) + len(SPECIES_COUNTERS) * s + j]
+        return d
+
+    def time(self):
+        t = C.c_double()
+        ts = C.c_int64()
+        self.lib.call("get_time", self.h, C.byref(t), C.byref(ts))
+        return t.value, ts.value
+
+    def device_errors(self) -> int:
+        w = C.c_uint32()
+        self.lib.call("device_errors", self.h, C.byref(w))
+        return w.value
+
+    def reduce_diagnostics(self) -> np.ndarray:
+        n = 6 * self.nspecies + 4
+        out = np.zeros(n, dtype=np.float64)
+        self.lib.call("reduce_diagnostics", self.h, _ptr(out, C.c_double), n)
+        return out
+
+    def set_timing(self, on: bool):
+        self.lib.call("set_timing", self.h, 1 if on else 0)
+
+    def timing(self) -> dict:
+        names = C.create_string_buffer(4096)
+        ms = np.zeros(64, dtype=np.float64)
+        n = C.c_int32()
+        self.lib.call("get_timing", self.h, names, 4096, _ptr(ms, C.c_double), 64, C.byref(n))
+        keys = names.value.decode().split(",") if names.value else []
+        return {k: ms[i] for i, k in enumerate(keys[: n.value])}
+
+    def last_launch_count(self) -> int:
+        n = C.c_int64()
+        self.lib.call("last_launch_count", self.h, C.byref(n))
+        return n.value
+
+    def stream(self) -> int:
+        return self.lib.fn["stream"](self.h) or 0
+
+    def set_deposit_order(self, order: int):
+        self.lib.call("set_deposit_order", self.h, order)
+
+    def set_threads(self, n: int):
+        self.lib.call("set_threads", self.h, n)
+
+
+_GPU_LIB: Optional[Library] = None
+
+
+def gpu_library_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "librhgpu.so")
+
+
+def gpu_library() -> Library:
+    """Loads the B200 library; raises if it has not been built. There is no
+    fallback: without the CUDA library the package cannot run the hot path."""
+    global _GPU_LIB
+    if _GPU_LIB is None:
+        path = gpu_library_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"rhybrid_b200: CUDA library {path} not built (run __graft_entry__.build())")
+        _GPU_LIB = Library(path, "rhgpu_")
+    return _GPU_LIB
