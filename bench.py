@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the RHybrid hot path on B200.
+
+Workload (default): the plain FP64 Mars-like obstacle run, 120x160x160 cells of
+300 km, absorbing sphere r=3390 km, solar-wind H+ (n=2e6 m^-3, 30 ppc) and He++
+(4 %, 1.5 ppc), V=-450 km/s, T=1e5 K, IMF (0,3,0) nT, dt=0.05 s; about 9.7e7
+ions. Inputs are synthetic (seeded uniform-in-cell Maxwellian fill, the
+reference's InjectorUniform), generated on the host.
+
+A step is one propagate(): push + migration + deposit + particle boundary
+conditions + field update, for all populations.
+
+  value   particle-steps/s over all GPUs, state resident in HBM (> L2, no flush needed)
+  e2e     the same metric through the C ABI with the state in pinned host memory
+          each step: upload of all particles, one step, download of the
+          particles and of rhoq, Ji, faceB (the round trip of a host that keeps
+          ownership of the particle lists, as Corsair/ParGrid does)
+
+--impl reference times the reference's own hot-path sources (oracle/_ref,
+compiled from the reference tree) on the host cores, as independent
+processes on sub-boxes of the same workload.
+
+Multi-GPU: replicas only (one independent run per GPU, no collective on the
+data path); timing is the maximum over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload(name, scale=1.0):
+    from rhybrid_b200 import config as cf
+    if name == "mars":
+        if scale == 1.0:
+            return cf.config_mars()
+        f = scale ** (1.0 / 3.0)
+        return cf.config_mars(nx=max(8, int(round(120 * f))), ny=max(8, int(round(160 * f))),
+                              nz=max(8, int(round(160 * f))))
+    if name == "empty_box":
+        return cf.config_empty_box(32, 32, 32, ppc=20.0)
+    raise ValueError(name)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own sources (oracle/_ref), one process per core
+
+def _cpu_worker(args):
+    """Runs `steps` steps of a sub-box of the workload in the reference build
+    (or the oracle port) and returns (particle_steps, seconds)."""
+    kind, wl, nz_sub, steps, warm = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    from rhybrid_b200 import abi
+    from rhybrid_b200 import config as cf
+    lib = oracle.reference() if kind == "reference" else oracle.port()
+    full = workload(wl)
+    # a slab through the middle of the box, periodic across its thickness so
+    # that its cells do the same work per ion as interior cells of the full run
+    cfg = full.replace(nz=nz_sub, z_min=-0.5 * nz_sub * full.dx,
+                       periodic=(full.periodic[0], full.periodic[1], 1))
+    grid, pops = cf.initial_state(cfg)
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg))
+    try:
+        ctx.upload_array("faceB", grid["faceB"])
+        ctx.upload_array("cellB", grid["cellB"])
+        ctx.upload_array("nodeEta", grid["nodeEta"])
+        ctx.upload_cell_flags(grid["flags"])
+        for s, (c, p) in enumerate(pops):
+            ctx.upload_particles(s, c, p)
+        for _ in range(warm):
+            ctx.step(1)
+        times, psteps = [], []
+        for _ in range(steps):
+            n = sum(ctx.num_particles(s) for s in range(len(pops)))
+            t0 = time.perf_counter()
+            ctx.step(1)
+            times.append(time.perf_counter() - t0)
+            psteps.append(n)
+        return psteps, times
+    finally:
+        ctx.close()
+
+
+def cpu_measure(wl, steps, warm, budget_cores=None, nz_sub=None):
+    """All host cores, one reference process per core, each on a slab of the
+    workload (nz_sub cells thick). Returns per-step aggregate rates."""
+    import multiprocessing as mp
+    from oracle import oracle
+    kind = "reference" if oracle.reference() is not None else "port"
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    if budget_cores:
+        cores = min(cores, budget_cores)
+    full = workload(wl)
+    if nz_sub is None:
+        nz_sub = max(3, min(full.nz, 4))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(kind, wl, nz_sub, steps, warm)] * cores)
+    rates = []
+    for st in range(steps):
+        tot = sum(r[0][st] for r in res)
+        wall = max(r[1][st] for r in res)
+        rates.append(tot / wall)
+    return {"kind": kind, "cores": cores, "rates": rates, "nz_sub": nz_sub,
+            "particles_per_core": res[0][0][0] if res and res[0][0] else 0}
+
+
+# ---------------------------------------------------------------------------
+
+def algorithmic_bytes(cfg, n_particles):
+    """Bytes the plain FP64 step must move (per step): 56 B read + 48 B
+    written per particle, and per cell 7 doubles read (faceB, rhoq, Ji) and
+    10 written (faceB, cellUe, rhoq, Ji), plus 6 for cellEp with electron
+    pressure on."""
+    per_cell = 136 + (48 if cfg.use_electron_pressure else 0)
+    return 104 * n_particles + per_cell * cfg.ncells
+
+
+KERNEL_BYTES = {
+    # algorithmic bytes per launch of the dominant kernels (units: particles p, cells c)
+    "push": lambda p, c: 96 * p + 72 * c,
+    "mig_scatter": lambda p, c: 112 * p,
+    "deposit_cell": lambda p, c: 56 * p + 32 * c,
+    "deposit_gather": lambda p, c: 32 * c,
+}
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    from rhybrid_b200 import abi
+    from rhybrid_b200 import config as cf
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    cfg = workload(args.workload, args.scale)
+    t0 = time.time()
+    grid, pops = cf.initial_state(cfg)
+    gen_s = time.time() - t0
+    lib = abi.gpu_library()
+    nps = [p[1].shape[0] for p in pops]
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + 1024 for n in nps], device=local_rank)
+    ctx.upload_array("faceB", grid["faceB"])
+    ctx.upload_array("cellB", grid["cellB"])
+    ctx.upload_array("nodeEta", grid["nodeEta"])
+    ctx.upload_cell_flags(grid["flags"])
+    for s, (c, p) in enumerate(pops):
+        ctx.upload_particles(s, c, p)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local_rank)
+    for _ in range(args.warmup):
+        ctx.step(1)
+    n0 = sum(ctx.num_particles(s) for s in range(len(pops)))
+    ctx.set_timing(True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = ctx.last_launch_count()
+    ktimes = ctx.timing()
+    ctx.set_timing(False)
+    n1 = sum(ctx.num_particles(s) for s in range(len(pops)))
+    psteps = 0.5 * (n0 + n1) * args.steps
+    if dist:
+        t = torch.tensor([ms, psteps], dtype=torch.float64, device="cuda")
+        tmax = t[0:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t[1:2].clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms_all, psteps_all = float(tmax.item()), float(tsum.item())
+    else:
+        ms_all, psteps_all = ms, psteps
+    value = psteps_all / (ms_all / 1e3)
+
+    # roofline of the dominant kernel class
+    peak, peak_kind = hbm_peak()
+    top = max(ktimes.items(), key=lambda kv: kv[1]) if ktimes else ("none", 0.0)
+    nlaunch_top = args.steps * (len(pops) if top[0] in ("push", "mig_scatter", "deposit_cell", "deposit_gather") else 1)
+    per_launch_ms = top[1] / max(nlaunch_top, 1)
+    roof = None
+    if top[0] in KERNEL_BYTES and per_launch_ms > 0:
+        # bytes of one launch: the first species dominates the particle count
+        pcount = 0.5 * (n0 + n1) / len(pops)
+        alg = KERNEL_BYTES[top[0]](pcount, cfg.ncells)
+        ach = alg / (per_launch_ms / 1e3) / 1e9
+        roof = {"kernel": top[0], "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "ms_per_launch": round(per_launch_ms, 4)}
+    step_alg = algorithmic_bytes(cfg, 0.5 * (n0 + n1))
+    step_ach = step_alg / ((ms / args.steps) / 1e3) / 1e9
+
+    # end to end through the C ABI with host-resident state (rank-local)
+    e2e = None
+    if not args.no_e2e:
+        cnts, parts = [], []
+        for s in range(len(pops)):
+            c, p = ctx.download_particles(s)
+            pin = torch.empty((max(p.shape[0], 1), 7), dtype=torch.float64, pin_memory=True).numpy()[: p.shape[0]]
+            pin[:] = p
+            cnts.append(c)
+            parts.append(pin)
+        out_pin = [torch.empty((max(p.shape[0], 1), 7), dtype=torch.float64, pin_memory=True).numpy() for p in parts]
+        ke = max(1, min(3, args.steps))
+        h2d = sum(p.nbytes + c.nbytes for p, c in zip(parts, cnts))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        e2e_ps = 0
+        for _ in range(ke):
+            for s in range(len(pops)):
+                ctx.upload_particles(s, cnts[s], parts[s])
+                e2e_ps += parts[s].shape[0]
+            ctx.step(1)
+            d2h = 0
+            for s in range(len(pops)):
+                n = ctx.num_particles(s)
+                if n > out_pin[s].shape[0]:
+                    out_pin[s] = np.empty((n, 7))
+                cnt = np.empty(cfg.ncells, dtype=np.uint32)
+                nout = abi.C.c_int64()
+                lib.call("download_particles", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
+                         abi._ptr(out_pin[s], abi.C.c_double), out_pin[s].shape[0], abi.C.byref(nout))
+                d2h += nout.value * 56 + cnt.nbytes
+            for name in ("cellRhoQi", "cellJi", "faceB"):
+                d2h += ctx.download_array(name).nbytes
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t1
+        if dist:
+            t = torch.tensor([e2e_s, float(e2e_ps)], dtype=torch.float64, device="cuda")
+            tm = t[0:1].clone()
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+            ts = t[1:2].clone()
+            dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+            e2e_s, e2e_ps = float(tm.item()), float(ts.item())
+        e2e = {"value": e2e_ps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": ke}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        m = cpu_measure(args.workload, steps=1, warm=0)
+        cpu = {"value": round(m["rates"][0], 1), "unit": "particle-steps/s", "cores": m["cores"], "kind": m["kind"],
+               "sample": f"{m['cores']} processes, each one step of a 120x160x{m['nz_sub']} slab of the workload "
+                         f"({m['particles_per_core']} ions per process), reference hot-path sources built with "
+                         f"g++ -O2 -ffp-contract=off"}
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": round(value, 1), "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_all / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform)",
+            "config": {"workload": cfg.name, "cells": [cfg.nx, cfg.ny, cfg.nz], "dx_m": cfg.dx, "dt_s": cfg.dt,
+                       "ions": int(0.5 * (n0 + n1)), "species": [p.name for p in cfg.populations],
+                       "parallelism": f"replicas x{world}", "l2": "state 10+ GB > 126 MB L2, no flush needed",
+                       "sim_s_per_wall_s": round(args.steps * cfg.dt / (ms_all / 1e3), 4),
+                       "step_roofline": {"achieved_gbs": round(step_ach, 1), "alg_bytes_per_step": int(step_alg),
+                                         "frac": round(step_ach / peak, 4)},
+                       "kernel_ms": {k: round(v / args.steps, 4) for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1])},
+                       "init_gen_s": round(gen_s, 1)},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    m = cpu_measure(args.workload, steps=args.steps, warm=args.warmup)
+    rates = m["rates"]
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": round(value, 1), "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform-in-cell Maxwellian fill)",
+        "config": {"workload": workload(args.workload).name, "sample": f"slabs 120x160x{m['nz_sub']}"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "particle-steps/s", "cores": m["cores"], "kind": m["kind"],
+                         "sample": f"{m['cores']} processes of the reference hot path, each on a 120x160x{m['nz_sub']} "
+                                   f"slab ({m['particles_per_core']} ions), median of {len(rates)} steps"},
+        "e2e": {"value": round(value, 1), "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="mars", choices=["mars", "empty_box"])
+    ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's cells (testing only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

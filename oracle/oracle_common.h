@@ -15,11 +15,12 @@
  * A particle still outside [0,dx) after one shift moved more than one cell in
  * a step; it is removed and counted (the maximum ion speed of 0.9 dx/dt,
  * src/user.cpp:1774-1777, keeps accelerated particles below one cell).
- * In the destination cell, particles are ordered by the direction they came
- * from (dir = (dz+1)*9 + (dy+1)*3 + (dx+1) with (dx,dy,dz) = source cell -
- * destination cell, so stayers have dir 13), then by their order in the
- * source cell. For cells away from periodic wraps this is a stable sort of
- * the old particle order by the new cell index.
+ * In the destination cell, the particles that stayed come first, in their
+ * previous order; then the arrivals, grouped by the direction they came from
+ * (dir = (dz+1)*9 + (dy+1)*3 + (dx+1) with (dx,dy,dz) = source cell -
+ * destination cell; stayers have dir 13) in increasing dir, each group in its
+ * order inside the source cell. rh_dir_rank() gives the position of a dir in
+ * that sequence.
  */
 #ifndef RH_ORACLE_COMMON_H
 #define RH_ORACLE_COMMON_H
@@ -36,6 +37,10 @@ static inline int rh_wrap(int* i,int n,int periodic) {
 static inline double rh_block_origin(double xmin,int i,double dx) { return xmin + (double)i*dx; }
 
 static inline int rh_dir_from_offset(int dxs,int dys,int dzs) { return (dzs+1)*9 + (dys+1)*3 + (dxs+1); }
+
+/* order of a direction group inside the destination cell: stayers (dir 13)
+ * first, then dir 0..12, 14..26 */
+static inline int rh_dir_rank(int dir) { return dir == 13 ? 0 : (dir < 13 ? dir + 1 : dir); }
 
 /* shifts r into [0,dx) by at most one cell per axis; off[a] in {-1,0,1};
  * returns nonzero if the particle moved more than one cell */

@@ -133,9 +133,9 @@ void setHybridStatics(RefCtx& c) {
 
 void migrate(RefCtx& c,int s) {
    /* the particle lists are rebuilt in the canonical order of
-    * rh_migrate_canonical (oracle_common.h): destination cell, then the
-    * direction the particle came from (0..26, stayers at 13), then the
-    * order inside the source cell */
+    * rh_migrate_canonical (oracle_common.h): destination cell, then
+    * rh_dir_rank of the direction the particle came from (stayers first),
+    * then the order inside the source cell */
    pargrid::DataWrapper<PARTICLE> w = c.sc.pargrid.getUserDataDynamic<PARTICLE>(c.particleIDs[s]);
    const int nx = c.P.nx, ny = c.P.ny, nz = c.P.nz;
    const size_t N = (size_t)nx*ny*nz;
@@ -160,7 +160,7 @@ void migrate(RefCtx& c,int s) {
             continue;
          }
          q.state[particle::X] = r[0]; q.state[particle::Y] = r[1]; q.state[particle::Z] = r[2];
-         const int dir = rh_dir_from_offset(-off[0],-off[1],-off[2]);
+         const int dir = rh_dir_rank(rh_dir_from_offset(-off[0],-off[1],-off[2]));
          const size_t d = (size_t)ti + nx*((size_t)tj + ny*(size_t)tk);
          all.push_back(q);
          key.push_back((int64_t)d*27 + dir);

@@ -320,7 +320,7 @@ static void migrate(Ctx* c,int sidx) {
             continue;
          }
          const size_t d = (size_t)ti + c->nx*((size_t)tj + c->ny*(size_t)tk);
-         key[p] = (int64_t)d*27 + rh_dir_from_offset(-off[0],-off[1],-off[2]);
+         key[p] = (int64_t)d*27 + rh_dir_rank(rh_dir_from_offset(-off[0],-off[1],-off[2]));
       }
    }
    int64_t* start = (int64_t*)calloc(N*27+1,sizeof(int64_t));

@@ -1,0 +1,342 @@
+// Particle kernels of the bit-exact path (sm_100a, FP64):
+//   k_push            BorisBuneman::propagate + getFields (particle_propagator_boris_buneman.h:64-194,
+//                     hybrid_propagator.cpp:1740-1891) and the migration decision
+//   k_mig_count / k_mig_incount / k_mig_scatter
+//                     stable counting sort of the particles into their new cells
+//   k_deposit_cell    Accumulator::accumulateCell (particle_accumulator.cpp:44-156): per cell, the
+//                     3x3x3 CIC sums in particle order
+//   k_deposit_gather  block::addValues3D in increasing source-cell order + finalize (:319-333)
+//   k_bc_exterior / k_bc_obstacle   ParticleBoundaryCondHybrid::apply (particle_boundary_cond_hybrid.h:112-185)
+// Particle storage per species, structure of arrays in HBM (7 doubles), grouped
+// by cell: cell c owns slots [start[c], start[c+1]); the first alive[c] of them
+// hold particles, pcell[p] is the cell of slot p or -1 for an empty slot.
+#pragma once
+
+#include "rh_device.cuh"
+#include "k_fields.cuh"
+
+namespace rh {
+
+struct PStore {
+   double* a[7];        // x, y, z (cell-local), vx, vy, vz, weight
+   int* pcell;          // cell of each slot, -1 if empty
+   long long* start;    // N+1 slot offsets
+   int* alive;          // alive particles per cell (a prefix of its slots)
+   long long nslots;
+   long long cap;
+};
+
+struct SpeciesDev {
+   double q, m, R2obs, qmideltT2;
+   int accelerate, accumulate;
+};
+
+struct PushParams {
+   int useIFT, use_ep, use_gravity;
+   double GMdt, maxVi2;
+};
+
+// device error word bits
+__device__ inline void raiseError(unsigned* err, unsigned bit) { atomicOr(err, bit); }
+
+__global__ void k_push(GridInfo g, Fields f, PStore P, SpeciesDev sp, PushParams pp, int* key,
+                       unsigned long long* cnt, double* cntd, unsigned* err, int sidx) {
+   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (p >= P.nslots) return;
+   const int c = P.pcell[p];
+   if (c < 0) { key[p] = -1; return; }
+   const long long N = g.N;
+   const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+   double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
+   double vx = P.a[3][p], vy = P.a[4][p], vz = P.a[5][p];
+   bool clamp = false;
+   const bool accelerate = sp.accelerate && !pp.useIFT && allNb(g, i, j, k);
+   if (accelerate) {
+      const double dx = g.dx;
+      double B[3], Ue[3], E[3];
+      {
+         const double xs = x / dx, ys = y / dx, zs = z / dx;
+         // positions in [0,dx) give floor()==0 (see oracle: the quotient never rounds up to 1)
+         const double w111x = xs - 0.0, w111y = ys - 0.0, w111z = zs - 0.0;
+         const double w011x = 1.0 - xs, w101y = 1.0 - ys, w110z = 1.0 - zs;
+         B[0] = w111x * f.faceB[0 * N + c] + w011x * f.faceB[0 * N + nbr(g, i, j, k, -1, 0, 0)];
+         B[1] = w111y * f.faceB[1 * N + c] + w101y * f.faceB[1 * N + nbr(g, i, j, k, 0, -1, 0)];
+         B[2] = w111z * f.faceB[2 * N + c] + w110z * f.faceB[2 * N + nbr(g, i, j, k, 0, 0, -1)];
+      }
+      for (int l = 0; l < 3; ++l) Ue[l] = f.cellUe[l * N + c];
+      E[0] = B[1] * Ue[2] - B[2] * Ue[1];
+      E[1] = B[2] * Ue[0] - B[0] * Ue[2];
+      E[2] = B[0] * Ue[1] - B[1] * Ue[0];
+      if (pp.use_ep) for (int l = 0; l < 3; ++l) E[l] += f.cellEp[l * N + c];
+      const double qm = sp.qmideltT2;
+      const double dvx = qm * E[0], dvy = qm * E[1], dvz = qm * E[2];
+      const double tx = qm * B[0], ty = qm * B[1], tz = qm * B[2];
+      const double t2 = tx * tx + ty * ty + tz * tz;
+      const double b2 = 2. / (1. + t2);
+      const double sx = b2 * tx, sy = b2 * ty, sz = b2 * tz;
+      const double vmx = vx + dvx, vmy = vy + dvy, vmz = vz + dvz;
+      const double v0x = vmx + vmy * tz - vmz * ty;
+      const double v0y = vmy + vmz * tx - vmx * tz;
+      const double v0z = vmz + vmx * ty - vmy * tx;
+      const double vpx = vmx + v0y * sz - v0z * sy;
+      const double vpy = vmy + v0z * sx - v0x * sz;
+      const double vpz = vmz + v0x * sy - v0y * sx;
+      vx = vpx + dvx; vy = vpy + dvy; vz = vpz + dvz;
+      if (pp.use_gravity) {
+         const double xg = x + blockOrigin(g.x_min, i, dx), yg = y + blockOrigin(g.y_min, j, dx),
+                      zg = z + blockOrigin(g.z_min, k, dx);
+         const double rr = sqrt(sq(xg) + sq(yg) + sq(zg));
+         const double r3 = rr * rr * rr;
+         if (r3 > 0) {
+            const double s = -pp.GMdt / r3;
+            vx += s * xg; vy += s * yg; vz += s * zg;
+         }
+      }
+      const double v2 = sq(vx) + sq(vy) + sq(vz);
+      if (v2 > pp.maxVi2) {
+         const double norm = sqrt(pp.maxVi2 / v2);
+         vx *= norm; vy *= norm; vz *= norm;
+         clamp = true;
+      }
+   }
+   countIf(clamp, &cnt[CNT_SPECIES_MAXVI + sidx]);
+   x += g.dt * vx;
+   y += g.dt * vy;
+   z += g.dt * vz;
+   if (isnan(x) || isnan(y) || isnan(z)) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
+   int ox, oy, oz;
+   int st = migrateAxis(x, ox, g.dx, g.dx_below);
+   st |= migrateAxis(y, oy, g.dx, g.dx_below);
+   st |= migrateAxis(z, oz, g.dx, g.dx_below);
+   int ti = i + ox, tj = j + oy, tk = k + oz;
+   const bool inside = wrapc(ti, g.nx, g.per[0]) && wrapc(tj, g.ny, g.per[1]) && wrapc(tk, g.nz, g.per[2]);
+   P.a[0][p] = x; P.a[1][p] = y; P.a[2][p] = z;
+   P.a[3][p] = vx; P.a[4][p] = vy; P.a[5][p] = vz;
+   if (st || !inside) {
+      const double w = P.a[6][p];
+      atomicAdd(&cntd[4 * sidx + 0], w);
+      atomicAdd(&cntd[4 * sidx + 1], w * (sq(vx) + sq(vy) + sq(vz)));
+      key[p] = -1;
+      return;
+   }
+   const long long d = cidx(g, ti, tj, tk);
+   key[p] = (int)(d * 27 + dirRank(dirFromOffset(-ox, -oy, -oz)));
+}
+
+// per source cell: counts per destination-direction rank, and the rank of
+// each particle inside its (source, direction) group
+__global__ void k_mig_count(GridInfo g, PStore P, const int* key, int* outCount, int* rank) {
+   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (c >= g.N) return;
+   int run[27];
+   for (int r = 0; r < 27; ++r) run[r] = 0;
+   const long long a = P.start[c], e = P.start[c + 1];
+   for (long long p = a; p < e; ++p) {
+      const int kk = key[p];
+      if (kk < 0) continue;
+      const int r = kk % 27;
+      rank[p] = run[r]++;
+   }
+   for (int r = 0; r < 27; ++r) outCount[(long long)r * g.N + c] = run[r];
+}
+
+// per destination cell: arrivals per direction rank (exclusive prefix) and total
+__global__ void k_mig_incount(GridInfo g, const int* outCount, int* inPrefix, long long* newCount) {
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const int j = blockIdx.y * blockDim.y + threadIdx.y;
+   const int k = blockIdx.z;
+   if (i >= g.nx || j >= g.ny) return;
+   const long long d = cidx(g, i, j, k);
+   int run = 0;
+   for (int r = 0; r < 27; ++r) {
+      const int dir = rankToDir(r);
+      const int sx = dir % 3 - 1, sy = (dir / 3) % 3 - 1, sz = dir / 9 - 1;
+      const long long s = nbr(g, i, j, k, sx, sy, sz);
+      inPrefix[(long long)r * g.N + d] = run;
+      if (s >= 0) run += outCount[(long long)r * g.N + s];
+   }
+   newCount[d] = run;
+}
+
+__global__ void k_mig_scatter(GridInfo g, PStore P, PStore Q, const int* key, const int* rank,
+                              const int* inPrefix, const long long* newStart, unsigned* err) {
+   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (p >= P.nslots) return;
+   const int kk = key[p];
+   if (kk < 0) return;
+   const long long d = kk / 27;
+   const int r = kk % 27;
+   const long long pos = newStart[d] + inPrefix[(long long)r * g.N + d] + rank[p];
+   if (pos < 0 || pos >= Q.cap) { raiseError(err, RHGPU_DEVERR_CAPACITY); return; }
+   for (int a = 0; a < 7; ++a) Q.a[a][pos] = P.a[a][p];
+   Q.pcell[pos] = (int)d;
+}
+
+__global__ void k_set_alive_from_count(long long N, const long long* cnt, int* alive) {
+   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (c < N) alive[c] = (int)cnt[c];
+}
+
+// CIC weights of one particle (particle_accumulator.cpp:68-110), corners in
+// the order 000,100,010,110,001,101,011,111 with their 3x3x3 indices
+__device__ inline void cicWeights(double x, double y, double z, double wq, double dx, double w8[8], int ind[8]) {
+   int i = (int)floor(x / dx), j = (int)floor(y / dx), k = (int)floor(z / dx);
+   if (x < (i + 0.5) * dx) { --i; }
+   if (y < (j + 0.5) * dx) { --j; }
+   if (z < (k + 0.5) * dx) { --k; }
+   ++i; ++j; ++k;
+   const double x0 = (i - 1 + 0.5) * dx, y0 = (j - 1 + 0.5) * dx, z0 = (k - 1 + 0.5) * dx;
+   const double w_x = (x - x0) / dx, w_y = (y - y0) / dx, w_z = (z - z0) / dx;
+   w8[0] = (1 - w_x) * (1 - w_y) * (1 - w_z) * wq;
+   w8[1] = w_x * (1 - w_y) * (1 - w_z) * wq;
+   w8[2] = (1 - w_x) * w_y * (1 - w_z) * wq;
+   w8[3] = w_x * w_y * (1 - w_z) * wq;
+   w8[4] = (1 - w_x) * (1 - w_y) * w_z * wq;
+   w8[5] = w_x * (1 - w_y) * w_z * wq;
+   w8[6] = (1 - w_x) * w_y * w_z * wq;
+   w8[7] = w_x * w_y * w_z * wq;
+   for (int o = 0; o < 8; ++o) {
+      const int a = i + (o & 1), b = j + ((o >> 1) & 1), cc = k + ((o >> 2) & 1);
+      ind[o] = a + 3 * (b + 3 * cc);
+   }
+}
+
+// S[e*N + c], e < 27: charge of 3x3x3 entry e; e = 27 + 3*entry + l: current l
+__global__ void k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err) {
+   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (c >= g.N) return;
+   double acc[108];
+   for (int e = 0; e < 108; ++e) acc[e] = 0.0;
+   const long long a = P.start[c];
+   const int na = P.alive[c];
+   for (int t = 0; t < na; ++t) {
+      const long long p = a + t;
+      const double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
+      const double v[3] = {P.a[3][p], P.a[4][p], P.a[5][p]};
+      const double wq = P.a[6][p] * q;
+      double w8[8];
+      int ind[8];
+      cicWeights(x, y, z, wq, g.dx, w8, ind);
+      bool ok = true;
+      for (int o = 0; o < 8; ++o) ok = ok && ind[o] >= 0 && ind[o] < 27;
+      if (!ok) { raiseError(err, RHGPU_DEVERR_NAN_PARTICLE); continue; }
+      for (int o = 0; o < 8; ++o) acc[ind[o]] += w8[o];
+      for (int l = 0; l < 3; ++l)
+         for (int o = 0; o < 8; ++o) acc[27 + ind[o] * 3 + l] += w8[o] * v[l];
+   }
+   for (int e = 0; e < 108; ++e) S[(long long)e * g.N + c] = acc[e];
+}
+
+// destination sums over the 27 source cells in increasing source index
+__global__ void k_deposit_gather(GridInfo g, Fields f, const double* S, int first, int last, double minRho,
+                                 unsigned long long* cnt) {
+   RH_CELL_PROLOGUE
+   // per axis: (coordinate, offset source-dest) of the up to 3 sources, sorted by coordinate
+   int cx[3], ox[3], nxs = 0, cy[3], oy[3], nys = 0, cz[3], oz[3], nzs = 0;
+   for (int d = -1; d <= 1; ++d) {
+      int a = i + d; if (wrapc(a, g.nx, g.per[0])) { cx[nxs] = a; ox[nxs] = d; ++nxs; }
+      int b = j + d; if (wrapc(b, g.ny, g.per[1])) { cy[nys] = b; oy[nys] = d; ++nys; }
+      int c = k + d; if (wrapc(c, g.nz, g.per[2])) { cz[nzs] = c; oz[nzs] = d; ++nzs; }
+   }
+#define RH_SORT3(cc, oo, nn)                                                           \
+   for (int u = 1; u < nn; ++u)                                                         \
+      for (int w = u; w > 0 && cc[w - 1] > cc[w]; --w) {                               \
+         int t1 = cc[w]; cc[w] = cc[w - 1]; cc[w - 1] = t1;                             \
+         int t2 = oo[w]; oo[w] = oo[w - 1]; oo[w - 1] = t2;                             \
+      }
+   RH_SORT3(cx, ox, nxs) RH_SORT3(cy, oy, nys) RH_SORT3(cz, oz, nzs)
+#undef RH_SORT3
+   double rho = first ? 0.0 : f.cellRho[n];
+   double J0 = first ? 0.0 : f.cellJi[0 * N + n];
+   double J1 = first ? 0.0 : f.cellJi[1 * N + n];
+   double J2 = first ? 0.0 : f.cellJi[2 * N + n];
+   for (int c3 = 0; c3 < nzs; ++c3)
+      for (int b3 = 0; b3 < nys; ++b3)
+         for (int a3 = 0; a3 < nxs; ++a3) {
+            const long long s = cidx(g, cx[a3], cy[b3], cz[c3]);
+            // destination seen from the source: offset -o, array index -o+1
+            const int e = (1 - ox[a3]) + 3 * ((1 - oy[b3]) + 3 * (1 - oz[c3]));
+            rho += S[(long long)e * N + s];
+            J0 += S[(long long)(27 + 3 * e + 0) * N + s];
+            J1 += S[(long long)(27 + 3 * e + 1) * N + s];
+            J2 += S[(long long)(27 + 3 * e + 2) * N + s];
+         }
+   bool clamp = false;
+   if (last) {
+      rho /= g.dV;
+      if (rho < minRho) { rho = minRho; clamp = true; }
+      J0 /= g.dV; J1 /= g.dV; J2 /= g.dV;
+   }
+   countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   f.cellRho[n] = rho;
+   f.cellJi[0 * N + n] = J0;
+   f.cellJi[1 * N + n] = J1;
+   f.cellJi[2 * N + n] = J2;
+}
+
+// finalize without deposit (no accumulating species): rho = 0/dV clamped
+__global__ void k_deposit_finalize_only(GridInfo g, Fields f, double minRho, unsigned long long* cnt) {
+   RH_CELL_PROLOGUE
+   double rho = 0.0 / g.dV;
+   bool clamp = false;
+   if (rho < minRho) { rho = minRho; clamp = true; }
+   countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   f.cellRho[n] = rho;
+   for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = 0.0 / g.dV;
+}
+
+__global__ void k_bc_exterior(GridInfo g, PStore P, const int* ext, int next, double* cntd, int sidx) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= next) return;
+   const int c = ext[e];
+   const long long a = P.start[c];
+   const int na = P.alive[c];
+   double sw = 0.0, se = 0.0;
+   for (int t = 0; t < na; ++t) {
+      const long long p = a + t;
+      const double w = P.a[6][p];
+      sw += w;
+      se += w * (sq(P.a[3][p]) + sq(P.a[4][p]) + sq(P.a[5][p]));
+      P.pcell[p] = -1;
+   }
+   if (na > 0) {
+      atomicAdd(&cntd[4 * sidx + 0], sw);
+      atomicAdd(&cntd[4 * sidx + 1], se);
+   }
+   P.alive[c] = 0;
+}
+
+// swap-remove of particles inside the obstacle, in the reference's order
+__global__ void k_bc_obstacle(GridInfo g, PStore P, const int* cells, int ncells, double R2, double* cntd, int sidx) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= ncells) return;
+   const int c = cells[e];
+   const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+   const double xB = blockOrigin(g.x_min, i, g.dx), yB = blockOrigin(g.y_min, j, g.dx), zB = blockOrigin(g.z_min, k, g.dx);
+   const long long a = P.start[c];
+   int cur = 0, end = P.alive[c] - 1;
+   double sw = 0.0, se = 0.0;
+   while (cur <= end) {
+      const long long p = a + cur;
+      const double xp = xB + P.a[0][p], yp = yB + P.a[1][p], zp = zB + P.a[2][p];
+      const double r2 = sq(xp) + sq(yp) + sq(zp);
+      if (r2 < R2) {
+         const double w = P.a[6][p];
+         sw += w;
+         se += w * (sq(P.a[3][p]) + sq(P.a[4][p]) + sq(P.a[5][p]));
+         const long long q = a + end;
+         for (int s = 0; s < 7; ++s) P.a[s][p] = P.a[s][q];
+         --end;
+         continue;
+      }
+      ++cur;
+   }
+   for (int t = cur; t < P.alive[c]; ++t) P.pcell[a + t] = -1;
+   if (sw != 0.0 || se != 0.0) {
+      atomicAdd(&cntd[4 * sidx + 2], sw);
+      atomicAdd(&cntd[4 * sidx + 3], se);
+   }
+   P.alive[c] = cur;
+}
+
+}  // namespace rh

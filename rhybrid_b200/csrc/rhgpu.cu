@@ -1,0 +1,836 @@
+// rhgpu: C ABI (include/rhgpu.h) of the B200 hybrid-PIC hot path.
+//
+// Host side of the library: context and device memory, the per-step launch
+// sequence replaying RHybrid's propagate() (src/user.cpp:118-134), upload /
+// download with the ParGrid layout, counters, timing and reductions. The
+// device code is in k_particles.cuh (push, migration, deposit, particle
+// boundary conditions) and k_fields.cuh (propagateB).
+#include <cub/device/device_scan.cuh>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rhgpu.h"
+#include "k_fields.cuh"
+#include "k_particles.cuh"
+
+using namespace rh;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+   g_err = msg;
+   return code;
+}
+
+#define RH_CUDA(call)                                                                     \
+   do {                                                                                   \
+      cudaError_t e_ = (call);                                                            \
+      if (e_ != cudaSuccess) return fail(RHGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+   } while (0)
+
+const int MAX_SPECIES = 8;
+const int NCNT_U = 32;   // field counters 0..15, species MaxVi at 16+s
+
+int arrayDim(int id) {
+   return (id == RHGPU_CELL_RHOQI || id == RHGPU_NODE_RHOQI || id == RHGPU_NODE_ETA) ? 1 : 3;
+}
+
+// neumannCell rules (hybrid_propagator.cpp:456-652) in the reference's order:
+// missing-wall mask (1=-x 2=+y 4=-y 8=+z 16=-z 32=+x) and source offset
+const int NEU_CELL[26][4] = {
+   {1, +1, 0, 0}, {2, 0, -1, 0}, {4, 0, +1, 0}, {8, 0, 0, -1}, {16, 0, 0, +1}, {32, -1, 0, 0},
+   {1 | 4, +1, +1, 0}, {1 | 2, +1, -1, 0}, {32 | 4, -1, +1, 0}, {32 | 2, -1, -1, 0},
+   {1 | 16, +1, 0, +1}, {1 | 8, +1, 0, -1}, {32 | 16, -1, 0, +1}, {32 | 8, -1, 0, -1},
+   {4 | 16, 0, +1, +1}, {4 | 8, 0, +1, -1}, {2 | 16, 0, -1, +1}, {2 | 8, 0, -1, -1},
+   {1 | 4 | 16, +1, +1, +1}, {1 | 4 | 8, +1, +1, -1}, {1 | 2 | 16, +1, -1, +1}, {1 | 2 | 8, +1, -1, -1},
+   {32 | 4 | 16, -1, +1, +1}, {32 | 4 | 8, -1, +1, -1}, {32 | 2 | 16, -1, -1, +1}, {32 | 2 | 8, -1, -1, -1}};
+
+// neumannFace rules (hybrid_propagator.cpp:673-901): per component, source offset (use flag)
+struct FaceRule { int mask; int src[3][3]; int use[3]; };
+const FaceRule NEU_FACE[] = {
+   {1, {{0, 0, 0}, {+1, 0, 0}, {+1, 0, 0}}, {0, 1, 1}},
+   {2, {{0, -1, 0}, {0, 0, 0}, {0, -1, 0}}, {1, 0, 1}},
+   {4, {{0, +1, 0}, {0, 0, 0}, {0, +1, 0}}, {1, 0, 1}},
+   {8, {{0, 0, -1}, {0, 0, -1}, {0, 0, 0}}, {1, 1, 0}},
+   {16, {{0, 0, +1}, {0, 0, +1}, {0, 0, 0}}, {1, 1, 0}},
+   {32, {{0, 0, 0}, {-1, 0, 0}, {-1, 0, 0}}, {0, 1, 1}},
+   {1 | 4, {{0, +1, 0}, {+1, 0, 0}, {+1, +1, 0}}, {1, 1, 1}},
+   {1 | 2, {{0, -1, 0}, {0, 0, 0}, {+1, -1, 0}}, {1, 0, 1}},
+   {32 | 4, {{0, 0, 0}, {-1, 0, 0}, {-1, +1, 0}}, {0, 1, 1}},
+   {32 | 2, {{0, 0, 0}, {0, 0, 0}, {-1, -1, 0}}, {0, 0, 1}},
+   {1 | 16, {{0, 0, +1}, {+1, 0, +1}, {+1, 0, 0}}, {1, 1, 1}},
+   {1 | 8, {{0, 0, -1}, {+1, 0, -1}, {0, 0, 0}}, {1, 1, 0}},
+   {32 | 16, {{0, 0, 0}, {-1, 0, +1}, {-1, 0, 0}}, {0, 1, 1}},
+   {32 | 8, {{0, 0, 0}, {-1, 0, -1}, {0, 0, 0}}, {0, 1, 0}},
+   {4 | 16, {{0, +1, +1}, {0, 0, +1}, {0, +1, 0}}, {1, 1, 1}},
+   {4 | 8, {{0, +1, -1}, {0, 0, -1}, {0, 0, 0}}, {1, 1, 0}},
+   {2 | 16, {{0, -1, +1}, {0, 0, 0}, {0, -1, 0}}, {1, 0, 1}},
+   {2 | 8, {{0, -1, -1}, {0, 0, 0}, {0, 0, 0}}, {1, 0, 0}},
+   {1 | 4 | 16, {{0, +1, +1}, {+1, 0, +1}, {+1, +1, 0}}, {1, 1, 1}},
+   {1 | 4 | 8, {{0, +1, -1}, {+1, 0, -1}, {0, 0, 0}}, {1, 1, 0}},
+   {1 | 2 | 16, {{0, -1, +1}, {0, 0, 0}, {+1, -1, 0}}, {1, 0, 1}},
+   {1 | 2 | 8, {{0, -1, -1}, {0, 0, 0}, {0, 0, 0}}, {1, 0, 0}},
+   {32 | 4 | 16, {{0, 0, 0}, {-1, 0, +1}, {-1, +1, 0}}, {0, 1, 1}},
+   {32 | 4 | 8, {{0, 0, 0}, {-1, 0, -1}, {0, 0, 0}}, {0, 1, 0}},
+   {32 | 2 | 16, {{0, 0, 0}, {0, 0, 0}, {-1, -1, 0}}, {0, 0, 1}},
+};
+
+NeumannTables buildNeumannTables() {
+   NeumannTables t;
+   std::memset(&t, 0, sizeof t);
+   for (int m = 0; m < 64; ++m) {
+      for (int r = 0; r < 26; ++r) {
+         if ((m & NEU_CELL[r][0]) != NEU_CELL[r][0]) continue;
+         for (int a = 0; a < 3; ++a) t.cellSrc[m][a] = (signed char)NEU_CELL[r][1 + a];
+      }
+      for (const FaceRule& fr : NEU_FACE) {
+         if ((m & fr.mask) != fr.mask) continue;
+         for (int l = 0; l < 3; ++l) {
+            if (!fr.use[l]) continue;
+            t.faceUse[m][l] = 1;
+            for (int a = 0; a < 3; ++a) t.faceSrc[m][l][a] = (signed char)fr.src[l][a];
+         }
+      }
+   }
+   return t;
+}
+
+struct TimerRec { int cls; int ea, eb; };
+
+}  // namespace
+
+struct rhgpu_ctx {
+   rhgpu_params P;
+   GridInfo g;
+   int device = 0;
+   cudaStream_t stream = nullptr;
+   int ns = 0;
+   rhgpu_species sp[MAX_SPECIES];
+   Fields f;
+   FieldParams fp;
+   double* arr[RHGPU_NUM_ARRAYS] = {};
+   double* tmp3 = nullptr;
+   uint8_t* flags = nullptr;
+   int* ext = nullptr;
+   int next = 0;
+   int* obst = nullptr;
+   int nobst = 0;
+   PStore ps[MAX_SPECIES];
+   PStore alt[MAX_SPECIES];   // migration target buffers
+   int* key = nullptr;
+   int* rank = nullptr;
+   long long keyCap = 0;
+   int* outCount = nullptr;
+   int* inPrefix = nullptr;
+   long long* newCount = nullptr;
+   void* scanTmp = nullptr;
+   size_t scanTmpBytes = 0;
+   double* S = nullptr;
+   unsigned long long* cntU = nullptr;
+   double* cntD = nullptr;
+   unsigned* err = nullptr;
+   double t = 0;
+   long long timestep = 0;
+   int useIFT = 0;
+   double gridAvgCounter = 0;
+   bool timing = false;
+   std::vector<cudaEvent_t> evPool;   // per-launch event pairs of the last rhgpu_step
+   size_t evUsed = 0;
+   std::vector<TimerRec> recs;
+   std::vector<std::string> clsNames;
+   long long launches = 0;
+   long long launchesStep = 0;
+   void* staging = nullptr;      // particle record staging for upload/download
+   size_t stagingBytes = 0;
+};
+
+namespace {
+
+dim3 cellBlock() { return dim3(32, 4, 1); }
+dim3 cellGrid(const GridInfo& g) { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz); }
+unsigned blocks1d(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Kernel timing: with timing on, every launch is bracketed by a pair of CUDA
+// events recorded on the context's stream (no synchronisation); the elapsed
+// times are summed per kernel class by rhgpu_get_timing.
+int timerBegin(rhgpu_ctx* c, const char* name) {
+   if (!c->timing) return -1;
+   int cls = -1;
+   for (size_t q = 0; q < c->clsNames.size(); ++q)
+      if (c->clsNames[q] == name) { cls = (int)q; break; }
+   if (cls < 0) { c->clsNames.push_back(name); cls = (int)c->clsNames.size() - 1; }
+   while (c->evPool.size() < c->evUsed + 2) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->evPool.push_back(e);
+   }
+   TimerRec r{cls, (int)c->evUsed, (int)c->evUsed + 1};
+   c->evUsed += 2;
+   cudaEventRecord(c->evPool[r.ea], c->stream);
+   c->recs.push_back(r);
+   return (int)c->recs.size() - 1;
+}
+void timerEnd(rhgpu_ctx* c, int r) {
+   if (r >= 0) cudaEventRecord(c->evPool[c->recs[r].eb], c->stream);
+}
+struct KScope {
+   rhgpu_ctx* c;
+   int r;
+   KScope(rhgpu_ctx* c_, const char* n) : c(c_), r(timerBegin(c_, n)) {}
+   ~KScope() { timerEnd(c, r); }
+};
+#define RH_TIME(c, name) KScope rh_scope_(c, name)
+
+int allocStore(PStore& s, long long cap, long long N) {
+   s.cap = cap;
+   s.nslots = 0;
+   for (int a = 0; a < 7; ++a) RH_CUDA(cudaMalloc(&s.a[a], sizeof(double) * (cap > 0 ? cap : 1)));
+   RH_CUDA(cudaMalloc(&s.pcell, sizeof(int) * (cap > 0 ? cap : 1)));
+   RH_CUDA(cudaMalloc(&s.start, sizeof(long long) * (N + 1)));
+   RH_CUDA(cudaMalloc(&s.alive, sizeof(int) * N));
+   RH_CUDA(cudaMemset(s.start, 0, sizeof(long long) * (N + 1)));
+   RH_CUDA(cudaMemset(s.alive, 0, sizeof(int) * N));
+   return RHGPU_OK;
+}
+
+void freeStore(PStore& s) {
+   for (int a = 0; a < 7; ++a) cudaFree(s.a[a]);
+   cudaFree(s.pcell);
+   cudaFree(s.start);
+   cudaFree(s.alive);
+   std::memset(&s, 0, sizeof s);
+}
+
+int checkLaunch(rhgpu_ctx* c) {
+   c->launches++;
+   c->launchesStep++;
+   cudaError_t e = cudaGetLastError();
+   if (e != cudaSuccess) return fail(RHGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+   return RHGPU_OK;
+}
+#define RH_LAUNCHED(c) do { int rc_ = checkLaunch(c); if (rc_) return rc_; } while (0)
+
+SpeciesDev speciesDev(const rhgpu_ctx* c, int s) {
+   SpeciesDev d;
+   d.q = c->sp[s].q;
+   d.m = c->sp[s].m;
+   d.R2obs = c->sp[s].R2_obstacle;
+   // qmideltT2 = 0.5*species.q*sim->dt/species.m (boris.h:112)
+   d.qmideltT2 = 0.5 * c->sp[s].q * c->P.dt / c->sp[s].m;
+   d.accelerate = c->sp[s].accelerate;
+   d.accumulate = c->sp[s].accumulate;
+   return d;
+}
+
+int ensureKeyCapacity(rhgpu_ctx* c, long long n) {
+   if (n <= c->keyCap) return RHGPU_OK;
+   cudaFree(c->key);
+   cudaFree(c->rank);
+   c->keyCap = n + n / 8 + 1024;
+   RH_CUDA(cudaMalloc(&c->key, sizeof(int) * c->keyCap));
+   RH_CUDA(cudaMalloc(&c->rank, sizeof(int) * c->keyCap));
+   return RHGPU_OK;
+}
+
+int migrate(rhgpu_ctx* c, int s) {
+   PStore& P = c->ps[s];
+   PStore& Q = c->alt[s];
+   const GridInfo& g = c->g;
+   {
+      RH_TIME(c, "mig_count");
+      k_mig_count<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, P, c->key, c->outCount, c->rank);
+      RH_LAUNCHED(c);
+   }
+   {
+      RH_TIME(c, "mig_incount");
+      k_mig_incount<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->outCount, c->inPrefix, c->newCount);
+      RH_LAUNCHED(c);
+   }
+   // exclusive scan of the new counts into Q.start[0..N], Q.start[N] = total
+   RH_CUDA(cudaMemsetAsync(c->newCount + g.N, 0, sizeof(long long), c->stream));
+   {
+      RH_TIME(c, "mig_scan");
+      size_t bytes = c->scanTmpBytes;
+      RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, Q.start, g.N + 1, c->stream));
+      c->launches += 2;
+      c->launchesStep += 2;
+   }
+   long long total = 0;
+   RH_CUDA(cudaMemcpyAsync(&total, Q.start + g.N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (total > Q.cap) return fail(RHGPU_ERR_CAPACITY, "particle capacity exceeded in migration");
+   Q.nslots = total;
+   {
+      RH_TIME(c, "mig_scatter");
+      k_mig_scatter<<<blocks1d(P.nslots > 0 ? P.nslots : 1, 256), 256, 0, c->stream>>>(g, P, Q, c->key, c->rank,
+                                                                                      c->inPrefix, Q.start, c->err);
+      RH_LAUNCHED(c);
+   }
+   {
+      RH_TIME(c, "mig_alive");
+      k_set_alive_from_count<<<blocks1d(g.N, 256), 256, 0, c->stream>>>(g.N, c->newCount, Q.alive);
+      RH_LAUNCHED(c);
+   }
+   std::swap(c->ps[s], c->alt[s]);
+   return RHGPU_OK;
+}
+
+int pushAll(rhgpu_ctx* c) {
+   c->timestep += 1;
+   // initial flow-through switch-off (user.cpp:52-59)
+   if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
+   PushParams pp;
+   pp.useIFT = c->useIFT;
+   pp.use_ep = c->P.use_electron_pressure;
+   pp.use_gravity = c->P.use_gravity;
+   pp.GMdt = c->P.GMdt;
+   pp.maxVi2 = c->P.max_ion_speed2;
+   for (int s = 0; s < c->ns; ++s) {
+      PStore& P = c->ps[s];
+      int rc = ensureKeyCapacity(c, P.nslots);
+      if (rc) return rc;
+      if (P.nslots > 0) {
+         RH_TIME(c, "push");
+         k_push<<<blocks1d(P.nslots, 256), 256, 0, c->stream>>>(c->g, c->f, P, speciesDev(c, s), pp, c->key,
+                                                                c->cntU, c->cntD, c->err, s);
+         RH_LAUNCHED(c);
+      }
+      rc = migrate(c, s);
+      if (rc) return rc;
+   }
+   return RHGPU_OK;
+}
+
+int accumulateAll(rhgpu_ctx* c) {
+   int last = -1, first = -1;
+   for (int s = 0; s < c->ns; ++s)
+      if (c->sp[s].accumulate) { if (first < 0) first = s; last = s; }
+   const GridInfo& g = c->g;
+   if (last < 0) {
+      RH_TIME(c, "deposit_gather");
+      k_deposit_finalize_only<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->f, c->P.min_ion_charge_density, c->cntU);
+      RH_LAUNCHED(c);
+   }
+   for (int s = 0; s < c->ns; ++s) {
+      if (!c->sp[s].accumulate) continue;
+      {
+         RH_TIME(c, "deposit_cell");
+         k_deposit_cell<<<blocks1d(g.N, 64), 64, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, c->S, c->err);
+         RH_LAUNCHED(c);
+      }
+      {
+         RH_TIME(c, "deposit_gather");
+         k_deposit_gather<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->f, c->S, s == first, s == last,
+                                                                      c->P.min_ion_charge_density, c->cntU);
+         RH_LAUNCHED(c);
+      }
+   }
+   return RHGPU_OK;
+}
+
+int boundariesAll(rhgpu_ctx* c) {
+   for (int s = 0; s < c->ns; ++s) {
+      if (c->next > 0) {
+         RH_TIME(c, "bc_exterior");
+         k_bc_exterior<<<blocks1d(c->next, 128), 128, 0, c->stream>>>(c->g, c->ps[s], c->ext, c->next, c->cntD, s);
+         RH_LAUNCHED(c);
+      }
+      if (c->nobst > 0) {
+         RH_TIME(c, "bc_obstacle");
+         k_bc_obstacle<<<blocks1d(c->nobst, 64), 64, 0, c->stream>>>(c->g, c->ps[s], c->obst, c->nobst,
+                                                                     c->sp[s].R2_obstacle, c->cntD, s);
+         RH_LAUNCHED(c);
+      }
+   }
+   return RHGPU_OK;
+}
+
+#define RH_FIELD_LAUNCH(name, grid, block, ...)              \
+   do {                                                      \
+      RH_TIME(c, #name);                                     \
+      name<<<grid, block, 0, c->stream>>>(__VA_ARGS__);      \
+      RH_LAUNCHED(c);                                        \
+   } while (0)
+
+int fieldsAll(rhgpu_ctx* c) {
+   const GridInfo& g = c->g;
+   const dim3 G = cellGrid(g), B = cellBlock();
+   const unsigned EB = blocks1d(c->next > 0 ? c->next : 1, 128);
+   RH_FIELD_LAUNCH(k_face2cell, G, B, g, c->f);
+   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
+   RH_FIELD_LAUNCH(k_cell2node_avg, G, B, g, c->f);
+   c->gridAvgCounter += 1;
+   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_face_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
+   RH_FIELD_LAUNCH(k_node_j, G, B, g, c->f, c->fp, c->cntU);
+   RH_FIELD_LAUNCH(k_cell_j_ue, G, B, g, c->f, c->fp, c->cntU);
+   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellUe, c->ext, c->next);
+   RH_FIELD_LAUNCH(k_node_ue_b_e, G, B, g, c->f, c->fp, c->cntU);
+   for (int it = 0; it < c->P.n_linear_smoothings_nodeE; ++it) {
+      RH_FIELD_LAUNCH(k_node2cell3, G, B, g, c->f.nodeE, c->f.cellJ);
+      if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellJ, c->ext, c->next);
+      RH_FIELD_LAUNCH(k_cell2node3, G, B, g, c->f.cellJ, c->f.nodeE);
+      RH_CUDA(cudaMemsetAsync(c->f.cellJ, 0, sizeof(double) * 3 * g.N, c->stream));
+   }
+   if (c->P.use_gaussian_smoothing_nodeE) {
+      RH_CUDA(cudaMemcpyAsync(c->tmp3, c->f.nodeE, sizeof(double) * 3 * g.N, cudaMemcpyDeviceToDevice, c->stream));
+      RH_FIELD_LAUNCH(k_node_avg, G, B, g, c->tmp3, c->f.nodeE, c->fp);
+   }
+   RH_FIELD_LAUNCH(k_faraday, G, B, g, c->f);
+   if (c->P.use_electron_pressure) RH_FIELD_LAUNCH(k_cell_ep, G, B, g, c->f, c->fp);
+   c->t += c->P.dt;
+   return RHGPU_OK;
+}
+
+int checkDeviceError(rhgpu_ctx* c) {
+   unsigned w = 0;
+   RH_CUDA(cudaMemcpyAsync(&w, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (w) return fail(RHGPU_ERR_DEVICE, "device error word " + std::to_string(w));
+   return RHGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rhgpu_last_error(void) { return g_err.c_str(); }
+
+const char* rhgpu_version(void) {
+   return "rhgpu 0.1 sm_100a fp64 (--fmad=false, IEEE div/sqrt), deposit=reference-order";
+}
+
+int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_species* species,
+                 const int64_t* capacity, int32_t device, rhgpu_ctx** out) {
+   if (!params || !species || !out || n_species < 1 || n_species > MAX_SPECIES)
+      return fail(RHGPU_ERR_ARG, "rhgpu_create: bad arguments");
+   if (params->nx < 3 || params->ny < 3 || params->nz < 3) return fail(RHGPU_ERR_ARG, "rhgpu_create: at least 3 cells per axis");
+   const long long N = (long long)params->nx * params->ny * params->nz;
+   if (N * 27 >= (1LL << 31)) return fail(RHGPU_ERR_ARG, "rhgpu_create: grid too large (27*cells must fit int32)");
+   RH_CUDA(cudaSetDevice(device));
+   rhgpu_ctx* c = new rhgpu_ctx();
+   c->P = *params;
+   c->device = device;
+   c->ns = n_species;
+   std::memcpy(c->sp, species, sizeof(rhgpu_species) * n_species);
+   GridInfo& g = c->g;
+   g.nx = params->nx; g.ny = params->ny; g.nz = params->nz;
+   for (int a = 0; a < 3; ++a) g.per[a] = params->periodic[a] ? 1 : 0;
+   g.N = N;
+   g.dx = params->dx;
+   g.dt = params->dt;
+   g.dV = params->dx * params->dx * params->dx;
+   g.dx_below = std::nextafter(params->dx, 0.0);
+   g.x_min = params->x_min; g.y_min = params->y_min; g.z_min = params->z_min;
+   c->t = params->t_initial;
+   c->useIFT = params->use_initial_flow_through;
+   FieldParams& fp = c->fp;
+   fp.use_hall = params->use_hall;
+   fp.use_ep = params->use_electron_pressure;
+   fp.isothermal = params->isothermal_electrons;
+   fp.ep_coeff = params->electron_pressure_coeff;
+   for (int l = 0; l < 3; ++l) fp.obstacleUe[l] = params->field_obstacle_Ue[l];
+   fp.maxUe2 = params->max_electron_speed2;
+   fp.minRho = params->min_ion_charge_density;
+   fp.maxE2 = params->max_electric_field2;
+   fp.maxVw = params->max_whistler_speed;
+   for (int l = 0; l < 4; ++l) fp.gauss[l] = params->gaussian_coeffs[l];
+   for (int l = 0; l < 3; ++l) fp.imf[l] = params->imf_B[l];
+   for (int w = 0; w < 6; ++w) { fp.imfCell[w] = params->imf_boundary_cellB[w]; fp.imfFace[w] = params->imf_boundary_faceB[w]; }
+
+   int rc = RHGPU_OK;
+   auto alloc = [&](void** p, size_t bytes) {
+      if (rc) return;
+      cudaError_t e = cudaMalloc(p, bytes);
+      if (e != cudaSuccess) rc = fail(RHGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      else cudaMemset(*p, 0, bytes);
+   };
+   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return fail(RHGPU_ERR_CUDA, "stream create failed");
+   }
+   for (int a = 0; a < RHGPU_NUM_ARRAYS; ++a) alloc((void**)&c->arr[a], sizeof(double) * N * arrayDim(a));
+   alloc((void**)&c->tmp3, sizeof(double) * 3 * N);
+   alloc((void**)&c->flags, N);
+   alloc((void**)&c->outCount, sizeof(int) * 27 * N);
+   alloc((void**)&c->inPrefix, sizeof(int) * 27 * N);
+   alloc((void**)&c->newCount, sizeof(long long) * (N + 1));
+   alloc((void**)&c->S, sizeof(double) * 108 * N);
+   alloc((void**)&c->cntU, sizeof(unsigned long long) * NCNT_U);
+   alloc((void**)&c->cntD, sizeof(double) * 4 * MAX_SPECIES);
+   alloc((void**)&c->err, sizeof(unsigned));
+   if (!rc) {
+      size_t bytes = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->newCount, c->newCount, N + 1, c->stream);
+      c->scanTmpBytes = bytes;
+      alloc(&c->scanTmp, bytes + 16);
+   }
+   for (int s = 0; s < n_species && !rc; ++s) {
+      const long long cap = capacity ? (long long)capacity[s] : 0;
+      rc = allocStore(c->ps[s], cap, N);
+      if (!rc) rc = allocStore(c->alt[s], cap, N);
+   }
+   // exterior cells (missing a neighbour) and obstacle-flagged cells are
+   // listed after upload_cell_flags; exterior list now
+   if (!rc) {
+      std::vector<int> ext;
+      for (int k = 0; k < g.nz; ++k)
+         for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i)
+               if (!allNb(g, i, j, k)) ext.push_back((int)cidx(g, i, j, k));
+      c->next = (int)ext.size();
+      alloc((void**)&c->ext, sizeof(int) * (ext.size() + 1));
+      if (!rc && !ext.empty()) {
+         if (cudaMemcpy(c->ext, ext.data(), sizeof(int) * ext.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(RHGPU_ERR_CUDA, "copy exterior list");
+      }
+   }
+   if (!rc) {
+      NeumannTables t = buildNeumannTables();
+      if (cudaMemcpyToSymbol(c_neu, &t, sizeof t) != cudaSuccess) rc = fail(RHGPU_ERR_CUDA, "neumann tables");
+   }
+   if (!rc) {
+      Fields& f = c->f;
+      f.faceB = c->arr[RHGPU_FACE_B]; f.cellB = c->arr[RHGPU_CELL_B]; f.cellUe = c->arr[RHGPU_CELL_UE];
+      f.cellEp = c->arr[RHGPU_CELL_EP]; f.cellRho = c->arr[RHGPU_CELL_RHOQI]; f.cellJi = c->arr[RHGPU_CELL_JI];
+      f.cellJ = c->arr[RHGPU_CELL_J]; f.nodeRho = c->arr[RHGPU_NODE_RHOQI]; f.nodeJi = c->arr[RHGPU_NODE_JI];
+      f.nodeJ = c->arr[RHGPU_NODE_J]; f.nodeUe = c->arr[RHGPU_NODE_UE]; f.nodeB = c->arr[RHGPU_NODE_B];
+      f.nodeE = c->arr[RHGPU_NODE_E]; f.nodeEta = c->arr[RHGPU_NODE_ETA]; f.cellAvgB = c->arr[RHGPU_CELL_AVERAGE_B];
+      f.tmp3 = c->tmp3;
+      f.flags = c->flags;
+   }
+   if (rc) {
+      rhgpu_destroy(c);
+      return rc;
+   }
+   if (cudaDeviceSynchronize() != cudaSuccess) return fail(RHGPU_ERR_CUDA, "create: sync failed");
+   *out = c;
+   return RHGPU_OK;
+}
+
+int rhgpu_destroy(rhgpu_ctx* c) {
+   if (!c) return RHGPU_OK;
+   cudaSetDevice(c->device);
+   if (c->stream) cudaStreamSynchronize(c->stream);
+   for (int a = 0; a < RHGPU_NUM_ARRAYS; ++a) cudaFree(c->arr[a]);
+   cudaFree(c->tmp3); cudaFree(c->flags); cudaFree(c->ext); cudaFree(c->obst);
+   cudaFree(c->key); cudaFree(c->rank); cudaFree(c->outCount); cudaFree(c->inPrefix);
+   cudaFree(c->newCount); cudaFree(c->scanTmp); cudaFree(c->S); cudaFree(c->cntU); cudaFree(c->cntD); cudaFree(c->err);
+   cudaFree(c->staging);
+   for (int s = 0; s < c->ns; ++s) { freeStore(c->ps[s]); freeStore(c->alt[s]); }
+   for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
+   if (c->stream) cudaStreamDestroy(c->stream);
+   delete c;
+   return RHGPU_OK;
+}
+
+// ----------------------------------------------------------------------------
+// grid arrays: ParGrid interleaved layout <-> component planes
+
+namespace {
+__global__ void k_interleaved_to_planes(const double* in, double* out, long long N, int dim) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= N * dim) return;
+   const long long n = t / dim;
+   const int l = (int)(t % dim);
+   out[(long long)l * N + n] = in[t];
+}
+__global__ void k_planes_to_interleaved(const double* in, double* out, long long N, int dim) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= N * dim) return;
+   const long long n = t / dim;
+   const int l = (int)(t % dim);
+   out[t] = in[(long long)l * N + n];
+}
+}  // namespace
+
+int rhgpu_upload_array(rhgpu_ctx* c, int32_t id, const double* host) {
+   if (!c || !host || id < 0 || id >= RHGPU_NUM_ARRAYS) return fail(RHGPU_ERR_ARG, "upload_array: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   const int dim = arrayDim(id);
+   const long long N = c->g.N;
+   RH_CUDA(cudaMemcpyAsync(c->tmp3, host, sizeof(double) * N * dim, cudaMemcpyHostToDevice, c->stream));
+   k_interleaved_to_planes<<<blocks1d(N * dim, 256), 256, 0, c->stream>>>(c->tmp3, c->arr[id], N, dim);
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+int rhgpu_download_array(rhgpu_ctx* c, int32_t id, double* host) {
+   if (!c || !host || id < 0 || id >= RHGPU_NUM_ARRAYS) return fail(RHGPU_ERR_ARG, "download_array: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   const int dim = arrayDim(id);
+   const long long N = c->g.N;
+   k_planes_to_interleaved<<<blocks1d(N * dim, 256), 256, 0, c->stream>>>(c->arr[id], c->tmp3, N, dim);
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaMemcpyAsync(host, c->tmp3, sizeof(double) * N * dim, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+int rhgpu_upload_cell_flags(rhgpu_ctx* c, const uint8_t* host) {
+   if (!c || !host) return fail(RHGPU_ERR_ARG, "upload_cell_flags: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaMemcpy(c->flags, host, c->g.N, cudaMemcpyHostToDevice));
+   std::vector<int> ob;
+   for (long long n = 0; n < c->g.N; ++n)
+      if (host[n] & RHGPU_FLAG_INNER_PARTICLE) ob.push_back((int)n);
+   cudaFree(c->obst);
+   c->obst = nullptr;
+   c->nobst = (int)ob.size();
+   RH_CUDA(cudaMalloc(&c->obst, sizeof(int) * (ob.size() + 1)));
+   if (!ob.empty()) RH_CUDA(cudaMemcpy(c->obst, ob.data(), sizeof(int) * ob.size(), cudaMemcpyHostToDevice));
+   return RHGPU_OK;
+}
+
+namespace {
+// per cell: slot range from the counts, cell index of every slot
+__global__ void k_counts_in(long long N, const uint32_t* counts, long long* cnt64, int* alive) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b < N) { cnt64[b] = counts[b]; alive[b] = (int)counts[b]; }
+   if (b == N) cnt64[N] = 0;
+}
+__global__ void k_fill_pcell(long long N, const long long* start, int* pcell) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b >= N) return;
+   for (long long p = start[b]; p < start[b + 1]; ++p) pcell[p] = (int)b;
+}
+// particle records (7 doubles) -> 7 component planes
+__global__ void k_aos_to_soa(const double* aos, PStore P, long long n) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= 7 * n) return;
+   const long long p = t / 7;
+   const int a = (int)(t % 7);
+   P.a[a][p] = aos[t];
+}
+// alive particles of each cell -> records at the cell's output offset
+__global__ void k_soa_to_aos(PStore P, long long N, const long long* outStart, double* aos, uint32_t* counts) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b >= N) return;
+   const long long s = P.start[b], o = outStart[b];
+   const int na = P.alive[b];
+   counts[b] = (uint32_t)na;
+   for (int t = 0; t < na; ++t)
+      for (int a = 0; a < 7; ++a) aos[7 * (o + t) + a] = P.a[a][s + t];
+}
+__global__ void k_alive_to64(long long N, const int* alive, long long* out) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b < N) out[b] = alive[b];
+   if (b == N) out[N] = 0;
+}
+
+int ensureStaging(rhgpu_ctx* c, size_t bytes) {
+   if (bytes <= c->stagingBytes) return RHGPU_OK;
+   cudaFree(c->staging);
+   c->staging = nullptr;
+   c->stagingBytes = 0;
+   RH_CUDA(cudaMalloc(&c->staging, bytes));
+   c->stagingBytes = bytes;
+   return RHGPU_OK;
+}
+}  // namespace
+
+int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, const double* particles, int64_t n) {
+   if (!c || s < 0 || s >= c->ns || !counts || (n > 0 && !particles) || n < 0)
+      return fail(RHGPU_ERR_ARG, "upload_particles: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   const long long N = c->g.N;
+   PStore& P = c->ps[s];
+   if (n > P.cap) return fail(RHGPU_ERR_CAPACITY, "upload_particles: more particles than capacity");
+   int rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   double* aos = (double*)c->staging;
+   uint32_t* dcounts = (uint32_t*)((char*)c->staging + sizeof(double) * 7 * (size_t)(n > 0 ? n : 1));
+   RH_CUDA(cudaMemcpyAsync(dcounts, counts, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream));
+   if (n) RH_CUDA(cudaMemcpyAsync(aos, particles, sizeof(double) * 7 * n, cudaMemcpyHostToDevice, c->stream));
+   k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, P.alive);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, P.start, N + 1, c->stream));
+   long long total = 0;
+   RH_CUDA(cudaMemcpyAsync(&total, P.start + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (total != n) return fail(RHGPU_ERR_ARG, "upload_particles: sum(counts) != n_particles");
+   k_fill_pcell<<<blocks1d(N, 128), 128, 0, c->stream>>>(N, P.start, P.pcell);
+   RH_CUDA(cudaGetLastError());
+   if (n) {
+      k_aos_to_soa<<<blocks1d(7 * n, 256), 256, 0, c->stream>>>(aos, P, n);
+      RH_CUDA(cudaGetLastError());
+   }
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   P.nslots = n;
+   return ensureKeyCapacity(c, n);
+}
+
+int rhgpu_num_particles(rhgpu_ctx* c, int32_t s, int64_t* n_out) {
+   if (!c || s < 0 || s >= c->ns || !n_out) return fail(RHGPU_ERR_ARG, "num_particles: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   std::vector<int> alive(c->g.N);
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   RH_CUDA(cudaMemcpy(alive.data(), c->ps[s].alive, sizeof(int) * c->g.N, cudaMemcpyDeviceToHost));
+   long long t = 0;
+   for (int a : alive) t += a;
+   *n_out = t;
+   return RHGPU_OK;
+}
+
+int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* particles, int64_t capacity,
+                             int64_t* n_out) {
+   if (!c || s < 0 || s >= c->ns || !counts || !n_out) return fail(RHGPU_ERR_ARG, "download_particles: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   const long long N = c->g.N;
+   PStore& P = c->ps[s];
+   // output offsets: exclusive scan of the alive counts (scratch: newCount, alt.start)
+   k_alive_to64<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, P.alive, c->newCount);
+   RH_CUDA(cudaGetLastError());
+   long long* outStart = c->alt[s].start;
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, outStart, N + 1, c->stream));
+   long long tot = 0;
+   RH_CUDA(cudaMemcpyAsync(&tot, outStart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (tot > capacity) return fail(RHGPU_ERR_ARG, "download_particles: capacity too small");
+   int rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(tot > 0 ? tot : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   double* aos = (double*)c->staging;
+   uint32_t* dcounts = (uint32_t*)((char*)c->staging + sizeof(double) * 7 * (size_t)(tot > 0 ? tot : 1));
+   k_soa_to_aos<<<blocks1d(N, 128), 128, 0, c->stream>>>(P, N, outStart, aos, dcounts);
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaMemcpyAsync(counts, dcounts, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
+   if (tot && particles) RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   *n_out = tot;
+   return RHGPU_OK;
+}
+
+int rhgpu_push(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   RH_CUDA(cudaSetDevice(c->device));
+   int rc = pushAll(c);
+   if (rc) return rc;
+   return checkDeviceError(c);
+}
+
+int rhgpu_accumulate(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   RH_CUDA(cudaSetDevice(c->device));
+   int rc = accumulateAll(c);
+   if (rc) return rc;
+   return checkDeviceError(c);
+}
+
+int rhgpu_apply_boundaries(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   RH_CUDA(cudaSetDevice(c->device));
+   int rc = boundariesAll(c);
+   if (rc) return rc;
+   return checkDeviceError(c);
+}
+
+int rhgpu_propagate_fields(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   RH_CUDA(cudaSetDevice(c->device));
+   int rc = fieldsAll(c);
+   if (rc) return rc;
+   return checkDeviceError(c);
+}
+
+int rhgpu_step(rhgpu_ctx* c, int32_t nsteps) {
+   if (!c || nsteps < 0) return fail(RHGPU_ERR_ARG, "step: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   c->launchesStep = 0;
+   c->recs.clear();
+   c->evUsed = 0;
+   for (int n = 0; n < nsteps; ++n) {
+      int rc = pushAll(c);
+      if (!rc) rc = accumulateAll(c);
+      if (!rc) rc = boundariesAll(c);
+      if (!rc) rc = fieldsAll(c);
+      if (rc) return rc;
+   }
+   return checkDeviceError(c);
+}
+
+int rhgpu_device_errors(rhgpu_ctx* c, uint32_t* word_out) {
+   if (!c || !word_out) return fail(RHGPU_ERR_ARG, "device_errors: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaMemcpyAsync(word_out, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+int rhgpu_get_counters(rhgpu_ctx* c, double* out, int32_t n) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "get_counters: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   unsigned long long u[NCNT_U];
+   double d[4 * MAX_SPECIES];
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   RH_CUDA(cudaMemcpy(u, c->cntU, sizeof u, cudaMemcpyDeviceToHost));
+   RH_CUDA(cudaMemcpy(d, c->cntD, sizeof d, cudaMemcpyDeviceToHost));
+   std::vector<double> v(RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES * c->ns, 0.0);
+   for (int i = 0; i < RHGPU_NUM_FIELD_COUNTERS; ++i) v[i] = (double)u[i];
+   v[RHGPU_CNT_GRID_AVERAGE_COUNTER] = c->gridAvgCounter;
+   for (int s = 0; s < c->ns; ++s) {
+      double* q = &v[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES * s];
+      q[0] = (double)u[CNT_SPECIES_MAXVI + s];
+      q[1] = d[4 * s + 0];
+      q[2] = d[4 * s + 1];
+      q[3] = d[4 * s + 2];
+      q[4] = d[4 * s + 3];
+   }
+   for (int i = 0; i < n && i < (int)v.size(); ++i) out[i] = v[i];
+   return RHGPU_OK;
+}
+
+int rhgpu_get_time(rhgpu_ctx* c, double* t_out, int64_t* ts_out) {
+   if (!c || !t_out || !ts_out) return fail(RHGPU_ERR_ARG, "get_time: bad arguments");
+   *t_out = c->t;
+   *ts_out = c->timestep;
+   return RHGPU_OK;
+}
+
+void* rhgpu_stream(rhgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int rhgpu_set_timing(rhgpu_ctx* c, int32_t enable) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   c->timing = enable != 0;
+   return RHGPU_OK;
+}
+
+int rhgpu_get_timing(rhgpu_ctx* c, char* names, int32_t name_cap, double* ms, int32_t n, int32_t* n_out) {
+   if (!c || !names || !ms || !n_out) return fail(RHGPU_ERR_ARG, "get_timing: bad arguments");
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   std::vector<double> tot(c->clsNames.size(), 0.0);
+   for (const TimerRec& r : c->recs) {
+      float x = 0;
+      if (cudaEventElapsedTime(&x, c->evPool[r.ea], c->evPool[r.eb]) == cudaSuccess) tot[r.cls] += x;
+   }
+   std::string s;
+   int m = 0;
+   for (size_t q = 0; q < tot.size() && (int)q < n; ++q, ++m) {
+      if (q) s += ",";
+      s += c->clsNames[q];
+      ms[q] = tot[q];
+   }
+   std::snprintf(names, name_cap, "%s", s.c_str());
+   *n_out = m;
+   return RHGPU_OK;
+}
+
+int rhgpu_last_launch_count(rhgpu_ctx* c, int64_t* out) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "bad arguments");
+   *out = c->launchesStep;
+   return RHGPU_OK;
+}
+
+int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "bad arguments");
+   return fail(RHGPU_ERR_STATE, "reduce_diagnostics: not available in this build");
+}
+
+}  // extern "C"

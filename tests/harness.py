@@ -96,3 +96,37 @@ def closed_box_config(nx=12, ny=10, nz=9, ppc=4.0, two_species=True, **kw):
                   max_whistler_velocity=1500e3, electric_field_linear_smoothing_number=1,
                   electric_field_smoothing_gauss_sigma=0.8, populations=pops, name="closed_box")
     return c.replace(**kw) if kw else c
+
+
+SUM_COUNTERS = ("particleEscape", "particleEscapeKineticEnergy", "particleImpact", "particleImpactKineticEnergy")
+
+
+def assert_state_equal(a, b, what="", bitwise=True, rtol=0.0, sum_rtol=1e-12):
+    """GPU-vs-oracle comparison: arrays and particles bitwise (or within rtol
+    relative to each array's max), integer counters exact, FP-sum counters
+    (escape/impact, accumulated with atomics on the GPU) within sum_rtol."""
+    for n in STATE_ARRAYS:
+        x, y = a["arrays"][n], b["arrays"][n]
+        if bitwise:
+            if not np.array_equal(x.view(np.uint64), y.view(np.uint64)):
+                bad = np.argwhere(x.view(np.uint64) != y.view(np.uint64))
+                raise AssertionError(f"{what}: {n} differs at {bad[:4].tolist()}, rel {rel_err(x, y):.3e}")
+        else:
+            e = rel_err(x, y)
+            assert e <= rtol, f"{what}: {n} rel err {e:.3e} > {rtol}"
+    for s, ((ca, pa), (cb, pb)) in enumerate(zip(a["particles"], b["particles"])):
+        assert np.array_equal(ca, cb), f"{what}: species {s} counts differ ({ca.sum()} vs {cb.sum()})"
+        if bitwise:
+            assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64)), \
+                f"{what}: species {s} particles differ, rel {rel_err(pa, pb):.3e}"
+        else:
+            for col in range(7):
+                e = rel_err(pa[:, col], pb[:, col])
+                assert e <= rtol, f"{what}: species {s} column {col} rel err {e:.3e}"
+    for k, v in a["counters"].items():
+        w = b["counters"][k]
+        if k.split("[")[0] in SUM_COUNTERS:
+            assert abs(v - w) <= sum_rtol * max(abs(w), 1e-300), f"{what}: counter {k}: {v} vs {w}"
+        else:
+            assert v == w, f"{what}: counter {k}: {v} != {w}"
+    assert a["time"][1] == b["time"][1] and abs(a["time"][0] - b["time"][0]) <= 1e-12 * max(1.0, abs(b["time"][0]))
