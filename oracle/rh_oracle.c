@@ -60,8 +60,14 @@ typedef struct {
    int useIFT;
    double dxBelow;
    double cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*RHO_MAX_SPECIES];
-   int depositOrder;
+   int depositOrder;   /* RHO_DEPOSIT_REFERENCE: cell storage; RHO_DEPOSIT_GPU: dual-cell storage */
    int nthreads;
+   /* fast-path restatement (dual-cell storage) */
+   int nd[3];          /* dual cells per axis: n (periodic) or n+1 */
+   size_t Nd;
+   double* RP;         /* row partial moments, 4 planes x rows x nx x 4 */
+   __int128* MM;       /* fixed-point moments of off-row movers, 4 x N (exact sums) */
+   int kR, kJ;         /* fixed-point exponents of charge and current */
 } Ctx;
 
 #define ALL_NBRS ((1u<<27)-1u)
@@ -74,6 +80,10 @@ typedef struct {
 #define ZNEG (1u<<TID(0,0,-1))
 
 static inline double sqr(double x) { return x*x; }
+static int dualUpload(Ctx* c,int sidx,const uint32_t* counts,const double* parts,int64_t n);
+static int dualDownload(Ctx* c,int sidx,uint32_t* counts,double* parts);
+static void dualPushAll(Ctx* c);
+static void dualGather(Ctx* c);
 static inline int nb(const Ctx* c,size_t b,int di,int dj,int dk) { return c->nbr[b*27 + TID(di,dj,dk)]; }
 static int arrayDim(int id) {
    return (id == RHGPU_CELL_RHOQI || id == RHGPU_NODE_RHOQI || id == RHGPU_NODE_ETA) ? 1 : 3;
@@ -132,10 +142,14 @@ int rho_create(const rhgpu_params* P,int32_t ns,const rhgpu_species* sp,const in
    }
    for (int a=0;a<RHGPU_NUM_ARRAYS;++a) c->arr[a] = (double*)calloc(c->N*arrayDim(a),sizeof(double));
    c->faceJ = (double*)calloc(3*c->N,sizeof(double));
+   for (int a=0;a<3;++a) c->nd[a] = (a==0 ? c->nx : a==1 ? c->ny : c->nz) + (P->periodic[a] ? 0 : 1);
+   c->Nd = (size_t)c->nd[0]*c->nd[1]*c->nd[2];
    for (int s=0;s<ns;++s) {
-      c->pop[s].cnt = (uint32_t*)calloc(c->N,sizeof(uint32_t));
-      c->pop[s].start = (int64_t*)calloc(c->N+1,sizeof(int64_t));
+      c->pop[s].cnt = (uint32_t*)calloc(c->Nd,sizeof(uint32_t));
+      c->pop[s].start = (int64_t*)calloc(c->Nd+1,sizeof(int64_t));
    }
+   c->RP = (double*)calloc((size_t)16*c->nd[1]*c->nd[2]*c->nx,sizeof(double));
+   c->MM = (__int128*)calloc(4*c->N,sizeof(__int128));
    c->t = P->t_initial;
    c->timestep = 0;
    c->useIFT = P->use_initial_flow_through;
@@ -150,6 +164,7 @@ int rho_destroy(void* h) {
    Ctx* c = (Ctx*)h;
    if (!c) return 0;
    free(c->nbr); free(c->nflags); free(c->cflags); free(c->exterior); free(c->faceJ);
+   free(c->RP); free(c->MM);
    for (int a=0;a<RHGPU_NUM_ARRAYS;++a) free(c->arr[a]);
    for (int s=0;s<c->ns;++s) { free(c->pop[s].p); free(c->pop[s].cnt); free(c->pop[s].start); }
    free(c);
@@ -194,6 +209,7 @@ int rho_upload_particles(void* h,int32_t sidx,const uint32_t* counts,const doubl
    int64_t tot = 0;
    for (size_t b=0;b<c->N;++b) tot += counts[b];
    if (tot != n) return fail(RHGPU_ERR_ARG,"sum(counts) != n_particles");
+   if (c->depositOrder == RHO_DEPOSIT_GPU) return dualUpload(c,sidx,counts,parts,n);
    popReserve(s,n);
    memcpy(s->cnt,counts,sizeof(uint32_t)*c->N);
    if (n) memcpy(s->p,parts,sizeof(double)*7*n);
@@ -205,6 +221,8 @@ int rho_download_particles(void* h,int32_t sidx,uint32_t* counts,double* parts,i
    Ctx* c = (Ctx*)h;
    PopStore* s = &c->pop[sidx];
    if (s->n > cap) return fail(RHGPU_ERR_ARG,"capacity too small");
+   *nout = s->n;
+   if (c->depositOrder == RHO_DEPOSIT_GPU) return dualDownload(c,sidx,counts,parts);
    memcpy(counts,s->cnt,sizeof(uint32_t)*c->N);
    if (s->n) memcpy(parts,s->p,sizeof(double)*7*s->n);
    *nout = s->n;
@@ -216,8 +234,9 @@ int rho_download_particles(void* h,int32_t sidx,uint32_t* counts,double* parts,i
  * with getFields (hybrid_propagator.cpp:1879-1891): face2r (:1740-1778) for B,
  * cell2r (:1838-1858) for Ue and Ep. */
 
-static void pushCell(Ctx* c,int sidx,size_t b) {
-   PopStore* s = &c->pop[sidx];
+/* push of one particle st[7] (local coordinates in cell b); returns 1 if
+ * the maximum ion speed clamp was applied */
+static int pushParticle(Ctx* c,int sidx,size_t b,double* st) {
    const rhgpu_params* P = &c->P;
    const rhgpu_species* S = &c->sp[sidx];
    const int ci = (int)(b % c->nx), cj = (int)((b / c->nx) % c->ny), ck = (int)(b / ((size_t)c->nx*c->ny));
@@ -230,9 +249,8 @@ static void pushCell(Ctx* c,int sidx,size_t b) {
    const double* cellUe = c->arr[RHGPU_CELL_UE];
    const double* cellEp = c->arr[RHGPU_CELL_EP];
    const double dt = P->dt, dx = P->dx;
-   double* cntMaxVi = &c->cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*sidx + 0];
-   for (int64_t p=s->start[b];p<s->start[b+1];++p) {
-      double* st = s->p + 7*p;
+   int clamped = 0;
+   {
       if (accelerate) {
          double B[3],Ue[3],Ep[3] = {0,0,0},E[3];
          const double rGlobal[3] = {st[0]+xBlock,st[1]+yBlock,st[2]+zBlock};
@@ -288,7 +306,7 @@ static void pushCell(Ctx* c,int sidx,size_t b) {
          if (v2 > P->max_ion_speed2) {
             const double norm = sqrt(P->max_ion_speed2/v2);
             st[3] *= norm; st[4] *= norm; st[5] *= norm;
-            *cntMaxVi += 1;
+            clamped = 1;
          }
       }
       /* drift (boris.h:191-193) */
@@ -296,6 +314,13 @@ static void pushCell(Ctx* c,int sidx,size_t b) {
       st[1] += dt*st[4];
       st[2] += dt*st[5];
    }
+   return clamped;
+}
+
+static void pushCell(Ctx* c,int sidx,size_t b) {
+   PopStore* s = &c->pop[sidx];
+   double* cntMaxVi = &c->cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*sidx + 0];
+   for (int64_t p=s->start[b];p<s->start[b+1];++p) *cntMaxVi += pushParticle(c,sidx,b,s->p + 7*p);
 }
 
 /* canonical migration (oracle_common.h) */
@@ -343,6 +368,7 @@ int rho_push(void* h) {
    Ctx* c = (Ctx*)h;
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
+   if (c->depositOrder == RHO_DEPOSIT_GPU) { dualPushAll(c); return 0; }
    for (int s=0;s<c->ns;++s) {
       if (c->nthreads > 1) {
          /* the speed-clamp counter is summed per thread in pushCell; use
@@ -419,21 +445,17 @@ static void depositReference(Ctx* c,int sidx) {
    }
 }
 
-/* GPU deposit order: see rhybrid_b200/csrc/rh_deposit.cuh. Each cell's
- * value is the sum, over its 27 source cells in increasing source index
- * order, of the source cell's sequential per-particle sum (the reference
- * order); the GPU kernels reproduce exactly this sum, so both orders agree. */
-static void depositGpuOrder(Ctx* c,int sidx) { depositReference(c,sidx); }
 
 int rho_accumulate(void* h) {
    Ctx* c = (Ctx*)h;
+   if (c->depositOrder == RHO_DEPOSIT_GPU) { dualGather(c); return 0; }
    double* rho = c->arr[RHGPU_CELL_RHOQI];
    double* Ji = c->arr[RHGPU_CELL_JI];
    memset(rho,0,sizeof(double)*c->N);
    memset(Ji,0,sizeof(double)*3*c->N);
    for (int s=0;s<c->ns;++s) {
       if (!c->sp[s].accumulate) continue;
-      if (c->depositOrder == RHO_DEPOSIT_GPU) depositGpuOrder(c,s); else depositReference(c,s);
+      depositReference(c,s);
    }
    const double dV = c->P.dx*c->P.dx*c->P.dx;
    for (size_t n=0;n<c->N;++n) {
@@ -451,6 +473,8 @@ int rho_accumulate(void* h) {
 /* particle boundary conditions (particle_boundary_cond_hybrid.h:112-185) */
 int rho_apply_boundaries(void* h) {
    Ctx* c = (Ctx*)h;
+   /* the fast path removes boundary particles inside its push (dualPushAll) */
+   if (c->depositOrder == RHO_DEPOSIT_GPU) return 0;
    for (int sidx=0;sidx<c->ns;++sidx) {
       PopStore* s = &c->pop[sidx];
       double* q = &c->cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*sidx];
@@ -500,6 +524,251 @@ int rho_apply_boundaries(void* h) {
       popStarts(c,s);
    }
    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Fast-path restatement (RHO_DEPOSIT_GPU): the order of operations of the
+ * GPU's fused push-and-deposit kernel, so that its results can be checked bit
+ * for bit. The arithmetic per particle and per cell is the reference's; only
+ * the order in which the CIC contributions are summed, and the order of the
+ * particles inside the storage, differ from RHO_DEPOSIT_REFERENCE.
+ *
+ * Storage: particles are grouped by CIC dual cell, the 2x2x2 block of cells
+ * whose centres surround the particle: base cell b = c + s - 1 per axis with
+ * s = 0 if x < 0.5 dx else 1 (the shift of accumulateCell, :78-84). Dual index
+ * u = b + 1 on a non-periodic axis (n+1 dual cells), b mod n on a periodic one.
+ * A dual row is the run of dual cells with the same (uy, uz).
+ *
+ * Step, per dual row, dual cells in increasing ux, species in order, particles
+ * in storage order: push (pushParticle), drift, migrate (rh_migrate_canonical),
+ * then the CIC weights of the new position. If the new dual cell is in the same
+ * row and at most one step away in x without wrapping, the particle's 8x4
+ * contributions are added to that dual cell's running sums (acc[u'][corner][q],
+ * q = rhoq, Jx, Jy, Jz); otherwise they are added, as 64-bit fixed point
+ * (value * 2^k rounded to nearest), to the moments of the 8 destination cells
+ * (MM). Each destination x of the row receives the row partial
+ *    RP[(oy,oz)][row][x][q] = acc[u_lo(x)][ox=1,oy,oz][q] + acc[u_hi(x)][ox=0,oy,oz][q]
+ * where u_lo/u_hi are the two dual cells of the row that contain x. A cell's
+ * moment is RP(0,0) + RP(1,0) + RP(0,1) + RP(1,1) (rows of base y-oy, z-oz)
+ * + MM*2^-k, then /dV and the minimum charge density clamp.
+ * Particles that end in an exterior cell, or inside the obstacle of a flagged
+ * cell, are deposited and then removed (the boundary conditions of the step);
+ * particles leaving the box are removed before depositing.
+ * New storage of a dual cell: its stayers in their previous order, then the
+ * particles from the x-neighbour dual cells of the row, then all others, each
+ * group in order of (source dual index, position in the source).
+ */
+static inline int dualU(int b,int n,int per) { return per ? ((b % n) + n) % n : b + 1; }
+static inline int dualB(int u,int per) { return per ? u : u - 1; }
+static inline int halfS(double x,double dx) { return (x < (0+0.5)*dx) ? 0 : 1; }
+
+static size_t dualIndexOf(const Ctx* c,int i,int j,int k,const double* st) {
+   const double dx = c->P.dx;
+   const int ux = dualU(i + halfS(st[0],dx) - 1,c->nx,c->P.periodic[0]);
+   const int uy = dualU(j + halfS(st[1],dx) - 1,c->ny,c->P.periodic[1]);
+   const int uz = dualU(k + halfS(st[2],dx) - 1,c->nz,c->P.periodic[2]);
+   return (size_t)ux + c->nd[0]*((size_t)uy + c->nd[1]*(size_t)uz);
+}
+
+/* cell of a particle stored in dual cell (ux,uy,uz) */
+static size_t cellOfDual(const Ctx* c,int ux,int uy,int uz,const double* st) {
+   const double dx = c->P.dx;
+   int i = dualB(ux,c->P.periodic[0]) + 1 - halfS(st[0],dx);
+   int j = dualB(uy,c->P.periodic[1]) + 1 - halfS(st[1],dx);
+   int k = dualB(uz,c->P.periodic[2]) + 1 - halfS(st[2],dx);
+   rh_wrap(&i,c->nx,1); rh_wrap(&j,c->ny,1); rh_wrap(&k,c->nz,1);
+   return (size_t)i + c->nx*((size_t)j + c->ny*(size_t)k);
+}
+
+static void dualStarts(Ctx* c,PopStore* s) {
+   s->start[0] = 0;
+   for (size_t d=0;d<c->Nd;++d) s->start[d+1] = s->start[d] + s->cnt[d];
+   s->n = s->start[c->Nd];
+}
+
+/* stable counting sort of n records (7 doubles) by key[] in [0,nkeys) */
+static void sortRecords(const double* in,const int64_t* key,int64_t n,int64_t nkeys,double* out,uint32_t* cntOut) {
+   int64_t* start = (int64_t*)calloc(nkeys+1,sizeof(int64_t));
+   for (int64_t p=0;p<n;++p) start[key[p]+1]++;
+   if (cntOut) for (int64_t q=0;q<nkeys;++q) cntOut[q] = (uint32_t)start[q+1];
+   for (int64_t q=0;q<nkeys;++q) start[q+1] += start[q];
+   for (int64_t p=0;p<n;++p) memcpy(out + 7*(start[key[p]]++),in + 7*p,7*sizeof(double));
+   free(start);
+}
+
+/* the fixed-point exponents: the largest possible contribution times 2^k
+ * stays below 2^62 (charge: max |w q|; current: max |w q| times 2 dx/dt, the
+ * largest velocity component of a particle that moved at most one cell) */
+static void fixedPointExponents(Ctx* c) {
+   double bR = 0.0;
+   for (int s=0;s<c->ns;++s) {
+      const PopStore* ps = &c->pop[s];
+      double mw = 0.0;
+      for (int64_t p=0;p<ps->n;++p) if (fabs(ps->p[7*p+6]) > mw) mw = fabs(ps->p[7*p+6]);
+      const double b = mw*fabs(c->sp[s].q);
+      if (b > bR) bR = b;
+   }
+   const double bJ = bR*(2.0*c->P.dx/c->P.dt);
+   int e;
+   frexp(bR > 0 ? bR : 1.0,&e); c->kR = 62 - e;
+   frexp(bJ > 0 ? bJ : 1.0,&e); c->kJ = 62 - e;
+}
+
+static int dualUpload(Ctx* c,int sidx,const uint32_t* counts,const double* parts,int64_t n) {
+   PopStore* s = &c->pop[sidx];
+   int64_t* key = (int64_t*)malloc(sizeof(int64_t)*(n > 0 ? n : 1));
+   int64_t p = 0;
+   for (size_t b=0;b<c->N;++b) {
+      const int i = (int)(b % c->nx), j = (int)((b / c->nx) % c->ny), k = (int)(b / ((size_t)c->nx*c->ny));
+      for (uint32_t t=0;t<counts[b];++t,++p) key[p] = (int64_t)dualIndexOf(c,i,j,k,parts + 7*p);
+   }
+   popReserve(s,n);
+   sortRecords(parts,key,n,(int64_t)c->Nd,s->p,s->cnt);
+   dualStarts(c,s);
+   free(key);
+   fixedPointExponents(c);
+   return 0;
+}
+
+static int dualDownload(Ctx* c,int sidx,uint32_t* counts,double* parts) {
+   PopStore* s = &c->pop[sidx];
+   int64_t* key = (int64_t*)malloc(sizeof(int64_t)*(s->n > 0 ? s->n : 1));
+   for (size_t d=0;d<c->Nd;++d) {
+      const int ux = (int)(d % c->nd[0]), uy = (int)((d / c->nd[0]) % c->nd[1]), uz = (int)(d / ((size_t)c->nd[0]*c->nd[1]));
+      for (int64_t p=s->start[d];p<s->start[d+1];++p) key[p] = (int64_t)cellOfDual(c,ux,uy,uz,s->p + 7*p);
+   }
+   sortRecords(s->p,key,s->n,(int64_t)c->N,parts,counts);
+   free(key);
+   return 0;
+}
+
+static void dualPushAll(Ctx* c) {
+   const rhgpu_params* P = &c->P;
+   const double dx = P->dx;
+   const int ndx = c->nd[0], ndy = c->nd[1], ndz = c->nd[2];
+   const size_t nrows = (size_t)ndy*ndz;
+   memset(c->RP,0,sizeof(double)*16*nrows*c->nx);
+   memset(c->MM,0,sizeof(__int128)*4*c->N);
+   const double scaleR = ldexp(1.0,c->kR), scaleJ = ldexp(1.0,c->kJ);
+   double* nw[RHO_MAX_SPECIES];
+   int64_t* nkey[RHO_MAX_SPECIES];
+   int64_t nn[RHO_MAX_SPECIES];
+   for (int s=0;s<c->ns;++s) {
+      nw[s] = (double*)malloc(sizeof(double)*7*(c->pop[s].n > 0 ? c->pop[s].n : 1));
+      nkey[s] = (int64_t*)malloc(sizeof(int64_t)*(c->pop[s].n > 0 ? c->pop[s].n : 1));
+      nn[s] = 0;
+   }
+   double* acc = (double*)malloc(sizeof(double)*32*ndx);
+   for (int uz=0;uz<ndz;++uz) for (int uy=0;uy<ndy;++uy) {
+      memset(acc,0,sizeof(double)*32*ndx);
+      const size_t row = (size_t)uy + (size_t)ndy*uz;
+      for (int ux=0;ux<ndx;++ux) for (int s=0;s<c->ns;++s) {
+         PopStore* ps = &c->pop[s];
+         double* q5 = &c->cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*s];
+         const size_t D = (size_t)ux + ndx*row;
+         for (int64_t r=0;r<(int64_t)ps->cnt[D];++r) {
+            double st[7];
+            memcpy(st,ps->p + 7*(ps->start[D]+r),sizeof st);
+            const size_t cb = cellOfDual(c,ux,uy,uz,st);
+            q5[0] += pushParticle(c,s,cb,st);
+            const int ci = (int)(cb % c->nx), cj = (int)((cb / c->nx) % c->ny), ck = (int)(cb / ((size_t)c->nx*c->ny));
+            int off[3];
+            const int bad = rh_migrate_canonical(st,dx,c->dxBelow,off);
+            int ti = ci+off[0], tj = cj+off[1], tk = ck+off[2];
+            const int inside = rh_wrap(&ti,c->nx,P->periodic[0]) && rh_wrap(&tj,c->ny,P->periodic[1]) && rh_wrap(&tk,c->nz,P->periodic[2]);
+            const double ke = st[6]*( sqr(st[3]) + sqr(st[4]) + sqr(st[5]) );
+            if (bad || !inside) { q5[1] += st[6]; q5[2] += ke; continue; }
+            const size_t cn = (size_t)ti + c->nx*((size_t)tj + c->ny*(size_t)tk);
+            const int sx = halfS(st[0],dx), sy = halfS(st[1],dx), sz = halfS(st[2],dx);
+            const int bx = ti + sx - 1, by = tj + sy - 1, bz = tk + sz - 1;
+            const int vx = dualU(bx,c->nx,P->periodic[0]), vy = dualU(by,c->ny,P->periodic[1]), vz = dualU(bz,c->nz,P->periodic[2]);
+            const size_t Dn = (size_t)vx + ndx*((size_t)vy + (size_t)ndy*vz);
+            const int inRow = vy == uy && vz == uz && abs(vx - ux) <= 1;
+            if (c->sp[s].accumulate) {
+               double w8[8]; int ind[8];
+               cicWeights(st,c->sp[s].q,dx,w8,ind);
+               if (inRow) {
+                  double* a = acc + 32*(size_t)vx;
+                  for (int o=0;o<8;++o) {
+                     a[4*o+0] += w8[o];
+                     for (int l=0;l<3;++l) a[4*o+1+l] += w8[o]*st[3+l];
+                  }
+               } else {
+                  for (int o=0;o<8;++o) {
+                     int dxc = bx + (o&1), dyc = by + ((o>>1)&1), dzc = bz + ((o>>2)&1);
+                     if (!rh_wrap(&dxc,c->nx,P->periodic[0]) || !rh_wrap(&dyc,c->ny,P->periodic[1]) || !rh_wrap(&dzc,c->nz,P->periodic[2])) continue;
+                     const size_t dc = (size_t)dxc + c->nx*((size_t)dyc + c->ny*(size_t)dzc);
+                     c->MM[dc] += (__int128)llrint(w8[o]*scaleR);
+                     for (int l=0;l<3;++l) c->MM[(size_t)(1+l)*c->N + dc] += (__int128)llrint(w8[o]*st[3+l]*scaleJ);
+                  }
+               }
+            }
+            /* boundary conditions of the step (particle_boundary_cond_hybrid.h:112-185) */
+            if (c->nflags[cn] != ALL_NBRS) { q5[1] += st[6]; q5[2] += ke; continue; }
+            if (c->cflags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
+               const double xp = rh_block_origin(P->x_min,ti,dx) + st[0];
+               const double yp = rh_block_origin(P->y_min,tj,dx) + st[1];
+               const double zp = rh_block_origin(P->z_min,tk,dx) + st[2];
+               if (sqr(xp) + sqr(yp) + sqr(zp) < c->sp[s].R2_obstacle) { q5[3] += st[6]; q5[4] += ke; continue; }
+            }
+            const int cls = Dn == D ? 0 : (inRow ? 1 : 2);
+            memcpy(nw[s] + 7*nn[s],st,sizeof st);
+            nkey[s][nn[s]] = (int64_t)Dn*3 + cls;
+            nn[s]++;
+         }
+      }
+      /* row partials of the destinations x of this row */
+      for (int x=0;x<c->nx;++x) {
+         const int ulo = P->periodic[0] ? (x + c->nx - 1) % c->nx : x;
+         const int uhi = P->periodic[0] ? x : x + 1;
+         for (int qq=0;qq<4;++qq) for (int l=0;l<4;++l) {
+            c->RP[(((size_t)qq*nrows + row)*c->nx + x)*4 + l] =
+               acc[32*(size_t)ulo + (size_t)(1 | (qq << 1))*4 + l] + acc[32*(size_t)uhi + (size_t)(qq << 1)*4 + l];
+         }
+      }
+   }
+   free(acc);
+   for (int s=0;s<c->ns;++s) {
+      PopStore* ps = &c->pop[s];
+      uint32_t* cnt3 = (uint32_t*)calloc(3*c->Nd,sizeof(uint32_t));
+      popReserve(ps,nn[s]);
+      sortRecords(nw[s],nkey[s],nn[s],3*(int64_t)c->Nd,ps->p,cnt3);
+      for (size_t d=0;d<c->Nd;++d) ps->cnt[d] = cnt3[3*d] + cnt3[3*d+1] + cnt3[3*d+2];
+      dualStarts(c,ps);
+      free(cnt3); free(nw[s]); free(nkey[s]);
+   }
+}
+
+/* 128-bit fixed point to double: hi*2^(64-k) + lo*2^-k, each term rounded */
+static double fixedToDouble(__int128 v,int k) {
+   const int64_t hi = (int64_t)(v >> 64);
+   const uint64_t lo = (uint64_t)v;
+   return ldexp((double)hi,64 - k) + ldexp((double)lo,-k);
+}
+
+static void dualGather(Ctx* c) {
+   const rhgpu_params* P = &c->P;
+   double* rho = c->arr[RHGPU_CELL_RHOQI];
+   double* Ji = c->arr[RHGPU_CELL_JI];
+   const size_t nrows = (size_t)c->nd[1]*c->nd[2];
+   const double dV = P->dx*P->dx*P->dx;
+   for (int z=0;z<c->nz;++z) for (int y=0;y<c->ny;++y) for (int x=0;x<c->nx;++x) {
+      const size_t n = (size_t)x + c->nx*((size_t)y + c->ny*(size_t)z);
+      double v[4];
+      for (int qq=0;qq<4;++qq) {
+         const int uy = dualU(y - (qq & 1),c->ny,P->periodic[1]);
+         const int uz = dualU(z - (qq >> 1),c->nz,P->periodic[2]);
+         const size_t row = (size_t)uy + (size_t)c->nd[1]*uz;
+         const double* rp = c->RP + (((size_t)qq*nrows + row)*c->nx + x)*4;
+         for (int l=0;l<4;++l) v[l] = qq == 0 ? rp[l] : v[l] + rp[l];
+      }
+      v[0] += fixedToDouble(c->MM[n],c->kR);
+      for (int l=0;l<3;++l) v[1+l] += fixedToDouble(c->MM[(size_t)(1+l)*c->N + n],c->kJ);
+      double r = v[0]/dV;
+      if (r < P->min_ion_charge_density) { r = P->min_ion_charge_density; c->cnt[RHGPU_CNT_FIELD_MIN_CELL_RHOQI] += 1; }
+      rho[n] = r;
+      for (int l=0;l<3;++l) Ji[3*n+l] = v[1+l]/dV;
+   }
 }
 
 /* ------------------------------------------------------------------ */

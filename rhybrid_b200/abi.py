@@ -14,6 +14,10 @@ from typing import Optional
 
 import numpy as np
 
+# rhgpu.h: particle paths
+PATH_FAST = 0
+PATH_EXACT = 1
+
 # rhgpu.h: status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_DEVICE, ERR_NOMEM, ERR_CAPACITY = range(7)
 
@@ -127,6 +131,7 @@ _OPTIONAL = {
     "stream": [_P],
     "version": [],
     "set_deposit_order": [_P, C.c_int32],
+    "set_path": [_P, C.c_int32],
     "set_threads": [_P, C.c_int32],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p}
@@ -306,6 +311,19 @@ class Context:
 
     def set_deposit_order(self, order: int):
         self.lib.call("set_deposit_order", self.h, order)
+
+    def set_path(self, path: int):
+        self.lib.call("set_path", self.h, path)
+
+    def select_path(self, fast: bool):
+        """The B200 library's particle path, or the oracle's matching order:
+        fast = dual-cell storage order, else the reference's order."""
+        if self.lib.has("set_path"):
+            self.set_path(PATH_FAST if fast else PATH_EXACT)
+        elif self.lib.has("set_deposit_order"):
+            self.set_deposit_order(1 if fast else 0)
+        elif fast:
+            raise RuntimeError(f"{self.lib.prefix}: no fast-path order")
 
     def set_threads(self, n: int):
         self.lib.call("set_threads", self.h, n)

@@ -201,30 +201,74 @@ __device__ inline void cicWeights(double x, double y, double z, double wq, doubl
    }
 }
 
-// S[e*N + c], e < 27: charge of 3x3x3 entry e; e = 27 + 3*entry + l: current l
-__global__ void k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err) {
-   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// Per cell, the 3x3x3 CIC sums of accumulateCell in particle order, one warp
+// per cell: lane L owns the accumulator entries e = L, L+32, L+64, L+96
+// (e < 27: charge of 3x3x3 entry e; e = 27 + 3*entry + l: current l). The
+// particles of the cell are taken 32 at a time, each lane computing one
+// particle's CIC weights into shared memory; then every lane walks those
+// particles in order and adds the contribution that falls on its entries, so
+// each entry is the same sequential sum as in the reference.
+// S[e*N + c] receives the 108 sums of cell c.
+constexpr int DEP_WARPS = 4;
+__global__ void __launch_bounds__(32 * DEP_WARPS) k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err) {
+   __shared__ double sw[DEP_WARPS][32][11];   // w8[0..7], v[0..2] of the batch's particles
+   __shared__ int soct[DEP_WARPS][32];        // octant (i + 2j + 4k) of the corner-000 entry, -1 if invalid
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const long long c = (long long)blockIdx.x * DEP_WARPS + warp;
    if (c >= g.N) return;
-   double acc[108];
-   for (int e = 0; e < 108; ++e) acc[e] = 0.0;
-   const long long a = P.start[c];
-   const int na = P.alive[c];
-   for (int t = 0; t < na; ++t) {
-      const long long p = a + t;
-      const double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
-      const double v[3] = {P.a[3][p], P.a[4][p], P.a[5][p]};
-      const double wq = P.a[6][p] * q;
-      double w8[8];
-      int ind[8];
-      cicWeights(x, y, z, wq, g.dx, w8, ind);
-      bool ok = true;
-      for (int o = 0; o < 8; ++o) ok = ok && ind[o] >= 0 && ind[o] < 27;
-      if (!ok) { raiseError(err, RHGPU_DEVERR_NAN_PARTICLE); continue; }
-      for (int o = 0; o < 8; ++o) acc[ind[o]] += w8[o];
-      for (int l = 0; l < 3; ++l)
-         for (int o = 0; o < 8; ++o) acc[27 + ind[o] * 3 + l] += w8[o] * v[l];
+   int ea[4], eb[4], ec[4], el[4];
+   double acc[4] = {0.0, 0.0, 0.0, 0.0};
+   const int ne = lane < 12 ? 4 : 3;
+#pragma unroll
+   for (int t = 0; t < 4; ++t) {
+      const int e = lane + 32 * t;
+      int ind, l;
+      if (e < 27) { ind = e; l = -1; } else { ind = (e - 27) / 3; l = (e - 27) % 3; }
+      ea[t] = ind % 3; eb[t] = (ind / 3) % 3; ec[t] = ind / 9; el[t] = l;
    }
-   for (int e = 0; e < 108; ++e) S[(long long)e * g.N + c] = acc[e];
+   const long long a0 = P.start[c];
+   const int na = P.alive[c];
+   for (int b0 = 0; b0 < na; b0 += 32) {
+      const int nb = min(32, na - b0);
+      if (lane < nb) {
+         const long long p = a0 + b0 + lane;
+         const double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
+         const double wq = P.a[6][p] * q;
+         double w8[8];
+         int ind[8];
+         cicWeights(x, y, z, wq, g.dx, w8, ind);
+         int oct = -1;
+         const int i0 = ind[0] % 3, j0 = (ind[0] / 3) % 3, k0 = ind[0] / 9;
+         if (ind[0] >= 0 && ind[0] < 27 && i0 <= 1 && j0 <= 1 && k0 <= 1) oct = i0 + 2 * j0 + 4 * k0;
+         else raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
+#pragma unroll
+         for (int o = 0; o < 8; ++o) sw[warp][lane][o] = w8[o];
+         sw[warp][lane][8] = P.a[3][p];
+         sw[warp][lane][9] = P.a[4][p];
+         sw[warp][lane][10] = P.a[5][p];
+         soct[warp][lane] = oct;
+      }
+      __syncwarp();
+      for (int j = 0; j < nb; ++j) {
+         const int oct = soct[warp][j];
+         if (oct < 0) continue;
+         const int i0 = oct & 1, j0 = (oct >> 1) & 1, k0 = oct >> 2;
+#pragma unroll
+         for (int t = 0; t < 4; ++t) {
+            if (t >= ne) break;
+            const int ox = ea[t] - i0, oy = eb[t] - j0, oz = ec[t] - k0;
+            if ((unsigned)ox <= 1u && (unsigned)oy <= 1u && (unsigned)oz <= 1u) {
+               const double w = sw[warp][j][ox + 2 * oy + 4 * oz];
+               if (el[t] < 0) acc[t] += w;
+               else acc[t] += w * sw[warp][j][8 + el[t]];
+            }
+         }
+      }
+      __syncwarp();
+   }
+#pragma unroll
+   for (int t = 0; t < 4; ++t)
+      if (t < ne) S[(long long)(lane + 32 * t) * g.N + c] = acc[t];
 }
 
 // destination sums over the 27 source cells in increasing source index

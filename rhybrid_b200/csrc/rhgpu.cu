@@ -5,6 +5,7 @@
 // download with the ParGrid layout, counters, timing and reductions. The
 // device code is in k_particles.cuh (push, migration, deposit, particle
 // boundary conditions) and k_fields.cuh (propagateB).
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <cmath>
@@ -16,6 +17,7 @@
 #include "../../include/rhgpu.h"
 #include "k_fields.cuh"
 #include "k_particles.cuh"
+#include "k_fast.cuh"
 
 using namespace rh;
 
@@ -148,6 +150,30 @@ struct rhgpu_ctx {
    long long launchesStep = 0;
    void* staging = nullptr;      // particle record staging for upload/download
    size_t stagingBytes = 0;
+   // fast path (dual-cell storage)
+   int path = RHGPU_PATH_FAST;
+   bool uploaded = false;
+   FastGeom fg;
+   DStore ds[MAX_SPECIES] = {};
+   DStore dalt[MAX_SPECIES] = {};
+   FastBufs fb = {};
+   int* finc = nullptr;          // off-row arrivals per (species, dual cell)
+   int* ffill = nullptr;
+   long long* foff = nullptr;
+   int* fbucket = nullptr;
+   int* fover = nullptr;
+   int kR = 0, kJ = 0;
+   void* sortTmp = nullptr;
+   size_t sortTmpBytes = 0;
+   long long* ftmp64 = nullptr;         // Nd+1
+   long long* ftmpCellStart = nullptr;  // N+1
+   long long* ftmpInc64 = nullptr;      // ns*Nd+1
+   long long* foffInc = nullptr;        // ns*Nd+1
+   unsigned* fsort = nullptr;
+   long long fsortCap = 0;
+   unsigned long long* fsortSlots = nullptr;
+   long long fsortSlotsCap = 0;
+   long long capHint[MAX_SPECIES] = {};
 };
 
 namespace {
@@ -308,6 +334,7 @@ int pushAll(rhgpu_ctx* c) {
 }
 
 int accumulateAll(rhgpu_ctx* c) {
+   if (!c->S) RH_CUDA(cudaMalloc(&c->S, sizeof(double) * 108 * c->g.N));
    int last = -1, first = -1;
    for (int s = 0; s < c->ns; ++s)
       if (c->sp[s].accumulate) { if (first < 0) first = s; last = s; }
@@ -321,7 +348,7 @@ int accumulateAll(rhgpu_ctx* c) {
       if (!c->sp[s].accumulate) continue;
       {
          RH_TIME(c, "deposit_cell");
-         k_deposit_cell<<<blocks1d(g.N, 64), 64, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, c->S, c->err);
+         k_deposit_cell<<<blocks1d(g.N, DEP_WARPS), 32 * DEP_WARPS, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, c->S, c->err);
          RH_LAUNCHED(c);
       }
       {
@@ -395,6 +422,371 @@ int checkDeviceError(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+// per cell: slot range from the counts, cell index of every slot
+__global__ void k_counts_in(long long N, const uint32_t* counts, long long* cnt64, int* alive) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b < N) { cnt64[b] = counts[b]; alive[b] = (int)counts[b]; }
+   if (b == N) cnt64[N] = 0;
+}
+__global__ void k_fill_pcell(long long N, const long long* start, int* pcell) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b >= N) return;
+   for (long long p = start[b]; p < start[b + 1]; ++p) pcell[p] = (int)b;
+}
+
+int ensureStaging(rhgpu_ctx* c, size_t bytes) {
+   if (bytes <= c->stagingBytes) return RHGPU_OK;
+   cudaFree(c->staging);
+   c->staging = nullptr;
+   c->stagingBytes = 0;
+   RH_CUDA(cudaMalloc(&c->staging, bytes));
+   c->stagingBytes = bytes;
+   return RHGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fast path, host side
+
+template <class T> int growBuffer(T*& p, long long& have, long long need) {
+   if (need <= have) return RHGPU_OK;
+   cudaFree(p);
+   p = nullptr;
+   have = 0;
+   const long long n = need + need / 8 + 64;
+   RH_CUDA(cudaMalloc(&p, sizeof(T) * n));
+   have = n;
+   return RHGPU_OK;
+}
+
+int ensureSortTmp(rhgpu_ctx* c, size_t bytes) {
+   if (bytes <= c->sortTmpBytes) return RHGPU_OK;
+   cudaFree(c->sortTmp);
+   c->sortTmp = nullptr;
+   RH_CUDA(cudaMalloc(&c->sortTmp, bytes + 256));
+   c->sortTmpBytes = bytes + 256;
+   return RHGPU_OK;
+}
+
+// particle arrays of a dual-cell store with room for `slots` slots
+int fastReserve(DStore& d, long long slots) {
+   if (slots <= d.cap && d.a[0]) return RHGPU_OK;
+   for (int a = 0; a < 7; ++a) { cudaFree(d.a[a]); d.a[a] = nullptr; }
+   const long long n = slots + slots / 16 + 1024;
+   for (int a = 0; a < 7; ++a) RH_CUDA(cudaMalloc(&d.a[a], sizeof(double) * n));
+   d.cap = n;
+   return RHGPU_OK;
+}
+
+// slot layout with slack from per-dual counts (+ extra arrivals): d.start, returns total slots
+int fastLayout(rhgpu_ctx* c, const int* cnt, const int* extra, DStore& d, long long* total) {
+   const long long Nd = c->fg.Nd;
+   k_fast_capacity<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(Nd, cnt, extra, c->foff);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->foff, d.start, Nd + 1, c->stream));
+   RH_CUDA(cudaMemcpyAsync(total, d.start + Nd, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+// pending-mover buffers of k_fast_push_deposit: one slot per particle slot of the largest dual cell
+int fastPendingBuffers(rhgpu_ctx* c) {
+   int mx = 1;
+   for (int s = 0; s < c->ns; ++s) {
+      RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+      k_fast_max_int<<<blocks1d(c->fg.Nd, 256), 256, 0, c->stream>>>(c->ds[s].start, c->fg.Nd, c->fover);
+      RH_CUDA(cudaGetLastError());
+      int m = 0;
+      RH_CUDA(cudaMemcpyAsync(&m, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      mx = std::max(mx, m);
+   }
+   if (mx > c->fb.pendCap) {
+      cudaFree(c->fb.pend);
+      c->fb.pend = nullptr;
+      const long long n = c->fg.nrows * c->ns * 2LL * mx * 8LL;
+      RH_CUDA(cudaMalloc(&c->fb.pend, sizeof(double) * n));
+      c->fb.pendCap = mx;
+   }
+   return RHGPU_OK;
+}
+
+// fixed-point exponents of the off-row deposit from the largest |w q| (oracle: fixedPointExponents)
+int fastExponents(rhgpu_ctx* c) {
+   double bR = 0.0;
+   for (int s = 0; s < c->ns; ++s) {
+      unsigned long long* mw = (unsigned long long*)c->fover;
+      RH_CUDA(cudaMemsetAsync(mw, 0, sizeof(unsigned long long), c->stream));
+      k_fast_max_abs_w<<<blocks1d(c->fg.Nd, 256), 256, 0, c->stream>>>(c->ds[s], c->fg.Nd, mw);
+      RH_CUDA(cudaGetLastError());
+      unsigned long long bits = 0;
+      RH_CUDA(cudaMemcpyAsync(&bits, mw, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      double w;
+      std::memcpy(&w, &bits, sizeof w);
+      const double b = w * std::fabs(c->sp[s].q);
+      if (b > bR) bR = b;
+   }
+   const double bJ = bR * (2.0 * c->P.dx / c->P.dt);
+   int e;
+   std::frexp(bR > 0 ? bR : 1.0, &e);
+   c->kR = 62 - e;
+   std::frexp(bJ > 0 ? bJ : 1.0, &e);
+   c->kJ = 62 - e;
+   c->fb.scaleR = std::ldexp(1.0, c->kR);
+   c->fb.scaleJ = std::ldexp(1.0, c->kJ);
+   return RHGPU_OK;
+}
+
+int fastMoverBuffers(rhgpu_ctx* c) {
+   long long tot = 0;
+   for (int s = 0; s < c->ns; ++s) tot += c->ds[s].cap;
+   const long long want = std::max(1LL << 20, tot / 8);
+   if (want > c->fb.moverCap) {
+      cudaFree(c->fb.movers);
+      cudaFree(c->fbucket);
+      c->fb.movers = nullptr;
+      c->fbucket = nullptr;
+      c->fb.moverCap = 0;
+      RH_CUDA(cudaMalloc(&c->fb.movers, sizeof(Mover) * want));
+      RH_CUDA(cudaMalloc(&c->fbucket, sizeof(int) * want));
+      c->fb.moverCap = want;
+   }
+   return RHGPU_OK;
+}
+
+FastSpecies fastSpecies(rhgpu_ctx* c) {
+   FastSpecies F;
+   std::memset(&F, 0, sizeof F);
+   F.ns = c->ns;
+   for (int s = 0; s < c->ns; ++s) {
+      F.st[s] = c->ds[s];
+      F.sp[s] = speciesDev(c, s);
+   }
+   return F;
+}
+
+__global__ void k_iota(unsigned* v, long long n) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) v[t] = (unsigned)t;
+}
+__global__ void k_int_to64(const int* in, long long n, long long* out) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t < n) out[t] = in[t];
+   if (t == n) out[n] = 0;
+}
+
+// relayout all species with room for their pending off-row arrivals (finc), order kept
+int fastRepack(rhgpu_ctx* c, bool withArrivals) {
+   const long long Nd = c->fg.Nd;
+   for (int s = 0; s < c->ns; ++s) {
+      DStore& from = c->ds[s];
+      DStore& to = c->dalt[s];
+      long long total = 0;
+      int rc = fastLayout(c, from.cnt, withArrivals ? c->finc + (long long)s * Nd : nullptr, to, &total);
+      if (rc) return rc;
+      rc = fastReserve(to, total);
+      if (rc) return rc;
+      k_fast_repack_copy<<<blocks1d(Nd, 128), 128, 0, c->stream>>>(Nd, from, to);
+      RH_CUDA(cudaGetLastError());
+      std::swap(c->ds[s], c->dalt[s]);
+   }
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   int rc = fastPendingBuffers(c);
+   if (rc) return rc;
+   return fastMoverBuffers(c);
+}
+
+int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n) {
+   const long long N = c->g.N, Nd = c->fg.Nd;
+   int rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   rc = ensureKeyCapacity(c, 2 * n + 2);
+   if (rc) return rc;
+   double* aos = (double*)c->staging;
+   uint32_t* dcounts = (uint32_t*)((char*)c->staging + sizeof(double) * 7 * (size_t)(n > 0 ? n : 1));
+   RH_CUDA(cudaMemcpyAsync(dcounts, counts, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream));
+   if (n) RH_CUDA(cudaMemcpyAsync(aos, particles, sizeof(double) * 7 * n, cudaMemcpyHostToDevice, c->stream));
+   // cell of every record
+   int* pcell = c->rank;
+   long long* cstart = c->ftmpCellStart;
+   k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, c->outCount);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, cstart, N + 1, c->stream));
+   long long total = 0;
+   RH_CUDA(cudaMemcpyAsync(&total, cstart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (total != n) return fail(RHGPU_ERR_ARG, "upload_particles: sum(counts) != n_particles");
+   k_fill_pcell<<<blocks1d(N, 128), 128, 0, c->stream>>>(N, cstart, pcell);
+   RH_CUDA(cudaGetLastError());
+   // dual index of every record, stable sort by it
+   rc = growBuffer(c->fsort, c->fsortCap, 2 * n + 2);
+   if (rc) return rc;
+   unsigned* keyIn = (unsigned*)c->key;
+   unsigned* keyOut = keyIn + (n + 1);
+   unsigned* idxIn = (unsigned*)c->fsort;
+   unsigned* idxOut = idxIn + (n + 1);
+   if (n) {
+      k_fast_dual_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, aos, pcell, n, keyIn);
+      k_iota<<<blocks1d(n, 256), 256, 0, c->stream>>>(idxIn, n);
+      RH_CUDA(cudaGetLastError());
+      size_t sb = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream);
+      rc = ensureSortTmp(c, sb);
+      if (rc) return rc;
+      sb = c->sortTmpBytes;
+      RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream));
+   }
+   DStore& D = c->ds[s];
+   RH_CUDA(cudaMemsetAsync(D.cnt, 0, sizeof(int) * Nd, c->stream));
+   if (n) {
+      k_fast_histogram<<<blocks1d(n, 256), 256, 0, c->stream>>>(keyOut, n, D.cnt);
+      RH_CUDA(cudaGetLastError());
+   }
+   long long slots = 0;
+   rc = fastLayout(c, D.cnt, nullptr, D, &slots);
+   if (rc) return rc;
+   rc = fastReserve(D, slots);
+   if (rc) return rc;
+   // first sorted position of every dual cell
+   k_int_to64<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(D.cnt, Nd, c->ftmp64);
+   RH_CUDA(cudaGetLastError());
+   bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->foff, Nd + 1, c->stream));
+   if (n) {
+      k_fast_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(aos, keyOut, idxOut, n, c->foff, D);
+      RH_CUDA(cudaGetLastError());
+   }
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   rc = fastPendingBuffers(c);
+   if (rc) return rc;
+   rc = fastExponents(c);
+   if (rc) return rc;
+   return fastMoverBuffers(c);
+}
+
+int fastNumParticles(rhgpu_ctx* c, int s, long long* n) {
+   const long long Nd = c->fg.Nd;
+   k_int_to64<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(c->ds[s].cnt, Nd, c->ftmp64);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->foff, Nd + 1, c->stream));
+   RH_CUDA(cudaMemcpyAsync(n, c->foff + Nd, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long long capacity, long long* n_out) {
+   const long long N = c->g.N, Nd = c->fg.Nd;
+   long long tot = 0;
+   int rc = fastNumParticles(c, s, &tot);   // leaves the sequence offsets in c->foff
+   if (rc) return rc;
+   if (tot > capacity) return fail(RHGPU_ERR_ARG, "download_particles: capacity too small");
+   rc = ensureKeyCapacity(c, 2 * tot + 2);
+   if (rc) return rc;
+   rc = growBuffer(c->fsortSlots, c->fsortSlotsCap, tot + 1);
+   if (rc) return rc;
+   rc = growBuffer(c->fsort, c->fsortCap, 2 * tot + 2);
+   if (rc) return rc;
+   rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(tot > 0 ? tot : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   unsigned* keyIn = (unsigned*)c->key;
+   unsigned* keyOut = keyIn + (tot + 1);
+   unsigned* idxIn = (unsigned*)c->fsort;
+   unsigned* idxOut = idxIn + (tot + 1);
+   double* aos = (double*)c->staging;
+   int* cellCnt = c->outCount;
+   RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
+   if (tot) {
+      k_fast_cell_keys<<<blocks1d(Nd, 128), 128, 0, c->stream>>>(c->g, c->fg, c->ds[s], c->foff, keyIn, c->fsortSlots);
+      k_iota<<<blocks1d(tot, 256), 256, 0, c->stream>>>(idxIn, tot);
+      RH_CUDA(cudaGetLastError());
+      size_t sb = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream);
+      rc = ensureSortTmp(c, sb);
+      if (rc) return rc;
+      sb = c->sortTmpBytes;
+      RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream));
+      k_fast_histogram<<<blocks1d(tot, 256), 256, 0, c->stream>>>(keyOut, tot, cellCnt);
+      k_fast_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(c->ds[s], c->fsortSlots, idxOut, tot, aos);
+      RH_CUDA(cudaGetLastError());
+   }
+   RH_CUDA(cudaMemcpyAsync(counts, cellCnt, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
+   if (tot && particles) RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   *n_out = tot;
+   return RHGPU_OK;
+}
+
+// fused push + deposit, then placement of the off-row movers
+int fastPush(rhgpu_ctx* c) {
+   c->timestep += 1;
+   if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
+   PushParams pp;
+   pp.useIFT = c->useIFT;
+   pp.use_ep = c->P.use_electron_pressure;
+   pp.use_gravity = c->P.use_gravity;
+   pp.GMdt = c->P.GMdt;
+   pp.maxVi2 = c->P.max_ion_speed2;
+   const long long N = c->g.N, Nd = c->fg.Nd;
+   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
+   {
+      RH_TIME(c, "fast_push_deposit");
+      k_fast_push_deposit<<<blocks1d(c->fg.nrows, FAST_WARPS), 32 * FAST_WARPS, 0, c->stream>>>(
+         c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD, c->cntU, c->err);
+      RH_LAUNCHED(c);
+   }
+   unsigned long long nm = 0;
+   RH_CUDA(cudaMemcpyAsync(&nm, c->fb.nmovers, sizeof nm, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if ((long long)nm > c->fb.moverCap) return fail(RHGPU_ERR_CAPACITY, "off-row mover list overflow");
+   if (nm == 0) return RHGPU_OK;
+   RH_TIME(c, "fast_migrate");
+   const long long nb = (long long)c->ns * Nd;
+   RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
+   RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+   k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, Nd, c->finc);
+   RH_LAUNCHED(c);
+   k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
+   RH_LAUNCHED(c);
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
+   k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, Nd, c->foffInc, c->ffill, c->fbucket);
+   RH_LAUNCHED(c);
+   k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), Nd, c->fb.movers, c->finc, c->foffInc,
+                                                              c->fbucket, c->fover);
+   RH_LAUNCHED(c);
+   int over = 0;
+   RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (over) {
+      // some dual cells lack room for their arrivals: relayout with room, place the rest
+      int rc = fastRepack(c, true);
+      if (rc) return rc;
+      RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+      k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), Nd, c->fb.movers, c->finc,
+                                                                 c->foffInc, c->fbucket, c->fover);
+      RH_LAUNCHED(c);
+      RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      if (over) return fail(RHGPU_ERR_CAPACITY, "dual-cell relayout did not make room");
+   }
+   return RHGPU_OK;
+}
+
+int fastGather(rhgpu_ctx* c) {
+   RH_TIME(c, "fast_gather");
+   const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
+   const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
+   k_fast_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->fb, hiR, loR, hiJ, loJ,
+                                                               c->P.min_ion_charge_density, c->cntU);
+   RH_LAUNCHED(c);
+   return RHGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -402,7 +794,7 @@ extern "C" {
 const char* rhgpu_last_error(void) { return g_err.c_str(); }
 
 const char* rhgpu_version(void) {
-   return "rhgpu 0.1 sm_100a fp64 (--fmad=false, IEEE div/sqrt), deposit=reference-order";
+   return "rhgpu 0.1 sm_100a fp64 (--fmad=false, IEEE div/sqrt), paths: fast (dual-cell order, default), exact (reference order)";
 }
 
 int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_species* species,
@@ -460,20 +852,42 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->outCount, sizeof(int) * 27 * N);
    alloc((void**)&c->inPrefix, sizeof(int) * 27 * N);
    alloc((void**)&c->newCount, sizeof(long long) * (N + 1));
-   alloc((void**)&c->S, sizeof(double) * 108 * N);
    alloc((void**)&c->cntU, sizeof(unsigned long long) * NCNT_U);
    alloc((void**)&c->cntD, sizeof(double) * 4 * MAX_SPECIES);
    alloc((void**)&c->err, sizeof(unsigned));
+   // fast-path geometry and buffers
+   FastGeom& fg = c->fg;
+   for (int a = 0; a < 3; ++a) fg.nd[a] = (a == 0 ? g.nx : a == 1 ? g.ny : g.nz) + (g.per[a] ? 0 : 1);
+   fg.Nd = (long long)fg.nd[0] * fg.nd[1] * fg.nd[2];
+   fg.nrows = (long long)fg.nd[1] * fg.nd[2];
+   const long long Nd = fg.Nd, nb = (long long)n_species * fg.Nd;
+   for (int s = 0; s < n_species; ++s) {
+      alloc((void**)&c->ds[s].start, sizeof(long long) * (Nd + 1));
+      alloc((void**)&c->ds[s].cnt, sizeof(int) * Nd);
+      alloc((void**)&c->dalt[s].start, sizeof(long long) * (Nd + 1));
+      alloc((void**)&c->dalt[s].cnt, sizeof(int) * Nd);
+      c->capHint[s] = capacity ? (long long)capacity[s] : 0;
+   }
+   alloc((void**)&c->fb.RP, sizeof(double) * 16 * fg.nrows * g.nx);
+   alloc((void**)&c->fb.MMlo, sizeof(unsigned long long) * 4 * N);
+   alloc((void**)&c->fb.MMhi, sizeof(unsigned long long) * 4 * N);
+   alloc((void**)&c->fb.touched, sizeof(unsigned) * (N / 32 + 1));
+   alloc((void**)&c->fb.nmovers, sizeof(unsigned long long));
+   alloc((void**)&c->finc, sizeof(int) * nb);
+   alloc((void**)&c->ffill, sizeof(int) * nb);
+   alloc((void**)&c->foff, sizeof(long long) * (Nd + 1));
+   alloc((void**)&c->ftmp64, sizeof(long long) * (Nd + 1));
+   alloc((void**)&c->ftmpCellStart, sizeof(long long) * (N + 1));
+   alloc((void**)&c->ftmpInc64, sizeof(long long) * (nb + 1));
+   alloc((void**)&c->foffInc, sizeof(long long) * (nb + 1));
+   alloc((void**)&c->fover, sizeof(unsigned long long));
    if (!rc) {
+      // scan scratch for the largest scan (cells, dual cells, species x dual cells)
       size_t bytes = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->newCount, c->newCount, N + 1, c->stream);
+      const long long mx = std::max(N, nb) + 1;
+      cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->foffInc, c->foffInc, mx, c->stream);
       c->scanTmpBytes = bytes;
       alloc(&c->scanTmp, bytes + 16);
-   }
-   for (int s = 0; s < n_species && !rc; ++s) {
-      const long long cap = capacity ? (long long)capacity[s] : 0;
-      rc = allocStore(c->ps[s], cap, N);
-      if (!rc) rc = allocStore(c->alt[s], cap, N);
    }
    // exterior cells (missing a neighbour) and obstacle-flagged cells are
    // listed after upload_cell_flags; exterior list now
@@ -522,6 +936,18 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->key); cudaFree(c->rank); cudaFree(c->outCount); cudaFree(c->inPrefix);
    cudaFree(c->newCount); cudaFree(c->scanTmp); cudaFree(c->S); cudaFree(c->cntU); cudaFree(c->cntD); cudaFree(c->err);
    cudaFree(c->staging);
+   for (int s = 0; s < c->ns; ++s) {
+      for (DStore* d : {&c->ds[s], &c->dalt[s]}) {
+         for (int a = 0; a < 7; ++a) cudaFree(d->a[a]);
+         cudaFree(d->start);
+         cudaFree(d->cnt);
+      }
+   }
+   cudaFree(c->fb.RP); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
+   cudaFree(c->fb.nmovers); cudaFree(c->fb.movers); cudaFree(c->fb.pend);
+   cudaFree(c->finc); cudaFree(c->ffill); cudaFree(c->foff); cudaFree(c->fbucket); cudaFree(c->fover);
+   cudaFree(c->sortTmp); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart); cudaFree(c->ftmpInc64);
+   cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots);
    for (int s = 0; s < c->ns; ++s) { freeStore(c->ps[s]); freeStore(c->alt[s]); }
    for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
    if (c->stream) cudaStreamDestroy(c->stream);
@@ -589,17 +1015,6 @@ int rhgpu_upload_cell_flags(rhgpu_ctx* c, const uint8_t* host) {
 }
 
 namespace {
-// per cell: slot range from the counts, cell index of every slot
-__global__ void k_counts_in(long long N, const uint32_t* counts, long long* cnt64, int* alive) {
-   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (b < N) { cnt64[b] = counts[b]; alive[b] = (int)counts[b]; }
-   if (b == N) cnt64[N] = 0;
-}
-__global__ void k_fill_pcell(long long N, const long long* start, int* pcell) {
-   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (b >= N) return;
-   for (long long p = start[b]; p < start[b + 1]; ++p) pcell[p] = (int)b;
-}
 // particle records (7 doubles) -> 7 component planes
 __global__ void k_aos_to_soa(const double* aos, PStore P, long long n) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -623,25 +1038,26 @@ __global__ void k_alive_to64(long long N, const int* alive, long long* out) {
    if (b < N) out[b] = alive[b];
    if (b == N) out[N] = 0;
 }
-
-int ensureStaging(rhgpu_ctx* c, size_t bytes) {
-   if (bytes <= c->stagingBytes) return RHGPU_OK;
-   cudaFree(c->staging);
-   c->staging = nullptr;
-   c->stagingBytes = 0;
-   RH_CUDA(cudaMalloc(&c->staging, bytes));
-   c->stagingBytes = bytes;
-   return RHGPU_OK;
-}
 }  // namespace
 
 int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, const double* particles, int64_t n) {
    if (!c || s < 0 || s >= c->ns || !counts || (n > 0 && !particles) || n < 0)
       return fail(RHGPU_ERR_ARG, "upload_particles: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
+   if (c->capHint[s] > 0 && n > c->capHint[s]) return fail(RHGPU_ERR_CAPACITY, "upload_particles: more particles than capacity");
+   c->uploaded = true;
+   if (c->path == RHGPU_PATH_FAST) return fastUpload(c, s, counts, particles, n);
    const long long N = c->g.N;
    PStore& P = c->ps[s];
-   if (n > P.cap) return fail(RHGPU_ERR_CAPACITY, "upload_particles: more particles than capacity");
+   if (n > P.cap) {
+      // bit-exact path storage, allocated on first use
+      const long long cap = std::max<long long>(c->capHint[s], (long long)n + n / 8 + 1024);
+      freeStore(c->ps[s]);
+      freeStore(c->alt[s]);
+      int rc0 = allocStore(c->ps[s], cap, N);
+      if (!rc0) rc0 = allocStore(c->alt[s], cap, N);
+      if (rc0) return rc0;
+   }
    int rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
    if (rc) return rc;
    double* aos = (double*)c->staging;
@@ -670,6 +1086,13 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
 int rhgpu_num_particles(rhgpu_ctx* c, int32_t s, int64_t* n_out) {
    if (!c || s < 0 || s >= c->ns || !n_out) return fail(RHGPU_ERR_ARG, "num_particles: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
+   if (c->path == RHGPU_PATH_FAST) {
+      long long t = 0;
+      int rc = fastNumParticles(c, s, &t);
+      *n_out = t;
+      return rc;
+   }
+   if (!c->ps[s].alive) { *n_out = 0; return RHGPU_OK; }
    std::vector<int> alive(c->g.N);
    RH_CUDA(cudaStreamSynchronize(c->stream));
    RH_CUDA(cudaMemcpy(alive.data(), c->ps[s].alive, sizeof(int) * c->g.N, cudaMemcpyDeviceToHost));
@@ -683,6 +1106,17 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
                              int64_t* n_out) {
    if (!c || s < 0 || s >= c->ns || !counts || !n_out) return fail(RHGPU_ERR_ARG, "download_particles: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
+   if (c->path == RHGPU_PATH_FAST) {
+      long long t = 0;
+      int rc = fastDownload(c, s, counts, particles, capacity, &t);
+      *n_out = t;
+      return rc;
+   }
+   if (!c->ps[s].alive) {
+      std::memset(counts, 0, sizeof(uint32_t) * c->g.N);
+      *n_out = 0;
+      return RHGPU_OK;
+   }
    const long long N = c->g.N;
    PStore& P = c->ps[s];
    // output offsets: exclusive scan of the alive counts (scratch: newCount, alt.start)
@@ -708,10 +1142,24 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
    return RHGPU_OK;
 }
 
+namespace {
+int phasePush(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? fastPush(c) : pushAll(c); }
+int phaseAccumulate(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? fastGather(c) : accumulateAll(c); }
+// the fast path removes boundary particles inside its push kernel
+int phaseBoundaries(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? RHGPU_OK : boundariesAll(c); }
+}  // namespace
+
+int rhgpu_set_path(rhgpu_ctx* c, int32_t path) {
+   if (!c || (path != RHGPU_PATH_FAST && path != RHGPU_PATH_EXACT)) return fail(RHGPU_ERR_ARG, "set_path: bad arguments");
+   if (c->uploaded && path != c->path) return fail(RHGPU_ERR_STATE, "set_path: particles already uploaded");
+   c->path = path;
+   return RHGPU_OK;
+}
+
 int rhgpu_push(rhgpu_ctx* c) {
    if (!c) return fail(RHGPU_ERR_ARG, "null context");
    RH_CUDA(cudaSetDevice(c->device));
-   int rc = pushAll(c);
+   int rc = phasePush(c);
    if (rc) return rc;
    return checkDeviceError(c);
 }
@@ -719,7 +1167,7 @@ int rhgpu_push(rhgpu_ctx* c) {
 int rhgpu_accumulate(rhgpu_ctx* c) {
    if (!c) return fail(RHGPU_ERR_ARG, "null context");
    RH_CUDA(cudaSetDevice(c->device));
-   int rc = accumulateAll(c);
+   int rc = phaseAccumulate(c);
    if (rc) return rc;
    return checkDeviceError(c);
 }
@@ -727,7 +1175,7 @@ int rhgpu_accumulate(rhgpu_ctx* c) {
 int rhgpu_apply_boundaries(rhgpu_ctx* c) {
    if (!c) return fail(RHGPU_ERR_ARG, "null context");
    RH_CUDA(cudaSetDevice(c->device));
-   int rc = boundariesAll(c);
+   int rc = phaseBoundaries(c);
    if (rc) return rc;
    return checkDeviceError(c);
 }
@@ -747,9 +1195,9 @@ int rhgpu_step(rhgpu_ctx* c, int32_t nsteps) {
    c->recs.clear();
    c->evUsed = 0;
    for (int n = 0; n < nsteps; ++n) {
-      int rc = pushAll(c);
-      if (!rc) rc = accumulateAll(c);
-      if (!rc) rc = boundariesAll(c);
+      int rc = phasePush(c);
+      if (!rc) rc = phaseAccumulate(c);
+      if (!rc) rc = phaseBoundaries(c);
       if (!rc) rc = fieldsAll(c);
       if (rc) return rc;
    }

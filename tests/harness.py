@@ -27,12 +27,16 @@ def snapshot(ctx):
     return st
 
 
-def run(lib, cfg, nsteps, grid=None, pops=None, capacity=None, setup=None, per_step=False):
+def run(lib, cfg, nsteps, grid=None, pops=None, capacity=None, setup=None, per_step=False, fast=False):
+    """fast=False: the reference's order (the GPU's bit-exact path, the
+    oracle's RHO_DEPOSIT_REFERENCE); fast=True: the GPU's fast path and the
+    oracle's restatement of its order."""
     if grid is None:
         grid, pops = cf.initial_state(cfg)
     cap = capacity or [int(1.5 * p[1].shape[0]) + 1024 for p in pops]
     ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=cap)
     try:
+        ctx.select_path(fast)
         if setup:
             setup(ctx)
         load(ctx, cfg, grid, pops)
@@ -130,3 +134,16 @@ def assert_state_equal(a, b, what="", bitwise=True, rtol=0.0, sum_rtol=1e-12):
         else:
             assert v == w, f"{what}: counter {k}: {v} != {w}"
     assert a["time"][1] == b["time"][1] and abs(a["time"][0] - b["time"][0]) <= 1e-12 * max(1.0, abs(b["time"][0]))
+
+
+def canonical_order(st):
+    """The same state with each cell's particles sorted by position: the fast
+    path stores a cell's particles grouped by CIC dual cell, so its per-cell
+    order differs from the reference's while the set is the same."""
+    out = {k: v for k, v in st.items() if k != "particles"}
+    out["particles"] = []
+    for cnt, p in st["particles"]:
+        cell = np.repeat(np.arange(cnt.size), cnt.astype(np.int64))
+        o = np.lexsort((p[:, 2], p[:, 1], p[:, 0], cell))
+        out["particles"].append((cnt, p[o]))
+    return out

@@ -1,15 +1,25 @@
 """GPU parity: the B200 library (through its C ABI) against the oracle
 restatement, which tests/test_oracle_pin.py pins bit for bit to the
-reference's own sources. The plain FP64 path is bit-exact: particle state,
-every grid array and the integer counters are compared bitwise; the FP64
-escape/impact sums, accumulated with atomics on the GPU, to 1e-12 relative."""
+reference's own sources.
+
+Exact path (RHGPU_PATH_EXACT): the reference's particle order and summation
+order; particle state, every grid array and the integer counters are
+compared bitwise with the oracle in reference order.
+Fast path (RHGPU_PATH_FAST, the default): particles stored by CIC dual cell,
+its own deterministic deposit order; bitwise against the oracle's
+restatement of that order, and within 1e-12 relative of the reference order.
+Both: the FP64 escape/impact sums, accumulated with atomics on the GPU,
+to 1e-12 relative."""
+import dataclasses
+
 import numpy as np
 import pytest
 
 from rhybrid_b200 import abi
 from rhybrid_b200 import config as cf
 
-from harness import (assert_state_equal, closed_box_config, load, rel_err, run, snapshot)
+from harness import (assert_state_equal, canonical_order, closed_box_config, load, rel_err, run,
+                     snapshot)
 
 pytestmark = pytest.mark.gpu
 
@@ -52,7 +62,8 @@ def test_empty_box_32cubed_100_steps(gpu_lib, port_lib):
     assert_state_equal(run(gpu_lib, cfg, 100), run(port_lib, cfg, 100), "empty box 32^3")
 
 
-def test_split_entry_points_match_step(gpu_lib, port_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_split_entry_points_match_step(gpu_lib, port_lib, fast):
     """push / accumulate / apply_boundaries / propagate_fields one at a time."""
     cfg = closed_box_config()
     grid, pops = cf.initial_state(cfg)
@@ -60,6 +71,7 @@ def test_split_entry_points_match_step(gpu_lib, port_lib):
     ctxs = [abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=cap) for lib in (gpu_lib, port_lib)]
     try:
         for c in ctxs:
+            c.select_path(fast)
             load(c, cfg, grid, pops)
         for phase in ["push", "accumulate", "apply_boundaries", "propagate_fields"] * 3:
             for c in ctxs:
@@ -97,14 +109,16 @@ def test_field_update_alone_random_moments(gpu_lib, port_lib):
             c.close()
 
 
-def test_deterministic(gpu_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_deterministic(gpu_lib, fast):
     cfg = closed_box_config()
-    a = run(gpu_lib, cfg, 5)
-    b = run(gpu_lib, cfg, 5)
+    a = run(gpu_lib, cfg, 5, fast=fast)
+    b = run(gpu_lib, cfg, 5, fast=fast)
     assert_state_equal(a, b, "two GPU runs", sum_rtol=1e-12)
 
 
-def test_charge_conservation_known_answer(gpu_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_charge_conservation_known_answer(gpu_lib, fast):
     """The reference's accumulation test (examples/test_accumulation_sum_grid.py):
     the deposited charge summed over the periodic grid equals the total
     macroparticle charge, sum(rho)*dV == sum(w)*q."""
@@ -112,6 +126,7 @@ def test_charge_conservation_known_answer(gpu_lib):
     grid, pops = cf.initial_state(cfg)
     ctx = abi.Context(gpu_lib, cf.params(cfg), cf.species(cfg), capacity=[pops[0][1].shape[0] + 64])
     try:
+        ctx.select_path(fast)
         load(ctx, cfg, grid, pops)
         ctx.push()
         ctx.accumulate()
@@ -123,22 +138,33 @@ def test_charge_conservation_known_answer(gpu_lib):
         ctx.close()
 
 
-def test_particle_upload_download_roundtrip(gpu_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_particle_upload_download_roundtrip(gpu_lib, fast):
+    """Exact path: the same particles in the same order. Fast path: the same
+    particles per cell (stored by dual cell, so the per-cell order may change)."""
     cfg = closed_box_config()
     grid, pops = cf.initial_state(cfg)
     ctx = abi.Context(gpu_lib, cf.params(cfg), cf.species(cfg), capacity=[p[1].shape[0] for p in pops])
     try:
+        ctx.select_path(fast)
         load(ctx, cfg, grid, pops)
         for s, (cnt, p) in enumerate(pops):
             c2, p2 = ctx.download_particles(s)
-            assert np.array_equal(cnt, c2) and np.array_equal(p, p2)
+            assert np.array_equal(cnt, c2)
+            if fast:
+                a = canonical_order({"particles": [(cnt, p)]})["particles"][0][1]
+                b = canonical_order({"particles": [(c2, p2)]})["particles"][0][1]
+                assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+            else:
+                assert np.array_equal(p.view(np.uint64), p2.view(np.uint64))
         for name in ("faceB", "cellB", "nodeEta"):
             assert np.array_equal(ctx.download_array(name).reshape(-1), np.asarray(grid[name]).reshape(-1))
     finally:
         ctx.close()
 
 
-def test_nonfinite_particle_raises_device_error(gpu_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_nonfinite_particle_raises_device_error(gpu_lib, fast):
     """Failure detection without a GPU fault: a corrupted particle (NaN
     velocity) is uploaded from the host; the push raises the device error word
     and rhgpu_step returns RHGPU_ERR_DEVICE; the context stays usable."""
@@ -149,6 +175,7 @@ def test_nonfinite_particle_raises_device_error(gpu_lib):
     p[5, 3] = np.nan
     ctx = abi.Context(gpu_lib, cf.params(cfg), cf.species(cfg), capacity=[p.shape[0] + 8])
     try:
+        ctx.select_path(fast)
         load(ctx, cfg, grid, [(cnt, p)])
         with pytest.raises(abi.RhError) as ei:
             ctx.step(1)
@@ -160,13 +187,85 @@ def test_nonfinite_particle_raises_device_error(gpu_lib):
         ctx.close()
 
 
-def test_capacity_is_enforced(gpu_lib):
+@pytest.mark.parametrize("fast", [False, True], ids=["exact", "fast"])
+def test_capacity_is_enforced(gpu_lib, fast):
     cfg = cf.config_empty_box(6, 6, 6, ppc=2.0)
     grid, pops = cf.initial_state(cfg)
     ctx = abi.Context(gpu_lib, cf.params(cfg), cf.species(cfg), capacity=[10])
     try:
+        ctx.select_path(fast)
         with pytest.raises(abi.RhError) as ei:
             ctx.upload_particles(0, *pops[0])
         assert ei.value.code == abi.ERR_CAPACITY
     finally:
         ctx.close()
+
+
+# ---- fast path ------------------------------------------------------------
+
+def test_fast_periodic_box_bitwise(gpu_lib, port_lib):
+    cfg = cf.config_empty_box(8, 8, 8, ppc=4.0)
+    assert_state_equal(run(gpu_lib, cfg, 25, fast=True), run(port_lib, cfg, 25, fast=True), "fast periodic 8^3")
+
+
+def test_fast_closed_box_bitwise_every_step(gpu_lib, port_lib):
+    cfg = closed_box_config()
+    a = run(gpu_lib, cfg, 8, per_step=True, fast=True)
+    b = run(port_lib, cfg, 8, per_step=True, fast=True)
+    for n, (x, y) in enumerate(zip(a, b)):
+        assert_state_equal(x, y, f"fast closed box step {n + 1}")
+
+
+@pytest.mark.parametrize("variant", ["isothermal_no_hall", "gravity_flowthrough", "mixed_periodic", "odd_sizes"])
+def test_fast_option_variants_bitwise(gpu_lib, port_lib, variant):
+    if variant == "isothermal_no_hall":
+        cfg = closed_box_config(electron_gamma=1, use_hall_term=False, electric_field_linear_smoothing_number=2,
+                                electric_field_smoothing_gauss_sigma=0.0, periodic=(1, 0, 1))
+    elif variant == "gravity_flowthrough":
+        cfg = closed_box_config(use_gravity=True, M_object=6.4e28, initial_flow_throughs=0.02,
+                                periodic=(0, 1, 0), max_electric_field=-1)
+    elif variant == "mixed_periodic":
+        cfg = closed_box_config(nx=9, ny=7, nz=11, periodic=(0, 0, 1), ppc=6.0)
+    else:
+        cfg = closed_box_config(nx=37, ny=5, nz=3, periodic=(1, 1, 0), ppc=9.0)
+    assert_state_equal(run(gpu_lib, cfg, 6, fast=True), run(port_lib, cfg, 6, fast=True), "fast " + variant)
+
+
+def test_fast_empty_box_32cubed_100_steps(gpu_lib, port_lib):
+    """The fast path on the periodic 32^3 box (655,360 ions, 100 steps):
+    bitwise against the oracle's restatement of the fast order, and within
+    1e-12 relative of the reference order (particles compared per cell)."""
+    cfg = cf.config_empty_box(32, 32, 32, ppc=20.0)
+    fast = run(gpu_lib, cfg, 100, fast=True)
+    assert_state_equal(fast, run(port_lib, cfg, 100, fast=True), "fast 32^3 vs oracle fast order")
+    ref = run(port_lib, cfg, 100, fast=False)
+    assert_state_equal(canonical_order(fast), canonical_order(ref), "fast 32^3 vs reference order",
+                       bitwise=False, rtol=1e-12)
+
+
+def test_fast_closed_box_vs_reference_order(gpu_lib, port_lib):
+    """Walls, an absorbing sphere and two species for 20 steps: the fast path
+    stays within 1e-12 relative of the reference order."""
+    cfg = closed_box_config(nx=16, ny=14, nz=12, ppc=8.0)
+    fast = run(gpu_lib, cfg, 20, fast=True)
+    ref = run(port_lib, cfg, 20, fast=False)
+    assert_state_equal(canonical_order(fast), canonical_order(ref), "fast closed box vs reference order",
+                       bitwise=False, rtol=1e-12, sum_rtol=1e-12)
+
+
+def test_fast_slack_overflow_repack(gpu_lib, port_lib):
+    """Two cold beams converging on the middle of a periodic box pile up more
+    particles in a dual cell than its slack holds: the in-row overflow and
+    repack paths stay bitwise with the oracle."""
+    cfg = cf.config_empty_box(16, 4, 4, ppc=12.0).replace(dt=0.06)
+    cfg = cfg.replace(populations=[dataclasses.replace(cfg.populations[0], temperature=1e2)])
+    grid, pops = cf.initial_state(cfg)
+    cnt, p = pops[0]
+    p = p.copy()
+    i = np.repeat(np.arange(cnt.size), cnt.astype(np.int64)) % cfg.nx
+    p[:, 3] = np.where(i < cfg.nx // 2, 1.2e6, -1.2e6)
+    pops = [(cnt, p)]
+    a = run(gpu_lib, cfg, 12, grid=grid, pops=pops, fast=True)
+    b = run(port_lib, cfg, 12, grid=grid, pops=pops, fast=True)
+    assert_state_equal(a, b, "fast converging beams")
+    assert a["particles"][0][0].max() > 1.5 * cnt.max()
