@@ -743,8 +743,10 @@ int fastPush(rhgpu_ctx* c) {
    RH_CUDA(cudaStreamSynchronize(c->stream));
    if ((long long)nm > c->fb.moverCap) return fail(RHGPU_ERR_CAPACITY, "off-row mover list overflow");
    if (nm == 0) return RHGPU_OK;
-   RH_TIME(c, "fast_migrate");
    const long long nb = (long long)c->ns * Nd;
+   int over = 0;
+   {
+   RH_TIME(c, "fast_migrate");
    RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
    RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
    RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
@@ -759,10 +761,11 @@ int fastPush(rhgpu_ctx* c) {
    k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), Nd, c->fb.movers, c->finc, c->foffInc,
                                                               c->fbucket, c->fover);
    RH_LAUNCHED(c);
-   int over = 0;
    RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+   }
    RH_CUDA(cudaStreamSynchronize(c->stream));
    if (over) {
+      RH_TIME(c, "fast_repack");
       // some dual cells lack room for their arrivals: relayout with room, place the rest
       int rc = fastRepack(c, true);
       if (rc) return rc;
