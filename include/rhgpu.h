@@ -164,16 +164,18 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
 int rhgpu_destroy(rhgpu_ctx* ctx);
 
 /* Particle path of a context, chosen before the first particle upload:
- *  RHGPU_PATH_FAST  (default) fused push + deposit over particles grouped by
- *                   CIC dual cell; the per-particle and per-cell arithmetic
- *                   is the reference's, the CIC sums are formed in a fixed
- *                   order of this library (results deterministic, equal to the
- *                   reference-order sums to round-off);
+ *  RHGPU_PATH_FAST  (default) fused push + deposit over particles binned by
+ *                   row segments of RHGPU_FAST_SEGMENT CIC dual cells; the
+ *                   per-particle and per-cell arithmetic is the reference's,
+ *                   the CIC sums are formed in a fixed order of this library
+ *                   (results deterministic, equal to the reference-order sums
+ *                   to round-off); the segment length fixes that order;
  *  RHGPU_PATH_EXACT particles grouped by cell and deposited in the reference's
  *                   summation order: bitwise identical to the reference's CPU
  *                   results, at a lower speed. */
 #define RHGPU_PATH_FAST  0
 #define RHGPU_PATH_EXACT 1
+#define RHGPU_FAST_SEGMENT 32
 int rhgpu_set_path(rhgpu_ctx* ctx, int32_t path);
 
 /* Uploads one grid array (AoS, dim values per cell, nx*ny*nz cells). */

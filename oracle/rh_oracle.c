@@ -40,6 +40,8 @@ typedef struct {
    int64_t* start;   /* N+1 offsets */
    int64_t n;
    int64_t cap;
+   uint8_t* lx;      /* fast-path storage: dual x within the segment */
+   int64_t capLx;
 } PopStore;
 
 typedef struct {
@@ -62,11 +64,14 @@ typedef struct {
    double cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*RHO_MAX_SPECIES];
    int depositOrder;   /* RHO_DEPOSIT_REFERENCE: cell storage; RHO_DEPOSIT_GPU: dual-cell storage */
    int nthreads;
-   /* fast-path restatement (dual-cell storage) */
+   /* fast-path restatement (row-segment storage) */
    int nd[3];          /* dual cells per axis: n (periodic) or n+1 */
    size_t Nd;
+   int nseg;           /* segments per dual row */
+   size_t NS;          /* segments */
    double* RP;         /* row partial moments, 4 planes x rows x nx x 4 */
-   __int128* MM;       /* fixed-point moments of off-row movers, 4 x N (exact sums) */
+   double* RPB;        /* segment-boundary partials, 4 planes x rows x nseg x 4 */
+   __int128* MM;       /* fixed-point moments of particles leaving their segment, 4 x N (exact sums) */
    int kR, kJ;         /* fixed-point exponents of charge and current */
 } Ctx;
 
@@ -144,11 +149,14 @@ int rho_create(const rhgpu_params* P,int32_t ns,const rhgpu_species* sp,const in
    c->faceJ = (double*)calloc(3*c->N,sizeof(double));
    for (int a=0;a<3;++a) c->nd[a] = (a==0 ? c->nx : a==1 ? c->ny : c->nz) + (P->periodic[a] ? 0 : 1);
    c->Nd = (size_t)c->nd[0]*c->nd[1]*c->nd[2];
+   c->nseg = (c->nd[0] + RHGPU_FAST_SEGMENT - 1)/RHGPU_FAST_SEGMENT;
+   c->NS = (size_t)c->nd[1]*c->nd[2]*c->nseg;
    for (int s=0;s<ns;++s) {
       c->pop[s].cnt = (uint32_t*)calloc(c->Nd,sizeof(uint32_t));
       c->pop[s].start = (int64_t*)calloc(c->Nd+1,sizeof(int64_t));
    }
    c->RP = (double*)calloc((size_t)16*c->nd[1]*c->nd[2]*c->nx,sizeof(double));
+   c->RPB = (double*)calloc((size_t)16*c->nd[1]*c->nd[2]*c->nseg,sizeof(double));
    c->MM = (__int128*)calloc(4*c->N,sizeof(__int128));
    c->t = P->t_initial;
    c->timestep = 0;
@@ -164,9 +172,9 @@ int rho_destroy(void* h) {
    Ctx* c = (Ctx*)h;
    if (!c) return 0;
    free(c->nbr); free(c->nflags); free(c->cflags); free(c->exterior); free(c->faceJ);
-   free(c->RP); free(c->MM);
+   free(c->RP); free(c->RPB); free(c->MM);
    for (int a=0;a<RHGPU_NUM_ARRAYS;++a) free(c->arr[a]);
-   for (int s=0;s<c->ns;++s) { free(c->pop[s].p); free(c->pop[s].cnt); free(c->pop[s].start); }
+   for (int s=0;s<c->ns;++s) { free(c->pop[s].p); free(c->pop[s].cnt); free(c->pop[s].start); free(c->pop[s].lx); }
    free(c);
    return 0;
 }
@@ -533,44 +541,42 @@ int rho_apply_boundaries(void* h) {
  * the order in which the CIC contributions are summed, and the order of the
  * particles inside the storage, differ from RHO_DEPOSIT_REFERENCE.
  *
- * Storage: particles are grouped by CIC dual cell, the 2x2x2 block of cells
- * whose centres surround the particle: base cell b = c + s - 1 per axis with
- * s = 0 if x < 0.5 dx else 1 (the shift of accumulateCell, :78-84). Dual index
- * u = b + 1 on a non-periodic axis (n+1 dual cells), b mod n on a periodic one.
- * A dual row is the run of dual cells with the same (uy, uz).
+ * Dual cells: the 2x2x2 block of cells whose centres surround the particle:
+ * base cell b = c + s - 1 per axis with s = 0 if x < 0.5 dx else 1 (the shift
+ * of accumulateCell, :78-84). Dual index u = b + 1 on a non-periodic axis
+ * (n+1 dual cells), b mod n on a periodic one. A dual row (uy, uz) is cut into
+ * segments of RHGPU_FAST_SEGMENT dual cells along x, S = row*nseg + ux/SEG.
+ * Particles are stored by segment, with their dual x within the segment.
  *
- * Step, per dual row, dual cells in increasing ux, species in order, particles
- * in storage order: push (pushParticle), drift, migrate (rh_migrate_canonical),
- * then the CIC weights of the new position. If the new dual cell is in the same
- * row and at most one step away in x without wrapping, the particle's 8x4
- * contributions are added to that dual cell's running sums (acc[u'][corner][q],
- * q = rhoq, Jx, Jy, Jz); otherwise they are added, as 64-bit fixed point
- * (value * 2^k rounded to nearest), to the moments of the 8 destination cells
- * (MM). Each destination x of the row receives the row partial
- *    RP[(oy,oz)][row][x][q] = acc[u_lo(x)][ox=1,oy,oz][q] + acc[u_hi(x)][ox=0,oy,oz][q]
- * where u_lo/u_hi are the two dual cells of the row that contain x. A cell's
- * moment is RP(0,0) + RP(1,0) + RP(0,1) + RP(1,1) (rows of base y-oy, z-oz)
- * + MM*2^-k, then /dV and the minimum charge density clamp.
+ * Step, per segment, species in order, particles in storage order: push
+ * (pushParticle), drift, migrate (rh_migrate_canonical), then the CIC weights
+ * of the new position. If the new dual cell lies in the same segment, the
+ * particle's record (new dual cell, w8, v) joins the segment's record list;
+ * otherwise its 8x4 contributions are added, as fixed point (value * 2^k
+ * rounded to nearest, summed exactly), to the moments of the 8 destination
+ * cells (MM). Per dual cell d of the segment and per (corner o, moment q):
+ *    acc[d][o][q] = 0.0, then += w8[o] * f[q] over the records of d in list
+ * order, with f = (1.0, vx, vy, vz).
+ * A cell x of the row receives corner ox = 1 of its lower dual cell u_lo and
+ * ox = 0 of its upper dual cell u_hi (non-periodic: u_lo = x, u_hi = x+1;
+ * periodic: u_lo = x-1, u_hi = x): the row partial
+ *    RP[(oy,oz)][row][x][q] = acc[u_lo][ox=1,oy,oz][q] + acc[u_hi][ox=0,oy,oz][q],
+ * formed as RP = acc_lo (+ RPB = acc_hi) when u_hi starts another segment.
+ * A cell's moment is RP(0,0) + RP(1,0) + RP(0,1) + RP(1,1) (rows of base
+ * y-oy, z-oz) + MM*2^-k, then /dV and the minimum charge density clamp.
  * Particles that end in an exterior cell, or inside the obstacle of a flagged
  * cell, are deposited and then removed (the boundary conditions of the step);
  * particles leaving the box are removed before depositing.
- * New storage of a dual cell: its stayers in their previous order, then the
- * particles from the x-neighbour dual cells of the row, then all others, each
- * group in order of (source dual index, position in the source).
+ * New storage of a segment: its stayers in their previous order, then the
+ * arrivals from other segments in order of (source segment, position in the
+ * source segment).
  */
 static inline int dualU(int b,int n,int per) { return per ? ((b % n) + n) % n : b + 1; }
 static inline int dualB(int u,int per) { return per ? u : u - 1; }
 static inline int halfS(double x,double dx) { return (x < (0+0.5)*dx) ? 0 : 1; }
+#define SEG RHGPU_FAST_SEGMENT
 
-static size_t dualIndexOf(const Ctx* c,int i,int j,int k,const double* st) {
-   const double dx = c->P.dx;
-   const int ux = dualU(i + halfS(st[0],dx) - 1,c->nx,c->P.periodic[0]);
-   const int uy = dualU(j + halfS(st[1],dx) - 1,c->ny,c->P.periodic[1]);
-   const int uz = dualU(k + halfS(st[2],dx) - 1,c->nz,c->P.periodic[2]);
-   return (size_t)ux + c->nd[0]*((size_t)uy + c->nd[1]*(size_t)uz);
-}
-
-/* cell of a particle stored in dual cell (ux,uy,uz) */
+/* cell of a particle of dual cell (ux,uy,uz) */
 static size_t cellOfDual(const Ctx* c,int ux,int uy,int uz,const double* st) {
    const double dx = c->P.dx;
    int i = dualB(ux,c->P.periodic[0]) + 1 - halfS(st[0],dx);
@@ -580,20 +586,32 @@ static size_t cellOfDual(const Ctx* c,int ux,int uy,int uz,const double* st) {
    return (size_t)i + c->nx*((size_t)j + c->ny*(size_t)k);
 }
 
-static void dualStarts(Ctx* c,PopStore* s) {
+static void segStarts(Ctx* c,PopStore* s) {
    s->start[0] = 0;
-   for (size_t d=0;d<c->Nd;++d) s->start[d+1] = s->start[d] + s->cnt[d];
-   s->n = s->start[c->Nd];
+   for (size_t d=0;d<c->NS;++d) s->start[d+1] = s->start[d] + s->cnt[d];
+   s->n = s->start[c->NS];
 }
 
-/* stable counting sort of n records (7 doubles) by key[] in [0,nkeys) */
-static void sortRecords(const double* in,const int64_t* key,int64_t n,int64_t nkeys,double* out,uint32_t* cntOut) {
+/* stable counting sort of n records (7 doubles + dual x byte) by key[] in [0,nkeys) */
+static void sortRecordsLx(const double* in,const uint8_t* inLx,const int64_t* key,int64_t n,int64_t nkeys,
+                          double* out,uint8_t* outLx,uint32_t* cntOut) {
    int64_t* start = (int64_t*)calloc(nkeys+1,sizeof(int64_t));
    for (int64_t p=0;p<n;++p) start[key[p]+1]++;
    if (cntOut) for (int64_t q=0;q<nkeys;++q) cntOut[q] = (uint32_t)start[q+1];
    for (int64_t q=0;q<nkeys;++q) start[q+1] += start[q];
-   for (int64_t p=0;p<n;++p) memcpy(out + 7*(start[key[p]]++),in + 7*p,7*sizeof(double));
+   for (int64_t p=0;p<n;++p) {
+      const int64_t d = start[key[p]]++;
+      memcpy(out + 7*d,in + 7*p,7*sizeof(double));
+      if (outLx) outLx[d] = inLx ? inLx[p] : 0;
+   }
    free(start);
+}
+
+static void popReserveLx(PopStore* s,int64_t n) {
+   if (n <= s->capLx) return;
+   popReserve(s,n);
+   s->capLx = s->cap;
+   s->lx = (uint8_t*)realloc(s->lx,s->capLx > 0 ? s->capLx : 1);
 }
 
 /* the fixed-point exponents: the largest possible contribution times 2^k
@@ -617,15 +635,24 @@ static void fixedPointExponents(Ctx* c) {
 static int dualUpload(Ctx* c,int sidx,const uint32_t* counts,const double* parts,int64_t n) {
    PopStore* s = &c->pop[sidx];
    int64_t* key = (int64_t*)malloc(sizeof(int64_t)*(n > 0 ? n : 1));
+   uint8_t* lx = (uint8_t*)malloc(n > 0 ? n : 1);
+   const double dx = c->P.dx;
    int64_t p = 0;
    for (size_t b=0;b<c->N;++b) {
       const int i = (int)(b % c->nx), j = (int)((b / c->nx) % c->ny), k = (int)(b / ((size_t)c->nx*c->ny));
-      for (uint32_t t=0;t<counts[b];++t,++p) key[p] = (int64_t)dualIndexOf(c,i,j,k,parts + 7*p);
+      for (uint32_t t=0;t<counts[b];++t,++p) {
+         const double* st = parts + 7*p;
+         const int ux = dualU(i + halfS(st[0],dx) - 1,c->nx,c->P.periodic[0]);
+         const int uy = dualU(j + halfS(st[1],dx) - 1,c->ny,c->P.periodic[1]);
+         const int uz = dualU(k + halfS(st[2],dx) - 1,c->nz,c->P.periodic[2]);
+         key[p] = ((int64_t)uy + (int64_t)c->nd[1]*uz)*c->nseg + ux/SEG;
+         lx[p] = (uint8_t)(ux % SEG);
+      }
    }
-   popReserve(s,n);
-   sortRecords(parts,key,n,(int64_t)c->Nd,s->p,s->cnt);
-   dualStarts(c,s);
-   free(key);
+   popReserveLx(s,n);
+   sortRecordsLx(parts,lx,key,n,(int64_t)c->NS,s->p,s->lx,s->cnt);
+   segStarts(c,s);
+   free(key); free(lx);
    fixedPointExponents(c);
    return 0;
 }
@@ -633,43 +660,64 @@ static int dualUpload(Ctx* c,int sidx,const uint32_t* counts,const double* parts
 static int dualDownload(Ctx* c,int sidx,uint32_t* counts,double* parts) {
    PopStore* s = &c->pop[sidx];
    int64_t* key = (int64_t*)malloc(sizeof(int64_t)*(s->n > 0 ? s->n : 1));
-   for (size_t d=0;d<c->Nd;++d) {
-      const int ux = (int)(d % c->nd[0]), uy = (int)((d / c->nd[0]) % c->nd[1]), uz = (int)(d / ((size_t)c->nd[0]*c->nd[1]));
-      for (int64_t p=s->start[d];p<s->start[d+1];++p) key[p] = (int64_t)cellOfDual(c,ux,uy,uz,s->p + 7*p);
+   for (size_t S=0;S<c->NS;++S) {
+      const size_t row = S / c->nseg;
+      const int u0 = (int)(S % c->nseg)*SEG;
+      const int uy = (int)(row % c->nd[1]), uz = (int)(row / c->nd[1]);
+      for (int64_t p=s->start[S];p<s->start[S+1];++p) key[p] = (int64_t)cellOfDual(c,u0 + s->lx[p],uy,uz,s->p + 7*p);
    }
-   sortRecords(s->p,key,s->n,(int64_t)c->N,parts,counts);
+   sortRecordsLx(s->p,NULL,key,s->n,(int64_t)c->N,parts,NULL,counts);
    free(key);
    return 0;
+}
+
+typedef struct { double st[7]; uint64_t key; int64_t dest; int lx; } OMover;
+typedef struct { int d; double w8[8]; double f[4]; } ORecord;
+
+static int cmpMover(const void* a,const void* b) {
+   const uint64_t x = ((const OMover*)a)->key, y = ((const OMover*)b)->key;
+   return x < y ? -1 : x > y;
 }
 
 static void dualPushAll(Ctx* c) {
    const rhgpu_params* P = &c->P;
    const double dx = P->dx;
-   const int ndx = c->nd[0], ndy = c->nd[1], ndz = c->nd[2];
-   const size_t nrows = (size_t)ndy*ndz;
+   const int ndx = c->nd[0], nseg = c->nseg;
+   const size_t nrows = (size_t)c->nd[1]*c->nd[2], NS = c->NS;
    memset(c->RP,0,sizeof(double)*16*nrows*c->nx);
+   memset(c->RPB,0,sizeof(double)*16*nrows*nseg);
    memset(c->MM,0,sizeof(__int128)*4*c->N);
    const double scaleR = ldexp(1.0,c->kR), scaleJ = ldexp(1.0,c->kJ);
-   double* nw[RHO_MAX_SPECIES];
-   int64_t* nkey[RHO_MAX_SPECIES];
-   int64_t nn[RHO_MAX_SPECIES];
+   /* per species: stayers (records + dual x) and their counts per segment, movers */
+   double* sw[RHO_MAX_SPECIES]; uint8_t* slx[RHO_MAX_SPECIES]; uint32_t* scnt[RHO_MAX_SPECIES]; int64_t sn[RHO_MAX_SPECIES];
+   OMover* mv[RHO_MAX_SPECIES]; int64_t mn[RHO_MAX_SPECIES];
    for (int s=0;s<c->ns;++s) {
-      nw[s] = (double*)malloc(sizeof(double)*7*(c->pop[s].n > 0 ? c->pop[s].n : 1));
-      nkey[s] = (int64_t*)malloc(sizeof(int64_t)*(c->pop[s].n > 0 ? c->pop[s].n : 1));
-      nn[s] = 0;
+      const int64_t n = c->pop[s].n > 0 ? c->pop[s].n : 1;
+      sw[s] = (double*)malloc(sizeof(double)*7*n); slx[s] = (uint8_t*)malloc(n);
+      scnt[s] = (uint32_t*)calloc(NS,sizeof(uint32_t)); sn[s] = 0;
+      mv[s] = (OMover*)malloc(sizeof(OMover)*n); mn[s] = 0;
    }
-   double* acc = (double*)malloc(sizeof(double)*32*ndx);
-   for (int uz=0;uz<ndz;++uz) for (int uy=0;uy<ndy;++uy) {
-      memset(acc,0,sizeof(double)*32*ndx);
-      const size_t row = (size_t)uy + (size_t)ndy*uz;
-      for (int ux=0;ux<ndx;++ux) for (int s=0;s<c->ns;++s) {
-         PopStore* ps = &c->pop[s];
+   int64_t maxSeg = 1;
+   for (size_t S=0;S<NS;++S) {
+      int64_t t = 0;
+      for (int s=0;s<c->ns;++s) t += c->pop[s].cnt[S];
+      if (t > maxSeg) maxSeg = t;
+   }
+   ORecord* recs = (ORecord*)malloc(sizeof(ORecord)*maxSeg);
+   double acc[SEG][32];
+   for (size_t S=0;S<NS;++S) {
+      const size_t row = S / nseg;
+      const int gseg = (int)(S % nseg);
+      const int uy = (int)(row % c->nd[1]), uz = (int)(row / c->nd[1]);
+      const int u0 = gseg*SEG, u1 = u0 + SEG < ndx ? u0 + SEG : ndx;
+      int64_t nrec = 0;
+      for (int s=0;s<c->ns;++s) {
+         const PopStore* ps = &c->pop[s];
          double* q5 = &c->cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*s];
-         const size_t D = (size_t)ux + ndx*row;
-         for (int64_t r=0;r<(int64_t)ps->cnt[D];++r) {
+         for (int64_t p=0;p<(int64_t)ps->cnt[S];++p) {
             double st[7];
-            memcpy(st,ps->p + 7*(ps->start[D]+r),sizeof st);
-            const size_t cb = cellOfDual(c,ux,uy,uz,st);
+            memcpy(st,ps->p + 7*(ps->start[S]+p),sizeof st);
+            const size_t cb = cellOfDual(c,u0 + ps->lx[ps->start[S]+p],uy,uz,st);
             q5[0] += pushParticle(c,s,cb,st);
             const int ci = (int)(cb % c->nx), cj = (int)((cb / c->nx) % c->ny), ck = (int)(cb / ((size_t)c->nx*c->ny));
             int off[3];
@@ -679,20 +727,17 @@ static void dualPushAll(Ctx* c) {
             const double ke = st[6]*( sqr(st[3]) + sqr(st[4]) + sqr(st[5]) );
             if (bad || !inside) { q5[1] += st[6]; q5[2] += ke; continue; }
             const size_t cn = (size_t)ti + c->nx*((size_t)tj + c->ny*(size_t)tk);
-            const int sx = halfS(st[0],dx), sy = halfS(st[1],dx), sz = halfS(st[2],dx);
-            const int bx = ti + sx - 1, by = tj + sy - 1, bz = tk + sz - 1;
+            const int bx = ti + halfS(st[0],dx) - 1, by = tj + halfS(st[1],dx) - 1, bz = tk + halfS(st[2],dx) - 1;
             const int vx = dualU(bx,c->nx,P->periodic[0]), vy = dualU(by,c->ny,P->periodic[1]), vz = dualU(bz,c->nz,P->periodic[2]);
-            const size_t Dn = (size_t)vx + ndx*((size_t)vy + (size_t)ndy*vz);
-            const int inRow = vy == uy && vz == uz && abs(vx - ux) <= 1;
+            const int inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (c->sp[s].accumulate) {
                double w8[8]; int ind[8];
                cicWeights(st,c->sp[s].q,dx,w8,ind);
-               if (inRow) {
-                  double* a = acc + 32*(size_t)vx;
-                  for (int o=0;o<8;++o) {
-                     a[4*o+0] += w8[o];
-                     for (int l=0;l<3;++l) a[4*o+1+l] += w8[o]*st[3+l];
-                  }
+               if (inSeg) {
+                  ORecord* r = &recs[nrec++];
+                  r->d = vx - u0;
+                  memcpy(r->w8,w8,sizeof w8);
+                  r->f[0] = 1.0; r->f[1] = st[3]; r->f[2] = st[4]; r->f[3] = st[5];
                } else {
                   for (int o=0;o<8;++o) {
                      int dxc = bx + (o&1), dyc = by + ((o>>1)&1), dzc = bz + ((o>>2)&1);
@@ -711,31 +756,72 @@ static void dualPushAll(Ctx* c) {
                const double zp = rh_block_origin(P->z_min,tk,dx) + st[2];
                if (sqr(xp) + sqr(yp) + sqr(zp) < c->sp[s].R2_obstacle) { q5[3] += st[6]; q5[4] += ke; continue; }
             }
-            const int cls = Dn == D ? 0 : (inRow ? 1 : 2);
-            memcpy(nw[s] + 7*nn[s],st,sizeof st);
-            nkey[s][nn[s]] = (int64_t)Dn*3 + cls;
-            nn[s]++;
+            if (inSeg) {
+               memcpy(sw[s] + 7*sn[s],st,sizeof st);
+               slx[s][sn[s]] = (uint8_t)(vx - u0);
+               sn[s]++;
+               scnt[s][S]++;
+            } else {
+               OMover* m = &mv[s][mn[s]++];
+               memcpy(m->st,st,sizeof st);
+               m->key = ((uint64_t)S << 32) | (uint64_t)p;
+               m->dest = ((int64_t)vy + (int64_t)c->nd[1]*vz)*nseg + vx/SEG;
+               m->lx = vx % SEG;
+            }
          }
       }
-      /* row partials of the destinations x of this row */
-      for (int x=0;x<c->nx;++x) {
-         const int ulo = P->periodic[0] ? (x + c->nx - 1) % c->nx : x;
-         const int uhi = P->periodic[0] ? x : x + 1;
-         for (int qq=0;qq<4;++qq) for (int l=0;l<4;++l) {
-            c->RP[(((size_t)qq*nrows + row)*c->nx + x)*4 + l] =
-               acc[32*(size_t)ulo + (size_t)(1 | (qq << 1))*4 + l] + acc[32*(size_t)uhi + (size_t)(qq << 1)*4 + l];
+      /* the segment's sums, records of each dual cell in list order */
+      for (int d=0;d<SEG;++d) for (int q=0;q<32;++q) acc[d][q] = 0.0;
+      for (int64_t r=0;r<nrec;++r)
+         for (int q=0;q<32;++q) acc[recs[r].d][q] += recs[r].w8[q >> 2]*recs[r].f[q & 3];
+      /* row partials of the cells whose lower dual cell is in this segment */
+      for (int dl=0;dl<u1-u0;++dl) {
+         const int lo = u0 + dl;
+         int x, hi;
+         if (P->periodic[0]) {
+            x = lo + 1 == c->nx ? 0 : lo + 1;
+            hi = lo + 1 < u1 ? dl + 1 : (nseg == 1 ? 0 : -1);
+         } else {
+            x = lo;
+            if (x >= c->nx) continue;
+            hi = lo + 1 < u1 ? dl + 1 : -1;
+         }
+         for (int qq=0;qq<4;++qq) for (int m=0;m<4;++m) {
+            double v = acc[dl][((1 + 2*qq) << 2) + m];
+            if (hi >= 0) v = v + acc[hi][((2*qq) << 2) + m];
+            c->RP[(((size_t)qq*nrows + row)*c->nx + x)*4 + m] = v;
          }
       }
+      if (P->periodic[0] ? nseg > 1 : gseg >= 1)
+         for (int qq=0;qq<4;++qq) for (int m=0;m<4;++m)
+            c->RPB[(((size_t)qq*nrows + row)*nseg + gseg)*4 + m] = acc[0][((2*qq) << 2) + m];
    }
-   free(acc);
+   free(recs);
+   /* new storage: per segment its stayers, then its arrivals by key */
    for (int s=0;s<c->ns;++s) {
       PopStore* ps = &c->pop[s];
-      uint32_t* cnt3 = (uint32_t*)calloc(3*c->Nd,sizeof(uint32_t));
-      popReserve(ps,nn[s]);
-      sortRecords(nw[s],nkey[s],nn[s],3*(int64_t)c->Nd,ps->p,cnt3);
-      for (size_t d=0;d<c->Nd;++d) ps->cnt[d] = cnt3[3*d] + cnt3[3*d+1] + cnt3[3*d+2];
-      dualStarts(c,ps);
-      free(cnt3); free(nw[s]); free(nkey[s]);
+      qsort(mv[s],mn[s],sizeof(OMover),cmpMover);
+      uint32_t* arr = (uint32_t*)calloc(NS,sizeof(uint32_t));
+      for (int64_t m=0;m<mn[s];++m) arr[mv[s][m].dest]++;
+      for (size_t S=0;S<NS;++S) ps->cnt[S] = scnt[s][S] + arr[S];
+      popReserveLx(ps,sn[s] + mn[s]);
+      segStarts(c,ps);
+      int64_t* fill = (int64_t*)malloc(sizeof(int64_t)*(NS > 0 ? NS : 1));
+      int64_t q = 0;
+      for (size_t S=0;S<NS;++S) {
+         memcpy(ps->p + 7*ps->start[S],sw[s] + 7*q,sizeof(double)*7*scnt[s][S]);
+         memcpy(ps->lx + ps->start[S],slx[s] + q,scnt[s][S]);
+         q += scnt[s][S];
+         fill[S] = ps->start[S] + scnt[s][S];
+      }
+      for (int64_t m=0;m<mn[s];++m) {
+         const OMover* M = &mv[s][m];
+         const int64_t d = fill[M->dest]++;
+         memcpy(ps->p + 7*d,M->st,sizeof M->st);
+         ps->lx[d] = (uint8_t)M->lx;
+      }
+      free(fill); free(arr);
+      free(sw[s]); free(slx[s]); free(scnt[s]); free(mv[s]);
    }
 }
 
@@ -754,13 +840,20 @@ static void dualGather(Ctx* c) {
    const double dV = P->dx*P->dx*P->dx;
    for (int z=0;z<c->nz;++z) for (int y=0;y<c->ny;++y) for (int x=0;x<c->nx;++x) {
       const size_t n = (size_t)x + c->nx*((size_t)y + c->ny*(size_t)z);
+      const int bnd = P->periodic[0] ? (c->nseg > 1 && x % SEG == 0) : ((x + 1) % SEG == 0);
+      const int gb = P->periodic[0] ? x / SEG : (x + 1) / SEG;
       double v[4];
       for (int qq=0;qq<4;++qq) {
          const int uy = dualU(y - (qq & 1),c->ny,P->periodic[1]);
          const int uz = dualU(z - (qq >> 1),c->nz,P->periodic[2]);
          const size_t row = (size_t)uy + (size_t)c->nd[1]*uz;
          const double* rp = c->RP + (((size_t)qq*nrows + row)*c->nx + x)*4;
-         for (int l=0;l<4;++l) v[l] = qq == 0 ? rp[l] : v[l] + rp[l];
+         const double* rb = c->RPB + (((size_t)qq*nrows + row)*c->nseg + gb)*4;
+         for (int l=0;l<4;++l) {
+            double r = rp[l];
+            if (bnd) r = r + rb[l];
+            v[l] = qq == 0 ? r : v[l] + r;
+         }
       }
       v[0] += fixedToDouble(c->MM[n],c->kR);
       for (int l=0;l<3;++l) v[1+l] += fixedToDouble(c->MM[(size_t)(1+l)*c->N + n],c->kJ);

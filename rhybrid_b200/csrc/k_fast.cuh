@@ -1,25 +1,35 @@
-// Fast path (sm_100a, FP64): fused push + CIC deposit over particles grouped
-// by CIC dual cell. Same per-particle and per-cell arithmetic as the bit-exact
-// path; the deposit sums are formed in a different (fixed) order, restated
-// bit for bit by the oracle's RHO_DEPOSIT_GPU mode (oracle/rh_oracle.c).
+// Fast path (sm_100a, FP64): fused push + CIC deposit over particles binned
+// by row segment. Same per-particle and per-cell arithmetic as the bit-exact
+// path (boris.h:64-194, particle_accumulator.cpp:65-333); the deposit sums are
+// formed in a different, fixed order, restated bit for bit by the oracle's
+// RHO_DEPOSIT_GPU mode (oracle/rh_oracle.c).
 //
-// Storage (per species): particles grouped by dual cell, the 2x2x2 block of
-// cells whose centres surround the particle (base b = c + s - 1 per axis,
-// s = 0 if x < 0.5 dx else 1, as accumulateCell's index shift,
-// particle_accumulator.cpp:78-84). Dual index u = b + 1 on a non-periodic axis,
-// b mod n on a periodic one. Dual cell D owns slots [start[D], start[D+1]);
-// the first cnt[D] hold particles.
+// Dual cells: the 2x2x2 block of cells whose centres surround a particle
+// (base b = c + s - 1 per axis, s = 0 if x < 0.5 dx else 1, the index shift of
+// accumulateCell, particle_accumulator.cpp:78-84). Dual index u = b + 1 on a
+// non-periodic axis (n + 1 dual cells), b mod n on a periodic one.
 //
-//   k_fast_push_deposit  one warp per dual row (uy, uz): push (boris.h:64-194)
-//                        + migration + CIC weights of the new position; the
-//                        contributions go to a 3-dual-cell window of running sums
-//                        held across the lanes (lane q = corner*4 + moment) and
-//                        leave as row partials; off-row movers are deposited as
-//                        exact 128-bit fixed-point sums; boundary removals
-//                        (particle_boundary_cond_hybrid.h:112-185) happen here
-//   k_fast_mig_*         placement of off-row movers, in a fixed order
-//   k_fast_gather        cell moments from the 4 row partials + fixed-point
-//                        part, then /dV and the rho clamp (particle_accumulator.cpp:319-333)
+// Storage (per species, structure of arrays): a dual row (uy, uz) is cut into
+// segments of RHGPU_FAST_SEGMENT dual cells along x; segment S = row * nseg + g
+// owns the slots [base[S], base[S+1]) (slack included), the first cnt[S] hold
+// its particles with their dual x index within the segment (lx, one byte).
+// Two buffers per species (current, next) share the layout.
+//
+//   k_fast_push_deposit  one block per segment, one thread per particle:
+//                        push + migration + CIC weights of the new position +
+//                        boundary removal (particle_boundary_cond_hybrid.h:112-185).
+//                        Particles that stay in the segment are written to the
+//                        next buffer in order; their deposit records go to
+//                        shared memory, are counting-sorted by target dual cell
+//                        (stable) and summed sequentially per (dual cell,
+//                        corner, moment) in FP64. Particles that leave the
+//                        segment go to the mover list and deposit as exact
+//                        128-bit fixed-point sums.
+//   k_fast_mig_*         placement of the movers after the stayers of their
+//                        destination segment, in (source segment, index) order
+//   k_fast_gather        cell moments from the four row partials (+ the segment
+//                        boundary partial) + the fixed-point part, then /dV and
+//                        the rho clamp (particle_accumulator.cpp:319-333)
 #pragma once
 
 #include "rh_device.cuh"
@@ -29,47 +39,52 @@
 namespace rh {
 
 constexpr int FAST_MAX_SPECIES = 8;
-constexpr int FAST_WARPS = 4;
+constexpr int SEG = RHGPU_FAST_SEGMENT;   // dual cells per segment
+constexpr int FT = 256;                   // threads of k_fast_push_deposit (one chunk of particles)
+constexpr int FW = FT / 32;
+constexpr int REC = 13;                   // doubles per deposit record: w8[8], 1.0, v[3], pad
+static_assert(SEG == 32 && SEG * FW == FT, "the deposit sort maps (dual cell, warp) to one thread");
 
-struct DStore {
-   double* a[7];
-   long long* start;   // Nd+1 slot offsets
-   int* cnt;           // particles per dual cell
-   long long cap;
+struct SegBuf {
+   double* a[7];        // x, y, z (cell-local), vx, vy, vz, weight
+   unsigned char* lx;   // dual x index within the segment
+   int* cnt;            // particles per segment
 };
-
-struct FastGeom {
-   int nd[3];
-   long long Nd;
-   long long nrows;
+struct SegSpecies {
+   SegBuf cur, nxt;
+   const long long* base;   // NS+1 slot offsets
 };
-
 struct FastSpecies {
    int ns;
-   DStore st[FAST_MAX_SPECIES];
+   SegSpecies st[FAST_MAX_SPECIES];
    SpeciesDev sp[FAST_MAX_SPECIES];
 };
+struct FastGeom {
+   int nd[3];        // dual cells per axis
+   int nseg;         // segments per dual row
+   long long nrows;  // dual rows
+   long long NS;     // segments
+};
 
-// off-row mover record: key orders the arrivals of a destination dual cell:
-// (class << 62) | (source dual index << 24) | rank in the source
+// a particle leaving its segment: key orders the arrivals of a destination
+// segment, (source segment << 32) | index in the source segment
 struct Mover {
    double s[7];
    unsigned long long key;
-   long long dest;      // destination dual index
+   long long dest;   // destination segment
    int species;
-   int pad;
+   int lx;
 };
 
 struct FastBufs {
-   double* RP;                 // 4 planes x nrows x nx x 4
+   double* RP;                 // row partials: 4 planes x nrows x nx x 4
+   double* RPB;                // segment-boundary partials: 4 planes x nrows x nseg x 4
    unsigned long long* MMlo;   // 4 x N
    unsigned long long* MMhi;   // 4 x N
    unsigned* touched;          // bit per cell: MM nonzero this step
    Mover* movers;
    unsigned long long* nmovers;
    long long moverCap;
-   double* pend;               // per row: ns x 2 x pendCap records of 8 doubles
-   int pendCap;
    double scaleR, scaleJ;      // 2^kR, 2^kJ
 };
 
@@ -150,126 +165,83 @@ __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const Species
    return clamp;
 }
 
-// per-warp state of the storage placement, one entry per species
-struct PlaceState {
-   int fill;      // particles placed in the previous dual cell of the row (u-1)
-   int full;      // the previous dual cell stopped taking in-row arrivals
-   int stay;      // stayers of the current dual cell placed so far
-   int npPrev;    // +x movers from u-1 waiting for the current dual cell
-   int npCur;     // +x movers from the current dual cell waiting for u+1
-   int pendSel;   // which of the two pending buffers is "prev"
-};
-
-__device__ inline void warpSumAtomic(double v, double* dst) {
-   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-   if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+// exclusive prefix sum over the FT threads of the block; *total = block sum
+__device__ inline int blockExclusiveScan(int v, int* s_w, int* total) {
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   int x = v;
+   for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+   }
+   if (lane == 31) s_w[warp] = x;
+   __syncthreads();
+   if (warp == 0) {
+      int t = lane < FW ? s_w[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+         const int y = __shfl_up_sync(0xffffffffu, t, o);
+         if (lane >= o) t += y;
+      }
+      if (lane < FW) s_w[lane] = t;
+   }
+   __syncthreads();
+   const int r = (warp ? s_w[warp - 1] : 0) + x - v;
+   *total = s_w[FW - 1];
+   __syncthreads();
+   return r;
 }
 
-__global__ void __launch_bounds__(32 * FAST_WARPS)
+__global__ void __launch_bounds__(FT)
 k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
-   __shared__ double s_w[FAST_WARPS][32][12];   // w8[8], v[3] of the batch's particles
-   __shared__ int s_tgt[FAST_WARPS][32];        // target dual x of the window, -1: none
-   __shared__ PlaceState s_ps[FAST_WARPS][FAST_MAX_SPECIES];
-   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   const long long row = (long long)blockIdx.x * FAST_WARPS + warp;
-   if (row >= fg.nrows) return;
-   const int ndx = fg.nd[0];
+   __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
+   __shared__ unsigned char s_rdual[FT];          // target dual x (in the segment) of each record
+   __shared__ short s_sidx[FT];                   // records sorted by target dual cell
+   __shared__ int s_off[SEG * FW + 1];            // (dual cell, warp) counts, then offsets
+   __shared__ int s_scan[FW];
+   __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
+   __shared__ int s_stay[FAST_MAX_SPECIES];
+   __shared__ int s_first[FAST_MAX_SPECIES];
+   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+   const long long S = blockIdx.x;
+   const long long row = S / fg.nseg;
+   const int gseg = (int)(S % fg.nseg);
    const int uy = (int)(row % fg.nd[1]), uz = (int)(row / fg.nd[1]);
+   const int ndx = fg.nd[0];
+   const int u0 = gseg * SEG, u1 = min(u0 + SEG, ndx);
    const int ns = FS.ns;
    const long long N = g.N;
-   const int nx = g.nx;
    const double dx = g.dx;
-   const int q = lane, qo = q >> 2, ql = q & 3;   // corner and moment of this lane's window sums
-   if (lane < ns) {
-      PlaceState z;
-      z.fill = 0; z.full = 0; z.stay = 0; z.npPrev = 0; z.npCur = 0; z.pendSel = 0;
-      s_ps[warp][lane] = z;
+   if (tid == 0) {
+      int a = 0;
+      for (int s = 0; s < ns; ++s) {
+         s_prefix[s] = a;
+         a += FS.st[s].cur.cnt[S];
+      }
+      s_prefix[ns] = a;
    }
-   __syncwarp();
-   // deposit window over dual x = wb, wb+1, wb+2
-   int wb = -1;
-   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-   double pend = 0.0, wrap0 = 0.0;
-   int nextFlush = 0;       // dual cells < nextFlush have been flushed
-   const int perx = g.per[0];
-   const long long nrows = fg.nrows;
-   double* RP = fb.RP;
+   if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
+   __syncthreads();
+   const int total = s_prefix[ns];
+   const int qo = lane >> 2, qm = 8 + (lane & 3);   // this lane's corner and moment factor in a record
+   double acc[4] = {0.0, 0.0, 0.0, 0.0};            // (dual cell warp + FW*j, corner*4 + moment lane)
 
-   // flush dual cell u: destination row partial of x = base(u)
-   auto flush = [&](int u) {
-      // window slot of u
-      const int sl = u - wb;
-      const double a = sl == 0 ? acc0 : (sl == 1 ? acc1 : acc2);
-      const double partner = __shfl_xor_sync(0xffffffffu, pend, 4);
-      const bool ox0 = ((qo & 1) == 0);
-      if (ox0) {
-         const double out = partner + a;
-         const int x = dualB(u, perx);
-         const int qq = qo >> 1;
-         if (perx && u == 0) {
-            wrap0 = a;
-         } else if (x >= 0 && x < nx) {
-            RP[(((long long)qq * nrows + row) * nx + x) * 4 + ql] = out;
-         }
-      } else {
-         pend = a;
-      }
-   };
-   auto slide = [&](int newWb) {
-      while (wb < newWb) {
-         if (wb >= 0 && wb >= nextFlush) { flush(wb); nextFlush = wb + 1; }
-         acc0 = acc1; acc1 = acc2; acc2 = 0.0;
-         ++wb;
-      }
-   };
-
-   const int ngroups = ndx * ns;
-   int G = 0, r0 = 0;
-   while (G < ngroups) {
-      // ---- form a batch from groups G .. G+31 --------------------------------
-      const int gl = G + lane;
-      int rem = 0;
-      long long gstart = 0;
-      if (gl < ngroups) {
-         const int u = gl / ns, s = gl % ns;
-         const long long D = (long long)u + (long long)ndx * row;
-         rem = FS.st[s].cnt[D] - (lane == 0 ? r0 : 0);
-         gstart = FS.st[s].start[D] + (lane == 0 ? r0 : 0);
-      }
-      int cum = rem;
-      for (int o = 1; o < 32; o <<= 1) {
-         const int t = __shfl_up_sync(0xffffffffu, cum, o);
-         if (lane >= o) cum += t;
-      }
-      const int total = __shfl_sync(0xffffffffu, cum, 31);
-      const int nb = total < 32 ? total : 32;
-      // group of this lane's particle: number of groups whose cumulative count is <= lane
-      int gidx = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-         const int cm = __shfl_sync(0xffffffffu, cum, gidx + step - 1);
-         if (cm <= lane) gidx += step;
-      }
-      if (gidx > 31) gidx = 31;
-      const int cumPrev = __shfl_sync(0xffffffffu, cum, gidx > 0 ? gidx - 1 : 0);
-      const long long gst = __shfl_sync(0xffffffffu, gstart, gidx);
-      const int within = lane - (gidx > 0 ? cumPrev : 0);
-      const int myG = G + gidx;
-      const int u = myG / ns, s = myG % ns;
-      const int rank = within + (gidx == 0 ? r0 : 0);
-      const bool active = lane < nb;
-      // ---- lane-parallel push, migration, classification ------------------------
+   for (int c0 = 0; c0 < total; c0 += FT) {
+      const int i = c0 + tid;
+      const bool active = i < total;
+      int s = 0;
+      if (active)
+         while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
       double st[7];
-      int cls = -1;         // 0 stay, 1 -x in-row, 2 +x in-row, 3 off-row, -1 removed/none
-      int tgt = -1;         // window target dual x
-      long long Dn = -1;
-      int ti = 0, tj = 0, tk = 0;
-      bool clamp = false;
+      bool stay = false, rec = false, leave = false, clamp = false;
+      int vx = 0, vy = 0, vz = 0;
+      double w8[8];
+      long long p = 0;
       if (active) {
-         const DStore& S = FS.st[s];
-         const long long p = gst + within;
-         for (int a = 0; a < 7; ++a) st[a] = S.a[a][p];
+         const SegSpecies& SS = FS.st[s];
+         p = i - s_prefix[s];
+         const long long slot = SS.base[S] + p;
+         for (int a = 0; a < 7; ++a) st[a] = SS.cur.a[a][slot];
+         const int u = u0 + SS.cur.lx[slot];
          int ci = dualB(u, g.per[0]) + 1 - halfS(st[0], dx);
          int cj = dualB(uy, g.per[1]) + 1 - halfS(st[1], dx);
          int ck = dualB(uz, g.per[2]) + 1 - halfS(st[2], dx);
@@ -280,26 +252,23 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          int bad = migrateAxis(st[0], ox, dx, g.dx_below);
          bad |= migrateAxis(st[1], oy, dx, g.dx_below);
          bad |= migrateAxis(st[2], oz, dx, g.dx_below);
-         ti = ci + ox; tj = cj + oy; tk = ck + oz;
+         int ti = ci + ox, tj = cj + oy, tk = ck + oz;
          const bool inside = wrapc(ti, g.nx, g.per[0]) && wrapc(tj, g.ny, g.per[1]) && wrapc(tk, g.nz, g.per[2]);
          const double ke = st[6] * (sq(st[3]) + sq(st[4]) + sq(st[5]));
          if (bad || !inside) {
             atomicAdd(&cntd[4 * s + 0], st[6]);
             atomicAdd(&cntd[4 * s + 1], ke);
          } else {
-            const int sx = halfS(st[0], dx), sy = halfS(st[1], dx), sz = halfS(st[2], dx);
-            const int bx = ti + sx - 1, by = tj + sy - 1, bz = tk + sz - 1;
-            const int vx = dualU(bx, g.nx, g.per[0]), vy = dualU(by, g.ny, g.per[1]), vz = dualU(bz, g.nz, g.per[2]);
-            Dn = (long long)vx + (long long)ndx * ((long long)vy + (long long)fg.nd[1] * vz);
-            const bool inRow = vy == uy && vz == uz && abs(vx - u) <= 1;
+            const int bx = ti + halfS(st[0], dx) - 1, by = tj + halfS(st[1], dx) - 1, bz = tk + halfS(st[2], dx) - 1;
+            vx = dualU(bx, g.nx, g.per[0]);
+            vy = dualU(by, g.ny, g.per[1]);
+            vz = dualU(bz, g.nz, g.per[2]);
+            const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.sp[s].accumulate) {
-               double w8[8];
                int ind[8];
                cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, dx, w8, ind);
-               if (inRow) {
-                  for (int o = 0; o < 8; ++o) s_w[warp][lane][o] = w8[o];
-                  s_w[warp][lane][8] = st[3]; s_w[warp][lane][9] = st[4]; s_w[warp][lane][10] = st[5];
-                  tgt = vx;
+               if (inSeg) {
+                  rec = true;
                } else {
                   for (int o = 0; o < 8; ++o) {
                      int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);
@@ -330,182 +299,138 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
                }
             }
             if (!removed) {
-               if (vx == u && vy == uy && vz == uz) cls = 0;
-               else if (inRow && vx == u - 1) cls = 1;
-               else if (inRow && vx == u + 1) cls = 2;
-               else cls = 3;
+               stay = inSeg;
+               leave = !inSeg;
             }
          }
       }
-      s_tgt[warp][lane] = active ? tgt : -1;
       if (clamp) atomicAdd(&cntu[CNT_SPECIES_MAXVI + s], 1ull);
-      __syncwarp();
-      // ---- transposed deposit of the batch, in particle order --------------------
-      for (int jj = 0; jj < nb; ++jj) {
-         const int tv = s_tgt[warp][jj];
-         if (tv < 0) continue;
-         const int uj = __shfl_sync(0xffffffffu, u, jj);
-         if (uj - 1 > wb) slide(uj - 1);
-         const double w = s_w[warp][jj][qo];
-         const double val = ql == 0 ? w : w * s_w[warp][jj][8 + ql - 1];
-         const int sl = tv - wb;
-         if (sl == 0) acc0 += val;
-         else if (sl == 1) acc1 += val;
-         else acc2 += val;
+
+      // ---- order of the chunk's stayers and records ------------------------------------
+      int tot;
+      const int ex = blockExclusiveScan((stay ? 1 : 0) | (rec ? 1 << 16 : 0), s_scan, &tot);
+      const int stayIdx = ex & 0xffff, recIdx = ex >> 16, nrec = tot >> 16;
+      if (active && i == max(s_prefix[s], c0)) s_first[s] = stayIdx;
+      __syncthreads();
+      if (stay) {
+         const SegSpecies& SS = FS.st[s];
+         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - s_first[s]);
+         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
+         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
       }
-      // ---- advance the group cursor ------------------------------------------------------
-      // groups G .. gEnd-1 are finished by this batch; group G+lastIdx may continue
-      int gEnd, lastIdx, r0n;
+      if (rec) {
+         double* r = s_rec + recIdx * REC;
+         for (int o = 0; o < 8; ++o) r[o] = w8[o];
+         r[8] = 1.0;
+         r[9] = st[3]; r[10] = st[4]; r[11] = st[5];
+         s_rdual[recIdx] = (unsigned char)(vx - u0);
+      }
       {
-         lastIdx = __shfl_sync(0xffffffffu, gidx, nb > 0 ? nb - 1 : 0);
-         const int lastCum = __shfl_sync(0xffffffffu, cum, lastIdx);
-         // groups after lastIdx (within the 32 read) with nothing left are finished too
-         const unsigned emptyAfter = __ballot_sync(0xffffffffu, lane > lastIdx && G + lane < ngroups && cum == nb);
-         if (nb == 0) {
-            gEnd = min(G + 32, ngroups);
-            r0n = 0;
-         } else if (nb == lastCum) {
-            int e = lastIdx + 1;
-            while (e < 32 && ((emptyAfter >> e) & 1u)) ++e;
-            gEnd = G + e;
-            r0n = 0;
-         } else {
-            gEnd = G + lastIdx;
-            const int lastPrevCum = lastIdx > 0 ? __shfl_sync(0xffffffffu, cum, lastIdx - 1) : 0;
-            r0n = (lastIdx == 0 ? r0 : 0) + (nb - lastPrevCum);
-         }
-      }
-      // ---- storage, one group at a time in group order: stayers in place, in-row
-      //      movers after the neighbour's stayers, off-row movers to the global list;
-      //      then the exit of every finished group --------------------------------------
-      const int gLoopEnd = max(gEnd, G + (nb > 0 ? lastIdx + 1 : 0));
-      const unsigned below = (1u << lane) - 1u;
-      for (int gg = G; gg < gLoopEnd; ++gg) {
-         const int ug = gg / ns, sg = gg % ns;
-         PlaceState& P = s_ps[warp][sg];
-         const DStore& S = FS.st[sg];
-         const long long Du = (long long)ug + (long long)ndx * row;
-         const bool mine = active && myG == gg;
-         const unsigned mStay = __ballot_sync(0xffffffffu, mine && cls == 0);
-         const unsigned mMinus = __ballot_sync(0xffffffffu, mine && cls == 1);
-         const unsigned mPlus = __ballot_sync(0xffffffffu, mine && cls == 2);
-         if (mine && cls >= 0) {
-            bool toSlow = cls == 3;
-            int slowClass = 2;
-            if (cls == 0) {
-               const long long pos = S.start[Du] + P.stay + __popc(mStay & below);
-               for (int a = 0; a < 7; ++a) S.a[a][pos] = st[a];
-            } else if (cls == 1) {
-               const int k = P.fill + __popc(mMinus & below);
-               const long long pos = S.start[Du - 1] + k;
-               if (!P.full && pos < S.start[Du]) {
-                  for (int a = 0; a < 7; ++a) S.a[a][pos] = st[a];
-               } else {
-                  toSlow = true;
-                  slowClass = 1;
-               }
-            } else if (cls == 2) {
-               const int k = P.npCur + __popc(mPlus & below);
-               if (k < fb.pendCap) {
-                  double* pb = fb.pend + (((row * ns + sg) * 2 + (P.pendSel ^ 1)) * (long long)fb.pendCap + k) * 8;
-                  for (int a = 0; a < 7; ++a) pb[a] = st[a];
-                  pb[7] = (double)rank;
-               } else {
-                  raiseError(err, RHGPU_DEVERR_CAPACITY);
-               }
-            }
-            if (toSlow) {
-               const unsigned long long m = atomicAdd(fb.nmovers, 1ull);
+         const unsigned lm = __ballot_sync(0xffffffffu, leave);
+         if (lm) {
+            const int leader = __ffs(lm) - 1;
+            unsigned long long b0 = 0;
+            if (lane == leader) b0 = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            if (leave) {
+               const unsigned long long m = b0 + __popc(lm & ((1u << lane) - 1u));
                if ((long long)m < fb.moverCap) {
                   Mover& M = fb.movers[m];
                   for (int a = 0; a < 7; ++a) M.s[a] = st[a];
-                  M.key = ((unsigned long long)slowClass << 62) | ((unsigned long long)Du << 24) | (unsigned long long)rank;
-                  M.dest = Dn;
-                  M.species = sg;
+                  M.key = ((unsigned long long)S << 32) | (unsigned long long)p;
+                  const int gd = vx / SEG;
+                  M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * fg.nseg + gd;
+                  M.species = s;
+                  M.lx = vx - gd * SEG;
                } else {
                   raiseError(err, RHGPU_DEVERR_CAPACITY);
                }
             }
          }
-         __syncwarp();
-         if (lane == 0) {
-            P.stay += __popc(mStay);
-            const int nm = __popc(mMinus);
-            if (nm) {
-               // once the previous dual cell is full, its -x arrivals keep going to the slow path
-               const int cap = (int)(S.start[Du] - S.start[Du - 1]);
-               if (P.full || P.fill + nm > cap) { P.fill = min(P.fill + nm, cap); P.full = 1; }
-               else P.fill += nm;
-            }
-            P.npCur += __popc(mPlus);
-         }
-         __syncwarp();
-         if (gg >= gEnd) continue;   // the last group continues in the next batch
-         // exit of group (ug, sg): the previous dual cell of this species is final
-         if (ug >= 1 && lane == 0) S.cnt[Du - 1] = P.fill;
-         // +x movers from ug-1 go after the stayers of ug
-         const int np = P.npPrev;
-         const long long base = S.start[Du] + P.stay;
-         const long long capEnd = S.start[Du + 1];
-         double* pb = fb.pend + (((row * ns + sg) * 2 + P.pendSel) * (long long)fb.pendCap) * 8;
-         const int fit = (int)max(0LL, min((long long)np, capEnd - base));
-         for (int k = lane; k < np; k += 32) {
-            const double* rec = pb + (long long)k * 8;
-            if (k < fit) {
-               for (int a = 0; a < 7; ++a) S.a[a][base + k] = rec[a];
-            } else {
-               const unsigned long long m = atomicAdd(fb.nmovers, 1ull);
-               if ((long long)m < fb.moverCap) {
-                  Mover& M = fb.movers[m];
-                  for (int a = 0; a < 7; ++a) M.s[a] = rec[a];
-                  const long long Dsrc = Du - 1;
-                  M.key = (1ull << 62) | ((unsigned long long)Dsrc << 24) | (unsigned long long)rec[7];
-                  M.dest = Du;
-                  M.species = sg;
-               } else {
-                  raiseError(err, RHGPU_DEVERR_CAPACITY);
-               }
-            }
-         }
-         __syncwarp();
-         if (lane == 0) {
-            P.fill = P.stay + fit;
-            P.full = fit < np ? 1 : 0;
-            P.stay = 0;
-            P.npPrev = P.npCur;
-            P.npCur = 0;
-            P.pendSel ^= 1;
-         }
-         __syncwarp();
       }
-      G = gEnd;
-      r0 = r0n;
+      __syncthreads();
+      // running stayer count of each species: the chunk's last thread of the species adds
+      if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - s_first[s];
+
+      // ---- records sorted by target dual cell (stable), then summed in that order -------
+      s_off[tid] = 0;
+      __syncthreads();
+      const bool hasRec = tid < nrec;
+      const int rd = hasRec ? s_rdual[tid] : 0;
+      const unsigned am = __ballot_sync(0xffffffffu, hasRec);
+      int rrank = 0;
+      if (hasRec) {
+         const unsigned mm = __match_any_sync(am, rd);
+         rrank = __popc(mm & ((1u << lane) - 1u));
+         if (rrank == 0) s_off[rd * FW + warp] = __popc(mm);
+      }
+      __syncthreads();
+      int dummy;
+      const int off = blockExclusiveScan(s_off[tid], s_scan, &dummy);
+      s_off[tid] = off;
+      if (tid == 0) s_off[SEG * FW] = nrec;
+      __syncthreads();
+      if (hasRec) s_sidx[s_off[rd * FW + warp] + rrank] = (short)tid;
+      __syncthreads();
+      for (int j = 0; j < 4; ++j) {
+         const int d = warp + FW * j;
+         const int r1 = s_off[(d + 1) * FW];
+         for (int r = s_off[d * FW]; r < r1; ++r) {
+            const double* rr = s_rec + s_sidx[r] * REC;
+            acc[j] += rr[qo] * rr[qm];
+         }
+      }
+      __syncthreads();
    }
-   // ---- end of row: finalize the last dual cell of every species, flush the window -----
-   if (lane < ns) {
-      const PlaceState& P = s_ps[warp][lane];
-      const long long Dl = (long long)(ndx - 1) + (long long)ndx * row;
-      FS.st[lane].cnt[Dl] = P.fill;
+
+   // ---- outputs: stayer counts, row partials, segment-boundary partial ---------------------
+   if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
+   for (int j = 0; j < 4; ++j) s_rec[(warp + FW * j) * 32 + lane] = acc[j];
+   __syncthreads();
+   const int nx = g.nx;
+   const long long nrows = fg.nrows;
+   for (int e = tid; e < SEG * 16; e += FT) {
+      const int dl = e >> 4, qq = (e >> 2) & 3, m = e & 3;
+      const int lo = u0 + dl;   // the dual cell giving corner ox = 1 to cell x
+      if (lo >= u1) continue;
+      int x, hi;
+      if (g.per[0]) {
+         x = lo + 1 == nx ? 0 : lo + 1;
+         hi = lo + 1 < u1 ? dl + 1 : (fg.nseg == 1 ? 0 : -1);
+      } else {
+         x = lo;
+         if (x >= nx) continue;
+         hi = lo + 1 < u1 ? dl + 1 : -1;
+      }
+      double v = s_rec[dl * 32 + ((1 + 2 * qq) << 2) + m];
+      if (hi >= 0) v = v + s_rec[hi * 32 + ((2 * qq) << 2) + m];
+      fb.RP[(((long long)qq * nrows + row) * nx + x) * 4 + m] = v;
    }
-   slide(ndx);
-   if (perx) {
-      // destination 0: corner 1 of the last dual cell + corner 0 of dual cell 0
-      const double partner = __shfl_xor_sync(0xffffffffu, pend, 4);
-      if ((qo & 1) == 0) RP[(((long long)(qo >> 1) * nrows + row) * nx + 0) * 4 + ql] = partner + wrap0;
+   // corner ox = 0 of the first dual cell, when the cell's other dual cell is in another segment
+   if (tid < 16 && (g.per[0] ? fg.nseg > 1 : gseg >= 1)) {
+      const int qq = tid >> 2, m = tid & 3;
+      fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = s_rec[((2 * qq) << 2) + m];
    }
 }
 
-// destination moments: four row partials + fixed-point part, then finalize
+// destination moments: four row partials (+ boundary partials) + fixed-point part, then finalize
 __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, double hiR, double loR, double hiJ,
                               double loJ, double minRho, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
+   const bool bnd = g.per[0] ? (fg.nseg > 1 && i % SEG == 0) : ((i + 1) % SEG == 0);
+   const int gb = g.per[0] ? i / SEG : (i + 1) / SEG;
    double v[4];
    for (int qq = 0; qq < 4; ++qq) {
       const int uyy = dualU(j - (qq & 1), g.ny, g.per[1]);
       const int uzz = dualU(k - (qq >> 1), g.nz, g.per[2]);
       const long long row = (long long)uyy + (long long)fg.nd[1] * uzz;
       const double* rp = fb.RP + (((long long)qq * fg.nrows + row) * g.nx + i) * 4;
-      for (int l = 0; l < 4; ++l) v[l] = qq == 0 ? rp[l] : v[l] + rp[l];
+      const double* rb = fb.RPB + (((long long)qq * fg.nrows + row) * fg.nseg + gb) * 4;
+      for (int l = 0; l < 4; ++l) {
+         double r = rp[l];
+         if (bnd) r = r + rb[l];
+         v[l] = qq == 0 ? r : v[l] + r;
+      }
    }
    if (fb.touched[n >> 5] & (1u << (n & 31))) {
       v[0] += fixedToDouble(fb.MMlo[n], fb.MMhi[n], hiR, loR);
@@ -520,46 +445,48 @@ __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, do
    for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = v[1 + l] / g.dV;
 }
 
-// ---- off-row mover placement ------------------------------------------------------
-__global__ void k_fast_mig_count(const Mover* mv, long long n, long long Nd, int* inc) {
+// ---- mover placement ------------------------------------------------------------------------
+__global__ void k_fast_mig_count(const Mover* mv, long long n, long long NS, int* inc) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= n) return;
-   atomicAdd(&inc[(long long)mv[t].species * Nd + mv[t].dest], 1);
+   atomicAdd(&inc[(long long)mv[t].species * NS + mv[t].dest], 1);
 }
-__global__ void k_fast_mig_bucket(const Mover* mv, long long n, long long Nd, const long long* off, int* fill, int* bucket) {
+__global__ void k_fast_mig_bucket(const Mover* mv, long long n, long long NS, const long long* off, int* fill, int* bucket) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= n) return;
-   const long long b = (long long)mv[t].species * Nd + mv[t].dest;
+   const long long b = (long long)mv[t].species * NS + mv[t].dest;
    const int k = atomicAdd(&fill[b], 1);
    bucket[off[b] + k] = (int)t;
 }
-// per destination (species, dual cell): arrivals sorted by key, appended after
-// the in-row placements; sets *overflow and places nothing if they do not fit
-__global__ void k_fast_mig_place(FastSpecies FS, long long Nd, const Mover* mv, int* inc, const long long* off,
+// per destination (species, segment): arrivals sorted by key, appended after the
+// stayers; sets *overflow and places nothing if they do not fit
+__global__ void k_fast_mig_place(FastSpecies FS, long long NS, const Mover* mv, int* inc, const long long* off,
                                  int* bucket, int* overflow) {
    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (b >= (long long)FS.ns * Nd) return;
+   if (b >= (long long)FS.ns * NS) return;
    const int k = inc[b];
    if (k == 0) return;
-   const int s = (int)(b / Nd);
-   const long long D = b % Nd;
+   const int s = (int)(b / NS);
+   const long long S = b % NS;
    int* bk = bucket + off[b];
    for (int a = 1; a < k; ++a)
-      for (int c = a; c > 0 && mv[bk[c - 1]].key > mv[bk[c]].key; --c) { int t = bk[c]; bk[c] = bk[c - 1]; bk[c - 1] = t; }
-   const DStore& S = FS.st[s];
-   const long long base = S.start[D] + S.cnt[D];
-   if (base + k > S.start[D + 1]) { atomicOr((unsigned*)overflow, 1u); return; }
+      for (int c = a; c > 0 && mv[bk[c - 1]].key > mv[bk[c]].key; --c) { const int t = bk[c]; bk[c] = bk[c - 1]; bk[c - 1] = t; }
+   const SegSpecies& SS = FS.st[s];
+   const long long pos = SS.base[S] + SS.nxt.cnt[S];
+   if (pos + k > SS.base[S + 1]) { atomicOr((unsigned*)overflow, 1u); return; }
    for (int a = 0; a < k; ++a) {
       const Mover& M = mv[bk[a]];
-      for (int e = 0; e < 7; ++e) S.a[e][base + a] = M.s[e];
+      for (int e = 0; e < 7; ++e) SS.nxt.a[e][pos + a] = M.s[e];
+      SS.nxt.lx[pos + a] = (unsigned char)M.lx;
    }
-   S.cnt[D] += k;
+   SS.nxt.cnt[S] += k;
    inc[b] = 0;
 }
 
-// ---- upload / download / repack support ------------------------------------------------
-// dual index of each uploaded particle (records grouped by cell)
-__global__ void k_fast_dual_of(GridInfo g, FastGeom fg, const double* aos, const int* pcell, long long n, unsigned* key) {
+// ---- upload / download / relayout support -----------------------------------------------------
+// segment and dual x (in the segment) of each uploaded particle (records grouped by cell)
+__global__ void k_fast_seg_of(GridInfo g, FastGeom fg, const double* aos, const int* pcell, long long n,
+                              unsigned* key, unsigned char* lx) {
    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (p >= n) return;
    const int c = pcell[p];
@@ -568,73 +495,80 @@ __global__ void k_fast_dual_of(GridInfo g, FastGeom fg, const double* aos, const
    const int ux = dualU(i + halfS(st[0], g.dx) - 1, g.nx, g.per[0]);
    const int uy = dualU(j + halfS(st[1], g.dx) - 1, g.ny, g.per[1]);
    const int uz = dualU(k + halfS(st[2], g.dx) - 1, g.nz, g.per[2]);
-   key[p] = (unsigned)((long long)ux + (long long)fg.nd[0] * ((long long)uy + (long long)fg.nd[1] * uz));
+   const int gs = ux / SEG;
+   key[p] = (unsigned)(((long long)uy + (long long)fg.nd[1] * uz) * fg.nseg + gs);
+   lx[p] = (unsigned char)(ux - gs * SEG);
 }
 __global__ void k_fast_histogram(const unsigned* key, long long n, int* cnt) {
    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (p < n) atomicAdd(&cnt[key[p]], 1);
 }
-// capacity with slack: cnt + max(8, cnt/2)
-__global__ void k_fast_capacity(long long Nd, const int* cnt, const int* extra, long long* cap) {
+// segment capacity with slack: c + max(32, c/4); entry NS is 0 (for the scan's total)
+__global__ void k_fast_capacity(long long NS, const int* cnt, const int* extra, long long* cap) {
    const long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (d < Nd) {
+   if (d < NS) {
       const long long c = (long long)cnt[d] + (extra ? extra[d] : 0);
-      cap[d] = c + max(8LL, c / 2);
-   }
-   if (d == Nd) cap[Nd] = 0;
-}
-// sorted particle i (dual key[i], original index idx[i]) -> slot start[D] + (i - first[D])
-__global__ void k_fast_scatter_sorted(const double* aos, const unsigned* key, const unsigned* idx, long long n,
-                                      const long long* first, DStore S) {
-   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (i >= n) return;
-   const unsigned D = key[i];
-   const long long pos = S.start[D] + (i - first[D]);
-   const double* st = aos + 7 * (long long)idx[i];
-   for (int a = 0; a < 7; ++a) S.a[a][pos] = st[a];
-}
-// cell index and storage sequence of every stored particle (download)
-__global__ void k_fast_cell_keys(GridInfo g, FastGeom fg, DStore S, const long long* seqStart, unsigned* key,
-                                 unsigned long long* slot) {
-   const long long D = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (D >= fg.Nd) return;
-   const int ux = (int)(D % fg.nd[0]), uy = (int)((D / fg.nd[0]) % fg.nd[1]), uz = (int)(D / ((long long)fg.nd[0] * fg.nd[1]));
-   const long long s0 = S.start[D], o = seqStart[D];
-   for (int t = 0; t < S.cnt[D]; ++t) {
-      const long long p = s0 + t;
-      int i = dualB(ux, g.per[0]) + 1 - halfS(S.a[0][p], g.dx);
-      int j = dualB(uy, g.per[1]) + 1 - halfS(S.a[1][p], g.dx);
-      int k = dualB(uz, g.per[2]) + 1 - halfS(S.a[2][p], g.dx);
-      wrapc(i, g.nx, 1); wrapc(j, g.ny, 1); wrapc(k, g.nz, 1);
-      key[o + t] = (unsigned)cidx(g, i, j, k);
-      slot[o + t] = (unsigned long long)p;
+      cap[d] = c + max(32LL, c / 4);
+   } else if (d == NS) {
+      cap[d] = 0;
    }
 }
-__global__ void k_fast_gather_records(DStore S, const unsigned long long* slot, const unsigned* order, long long n, double* aos) {
-   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= n) return;
-   const long long p = (long long)slot[order[t]];
-   for (int a = 0; a < 7; ++a) aos[7 * t + a] = S.a[a][p];
+// sorted upload records -> segment slots
+__global__ void k_fast_scatter_sorted(const double* aos, const unsigned char* lxIn, const unsigned* key,
+                                      const unsigned* idx, long long n, const long long* first, SegBuf B,
+                                      const long long* base) {
+   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (j >= n) return;
+   const unsigned S = key[j];
+   const long long slot = base[S] + (j - first[S]);
+   const unsigned src = idx[j];
+   for (int a = 0; a < 7; ++a) B.a[a][slot] = aos[7LL * src + a];
+   B.lx[slot] = lxIn[src];
 }
-__global__ void k_fast_repack_copy(long long Nd, DStore from, DStore to) {
-   const long long D = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (D >= Nd) return;
-   const long long a = from.start[D], b = to.start[D];
-   const int c = from.cnt[D];
-   for (int t = 0; t < c; ++t)
-      for (int e = 0; e < 7; ++e) to.a[e][b + t] = from.a[e][a + t];
-   to.cnt[D] = c;
+// one block per segment: cell key and slot of every particle, in storage order
+__global__ void k_fast_cell_keys(GridInfo g, FastGeom fg, SegBuf B, const long long* base, const long long* first,
+                                 unsigned* key, unsigned long long* slots) {
+   const long long S = blockIdx.x;
+   const long long row = S / fg.nseg;
+   const int gs = (int)(S % fg.nseg);
+   const int uy = (int)(row % fg.nd[1]), uz = (int)(row / fg.nd[1]);
+   const int c = B.cnt[S];
+   for (int r = threadIdx.x; r < c; r += blockDim.x) {
+      const long long slot = base[S] + r;
+      const int u = gs * SEG + B.lx[slot];
+      int ci = dualB(u, g.per[0]) + 1 - halfS(B.a[0][slot], g.dx);
+      int cj = dualB(uy, g.per[1]) + 1 - halfS(B.a[1][slot], g.dx);
+      int ck = dualB(uz, g.per[2]) + 1 - halfS(B.a[2][slot], g.dx);
+      wrapc(ci, g.nx, 1); wrapc(cj, g.ny, 1); wrapc(ck, g.nz, 1);
+      key[first[S] + r] = (unsigned)cidx(g, ci, cj, ck);
+      slots[first[S] + r] = (unsigned long long)slot;
+   }
 }
-__global__ void k_fast_max_abs_w(DStore S, long long Nd, unsigned long long* out) {
-   const long long D = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (D >= Nd) return;
+__global__ void k_fast_gather_records(SegBuf B, const unsigned long long* slots, const unsigned* idx, long long n,
+                                      double* aos) {
+   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (j >= n) return;
+   const unsigned long long slot = slots[idx[j]];
+   for (int a = 0; a < 7; ++a) aos[7 * j + a] = B.a[a][slot];
+}
+// one block per segment: copy the particles of a segment to another layout
+__global__ void k_fast_relayout(SegBuf from, const long long* fromBase, SegBuf to, const long long* toBase) {
+   const long long S = blockIdx.x;
+   const int c = from.cnt[S];
+   const long long a0 = fromBase[S], b0 = toBase[S];
+   for (int r = threadIdx.x; r < c; r += blockDim.x) {
+      for (int e = 0; e < 7; ++e) to.a[e][b0 + r] = from.a[e][a0 + r];
+      to.lx[b0 + r] = from.lx[a0 + r];
+   }
+   if (threadIdx.x == 0) to.cnt[S] = c;
+}
+// one block per segment: largest |weight|
+__global__ void k_fast_max_abs_w(SegBuf B, const long long* base, unsigned long long* out) {
+   const long long S = blockIdx.x;
+   const int c = B.cnt[S];
    double m = 0.0;
-   for (int t = 0; t < S.cnt[D]; ++t) m = fmax(m, fabs(S.a[6][S.start[D] + t]));
-   atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
-__global__ void k_fast_max_int(const long long* start, long long Nd, int* out) {
-   const long long D = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (D < Nd) atomicMax(out, (int)(start[D + 1] - start[D]));
+   for (int r = threadIdx.x; r < c; r += blockDim.x) m = fmax(m, fabs(B.a[6][base[S] + r]));
+   if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
 }  // namespace rh

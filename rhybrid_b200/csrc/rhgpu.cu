@@ -105,6 +105,17 @@ NeumannTables buildNeumannTables() {
 
 struct TimerRec { int cls; int ea, eb; };
 
+// one species' row-segment storage: two particle buffers sharing the layout `base`
+struct SegHost {
+   double* a[2][7] = {};
+   unsigned char* lx[2] = {};
+   int* cnt[2] = {};
+   long long capOf[2] = {0, 0};   // slots allocated in each buffer
+   long long* base = nullptr;      // NS+1 slot offsets
+   long long* baseAlt = nullptr;   // NS+1, relayout target
+   int cur = 0;                    // buffer holding the current particles
+};
+
 }  // namespace
 
 struct rhgpu_ctx {
@@ -150,29 +161,31 @@ struct rhgpu_ctx {
    long long launchesStep = 0;
    void* staging = nullptr;      // particle record staging for upload/download
    size_t stagingBytes = 0;
-   // fast path (dual-cell storage)
+   // fast path (row-segment storage)
    int path = RHGPU_PATH_FAST;
    bool uploaded = false;
    FastGeom fg;
-   DStore ds[MAX_SPECIES] = {};
-   DStore dalt[MAX_SPECIES] = {};
+   SegHost seg[MAX_SPECIES];
    FastBufs fb = {};
-   int* finc = nullptr;          // off-row arrivals per (species, dual cell)
+   int* finc = nullptr;                 // arrivals per (species, segment)
    int* ffill = nullptr;
-   long long* foff = nullptr;
    int* fbucket = nullptr;
-   int* fover = nullptr;
+   int* fover = nullptr;                // 8 bytes
    int kR = 0, kJ = 0;
    void* sortTmp = nullptr;
    size_t sortTmpBytes = 0;
-   long long* ftmp64 = nullptr;         // Nd+1
+   long long* fcap = nullptr;           // NS+1
+   long long* ffirst = nullptr;         // NS+1
+   long long* ftmp64 = nullptr;         // NS+1
    long long* ftmpCellStart = nullptr;  // N+1
-   long long* ftmpInc64 = nullptr;      // ns*Nd+1
-   long long* foffInc = nullptr;        // ns*Nd+1
+   long long* ftmpInc64 = nullptr;      // ns*NS+1
+   long long* foffInc = nullptr;        // ns*NS+1
    unsigned* fsort = nullptr;
    long long fsortCap = 0;
    unsigned long long* fsortSlots = nullptr;
    long long fsortSlotsCap = 0;
+   unsigned char* flxTmp = nullptr;
+   long long flxTmpCap = 0;
    long long capHint[MAX_SPECIES] = {};
 };
 
@@ -467,57 +480,61 @@ int ensureSortTmp(rhgpu_ctx* c, size_t bytes) {
    return RHGPU_OK;
 }
 
-// particle arrays of a dual-cell store with room for `slots` slots
-int fastReserve(DStore& d, long long slots) {
-   if (slots <= d.cap && d.a[0]) return RHGPU_OK;
-   for (int a = 0; a < 7; ++a) { cudaFree(d.a[a]); d.a[a] = nullptr; }
+SegBuf segView(const SegHost& h, int which) {
+   SegBuf b;
+   for (int a = 0; a < 7; ++a) b.a[a] = h.a[which][a];
+   b.lx = h.lx[which];
+   b.cnt = h.cnt[which];
+   return b;
+}
+
+// particle arrays of buffer `which` with room for `slots` slots
+int segReserve(SegHost& h, int which, long long slots) {
+   if (slots <= h.capOf[which] && h.a[which][0]) return RHGPU_OK;
+   for (int a = 0; a < 7; ++a) { cudaFree(h.a[which][a]); h.a[which][a] = nullptr; }
+   cudaFree(h.lx[which]);
+   h.lx[which] = nullptr;
+   h.capOf[which] = 0;
    const long long n = slots + slots / 16 + 1024;
-   for (int a = 0; a < 7; ++a) RH_CUDA(cudaMalloc(&d.a[a], sizeof(double) * n));
-   d.cap = n;
+   for (int a = 0; a < 7; ++a) RH_CUDA(cudaMalloc(&h.a[which][a], sizeof(double) * n));
+   RH_CUDA(cudaMalloc(&h.lx[which], n));
+   h.capOf[which] = n;
    return RHGPU_OK;
 }
 
-// slot layout with slack from per-dual counts (+ extra arrivals): d.start, returns total slots
-int fastLayout(rhgpu_ctx* c, const int* cnt, const int* extra, DStore& d, long long* total) {
-   const long long Nd = c->fg.Nd;
-   k_fast_capacity<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(Nd, cnt, extra, c->foff);
+// segment layout with slack from per-segment counts (+ pending arrivals): base, total slots
+int fastLayout(rhgpu_ctx* c, const int* cnt, const int* extra, long long* base, long long* total) {
+   const long long NS = c->fg.NS;
+   k_fast_capacity<<<blocks1d(NS + 1, 256), 256, 0, c->stream>>>(NS, cnt, extra, c->fcap);
    RH_CUDA(cudaGetLastError());
    size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->foff, d.start, Nd + 1, c->stream));
-   RH_CUDA(cudaMemcpyAsync(total, d.start + Nd, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->fcap, base, NS + 1, c->stream));
+   RH_CUDA(cudaMemcpyAsync(total, base + NS, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
    return RHGPU_OK;
 }
 
-// pending-mover buffers of k_fast_push_deposit: one slot per particle slot of the largest dual cell
-int fastPendingBuffers(rhgpu_ctx* c) {
-   int mx = 1;
+FastSpecies fastSpecies(rhgpu_ctx* c) {
+   FastSpecies F;
+   std::memset(&F, 0, sizeof F);
+   F.ns = c->ns;
    for (int s = 0; s < c->ns; ++s) {
-      RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-      k_fast_max_int<<<blocks1d(c->fg.Nd, 256), 256, 0, c->stream>>>(c->ds[s].start, c->fg.Nd, c->fover);
-      RH_CUDA(cudaGetLastError());
-      int m = 0;
-      RH_CUDA(cudaMemcpyAsync(&m, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-      RH_CUDA(cudaStreamSynchronize(c->stream));
-      mx = std::max(mx, m);
+      const SegHost& h = c->seg[s];
+      F.st[s].cur = segView(h, h.cur);
+      F.st[s].nxt = segView(h, h.cur ^ 1);
+      F.st[s].base = h.base;
+      F.sp[s] = speciesDev(c, s);
    }
-   if (mx > c->fb.pendCap) {
-      cudaFree(c->fb.pend);
-      c->fb.pend = nullptr;
-      const long long n = c->fg.nrows * c->ns * 2LL * mx * 8LL;
-      RH_CUDA(cudaMalloc(&c->fb.pend, sizeof(double) * n));
-      c->fb.pendCap = mx;
-   }
-   return RHGPU_OK;
+   return F;
 }
 
-// fixed-point exponents of the off-row deposit from the largest |w q| (oracle: fixedPointExponents)
+// fixed-point exponents of the out-of-segment deposit from the largest |w q| (oracle: fixedPointExponents)
 int fastExponents(rhgpu_ctx* c) {
    double bR = 0.0;
    for (int s = 0; s < c->ns; ++s) {
       unsigned long long* mw = (unsigned long long*)c->fover;
       RH_CUDA(cudaMemsetAsync(mw, 0, sizeof(unsigned long long), c->stream));
-      k_fast_max_abs_w<<<blocks1d(c->fg.Nd, 256), 256, 0, c->stream>>>(c->ds[s], c->fg.Nd, mw);
+      k_fast_max_abs_w<<<(unsigned)c->fg.NS, 128, 0, c->stream>>>(segView(c->seg[s], c->seg[s].cur), c->seg[s].base, mw);
       RH_CUDA(cudaGetLastError());
       unsigned long long bits = 0;
       RH_CUDA(cudaMemcpyAsync(&bits, mw, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
@@ -538,10 +555,11 @@ int fastExponents(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+// mover list: a quarter of all slots (at least 2^20)
 int fastMoverBuffers(rhgpu_ctx* c) {
    long long tot = 0;
-   for (int s = 0; s < c->ns; ++s) tot += c->ds[s].cap;
-   const long long want = std::max(1LL << 20, tot / 8);
+   for (int s = 0; s < c->ns; ++s) tot += c->seg[s].capOf[c->seg[s].cur];
+   const long long want = std::max(1LL << 20, tot / 4);
    if (want > c->fb.moverCap) {
       cudaFree(c->fb.movers);
       cudaFree(c->fbucket);
@@ -555,17 +573,6 @@ int fastMoverBuffers(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
-FastSpecies fastSpecies(rhgpu_ctx* c) {
-   FastSpecies F;
-   std::memset(&F, 0, sizeof F);
-   F.ns = c->ns;
-   for (int s = 0; s < c->ns; ++s) {
-      F.st[s] = c->ds[s];
-      F.sp[s] = speciesDev(c, s);
-   }
-   return F;
-}
-
 __global__ void k_iota(unsigned* v, long long n) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t < n) v[t] = (unsigned)t;
@@ -576,29 +583,42 @@ __global__ void k_int_to64(const int* in, long long n, long long* out) {
    if (t == n) out[n] = 0;
 }
 
-// relayout all species with room for their pending off-row arrivals (finc), order kept
-int fastRepack(rhgpu_ctx* c, bool withArrivals) {
-   const long long Nd = c->fg.Nd;
+// exclusive prefix of a per-segment count array (NS+1 entries into c->ffirst); returns the total
+int segPrefix(rhgpu_ctx* c, const int* cnt, long long* total) {
+   const long long NS = c->fg.NS;
+   k_int_to64<<<blocks1d(NS + 1, 256), 256, 0, c->stream>>>(cnt, NS, c->ftmp64);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->ffirst, NS + 1, c->stream));
+   RH_CUDA(cudaMemcpyAsync(total, c->ffirst + NS, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+
+// relayout of every species' next buffer with room for its pending arrivals (finc), order kept
+int fastRelayoutNext(rhgpu_ctx* c) {
+   const long long NS = c->fg.NS;
    for (int s = 0; s < c->ns; ++s) {
-      DStore& from = c->ds[s];
-      DStore& to = c->dalt[s];
+      SegHost& h = c->seg[s];
+      const int nx = h.cur ^ 1;   // holds the step's particles; h.cur is free
       long long total = 0;
-      int rc = fastLayout(c, from.cnt, withArrivals ? c->finc + (long long)s * Nd : nullptr, to, &total);
+      int rc = fastLayout(c, h.cnt[nx], c->finc + (long long)s * NS, h.baseAlt, &total);
       if (rc) return rc;
-      rc = fastReserve(to, total);
+      rc = segReserve(h, h.cur, total);
       if (rc) return rc;
-      k_fast_repack_copy<<<blocks1d(Nd, 128), 128, 0, c->stream>>>(Nd, from, to);
+      k_fast_relayout<<<(unsigned)NS, 128, 0, c->stream>>>(segView(h, nx), h.base, segView(h, h.cur), h.baseAlt);
       RH_CUDA(cudaGetLastError());
-      std::swap(c->ds[s], c->dalt[s]);
+      std::swap(h.base, h.baseAlt);
+      h.cur ^= 1;   // the relaid buffer takes the "next" role
+      rc = segReserve(h, h.cur, total);
+      if (rc) return rc;
    }
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   int rc = fastPendingBuffers(c);
-   if (rc) return rc;
    return fastMoverBuffers(c);
 }
 
 int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n) {
-   const long long N = c->g.N, Nd = c->fg.Nd;
+   const long long N = c->g.N, NS = c->fg.NS;
    int rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
    if (rc) return rc;
    rc = ensureKeyCapacity(c, 2 * n + 2);
@@ -620,15 +640,17 @@ int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* partic
    if (total != n) return fail(RHGPU_ERR_ARG, "upload_particles: sum(counts) != n_particles");
    k_fill_pcell<<<blocks1d(N, 128), 128, 0, c->stream>>>(N, cstart, pcell);
    RH_CUDA(cudaGetLastError());
-   // dual index of every record, stable sort by it
+   // segment of every record, stable sort by it
    rc = growBuffer(c->fsort, c->fsortCap, 2 * n + 2);
+   if (rc) return rc;
+   rc = growBuffer(c->flxTmp, c->flxTmpCap, n + 1);
    if (rc) return rc;
    unsigned* keyIn = (unsigned*)c->key;
    unsigned* keyOut = keyIn + (n + 1);
    unsigned* idxIn = (unsigned*)c->fsort;
    unsigned* idxOut = idxIn + (n + 1);
    if (n) {
-      k_fast_dual_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, aos, pcell, n, keyIn);
+      k_fast_seg_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, aos, pcell, n, keyIn, c->flxTmp);
       k_iota<<<blocks1d(n, 256), 256, 0, c->stream>>>(idxIn, n);
       RH_CUDA(cudaGetLastError());
       size_t sb = 0;
@@ -638,49 +660,41 @@ int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* partic
       sb = c->sortTmpBytes;
       RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream));
    }
-   DStore& D = c->ds[s];
-   RH_CUDA(cudaMemsetAsync(D.cnt, 0, sizeof(int) * Nd, c->stream));
+   SegHost& h = c->seg[s];
+   RH_CUDA(cudaMemsetAsync(h.cnt[h.cur], 0, sizeof(int) * NS, c->stream));
    if (n) {
-      k_fast_histogram<<<blocks1d(n, 256), 256, 0, c->stream>>>(keyOut, n, D.cnt);
+      k_fast_histogram<<<blocks1d(n, 256), 256, 0, c->stream>>>(keyOut, n, h.cnt[h.cur]);
       RH_CUDA(cudaGetLastError());
    }
    long long slots = 0;
-   rc = fastLayout(c, D.cnt, nullptr, D, &slots);
+   rc = fastLayout(c, h.cnt[h.cur], nullptr, h.base, &slots);
    if (rc) return rc;
-   rc = fastReserve(D, slots);
+   rc = segReserve(h, 0, slots);
    if (rc) return rc;
-   // first sorted position of every dual cell
-   k_int_to64<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(D.cnt, Nd, c->ftmp64);
-   RH_CUDA(cudaGetLastError());
-   bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->foff, Nd + 1, c->stream));
+   rc = segReserve(h, 1, slots);
+   if (rc) return rc;
+   long long tot2 = 0;
+   rc = segPrefix(c, h.cnt[h.cur], &tot2);
+   if (rc) return rc;
    if (n) {
-      k_fast_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(aos, keyOut, idxOut, n, c->foff, D);
+      k_fast_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(aos, c->flxTmp, keyOut, idxOut, n, c->ffirst,
+                                                                     segView(h, h.cur), h.base);
       RH_CUDA(cudaGetLastError());
    }
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   rc = fastPendingBuffers(c);
-   if (rc) return rc;
    rc = fastExponents(c);
    if (rc) return rc;
    return fastMoverBuffers(c);
 }
 
 int fastNumParticles(rhgpu_ctx* c, int s, long long* n) {
-   const long long Nd = c->fg.Nd;
-   k_int_to64<<<blocks1d(Nd + 1, 256), 256, 0, c->stream>>>(c->ds[s].cnt, Nd, c->ftmp64);
-   RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->foff, Nd + 1, c->stream));
-   RH_CUDA(cudaMemcpyAsync(n, c->foff + Nd, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
-   RH_CUDA(cudaStreamSynchronize(c->stream));
-   return RHGPU_OK;
+   return segPrefix(c, c->seg[s].cnt[c->seg[s].cur], n);
 }
 
 int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long long capacity, long long* n_out) {
-   const long long N = c->g.N, Nd = c->fg.Nd;
+   const long long N = c->g.N, NS = c->fg.NS;
    long long tot = 0;
-   int rc = fastNumParticles(c, s, &tot);   // leaves the sequence offsets in c->foff
+   int rc = fastNumParticles(c, s, &tot);   // leaves the segment offsets in c->ffirst
    if (rc) return rc;
    if (tot > capacity) return fail(RHGPU_ERR_ARG, "download_particles: capacity too small");
    rc = ensureKeyCapacity(c, 2 * tot + 2);
@@ -697,9 +711,11 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
    unsigned* idxOut = idxIn + (tot + 1);
    double* aos = (double*)c->staging;
    int* cellCnt = c->outCount;
+   const SegHost& h = c->seg[s];
    RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
    if (tot) {
-      k_fast_cell_keys<<<blocks1d(Nd, 128), 128, 0, c->stream>>>(c->g, c->fg, c->ds[s], c->foff, keyIn, c->fsortSlots);
+      k_fast_cell_keys<<<(unsigned)NS, 128, 0, c->stream>>>(c->g, c->fg, segView(h, h.cur), h.base, c->ffirst, keyIn,
+                                                           c->fsortSlots);
       k_iota<<<blocks1d(tot, 256), 256, 0, c->stream>>>(idxIn, tot);
       RH_CUDA(cudaGetLastError());
       size_t sb = 0;
@@ -709,7 +725,7 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
       sb = c->sortTmpBytes;
       RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream));
       k_fast_histogram<<<blocks1d(tot, 256), 256, 0, c->stream>>>(keyOut, tot, cellCnt);
-      k_fast_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(c->ds[s], c->fsortSlots, idxOut, tot, aos);
+      k_fast_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(segView(h, h.cur), c->fsortSlots, idxOut, tot, aos);
       RH_CUDA(cudaGetLastError());
    }
    RH_CUDA(cudaMemcpyAsync(counts, cellCnt, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
@@ -719,7 +735,7 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
    return RHGPU_OK;
 }
 
-// fused push + deposit, then placement of the off-row movers
+// fused push + deposit, then placement of the particles that left their segment
 int fastPush(rhgpu_ctx* c) {
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
@@ -729,54 +745,57 @@ int fastPush(rhgpu_ctx* c) {
    pp.use_gravity = c->P.use_gravity;
    pp.GMdt = c->P.GMdt;
    pp.maxVi2 = c->P.max_ion_speed2;
-   const long long N = c->g.N, Nd = c->fg.Nd;
+   const long long N = c->g.N, NS = c->fg.NS;
    RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "fast_push_deposit");
-      k_fast_push_deposit<<<blocks1d(c->fg.nrows, FAST_WARPS), 32 * FAST_WARPS, 0, c->stream>>>(
-         c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD, c->cntU, c->err);
+      k_fast_push_deposit<<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD,
+                                                             c->cntU, c->err);
       RH_LAUNCHED(c);
    }
    unsigned long long nm = 0;
    RH_CUDA(cudaMemcpyAsync(&nm, c->fb.nmovers, sizeof nm, cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   if ((long long)nm > c->fb.moverCap) return fail(RHGPU_ERR_CAPACITY, "off-row mover list overflow");
-   if (nm == 0) return RHGPU_OK;
-   const long long nb = (long long)c->ns * Nd;
-   int over = 0;
-   {
-   RH_TIME(c, "fast_migrate");
-   RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
-   RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
-   RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-   k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, Nd, c->finc);
-   RH_LAUNCHED(c);
-   k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
-   RH_LAUNCHED(c);
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
-   k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, Nd, c->foffInc, c->ffill, c->fbucket);
-   RH_LAUNCHED(c);
-   k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), Nd, c->fb.movers, c->finc, c->foffInc,
-                                                              c->fbucket, c->fover);
-   RH_LAUNCHED(c);
-   RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-   }
-   RH_CUDA(cudaStreamSynchronize(c->stream));
-   if (over) {
-      RH_TIME(c, "fast_repack");
-      // some dual cells lack room for their arrivals: relayout with room, place the rest
-      int rc = fastRepack(c, true);
-      if (rc) return rc;
-      RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-      k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), Nd, c->fb.movers, c->finc,
-                                                                 c->foffInc, c->fbucket, c->fover);
-      RH_LAUNCHED(c);
-      RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+   if ((long long)nm > c->fb.moverCap) return fail(RHGPU_ERR_CAPACITY, "mover list overflow");
+   if (nm > 0) {
+      const long long nb = (long long)c->ns * NS;
+      int over = 0;
+      {
+         RH_TIME(c, "fast_migrate");
+         RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
+         RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
+         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+         k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, NS, c->finc);
+         RH_LAUNCHED(c);
+         k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
+         RH_LAUNCHED(c);
+         size_t bytes = c->scanTmpBytes;
+         RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
+         k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, NS, c->foffInc, c->ffill,
+                                                                     c->fbucket);
+         RH_LAUNCHED(c);
+         k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->fb.movers, c->finc,
+                                                                    c->foffInc, c->fbucket, c->fover);
+         RH_LAUNCHED(c);
+         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      }
       RH_CUDA(cudaStreamSynchronize(c->stream));
-      if (over) return fail(RHGPU_ERR_CAPACITY, "dual-cell relayout did not make room");
+      if (over) {
+         // some segments lack room for their arrivals: relayout with room, place the rest
+         RH_TIME(c, "fast_relayout");
+         int rc = fastRelayoutNext(c);
+         if (rc) return rc;
+         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+         k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->fb.movers, c->finc,
+                                                                    c->foffInc, c->fbucket, c->fover);
+         RH_LAUNCHED(c);
+         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+         RH_CUDA(cudaStreamSynchronize(c->stream));
+         if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+      }
    }
+   for (int s = 0; s < c->ns; ++s) c->seg[s].cur ^= 1;
    return RHGPU_OK;
 }
 
@@ -861,29 +880,40 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    // fast-path geometry and buffers
    FastGeom& fg = c->fg;
    for (int a = 0; a < 3; ++a) fg.nd[a] = (a == 0 ? g.nx : a == 1 ? g.ny : g.nz) + (g.per[a] ? 0 : 1);
-   fg.Nd = (long long)fg.nd[0] * fg.nd[1] * fg.nd[2];
+   fg.nseg = (fg.nd[0] + SEG - 1) / SEG;
    fg.nrows = (long long)fg.nd[1] * fg.nd[2];
-   const long long Nd = fg.Nd, nb = (long long)n_species * fg.Nd;
+   fg.NS = fg.nrows * fg.nseg;
+   const long long NS = fg.NS, nb = (long long)n_species * fg.NS;
    for (int s = 0; s < n_species; ++s) {
-      alloc((void**)&c->ds[s].start, sizeof(long long) * (Nd + 1));
-      alloc((void**)&c->ds[s].cnt, sizeof(int) * Nd);
-      alloc((void**)&c->dalt[s].start, sizeof(long long) * (Nd + 1));
-      alloc((void**)&c->dalt[s].cnt, sizeof(int) * Nd);
+      SegHost& h = c->seg[s];
+      alloc((void**)&h.cnt[0], sizeof(int) * NS);
+      alloc((void**)&h.cnt[1], sizeof(int) * NS);
+      alloc((void**)&h.base, sizeof(long long) * (NS + 1));
+      alloc((void**)&h.baseAlt, sizeof(long long) * (NS + 1));
       c->capHint[s] = capacity ? (long long)capacity[s] : 0;
    }
    alloc((void**)&c->fb.RP, sizeof(double) * 16 * fg.nrows * g.nx);
+   alloc((void**)&c->fb.RPB, sizeof(double) * 16 * fg.nrows * fg.nseg);
    alloc((void**)&c->fb.MMlo, sizeof(unsigned long long) * 4 * N);
    alloc((void**)&c->fb.MMhi, sizeof(unsigned long long) * 4 * N);
    alloc((void**)&c->fb.touched, sizeof(unsigned) * (N / 32 + 1));
    alloc((void**)&c->fb.nmovers, sizeof(unsigned long long));
    alloc((void**)&c->finc, sizeof(int) * nb);
    alloc((void**)&c->ffill, sizeof(int) * nb);
-   alloc((void**)&c->foff, sizeof(long long) * (Nd + 1));
-   alloc((void**)&c->ftmp64, sizeof(long long) * (Nd + 1));
+   alloc((void**)&c->fcap, sizeof(long long) * (NS + 1));
+   alloc((void**)&c->ffirst, sizeof(long long) * (NS + 1));
+   alloc((void**)&c->ftmp64, sizeof(long long) * (NS + 1));
    alloc((void**)&c->ftmpCellStart, sizeof(long long) * (N + 1));
    alloc((void**)&c->ftmpInc64, sizeof(long long) * (nb + 1));
    alloc((void**)&c->foffInc, sizeof(long long) * (nb + 1));
    alloc((void**)&c->fover, sizeof(unsigned long long));
+   if (!rc) {
+      // MM starts at zero; k_fast_gather clears what a step touched
+      if (cudaMemset(c->fb.MMlo, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
+          cudaMemset(c->fb.MMhi, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
+          cudaMemset(c->fb.RPB, 0, sizeof(double) * 16 * fg.nrows * fg.nseg) != cudaSuccess)
+         rc = fail(RHGPU_ERR_CUDA, "create: clear fast-path sums");
+   }
    if (!rc) {
       // scan scratch for the largest scan (cells, dual cells, species x dual cells)
       size_t bytes = 0;
@@ -940,17 +970,20 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->newCount); cudaFree(c->scanTmp); cudaFree(c->S); cudaFree(c->cntU); cudaFree(c->cntD); cudaFree(c->err);
    cudaFree(c->staging);
    for (int s = 0; s < c->ns; ++s) {
-      for (DStore* d : {&c->ds[s], &c->dalt[s]}) {
-         for (int a = 0; a < 7; ++a) cudaFree(d->a[a]);
-         cudaFree(d->start);
-         cudaFree(d->cnt);
+      SegHost& h = c->seg[s];
+      for (int b = 0; b < 2; ++b) {
+         for (int a = 0; a < 7; ++a) cudaFree(h.a[b][a]);
+         cudaFree(h.lx[b]);
+         cudaFree(h.cnt[b]);
       }
+      cudaFree(h.base);
+      cudaFree(h.baseAlt);
    }
-   cudaFree(c->fb.RP); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
-   cudaFree(c->fb.nmovers); cudaFree(c->fb.movers); cudaFree(c->fb.pend);
-   cudaFree(c->finc); cudaFree(c->ffill); cudaFree(c->foff); cudaFree(c->fbucket); cudaFree(c->fover);
-   cudaFree(c->sortTmp); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart); cudaFree(c->ftmpInc64);
-   cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots);
+   cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
+   cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
+   cudaFree(c->finc); cudaFree(c->ffill); cudaFree(c->fbucket); cudaFree(c->fover);
+   cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
+   cudaFree(c->ftmpInc64); cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots); cudaFree(c->flxTmp);
    for (int s = 0; s < c->ns; ++s) { freeStore(c->ps[s]); freeStore(c->alt[s]); }
    for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
    if (c->stream) cudaStreamDestroy(c->stream);

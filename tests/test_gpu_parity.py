@@ -216,8 +216,11 @@ def test_fast_closed_box_bitwise_every_step(gpu_lib, port_lib):
         assert_state_equal(x, y, f"fast closed box step {n + 1}")
 
 
-@pytest.mark.parametrize("variant", ["isothermal_no_hall", "gravity_flowthrough", "mixed_periodic", "odd_sizes"])
+@pytest.mark.parametrize("variant", ["isothermal_no_hall", "gravity_flowthrough", "mixed_periodic", "odd_sizes",
+                                     "segments_walls", "segments_periodic"])
 def test_fast_option_variants_bitwise(gpu_lib, port_lib, variant):
+    """Option variants; the last two have rows of 3 storage segments (71 and
+    70 dual cells), so particles cross segment boundaries."""
     if variant == "isothermal_no_hall":
         cfg = closed_box_config(electron_gamma=1, use_hall_term=False, electric_field_linear_smoothing_number=2,
                                 electric_field_smoothing_gauss_sigma=0.0, periodic=(1, 0, 1))
@@ -226,8 +229,12 @@ def test_fast_option_variants_bitwise(gpu_lib, port_lib, variant):
                                 periodic=(0, 1, 0), max_electric_field=-1)
     elif variant == "mixed_periodic":
         cfg = closed_box_config(nx=9, ny=7, nz=11, periodic=(0, 0, 1), ppc=6.0)
-    else:
+    elif variant == "odd_sizes":
         cfg = closed_box_config(nx=37, ny=5, nz=3, periodic=(1, 1, 0), ppc=9.0)
+    elif variant == "segments_walls":
+        cfg = closed_box_config(nx=70, ny=5, nz=4, ppc=5.0)
+    else:
+        cfg = closed_box_config(nx=70, ny=4, nz=5, periodic=(1, 0, 1), ppc=5.0)
     assert_state_equal(run(gpu_lib, cfg, 6, fast=True), run(port_lib, cfg, 6, fast=True), "fast " + variant)
 
 
@@ -253,17 +260,17 @@ def test_fast_closed_box_vs_reference_order(gpu_lib, port_lib):
                        bitwise=False, rtol=1e-12, sum_rtol=1e-12)
 
 
-def test_fast_slack_overflow_repack(gpu_lib, port_lib):
-    """Two cold beams converging on the middle of a periodic box pile up more
-    particles in a dual cell than its slack holds: the in-row overflow and
-    repack paths stay bitwise with the oracle."""
-    cfg = cf.config_empty_box(16, 4, 4, ppc=12.0).replace(dt=0.06)
+def test_fast_segment_overflow_relayout(gpu_lib, port_lib):
+    """Two cold beams converging in y pile up more particles in the middle
+    dual rows than their segments' slack holds: the mover placement overflows,
+    the storage is relaid out, and the result stays bitwise with the oracle."""
+    cfg = cf.config_empty_box(16, 16, 4, ppc=12.0).replace(dt=0.06)
     cfg = cfg.replace(populations=[dataclasses.replace(cfg.populations[0], temperature=1e2)])
     grid, pops = cf.initial_state(cfg)
     cnt, p = pops[0]
     p = p.copy()
-    i = np.repeat(np.arange(cnt.size), cnt.astype(np.int64)) % cfg.nx
-    p[:, 3] = np.where(i < cfg.nx // 2, 1.2e6, -1.2e6)
+    j = (np.repeat(np.arange(cnt.size), cnt.astype(np.int64)) // cfg.nx) % cfg.ny
+    p[:, 4] = np.where(j < cfg.ny // 2, 1.2e6, -1.2e6)
     pops = [(cnt, p)]
     a = run(gpu_lib, cfg, 12, grid=grid, pops=pops, fast=True)
     b = run(port_lib, cfg, 12, grid=grid, pops=pops, fast=True)
