@@ -20,11 +20,13 @@
 //                        boundary removal (particle_boundary_cond_hybrid.h:112-185).
 //                        Particles that stay in the segment are written to the
 //                        next buffer in order; their deposit records go to
-//                        shared memory, are counting-sorted by target dual cell
-//                        (stable) and summed sequentially per (dual cell,
-//                        corner, moment) in FP64. Particles that leave the
-//                        segment go to the mover list and deposit as exact
-//                        128-bit fixed-point sums.
+//                        shared memory counting-sorted by target dual cell
+//                        (stable) and are summed sequentially per (dual cell,
+//                        corner, moment) in FP64, one thread per (dual cell,
+//                        corner). Particles that leave the segment go to the
+//                        mover list.
+//   k_fast_mover_deposit the movers' CIC contributions as exact 128-bit
+//                        fixed-point sums (order-independent)
 //   k_fast_mig_*         placement of the movers after the stayers of their
 //                        destination segment, in (source segment, index) order
 //   k_fast_gather        cell moments from the four row partials (+ the segment
@@ -42,8 +44,8 @@ constexpr int FAST_MAX_SPECIES = 8;
 constexpr int SEG = RHGPU_FAST_SEGMENT;   // dual cells per segment
 constexpr int FT = 256;                   // threads of k_fast_push_deposit (one chunk of particles)
 constexpr int FW = FT / 32;
-constexpr int REC = 13;                   // doubles per deposit record: w8[8], 1.0, v[3], pad
-static_assert(SEG == 32 && SEG * FW == FT, "the deposit sort maps (dual cell, warp) to one thread");
+constexpr int REC = 11;                   // doubles per deposit record: w8[8], v[3]
+static_assert(SEG == 32 && SEG * 8 == FT, "the deposit sums map (dual cell, corner) to one thread");
 
 struct SegBuf {
    double* a[7];        // x, y, z (cell-local), vx, vy, vz, weight
@@ -73,8 +75,10 @@ struct Mover {
    unsigned long long key;
    long long dest;   // destination segment
    int species;
-   int lx;
+   int lx;           // dual x in the destination segment | MOVER_* flags
 };
+constexpr int MOVER_DEPOSIT = 1 << 8;   // deposits its CIC contributions (fixed point)
+constexpr int MOVER_PLACE = 1 << 9;     // is stored in the destination segment
 
 struct FastBufs {
    double* RP;                 // row partials: 4 planes x nrows x nx x 4
@@ -88,7 +92,8 @@ struct FastBufs {
    double scaleR, scaleJ;      // 2^kR, 2^kJ
 };
 
-__host__ __device__ inline int dualU(int b, int n, int per) { return per ? ((b % n) + n) % n : b + 1; }
+// b in [-n, 2n)
+__host__ __device__ inline int dualU(int b, int n, int per) { return per ? (b < 0 ? b + n : (b >= n ? b - n : b)) : b + 1; }
 __host__ __device__ inline int dualB(int u, int per) { return per ? u : u - 1; }
 __host__ __device__ inline int halfS(double x, double dx) { return (x < (0 + 0.5) * dx) ? 0 : 1; }
 
@@ -165,43 +170,18 @@ __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const Species
    return clamp;
 }
 
-// exclusive prefix sum over the FT threads of the block; *total = block sum
-__device__ inline int blockExclusiveScan(int v, int* s_w, int* total) {
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   int x = v;
-   for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-   }
-   if (lane == 31) s_w[warp] = x;
-   __syncthreads();
-   if (warp == 0) {
-      int t = lane < FW ? s_w[lane] : 0;
-      for (int o = 1; o < 32; o <<= 1) {
-         const int y = __shfl_up_sync(0xffffffffu, t, o);
-         if (lane >= o) t += y;
-      }
-      if (lane < FW) s_w[lane] = t;
-   }
-   __syncthreads();
-   const int r = (warp ? s_w[warp - 1] : 0) + x - v;
-   *total = s_w[FW - 1];
-   __syncthreads();
-   return r;
-}
-
-__global__ void __launch_bounds__(FT)
+__global__ void __launch_bounds__(FT, 3)
 k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
    __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
-   __shared__ unsigned char s_rdual[FT];          // target dual x (in the segment) of each record
-   __shared__ short s_sidx[FT];                   // records sorted by target dual cell
-   __shared__ int s_off[SEG * FW + 1];            // (dual cell, warp) counts, then offsets
-   __shared__ int s_scan[FW];
+   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell)
+   __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell
+   __shared__ int s_wcnt[FW];                     // stayers | records << 16 per warp
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ int s_first[FAST_MAX_SPECIES];
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+   const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
    const long long row = S / fg.nseg;
    const int gseg = (int)(S % fg.nseg);
@@ -209,7 +189,6 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    const int ndx = fg.nd[0];
    const int u0 = gseg * SEG, u1 = min(u0 + SEG, ndx);
    const int ns = FS.ns;
-   const long long N = g.N;
    const double dx = g.dx;
    if (tid == 0) {
       int a = 0;
@@ -222,8 +201,8 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
    __syncthreads();
    const int total = s_prefix[ns];
-   const int qo = lane >> 2, qm = 8 + (lane & 3);   // this lane's corner and moment factor in a record
-   double acc[4] = {0.0, 0.0, 0.0, 0.0};            // (dual cell warp + FW*j, corner*4 + moment lane)
+   const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
+   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 
    for (int c0 = 0; c0 < total; c0 += FT) {
       const int i = c0 + tid;
@@ -233,6 +212,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
       double st[7];
       bool stay = false, rec = false, leave = false, clamp = false;
+      int mflags = 0;
       int vx = 0, vy = 0, vz = 0;
       double w8[8];
       long long p = 0;
@@ -245,7 +225,9 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          int ci = dualB(u, g.per[0]) + 1 - halfS(st[0], dx);
          int cj = dualB(uy, g.per[1]) + 1 - halfS(st[1], dx);
          int ck = dualB(uz, g.per[2]) + 1 - halfS(st[2], dx);
-         wrapc(ci, g.nx, 1); wrapc(cj, g.ny, 1); wrapc(ck, g.nz, 1);
+         if (ci >= g.nx) ci -= g.nx;   // periodic axes: dual cell 0 holds the upper half of the last cell
+         if (cj >= g.ny) cj -= g.ny;
+         if (ck >= g.nz) ck -= g.nz;
          clamp = pushOne(g, f, FS.sp[s], pp, ci, cj, ck, st);
          if (isnan(st[0]) || isnan(st[1]) || isnan(st[2])) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
          int ox, oy, oz;
@@ -259,26 +241,17 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             atomicAdd(&cntd[4 * s + 0], st[6]);
             atomicAdd(&cntd[4 * s + 1], ke);
          } else {
-            const int bx = ti + halfS(st[0], dx) - 1, by = tj + halfS(st[1], dx) - 1, bz = tk + halfS(st[2], dx) - 1;
-            vx = dualU(bx, g.nx, g.per[0]);
-            vy = dualU(by, g.ny, g.per[1]);
-            vz = dualU(bz, g.nz, g.per[2]);
+            vx = dualU(ti + halfS(st[0], dx) - 1, g.nx, g.per[0]);
+            vy = dualU(tj + halfS(st[1], dx) - 1, g.ny, g.per[1]);
+            vz = dualU(tk + halfS(st[2], dx) - 1, g.nz, g.per[2]);
             const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.sp[s].accumulate) {
-               int ind[8];
-               cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, dx, w8, ind);
                if (inSeg) {
+                  int ind[8];
+                  cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, dx, w8, ind);
                   rec = true;
                } else {
-                  for (int o = 0; o < 8; ++o) {
-                     int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);
-                     if (!wrapc(dxc, g.nx, g.per[0]) || !wrapc(dyc, g.ny, g.per[1]) || !wrapc(dzc, g.nz, g.per[2])) continue;
-                     const long long dc = cidx(g, dxc, dyc, dzc);
-                     add128(&fb.MMlo[dc], &fb.MMhi[dc], w8[o], fb.scaleR);
-                     for (int l = 0; l < 3; ++l)
-                        add128(&fb.MMlo[(1 + l) * N + dc], &fb.MMhi[(1 + l) * N + dc], w8[o] * st[3 + l], fb.scaleJ);
-                     atomicOr(&fb.touched[dc >> 5], 1u << (dc & 31));
-                  }
+                  mflags |= MOVER_DEPOSIT;   // deposited by k_fast_mover_deposit
                }
             }
             // boundary conditions of the step
@@ -300,17 +273,30 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             }
             if (!removed) {
                stay = inSeg;
-               leave = !inSeg;
+               if (!inSeg) mflags |= MOVER_PLACE;
             }
+            leave = mflags != 0;
          }
       }
       if (clamp) atomicAdd(&cntu[CNT_SPECIES_MAXVI + s], 1ull);
 
-      // ---- order of the chunk's stayers and records ------------------------------------
-      int tot;
-      const int ex = blockExclusiveScan((stay ? 1 : 0) | (rec ? 1 << 16 : 0), s_scan, &tot);
-      const int stayIdx = ex & 0xffff, recIdx = ex >> 16, nrec = tot >> 16;
+      // ---- order of the chunk's stayers and records: warp ballots + per-warp totals -----
+      const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
+      if (lane == 0) s_wcnt[warp] = __popc(bs) | (__popc(br) << 16);
+      s_wd[warp][lane] = 0;
+      __syncthreads();
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += s_wcnt[w];
+      const int stayIdx = (before & 0xffff) + __popc(bs & below);
       if (active && i == max(s_prefix[s], c0)) s_first[s] = stayIdx;
+      // records per (warp, dual cell) and the rank within the warp
+      const int rd = rec ? vx - u0 : 0;
+      int rrank = 0;
+      if (rec) {
+         const unsigned mm = __match_any_sync(br, rd);
+         rrank = __popc(mm & below);
+         if (rrank == 0) s_wd[warp][rd] = __popc(mm);
+      }
       __syncthreads();
       if (stay) {
          const SegSpecies& SS = FS.st[s];
@@ -318,12 +304,17 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
          SS.nxt.lx[slot] = (unsigned char)(vx - u0);
       }
-      if (rec) {
-         double* r = s_rec + recIdx * REC;
-         for (int o = 0; o < 8; ++o) r[o] = w8[o];
-         r[8] = 1.0;
-         r[9] = st[3]; r[10] = st[4]; r[11] = st[5];
-         s_rdual[recIdx] = (unsigned char)(vx - u0);
+      if (warp == 0) {
+         // first sorted record of each dual cell
+         int t = 0;
+         for (int w = 0; w < FW; ++w) t += s_wd[w][lane];
+         int x = t;
+         for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+         }
+         s_bin[lane] = x - t;
+         if (lane == 31) s_bin[SEG] = x;
       }
       {
          const unsigned lm = __ballot_sync(0xffffffffu, leave);
@@ -333,7 +324,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             if (lane == leader) b0 = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
             b0 = __shfl_sync(0xffffffffu, b0, leader);
             if (leave) {
-               const unsigned long long m = b0 + __popc(lm & ((1u << lane) - 1u));
+               const unsigned long long m = b0 + __popc(lm & below);
                if ((long long)m < fb.moverCap) {
                   Mover& M = fb.movers[m];
                   for (int a = 0; a < 7; ++a) M.s[a] = st[a];
@@ -341,7 +332,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
                   const int gd = vx / SEG;
                   M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * fg.nseg + gd;
                   M.species = s;
-                  M.lx = vx - gd * SEG;
+                  M.lx = (vx - gd * SEG) | mflags;
                } else {
                   raiseError(err, RHGPU_DEVERR_CAPACITY);
                }
@@ -351,33 +342,24 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       __syncthreads();
       // running stayer count of each species: the chunk's last thread of the species adds
       if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - s_first[s];
-
-      // ---- records sorted by target dual cell (stable), then summed in that order -------
-      s_off[tid] = 0;
-      __syncthreads();
-      const bool hasRec = tid < nrec;
-      const int rd = hasRec ? s_rdual[tid] : 0;
-      const unsigned am = __ballot_sync(0xffffffffu, hasRec);
-      int rrank = 0;
-      if (hasRec) {
-         const unsigned mm = __match_any_sync(am, rd);
-         rrank = __popc(mm & ((1u << lane) - 1u));
-         if (rrank == 0) s_off[rd * FW + warp] = __popc(mm);
+      if (rec) {
+         int pos = s_bin[rd] + rrank;
+         for (int w = 0; w < warp; ++w) pos += s_wd[w][rd];
+         double* r = s_rec + pos * REC;
+         for (int o = 0; o < 8; ++o) r[o] = w8[o];
+         r[8] = st[3]; r[9] = st[4]; r[10] = st[5];
       }
       __syncthreads();
-      int dummy;
-      const int off = blockExclusiveScan(s_off[tid], s_scan, &dummy);
-      s_off[tid] = off;
-      if (tid == 0) s_off[SEG * FW] = nrec;
-      __syncthreads();
-      if (hasRec) s_sidx[s_off[rd * FW + warp] + rrank] = (short)tid;
-      __syncthreads();
-      for (int j = 0; j < 4; ++j) {
-         const int d = warp + FW * j;
-         const int r1 = s_off[(d + 1) * FW];
-         for (int r = s_off[d * FW]; r < r1; ++r) {
-            const double* rr = s_rec + s_sidx[r] * REC;
-            acc[j] += rr[qo] * rr[qm];
+      // ---- sums of this thread's (dual cell, corner), records in list order ----------------
+      {
+         const int r1 = s_bin[myDual + 1];
+         for (int r = s_bin[myDual]; r < r1; ++r) {
+            const double* rr = s_rec + r * REC;
+            const double w = rr[myCorner];
+            a0 += w;
+            a1 += w * rr[8];
+            a2 += w * rr[9];
+            a3 += w * rr[10];
          }
       }
       __syncthreads();
@@ -385,7 +367,10 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
 
    // ---- outputs: stayer counts, row partials, segment-boundary partial ---------------------
    if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
-   for (int j = 0; j < 4; ++j) s_rec[(warp + FW * j) * 32 + lane] = acc[j];
+   {
+      double* q = s_rec + myDual * 32 + myCorner * 4;
+      q[0] = a0; q[1] = a1; q[2] = a2; q[3] = a3;
+   }
    __syncthreads();
    const int nx = g.nx;
    const long long nrows = fg.nrows;
@@ -410,6 +395,34 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    if (tid < 16 && (g.per[0] ? fg.nseg > 1 : gseg >= 1)) {
       const int qq = tid >> 2, m = tid & 3;
       fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = s_rec[((2 * qq) << 2) + m];
+   }
+}
+
+// CIC contributions of the particles that left their segment, as exact fixed-point sums (MM)
+__global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, FastBufs fb, long long n) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= n) return;
+   const Mover& M = fb.movers[t];
+   if (!(M.lx & MOVER_DEPOSIT)) return;
+   const int s = M.species;
+   const long long row = M.dest / fg.nseg;
+   const int vx = (int)(M.dest % fg.nseg) * SEG + (M.lx & 0xff);
+   const int vy = (int)(row % fg.nd[1]), vz = (int)(row / fg.nd[1]);
+   const int bx = dualB(vx, g.per[0]), by = dualB(vy, g.per[1]), bz = dualB(vz, g.per[2]);
+   double st[7];
+   for (int a = 0; a < 7; ++a) st[a] = M.s[a];
+   double w8[8];
+   int ind[8];
+   cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, g.dx, w8, ind);
+   const long long N = g.N;
+   for (int o = 0; o < 8; ++o) {
+      int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);
+      if (!wrapc(dxc, g.nx, g.per[0]) || !wrapc(dyc, g.ny, g.per[1]) || !wrapc(dzc, g.nz, g.per[2])) continue;
+      const long long dc = cidx(g, dxc, dyc, dzc);
+      add128(&fb.MMlo[dc], &fb.MMhi[dc], w8[o], fb.scaleR);
+      for (int l = 0; l < 3; ++l)
+         add128(&fb.MMlo[(1 + l) * N + dc], &fb.MMhi[(1 + l) * N + dc], w8[o] * st[3 + l], fb.scaleJ);
+      atomicOr(&fb.touched[dc >> 5], 1u << (dc & 31));
    }
 }
 
@@ -448,12 +461,12 @@ __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, do
 // ---- mover placement ------------------------------------------------------------------------
 __global__ void k_fast_mig_count(const Mover* mv, long long n, long long NS, int* inc) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= n) return;
+   if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    atomicAdd(&inc[(long long)mv[t].species * NS + mv[t].dest], 1);
 }
 __global__ void k_fast_mig_bucket(const Mover* mv, long long n, long long NS, const long long* off, int* fill, int* bucket) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= n) return;
+   if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    const long long b = (long long)mv[t].species * NS + mv[t].dest;
    const int k = atomicAdd(&fill[b], 1);
    bucket[off[b] + k] = (int)t;
@@ -477,7 +490,7 @@ __global__ void k_fast_mig_place(FastSpecies FS, long long NS, const Mover* mv, 
    for (int a = 0; a < k; ++a) {
       const Mover& M = mv[bk[a]];
       for (int e = 0; e < 7; ++e) SS.nxt.a[e][pos + a] = M.s[e];
-      SS.nxt.lx[pos + a] = (unsigned char)M.lx;
+      SS.nxt.lx[pos + a] = (unsigned char)(M.lx & 0xff);
    }
    SS.nxt.cnt[S] += k;
    inc[b] = 0;

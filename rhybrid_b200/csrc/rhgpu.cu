@@ -759,6 +759,11 @@ int fastPush(rhgpu_ctx* c) {
    RH_CUDA(cudaStreamSynchronize(c->stream));
    if ((long long)nm > c->fb.moverCap) return fail(RHGPU_ERR_CAPACITY, "mover list overflow");
    if (nm > 0) {
+      RH_TIME(c, "fast_mover_deposit");
+      k_fast_mover_deposit<<<blocks1d(nm, 128), 128, 0, c->stream>>>(c->g, c->fg, fastSpecies(c), c->fb, nm);
+      RH_LAUNCHED(c);
+   }
+   if (nm > 0) {
       const long long nb = (long long)c->ns * NS;
       int over = 0;
       {
