@@ -170,7 +170,7 @@ __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const Species
    return clamp;
 }
 
-__global__ void __launch_bounds__(FT, 3)
+__global__ void __launch_bounds__(FT, 4)
 k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
    __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
