@@ -6,7 +6,10 @@
  *      (src/particle_propagator_boris_buneman.h:64-194, getFields
  *      src/hybrid_propagator.cpp:1879-1891): face-linear B, NGP Ue and Ep.
  *   2. Cell-to-cell migration of particles that left their cell (Corsair's
- *      particle list, not vendored; rule restated in DESIGN.md).
+ *      particle list, not vendored): a coordinate that left [0,dx) shifts by
+ *      exactly one cell (x+dx or x-dx; x+dx >= dx becomes the largest double
+ *      below dx); a particle that moved more than one cell, or left a
+ *      non-periodic box, is removed and counted as an escape.
  *   3. CIC charge and ion-current deposit (src/particle_accumulator.cpp:44-156)
  *      with the finalize step /dV and rho clamp (:319-333).
  *   4. Particle boundary conditions (src/particle_boundary_cond_hybrid.h:112-185).

@@ -76,9 +76,10 @@ __host__ __device__ inline int dirFromOffset(int dxs, int dys, int dzs) { return
 __host__ __device__ inline int dirRank(int dir) { return dir == 13 ? 0 : (dir < 13 ? dir + 1 : dir); }
 __host__ __device__ inline int rankToDir(int r) { return r == 0 ? 13 : (r <= 13 ? r - 1 : r); }
 
-// Particle migration rule ("Migration"): a local coordinate
-// that left [0,dx) shifts by exactly one cell. Returns nonzero when the
-// particle moved more than one cell.
+// Particle migration (Corsair's particle list is not vendored; this is the
+// rule the oracle restates too): a local coordinate that left [0,dx) shifts
+// by exactly one cell, x + dx rounding up to dx becomes the largest double
+// below dx. Returns nonzero when the particle moved more than one cell.
 __host__ __device__ inline int migrateAxis(double& x, int& off, double dx, double dx_below) {
    int st = 0;
    off = 0;
