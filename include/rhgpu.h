@@ -218,6 +218,7 @@ int rhgpu_accumulate(rhgpu_ctx* ctx);        /* clear, deposit all species, fina
 int rhgpu_apply_boundaries(rhgpu_ctx* ctx);  /* exterior-cell and obstacle removal */
 int rhgpu_propagate_fields(rhgpu_ctx* ctx);  /* propagateB */
 
+
 /* Synchronises and returns the accumulated device error word (RHGPU_DEVERR_*). */
 int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);
 

@@ -105,6 +105,7 @@ NeumannTables buildNeumannTables() {
 
 struct TimerRec { int cls; int ea, eb; };
 
+
 // one species' row-segment storage: two particle buffers sharing the layout `base`
 struct SegHost {
    double* a[2][7] = {};
@@ -332,6 +333,7 @@ int pushAll(rhgpu_ctx* c) {
    pp.maxVi2 = c->P.max_ion_speed2;
    for (int s = 0; s < c->ns; ++s) {
       PStore& P = c->ps[s];
+      if (!P.start) continue;   // species without uploaded particles
       int rc = ensureKeyCapacity(c, P.nslots);
       if (rc) return rc;
       if (P.nslots > 0) {
@@ -346,11 +348,14 @@ int pushAll(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
-int accumulateAll(rhgpu_ctx* c) {
-   if (!c->S) RH_CUDA(cudaMalloc(&c->S, sizeof(double) * 108 * c->g.N));
+// species whose particles the exact-path deposit adds (accumulating, particles uploaded)
+bool deposits(const rhgpu_ctx* c, int s) { return c->sp[s].accumulate && c->ps[s].start; }
+
+// exact-path deposit with the 108 per-cell sums in S (108 * N doubles)
+int depositExact(rhgpu_ctx* c, double* S) {
    int last = -1, first = -1;
    for (int s = 0; s < c->ns; ++s)
-      if (c->sp[s].accumulate) { if (first < 0) first = s; last = s; }
+      if (deposits(c, s)) { if (first < 0) first = s; last = s; }
    const GridInfo& g = c->g;
    if (last < 0) {
       RH_TIME(c, "deposit_gather");
@@ -358,15 +363,15 @@ int accumulateAll(rhgpu_ctx* c) {
       RH_LAUNCHED(c);
    }
    for (int s = 0; s < c->ns; ++s) {
-      if (!c->sp[s].accumulate) continue;
+      if (!deposits(c, s)) continue;
       {
          RH_TIME(c, "deposit_cell");
-         k_deposit_cell<<<blocks1d(g.N, DEP_WARPS), 32 * DEP_WARPS, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, c->S, c->err);
+         k_deposit_cell<<<blocks1d(g.N, DEP_WARPS), 32 * DEP_WARPS, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, S, c->err);
          RH_LAUNCHED(c);
       }
       {
          RH_TIME(c, "deposit_gather");
-         k_deposit_gather<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->f, c->S, s == first, s == last,
+         k_deposit_gather<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->f, S, s == first, s == last,
                                                                       c->P.min_ion_charge_density, c->cntU);
          RH_LAUNCHED(c);
       }
@@ -374,8 +379,14 @@ int accumulateAll(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+int accumulateAll(rhgpu_ctx* c) {
+   if (!c->S) RH_CUDA(cudaMalloc(&c->S, sizeof(double) * 108 * c->g.N));
+   return depositExact(c, c->S);
+}
+
 int boundariesAll(rhgpu_ctx* c) {
    for (int s = 0; s < c->ns; ++s) {
+      if (!c->ps[s].start) continue;
       if (c->next > 0) {
          RH_TIME(c, "bc_exterior");
          k_bc_exterior<<<blocks1d(c->next, 128), 128, 0, c->stream>>>(c->g, c->ps[s], c->ext, c->next, c->cntD, s);
