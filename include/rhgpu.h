@@ -218,6 +218,22 @@ int rhgpu_accumulate(rhgpu_ctx* ctx);        /* clear, deposit all species, fina
 int rhgpu_apply_boundaries(rhgpu_ctx* ctx);  /* exterior-cell and obstacle removal */
 int rhgpu_propagate_fields(rhgpu_ctx* ctx);  /* propagateB */
 
+/* rhgpu_accumulate for callers that cannot allocate device memory once the
+ * run has started: a host that has handed the remaining GPU memory to its
+ * own pool, or one that cannot afford the implicit device synchronisation a
+ * cudaMalloc may cause. No counterpart in the reference (which has no device
+ * memory); it computes exactly what rhgpu_accumulate computes on the exact
+ * path, but keeps the deposit's per-cell scratch (108 doubles per cell) in a
+ * fixed array in the library's static device memory instead of a buffer
+ * allocated on first use, and allocates nothing at any call.
+ * Limits: the context must use RHGPU_PATH_EXACT (else RHGPU_ERR_STATE) and
+ * its grid must have at most RHGPU_NOALLOC_MAX_CELLS cells (else
+ * RHGPU_ERR_ARG). The first call on a device looks up the scratch's device
+ * address (cudaGetSymbolAddress) with that device current; make it before
+ * any stream capture. The scratch is shared by every context on the device:
+ * calls that overlap in time (other threads, other streams) race. */
+#define RHGPU_NOALLOC_MAX_CELLS 16384
+int rhgpu_accumulate_noalloc(rhgpu_ctx* ctx);
 
 /* Synchronises and returns the accumulated device error word (RHGPU_DEVERR_*). */
 int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);

@@ -132,6 +132,7 @@ _OPTIONAL = {
     "version": [],
     "set_deposit_order": [_P, C.c_int32],
     "set_path": [_P, C.c_int32],
+    "accumulate_noalloc": [_P],
     "set_threads": [_P, C.c_int32],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p}
@@ -311,6 +312,10 @@ class Context:
 
     def set_deposit_order(self, order: int):
         self.lib.call("set_deposit_order", self.h, order)
+
+    def accumulate_noalloc(self):
+        """rhgpu_accumulate_noalloc: the exact-path deposit without any device allocation."""
+        self.lib.call("accumulate_noalloc", self.h)
 
     def set_path(self, path: int):
         self.lib.call("set_path", self.h, path)

@@ -105,6 +105,14 @@ NeumannTables buildNeumannTables() {
 
 struct TimerRec { int cls; int ea, eb; };
 
+// Scratch of rhgpu_accumulate_noalloc: the exact-path deposit's 108 per-cell
+// sums (S[e*N + c]) for grids of up to RHGPU_NOALLOC_MAX_CELLS cells, in the
+// module's static device memory; every entry of a cell is written before it
+// is read, so nothing needs clearing. Its device address is looked up once
+// per device.
+__device__ __align__(256) double g_noallocScratch[108 * (size_t)RHGPU_NOALLOC_MAX_CELLS];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double* g_noallocPtr[NOALLOC_MAX_DEVICES] = {};
 
 // one species' row-segment storage: two particle buffers sharing the layout `base`
 struct SegHost {
@@ -1220,6 +1228,32 @@ int rhgpu_accumulate(rhgpu_ctx* c) {
    if (!c) return fail(RHGPU_ERR_ARG, "null context");
    RH_CUDA(cudaSetDevice(c->device));
    int rc = phaseAccumulate(c);
+   if (rc) return rc;
+   return checkDeviceError(c);
+}
+
+int rhgpu_accumulate_noalloc(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   if (c->path != RHGPU_PATH_EXACT) return fail(RHGPU_ERR_STATE, "accumulate_noalloc: the context must use RHGPU_PATH_EXACT");
+   if (c->g.N > RHGPU_NOALLOC_MAX_CELLS)
+      return fail(RHGPU_ERR_ARG, "accumulate_noalloc: the grid has more cells than RHGPU_NOALLOC_MAX_CELLS (" +
+                                     std::to_string(RHGPU_NOALLOC_MAX_CELLS) + ")");
+   if (c->device < 0 || c->device >= NOALLOC_MAX_DEVICES) return fail(RHGPU_ERR_ARG, "accumulate_noalloc: device index out of range");
+   RH_CUDA(cudaSetDevice(c->device));
+   double* S = g_noallocPtr[c->device];
+   if (!S) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+      if (e != cudaSuccess || !p)
+         return fail(RHGPU_ERR_CUDA, std::string("accumulate_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      S = (double*)p;
+      g_noallocPtr[c->device] = S;
+   }
+   // the kernel timer creates events on demand: off for this call
+   const bool timing = c->timing;
+   c->timing = false;
+   const int rc = depositExact(c, S);
+   c->timing = timing;
    if (rc) return rc;
    return checkDeviceError(c);
 }
