@@ -512,9 +512,19 @@ __global__ void k_fast_seg_of(GridInfo g, FastGeom fg, const double* aos, const 
    key[p] = (unsigned)(((long long)uy + (long long)fg.nd[1] * uz) * fg.nseg + gs);
    lx[p] = (unsigned char)(ux - gs * SEG);
 }
-__global__ void k_fast_histogram(const unsigned* key, long long n, int* cnt) {
-   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (p < n) atomicAdd(&cnt[key[p]], 1);
+// for keys sorted ascending: first[k] = first position with key >= k, k in [0, nkeys]
+// (every k written exactly once, no atomics)
+__global__ void k_sorted_bounds(const unsigned* key, long long n, long long nkeys, long long* first) {
+   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (j > n) return;
+   const long long lo = j == 0 ? 0 : (long long)key[j - 1] + 1;
+   const long long hi = j == n ? nkeys : (long long)key[j];
+   for (long long k = lo; k <= hi; ++k) first[k] = j;
+}
+// counts from the bounds
+__global__ void k_bounds_counts(const long long* first, long long nkeys, int* cnt) {
+   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (k < nkeys) cnt[k] = (int)(first[k + 1] - first[k]);
 }
 // segment capacity with slack: c + max(32, c/4); entry NS is 0 (for the scan's total)
 __global__ void k_fast_capacity(long long NS, const int* cnt, const int* extra, long long* cap) {
@@ -576,12 +586,20 @@ __global__ void k_fast_relayout(SegBuf from, const long long* fromBase, SegBuf t
    if (threadIdx.x == 0) to.cnt[S] = c;
 }
 // one block per segment: largest |weight|
+// (non-negative doubles order like their bit patterns; one atomic per block)
 __global__ void k_fast_max_abs_w(SegBuf B, const long long* base, unsigned long long* out) {
+   __shared__ double sm[32];
    const long long S = blockIdx.x;
    const int c = B.cnt[S];
    double m = 0.0;
    for (int r = threadIdx.x; r < c; r += blockDim.x) m = fmax(m, fabs(B.a[6][base[S] + r]));
-   if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+   if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sm[w]);
+      if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+   }
 }
 
 }  // namespace rh

@@ -680,20 +680,16 @@ int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* partic
       RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream));
    }
    SegHost& h = c->seg[s];
-   RH_CUDA(cudaMemsetAsync(h.cnt[h.cur], 0, sizeof(int) * NS, c->stream));
-   if (n) {
-      k_fast_histogram<<<blocks1d(n, 256), 256, 0, c->stream>>>(keyOut, n, h.cnt[h.cur]);
-      RH_CUDA(cudaGetLastError());
-   }
+   // first sorted record of every segment and the counts, from the sorted keys
+   k_sorted_bounds<<<blocks1d(n + 1, 256), 256, 0, c->stream>>>(keyOut, n, NS, c->ffirst);
+   k_bounds_counts<<<blocks1d(NS, 256), 256, 0, c->stream>>>(c->ffirst, NS, h.cnt[h.cur]);
+   RH_CUDA(cudaGetLastError());
    long long slots = 0;
    rc = fastLayout(c, h.cnt[h.cur], nullptr, h.base, &slots);
    if (rc) return rc;
    rc = segReserve(h, 0, slots);
    if (rc) return rc;
    rc = segReserve(h, 1, slots);
-   if (rc) return rc;
-   long long tot2 = 0;
-   rc = segPrefix(c, h.cnt[h.cur], &tot2);
    if (rc) return rc;
    if (n) {
       k_fast_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(aos, c->flxTmp, keyOut, idxOut, n, c->ffirst,
@@ -731,7 +727,6 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
    double* aos = (double*)c->staging;
    int* cellCnt = c->outCount;
    const SegHost& h = c->seg[s];
-   RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
    if (tot) {
       k_fast_cell_keys<<<(unsigned)NS, 128, 0, c->stream>>>(c->g, c->fg, segView(h, h.cur), h.base, c->ffirst, keyIn,
                                                            c->fsortSlots);
@@ -743,9 +738,12 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
       if (rc) return rc;
       sb = c->sortTmpBytes;
       RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream));
-      k_fast_histogram<<<blocks1d(tot, 256), 256, 0, c->stream>>>(keyOut, tot, cellCnt);
+      k_sorted_bounds<<<blocks1d(tot + 1, 256), 256, 0, c->stream>>>(keyOut, tot, N, c->ftmpCellStart);
+      k_bounds_counts<<<blocks1d(N, 256), 256, 0, c->stream>>>(c->ftmpCellStart, N, cellCnt);
       k_fast_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(segView(h, h.cur), c->fsortSlots, idxOut, tot, aos);
       RH_CUDA(cudaGetLastError());
+   } else {
+      RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
    }
    RH_CUDA(cudaMemcpyAsync(counts, cellCnt, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
    if (tot && particles) RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
