@@ -112,6 +112,152 @@ __device__ inline double fixedToDouble(unsigned long long lo, unsigned long long
    return __ll2double_rn((long long)hi) * hiScale + __ull2double_rn(lo) * loScale;
 }
 
+// x / dx, correctly rounded, without a division: Markstein's method (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000 processor",
+// IBM J. Res. Dev. 34(1), 1990). With r = RN(1/dx) and q = RN(x r), the residual
+// e = x - q dx is exact in one fused multiply-add and RN(q + e r) = RN(x / dx).
+// The method needs no overflow or underflow on the way: quotients outside
+// [2^-500, 2^500] in magnitude (zeros, NaN and infinities included) take the
+// IEEE division; rhgpu_create keeps dx within [2^-200, 2^200].
+__device__ inline double divDx(double x, const GridInfo& g) {
+   const double q = x * g.rdx;
+   const double aq = fabs(q);
+   if (!(aq >= 0x1p-500 && aq <= 0x1p+500)) return x / g.dx;
+   const double e = fma(-q, g.dx, x);
+   return fma(e, g.rdx, q);
+}
+
+// cicWeights (particle_accumulator.cpp:68-110) with the divisions by dx done by divDx
+__device__ inline void cicWeightsDx(double x, double y, double z, double wq, const GridInfo& g, double w8[8]) {
+   const double dx = g.dx;
+   int i = (int)floor(divDx(x, g)), j = (int)floor(divDx(y, g)), k = (int)floor(divDx(z, g));
+   if (x < (i + 0.5) * dx) { --i; }
+   if (y < (j + 0.5) * dx) { --j; }
+   if (z < (k + 0.5) * dx) { --k; }
+   ++i; ++j; ++k;
+   const double x0 = (i - 1 + 0.5) * dx, y0 = (j - 1 + 0.5) * dx, z0 = (k - 1 + 0.5) * dx;
+   const double w_x = divDx(x - x0, g), w_y = divDx(y - y0, g), w_z = divDx(z - z0, g);
+   w8[0] = (1 - w_x) * (1 - w_y) * (1 - w_z) * wq;
+   w8[1] = w_x * (1 - w_y) * (1 - w_z) * wq;
+   w8[2] = (1 - w_x) * w_y * (1 - w_z) * wq;
+   w8[3] = w_x * w_y * (1 - w_z) * wq;
+   w8[4] = (1 - w_x) * (1 - w_y) * w_z * wq;
+   w8[5] = w_x * (1 - w_y) * w_z * wq;
+   w8[6] = (1 - w_x) * w_y * w_z * wq;
+   w8[7] = w_x * w_y * w_z * wq;
+}
+
+// the field stencil of one segment's cells in shared memory: local cell
+// (lc, ly, lz) = global (xs0 + lc, ys0 + ly, zs0 + lz), lc in [0, SEG],
+// ly, lz in {0, 1}; faceB also holds the -x / -y / -z neighbour faces
+struct SegFields {
+   double bx[2][2][SEG + 2];    // [lz][ly][lc + 1]
+   double by[2][3][SEG + 1];    // [lz][ly + 1][lc]
+   double bz[3][2][SEG + 1];    // [lz + 1][ly][lc]
+   double ue[3][2][2][SEG + 1]; // [l][lz][ly][lc]
+   double ep[3][2][2][SEG + 1];
+};
+constexpr int SF_BX = 2 * 2 * (SEG + 2), SF_BY = 2 * 3 * (SEG + 1), SF_BZ = 3 * 2 * (SEG + 1);
+constexpr int SF_UE = 3 * 2 * 2 * (SEG + 1);
+
+// one global value of the stencil, 0 outside a non-periodic box (never read there:
+// the push accelerates only particles of cells with all neighbours)
+__device__ inline double stencilLoad(const GridInfo& g, const double* a, int l, int x, int y, int z) {
+   if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
+   if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
+   if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
+   if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) return 0.0;
+   return a[(long long)l * g.N + cidx(g, x, y, z)];
+}
+
+__device__ inline void stageSegFields(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
+                                      SegFields& F) {
+   const int total = SF_BX + SF_BY + SF_BZ + SF_UE * (useEp ? 2 : 1);
+   for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int r = e;
+      if (r < SF_BX) {
+         const int lc = r % (SEG + 2) - 1, ly = (r / (SEG + 2)) % 2, lz = r / (2 * (SEG + 2));
+         F.bx[lz][ly][lc + 1] = stencilLoad(g, f.faceB, 0, xs0 + lc, ys0 + ly, zs0 + lz);
+         continue;
+      }
+      r -= SF_BX;
+      if (r < SF_BY) {
+         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 3 - 1, lz = r / (3 * (SEG + 1));
+         F.by[lz][ly + 1][lc] = stencilLoad(g, f.faceB, 1, xs0 + lc, ys0 + ly, zs0 + lz);
+         continue;
+      }
+      r -= SF_BY;
+      if (r < SF_BZ) {
+         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = r / (2 * (SEG + 1)) - 1;
+         F.bz[lz + 1][ly][lc] = stencilLoad(g, f.faceB, 2, xs0 + lc, ys0 + ly, zs0 + lz);
+         continue;
+      }
+      r -= SF_BZ;
+      const bool ep = r >= SF_UE;
+      if (ep) r -= SF_UE;
+      const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = (r / (2 * (SEG + 1))) % 2, l = r / (4 * (SEG + 1));
+      if (ep) F.ep[l][lz][ly][lc] = stencilLoad(g, f.cellEp, l, xs0 + lc, ys0 + ly, zs0 + lz);
+      else F.ue[l][lz][ly][lc] = stencilLoad(g, f.cellUe, l, xs0 + lc, ys0 + ly, zs0 + lz);
+   }
+}
+
+// pushOne with the fields from the segment's staged stencil and divDx; the
+// same arithmetic in the same order
+__device__ inline bool pushStaged(const GridInfo& g, const SegFields& F, const SpeciesDev& sp, const PushParams& pp,
+                                  int i, int j, int k, int lc, int ly, int lz, double st[7]) {
+   bool clamp = false;
+   const bool accelerate = sp.accelerate && !pp.useIFT && allNb(g, i, j, k);
+   double vx = st[3], vy = st[4], vz = st[5];
+   if (accelerate) {
+      const double dx = g.dx;
+      double B[3], Ue[3], E[3];
+      const double xs = divDx(st[0], g), ys = divDx(st[1], g), zs = divDx(st[2], g);
+      B[0] = (xs - 0.0) * F.bx[lz][ly][lc + 1] + (1.0 - xs) * F.bx[lz][ly][lc];
+      B[1] = (ys - 0.0) * F.by[lz][ly + 1][lc] + (1.0 - ys) * F.by[lz][ly][lc];
+      B[2] = (zs - 0.0) * F.bz[lz + 1][ly][lc] + (1.0 - zs) * F.bz[lz][ly][lc];
+      for (int l = 0; l < 3; ++l) Ue[l] = F.ue[l][lz][ly][lc];
+      E[0] = B[1] * Ue[2] - B[2] * Ue[1];
+      E[1] = B[2] * Ue[0] - B[0] * Ue[2];
+      E[2] = B[0] * Ue[1] - B[1] * Ue[0];
+      if (pp.use_ep) for (int l = 0; l < 3; ++l) E[l] += F.ep[l][lz][ly][lc];
+      const double qm = sp.qmideltT2;
+      const double dvx = qm * E[0], dvy = qm * E[1], dvz = qm * E[2];
+      const double tx = qm * B[0], ty = qm * B[1], tz = qm * B[2];
+      const double t2 = tx * tx + ty * ty + tz * tz;
+      const double b2 = 2. / (1. + t2);
+      const double sx = b2 * tx, sy = b2 * ty, sz = b2 * tz;
+      const double vmx = vx + dvx, vmy = vy + dvy, vmz = vz + dvz;
+      const double v0x = vmx + vmy * tz - vmz * ty;
+      const double v0y = vmy + vmz * tx - vmx * tz;
+      const double v0z = vmz + vmx * ty - vmy * tx;
+      const double vpx = vmx + v0y * sz - v0z * sy;
+      const double vpy = vmy + v0z * sx - v0x * sz;
+      const double vpz = vmz + v0x * sy - v0y * sx;
+      vx = vpx + dvx; vy = vpy + dvy; vz = vpz + dvz;
+      if (pp.use_gravity) {
+         const double xg = st[0] + blockOrigin(g.x_min, i, dx), yg = st[1] + blockOrigin(g.y_min, j, dx),
+                      zg = st[2] + blockOrigin(g.z_min, k, dx);
+         const double rr = sqrt(sq(xg) + sq(yg) + sq(zg));
+         const double r3 = rr * rr * rr;
+         if (r3 > 0) {
+            const double s = -pp.GMdt / r3;
+            vx += s * xg; vy += s * yg; vz += s * zg;
+         }
+      }
+      const double v2 = sq(vx) + sq(vy) + sq(vz);
+      if (v2 > pp.maxVi2) {
+         const double norm = sqrt(pp.maxVi2 / v2);
+         vx *= norm; vy *= norm; vz *= norm;
+         clamp = true;
+      }
+   }
+   st[3] = vx; st[4] = vy; st[5] = vz;
+   st[0] += g.dt * vx;
+   st[1] += g.dt * vy;
+   st[2] += g.dt * vz;
+   return clamp;
+}
+
 // push of one particle at local position st[0..2] in cell (i,j,k); returns true if clamped
 __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const SpeciesDev& sp, const PushParams& pp,
                                int i, int j, int k, double st[7]) {
@@ -180,6 +326,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ int s_first[FAST_MAX_SPECIES];
+   __shared__ SegFields s_f;
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -199,6 +346,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       s_prefix[ns] = a;
    }
    if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
+   stageSegFields(g, f, pp.use_ep, dualB(u0, g.per[0]), dualB(uy, g.per[1]), dualB(uz, g.per[2]), s_f);
    __syncthreads();
    const int total = s_prefix[ns];
    const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
@@ -221,14 +369,15 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          p = i - s_prefix[s];
          const long long slot = SS.base[S] + p;
          for (int a = 0; a < 7; ++a) st[a] = SS.cur.a[a][slot];
-         const int u = u0 + SS.cur.lx[slot];
-         int ci = dualB(u, g.per[0]) + 1 - halfS(st[0], dx);
-         int cj = dualB(uy, g.per[1]) + 1 - halfS(st[1], dx);
-         int ck = dualB(uz, g.per[2]) + 1 - halfS(st[2], dx);
+         const int lu = SS.cur.lx[slot];
+         const int lc = lu + 1 - halfS(st[0], dx), ly = 1 - halfS(st[1], dx), lz = 1 - halfS(st[2], dx);
+         int ci = dualB(u0 + lu, g.per[0]) + 1 - halfS(st[0], dx);
+         int cj = dualB(uy, g.per[1]) + ly;
+         int ck = dualB(uz, g.per[2]) + lz;
          if (ci >= g.nx) ci -= g.nx;   // periodic axes: dual cell 0 holds the upper half of the last cell
          if (cj >= g.ny) cj -= g.ny;
          if (ck >= g.nz) ck -= g.nz;
-         clamp = pushOne(g, f, FS.sp[s], pp, ci, cj, ck, st);
+         clamp = pushStaged(g, s_f, FS.sp[s], pp, ci, cj, ck, lc, ly, lz, st);
          if (isnan(st[0]) || isnan(st[1]) || isnan(st[2])) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
          int ox, oy, oz;
          int bad = migrateAxis(st[0], ox, dx, g.dx_below);
@@ -247,8 +396,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.sp[s].accumulate) {
                if (inSeg) {
-                  int ind[8];
-                  cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, dx, w8, ind);
+                  cicWeightsDx(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
                   rec = true;
                } else {
                   mflags |= MOVER_DEPOSIT;   // deposited by k_fast_mover_deposit
@@ -412,8 +560,7 @@ __global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, Fa
    double st[7];
    for (int a = 0; a < 7; ++a) st[a] = M.s[a];
    double w8[8];
-   int ind[8];
-   cicWeights(st[0], st[1], st[2], st[6] * FS.sp[s].q, g.dx, w8, ind);
+   cicWeightsDx(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
    const long long N = g.N;
    for (int o = 0; o < 8; ++o) {
       int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);

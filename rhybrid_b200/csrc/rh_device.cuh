@@ -19,6 +19,7 @@ struct GridInfo {
    int per[3];
    long long N;
    double dx, dt, dV, dx_below;
+   double rdx;   // 1/dx, correctly rounded
    double x_min, y_min, z_min;
 };
 

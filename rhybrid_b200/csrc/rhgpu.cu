@@ -848,6 +848,8 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    if (params->nx < 3 || params->ny < 3 || params->nz < 3) return fail(RHGPU_ERR_ARG, "rhgpu_create: at least 3 cells per axis");
    const long long N = (long long)params->nx * params->ny * params->nz;
    if (N * 27 >= (1LL << 31)) return fail(RHGPU_ERR_ARG, "rhgpu_create: grid too large (27*cells must fit int32)");
+   if (!(params->dx >= std::ldexp(1.0, -200) && params->dx <= std::ldexp(1.0, 200)) || !(params->dt > 0))
+      return fail(RHGPU_ERR_ARG, "rhgpu_create: dx must lie in [2^-200, 2^200] and dt must be positive");
    RH_CUDA(cudaSetDevice(device));
    rhgpu_ctx* c = new rhgpu_ctx();
    c->P = *params;
@@ -862,6 +864,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    g.dt = params->dt;
    g.dV = params->dx * params->dx * params->dx;
    g.dx_below = std::nextafter(params->dx, 0.0);
+   g.rdx = 1.0 / params->dx;   // correctly rounded reciprocal, for divDx
    g.x_min = params->x_min; g.y_min = params->y_min; g.z_min = params->z_min;
    c->t = params->t_initial;
    c->useIFT = params->use_initial_flow_through;
