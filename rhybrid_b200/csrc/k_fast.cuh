@@ -45,6 +45,7 @@ constexpr int SEG = RHGPU_FAST_SEGMENT;   // dual cells per segment
 constexpr int FT = 256;                   // threads of k_fast_push_deposit (one chunk of particles)
 constexpr int FW = FT / 32;
 constexpr int REC = 11;                   // doubles per deposit record: w8[8], v[3]
+constexpr int FAST_DYN_SMEM = 7 * FT * sizeof(double);   // dynamic shared memory of k_fast_push_deposit
 static_assert(SEG == 32 && SEG * 8 == FT, "the deposit sums map (dual cell, corner) to one thread");
 
 struct SegBuf {
@@ -156,6 +157,7 @@ struct SegFields {
    double bz[3][2][SEG + 1];    // [lz + 1][ly][lc]
    double ue[3][2][2][SEG + 1]; // [l][lz][ly][lc]
    double ep[3][2][2][SEG + 1];
+   unsigned char fl[4][4][SEG + 3];   // cell flags [lz + 1][ly + 1][lc + 1], lc in [-1, SEG + 1]
 };
 constexpr int SF_BX = 2 * 2 * (SEG + 2), SF_BY = 2 * 3 * (SEG + 1), SF_BZ = 3 * 2 * (SEG + 1);
 constexpr int SF_UE = 3 * 2 * 2 * (SEG + 1);
@@ -172,6 +174,15 @@ __device__ inline double stencilLoad(const GridInfo& g, const double* a, int l, 
 
 __device__ inline void stageSegFields(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
                                       SegFields& F) {
+   for (int e = threadIdx.x; e < 4 * 4 * (SEG + 3); e += blockDim.x) {
+      const int lc = e % (SEG + 3) - 1, ly = (e / (SEG + 3)) % 4 - 1, lz = e / (4 * (SEG + 3)) - 1;
+      int x = xs0 + lc, y = ys0 + ly, z = zs0 + lz;
+      if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
+      if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
+      if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
+      const bool in = x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+      F.fl[lz + 1][ly + 1][lc + 1] = in ? f.flags[cidx(g, x, y, z)] : (unsigned char)0;
+   }
    const int total = SF_BX + SF_BY + SF_BZ + SF_UE * (useEp ? 2 : 1);
    for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int r = e;
@@ -327,6 +338,8 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ int s_first[FAST_MAX_SPECIES];
    __shared__ SegFields s_f;
+   extern __shared__ double s_dyn[];               // FAST_DYN_SMEM bytes
+   double (*s_pf)[FT] = reinterpret_cast<double (*)[FT]>(s_dyn);   // the next chunk's particles (cp.async prefetch)
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -352,24 +365,50 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 
+   // each thread copies its own particle of the next chunk into s_pf[.][tid]
+   // (asynchronous, 8 bytes per array) and reads it back after waiting for its
+   // own copies, so no barrier guards the prefetch buffer; the copies into a
+   // slot are issued only after the values read from it have arrived (dep)
+   int nS = 0, nLu = 0;
+   long long nP = 0;
+   auto prefetch = [&](int i, unsigned long long dep) {
+      asm volatile("" ::"l"(dep) : "memory");
+      if (i < total) {
+         int sp = 0;
+         while (sp + 1 < ns && i >= s_prefix[sp + 1]) ++sp;
+         const SegSpecies& SS = FS.st[sp];
+         nS = sp;
+         nP = i - s_prefix[sp];
+         const long long slot = SS.base[S] + nP;
+         for (int a = 0; a < 7; ++a) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(&s_pf[a][tid]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(SS.cur.a[a] + slot) : "memory");
+         }
+         nLu = SS.cur.lx[slot];
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+   };
+   prefetch(tid, 0ull);
+
    for (int c0 = 0; c0 < total; c0 += FT) {
       const int i = c0 + tid;
       const bool active = i < total;
-      int s = 0;
-      if (active)
-         while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       double st[7];
+      unsigned long long dep = 0;
+      for (int a = 0; a < 7; ++a) {
+         st[a] = s_pf[a][tid];
+         dep |= (unsigned long long)__double_as_longlong(st[a]);
+      }
+      const int s = active ? nS : 0;
+      const long long p = nP;
+      const int lu = nLu;
+      prefetch(i + FT, dep);
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0;
       int vx = 0, vy = 0, vz = 0;
       double w8[8];
-      long long p = 0;
       if (active) {
-         const SegSpecies& SS = FS.st[s];
-         p = i - s_prefix[s];
-         const long long slot = SS.base[S] + p;
-         for (int a = 0; a < 7; ++a) st[a] = SS.cur.a[a][slot];
-         const int lu = SS.cur.lx[slot];
          const int lc = lu + 1 - halfS(st[0], dx), ly = 1 - halfS(st[1], dx), lz = 1 - halfS(st[2], dx);
          int ci = dualB(u0 + lu, g.per[0]) + 1 - halfS(st[0], dx);
          int cj = dualB(uy, g.per[1]) + ly;
@@ -403,13 +442,12 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
                }
             }
             // boundary conditions of the step
-            const long long cn = cidx(g, ti, tj, tk);
             bool removed = false;
             if (!allNb(g, ti, tj, tk)) {
                removed = true;
                atomicAdd(&cntd[4 * s + 0], st[6]);
                atomicAdd(&cntd[4 * s + 1], ke);
-            } else if (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
+            } else if (s_f.fl[lz + oz + 1][ly + oy + 1][lc + ox + 1] & RHGPU_FLAG_INNER_PARTICLE) {
                const double xp = blockOrigin(g.x_min, ti, dx) + st[0];
                const double yp = blockOrigin(g.y_min, tj, dx) + st[1];
                const double zp = blockOrigin(g.z_min, tk, dx) + st[2];
