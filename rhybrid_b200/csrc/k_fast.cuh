@@ -45,7 +45,6 @@ constexpr int SEG = RHGPU_FAST_SEGMENT;   // dual cells per segment
 constexpr int FT = 256;                   // threads of k_fast_push_deposit (one chunk of particles)
 constexpr int FW = FT / 32;
 constexpr int REC = 11;                   // doubles per deposit record: w8[8], v[3]
-constexpr int FAST_DYN_SMEM = 7 * FT * sizeof(double);   // dynamic shared memory of k_fast_push_deposit
 static_assert(SEG == 32 && SEG * 8 == FT, "the deposit sums map (dual cell, corner) to one thread");
 
 struct SegBuf {
@@ -157,7 +156,6 @@ struct SegFields {
    double bz[3][2][SEG + 1];    // [lz + 1][ly][lc]
    double ue[3][2][2][SEG + 1]; // [l][lz][ly][lc]
    double ep[3][2][2][SEG + 1];
-   unsigned char fl[4][4][SEG + 3];   // cell flags [lz + 1][ly + 1][lc + 1], lc in [-1, SEG + 1]
 };
 constexpr int SF_BX = 2 * 2 * (SEG + 2), SF_BY = 2 * 3 * (SEG + 1), SF_BZ = 3 * 2 * (SEG + 1);
 constexpr int SF_UE = 3 * 2 * 2 * (SEG + 1);
@@ -174,15 +172,6 @@ __device__ inline double stencilLoad(const GridInfo& g, const double* a, int l, 
 
 __device__ inline void stageSegFields(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
                                       SegFields& F) {
-   for (int e = threadIdx.x; e < 4 * 4 * (SEG + 3); e += blockDim.x) {
-      const int lc = e % (SEG + 3) - 1, ly = (e / (SEG + 3)) % 4 - 1, lz = e / (4 * (SEG + 3)) - 1;
-      int x = xs0 + lc, y = ys0 + ly, z = zs0 + lz;
-      if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
-      if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
-      if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
-      const bool in = x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
-      F.fl[lz + 1][ly + 1][lc + 1] = in ? f.flags[cidx(g, x, y, z)] : (unsigned char)0;
-   }
    const int total = SF_BX + SF_BY + SF_BZ + SF_UE * (useEp ? 2 : 1);
    for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int r = e;
@@ -336,10 +325,8 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    __shared__ int s_wcnt[FW];                     // stayers | records << 16 per warp
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
-   __shared__ int s_first[FAST_MAX_SPECIES];
+   __shared__ unsigned s_bs[FW];                  // stayer ballot of each warp
    __shared__ SegFields s_f;
-   extern __shared__ double s_dyn[];               // FAST_DYN_SMEM bytes
-   double (*s_pf)[FT] = reinterpret_cast<double (*)[FT]>(s_dyn);   // the next chunk's particles (cp.async prefetch)
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -365,50 +352,24 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 
-   // each thread copies its own particle of the next chunk into s_pf[.][tid]
-   // (asynchronous, 8 bytes per array) and reads it back after waiting for its
-   // own copies, so no barrier guards the prefetch buffer; the copies into a
-   // slot are issued only after the values read from it have arrived (dep)
-   int nS = 0, nLu = 0;
-   long long nP = 0;
-   auto prefetch = [&](int i, unsigned long long dep) {
-      asm volatile("" ::"l"(dep) : "memory");
-      if (i < total) {
-         int sp = 0;
-         while (sp + 1 < ns && i >= s_prefix[sp + 1]) ++sp;
-         const SegSpecies& SS = FS.st[sp];
-         nS = sp;
-         nP = i - s_prefix[sp];
-         const long long slot = SS.base[S] + nP;
-         for (int a = 0; a < 7; ++a) {
-            const unsigned d = (unsigned)__cvta_generic_to_shared(&s_pf[a][tid]);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(SS.cur.a[a] + slot) : "memory");
-         }
-         nLu = SS.cur.lx[slot];
-      }
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-   };
-   prefetch(tid, 0ull);
-
    for (int c0 = 0; c0 < total; c0 += FT) {
       const int i = c0 + tid;
       const bool active = i < total;
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      int s = 0;
+      if (active)
+         while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
       double st[7];
-      unsigned long long dep = 0;
-      for (int a = 0; a < 7; ++a) {
-         st[a] = s_pf[a][tid];
-         dep |= (unsigned long long)__double_as_longlong(st[a]);
-      }
-      const int s = active ? nS : 0;
-      const long long p = nP;
-      const int lu = nLu;
-      prefetch(i + FT, dep);
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0;
       int vx = 0, vy = 0, vz = 0;
       double w8[8];
+      long long p = 0;
       if (active) {
+         const SegSpecies& SS = FS.st[s];
+         p = i - s_prefix[s];
+         const long long slot = SS.base[S] + p;
+         for (int a = 0; a < 7; ++a) st[a] = SS.cur.a[a][slot];
+         const int lu = SS.cur.lx[slot];
          const int lc = lu + 1 - halfS(st[0], dx), ly = 1 - halfS(st[1], dx), lz = 1 - halfS(st[2], dx);
          int ci = dualB(u0 + lu, g.per[0]) + 1 - halfS(st[0], dx);
          int cj = dualB(uy, g.per[1]) + ly;
@@ -442,12 +403,13 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
                }
             }
             // boundary conditions of the step
+            const long long cn = cidx(g, ti, tj, tk);
             bool removed = false;
             if (!allNb(g, ti, tj, tk)) {
                removed = true;
                atomicAdd(&cntd[4 * s + 0], st[6]);
                atomicAdd(&cntd[4 * s + 1], ke);
-            } else if (s_f.fl[lz + oz + 1][ly + oy + 1][lc + ox + 1] & RHGPU_FLAG_INNER_PARTICLE) {
+            } else if (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
                const double xp = blockOrigin(g.x_min, ti, dx) + st[0];
                const double yp = blockOrigin(g.y_min, tj, dx) + st[1];
                const double zp = blockOrigin(g.z_min, tk, dx) + st[2];
@@ -466,16 +428,15 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       }
       if (clamp) atomicAdd(&cntu[CNT_SPECIES_MAXVI + s], 1ull);
 
-      // ---- order of the chunk's stayers and records: warp ballots + per-warp totals -----
+      // ---- order of the chunk's stayers and records --------------------------------------
+      // warp-local first: stayer/record ballots and the records per (warp, dual cell)
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
-      if (lane == 0) s_wcnt[warp] = __popc(bs) | (__popc(br) << 16);
+      if (lane == 0) {
+         s_wcnt[warp] = __popc(bs) | (__popc(br) << 16);
+         s_bs[warp] = bs;
+      }
       s_wd[warp][lane] = 0;
-      __syncthreads();
-      int before = 0;
-      for (int w = 0; w < warp; ++w) before += s_wcnt[w];
-      const int stayIdx = (before & 0xffff) + __popc(bs & below);
-      if (active && i == max(s_prefix[s], c0)) s_first[s] = stayIdx;
-      // records per (warp, dual cell) and the rank within the warp
+      __syncwarp();
       const int rd = rec ? vx - u0 : 0;
       int rrank = 0;
       if (rec) {
@@ -484,9 +445,19 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          if (rrank == 0) s_wd[warp][rd] = __popc(mm);
       }
       __syncthreads();
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += s_wcnt[w];
+      const int stayIdx = (before & 0xffff) + __popc(bs & below);
+      // stayers of the chunk before the first particle of this thread's species
+      int firstIdx = 0;
+      if (stay || (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1))) {
+         const int P0 = max(s_prefix[s], c0) - c0;
+         for (int w = 0; w < (P0 >> 5); ++w) firstIdx += __popc(s_bs[w]);
+         firstIdx += __popc(s_bs[P0 >> 5] & ((1u << (P0 & 31)) - 1u));
+      }
       if (stay) {
          const SegSpecies& SS = FS.st[s];
-         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - s_first[s]);
+         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
          for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
          SS.nxt.lx[slot] = (unsigned char)(vx - u0);
       }
@@ -527,7 +498,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       }
       __syncthreads();
       // running stayer count of each species: the chunk's last thread of the species adds
-      if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - s_first[s];
+      if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - firstIdx;
       if (rec) {
          int pos = s_bin[rd] + rrank;
          for (int w = 0; w < warp; ++w) pos += s_wd[w][rd];
@@ -548,10 +519,12 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             a3 += w * rr[10];
          }
       }
-      __syncthreads();
+      // no barrier here: the next chunk's first barrier orders these reads before
+      // its record writes
    }
 
    // ---- outputs: stayer counts, row partials, segment-boundary partial ---------------------
+   __syncthreads();
    if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
    {
       double* q = s_rec + myDual * 32 + myCorner * 4;

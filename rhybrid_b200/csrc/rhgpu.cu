@@ -767,7 +767,7 @@ int fastPush(rhgpu_ctx* c) {
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "fast_push_deposit");
-      k_fast_push_deposit<<<(unsigned)NS, FT, FAST_DYN_SMEM, c->stream>>>(c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD,
+      k_fast_push_deposit<<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD,
                                                              c->cntU, c->err);
       RH_LAUNCHED(c);
    }
@@ -962,8 +962,6 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
             rc = fail(RHGPU_ERR_CUDA, "copy exterior list");
       }
    }
-   if (!rc && cudaFuncSetAttribute(k_fast_push_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, FAST_DYN_SMEM) != cudaSuccess)
-      rc = fail(RHGPU_ERR_CUDA, "create: shared memory size of the fast kernel");
    if (!rc) {
       NeumannTables t = buildNeumannTables();
       if (cudaMemcpyToSymbol(c_neu, &t, sizeof t) != cudaSuccess) rc = fail(RHGPU_ERR_CUDA, "neumann tables");
