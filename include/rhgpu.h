@@ -244,11 +244,18 @@ int rhgpu_get_counters(rhgpu_ctx* ctx, double* out, int32_t n);
 /* Current simulation time and time-step number (Simulation::t, ::timestep). */
 int rhgpu_get_time(rhgpu_ctx* ctx, double* t_out, int64_t* timestep_out);
 
-/* Device-side FP64 reductions for the field and population logs
- * (diagnostics.h:187-404): out[0..] = per species {sum w, sum w*vx, sum w*vy,
- * sum w*vz, sum w*v^2, N macroparticles}, then field {sum faceB^2 over
- * non-exterior cells, max |cellB|, sum cellRhoQi, max cellRhoQi}. Length
- * 6*n_species + 4. */
+/* Device-side FP64 reductions of the population and field logs
+ * (logCalcParticle / logCalcField, diagnostics.h:187-404), n >= 8*n_species + 30:
+ * out[8*s + 0..7] per species s: N macroparticles, sum w, sum w*vx, sum w*vy,
+ *   sum w*vz, sum w*|v|, sum w*v^2, max |v|;
+ * then 30 field values over the cells with all neighbours outside the inner
+ * field boundary (the reference's default, includeInnerCellsInFieldLog = false):
+ *   N cells, sum Bx, By, Bz, |B|, max |B|, sum |divB|, max |divB|, max |divB|/|B|,
+ *   sum B^2 (cell B = mean of its two faces); sum Jix, Jiy, Jiz, |Ji|, max |Ji|;
+ *   sum Epx, Epy, Epz, |Ep|, max |Ep|, sum Ep^2; sum nodeEx, Ey, Ez, |E|, max |E|,
+ *   sum E^2; sum |Ue x B|^2; max |Ue|; sum cellRhoQi.
+ * Sums are formed per block in a fixed tree and added on the host in block
+ * order: deterministic, equal to the reference's sequential sums to round-off. */
 int rhgpu_reduce_diagnostics(rhgpu_ctx* ctx, double* out, int32_t n);
 
 /* The CUDA stream (cudaStream_t) the context enqueues on. */

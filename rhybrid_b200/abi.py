@@ -48,6 +48,14 @@ FIELD_COUNTERS = [
 SPECIES_COUNTERS = ["particleMaxVi", "particleEscape", "particleEscapeKineticEnergy",
                     "particleImpact", "particleImpactKineticEnergy"]
 
+# rhgpu.h: rhgpu_reduce_diagnostics layout
+DIAG_PARTICLE = ["N_macroParticles", "N_realParticles", "sumVx", "sumVy", "sumVz", "sumV", "sumWV2", "maxVi"]
+DIAG_FIELD = ["N_cells", "sumBx", "sumBy", "sumBz", "sumB", "maxB", "sumDivB", "maxDivB", "maxDivBPerB", "sumB2",
+              "sumCellJix", "sumCellJiy", "sumCellJiz", "sumCellJi", "maxCellJi",
+              "sumCellEpx", "sumCellEpy", "sumCellEpz", "sumCellEp", "maxCellEp", "sumCellEp2",
+              "sumNodeEx", "sumNodeEy", "sumNodeEz", "sumNodeE", "maxNodeE", "sumNodeE2",
+              "sumCellE2", "maxUe", "sumCellRhoQi"]
+
 # rhgpu.h: physical constants
 PERMEABILITY = 1.2566370614359173e-06
 CHARGE_ELEMENTARY = 1.602176634e-19
@@ -285,11 +293,13 @@ class Context:
         self.lib.call("device_errors", self.h, C.byref(w))
         return w.value
 
-    def reduce_diagnostics(self) -> np.ndarray:
-        n = 6 * self.nspecies + 4
+    def reduce_diagnostics(self) -> dict:
+        """rhgpu_reduce_diagnostics: the population log per species and the field log."""
+        n = 8 * self.nspecies + 30
         out = np.zeros(n, dtype=np.float64)
         self.lib.call("reduce_diagnostics", self.h, _ptr(out, C.c_double), n)
-        return out
+        pops = [dict(zip(DIAG_PARTICLE, out[8 * s:8 * s + 8])) for s in range(self.nspecies)]
+        return {"populations": pops, "field": dict(zip(DIAG_FIELD, out[8 * self.nspecies:]))}
 
     def set_timing(self, on: bool):
         self.lib.call("set_timing", self.h, 1 if on else 0)

@@ -18,6 +18,7 @@
 #include "k_fields.cuh"
 #include "k_particles.cuh"
 #include "k_fast.cuh"
+#include "k_diag.cuh"
 
 using namespace rh;
 
@@ -196,6 +197,7 @@ struct rhgpu_ctx {
    unsigned char* flxTmp = nullptr;
    long long flxTmpCap = 0;
    long long capHint[MAX_SPECIES] = {};
+   double* diagPart = nullptr;          // DIAG_BLOCKS x DIAG_F partial rows of rhgpu_reduce_diagnostics
 };
 
 namespace {
@@ -932,6 +934,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->ftmpInc64, sizeof(long long) * (nb + 1));
    alloc((void**)&c->foffInc, sizeof(long long) * (nb + 1));
    alloc((void**)&c->fover, sizeof(unsigned long long));
+   alloc((void**)&c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_F);
    if (!rc) {
       // MM starts at zero; k_fast_gather clears what a step touched
       if (cudaMemset(c->fb.MMlo, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
@@ -1009,6 +1012,7 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->finc); cudaFree(c->ffill); cudaFree(c->fbucket); cudaFree(c->fover);
    cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
    cudaFree(c->ftmpInc64); cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots); cudaFree(c->flxTmp);
+   cudaFree(c->diagPart);
    for (int s = 0; s < c->ns; ++s) { freeStore(c->ps[s]); freeStore(c->alt[s]); }
    for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
    if (c->stream) cudaStreamDestroy(c->stream);
@@ -1363,9 +1367,53 @@ int rhgpu_last_launch_count(rhgpu_ctx* c, int64_t* out) {
    return RHGPU_OK;
 }
 
+namespace {
+// adds the DIAG_BLOCKS partial rows of width w in block order (sums, or maxima where maxMask has the bit)
+void diagCombine(const std::vector<double>& h, int w, unsigned long long maxMask, double* out) {
+   for (int q = 0; q < w; ++q) {
+      double a = 0.0;
+      for (int b = 0; b < DIAG_BLOCKS; ++b) {
+         const double x = h[(size_t)b * w + q];
+         a = ((maxMask >> q) & 1ull) ? std::max(a, x) : a + x;
+      }
+      out[q] = a;
+   }
+}
+}  // namespace
+
 int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
    if (!c || !out) return fail(RHGPU_ERR_ARG, "bad arguments");
-   return fail(RHGPU_ERR_STATE, "reduce_diagnostics: not available in this build");
+   if (n < DIAG_P * c->ns + DIAG_F) return fail(RHGPU_ERR_ARG, "reduce_diagnostics: out needs 8*n_species + 30 doubles");
+   RH_CUDA(cudaSetDevice(c->device));
+   std::vector<double> h((size_t)DIAG_BLOCKS * DIAG_F);
+   for (int s = 0; s < c->ns; ++s) {
+      double* o = out + DIAG_P * s;
+      bool launched = false;
+      if (c->path == RHGPU_PATH_FAST) {
+         const SegHost& sh = c->seg[s];
+         if (sh.a[sh.cur][0]) {
+            k_diag_particles_seg<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(segView(sh, sh.cur), sh.base, c->fg.NS, c->diagPart);
+            launched = true;
+         }
+      } else if (c->ps[s].start) {
+         k_diag_particles_cell<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(c->ps[s], c->g.N, c->diagPart);
+         launched = true;
+      }
+      if (!launched) {
+         for (int q = 0; q < DIAG_P; ++q) o[q] = 0.0;
+         continue;
+      }
+      RH_CUDA(cudaGetLastError());
+      RH_CUDA(cudaMemcpyAsync(h.data(), c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_P, cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      diagCombine(h, DIAG_P, DIAG_P_MAX, o);
+   }
+   k_diag_field<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(c->g, c->f, c->diagPart);
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaMemcpyAsync(h.data(), c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_F, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   diagCombine(h, DIAG_F, DIAG_F_MAX, out + DIAG_P * c->ns);
+   return RHGPU_OK;
 }
 
 }  // extern "C"
