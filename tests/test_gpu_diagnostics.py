@@ -61,7 +61,7 @@ def expected(ctx, cfg):
 def check(got, want, what, scale_of):
     for k, w in want.items():
         v = got[k]
-        if k.startswith("max") or k.startswith("N_"):
+        if k.startswith("max") or k in ("N_macroParticles", "N_cells"):
             assert v == pytest.approx(w, rel=1e-15, abs=0.0), f"{what} {k}: {v} vs {w}"
         else:
             assert abs(v - w) <= 1e-12 * scale_of(k), f"{what} {k}: {v} vs {w}"
