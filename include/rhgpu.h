@@ -175,9 +175,17 @@ int rhgpu_destroy(rhgpu_ctx* ctx);
  *                   to round-off); the segment length fixes that order;
  *  RHGPU_PATH_EXACT particles grouped by cell and deposited in the reference's
  *                   summation order: bitwise identical to the reference's CPU
- *                   results, at a lower speed. */
+ *                   results, at a lower speed;
+ *  RHGPU_PATH_FP32  the precision form: particles stored as an int32 cell
+ *                   index, FP32 offsets in the cell and FP32 velocities (one
+ *                   macroparticle weight per species, checked at upload),
+ *                   pushed and deposited in FP32 with FP32 accumulation; the
+ *                   field update, the moments handed to it and the diagnostic
+ *                   sums stay FP64. Its error against the FP64 paths is
+ *                   measured, not bounded. */
 #define RHGPU_PATH_FAST  0
 #define RHGPU_PATH_EXACT 1
+#define RHGPU_PATH_FP32  2
 #define RHGPU_FAST_SEGMENT 32
 int rhgpu_set_path(rhgpu_ctx* ctx, int32_t path);
 

@@ -17,6 +17,7 @@ import numpy as np
 # rhgpu.h: particle paths
 PATH_FAST = 0
 PATH_EXACT = 1
+PATH_FP32 = 2
 
 # rhgpu.h: status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_DEVICE, ERR_NOMEM, ERR_CAPACITY = range(7)

@@ -617,12 +617,14 @@ __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, do
 }
 
 // ---- mover placement ------------------------------------------------------------------------
-__global__ void k_fast_mig_count(const Mover* mv, long long n, long long NS, int* inc) {
+template <class MV>
+__global__ void k_fast_mig_count(const MV* mv, long long n, long long NS, int* inc) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    atomicAdd(&inc[(long long)mv[t].species * NS + mv[t].dest], 1);
 }
-__global__ void k_fast_mig_bucket(const Mover* mv, long long n, long long NS, const long long* off, int* fill, int* bucket) {
+template <class MV>
+__global__ void k_fast_mig_bucket(const MV* mv, long long n, long long NS, const long long* off, int* fill, int* bucket) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    const long long b = (long long)mv[t].species * NS + mv[t].dest;

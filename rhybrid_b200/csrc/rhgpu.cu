@@ -19,6 +19,7 @@
 #include "k_particles.cuh"
 #include "k_fast.cuh"
 #include "k_diag.cuh"
+#include "k_f32.cuh"
 
 using namespace rh;
 
@@ -115,6 +116,19 @@ __device__ __align__(256) double g_noallocScratch[108 * (size_t)RHGPU_NOALLOC_MA
 constexpr int NOALLOC_MAX_DEVICES = 64;
 double* g_noallocPtr[NOALLOC_MAX_DEVICES] = {};
 
+// one species' FP32-form storage: cell index, FP32 offsets and velocities
+struct F32Host {
+   int* cell[2] = {};
+   float* o[2][3] = {};
+   float* v[2][3] = {};
+   int* cnt[2] = {};
+   long long capOf[2] = {0, 0};
+   long long* base = nullptr;
+   long long* baseAlt = nullptr;
+   int cur = 0;
+   double w = 0.0;   // macroparticle weight of the species
+};
+
 // one species' row-segment storage: two particle buffers sharing the layout `base`
 struct SegHost {
    double* a[2][7] = {};
@@ -180,7 +194,7 @@ struct rhgpu_ctx {
    int* finc = nullptr;                 // arrivals per (species, segment)
    int* ffill = nullptr;
    int* fbucket = nullptr;
-   int* fover = nullptr;                // 8 bytes
+   int* fover = nullptr;                // 16 bytes
    int kR = 0, kJ = 0;
    void* sortTmp = nullptr;
    size_t sortTmpBytes = 0;
@@ -198,6 +212,10 @@ struct rhgpu_ctx {
    long long flxTmpCap = 0;
    long long capHint[MAX_SPECIES] = {};
    double* diagPart = nullptr;          // DIAG_BLOCKS x DIAG_F partial rows of rhgpu_reduce_diagnostics
+   // FP32 precision form
+   bool f32ready = false;
+   F32Host f32[MAX_SPECIES];
+   F32Bufs f32b = {};
 };
 
 namespace {
@@ -833,6 +851,372 @@ int fastGather(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// FP32 precision form, host side
+
+F32Buf f32View(const F32Host& h, int which) {
+   F32Buf b;
+   b.cell = h.cell[which];
+   for (int a = 0; a < 3; ++a) { b.o[a] = h.o[which][a]; b.v[a] = h.v[which][a]; }
+   b.cnt = h.cnt[which];
+   return b;
+}
+
+int f32Reserve(F32Host& h, int which, long long slots) {
+   if (slots <= h.capOf[which] && h.cell[which]) return RHGPU_OK;
+   cudaFree(h.cell[which]);
+   h.cell[which] = nullptr;
+   for (int a = 0; a < 3; ++a) {
+      cudaFree(h.o[which][a]); cudaFree(h.v[which][a]);
+      h.o[which][a] = nullptr; h.v[which][a] = nullptr;
+   }
+   h.capOf[which] = 0;
+   const long long n = slots + slots / 16 + 1024;
+   RH_CUDA(cudaMalloc(&h.cell[which], sizeof(int) * n));
+   for (int a = 0; a < 3; ++a) {
+      RH_CUDA(cudaMalloc(&h.o[which][a], sizeof(float) * n));
+      RH_CUDA(cudaMalloc(&h.v[which][a], sizeof(float) * n));
+   }
+   h.capOf[which] = n;
+   return RHGPU_OK;
+}
+
+// buffers of the FP32 form, allocated when a context chooses it
+int f32Init(rhgpu_ctx* c) {
+   if (c->f32ready) return RHGPU_OK;
+   const long long NS = c->fg.NS;
+   for (int s = 0; s < c->ns; ++s) {
+      F32Host& h = c->f32[s];
+      for (int b = 0; b < 2; ++b) {
+         RH_CUDA(cudaMalloc(&h.cnt[b], sizeof(int) * NS));
+         RH_CUDA(cudaMemset(h.cnt[b], 0, sizeof(int) * NS));
+      }
+      RH_CUDA(cudaMalloc(&h.base, sizeof(long long) * (NS + 1)));
+      RH_CUDA(cudaMemset(h.base, 0, sizeof(long long) * (NS + 1)));
+      RH_CUDA(cudaMalloc(&h.baseAlt, sizeof(long long) * (NS + 1)));
+   }
+   RH_CUDA(cudaMalloc(&c->f32b.RP, sizeof(float) * 16 * c->fg.nrows * c->g.nx));
+   RH_CUDA(cudaMalloc(&c->f32b.RPB, sizeof(float) * 16 * c->fg.nrows * c->fg.nseg));
+   RH_CUDA(cudaMemset(c->f32b.RPB, 0, sizeof(float) * 16 * c->fg.nrows * c->fg.nseg));
+   c->f32b.MMlo = c->fb.MMlo;
+   c->f32b.MMhi = c->fb.MMhi;
+   c->f32b.touched = c->fb.touched;
+   c->f32b.nmovers = c->fb.nmovers;
+   RH_CUDA(cudaDeviceSynchronize());   // the clears above run on the default stream
+   c->f32ready = true;
+   return RHGPU_OK;
+}
+
+// (w q) of the first species that deposits anything: the unit of the FP32 sums
+double f32WqRef(const rhgpu_ctx* c) {
+   for (int s = 0; s < c->ns; ++s) {
+      const double wq = c->f32[s].w * c->sp[s].q;
+      if (wq != 0.0) return wq;
+   }
+   return 1.0;
+}
+
+F32Set f32Set(rhgpu_ctx* c) {
+   F32Set F;
+   std::memset(&F, 0, sizeof F);
+   F.ns = c->ns;
+   const double ref = f32WqRef(c);
+   for (int s = 0; s < c->ns; ++s) {
+      const F32Host& h = c->f32[s];
+      F.st[s].cur = f32View(h, h.cur);
+      F.st[s].nxt = f32View(h, h.cur ^ 1);
+      F.st[s].base = h.base;
+      F.accumulate[s] = c->sp[s].accumulate;
+      F.accelerate[s] = c->sp[s].accelerate;
+      F.qm[s] = (float)(0.5 * c->sp[s].q * c->P.dt / c->sp[s].m);
+      F.wqRel[s] = (float)(h.w * c->sp[s].q / ref);
+      F.R2obs[s] = (float)c->sp[s].R2_obstacle;
+      F.w[s] = h.w;
+   }
+   return F;
+}
+
+F32Params f32Params(rhgpu_ctx* c) {
+   F32Params pp;
+   pp.dtdx = (float)(c->P.dt / c->P.dx);
+   pp.dt = (float)c->P.dt;
+   pp.dx = (float)c->P.dx;
+   pp.below1 = std::nextafter(1.0f, 0.0f);
+   pp.maxVi2 = (float)c->P.max_ion_speed2;
+   pp.GMdt = (float)c->P.GMdt;
+   pp.useIFT = c->useIFT;
+   pp.use_ep = c->P.use_electron_pressure;
+   pp.use_gravity = c->P.use_gravity;
+   return pp;
+}
+
+// fixed-point exponents of the out-of-segment sums, in units of the reference (w q)
+void f32Exponents(rhgpu_ctx* c) {
+   const double ref = f32WqRef(c);
+   double bR = 0.0;
+   for (int s = 0; s < c->ns; ++s) bR = std::max(bR, std::fabs(c->f32[s].w * c->sp[s].q / ref));
+   // FP32 weights and velocities: allow the rounding of a float above the bound
+   bR *= 1.0 + 1e-6;
+   const double bJ = bR * (2.0 * c->P.dx / c->P.dt);
+   int e;
+   std::frexp(bR > 0 ? bR : 1.0, &e);
+   c->kR = 62 - e;
+   std::frexp(bJ > 0 ? bJ : 1.0, &e);
+   c->kJ = 62 - e;
+   c->f32b.scaleR = std::ldexp(1.0, c->kR);
+   c->f32b.scaleJ = std::ldexp(1.0, c->kJ);
+}
+
+int f32MoverBuffers(rhgpu_ctx* c) {
+   long long tot = 0;
+   for (int s = 0; s < c->ns; ++s) tot += c->f32[s].capOf[c->f32[s].cur];
+   const long long want = std::max(1LL << 20, tot / 4);
+   if (want > c->f32b.moverCap) {
+      cudaFree(c->f32b.movers);
+      cudaFree(c->fbucket);
+      c->f32b.movers = nullptr;
+      c->fbucket = nullptr;
+      c->f32b.moverCap = 0;
+      c->fb.moverCap = 0;
+      RH_CUDA(cudaMalloc(&c->f32b.movers, sizeof(Mover32) * want));
+      RH_CUDA(cudaMalloc(&c->fbucket, sizeof(int) * want));
+      c->f32b.moverCap = want;
+   }
+   return RHGPU_OK;
+}
+
+int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n) {
+   int rc = f32Init(c);
+   if (rc) return rc;
+   const long long N = c->g.N, NS = c->fg.NS;
+   rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   rc = ensureKeyCapacity(c, 2 * n + 2);
+   if (rc) return rc;
+   double* aos = (double*)c->staging;
+   uint32_t* dcounts = (uint32_t*)((char*)c->staging + sizeof(double) * 7 * (size_t)(n > 0 ? n : 1));
+   RH_CUDA(cudaMemcpyAsync(dcounts, counts, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream));
+   if (n) RH_CUDA(cudaMemcpyAsync(aos, particles, sizeof(double) * 7 * n, cudaMemcpyHostToDevice, c->stream));
+   F32Host& h = c->f32[s];
+   // one weight per species
+   if (n) {
+      unsigned long long* mm = (unsigned long long*)c->fover;   // [0] min, [1] max
+      const unsigned long long init[2] = {~0ull, 0ull};
+      RH_CUDA(cudaMemcpyAsync(mm, init, sizeof init, cudaMemcpyHostToDevice, c->stream));
+      k_weight_range<<<DIAG_BLOCKS, 256, 0, c->stream>>>(aos, n, mm, mm + 1);
+      RH_CUDA(cudaGetLastError());
+      unsigned long long r[2];
+      RH_CUDA(cudaMemcpyAsync(r, mm, sizeof r, cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      double lo, hi;
+      std::memcpy(&lo, &r[0], 8);
+      std::memcpy(&hi, &r[1], 8);
+      if (lo != hi) return fail(RHGPU_ERR_ARG, "upload_particles: the FP32 form stores one weight per species");
+      h.w = hi;
+   } else {
+      h.w = 0.0;
+   }
+   int* pcell = c->rank;
+   long long* cstart = c->ftmpCellStart;
+   k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, c->outCount);
+   RH_CUDA(cudaGetLastError());
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, cstart, N + 1, c->stream));
+   long long total = 0;
+   RH_CUDA(cudaMemcpyAsync(&total, cstart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (total != n) return fail(RHGPU_ERR_ARG, "upload_particles: sum(counts) != n_particles");
+   k_fill_pcell<<<blocks1d(N, 128), 128, 0, c->stream>>>(N, cstart, pcell);
+   RH_CUDA(cudaGetLastError());
+   rc = growBuffer(c->fsort, c->fsortCap, 2 * n + 2);
+   if (rc) return rc;
+   unsigned* keyIn = (unsigned*)c->key;
+   unsigned* keyOut = keyIn + (n + 1);
+   unsigned* idxIn = (unsigned*)c->fsort;
+   unsigned* idxOut = idxIn + (n + 1);
+   const float below1 = std::nextafter(1.0f, 0.0f);
+   if (n) {
+      k_f32_seg_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, aos, pcell, n, below1, keyIn);
+      k_iota<<<blocks1d(n, 256), 256, 0, c->stream>>>(idxIn, n);
+      RH_CUDA(cudaGetLastError());
+      size_t sb = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream);
+      rc = ensureSortTmp(c, sb);
+      if (rc) return rc;
+      sb = c->sortTmpBytes;
+      RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)n, 0, 32, c->stream));
+   }
+   k_sorted_bounds<<<blocks1d(n + 1, 256), 256, 0, c->stream>>>(keyOut, n, NS, c->ffirst);
+   k_bounds_counts<<<blocks1d(NS, 256), 256, 0, c->stream>>>(c->ffirst, NS, h.cnt[h.cur]);
+   RH_CUDA(cudaGetLastError());
+   long long slots = 0;
+   rc = fastLayout(c, h.cnt[h.cur], nullptr, h.base, &slots);
+   if (rc) return rc;
+   rc = f32Reserve(h, 0, slots);
+   if (rc) return rc;
+   rc = f32Reserve(h, 1, slots);
+   if (rc) return rc;
+   if (n) {
+      k_f32_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, aos, pcell, keyOut, idxOut, n, c->ffirst,
+                                                                    f32View(h, h.cur), h.base, below1);
+      RH_CUDA(cudaGetLastError());
+   }
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   f32Exponents(c);
+   return f32MoverBuffers(c);
+}
+
+int f32NumParticles(rhgpu_ctx* c, int s, long long* n) {
+   if (!c->f32ready) { *n = 0; return RHGPU_OK; }
+   return segPrefix(c, c->f32[s].cnt[c->f32[s].cur], n);
+}
+
+int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long long capacity, long long* n_out) {
+   const long long N = c->g.N, NS = c->fg.NS;
+   int rc = f32Init(c);
+   if (rc) return rc;
+   long long tot = 0;
+   rc = f32NumParticles(c, s, &tot);
+   if (rc) return rc;
+   if (tot > capacity) return fail(RHGPU_ERR_ARG, "download_particles: capacity too small");
+   rc = ensureKeyCapacity(c, 2 * tot + 2);
+   if (rc) return rc;
+   rc = growBuffer(c->fsortSlots, c->fsortSlotsCap, tot + 1);
+   if (rc) return rc;
+   rc = growBuffer(c->fsort, c->fsortCap, 2 * tot + 2);
+   if (rc) return rc;
+   rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(tot > 0 ? tot : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   if (rc) return rc;
+   unsigned* keyIn = (unsigned*)c->key;
+   unsigned* keyOut = keyIn + (tot + 1);
+   unsigned* idxIn = (unsigned*)c->fsort;
+   unsigned* idxOut = idxIn + (tot + 1);
+   double* aos = (double*)c->staging;
+   int* cellCnt = c->outCount;
+   const F32Host& h = c->f32[s];
+   if (tot) {
+      k_f32_cell_keys<<<(unsigned)NS, 128, 0, c->stream>>>(c->fg, f32View(h, h.cur), h.base, c->ffirst, keyIn, c->fsortSlots);
+      k_iota<<<blocks1d(tot, 256), 256, 0, c->stream>>>(idxIn, tot);
+      RH_CUDA(cudaGetLastError());
+      size_t sb = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream);
+      rc = ensureSortTmp(c, sb);
+      if (rc) return rc;
+      sb = c->sortTmpBytes;
+      RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream));
+      k_sorted_bounds<<<blocks1d(tot + 1, 256), 256, 0, c->stream>>>(keyOut, tot, N, c->ftmpCellStart);
+      k_bounds_counts<<<blocks1d(N, 256), 256, 0, c->stream>>>(c->ftmpCellStart, N, cellCnt);
+      k_f32_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(f32View(h, h.cur), c->fsortSlots, idxOut, tot,
+                                                                      c->P.dx, h.w, aos);
+      RH_CUDA(cudaGetLastError());
+   } else {
+      RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
+   }
+   RH_CUDA(cudaMemcpyAsync(counts, cellCnt, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
+   if (tot && particles) RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   *n_out = tot;
+   return RHGPU_OK;
+}
+
+int f32RelayoutNext(rhgpu_ctx* c) {
+   const long long NS = c->fg.NS;
+   for (int s = 0; s < c->ns; ++s) {
+      F32Host& h = c->f32[s];
+      const int nx = h.cur ^ 1;
+      long long total = 0;
+      int rc = fastLayout(c, h.cnt[nx], c->finc + (long long)s * NS, h.baseAlt, &total);
+      if (rc) return rc;
+      rc = f32Reserve(h, h.cur, total);
+      if (rc) return rc;
+      k_f32_relayout<<<(unsigned)NS, 128, 0, c->stream>>>(f32View(h, nx), h.base, f32View(h, h.cur), h.baseAlt);
+      RH_CUDA(cudaGetLastError());
+      std::swap(h.base, h.baseAlt);
+      h.cur ^= 1;
+      rc = f32Reserve(h, h.cur, total);
+      if (rc) return rc;
+   }
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return f32MoverBuffers(c);
+}
+
+int f32Push(rhgpu_ctx* c) {
+   int rc = f32Init(c);
+   if (rc) return rc;
+   c->timestep += 1;
+   if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
+   const long long N = c->g.N, NS = c->fg.NS;
+   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
+   {
+      RH_TIME(c, "f32_push_deposit");
+      k_f32_push_deposit<<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, f32Set(c), f32Params(c), c->f32b, c->cntD,
+                                                            c->cntU, c->err);
+      RH_LAUNCHED(c);
+   }
+   unsigned long long nm = 0;
+   RH_CUDA(cudaMemcpyAsync(&nm, c->fb.nmovers, sizeof nm, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if ((long long)nm > c->f32b.moverCap) return fail(RHGPU_ERR_CAPACITY, "mover list overflow");
+   if (nm > 0) {
+      {
+         RH_TIME(c, "f32_mover_deposit");
+         k_f32_mover_deposit<<<blocks1d(nm, 128), 128, 0, c->stream>>>(c->g, c->fg, f32Set(c), c->f32b, nm);
+         RH_LAUNCHED(c);
+      }
+      const long long nb = (long long)c->ns * NS;
+      int over = 0;
+      {
+         RH_TIME(c, "f32_migrate");
+         RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
+         RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
+         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+         k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->f32b.movers, nm, NS, c->finc);
+         RH_LAUNCHED(c);
+         k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
+         RH_LAUNCHED(c);
+         size_t bytes = c->scanTmpBytes;
+         RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
+         k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->f32b.movers, nm, NS, c->foffInc, c->ffill,
+                                                                     c->fbucket);
+         RH_LAUNCHED(c);
+         k_f32_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->f32b.movers, c->finc, c->foffInc,
+                                                                   c->fbucket, c->fover);
+         RH_LAUNCHED(c);
+         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      }
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      if (over) {
+         RH_TIME(c, "f32_relayout");
+         rc = f32RelayoutNext(c);
+         if (rc) return rc;
+         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+         k_f32_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->f32b.movers, c->finc, c->foffInc,
+                                                                   c->fbucket, c->fover);
+         RH_LAUNCHED(c);
+         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+         RH_CUDA(cudaStreamSynchronize(c->stream));
+         if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+      }
+   }
+   for (int s = 0; s < c->ns; ++s) c->f32[s].cur ^= 1;
+   return RHGPU_OK;
+}
+
+int f32Gather(rhgpu_ctx* c) {
+   int rc = f32Init(c);
+   if (rc) return rc;
+   RH_TIME(c, "f32_gather");
+   const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
+   const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
+   const double scale = f32WqRef(c) / c->g.dV;
+   k_f32_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->f32b, hiR, loR, hiJ, loJ, scale,
+                                                              c->P.min_ion_charge_density, c->cntU);
+   RH_LAUNCHED(c);
+   return RHGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -933,7 +1317,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->ftmpCellStart, sizeof(long long) * (N + 1));
    alloc((void**)&c->ftmpInc64, sizeof(long long) * (nb + 1));
    alloc((void**)&c->foffInc, sizeof(long long) * (nb + 1));
-   alloc((void**)&c->fover, sizeof(unsigned long long));
+   alloc((void**)&c->fover, 2 * sizeof(unsigned long long));
    alloc((void**)&c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_F);
    if (!rc) {
       // MM starts at zero; k_fast_gather clears what a step touched
@@ -1013,6 +1397,17 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
    cudaFree(c->ftmpInc64); cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots); cudaFree(c->flxTmp);
    cudaFree(c->diagPart);
+   for (int s = 0; s < c->ns; ++s) {
+      F32Host& h = c->f32[s];
+      for (int b = 0; b < 2; ++b) {
+         cudaFree(h.cell[b]);
+         for (int a = 0; a < 3; ++a) { cudaFree(h.o[b][a]); cudaFree(h.v[b][a]); }
+         cudaFree(h.cnt[b]);
+      }
+      cudaFree(h.base);
+      cudaFree(h.baseAlt);
+   }
+   cudaFree(c->f32b.RP); cudaFree(c->f32b.RPB); cudaFree(c->f32b.movers);
    for (int s = 0; s < c->ns; ++s) { freeStore(c->ps[s]); freeStore(c->alt[s]); }
    for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
    if (c->stream) cudaStreamDestroy(c->stream);
@@ -1112,6 +1507,7 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
    if (c->capHint[s] > 0 && n > c->capHint[s]) return fail(RHGPU_ERR_CAPACITY, "upload_particles: more particles than capacity");
    c->uploaded = true;
    if (c->path == RHGPU_PATH_FAST) return fastUpload(c, s, counts, particles, n);
+   if (c->path == RHGPU_PATH_FP32) return f32Upload(c, s, counts, particles, n);
    const long long N = c->g.N;
    PStore& P = c->ps[s];
    if (n > P.cap) {
@@ -1151,9 +1547,9 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
 int rhgpu_num_particles(rhgpu_ctx* c, int32_t s, int64_t* n_out) {
    if (!c || s < 0 || s >= c->ns || !n_out) return fail(RHGPU_ERR_ARG, "num_particles: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
-   if (c->path == RHGPU_PATH_FAST) {
+   if (c->path == RHGPU_PATH_FAST || c->path == RHGPU_PATH_FP32) {
       long long t = 0;
-      int rc = fastNumParticles(c, s, &t);
+      int rc = c->path == RHGPU_PATH_FAST ? fastNumParticles(c, s, &t) : f32NumParticles(c, s, &t);
       *n_out = t;
       return rc;
    }
@@ -1171,9 +1567,10 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
                              int64_t* n_out) {
    if (!c || s < 0 || s >= c->ns || !counts || !n_out) return fail(RHGPU_ERR_ARG, "download_particles: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
-   if (c->path == RHGPU_PATH_FAST) {
+   if (c->path == RHGPU_PATH_FAST || c->path == RHGPU_PATH_FP32) {
       long long t = 0;
-      int rc = fastDownload(c, s, counts, particles, capacity, &t);
+      int rc = c->path == RHGPU_PATH_FAST ? fastDownload(c, s, counts, particles, capacity, &t)
+                                          : f32Download(c, s, counts, particles, capacity, &t);
       *n_out = t;
       return rc;
    }
@@ -1208,14 +1605,19 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
 }
 
 namespace {
-int phasePush(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? fastPush(c) : pushAll(c); }
-int phaseAccumulate(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? fastGather(c) : accumulateAll(c); }
+int phasePush(rhgpu_ctx* c) {
+   return c->path == RHGPU_PATH_FAST ? fastPush(c) : c->path == RHGPU_PATH_FP32 ? f32Push(c) : pushAll(c);
+}
+int phaseAccumulate(rhgpu_ctx* c) {
+   return c->path == RHGPU_PATH_FAST ? fastGather(c) : c->path == RHGPU_PATH_FP32 ? f32Gather(c) : accumulateAll(c);
+}
 // the fast path removes boundary particles inside its push kernel
-int phaseBoundaries(rhgpu_ctx* c) { return c->path == RHGPU_PATH_FAST ? RHGPU_OK : boundariesAll(c); }
+int phaseBoundaries(rhgpu_ctx* c) { return c->path == RHGPU_PATH_EXACT ? boundariesAll(c) : RHGPU_OK; }
 }  // namespace
 
 int rhgpu_set_path(rhgpu_ctx* c, int32_t path) {
-   if (!c || (path != RHGPU_PATH_FAST && path != RHGPU_PATH_EXACT)) return fail(RHGPU_ERR_ARG, "set_path: bad arguments");
+   if (!c || (path != RHGPU_PATH_FAST && path != RHGPU_PATH_EXACT && path != RHGPU_PATH_FP32))
+      return fail(RHGPU_ERR_ARG, "set_path: bad arguments");
    if (c->uploaded && path != c->path) return fail(RHGPU_ERR_STATE, "set_path: particles already uploaded");
    c->path = path;
    return RHGPU_OK;
@@ -1393,6 +1795,13 @@ int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
          const SegHost& sh = c->seg[s];
          if (sh.a[sh.cur][0]) {
             k_diag_particles_seg<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(segView(sh, sh.cur), sh.base, c->fg.NS, c->diagPart);
+            launched = true;
+         }
+      } else if (c->path == RHGPU_PATH_FP32) {
+         const F32Host& fh = c->f32[s];
+         if (c->f32ready && fh.cell[fh.cur]) {
+            k_diag_particles_f32<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(f32View(fh, fh.cur), fh.base, c->fg.NS,
+                                                                            fh.w, c->diagPart);
             launched = true;
          }
       } else if (c->ps[s].start) {
