@@ -207,6 +207,9 @@ KERNEL_BYTES = {
     # read and 4 moment partials per cell written)
     "fast_push_deposit": (lambda p, c: 104 * p + 104 * c, False),
     "fast_gather": (lambda p, c: 32 * c, False),
+    # FP32 form: 28 B read + 28 B written per particle (cell, 3 offsets, 3 velocities)
+    "f32_push_deposit": (lambda p, c: 56 * p + 104 * c, False),
+    "f32_gather": (lambda p, c: 32 * c, False),
 }
 
 
@@ -228,7 +231,7 @@ def run_gpu(args, rank, world, local_rank):
     lib = abi.gpu_library()
     nps = [p[1].shape[0] for p in pops]
     ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + 1024 for n in nps], device=local_rank)
-    ctx.select_path(args.path == "fast")
+    ctx.set_path({"fast": abi.PATH_FAST, "exact": abi.PATH_EXACT, "fp32": abi.PATH_FP32}[args.path])
     ctx.upload_array("faceB", grid["faceB"])
     ctx.upload_array("cellB", grid["cellB"])
     ctx.upload_array("nodeEta", grid["nodeEta"])
@@ -396,8 +399,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's cells (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--path", default="fast", choices=["fast", "exact"],
-                    help="fast: dual-cell storage and deposit order (default); exact: the reference's order")
+    ap.add_argument("--path", default="fast", choices=["fast", "exact", "fp32"],
+                    help="fast: FP64, segment storage and deposit order (default); exact: the reference's order; "
+                         "fp32: the FP32 precision form")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
