@@ -246,6 +246,47 @@ int rhgpu_accumulate_noalloc(rhgpu_ctx* ctx);
 /* Synchronises and returns the accumulated device error word (RHGPU_DEVERR_*). */
 int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);
 
+/* ---- learned denoiser of the moments (the learned form) -------------------
+ * No counterpart in the reference. A 3-layer 3D convolutional network (3x3x3
+ * kernels, 16 channels, ReLU, residual) maps the (rho, Jx, Jy, Jz) moments of
+ * a low particles-per-cell run to those of a high-ppc run. BF16 activations
+ * and weights, FP32 accumulation on the tensor cores; forward, backward and
+ * Adam training run on the GPU. Training pairs come from the method itself:
+ * rhgpu_dn_add_pair deposits one in `factor` particles of a (high-ppc) fast
+ * path context with weights times factor (the low-ppc input) next to that
+ * context's full moments (the target). rhgpu_set_denoiser applies it in
+ * rhgpu_step between the deposit and the field update; the host switches it
+ * off when its error against a high-ppc check run exceeds the threshold.
+ * Parameters (FP32): per layer W[27][16 cin][16 cout] then b[16], tap
+ * t = (dx+1) + 3(dy+1) + 9(dz+1); layer 0 reads cin < 4, layer 2 writes
+ * cout < 4, the other entries are kept zero. Inputs are normalized by
+ * rho_scale and j_scale (rhgpu_dn_set_scales). */
+#define RHGPU_DN_PARAMS 20784
+typedef struct rhgpu_dn rhgpu_dn;
+int rhgpu_dn_create(int32_t nx, int32_t ny, int32_t nz, const int32_t* periodic, int32_t pair_capacity,
+                    int32_t device, rhgpu_dn** out);
+int rhgpu_dn_destroy(rhgpu_dn* dn);
+int rhgpu_dn_set_params(rhgpu_dn* dn, const float* params, int64_t n);
+int rhgpu_dn_get_params(rhgpu_dn* dn, float* params, int64_t n);
+int rhgpu_dn_set_scales(rhgpu_dn* dn, double rho_scale, double j_scale);
+/* host moments in the ABI layout (rho per cell, Ji interleaved) in and out;
+ * rho_out is clamped at min_rho as the deposit's finalize does */
+int rhgpu_dn_apply(rhgpu_dn* dn, const double* rho_in, const double* ji_in, double* rho_out, double* ji_out,
+                   double min_rho);
+/* mean squared error of the network on (in, target), normalized moments, and
+ * its gradient (RHGPU_DN_PARAMS floats, zero where untrainable; may be NULL) */
+int rhgpu_dn_loss_grad(rhgpu_dn* dn, const double* rho_in, const double* ji_in, const double* rho_target,
+                       const double* ji_target, double* loss, float* grad);
+int rhgpu_dn_add_pair(rhgpu_dn* dn, rhgpu_ctx* ctx, int32_t factor, int32_t offset);
+/* Adam steps, one random stored pair per step; mean loss over the steps */
+int rhgpu_dn_train(rhgpu_dn* dn, int32_t iterations, float lr, double* mean_loss);
+int rhgpu_set_denoiser(rhgpu_ctx* ctx, rhgpu_dn* dn, int32_t enabled);
+/* relative L2 errors of stored pair `pair` against its target:
+ * out4 = {raw rho, raw J, denoised rho, denoised J} */
+int rhgpu_dn_pair_error(rhgpu_dn* dn, int32_t pair, double* out4);
+/* pairs stored and the index of the newest */
+int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
+
 /* Counters: RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*n_species doubles. */
 int rhgpu_get_counters(rhgpu_ctx* ctx, double* out, int32_t n);
 

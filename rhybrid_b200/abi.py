@@ -19,6 +19,9 @@ PATH_FAST = 0
 PATH_EXACT = 1
 PATH_FP32 = 2
 
+# rhgpu.h: learned denoiser parameter count
+DN_PARAMS = 20784
+
 # rhgpu.h: status codes
 OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_DEVICE, ERR_NOMEM, ERR_CAPACITY = range(7)
 
@@ -142,6 +145,18 @@ _OPTIONAL = {
     "set_deposit_order": [_P, C.c_int32],
     "set_path": [_P, C.c_int32],
     "accumulate_noalloc": [_P],
+    "dn_create": [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(_P)],
+    "dn_destroy": [_P],
+    "dn_set_params": [_P, C.POINTER(C.c_float), C.c_int64],
+    "dn_get_params": [_P, C.POINTER(C.c_float), C.c_int64],
+    "dn_set_scales": [_P, C.c_double, C.c_double],
+    "dn_apply": [_P, _D, _D, _D, _D, C.c_double],
+    "dn_loss_grad": [_P, _D, _D, _D, _D, _D, C.POINTER(C.c_float)],
+    "dn_add_pair": [_P, _P, C.c_int32, C.c_int32],
+    "dn_train": [_P, C.c_int32, C.c_float, _D],
+    "dn_pair_error": [_P, C.c_int32, _D],
+    "dn_num_pairs": [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+    "set_denoiser": [_P, _P, C.c_int32],
     "set_threads": [_P, C.c_int32],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p}
@@ -328,6 +343,10 @@ class Context:
         """rhgpu_accumulate_noalloc: the exact-path deposit without any device allocation."""
         self.lib.call("accumulate_noalloc", self.h)
 
+    def set_denoiser(self, dn, enabled: bool = True):
+        """rhgpu_set_denoiser: apply `dn` to the moments in every step (None: none)."""
+        self.lib.call("set_denoiser", self.h, dn.h if dn is not None else None, 1 if enabled else 0)
+
     def set_path(self, path: int):
         self.lib.call("set_path", self.h, path)
 
@@ -362,3 +381,72 @@ def gpu_library() -> Library:
             raise RuntimeError(f"rhybrid_b200: CUDA library {path} not built (run __graft_entry__.build())")
         _GPU_LIB = Library(path, "rhgpu_")
     return _GPU_LIB
+
+
+class Denoiser:
+    """rhgpu_dn: the learned moment denoiser (BF16 tensor-core network)."""
+
+    def __init__(self, lib: Library, nx: int, ny: int, nz: int, periodic, pair_capacity: int = 0, device: int = 0):
+        self.lib = lib
+        self.ncells = nx * ny * nz
+        per = (C.c_int32 * 3)(*[1 if p else 0 for p in periodic])
+        h = C.c_void_p()
+        lib.call("dn_create", nx, ny, nz, per, pair_capacity, device, C.byref(h))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.call("dn_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, p: np.ndarray):
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        assert a.size == DN_PARAMS
+        self.lib.call("dn_set_params", self.h, _ptr(a, C.c_float), a.size)
+
+    def params(self) -> np.ndarray:
+        a = np.zeros(DN_PARAMS, dtype=np.float32)
+        self.lib.call("dn_get_params", self.h, _ptr(a, C.c_float), a.size)
+        return a
+
+    def set_scales(self, rho_scale: float, j_scale: float):
+        self.lib.call("dn_set_scales", self.h, rho_scale, j_scale)
+
+    def apply(self, rho: np.ndarray, ji: np.ndarray, min_rho: float = -np.inf):
+        r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        j = np.ascontiguousarray(ji, dtype=np.float64).reshape(-1)
+        ro, jo = np.empty_like(r), np.empty_like(j)
+        self.lib.call("dn_apply", self.h, _ptr(r, C.c_double), _ptr(j, C.c_double), _ptr(ro, C.c_double),
+                      _ptr(jo, C.c_double), min_rho)
+        return ro, jo.reshape(-1, 3)
+
+    def loss_grad(self, rho, ji, rho_t, ji_t):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, ji, rho_t, ji_t)]
+        loss = C.c_double()
+        g = np.zeros(DN_PARAMS, dtype=np.float32)
+        self.lib.call("dn_loss_grad", self.h, *[_ptr(a, C.c_double) for a in arrs], C.byref(loss), _ptr(g, C.c_float))
+        return loss.value, g
+
+    def add_pair(self, ctx, factor: int, offset: int):
+        self.lib.call("dn_add_pair", self.h, ctx.h, factor, offset)
+
+    def train(self, iterations: int, lr: float) -> float:
+        loss = C.c_double()
+        self.lib.call("dn_train", self.h, iterations, lr, C.byref(loss))
+        return loss.value
+
+    def pair_error(self, pair: int):
+        out = np.zeros(4)
+        self.lib.call("dn_pair_error", self.h, pair, _ptr(out, C.c_double))
+        return {"raw_rho": out[0], "raw_J": out[1], "dn_rho": out[2], "dn_J": out[3]}
+
+    def num_pairs(self):
+        n, newest = C.c_int32(), C.c_int32()
+        self.lib.call("dn_num_pairs", self.h, C.byref(n), C.byref(newest))
+        return n.value, newest.value

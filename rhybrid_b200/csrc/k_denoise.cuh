@@ -1,0 +1,346 @@
+// Learned denoiser of the charge/current moments (sm_100a): a 3-layer 3D
+// convolutional network, 3x3x3 kernels, 16 channels (4 in, 4 out, residual),
+// ReLU between layers, on BF16 activations with FP32 accumulation on the tensor
+// cores (mma.sync m16n8k16 bf16), forward and backward written here.
+//
+// Activations are channels-last, 16 BF16 channels per voxel (32 B), voxel
+// index v = i + nx (j + ny k); padded channels are zero. A convolution is an
+// implicit GEMM: for a tile of 16 consecutive voxels (rows) and the 16 output
+// channels (two n8 tiles), the K dimension runs over 27 taps x 16 input
+// channels. Outside a non-periodic box the input is zero; periodic axes wrap.
+//
+// Parameters (FP32 master copy): per layer W[27][16 cin][16 cout] then b[16];
+// tap t = (dx+1) + 3 (dy+1) + 9 (dz+1). Layer 0 uses cin < 4, layer 2 cout < 4;
+// the other entries stay zero (their gradients are masked).
+#pragma once
+
+#include <cuda_bf16.h>
+#include "rh_device.cuh"
+#include "k_fast.cuh"
+
+namespace rh {
+
+constexpr int DN_C = 16;                  // channels (padded)
+constexpr int DN_TAPS = 27;
+constexpr int DN_LAYER = DN_TAPS * DN_C * DN_C + DN_C;   // floats per layer
+constexpr int DN_PARAMS = 3 * DN_LAYER;
+constexpr int DN_WARPS = 4;               // warps per block of the convolution kernels
+constexpr int DN_WGRAD_VOX = 1024;        // voxels per block of the weight-gradient kernel
+
+struct DnGrid {
+   int nx, ny, nz;
+   int per[3];
+   long long N;
+};
+
+// B fragments of one layer for mma.m16n8k16 (.col): [tap][ntile][lane][2] u32,
+// b0 = W[k = 2q, 2q+1][n = g], b1 = W[k = 2q+8, 2q+9][n = g] (g = lane/4, q = lane%4)
+constexpr int DN_FRAG = DN_TAPS * 2 * 32 * 2;   // u32 per layer
+
+__device__ inline unsigned packBf16(float lo, float hi) {
+   const __nv_bfloat16 a = __float2bfloat16_rn(lo), b = __float2bfloat16_rn(hi);
+   return (unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16);
+}
+__device__ inline float bf16lo(unsigned u) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(u & 0xffffu))); }
+__device__ inline float bf16hi(unsigned u) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(u >> 16))); }
+
+__device__ inline void mma16816(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+   asm volatile(
+       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// neighbour voxel of v at tap offset (dx,dy,dz) (sign s = +1 forward, -1 transposed), -1 outside
+__device__ inline long long dnNeighbour(const DnGrid& g, long long v, int t, int sgn) {
+   if (v < 0 || v >= g.N) return -1;
+   int i = (int)(v % g.nx), j = (int)((v / g.nx) % g.ny), k = (int)(v / ((long long)g.nx * g.ny));
+   i += sgn * (t % 3 - 1);
+   j += sgn * ((t / 3) % 3 - 1);
+   k += sgn * (t / 9 - 1);
+   if (i < 0 || i >= g.nx) { if (!g.per[0]) return -1; i = i < 0 ? i + g.nx : i - g.nx; }
+   if (j < 0 || j >= g.ny) { if (!g.per[1]) return -1; j = j < 0 ? j + g.ny : j - g.ny; }
+   if (k < 0 || k >= g.nz) { if (!g.per[2]) return -1; k = k < 0 ? k + g.nz : k - g.nz; }
+   return (long long)i + (long long)g.nx * ((long long)j + (long long)g.ny * k);
+}
+
+// B fragments from FP32 weights W[27][16][16] (cin, cout); transposed: use W[t][cout][cin]
+__global__ void k_dn_frags(const float* W, unsigned* frag, int transposed) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (t, nt, lane)
+   if (e >= DN_TAPS * 2 * 32) return;
+   const int lane = e & 31, nt = (e >> 5) & 1, t = e >> 6;
+   const int g = lane >> 2, q = lane & 3;
+   const int n = nt * 8 + g;
+   auto w = [&](int k) {
+      return transposed ? W[(t * DN_C + n) * DN_C + k] : W[(t * DN_C + k) * DN_C + n];
+   };
+   frag[e * 2 + 0] = packBf16(w(2 * q), w(2 * q + 1));
+   frag[e * 2 + 1] = packBf16(w(2 * q + 8), w(2 * q + 9));
+}
+
+// One convolution layer over all voxels (transposed: the data-gradient
+// convolution, taps mirrored and W transposed, no bias). Each warp: 16 voxels x
+// 16 output channels. mode 0: out = relu(conv + b) as BF16; mode 1: out =
+// conv + b as BF16 (no relu); mode 2: out = (conv) * (mask > 0) as BF16 (ReLU
+// backward, mask = that layer's input activation); mode 3: FP32 out (4
+// channels) = conv + b + residual (the first 4 channels of res, FP32).
+__global__ void __launch_bounds__(32 * DN_WARPS)
+k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int transposed, int mode,
+          unsigned* out, const unsigned* mask, float* out32, const float* res) {
+   __shared__ unsigned sfrag[DN_FRAG];
+   for (int e = threadIdx.x; e < DN_FRAG; e += blockDim.x) sfrag[e] = frag[e];
+   __syncthreads();
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int gq = lane >> 2, q = lane & 3;
+   const long long v0 = ((long long)blockIdx.x * DN_WARPS + warp) * 16;
+   if (v0 >= g.N) return;
+   const long long va = v0 + gq, vb = v0 + gq + 8;   // this thread's two rows
+   float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+   const int sgn = transposed ? -1 : 1;
+   for (int t = 0; t < DN_TAPS; ++t) {
+      const long long na = dnNeighbour(g, va, t, sgn), nb = dnNeighbour(g, vb, t, sgn);
+      unsigned a[4];
+      // activations: 8 u32 (16 bf16) per voxel; this thread needs channels 2q..2q+1 and 2q+8..2q+9
+      a[0] = na >= 0 ? in[na * 8 + q] : 0u;
+      a[1] = nb >= 0 ? in[nb * 8 + q] : 0u;
+      a[2] = na >= 0 ? in[na * 8 + 4 + q] : 0u;
+      a[3] = nb >= 0 ? in[nb * 8 + 4 + q] : 0u;
+      const unsigned* f = sfrag + (t * 2) * 64;
+      mma16816(c[0], a, f[lane * 2], f[lane * 2 + 1]);
+      mma16816(c[1], a, f[64 + lane * 2], f[64 + lane * 2 + 1]);
+   }
+   // c[nt][0,1]: row gq, channels nt*8 + 2q, +1; c[nt][2,3]: row gq+8
+   for (int nt = 0; nt < 2; ++nt) {
+      const int ch = nt * 8 + 2 * q;
+      float x0 = c[nt][0], x1 = c[nt][1], x2 = c[nt][2], x3 = c[nt][3];
+      if (!transposed && bias) { x0 += bias[ch]; x1 += bias[ch + 1]; x2 += bias[ch]; x3 += bias[ch + 1]; }
+      if (mode == 0) { x0 = fmaxf(x0, 0.f); x1 = fmaxf(x1, 0.f); x2 = fmaxf(x2, 0.f); x3 = fmaxf(x3, 0.f); }
+      if (mode == 2) {
+         if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 = 0.f; if (!(bf16hi(m) > 0.f)) x1 = 0.f; }
+         if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 = 0.f; if (!(bf16hi(m) > 0.f)) x3 = 0.f; }
+      }
+      if (mode == 3) {
+         if (nt == 0 && q < 2) {
+            if (va < g.N) { out32[va * 4 + ch] = x0 + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1 + res[va * 4 + ch + 1]; }
+            if (vb < g.N) { out32[vb * 4 + ch] = x2 + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3 + res[vb * 4 + ch + 1]; }
+         }
+         continue;
+      }
+      if (va < g.N) out[va * 8 + nt * 4 + q] = packBf16(x0, x1);
+      if (vb < g.N) out[vb * 8 + nt * 4 + q] = packBf16(x2, x3);
+   }
+}
+
+// Weight gradient of one layer: dW[t][ci][co] = sum_v X[nb(v,t)][ci] dY[v][co].
+// Block (blockIdx.x, tap blockIdx.y) covers DN_WGRAD_VOX voxels, each warp a
+// quarter in k-steps of 16 voxels: C[ci][co] += A[ci][vox] B[vox][co] (mma),
+// then the 4 warps are added in order and the block's partial row written.
+__global__ void __launch_bounds__(32 * DN_WARPS)
+k_dn_wgrad(DnGrid g, const unsigned* X, const unsigned* dY, float* part) {
+   __shared__ float sacc[DN_WARPS][DN_C * DN_C];
+   const unsigned short* x16 = reinterpret_cast<const unsigned short*>(X);
+   const unsigned short* y16 = reinterpret_cast<const unsigned short*>(dY);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int gq = lane >> 2, q = lane & 3;
+   const int t = blockIdx.y;
+   float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+   const long long vw = (long long)blockIdx.x * DN_WGRAD_VOX + warp * (DN_WGRAD_VOX / DN_WARPS);
+   auto xv = [&](long long v, int ch) -> unsigned {
+      const long long n = dnNeighbour(g, v, t, 1);
+      return n >= 0 ? (unsigned)x16[n * DN_C + ch] : 0u;
+   };
+   auto yv = [&](long long v, int ch) -> unsigned { return (v < g.N) ? (unsigned)y16[v * DN_C + ch] : 0u; };
+   for (int ks = 0; ks < DN_WGRAD_VOX / DN_WARPS; ks += 16) {
+      const long long vk = vw + ks;
+      if (vk >= g.N) break;
+      unsigned a[4];
+      a[0] = xv(vk + 2 * q, gq) | (xv(vk + 2 * q + 1, gq) << 16);
+      a[1] = xv(vk + 2 * q, gq + 8) | (xv(vk + 2 * q + 1, gq + 8) << 16);
+      a[2] = xv(vk + 2 * q + 8, gq) | (xv(vk + 2 * q + 9, gq) << 16);
+      a[3] = xv(vk + 2 * q + 8, gq + 8) | (xv(vk + 2 * q + 9, gq + 8) << 16);
+      for (int nt = 0; nt < 2; ++nt) {
+         const int co = nt * 8 + gq;
+         const unsigned b0 = yv(vk + 2 * q, co) | (yv(vk + 2 * q + 1, co) << 16);
+         const unsigned b1 = yv(vk + 2 * q + 8, co) | (yv(vk + 2 * q + 9, co) << 16);
+         mma16816(c[nt], a, b0, b1);
+      }
+   }
+   // c[nt][0,1]: ci = gq, co = nt*8 + 2q, +1; c[nt][2,3]: ci = gq + 8
+   for (int nt = 0; nt < 2; ++nt) {
+      const int co = nt * 8 + 2 * q;
+      sacc[warp][gq * DN_C + co] = c[nt][0];
+      sacc[warp][gq * DN_C + co + 1] = c[nt][1];
+      sacc[warp][(gq + 8) * DN_C + co] = c[nt][2];
+      sacc[warp][(gq + 8) * DN_C + co + 1] = c[nt][3];
+   }
+   __syncthreads();
+   for (int e = threadIdx.x; e < DN_C * DN_C; e += blockDim.x) {
+      float a = 0.f;
+      for (int w = 0; w < DN_WARPS; ++w) a += sacc[w][e];
+      part[((long long)blockIdx.x * DN_TAPS + t) * DN_C * DN_C + e] = a;
+   }
+}
+
+// bias gradient partials: sum over the block's voxels of dY[v][co]
+__global__ void k_dn_bgrad(DnGrid g, const unsigned* dY, float* part) {
+   __shared__ float s[256][DN_C];
+   const unsigned short* y16 = reinterpret_cast<const unsigned short*>(dY);
+   float a[DN_C];
+   for (int c = 0; c < DN_C; ++c) a[c] = 0.f;
+   for (long long v = (long long)blockIdx.x * DN_WGRAD_VOX + threadIdx.x;
+        v < min(g.N, (long long)(blockIdx.x + 1) * DN_WGRAD_VOX); v += blockDim.x)
+      for (int c = 0; c < DN_C; ++c) a[c] += __bfloat162float(__ushort_as_bfloat16(y16[v * DN_C + c]));
+   for (int c = 0; c < DN_C; ++c) s[threadIdx.x][c] = a[c];
+   __syncthreads();
+   if (threadIdx.x < DN_C) {
+      float t = 0.f;
+      for (int r = 0; r < (int)blockDim.x; ++r) t += s[r][threadIdx.x];
+      part[(long long)blockIdx.x * DN_C + threadIdx.x] = t;
+   }
+}
+
+// sum of the block partials in block order -> grad (n values per row)
+__global__ void k_dn_reduce_rows(const float* part, long long rows, int n, float* out) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= n) return;
+   float a = 0.f;
+   for (long long r = 0; r < rows; ++r) a += part[r * n + e];
+   out[e] = a;
+}
+
+// MSE loss over the 4 real channels and its gradient (BF16, 16 channels)
+__global__ void k_dn_loss(DnGrid g, const float* pred, const float* target, double inv, unsigned* dY, double* part) {
+   __shared__ double s[256];
+   double l = 0.0;
+   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < g.N; v += (long long)gridDim.x * blockDim.x) {
+      float d[4];
+      for (int c = 0; c < 4; ++c) {
+         d[c] = pred[v * 4 + c] - target[v * 4 + c];
+         l += (double)d[c] * d[c];
+      }
+      const float k = (float)(2.0 * inv);
+      dY[v * 8 + 0] = packBf16(k * d[0], k * d[1]);
+      dY[v * 8 + 1] = packBf16(k * d[2], k * d[3]);
+      for (int u = 2; u < 8; ++u) dY[v * 8 + u] = 0u;
+   }
+   s[threadIdx.x] = l;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double a = 0.0;
+      for (int r = 0; r < (int)blockDim.x; ++r) a += s[r];
+      part[blockIdx.x] = a;
+   }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters; mask 0 keeps padding at zero
+__global__ void k_dn_adam(float* p, const float* gr, float* m, float* v, const unsigned char* mask, int n, float lr,
+                          float b1, float b2, float eps, float c1, float c2) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= n || !mask[e]) return;
+   const float g = gr[e];
+   m[e] = b1 * m[e] + (1.f - b1) * g;
+   v[e] = b2 * v[e] + (1.f - b2) * g * g;
+   p[e] -= lr * (m[e] / c1) / (sqrtf(v[e] / c2) + eps);
+}
+
+// planar FP64 moments (rho N, J 3N) -> normalized FP32 residual copy (N x 4) + BF16 input (16 channels)
+__global__ void k_dn_pack(long long N, const double* rho, const double* J, double sr, double sj, float* res,
+                          unsigned* act) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= N) return;
+   const float x0 = (float)(rho[v] / sr), x1 = (float)(J[v] / sj), x2 = (float)(J[N + v] / sj), x3 = (float)(J[2 * N + v] / sj);
+   res[v * 4 + 0] = x0; res[v * 4 + 1] = x1; res[v * 4 + 2] = x2; res[v * 4 + 3] = x3;
+   act[v * 8 + 0] = packBf16(x0, x1);
+   act[v * 8 + 1] = packBf16(x2, x3);
+   for (int u = 2; u < 8; ++u) act[v * 8 + u] = 0u;
+}
+// network output (normalized FP32, N x 4) -> planar FP64 moments, rho clamped as the deposit's finalize
+__global__ void k_dn_unpack(long long N, const float* out, double sr, double sj, double minRho, double* rho, double* J) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= N) return;
+   double r = (double)out[v * 4] * sr;
+   if (r < minRho) r = minRho;
+   rho[v] = r;
+   for (int l = 0; l < 3; ++l) J[l * N + v] = (double)out[v * 4 + 1 + l] * sj;
+}
+// normalized FP32 copy (N x 4) of planar FP64 moments (training targets)
+__global__ void k_dn_norm(long long N, const double* rho, const double* J, double sr, double sj, float* out) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= N) return;
+   out[v * 4] = (float)(rho[v] / sr);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(J[l * N + v] / sj);
+}
+
+// FP32 normalized moments (N x 4) -> BF16 network input (16 channels)
+__global__ void k_dn_res_to_act(long long N, const float* res, unsigned* act) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= N) return;
+   act[v * 8 + 0] = packBf16(res[v * 4], res[v * 4 + 1]);
+   act[v * 8 + 1] = packBf16(res[v * 4 + 2], res[v * 4 + 3]);
+   for (int u = 2; u < 8; ++u) act[v * 8 + u] = 0u;
+}
+
+// CIC deposit of one in `factor` particles of the fast-path store (index in the
+// segment = offset mod factor), weights times factor, into FP64 sums (4 x N,
+// atomics: training data only). One block per segment.
+__global__ void k_dn_subsample_deposit(GridInfo g, FastGeom fg, SegBuf B, const long long* base, double q, int factor,
+                                       int offset, double* acc) {
+   const long long S = blockIdx.x;
+   const long long row = S / fg.nseg;
+   const int gs = (int)(S % fg.nseg);
+   const int uy = (int)(row % fg.nd[1]), uz = (int)(row / fg.nd[1]);
+   const long long N = g.N;
+   for (int r = threadIdx.x; r < B.cnt[S]; r += blockDim.x) {
+      if (r % factor != offset) continue;
+      const long long slot = base[S] + r;
+      double st[7];
+      for (int a = 0; a < 7; ++a) st[a] = B.a[a][slot];
+      const int u = gs * SEG + B.lx[slot];
+      const int bx = dualB(u, g.per[0]), by = dualB(uy, g.per[1]), bz = dualB(uz, g.per[2]);
+      double w8[8];
+      cicWeightsDx(st[0], st[1], st[2], st[6] * q * factor, g, w8);
+      for (int o = 0; o < 8; ++o) {
+         int x = bx + (o & 1), y = by + ((o >> 1) & 1), z = bz + ((o >> 2) & 1);
+         if (!wrapc(x, g.nx, g.per[0]) || !wrapc(y, g.ny, g.per[1]) || !wrapc(z, g.nz, g.per[2])) continue;
+         const long long c = cidx(g, x, y, z);
+         atomicAdd(&acc[c], w8[o]);
+         for (int l = 0; l < 3; ++l) atomicAdd(&acc[(1 + l) * N + c], w8[o] * st[3 + l]);
+      }
+   }
+}
+// the deposit's finalize on the subsample sums: /dV, rho clamp, then normalized FP32 (N x 4)
+__global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double sr, double sj,
+                                      float* out) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= N) return;
+   double r = acc[v] / dV;
+   if (r < minRho) r = minRho;
+   out[v * 4] = (float)(r / sr);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(acc[(1 + l) * N + v] / dV / sj);
+}
+
+// squared-error sums for the relative L2 errors of one pair: per block
+// {sum |a-t|^2 rho, sum |t|^2 rho, sum |a-t|^2 J, sum |t|^2 J}
+__global__ void k_dn_err(long long N, const float* a, const float* t, double* part) {
+   __shared__ double s[256][4];
+   double e[4] = {0, 0, 0, 0};
+   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+      const double d0 = (double)a[v * 4] - t[v * 4];
+      e[0] += d0 * d0;
+      e[1] += (double)t[v * 4] * t[v * 4];
+      for (int l = 1; l < 4; ++l) {
+         const double d = (double)a[v * 4 + l] - t[v * 4 + l];
+         e[2] += d * d;
+         e[3] += (double)t[v * 4 + l] * t[v * 4 + l];
+      }
+   }
+   for (int q = 0; q < 4; ++q) s[threadIdx.x][q] = e[q];
+   __syncthreads();
+   if (threadIdx.x < 4) {
+      double a2 = 0.0;
+      for (int r = 0; r < (int)blockDim.x; ++r) a2 += s[r][threadIdx.x];
+      part[blockIdx.x * 4 + threadIdx.x] = a2;
+   }
+}
+
+}  // namespace rh
