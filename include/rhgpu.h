@@ -253,8 +253,8 @@ int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);
  * and weights, FP32 accumulation on the tensor cores; forward, backward and
  * Adam training run on the GPU. Training pairs come from the method itself:
  * rhgpu_dn_add_pair deposits one in `factor` particles of a (high-ppc) fast
- * path context with weights times factor (the low-ppc input) next to that
- * context's full moments (the target). rhgpu_set_denoiser applies it in
+ * path context with weights times factor (the low-ppc input) next to the
+ * deposit of all its particles (the target), both from its current state. rhgpu_set_denoiser applies it in
  * rhgpu_step between the deposit and the field update; the host switches it
  * off when its error against a high-ppc check run exceeds the threshold.
  * Parameters (FP32): per layer W[27][16 cin][16 cout] then b[16], tap

@@ -2116,17 +2116,21 @@ int rhgpu_dn_add_pair(rhgpu_dn* d, rhgpu_ctx* c, int32_t factor, int32_t offset)
    const long long N = d->g.N;
    float* in = d->pairIn + (size_t)d->pairNext * 4 * N;
    float* tg = d->pairOut + (size_t)d->pairNext * 4 * N;
-   RH_CUDA(cudaMemsetAsync(d->acc, 0, sizeof(double) * 4 * N, d->stream));
-   for (int s = 0; s < c->ns; ++s) {
-      if (!c->sp[s].accumulate) continue;
-      const SegHost& h = c->seg[s];
-      if (!h.a[h.cur][0]) continue;
-      k_dn_subsample_deposit<<<(unsigned)c->fg.NS, 128, 0, d->stream>>>(c->g, c->fg, segView(h, h.cur), h.base, c->sp[s].q,
-                                                                       factor, offset, d->acc);
+   // input: one in `factor` particles, weights times factor; target: all particles,
+   // by the same deposit of the same state
+   for (int pass = 0; pass < 2; ++pass) {
+      const int k = pass == 0 ? factor : 1, off = pass == 0 ? offset : 0;
+      RH_CUDA(cudaMemsetAsync(d->acc, 0, sizeof(double) * 4 * N, d->stream));
+      for (int s = 0; s < c->ns; ++s) {
+         if (!c->sp[s].accumulate) continue;
+         const SegHost& h = c->seg[s];
+         if (!h.a[h.cur][0]) continue;
+         k_dn_subsample_deposit<<<(unsigned)c->fg.NS, 128, 0, d->stream>>>(c->g, c->fg, segView(h, h.cur), h.base,
+                                                                          c->sp[s].q, k, off, d->acc);
+      }
+      k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, c->g.dV, c->P.min_ion_charge_density,
+                                                                    d->sr, d->sj, pass == 0 ? in : tg);
    }
-   k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, c->g.dV, c->P.min_ion_charge_density, d->sr,
-                                                                 d->sj, in);
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, c->f.cellRho, c->f.cellJi, d->sr, d->sj, tg);
    RH_CUDA(cudaGetLastError());
    RH_CUDA(cudaStreamSynchronize(d->stream));
    d->pairNext = (d->pairNext + 1) % d->pairCap;

@@ -6,7 +6,7 @@ against a high-ppc plain run.
 Training pairs (train_on_run): a high-ppc fast-path context is stepped; after
 each step, rhgpu_dn_add_pair deposits one in `factor` of its particles with
 the weights multiplied by `factor` (a low-ppc sample of the same state) and
-stores it next to the context's full moments. Adam steps on random stored
+stores it next to the deposit of all its particles. Adam steps on random stored
 pairs follow (rhgpu_dn_train).
 
 The gate (LearnedForm.judge): at each output step the denoised moments of the
