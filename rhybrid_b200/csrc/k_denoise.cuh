@@ -51,17 +51,26 @@ __device__ inline void mma16816(float c[4], const unsigned a[4], unsigned b0, un
        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// neighbour voxel of v at tap offset (dx,dy,dz) (sign s = +1 forward, -1 transposed), -1 outside
-__device__ inline long long dnNeighbour(const DnGrid& g, long long v, int t, int sgn) {
-   if (v < 0 || v >= g.N) return -1;
-   int i = (int)(v % g.nx), j = (int)((v / g.nx) % g.ny), k = (int)(v / ((long long)g.nx * g.ny));
-   i += sgn * (t % 3 - 1);
-   j += sgn * ((t / 3) % 3 - 1);
-   k += sgn * (t / 9 - 1);
+// (i, j, k) of voxel v (v < N < 2^31), -1 in i when v is outside
+struct DnPos { int i, j, k; };
+__device__ inline DnPos dnDecode(const DnGrid& g, long long v) {
+   DnPos p;
+   if (v < 0 || v >= g.N) { p.i = -1; p.j = 0; p.k = 0; return p; }
+   const unsigned u = (unsigned)v, nx = (unsigned)g.nx, ny = (unsigned)g.ny;
+   const unsigned r = u / nx;
+   p.i = (int)(u - r * nx);
+   p.k = (int)(r / ny);
+   p.j = (int)(r - (unsigned)p.k * ny);
+   return p;
+}
+// neighbour of a decoded voxel at tap t (sign sgn), -1 outside
+__device__ inline int dnNb(const DnGrid& g, DnPos p, int t, int sgn) {
+   if (p.i < 0) return -1;
+   int i = p.i + sgn * (t % 3 - 1), j = p.j + sgn * ((t / 3) % 3 - 1), k = p.k + sgn * (t / 9 - 1);
    if (i < 0 || i >= g.nx) { if (!g.per[0]) return -1; i = i < 0 ? i + g.nx : i - g.nx; }
    if (j < 0 || j >= g.ny) { if (!g.per[1]) return -1; j = j < 0 ? j + g.ny : j - g.ny; }
    if (k < 0 || k >= g.nz) { if (!g.per[2]) return -1; k = k < 0 ? k + g.nz : k - g.nz; }
-   return (long long)i + (long long)g.nx * ((long long)j + (long long)g.ny * k);
+   return i + g.nx * (j + g.ny * k);
 }
 
 // B fragments from FP32 weights W[27][16][16] (cin, cout); transposed: use W[t][cout][cin]
@@ -97,14 +106,16 @@ k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias,
    const long long va = v0 + gq, vb = v0 + gq + 8;   // this thread's two rows
    float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
    const int sgn = transposed ? -1 : 1;
+   const DnPos pa = dnDecode(g, va), pb = dnDecode(g, vb);
+#pragma unroll 3
    for (int t = 0; t < DN_TAPS; ++t) {
-      const long long na = dnNeighbour(g, va, t, sgn), nb = dnNeighbour(g, vb, t, sgn);
+      const int na = dnNb(g, pa, t, sgn), nb = dnNb(g, pb, t, sgn);
       unsigned a[4];
       // activations: 8 u32 (16 bf16) per voxel; this thread needs channels 2q..2q+1 and 2q+8..2q+9
-      a[0] = na >= 0 ? in[na * 8 + q] : 0u;
-      a[1] = nb >= 0 ? in[nb * 8 + q] : 0u;
-      a[2] = na >= 0 ? in[na * 8 + 4 + q] : 0u;
-      a[3] = nb >= 0 ? in[nb * 8 + 4 + q] : 0u;
+      a[0] = na >= 0 ? in[(long long)na * 8 + q] : 0u;
+      a[1] = nb >= 0 ? in[(long long)nb * 8 + q] : 0u;
+      a[2] = na >= 0 ? in[(long long)na * 8 + 4 + q] : 0u;
+      a[3] = nb >= 0 ? in[(long long)nb * 8 + 4 + q] : 0u;
       const unsigned* f = sfrag + (t * 2) * 64;
       mma16816(c[0], a, f[lane * 2], f[lane * 2 + 1]);
       mma16816(c[1], a, f[64 + lane * 2], f[64 + lane * 2 + 1]);
@@ -145,19 +156,19 @@ k_dn_wgrad(DnGrid g, const unsigned* X, const unsigned* dY, float* part) {
    const int t = blockIdx.y;
    float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
    const long long vw = (long long)blockIdx.x * DN_WGRAD_VOX + warp * (DN_WGRAD_VOX / DN_WARPS);
-   auto xv = [&](long long v, int ch) -> unsigned {
-      const long long n = dnNeighbour(g, v, t, 1);
-      return n >= 0 ? (unsigned)x16[n * DN_C + ch] : 0u;
-   };
    auto yv = [&](long long v, int ch) -> unsigned { return (v < g.N) ? (unsigned)y16[v * DN_C + ch] : 0u; };
    for (int ks = 0; ks < DN_WGRAD_VOX / DN_WARPS; ks += 16) {
       const long long vk = vw + ks;
       if (vk >= g.N) break;
+      // the input voxels (at tap t) of this thread's four k indices
+      const int n0 = dnNb(g, dnDecode(g, vk + 2 * q), t, 1), n1 = dnNb(g, dnDecode(g, vk + 2 * q + 1), t, 1);
+      const int n8 = dnNb(g, dnDecode(g, vk + 2 * q + 8), t, 1), n9 = dnNb(g, dnDecode(g, vk + 2 * q + 9), t, 1);
+      auto xv = [&](int n, int ch) -> unsigned { return n >= 0 ? (unsigned)x16[(long long)n * DN_C + ch] : 0u; };
       unsigned a[4];
-      a[0] = xv(vk + 2 * q, gq) | (xv(vk + 2 * q + 1, gq) << 16);
-      a[1] = xv(vk + 2 * q, gq + 8) | (xv(vk + 2 * q + 1, gq + 8) << 16);
-      a[2] = xv(vk + 2 * q + 8, gq) | (xv(vk + 2 * q + 9, gq) << 16);
-      a[3] = xv(vk + 2 * q + 8, gq + 8) | (xv(vk + 2 * q + 9, gq + 8) << 16);
+      a[0] = xv(n0, gq) | (xv(n1, gq) << 16);
+      a[1] = xv(n0, gq + 8) | (xv(n1, gq + 8) << 16);
+      a[2] = xv(n8, gq) | (xv(n9, gq) << 16);
+      a[3] = xv(n8, gq + 8) | (xv(n9, gq + 8) << 16);
       for (int nt = 0; nt < 2; ++nt) {
          const int co = nt * 8 + gq;
          const unsigned b0 = yv(vk + 2 * q, co) | (yv(vk + 2 * q + 1, co) << 16);

@@ -26,16 +26,23 @@ LAYER = TAPS * C * C + C
 
 
 def init_params(seed: int = 0) -> np.ndarray:
-    """He-normal weights for the two hidden layers (real input channels only),
-    zero biases, and a zero last layer: the untrained network is the identity
-    through its residual connection."""
+    """Signed pass-through start: layer 0 maps each input channel c to
+    relu(x_c) and relu(-x_c) (channels c and c+4) at the centre tap, layer 1
+    carries channels 0-7 through unchanged, channels 8-15 of both are
+    He-normal random features, and the last layer is zero, so the untrained
+    network is the identity (residual) and any linear filter of the input is
+    one layer of training away."""
     rng = np.random.default_rng(seed)
     p = np.zeros(abi.DN_PARAMS, dtype=np.float32)
-    for l, fan_in in ((0, TAPS * 4), (1, TAPS * C)):
-        w = rng.normal(0.0, np.sqrt(2.0 / fan_in), (TAPS, C, C)).astype(np.float32)
-        if l == 0:
-            w[:, 4:, :] = 0.0
-        p[l * LAYER:l * LAYER + TAPS * C * C] = w.reshape(-1)
+    W0 = p[0:TAPS * C * C].reshape(TAPS, C, C)
+    W1 = p[LAYER:LAYER + TAPS * C * C].reshape(TAPS, C, C)
+    for c in range(4):
+        W0[13, c, c] = 1.0
+        W0[13, c, c + 4] = -1.0
+    W0[:, :4, 8:] = rng.normal(0.0, np.sqrt(2.0 / (TAPS * 4)), (TAPS, 4, 8))
+    for c in range(8):
+        W1[13, c, c] = 1.0
+    W1[:, :, 8:] = rng.normal(0.0, np.sqrt(2.0 / (TAPS * C)), (TAPS, C, 8))
     return p
 
 
