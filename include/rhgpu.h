@@ -248,7 +248,7 @@ int rhgpu_device_errors(rhgpu_ctx* ctx, uint32_t* word_out);
 
 /* ---- learned denoiser of the moments (the learned form) -------------------
  * No counterpart in the reference. A 3-layer 3D convolutional network (3x3x3
- * kernels, 16 channels, ReLU, residual) maps the (rho, Jx, Jy, Jz) moments of
+ * kernels, 16 channels, leaky ReLU, residual) maps the (rho, Jx, Jy, Jz) moments of
  * a low particles-per-cell run to those of a high-ppc run. BF16 activations
  * and weights, FP32 accumulation on the tensor cores; forward, backward and
  * Adam training run on the GPU. Training pairs come from the method itself:

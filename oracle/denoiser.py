@@ -13,6 +13,7 @@ import numpy as np
 
 C = 16
 TAPS = 27
+LEAK = 0.125   # leaky ReLU slope below zero
 LAYER = TAPS * C * C + C
 PARAMS = 3 * LAYER
 
@@ -80,9 +81,10 @@ def forward(p, x, periodic, bf16_mode=True):
     x = np.asarray(x, dtype=np.float32 if bf16_mode else np.float64)
     a0 = np.zeros(x.shape[:3] + (C,), dtype=np.float64)
     a0[..., :4] = rnd(x)
-    h1 = np.maximum(conv(a0, Wr[0], periodic) + bs[0], 0.0)
+    lrelu = lambda h: np.where(h > 0, h, LEAK * h)   # noqa: E731
+    h1 = lrelu(conv(a0, Wr[0], periodic) + bs[0])
     a1 = rnd(h1.astype(np.float32)) if bf16_mode else h1
-    h2 = np.maximum(conv(a1, Wr[1], periodic) + bs[1], 0.0)
+    h2 = lrelu(conv(a1, Wr[1], periodic) + bs[1])
     a2 = rnd(h2.astype(np.float32)) if bf16_mode else h2
     y = conv(a2, Wr[2], periodic) + bs[2]
     out = y[..., :4] + x.astype(np.float64)
@@ -110,7 +112,7 @@ def loss_grad(p, x, target, periodic, bf16_mode=True):
         g[base:base + TAPS * C * C] = gW.reshape(-1)
         g[base + TAPS * C * C:base + LAYER] = dY.reshape(-1, C).sum(0)
         if l > 0:
-            dX = conv(dY, Wr[l], periodic, transposed=True) * (acts[l] > 0)
+            dX = conv(dY, Wr[l], periodic, transposed=True) * np.where(acts[l] > 0, 1.0, LEAK)
             dY = rnd(dX.astype(np.float32)) if bf16_mode else dX
     # untrainable entries (padding channels) are zero
     for l in range(3):

@@ -26,6 +26,7 @@ constexpr int DN_LAYER = DN_TAPS * DN_C * DN_C + DN_C;   // floats per layer
 constexpr int DN_PARAMS = 3 * DN_LAYER;
 constexpr int DN_WARPS = 4;               // warps per block of the convolution kernels
 constexpr int DN_WGRAD_VOX = 1024;        // voxels per block of the weight-gradient kernel
+constexpr float DN_LEAK = 0.125f;         // slope of the leaky ReLU below zero
 
 struct DnGrid {
    int nx, ny, nz;
@@ -89,9 +90,9 @@ __global__ void k_dn_frags(const float* W, unsigned* frag, int transposed) {
 
 // One convolution layer over all voxels (transposed: the data-gradient
 // convolution, taps mirrored and W transposed, no bias). Each warp: 16 voxels x
-// 16 output channels. mode 0: out = relu(conv + b) as BF16; mode 1: out =
-// conv + b as BF16 (no relu); mode 2: out = (conv) * (mask > 0) as BF16 (ReLU
-// backward, mask = that layer's input activation); mode 3: FP32 out (4
+// 16 output channels. mode 0: out = lrelu(conv + b) as BF16; mode 1: out =
+// conv + b as BF16; mode 2: out = conv * (mask > 0 ? 1 : 1/8) as BF16 (leaky
+// ReLU backward, mask = that layer's input activation); mode 3: FP32 out (4
 // channels) = conv + b + residual (the first 4 channels of res, FP32).
 __global__ void __launch_bounds__(32 * DN_WARPS)
 k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int transposed, int mode,
@@ -125,10 +126,14 @@ k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias,
       const int ch = nt * 8 + 2 * q;
       float x0 = c[nt][0], x1 = c[nt][1], x2 = c[nt][2], x3 = c[nt][3];
       if (!transposed && bias) { x0 += bias[ch]; x1 += bias[ch + 1]; x2 += bias[ch]; x3 += bias[ch + 1]; }
-      if (mode == 0) { x0 = fmaxf(x0, 0.f); x1 = fmaxf(x1, 0.f); x2 = fmaxf(x2, 0.f); x3 = fmaxf(x3, 0.f); }
+      if (mode == 0) {
+         x0 = x0 > 0.f ? x0 : DN_LEAK * x0; x1 = x1 > 0.f ? x1 : DN_LEAK * x1;
+         x2 = x2 > 0.f ? x2 : DN_LEAK * x2; x3 = x3 > 0.f ? x3 : DN_LEAK * x3;
+      }
       if (mode == 2) {
-         if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 = 0.f; if (!(bf16hi(m) > 0.f)) x1 = 0.f; }
-         if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 = 0.f; if (!(bf16hi(m) > 0.f)) x3 = 0.f; }
+         // leaky ReLU backward: the activation's sign is its input's sign
+         if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1 *= DN_LEAK; }
+         if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3 *= DN_LEAK; }
       }
       if (mode == 3) {
          if (nt == 0 && q < 2) {

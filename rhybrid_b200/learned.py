@@ -27,7 +27,7 @@ LAYER = TAPS * C * C + C
 
 def init_params(seed: int = 0) -> np.ndarray:
     """Signed pass-through start: layer 0 maps each input channel c to
-    relu(x_c) and relu(-x_c) (channels c and c+4) at the centre tap, layer 1
+    lrelu(x_c) and lrelu(-x_c) (channels c and c+4) at the centre tap, layer 1
     carries channels 0-7 through unchanged, channels 8-15 of both are
     He-normal random features, and the last layer is zero, so the untrained
     network is the identity (residual) and any linear filter of the input is
