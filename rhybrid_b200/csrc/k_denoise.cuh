@@ -98,52 +98,65 @@ __global__ void __launch_bounds__(32 * DN_WARPS)
 k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int transposed, int mode,
           unsigned* out, const unsigned* mask, float* out32, const float* res) {
    __shared__ unsigned sfrag[DN_FRAG];
+   __shared__ int soff[DN_TAPS];   // neighbour offsets of an interior voxel
    for (int e = threadIdx.x; e < DN_FRAG; e += blockDim.x) sfrag[e] = frag[e];
+   const int sgn = transposed ? -1 : 1;
+   if (threadIdx.x < DN_TAPS) {
+      const int t = threadIdx.x;
+      soff[t] = sgn * ((t % 3 - 1) + g.nx * (((t / 3) % 3 - 1) + g.ny * (t / 9 - 1)));
+   }
    __syncthreads();
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    const int gq = lane >> 2, q = lane & 3;
-   const long long v0 = ((long long)blockIdx.x * DN_WARPS + warp) * 16;
-   if (v0 >= g.N) return;
-   const long long va = v0 + gq, vb = v0 + gq + 8;   // this thread's two rows
-   float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-   const int sgn = transposed ? -1 : 1;
-   const DnPos pa = dnDecode(g, va), pb = dnDecode(g, vb);
+   const long long ntiles = (g.N + 15) / 16;
+   // persistent: the block keeps its weight fragments for many 16-voxel tiles
+   for (long long tile = (long long)blockIdx.x * DN_WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * DN_WARPS) {
+      const long long v0 = tile * 16;
+      const long long va = v0 + gq, vb = v0 + gq + 8;   // this thread's two rows
+      float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+      const DnPos pa = dnDecode(g, va), pb = dnDecode(g, vb);
+      auto interior = [&](const DnPos& p) {
+         return p.i >= 1 && p.i < g.nx - 1 && p.j >= 1 && p.j < g.ny - 1 && p.k >= 1 && p.k < g.nz - 1;
+      };
+      const bool ia = interior(pa), ib = interior(pb);
 #pragma unroll 3
-   for (int t = 0; t < DN_TAPS; ++t) {
-      const int na = dnNb(g, pa, t, sgn), nb = dnNb(g, pb, t, sgn);
-      unsigned a[4];
-      // activations: 8 u32 (16 bf16) per voxel; this thread needs channels 2q..2q+1 and 2q+8..2q+9
-      a[0] = na >= 0 ? in[(long long)na * 8 + q] : 0u;
-      a[1] = nb >= 0 ? in[(long long)nb * 8 + q] : 0u;
-      a[2] = na >= 0 ? in[(long long)na * 8 + 4 + q] : 0u;
-      a[3] = nb >= 0 ? in[(long long)nb * 8 + 4 + q] : 0u;
-      const unsigned* f = sfrag + (t * 2) * 64;
-      mma16816(c[0], a, f[lane * 2], f[lane * 2 + 1]);
-      mma16816(c[1], a, f[64 + lane * 2], f[64 + lane * 2 + 1]);
-   }
-   // c[nt][0,1]: row gq, channels nt*8 + 2q, +1; c[nt][2,3]: row gq+8
-   for (int nt = 0; nt < 2; ++nt) {
-      const int ch = nt * 8 + 2 * q;
-      float x0 = c[nt][0], x1 = c[nt][1], x2 = c[nt][2], x3 = c[nt][3];
-      if (!transposed && bias) { x0 += bias[ch]; x1 += bias[ch + 1]; x2 += bias[ch]; x3 += bias[ch + 1]; }
-      if (mode == 0) {
-         x0 = x0 > 0.f ? x0 : DN_LEAK * x0; x1 = x1 > 0.f ? x1 : DN_LEAK * x1;
-         x2 = x2 > 0.f ? x2 : DN_LEAK * x2; x3 = x3 > 0.f ? x3 : DN_LEAK * x3;
+      for (int t = 0; t < DN_TAPS; ++t) {
+         const int na = ia ? (int)va + soff[t] : dnNb(g, pa, t, sgn);
+         const int nb = ib ? (int)vb + soff[t] : dnNb(g, pb, t, sgn);
+         unsigned a[4];
+         // activations: 8 u32 (16 bf16) per voxel; this thread needs channels 2q..2q+1 and 2q+8..2q+9
+         a[0] = na >= 0 ? in[(long long)na * 8 + q] : 0u;
+         a[1] = nb >= 0 ? in[(long long)nb * 8 + q] : 0u;
+         a[2] = na >= 0 ? in[(long long)na * 8 + 4 + q] : 0u;
+         a[3] = nb >= 0 ? in[(long long)nb * 8 + 4 + q] : 0u;
+         const unsigned* f = sfrag + (t * 2) * 64;
+         mma16816(c[0], a, f[lane * 2], f[lane * 2 + 1]);
+         mma16816(c[1], a, f[64 + lane * 2], f[64 + lane * 2 + 1]);
       }
-      if (mode == 2) {
-         // leaky ReLU backward: the activation's sign is its input's sign
-         if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1 *= DN_LEAK; }
-         if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3 *= DN_LEAK; }
-      }
-      if (mode == 3) {
-         if (nt == 0 && q < 2) {
-            if (va < g.N) { out32[va * 4 + ch] = x0 + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1 + res[va * 4 + ch + 1]; }
-            if (vb < g.N) { out32[vb * 4 + ch] = x2 + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3 + res[vb * 4 + ch + 1]; }
+      // c[nt][0,1]: row gq, channels nt*8 + 2q, +1; c[nt][2,3]: row gq+8
+      for (int nt = 0; nt < 2; ++nt) {
+         const int ch = nt * 8 + 2 * q;
+         float x0 = c[nt][0], x1 = c[nt][1], x2 = c[nt][2], x3 = c[nt][3];
+         if (!transposed && bias) { x0 += bias[ch]; x1 += bias[ch + 1]; x2 += bias[ch]; x3 += bias[ch + 1]; }
+         if (mode == 0) {
+            x0 = x0 > 0.f ? x0 : DN_LEAK * x0; x1 = x1 > 0.f ? x1 : DN_LEAK * x1;
+            x2 = x2 > 0.f ? x2 : DN_LEAK * x2; x3 = x3 > 0.f ? x3 : DN_LEAK * x3;
          }
-         continue;
+         if (mode == 2) {
+            // leaky ReLU backward: the activation's sign is its input's sign
+            if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1 *= DN_LEAK; }
+            if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3 *= DN_LEAK; }
+         }
+         if (mode == 3) {
+            if (nt == 0 && q < 2) {
+               if (va < g.N) { out32[va * 4 + ch] = x0 + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1 + res[va * 4 + ch + 1]; }
+               if (vb < g.N) { out32[vb * 4 + ch] = x2 + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3 + res[vb * 4 + ch + 1]; }
+            }
+            continue;
+         }
+         if (va < g.N) out[va * 8 + nt * 4 + q] = packBf16(x0, x1);
+         if (vb < g.N) out[vb * 8 + nt * 4 + q] = packBf16(x2, x3);
       }
-      if (va < g.N) out[va * 8 + nt * 4 + q] = packBf16(x0, x1);
-      if (vb < g.N) out[vb * 8 + nt * 4 + q] = packBf16(x2, x3);
    }
 }
 

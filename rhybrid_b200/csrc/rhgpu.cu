@@ -1267,7 +1267,11 @@ int dnRebuildFrags(rhgpu_dn* d) {
    return RHGPU_OK;
 }
 
-unsigned dnConvBlocks(const rhgpu_dn* d) { return (unsigned)((d->g.N + 16 * DN_WARPS - 1) / (16 * DN_WARPS)); }
+// persistent convolution blocks: up to 8 per SM (148 SMs), fewer for small grids
+unsigned dnConvBlocks(const rhgpu_dn* d) {
+   const long long need = (d->g.N + 16 * DN_WARPS - 1) / (16 * DN_WARPS);
+   return (unsigned)std::min<long long>(need, 148LL * 8);
+}
 
 // forward of the network on d->res (normalized FP32 input) into d->out32
 int dnForward(rhgpu_dn* d) {
