@@ -213,6 +213,19 @@ KERNEL_BYTES = {
 }
 
 
+def reduce_over_ranks(dist, seconds: float, work: float, device: str):
+    """Whole-job figures of a replica run: the slowest rank's time and the
+    total work of all ranks (one collective each; every rank calls it)."""
+    if dist is None:
+        return seconds, work
+    import torch
+    tmax = torch.tensor([seconds], dtype=torch.float64, device=device)
+    tsum = torch.tensor([work], dtype=torch.float64, device=device)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax.item()), float(tsum.item())
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     from rhybrid_b200 import abi
@@ -263,15 +276,7 @@ def run_gpu(args, rank, world, local_rank):
     ctx.set_timing(False)
     n1 = sum(ctx.num_particles(s) for s in range(len(pops)))
     psteps = 0.5 * (n0 + n1) * args.steps
-    if dist:
-        t = torch.tensor([ms, psteps], dtype=torch.float64, device="cuda")
-        tmax = t[0:1].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t[1:2].clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        ms_all, psteps_all = float(tmax.item()), float(tsum.item())
-    else:
-        ms_all, psteps_all = ms, psteps
+    ms_all, psteps_all = reduce_over_ranks(dist, ms, psteps, "cuda")
     value = psteps_all / (ms_all / 1e3)
 
     # roofline of the dominant kernel class
@@ -329,13 +334,7 @@ def run_gpu(args, rank, world, local_rank):
                 d2h += ctx.download_array(name).nbytes
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t1
-        if dist:
-            t = torch.tensor([e2e_s, float(e2e_ps)], dtype=torch.float64, device="cuda")
-            tm = t[0:1].clone()
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-            ts = t[1:2].clone()
-            dist.all_reduce(ts, op=dist.ReduceOp.SUM)
-            e2e_s, e2e_ps = float(tm.item()), float(ts.item())
+        e2e_s, e2e_ps = reduce_over_ranks(dist, e2e_s, float(e2e_ps), "cuda")
         e2e = {"value": e2e_ps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": ke}
 
