@@ -212,6 +212,27 @@ KERNEL_BYTES = {
     "f32_gather": (lambda p, c: 32 * c, False),
 }
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+# from an ncu --set full capture at 5 % of the cells (44x59x59, 4.080e6 ions):
+#   ncu --set full --clock-control none -k regex:<kernel> -s 3 -c 1 -o prof \
+#       python bench.py --scale 0.05 --steps 2 --warmup 3 --no-e2e --no-cpu-baseline [--path fp32]
+# The full workload is too large to capture with ~40 replay passes, so the
+# traffic of a full launch is this capture's traffic scaled by the units
+# processed (its algorithmic bytes), as particle and cell traffic grow in
+# proportion with the number of particles and cells.
+KERNEL_TRAFFIC = {
+    # kernel: (traffic bytes, particles, cells) of the captured launch
+    "fast_push_deposit": (262.132736e6 + 222.141952e6, 4080025, 44 * 59 * 59),
+    "f32_push_deposit": (142.863360e6 + 88.712704e6, 4080025, 44 * 59 * 59),
+}
+
+
+def scaled_traffic(kernel: str, alg_bytes: float):
+    if kernel not in KERNEL_TRAFFIC:
+        return None
+    t, p, c = KERNEL_TRAFFIC[kernel]
+    return t * alg_bytes / KERNEL_BYTES[kernel][0](p, c)
+
 
 def reduce_over_ranks(dist, seconds: float, work: float, device: str):
     """Whole-job figures of a replica run: the slowest rank's time and the
@@ -294,6 +315,12 @@ def run_gpu(args, rank, world, local_rank):
         roof = {"kernel": top[0], "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "ms_per_launch": round(per_launch_ms, 4)}
+        tr = scaled_traffic(top[0], alg)
+        if tr is not None:
+            roof["traffic"] = int(tr)
+            roof["algorithmic_bytes"] = int(alg)
+            roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 5 % of "
+                                      "the cells, scaled by the units processed")
     step_alg = algorithmic_bytes(cfg, 0.5 * (n0 + n1))
     step_ach = step_alg / ((ms / args.steps) / 1e3) / 1e9
 
@@ -350,7 +377,8 @@ def run_gpu(args, rank, world, local_rank):
         line = {
             "metric": "particle-steps/s", "value": round(value, 1), "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_all / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.path == "fp32" else "f64",
             "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform)",
             "config": {"workload": cfg.name, "cells": [cfg.nx, cfg.ny, cfg.nz], "dx_m": cfg.dx, "dt_s": cfg.dt,
                        "ions": int(0.5 * (n0 + n1)), "species": [p.name for p in cfg.populations],
