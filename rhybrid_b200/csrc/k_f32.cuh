@@ -82,45 +82,8 @@ struct F32Bufs {
 
 __device__ inline int halfSf(float o) { return o < 0.5f ? 0 : 1; }
 
-// the segment's field stencil as FP32 (layout of SegFields)
-struct SegFields32 {
-   float bx[2][2][SEG + 2];
-   float by[2][3][SEG + 1];
-   float bz[3][2][SEG + 1];
-   float ue[3][2][2][SEG + 1];
-   float ep[3][2][2][SEG + 1];
-};
-
-__device__ inline void stageSegFields32(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
-                                        SegFields32& F) {
-   const int total = SF_BX + SF_BY + SF_BZ + SF_UE * (useEp ? 2 : 1);
-   for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      int r = e;
-      if (r < SF_BX) {
-         const int lc = r % (SEG + 2) - 1, ly = (r / (SEG + 2)) % 2, lz = r / (2 * (SEG + 2));
-         F.bx[lz][ly][lc + 1] = (float)stencilLoad(g, f.faceB, 0, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
-      }
-      r -= SF_BX;
-      if (r < SF_BY) {
-         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 3 - 1, lz = r / (3 * (SEG + 1));
-         F.by[lz][ly + 1][lc] = (float)stencilLoad(g, f.faceB, 1, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
-      }
-      r -= SF_BY;
-      if (r < SF_BZ) {
-         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = r / (2 * (SEG + 1)) - 1;
-         F.bz[lz + 1][ly][lc] = (float)stencilLoad(g, f.faceB, 2, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
-      }
-      r -= SF_BZ;
-      const bool ep = r >= SF_UE;
-      if (ep) r -= SF_UE;
-      const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = (r / (2 * (SEG + 1))) % 2, l = r / (4 * (SEG + 1));
-      if (ep) F.ep[l][lz][ly][lc] = (float)stencilLoad(g, f.cellEp, l, xs0 + lc, ys0 + ly, zs0 + lz);
-      else F.ue[l][lz][ly][lc] = (float)stencilLoad(g, f.cellUe, l, xs0 + lc, ys0 + ly, zs0 + lz);
-   }
-}
+// the segment's field stencil as FP32 (staged by stageSegFields<float>)
+using SegFields32 = SegFieldsT<float>;
 
 // Boris-Buneman push in FP32 (boris.h:64-194 in cell units); o: offsets, v: velocity
 __device__ inline bool pushF32(const GridInfo& g, const SegFields32& F, const F32Set& FS, int s, const F32Params& pp,
@@ -215,10 +178,10 @@ constexpr int REC32 = 11;   // floats per deposit record: w8[8], v[3]
 __global__ void __launch_bounds__(FT, 4)
 k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F32Bufs fb, double* cntd,
                    unsigned long long* cntu, unsigned* err) {
-   __shared__ float s_rec[FT * REC32];            // deposit records; at the end acc[SEG][32]
-   __shared__ int s_wd[FW][SEG];
-   __shared__ int s_bin[SEG + 1];
-   __shared__ int s_wcnt[FW];
+   __shared__ float s_rec[FT * REC32];            // deposit records of a chunk; at the end acc[SEG][32]
+   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
+   __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell
+   __shared__ int s_wcnt[FW];                     // stayers per warp, then the stayers of the warps before
    __shared__ unsigned s_bs[FW];
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
@@ -242,7 +205,7 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
    }
    if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
    const int by0 = dualB(uy, g.per[1]), bz0 = dualB(uz, g.per[2]);
-   stageSegFields32(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, s_f);
+   stageSegFields(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, s_f);
    __syncthreads();
    const int total = s_prefix[ns];
    const int myDual = tid >> 3, myCorner = tid & 7;
@@ -325,7 +288,7 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
 
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
       if (lane == 0) {
-         s_wcnt[warp] = __popc(bs) | (__popc(br) << 16);
+         s_wcnt[warp] = __popc(bs);
          s_bs[warp] = bs;
       }
       s_wd[warp][lane] = 0;
@@ -338,31 +301,27 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
          if (rrank == 0) s_wd[warp][rd] = __popc(mm);
       }
       __syncthreads();
-      int before = 0;
-      for (int w = 0; w < warp; ++w) before += s_wcnt[w];
-      const int stayIdx = (before & 0xffff) + __popc(bs & below);
-      int firstIdx = 0;
-      if (stay || (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1))) {
-         const int P0 = max(s_prefix[s], c0) - c0;
-         for (int w = 0; w < (P0 >> 5); ++w) firstIdx += __popc(s_bs[w]);
-         firstIdx += __popc(s_bs[P0 >> 5] & ((1u << (P0 & 31)) - 1u));
-      }
-      if (stay) {
-         const F32Species& SS = FS.st[s];
-         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
-         SS.nxt.cell[slot] = (int)cidx(g, ti, tj, tk);
-         for (int a = 0; a < 3; ++a) { SS.nxt.o[a][slot] = o[a]; SS.nxt.v[a][slot] = v[a]; }
-      }
       if (warp == 0) {
          int t = 0;
-         for (int w = 0; w < FW; ++w) t += s_wd[w][lane];
+         int c[FW];
+         for (int w = 0; w < FW; ++w) { c[w] = s_wd[w][lane]; t += c[w]; }
          int x = t;
          for (int q = 1; q < 32; q <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, q);
             if (lane >= q) x += y;
          }
-         s_bin[lane] = x - t;
+         int b = x - t;
+         s_bin[lane] = b;
          if (lane == 31) s_bin[SEG] = x;
+         for (int w = 0; w < FW; ++w) { s_wd[w][lane] = b; b += c[w]; }
+         const int sw = lane < FW ? s_wcnt[lane] : 0;
+         int xs = sw;
+         for (int q = 1; q < FW; q <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, xs, q);
+            if (lane >= q) xs += y;
+         }
+         __syncwarp();
+         if (lane < FW) s_wcnt[lane] = xs - sw;
       }
       {
          const unsigned lm = __ballot_sync(0xffffffffu, leave);
@@ -389,15 +348,22 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
          }
       }
       __syncthreads();
-      if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - firstIdx;
+      if (stay) {
+         const int stayIdx = s_wcnt[warp] + __popc(bs & below);
+         const int firstIdx = stayersIn(s_bs, 0, max(s_prefix[s], c0) - c0);
+         const F32Species& SS = FS.st[s];
+         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
+         SS.nxt.cell[slot] = (int)cidx(g, ti, tj, tk);
+         for (int a = 0; a < 3; ++a) { SS.nxt.o[a][slot] = o[a]; SS.nxt.v[a][slot] = v[a]; }
+      }
+      const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
       if (rec) {
-         int pos = s_bin[rd] + rrank;
-         for (int w = 0; w < warp; ++w) pos += s_wd[w][rd];
-         float* r = s_rec + pos * REC32;
+         float* r = s_rec + (s_wd[warp][rd] + rrank) * REC32;
          for (int q = 0; q < 8; ++q) r[q] = w8[q];
          r[8] = v[0]; r[9] = v[1]; r[10] = v[2];
       }
       __syncthreads();
+      if (tid < ns) s_stay[tid] += stayAdd;
       {
          const int r1 = s_bin[myDual + 1];
          for (int r = s_bin[myDual]; r < r1; ++r) {

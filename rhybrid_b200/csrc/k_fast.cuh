@@ -147,57 +147,124 @@ __device__ inline void cicWeightsDx(double x, double y, double z, double wq, con
    w8[7] = w_x * w_y * w_z * wq;
 }
 
+// cicWeightsDx for a cell-local position in [0, dx), as every particle has
+// after its migration: there floor(x / dx) = 0 (x / dx rounds below 1), so the
+// dual base of each axis is the half-cell shift alone and the weights are
+// those of cicWeightsDx, bit for bit
+__device__ inline void cicWeightsLocal(double x, double y, double z, double wq, const GridInfo& g, double w8[8]) {
+   const double dx = g.dx;
+   const int i = halfS(x, dx), j = halfS(y, dx), k = halfS(z, dx);
+   const double x0 = (i - 1 + 0.5) * dx, y0 = (j - 1 + 0.5) * dx, z0 = (k - 1 + 0.5) * dx;
+   const double w_x = divDx(x - x0, g), w_y = divDx(y - y0, g), w_z = divDx(z - z0, g);
+   w8[0] = (1 - w_x) * (1 - w_y) * (1 - w_z) * wq;
+   w8[1] = w_x * (1 - w_y) * (1 - w_z) * wq;
+   w8[2] = (1 - w_x) * w_y * (1 - w_z) * wq;
+   w8[3] = w_x * w_y * (1 - w_z) * wq;
+   w8[4] = (1 - w_x) * (1 - w_y) * w_z * wq;
+   w8[5] = w_x * (1 - w_y) * w_z * wq;
+   w8[6] = (1 - w_x) * w_y * w_z * wq;
+   w8[7] = w_x * w_y * w_z * wq;
+}
+
+// stayers of a chunk in the chunk positions [p0, p1), from the warps' stayer ballots
+__device__ inline int stayersIn(const unsigned* bs, int p0, int p1) {
+   int n = 0;
+   for (int w = 0; w < FW; ++w) {
+      const int lo = max(p0 - 32 * w, 0), hi = min(p1 - 32 * w, 32);
+      if (lo >= hi) continue;
+      const unsigned m = (hi == 32 ? ~0u : ((1u << hi) - 1u)) & (~0u << lo);
+      n += __popc(bs[w] & m);
+   }
+   return n;
+}
+
 // the field stencil of one segment's cells in shared memory: local cell
 // (lc, ly, lz) = global (xs0 + lc, ys0 + ly, zs0 + lz), lc in [0, SEG],
 // ly, lz in {0, 1}; faceB also holds the -x / -y / -z neighbour faces
-struct SegFields {
-   double bx[2][2][SEG + 2];    // [lz][ly][lc + 1]
-   double by[2][3][SEG + 1];    // [lz][ly + 1][lc]
-   double bz[3][2][SEG + 1];    // [lz + 1][ly][lc]
-   double ue[3][2][2][SEG + 1]; // [l][lz][ly][lc]
-   double ep[3][2][2][SEG + 1];
+template <class T>
+struct SegFieldsT {
+   T bx[2][2][SEG + 2];    // [lz][ly][lc + 1]
+   T by[2][3][SEG + 1];    // [lz][ly + 1][lc]
+   T bz[3][2][SEG + 1];    // [lz + 1][ly][lc]
+   T ue[3][2][2][SEG + 1]; // [l][lz][ly][lc]
+   T ep[3][2][2][SEG + 1];
 };
-constexpr int SF_BX = 2 * 2 * (SEG + 2), SF_BY = 2 * 3 * (SEG + 1), SF_BZ = 3 * 2 * (SEG + 1);
-constexpr int SF_UE = 3 * 2 * 2 * (SEG + 1);
+using SegFields = SegFieldsT<double>;
+constexpr int SF_ROWS_B = 4 + 6 + 6;    // x-rows of faceB components in the stencil
+constexpr int SF_ROWS_C = 12;           // x-rows of one cell vector field (3 components x 2 x 2)
+constexpr int SF_ROW_WARPS = 5;         // rows per warp of a 256-thread block: ceil((16 + 24) / 8)
 
-// one global value of the stencil, 0 outside a non-periodic box (never read there:
-// the push accelerates only particles of cells with all neighbours)
-__device__ inline double stencilLoad(const GridInfo& g, const double* a, int l, int x, int y, int z) {
-   if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
-   if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
-   if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
-   if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) return 0.0;
-   return a[(long long)l * g.N + cidx(g, x, y, z)];
+// one x-row of the stencil: its shared-memory start, length, first global x,
+// and the global array, component and (y, z)
+template <class T>
+__device__ inline T* stencilRow(SegFieldsT<T>& F, const Fields& f, int r, int& len, int& dxs, const double*& arr,
+                                int& l, int& dy, int& dz) {
+   if (r < 4) {   // faceB x: ly, lz in {0, 1}, lc from -1
+      const int lz = r >> 1, ly = r & 1;
+      len = SEG + 2; dxs = -1; arr = f.faceB; l = 0; dy = ly; dz = lz;
+      return &F.bx[lz][ly][0];
+   }
+   if (r < 10) {  // faceB y: ly from -1
+      const int q = r - 4, lz = q / 3, lyp = q - 3 * lz;
+      len = SEG + 1; dxs = 0; arr = f.faceB; l = 1; dy = lyp - 1; dz = lz;
+      return &F.by[lz][lyp][0];
+   }
+   if (r < 16) {  // faceB z: lz from -1
+      const int q = r - 10, lzp = q >> 1, ly = q & 1;
+      len = SEG + 1; dxs = 0; arr = f.faceB; l = 2; dy = ly; dz = lzp - 1;
+      return &F.bz[lzp][ly][0];
+   }
+   const int q = (r - 16) % SF_ROWS_C, c = q >> 2, lz = (q >> 1) & 1, ly = q & 1;
+   len = SEG + 1; dxs = 0; l = c; dy = ly; dz = lz;
+   if (r < 16 + SF_ROWS_C) {
+      arr = f.cellUe;
+      return &F.ue[c][lz][ly][0];
+   }
+   arr = f.cellEp;
+   return &F.ep[c][lz][ly][0];
 }
 
+// the stencil, one warp per x-row (values 0 outside a non-periodic box; the
+// push accelerates only particles of cells with all neighbours, so those are
+// never read); all loads of a warp are issued before its shared-memory stores
+template <class T>
 __device__ inline void stageSegFields(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
-                                      SegFields& F) {
-   const int total = SF_BX + SF_BY + SF_BZ + SF_UE * (useEp ? 2 : 1);
-   for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      int r = e;
-      if (r < SF_BX) {
-         const int lc = r % (SEG + 2) - 1, ly = (r / (SEG + 2)) % 2, lz = r / (2 * (SEG + 2));
-         F.bx[lz][ly][lc + 1] = stencilLoad(g, f.faceB, 0, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
+                                      SegFieldsT<T>& F) {
+   const int nrows = SF_ROWS_B + SF_ROWS_C * (useEp ? 2 : 1);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   double v[SF_ROW_WARPS][2];
+   T* dst[SF_ROW_WARPS];
+   int lens[SF_ROW_WARPS];
+#pragma unroll
+   for (int k = 0; k < SF_ROW_WARPS; ++k) {
+      const int r = warp + (FT / 32) * k;
+      v[k][0] = v[k][1] = 0.0;
+      dst[k] = nullptr;
+      lens[k] = 0;
+      if (r >= nrows) continue;
+      int len, dxs, l, dy, dz;
+      const double* arr;
+      dst[k] = stencilRow(F, f, r, len, dxs, arr, l, dy, dz);
+      lens[k] = len;
+      int y = ys0 + dy, z = zs0 + dz;
+      if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
+      if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
+      if (y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+      const double* base = arr + (long long)l * g.N + (long long)g.nx * ((long long)y + (long long)g.ny * z);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+         const int e = lane + 32 * h;
+         if (e >= len) continue;
+         int x = xs0 + dxs + e;
+         if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
+         if (x >= 0 && x < g.nx) v[k][h] = base[x];
       }
-      r -= SF_BX;
-      if (r < SF_BY) {
-         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 3 - 1, lz = r / (3 * (SEG + 1));
-         F.by[lz][ly + 1][lc] = stencilLoad(g, f.faceB, 1, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
-      }
-      r -= SF_BY;
-      if (r < SF_BZ) {
-         const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = r / (2 * (SEG + 1)) - 1;
-         F.bz[lz + 1][ly][lc] = stencilLoad(g, f.faceB, 2, xs0 + lc, ys0 + ly, zs0 + lz);
-         continue;
-      }
-      r -= SF_BZ;
-      const bool ep = r >= SF_UE;
-      if (ep) r -= SF_UE;
-      const int lc = r % (SEG + 1), ly = (r / (SEG + 1)) % 2, lz = (r / (2 * (SEG + 1))) % 2, l = r / (4 * (SEG + 1));
-      if (ep) F.ep[l][lz][ly][lc] = stencilLoad(g, f.cellEp, l, xs0 + lc, ys0 + ly, zs0 + lz);
-      else F.ue[l][lz][ly][lc] = stencilLoad(g, f.cellUe, l, xs0 + lc, ys0 + ly, zs0 + lz);
+   }
+#pragma unroll
+   for (int k = 0; k < SF_ROW_WARPS; ++k) {
+      if (!dst[k]) continue;
+      dst[k][lane] = (T)v[k][0];
+      if (lane + 32 < lens[k]) dst[k][lane + 32] = (T)v[k][1];
    }
 }
 
@@ -320,9 +387,9 @@ __global__ void __launch_bounds__(FT, 4)
 k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
    __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
-   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell)
+   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
    __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell
-   __shared__ int s_wcnt[FW];                     // stayers | records << 16 per warp
+   __shared__ int s_wcnt[FW];                     // stayers per warp, then the stayers of the warps before
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ unsigned s_bs[FW];                  // stayer ballot of each warp
@@ -396,7 +463,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
             const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.sp[s].accumulate) {
                if (inSeg) {
-                  cicWeightsDx(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
+                  cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
                   rec = true;
                } else {
                   mflags |= MOVER_DEPOSIT;   // deposited by k_fast_mover_deposit
@@ -432,7 +499,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       // warp-local first: stayer/record ballots and the records per (warp, dual cell)
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
       if (lane == 0) {
-         s_wcnt[warp] = __popc(bs) | (__popc(br) << 16);
+         s_wcnt[warp] = __popc(bs);
          s_bs[warp] = bs;
       }
       s_wd[warp][lane] = 0;
@@ -445,33 +512,29 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          if (rrank == 0) s_wd[warp][rd] = __popc(mm);
       }
       __syncthreads();
-      int before = 0;
-      for (int w = 0; w < warp; ++w) before += s_wcnt[w];
-      const int stayIdx = (before & 0xffff) + __popc(bs & below);
-      // stayers of the chunk before the first particle of this thread's species
-      int firstIdx = 0;
-      if (stay || (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1))) {
-         const int P0 = max(s_prefix[s], c0) - c0;
-         for (int w = 0; w < (P0 >> 5); ++w) firstIdx += __popc(s_bs[w]);
-         firstIdx += __popc(s_bs[P0 >> 5] & ((1u << (P0 & 31)) - 1u));
-      }
-      if (stay) {
-         const SegSpecies& SS = FS.st[s];
-         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
-         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
-         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
-      }
       if (warp == 0) {
-         // first sorted record of each dual cell
+         // per dual cell (lane): first sorted record of the dual cell and of each
+         // warp's records for it; stayers of the warps before each warp
          int t = 0;
-         for (int w = 0; w < FW; ++w) t += s_wd[w][lane];
+         int c[FW];
+         for (int w = 0; w < FW; ++w) { c[w] = s_wd[w][lane]; t += c[w]; }
          int x = t;
          for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
          }
-         s_bin[lane] = x - t;
+         int b = x - t;
+         s_bin[lane] = b;
          if (lane == 31) s_bin[SEG] = x;
+         for (int w = 0; w < FW; ++w) { s_wd[w][lane] = b; b += c[w]; }
+         const int sw = lane < FW ? s_wcnt[lane] : 0;
+         int xs = sw;
+         for (int o = 1; o < FW; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, xs, o);
+            if (lane >= o) xs += y;
+         }
+         __syncwarp();
+         if (lane < FW) s_wcnt[lane] = xs - sw;
       }
       {
          const unsigned lm = __ballot_sync(0xffffffffu, leave);
@@ -497,16 +560,25 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          }
       }
       __syncthreads();
-      // running stayer count of each species: the chunk's last thread of the species adds
-      if (active && (i + 1 == s_prefix[s + 1] || tid == FT - 1)) s_stay[s] += stayIdx + (stay ? 1 : 0) - firstIdx;
+      if (stay) {
+         const int stayIdx = s_wcnt[warp] + __popc(bs & below);
+         // stayers of the chunk before the first particle of this thread's species
+         const int firstIdx = stayersIn(s_bs, 0, max(s_prefix[s], c0) - c0);
+         const SegSpecies& SS = FS.st[s];
+         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
+         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
+         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
+      }
+      // stayers of species tid in this chunk
+      const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
       if (rec) {
-         int pos = s_bin[rd] + rrank;
-         for (int w = 0; w < warp; ++w) pos += s_wd[w][rd];
-         double* r = s_rec + pos * REC;
+         double* r = s_rec + (s_wd[warp][rd] + rrank) * REC;
          for (int o = 0; o < 8; ++o) r[o] = w8[o];
          r[8] = st[3]; r[9] = st[4]; r[10] = st[5];
       }
       __syncthreads();
+      // running stayer count of each species (all reads of s_stay for this chunk are done)
+      if (tid < ns) s_stay[tid] += stayAdd;
       // ---- sums of this thread's (dual cell, corner), records in list order ----------------
       {
          const int r1 = s_bin[myDual + 1];
@@ -571,7 +643,7 @@ __global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, Fa
    double st[7];
    for (int a = 0; a < 7; ++a) st[a] = M.s[a];
    double w8[8];
-   cicWeightsDx(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
+   cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
    const long long N = g.N;
    for (int o = 0; o < 8; ++o) {
       int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);
