@@ -82,7 +82,7 @@ struct F32Bufs {
 
 __device__ inline int halfSf(float o) { return o < 0.5f ? 0 : 1; }
 
-// the segment's field stencil as FP32 (staged by stageSegFields<float>)
+// the segment's field stencil as FP32 (staged by stageSegRows<float>)
 using SegFields32 = SegFieldsT<float>;
 
 // Boris-Buneman push in FP32 (boris.h:64-194 in cell units); o: offsets, v: velocity
@@ -186,6 +186,7 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ SegFields32 s_f;
+   __shared__ StencilRow s_rows[SF_MAX_ROWS];
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -205,7 +206,7 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
    }
    if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
    const int by0 = dualB(uy, g.per[1]), bz0 = dualB(uz, g.per[2]);
-   stageSegFields(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, s_f);
+   stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, s_f, s_rows);
    __syncthreads();
    const int total = s_prefix[ns];
    const int myDual = tid >> 3, myCorner = tid & 7;

@@ -192,7 +192,6 @@ struct SegFieldsT {
 using SegFields = SegFieldsT<double>;
 constexpr int SF_ROWS_B = 4 + 6 + 6;    // x-rows of faceB components in the stencil
 constexpr int SF_ROWS_C = 12;           // x-rows of one cell vector field (3 components x 2 x 2)
-constexpr int SF_ROW_WARPS = 5;         // rows per warp of a 256-thread block: ceil((16 + 24) / 8)
 
 // one x-row of the stencil: its shared-memory start, length, first global x,
 // and the global array, component and (y, z)
@@ -224,48 +223,64 @@ __device__ inline T* stencilRow(SegFieldsT<T>& F, const Fields& f, int r, int& l
    return &F.ep[c][lz][ly][0];
 }
 
-// the stencil, one warp per x-row (values 0 outside a non-periodic box; the
-// push accelerates only particles of cells with all neighbours, so those are
-// never read); all loads of a warp are issued before its shared-memory stores
+// the stencil in two passes: threads 0..nrows-1 describe one x-row each
+// (source row or none outside a non-periodic box in y/z, first global x,
+// shared-memory offset), then all threads copy the rows' elements, SF_ROW_W
+// slots per row (values 0 outside a non-periodic box; the push accelerates
+// only particles of cells with all neighbours, so those are never read); all
+// loads of a thread are issued before its shared-memory stores
+constexpr int SF_ROW_W = SEG + 2;                               // slots per row (bx rows use all)
+constexpr int SF_MAX_ROWS = SF_ROWS_B + 2 * SF_ROWS_C;
+constexpr int SF_PER_THREAD = (SF_MAX_ROWS * SF_ROW_W + FT - 1) / FT;
+struct StencilRow {
+   const double* src;   // global x = 0 of the row, or nullptr (zeros)
+   int dst;             // element offset of the row in the stencil
+   int xs;              // global x of the row's first element
+   int len;             // elements of the row
+};
+
 template <class T>
-__device__ inline void stageSegFields(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
-                                      SegFieldsT<T>& F) {
+__device__ inline void stageSegRows(const GridInfo& g, const Fields& f, bool useEp, int xs0, int ys0, int zs0,
+                                    SegFieldsT<T>& F, StencilRow* rows) {
    const int nrows = SF_ROWS_B + SF_ROWS_C * (useEp ? 2 : 1);
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   double v[SF_ROW_WARPS][2];
-   T* dst[SF_ROW_WARPS];
-   int lens[SF_ROW_WARPS];
-#pragma unroll
-   for (int k = 0; k < SF_ROW_WARPS; ++k) {
-      const int r = warp + (FT / 32) * k;
-      v[k][0] = v[k][1] = 0.0;
-      dst[k] = nullptr;
-      lens[k] = 0;
-      if (r >= nrows) continue;
+   const int tid = threadIdx.x;
+   if (tid < nrows) {
       int len, dxs, l, dy, dz;
       const double* arr;
-      dst[k] = stencilRow(F, f, r, len, dxs, arr, l, dy, dz);
-      lens[k] = len;
+      T* dst = stencilRow(F, f, tid, len, dxs, arr, l, dy, dz);
       int y = ys0 + dy, z = zs0 + dz;
       if (g.per[1]) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
       if (g.per[2]) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
-      if (y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
-      const double* base = arr + (long long)l * g.N + (long long)g.nx * ((long long)y + (long long)g.ny * z);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-         const int e = lane + 32 * h;
-         if (e >= len) continue;
-         int x = xs0 + dxs + e;
-         if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
-         if (x >= 0 && x < g.nx) v[k][h] = base[x];
-      }
+      StencilRow r;
+      r.src = (y >= 0 && y < g.ny && z >= 0 && z < g.nz)
+                  ? arr + (long long)l * g.N + (long long)g.nx * ((long long)y + (long long)g.ny * z)
+                  : nullptr;
+      r.dst = (int)(dst - (T*)&F);
+      r.xs = xs0 + dxs;
+      r.len = len;
+      rows[tid] = r;
    }
+   __syncthreads();
+   double v[SF_PER_THREAD];
+   int d[SF_PER_THREAD];
 #pragma unroll
-   for (int k = 0; k < SF_ROW_WARPS; ++k) {
-      if (!dst[k]) continue;
-      dst[k][lane] = (T)v[k][0];
-      if (lane + 32 < lens[k]) dst[k][lane + 32] = (T)v[k][1];
+   for (int k = 0; k < SF_PER_THREAD; ++k) {
+      const int e = tid + FT * k;
+      const int ri = e / SF_ROW_W, c = e - ri * SF_ROW_W;
+      v[k] = 0.0;
+      d[k] = -1;
+      if (ri >= nrows) continue;
+      const StencilRow r = rows[ri];
+      if (c >= r.len) continue;
+      d[k] = r.dst + c;
+      int x = r.xs + c;
+      if (g.per[0]) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
+      if (r.src && x >= 0 && x < g.nx) v[k] = r.src[x];
    }
+   T* const base = (T*)&F;
+#pragma unroll
+   for (int k = 0; k < SF_PER_THREAD; ++k)
+      if (d[k] >= 0) base[d[k]] = (T)v[k];
 }
 
 // pushOne with the fields from the segment's staged stencil and divDx; the
@@ -394,6 +409,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ unsigned s_bs[FW];                  // stayer ballot of each warp
    __shared__ SegFields s_f;
+   __shared__ StencilRow s_rows[SF_MAX_ROWS];
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -413,7 +429,7 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       s_prefix[ns] = a;
    }
    if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
-   stageSegFields(g, f, pp.use_ep, dualB(u0, g.per[0]), dualB(uy, g.per[1]), dualB(uz, g.per[2]), s_f);
+   stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), dualB(uy, g.per[1]), dualB(uz, g.per[2]), s_f, s_rows);
    __syncthreads();
    const int total = s_prefix[ns];
    const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
