@@ -1,7 +1,8 @@
 // Learned denoiser of the charge/current moments (sm_100a): a 3-layer 3D
 // convolutional network, 3x3x3 kernels, 16 channels (4 in, 4 out, residual),
-// ReLU between layers, on BF16 activations with FP32 accumulation on the tensor
-// cores (mma.sync m16n8k16 bf16), forward and backward written here.
+// leaky ReLU between layers, on BF16 activations with FP32 accumulation on the
+// tensor cores (mma.sync m16n8k16 bf16, A fragments by ldmatrix from a
+// shared-memory brick), forward and backward written here.
 //
 // Activations are channels-last, 16 BF16 channels per voxel (32 B), voxel
 // index v = i + nx (j + ny k); padded channels are zero. A convolution is an
@@ -88,74 +89,128 @@ __global__ void k_dn_frags(const float* W, unsigned* frag, int transposed) {
    frag[e * 2 + 1] = packBf16(w(2 * q + 8), w(2 * q + 9));
 }
 
-// One convolution layer over all voxels (transposed: the data-gradient
-// convolution, taps mirrored and W transposed, no bias). Each warp: 16 voxels x
-// 16 output channels. mode 0: out = lrelu(conv + b) as BF16; mode 1: out =
-// conv + b as BF16; mode 2: out = conv * (mask > 0 ? 1 : 1/8) as BF16 (leaky
-// ReLU backward, mask = that layer's input activation); mode 3: FP32 out (4
-// channels) = conv + b + residual (the first 4 channels of res, FP32).
-__global__ void __launch_bounds__(32 * DN_WARPS)
+// One convolution layer (transposed: the data-gradient convolution, taps
+// mirrored and W transposed, no bias). A block covers a brick of DN_BX x DN_BY
+// x DN_BZ output voxels: the input brick with a one-voxel halo (zero outside a
+// non-periodic box, wrapped on periodic axes) is staged in shared memory with
+// 16-byte copies, and each warp runs 4 x-rows of 16 voxels (M) x 16 output
+// channels (two n8 tiles) over the 27 taps (K = 16 input channels per tap),
+// the A fragments read with ldmatrix. Voxel lv of the brick keeps its two
+// 16-byte channel halves h at 16-byte slots 2 lv + (h ^ bit 2 of lv), so the
+// 8 rows of each ldmatrix phase fall on 8 different bank groups.
+// mode 0: out = lrelu(conv + b) as BF16; mode 1: out = conv + b as BF16;
+// mode 2: out = conv * (mask > 0 ? 1 : 1/8) as BF16 (leaky ReLU backward, mask
+// = that layer's input activation); mode 3: FP32 out (4 channels) = conv + b +
+// residual (the first 4 channels of res, FP32).
+constexpr int DN_BX = 16, DN_BY = 8, DN_BZ = 4;                 // output brick
+constexpr int DN_HX = DN_BX + 2, DN_HY = DN_BY + 2, DN_HZ = DN_BZ + 2;
+constexpr int DN_HV = DN_HX * DN_HY * DN_HZ;                    // staged voxels
+constexpr int DN_TWARPS = 8;                                    // warps of k_dn_conv
+constexpr int DN_ROWS = DN_BY * DN_BZ / DN_TWARPS;              // x-rows per warp
+constexpr int DN_STAGE = (2 * DN_HV + 32 * DN_TWARPS - 1) / (32 * DN_TWARPS);   // 16-byte copies per thread
+static_assert(DN_BX == 16 && DN_BY * DN_BZ % DN_TWARPS == 0, "one m16 tile per brick x-row");
+
+__device__ inline int dnSlot(int lv, int h) { return 2 * lv + (h ^ ((lv >> 2) & 1)); }
+__device__ inline int dnWrap(int x, int n, int per) {
+   if (x >= 0 && x < n) return x;
+   if (!per) return -1;
+   x %= n;
+   return x < 0 ? x + n : x;
+}
+
+__global__ void __launch_bounds__(32 * DN_TWARPS)
 k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int transposed, int mode,
           unsigned* out, const unsigned* mask, float* out32, const float* res) {
-   __shared__ unsigned sfrag[DN_FRAG];
-   __shared__ int soff[DN_TAPS];   // neighbour offsets of an interior voxel
-   for (int e = threadIdx.x; e < DN_FRAG; e += blockDim.x) sfrag[e] = frag[e];
-   const int sgn = transposed ? -1 : 1;
-   if (threadIdx.x < DN_TAPS) {
-      const int t = threadIdx.x;
-      soff[t] = sgn * ((t % 3 - 1) + g.nx * (((t / 3) % 3 - 1) + g.ny * (t / 9 - 1)));
+   __shared__ __align__(16) uint4 sin[2 * DN_HV];
+   __shared__ __align__(16) unsigned sfrag[DN_FRAG];
+   const int tid = threadIdx.x;
+   const int x0 = blockIdx.x * DN_BX, y0 = blockIdx.y * DN_BY, z0 = blockIdx.z * DN_BZ;
+   {
+      const uint4* f4 = reinterpret_cast<const uint4*>(frag);
+      uint4* s4 = reinterpret_cast<uint4*>(sfrag);
+      for (int e = tid; e < DN_FRAG / 4; e += blockDim.x) s4[e] = f4[e];
+      uint4 v[DN_STAGE];
+      int slot[DN_STAGE];
+#pragma unroll
+      for (int k = 0; k < DN_STAGE; ++k) {
+         const int e = tid + 32 * DN_TWARPS * k;
+         v[k] = make_uint4(0u, 0u, 0u, 0u);
+         slot[k] = -1;
+         if (e >= 2 * DN_HV) continue;
+         const int lv = e >> 1, h = e & 1;
+         const int hx = lv % DN_HX, r = lv / DN_HX, hy = r % DN_HY, hz = r / DN_HY;
+         slot[k] = dnSlot(lv, h);
+         const int x = dnWrap(x0 - 1 + hx, g.nx, g.per[0]), y = dnWrap(y0 - 1 + hy, g.ny, g.per[1]),
+                   z = dnWrap(z0 - 1 + hz, g.nz, g.per[2]);
+         if (x < 0 || y < 0 || z < 0) continue;
+         const long long gv = (long long)x + (long long)g.nx * ((long long)y + (long long)g.ny * z);
+         v[k] = reinterpret_cast<const uint4*>(in)[gv * 2 + h];
+      }
+#pragma unroll
+      for (int k = 0; k < DN_STAGE; ++k)
+         if (slot[k] >= 0) sin[slot[k]] = v[k];
    }
    __syncthreads();
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int lane = tid & 31, warp = tid >> 5;
    const int gq = lane >> 2, q = lane & 3;
-   const long long ntiles = (g.N + 15) / 16;
-   // persistent: the block keeps its weight fragments for many 16-voxel tiles
-   for (long long tile = (long long)blockIdx.x * DN_WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * DN_WARPS) {
-      const long long v0 = tile * 16;
-      const long long va = v0 + gq, vb = v0 + gq + 8;   // this thread's two rows
-      float c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-      const DnPos pa = dnDecode(g, va), pb = dnDecode(g, vb);
-      auto interior = [&](const DnPos& p) {
-         return p.i >= 1 && p.i < g.nx - 1 && p.j >= 1 && p.j < g.ny - 1 && p.k >= 1 && p.k < g.nz - 1;
-      };
-      const bool ia = interior(pa), ib = interior(pb);
-#pragma unroll 3
-      for (int t = 0; t < DN_TAPS; ++t) {
-         const int na = ia ? (int)va + soff[t] : dnNb(g, pa, t, sgn);
-         const int nb = ib ? (int)vb + soff[t] : dnNb(g, pb, t, sgn);
+   const int lr = lane & 15, lh = lane >> 4;   // ldmatrix: this lane's row and channel half
+   const unsigned sbase = (unsigned)__cvta_generic_to_shared(sin);
+   const int sgn = transposed ? -1 : 1;
+   float c[DN_ROWS][2][4];
+#pragma unroll
+   for (int r = 0; r < DN_ROWS; ++r)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) c[r][nt][0] = c[r][nt][1] = c[r][nt][2] = c[r][nt][3] = 0.f;
+#pragma unroll 1
+   for (int t = 0; t < DN_TAPS; ++t) {
+      const int dx = sgn * (t % 3 - 1), dy = sgn * ((t / 3) % 3 - 1), dz = sgn * (t / 9 - 1);
+      const unsigned* f = sfrag + (t * 2) * 64;
+      const uint2 bf0 = *reinterpret_cast<const uint2*>(f + lane * 2);
+      const uint2 bf1 = *reinterpret_cast<const uint2*>(f + 64 + lane * 2);
+#pragma unroll
+      for (int r = 0; r < DN_ROWS; ++r) {
+         const int row = warp * DN_ROWS + r, ry = row % DN_BY, rz = row / DN_BY;
+         const int lv = (lr + dx + 1) + DN_HX * ((ry + dy + 1) + DN_HY * (rz + dz + 1));
+         const unsigned addr = sbase + 16u * (unsigned)dnSlot(lv, lh);
          unsigned a[4];
-         // activations: 8 u32 (16 bf16) per voxel; this thread needs channels 2q..2q+1 and 2q+8..2q+9
-         a[0] = na >= 0 ? in[(long long)na * 8 + q] : 0u;
-         a[1] = nb >= 0 ? in[(long long)nb * 8 + q] : 0u;
-         a[2] = na >= 0 ? in[(long long)na * 8 + 4 + q] : 0u;
-         a[3] = nb >= 0 ? in[(long long)nb * 8 + 4 + q] : 0u;
-         const unsigned* f = sfrag + (t * 2) * 64;
-         mma16816(c[0], a, f[lane * 2], f[lane * 2 + 1]);
-         mma16816(c[1], a, f[64 + lane * 2], f[64 + lane * 2 + 1]);
+         asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                      : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+                      : "r"(addr));
+         mma16816(c[r][0], a, bf0.x, bf0.y);
+         mma16816(c[r][1], a, bf1.x, bf1.y);
       }
-      // c[nt][0,1]: row gq, channels nt*8 + 2q, +1; c[nt][2,3]: row gq+8
+   }
+   // c[r][nt][0,1]: voxel x = gq, channels nt*8 + 2q, +1; c[r][nt][2,3]: x = gq + 8
+#pragma unroll
+   for (int r = 0; r < DN_ROWS; ++r) {
+      const int row = warp * DN_ROWS + r, y = y0 + row % DN_BY, z = z0 + row / DN_BY;
+      if (y >= g.ny || z >= g.nz) continue;
+      const long long rowv = (long long)g.nx * ((long long)y + (long long)g.ny * z);
+      const bool oka = x0 + gq < g.nx, okb = x0 + gq + 8 < g.nx;
+      const long long va = rowv + x0 + gq, vb = va + 8;
+#pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
          const int ch = nt * 8 + 2 * q;
-         float x0 = c[nt][0], x1 = c[nt][1], x2 = c[nt][2], x3 = c[nt][3];
-         if (!transposed && bias) { x0 += bias[ch]; x1 += bias[ch + 1]; x2 += bias[ch]; x3 += bias[ch + 1]; }
+         float x0v = c[r][nt][0], x1v = c[r][nt][1], x2v = c[r][nt][2], x3v = c[r][nt][3];
+         if (!transposed && bias) { x0v += bias[ch]; x1v += bias[ch + 1]; x2v += bias[ch]; x3v += bias[ch + 1]; }
          if (mode == 0) {
-            x0 = x0 > 0.f ? x0 : DN_LEAK * x0; x1 = x1 > 0.f ? x1 : DN_LEAK * x1;
-            x2 = x2 > 0.f ? x2 : DN_LEAK * x2; x3 = x3 > 0.f ? x3 : DN_LEAK * x3;
+            x0v = x0v > 0.f ? x0v : DN_LEAK * x0v; x1v = x1v > 0.f ? x1v : DN_LEAK * x1v;
+            x2v = x2v > 0.f ? x2v : DN_LEAK * x2v; x3v = x3v > 0.f ? x3v : DN_LEAK * x3v;
          }
          if (mode == 2) {
             // leaky ReLU backward: the activation's sign is its input's sign
-            if (va < g.N) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1 *= DN_LEAK; }
-            if (vb < g.N) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2 *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3 *= DN_LEAK; }
+            if (oka) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0v *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1v *= DN_LEAK; }
+            if (okb) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2v *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3v *= DN_LEAK; }
          }
          if (mode == 3) {
             if (nt == 0 && q < 2) {
-               if (va < g.N) { out32[va * 4 + ch] = x0 + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1 + res[va * 4 + ch + 1]; }
-               if (vb < g.N) { out32[vb * 4 + ch] = x2 + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3 + res[vb * 4 + ch + 1]; }
+               if (oka) { out32[va * 4 + ch] = x0v + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1v + res[va * 4 + ch + 1]; }
+               if (okb) { out32[vb * 4 + ch] = x2v + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3v + res[vb * 4 + ch + 1]; }
             }
             continue;
          }
-         if (va < g.N) out[va * 8 + nt * 4 + q] = packBf16(x0, x1);
-         if (vb < g.N) out[vb * 8 + nt * 4 + q] = packBf16(x2, x3);
+         if (oka) out[va * 8 + nt * 4 + q] = packBf16(x0v, x1v);
+         if (okb) out[vb * 8 + nt * 4 + q] = packBf16(x2v, x3v);
       }
    }
 }

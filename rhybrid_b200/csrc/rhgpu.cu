@@ -1267,10 +1267,10 @@ int dnRebuildFrags(rhgpu_dn* d) {
    return RHGPU_OK;
 }
 
-// persistent convolution blocks: up to 8 per SM (148 SMs), fewer for small grids
-unsigned dnConvBlocks(const rhgpu_dn* d) {
-   const long long need = (d->g.N + 16 * DN_WARPS - 1) / (16 * DN_WARPS);
-   return (unsigned)std::min<long long>(need, 148LL * 8);
+// convolution blocks: one per output brick
+dim3 dnConvBlocks(const rhgpu_dn* d) {
+   return dim3((unsigned)((d->g.nx + DN_BX - 1) / DN_BX), (unsigned)((d->g.ny + DN_BY - 1) / DN_BY),
+               (unsigned)((d->g.nz + DN_BZ - 1) / DN_BZ));
 }
 
 // forward of the network on d->res (normalized FP32 input) into d->out32
@@ -1280,10 +1280,10 @@ int dnForward(rhgpu_dn* d) {
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_WARPS, 0, d->stream>>>(d->g, d->act[0], d->frag, b0, 0, 0, d->act[1], nullptr, nullptr, nullptr);
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_WARPS, 0, d->stream>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, 0, d->act[2], nullptr,
+   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[0], d->frag, b0, 0, 0, d->act[1], nullptr, nullptr, nullptr);
+   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, 0, d->act[2], nullptr,
                                                               nullptr, nullptr);
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_WARPS, 0, d->stream>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 0, 3, nullptr,
+   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 0, 3, nullptr,
                                                               nullptr, d->out32, d->res);
    RH_CUDA(cudaGetLastError());
    return RHGPU_OK;
@@ -1301,7 +1301,7 @@ int dnBackward(rhgpu_dn* d, const float* target, double* loss) {
       k_dn_bgrad<<<wb, 256, 0, d->stream>>>(d->g, d->dY[l], d->part);
       k_dn_reduce_rows<<<1, DN_C, 0, d->stream>>>(d->part, wb, DN_C, d->grad + (size_t)l * DN_LAYER + DN_TAPS * DN_C * DN_C);
       if (l > 0)
-         k_dn_conv<<<dnConvBlocks(d), 32 * DN_WARPS, 0, d->stream>>>(d->g, d->dY[l], d->frag + (size_t)(3 + l) * DN_FRAG, nullptr, 1,
+         k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->dY[l], d->frag + (size_t)(3 + l) * DN_FRAG, nullptr, 1,
                                                                     2, d->dY[l - 1], d->act[l], nullptr, nullptr);
    }
    RH_CUDA(cudaGetLastError());
