@@ -95,13 +95,25 @@ __global__ void k_dn_frags(const float* W, unsigned* frag, int transposed) {
 // non-periodic box, wrapped on periodic axes) is staged in shared memory with
 // 16-byte copies, and each warp runs 4 x-rows of 16 voxels (M) x 16 output
 // channels (two n8 tiles) over the 27 taps (K = 16 input channels per tap),
-// the A fragments read with ldmatrix. Voxel lv of the brick keeps its two
-// 16-byte channel halves h at 16-byte slots 2 lv + (h ^ bit 2 of lv), so the
-// 8 rows of each ldmatrix phase fall on 8 different bank groups.
+// the A fragments read with ldmatrix. Voxel lv = hx + DN_HX (hy + DN_HY hz) of
+// the brick keeps its two 16-byte channel halves h at 16-byte slots
+// 2 lv + (h ^ bit 2 of hx): the 8 rows of an ldmatrix phase (8 consecutive hx)
+// fall on 8 different bank groups, and a tap's y/z shift keeps each lane's
+// swizzle, so the taps' addresses are a per-lane x part plus constants.
 // mode 0: out = lrelu(conv + b) as BF16; mode 1: out = conv + b as BF16;
 // mode 2: out = conv * (mask > 0 ? 1 : 1/8) as BF16 (leaky ReLU backward, mask
 // = that layer's input activation); mode 3: FP32 out (4 channels) = conv + b +
-// residual (the first 4 channels of res, FP32).
+// residual (the first 4 channels of res, FP32); mode 4: the moments mom.rho,
+// mom.J (FP64, planar) overwritten in place by (conv + b + their normalized
+// FP32 values) times the scales, rho clamped at mom.minRho. With `in` null,
+// the input is read from the moments mom: channels 0-3 = BF16(FP32(rho rsr)),
+// BF16(FP32(J rsj)), the rest zero (rsr = 1 / sr, rsj = 1 / sj, as k_dn_norm).
+struct DnMoments {
+   double* rho;    // N
+   double* J;      // 3 x N
+   double sr, sj, rsr, rsj, minRho;
+   long long N;
+};
 constexpr int DN_BX = 16, DN_BY = 8, DN_BZ = 4;                 // output brick
 constexpr int DN_HX = DN_BX + 2, DN_HY = DN_BY + 2, DN_HZ = DN_BZ + 2;
 constexpr int DN_HV = DN_HX * DN_HY * DN_HZ;                    // staged voxels
@@ -110,7 +122,7 @@ constexpr int DN_ROWS = DN_BY * DN_BZ / DN_TWARPS;              // x-rows per wa
 constexpr int DN_STAGE = (2 * DN_HV + 32 * DN_TWARPS - 1) / (32 * DN_TWARPS);   // 16-byte copies per thread
 static_assert(DN_BX == 16 && DN_BY * DN_BZ % DN_TWARPS == 0, "one m16 tile per brick x-row");
 
-__device__ inline int dnSlot(int lv, int h) { return 2 * lv + (h ^ ((lv >> 2) & 1)); }
+__device__ inline int dnSlot(int hx, int lv, int h) { return 2 * lv + (h ^ ((hx >> 2) & 1)); }
 __device__ inline int dnWrap(int x, int n, int per) {
    if (x >= 0 && x < n) return x;
    if (!per) return -1;
@@ -118,9 +130,11 @@ __device__ inline int dnWrap(int x, int n, int per) {
    return x < 0 ? x + n : x;
 }
 
+template <bool TRANSPOSED>
 __global__ void __launch_bounds__(32 * DN_TWARPS)
-k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int transposed, int mode,
-          unsigned* out, const unsigned* mask, float* out32, const float* res) {
+k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int mode, unsigned* out,
+          const unsigned* mask, float* out32, const float* res, DnMoments mom) {
+   constexpr bool transposed = TRANSPOSED;
    __shared__ __align__(16) uint4 sin[2 * DN_HV];
    __shared__ __align__(16) unsigned sfrag[DN_FRAG];
    const int tid = threadIdx.x;
@@ -139,12 +153,19 @@ k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias,
          if (e >= 2 * DN_HV) continue;
          const int lv = e >> 1, h = e & 1;
          const int hx = lv % DN_HX, r = lv / DN_HX, hy = r % DN_HY, hz = r / DN_HY;
-         slot[k] = dnSlot(lv, h);
+         slot[k] = dnSlot(hx, lv, h);
          const int x = dnWrap(x0 - 1 + hx, g.nx, g.per[0]), y = dnWrap(y0 - 1 + hy, g.ny, g.per[1]),
                    z = dnWrap(z0 - 1 + hz, g.nz, g.per[2]);
          if (x < 0 || y < 0 || z < 0) continue;
          const long long gv = (long long)x + (long long)g.nx * ((long long)y + (long long)g.ny * z);
-         v[k] = reinterpret_cast<const uint4*>(in)[gv * 2 + h];
+         if (!in) {
+            if (h == 0)
+               v[k] = make_uint4(packBf16((float)(mom.rho[gv] * mom.rsr), (float)(mom.J[gv] * mom.rsj)),
+                                 packBf16((float)(mom.J[mom.N + gv] * mom.rsj), (float)(mom.J[2 * mom.N + gv] * mom.rsj)),
+                                 0u, 0u);
+         } else {
+            v[k] = reinterpret_cast<const uint4*>(in)[gv * 2 + h];
+         }
       }
 #pragma unroll
       for (int k = 0; k < DN_STAGE; ++k)
@@ -155,23 +176,35 @@ k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias,
    const int gq = lane >> 2, q = lane & 3;
    const int lr = lane & 15, lh = lane >> 4;   // ldmatrix: this lane's row and channel half
    const unsigned sbase = (unsigned)__cvta_generic_to_shared(sin);
-   const int sgn = transposed ? -1 : 1;
+   constexpr int sgn = TRANSPOSED ? -1 : 1;
+   // byte offsets: x part of this lane at hx = lr + dx + 1 (dx = -1, 0, 1), and of each row
+   unsigned xo[3];
+#pragma unroll
+   for (int d = 0; d < 3; ++d) {
+      const int hx = lr + d;
+      xo[d] = sbase + 16u * (unsigned)(2 * hx + (lh ^ ((hx >> 2) & 1)));
+   }
+   unsigned ro[DN_ROWS];
+#pragma unroll
+   for (int r = 0; r < DN_ROWS; ++r) {
+      const int row = warp * DN_ROWS + r, ry = row % DN_BY, rz = row / DN_BY;
+      ro[r] = 32u * (unsigned)(DN_HX * ((ry + 1) + DN_HY * (rz + 1)));
+   }
    float c[DN_ROWS][2][4];
 #pragma unroll
    for (int r = 0; r < DN_ROWS; ++r)
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) c[r][nt][0] = c[r][nt][1] = c[r][nt][2] = c[r][nt][3] = 0.f;
-#pragma unroll 1
+#pragma unroll
    for (int t = 0; t < DN_TAPS; ++t) {
       const int dx = sgn * (t % 3 - 1), dy = sgn * ((t / 3) % 3 - 1), dz = sgn * (t / 9 - 1);
+      const int tyz = 32 * DN_HX * (dy + DN_HY * dz);   // byte offset of the tap's y/z shift
       const unsigned* f = sfrag + (t * 2) * 64;
       const uint2 bf0 = *reinterpret_cast<const uint2*>(f + lane * 2);
       const uint2 bf1 = *reinterpret_cast<const uint2*>(f + 64 + lane * 2);
 #pragma unroll
       for (int r = 0; r < DN_ROWS; ++r) {
-         const int row = warp * DN_ROWS + r, ry = row % DN_BY, rz = row / DN_BY;
-         const int lv = (lr + dx + 1) + DN_HX * ((ry + dy + 1) + DN_HY * (rz + dz + 1));
-         const unsigned addr = sbase + 16u * (unsigned)dnSlot(lv, lh);
+         const unsigned addr = xo[dx + 1] + ro[r] + (unsigned)tyz;
          unsigned a[4];
          asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                       : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
@@ -206,6 +239,24 @@ k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias,
             if (nt == 0 && q < 2) {
                if (oka) { out32[va * 4 + ch] = x0v + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1v + res[va * 4 + ch + 1]; }
                if (okb) { out32[vb * 4 + ch] = x2v + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3v + res[vb * 4 + ch + 1]; }
+            }
+            continue;
+         }
+         if (mode == 4) {
+            // channels ch, ch + 1 of voxels va, vb: (rho, Jx) for q = 0, (Jy, Jz) for q = 1
+            if (nt == 0 && q < 2) {
+               double* p0 = q == 0 ? mom.rho : mom.J + mom.N;
+               double* p1 = q == 0 ? mom.J : mom.J + 2 * mom.N;
+               const double s0 = q == 0 ? mom.sr : mom.sj, rs0 = q == 0 ? mom.rsr : mom.rsj;
+               auto put = [&](long long v, float y0, float y1) {
+                  double r0 = (double)(y0 + (float)(p0[v] * rs0)) * s0;
+                  const double r1 = (double)(y1 + (float)(p1[v] * mom.rsj)) * mom.sj;
+                  if (q == 0 && r0 < mom.minRho) r0 = mom.minRho;
+                  p0[v] = r0;
+                  p1[v] = r1;
+               };
+               if (oka) put(va, x0v, x1v);
+               if (okb) put(vb, x2v, x3v);
             }
             continue;
          }
@@ -328,31 +379,13 @@ __global__ void k_dn_adam(float* p, const float* gr, float* m, float* v, const u
 }
 
 // planar FP64 moments (rho N, J 3N) -> normalized FP32 residual copy (N x 4) + BF16 input (16 channels)
-__global__ void k_dn_pack(long long N, const double* rho, const double* J, double sr, double sj, float* res,
-                          unsigned* act) {
+// normalized FP32 copy (N x 4) of planar FP64 moments: rho / sr and J / sj as
+// products with the reciprocals rsr = 1 / sr, rsj = 1 / sj
+__global__ void k_dn_norm(long long N, const double* rho, const double* J, double rsr, double rsj, float* out) {
    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (v >= N) return;
-   const float x0 = (float)(rho[v] / sr), x1 = (float)(J[v] / sj), x2 = (float)(J[N + v] / sj), x3 = (float)(J[2 * N + v] / sj);
-   res[v * 4 + 0] = x0; res[v * 4 + 1] = x1; res[v * 4 + 2] = x2; res[v * 4 + 3] = x3;
-   act[v * 8 + 0] = packBf16(x0, x1);
-   act[v * 8 + 1] = packBf16(x2, x3);
-   for (int u = 2; u < 8; ++u) act[v * 8 + u] = 0u;
-}
-// network output (normalized FP32, N x 4) -> planar FP64 moments, rho clamped as the deposit's finalize
-__global__ void k_dn_unpack(long long N, const float* out, double sr, double sj, double minRho, double* rho, double* J) {
-   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (v >= N) return;
-   double r = (double)out[v * 4] * sr;
-   if (r < minRho) r = minRho;
-   rho[v] = r;
-   for (int l = 0; l < 3; ++l) J[l * N + v] = (double)out[v * 4 + 1 + l] * sj;
-}
-// normalized FP32 copy (N x 4) of planar FP64 moments (training targets)
-__global__ void k_dn_norm(long long N, const double* rho, const double* J, double sr, double sj, float* out) {
-   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (v >= N) return;
-   out[v * 4] = (float)(rho[v] / sr);
-   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(J[l * N + v] / sj);
+   out[v * 4] = (float)(rho[v] * rsr);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(J[l * N + v] * rsj);
 }
 
 // FP32 normalized moments (N x 4) -> BF16 network input (16 channels)
@@ -393,14 +426,14 @@ __global__ void k_dn_subsample_deposit(GridInfo g, FastGeom fg, SegBuf B, const 
    }
 }
 // the deposit's finalize on the subsample sums: /dV, rho clamp, then normalized FP32 (N x 4)
-__global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double sr, double sj,
+__global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double rsr, double rsj,
                                       float* out) {
    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (v >= N) return;
    double r = acc[v] / dV;
    if (r < minRho) r = minRho;
-   out[v * 4] = (float)(r / sr);
-   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(acc[(1 + l) * N + v] / dV / sj);
+   out[v * 4] = (float)(r * rsr);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(acc[(1 + l) * N + v] / dV * rsj);
 }
 
 // squared-error sums for the relative L2 errors of one pair: per block

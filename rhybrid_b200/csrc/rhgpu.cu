@@ -1280,11 +1280,11 @@ int dnForward(rhgpu_dn* d) {
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[0], d->frag, b0, 0, 0, d->act[1], nullptr, nullptr, nullptr);
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, 0, d->act[2], nullptr,
-                                                              nullptr, nullptr);
-   k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 0, 3, nullptr,
-                                                              nullptr, d->out32, d->res);
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[0], d->frag, b0, 0, d->act[1], nullptr, nullptr, nullptr, DnMoments{});
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, d->act[2], nullptr,
+                                                              nullptr, nullptr, DnMoments{});
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 3, nullptr,
+                                                              nullptr, d->out32, d->res, DnMoments{});
    RH_CUDA(cudaGetLastError());
    return RHGPU_OK;
 }
@@ -1301,8 +1301,9 @@ int dnBackward(rhgpu_dn* d, const float* target, double* loss) {
       k_dn_bgrad<<<wb, 256, 0, d->stream>>>(d->g, d->dY[l], d->part);
       k_dn_reduce_rows<<<1, DN_C, 0, d->stream>>>(d->part, wb, DN_C, d->grad + (size_t)l * DN_LAYER + DN_TAPS * DN_C * DN_C);
       if (l > 0)
-         k_dn_conv<<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->dY[l], d->frag + (size_t)(3 + l) * DN_FRAG, nullptr, 1,
-                                                                    2, d->dY[l - 1], d->act[l], nullptr, nullptr);
+         k_dn_conv<true><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->dY[l], d->frag + (size_t)(3 + l) * DN_FRAG, nullptr,
+                                                                    2, d->dY[l - 1], d->act[l], nullptr, nullptr,
+                                                                    DnMoments{});
    }
    RH_CUDA(cudaGetLastError());
    std::vector<double> lp(DN_LOSS_BLOCKS);
@@ -1328,22 +1329,28 @@ int dnUploadMoments(rhgpu_dn* d, const double* rho, const double* ji, double* pl
 }
 
 
+// the network on planar device moments (rho N, J 3 x N), in place: the first layer
+// reads and normalizes them, the last adds its output to their normalized values
+// and scales back (rho clamped at minRho), in three launches
+int dnApplyMoments(rhgpu_dn* d, cudaStream_t st, double* rho, double* J, double minRho) {
+   const long long N = d->g.N;
+   const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N};
+   const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
+   const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
+   const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, nullptr, d->frag, b0, 0, d->act[1], nullptr, nullptr,
+                                                        nullptr, mom);
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, d->act[2], nullptr,
+                                                        nullptr, nullptr, DnMoments{});
+   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 4, nullptr,
+                                                        nullptr, nullptr, nullptr, mom);
+   return cudaGetLastError() != cudaSuccess ? fail(RHGPU_ERR_CUDA, "dn_apply: launch") : RHGPU_OK;
+}
+
 // the denoiser on the context's moments (device, on the context's stream), before the field update
 int dnApplyCtx(rhgpu_ctx* c) {
-   rhgpu_dn* d = c->dn;
    RH_TIME(c, "dn_apply");
-   const long long N = d->g.N;
-   cudaStream_t own = d->stream;
-   d->stream = c->stream;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, c->stream>>>(N, c->f.cellRho, c->f.cellJi, d->sr, d->sj, d->res);
-   int rc = dnForward(d);
-   if (!rc) {
-      k_dn_unpack<<<blocks1d(N, 256), 256, 0, c->stream>>>(N, d->out32, d->sr, d->sj, c->P.min_ion_charge_density,
-                                                           c->f.cellRho, c->f.cellJi);
-      if (cudaGetLastError() != cudaSuccess) rc = fail(RHGPU_ERR_CUDA, "dn_apply: launch");
-   }
-   d->stream = own;
-   return rc;
+   return dnApplyMoments(c->dn, c->stream, c->f.cellRho, c->f.cellJi, c->P.min_ion_charge_density);
 }
 
 }  // namespace
@@ -2066,11 +2073,8 @@ int rhgpu_dn_apply(rhgpu_dn* d, const double* rho_in, const double* ji_in, doubl
    const long long N = d->g.N;
    int rc = dnUploadMoments(d, rho_in, ji_in, d->acc);
    if (rc) return rc;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, d->sr, d->sj, d->res);
-   rc = dnForward(d);
+   rc = dnApplyMoments(d, d->stream, d->acc, d->acc + N, min_rho);
    if (rc) return rc;
-   k_dn_unpack<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->out32, d->sr, d->sj, min_rho, d->acc, d->acc + N);
-   RH_CUDA(cudaGetLastError());
    std::vector<double> h(4 * (size_t)N);
    RH_CUDA(cudaMemcpyAsync(h.data(), d->acc, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, d->stream));
    RH_CUDA(cudaStreamSynchronize(d->stream));
@@ -2088,13 +2092,13 @@ int rhgpu_dn_loss_grad(rhgpu_dn* d, const double* rho_in, const double* ji_in, c
    const long long N = d->g.N;
    int rc = dnUploadMoments(d, rho_t, ji_t, d->acc);
    if (rc) return rc;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, d->sr, d->sj, d->out32);
+   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->out32);
    // target kept in dY[0]'s storage as FP32 (N x 4 floats fit in 8 u32 per voxel)
    float* target = reinterpret_cast<float*>(d->dY[0]);
    RH_CUDA(cudaMemcpyAsync(target, d->out32, sizeof(float) * 4 * N, cudaMemcpyDeviceToDevice, d->stream));
    rc = dnUploadMoments(d, rho_in, ji_in, d->acc);
    if (rc) return rc;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, d->sr, d->sj, d->res);
+   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->res);
    rc = dnForward(d);
    if (rc) return rc;
    // the loss kernel reads the target before the backward overwrites dY[0]
@@ -2133,7 +2137,7 @@ int rhgpu_dn_add_pair(rhgpu_dn* d, rhgpu_ctx* c, int32_t factor, int32_t offset)
                                                                           c->sp[s].q, k, off, d->acc);
       }
       k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, c->g.dV, c->P.min_ion_charge_density,
-                                                                    d->sr, d->sj, pass == 0 ? in : tg);
+                                                                    1.0 / d->sr, 1.0 / d->sj, pass == 0 ? in : tg);
    }
    RH_CUDA(cudaGetLastError());
    RH_CUDA(cudaStreamSynchronize(d->stream));
