@@ -410,28 +410,20 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
    }
 }
 
-// per destination (species, segment): arrivals sorted by key, appended after the stayers
-__global__ void k_f32_mig_place(F32Set FS, long long NS, const Mover32* mv, int* inc, const long long* off,
-                                int* bucket, int* overflow) {
-   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (b >= (long long)FS.ns * NS) return;
-   const int k = inc[b];
-   if (k == 0) return;
+// mover order[q] to slot q - off[bucket] after its bucket's stayers (bucket nb: not placed)
+__global__ void k_f32_mig_place(F32Set FS, long long NS, long long nb, const Mover32* mv, const unsigned* order,
+                                const unsigned* bkt, const long long* off, long long n) {
+   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (q >= n) return;
+   const long long b = bkt[q];
+   if (b >= nb) return;
    const int s = (int)(b / NS);
    const long long S = b % NS;
-   int* bk = bucket + off[b];
-   for (int a = 1; a < k; ++a)
-      for (int c = a; c > 0 && mv[bk[c - 1]].key > mv[bk[c]].key; --c) { const int t = bk[c]; bk[c] = bk[c - 1]; bk[c - 1] = t; }
    const F32Species& SS = FS.st[s];
-   const long long pos = SS.base[S] + SS.nxt.cnt[S];
-   if (pos + k > SS.base[S + 1]) { atomicOr((unsigned*)overflow, 1u); return; }
-   for (int a = 0; a < k; ++a) {
-      const Mover32& M = mv[bk[a]];
-      SS.nxt.cell[pos + a] = M.cell;
-      for (int e = 0; e < 3; ++e) { SS.nxt.o[e][pos + a] = M.o[e]; SS.nxt.v[e][pos + a] = M.v[e]; }
-   }
-   SS.nxt.cnt[S] += k;
-   inc[b] = 0;
+   const long long pos = SS.base[S] + SS.nxt.cnt[S] + (q - off[b]);
+   const Mover32& M = mv[order[q]];
+   SS.nxt.cell[pos] = M.cell;
+   for (int e = 0; e < 3; ++e) { SS.nxt.o[e][pos] = M.o[e]; SS.nxt.v[e][pos] = M.v[e]; }
 }
 
 // CIC contributions of the particles that left their segment, exact fixed-point sums

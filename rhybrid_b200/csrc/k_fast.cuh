@@ -27,7 +27,7 @@
 //                        mover list.
 //   k_fast_mover_deposit the movers' CIC contributions as exact 128-bit
 //                        fixed-point sums (order-independent)
-//   k_fast_mig_*         placement of the movers after the stayers of their
+//   k_mig_*, k_fast_mig_place  placement of the movers after the stayers of their
 //                        destination segment, in (source segment, index) order
 //   k_fast_gather        cell moments from the four row partials (+ the segment
 //                        boundary partial) + the fixed-point part, then /dV and
@@ -576,14 +576,12 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
          }
       }
       __syncthreads();
+      long long slot = 0;   // next-buffer slot of a stayer (stored after the barrier)
       if (stay) {
          const int stayIdx = s_wcnt[warp] + __popc(bs & below);
          // stayers of the chunk before the first particle of this thread's species
          const int firstIdx = stayersIn(s_bs, 0, max(s_prefix[s], c0) - c0);
-         const SegSpecies& SS = FS.st[s];
-         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
-         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
-         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
+         slot = FS.st[s].base[S] + s_stay[s] + (stayIdx - firstIdx);
       }
       // stayers of species tid in this chunk
       const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
@@ -595,6 +593,11 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       __syncthreads();
       // running stayer count of each species (all reads of s_stay for this chunk are done)
       if (tid < ns) s_stay[tid] += stayAdd;
+      if (stay) {
+         const SegSpecies& SS = FS.st[s];
+         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
+         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
+      }
       // ---- sums of this thread's (dual cell, corner), records in list order ----------------
       {
          const int r1 = s_bin[myDual + 1];
@@ -711,37 +714,78 @@ __global__ void k_fast_mig_count(const MV* mv, long long n, long long NS, int* i
    if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    atomicAdd(&inc[(long long)mv[t].species * NS + mv[t].dest], 1);
 }
+// Placement order of the arrivals of a destination (species, segment) bucket:
+// by mover key (source segment, index in it). The movers are sorted by key and
+// then, stably, by bucket (radix sorts on the host side); these kernels prepare
+// the sort keys, check the room of every bucket, place the movers (one thread
+// each) after the bucket's stayers, and add the arrivals to the counts.
 template <class MV>
-__global__ void k_fast_mig_bucket(const MV* mv, long long n, long long NS, const long long* off, int* fill, int* bucket) {
+__global__ void k_mig_sort_keys(const MV* mv, long long n, long long NS, long long nb, unsigned long long* key,
+                                unsigned* val, unsigned* bkt) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= n) return;
+   key[t] = mv[t].key;
+   val[t] = (unsigned)t;
+   bkt[t] = (mv[t].lx & MOVER_PLACE) ? (unsigned)((long long)mv[t].species * NS + mv[t].dest) : (unsigned)nb;
+}
+template <class SET>
+__global__ void k_mig_check(SET FS, long long NS, const int* inc, int* overflow) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b >= (long long)FS.ns * NS || inc[b] == 0) return;
+   const int s = (int)(b / NS);
+   const long long S = b % NS;
+   if (FS.st[s].base[S] + FS.st[s].nxt.cnt[S] + inc[b] > FS.st[s].base[S + 1]) atomicOr((unsigned*)overflow, 1u);
+}
+template <class SET>
+__global__ void k_mig_counts(SET FS, long long NS, int* inc) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b >= (long long)FS.ns * NS || inc[b] == 0) return;
+   FS.st[(int)(b / NS)].nxt.cnt[b % NS] += inc[b];
+   inc[b] = 0;
+}
+// small buckets: the arrivals of each bucket listed (in any order) at off[b] by
+// k_mig_bucket, then one thread per bucket orders them by key (insertion sort)
+// into order[], the same order as the sorts
+template <class MV>
+__global__ void k_mig_bucket(const MV* mv, long long n, long long NS, const long long* off, int* fill,
+                             unsigned* list) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t >= n || !(mv[t].lx & MOVER_PLACE)) return;
    const long long b = (long long)mv[t].species * NS + mv[t].dest;
    const int k = atomicAdd(&fill[b], 1);
-   bucket[off[b] + k] = (int)t;
+   list[off[b] + k] = (unsigned)t;
 }
-// per destination (species, segment): arrivals sorted by key, appended after the
-// stayers; sets *overflow and places nothing if they do not fit
-__global__ void k_fast_mig_place(FastSpecies FS, long long NS, const Mover* mv, int* inc, const long long* off,
-                                 int* bucket, int* overflow) {
+template <class MV>
+__global__ void k_mig_order_small(const MV* mv, long long nb, const int* inc, const long long* off, unsigned* list,
+                                  unsigned* bkt) {
    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (b >= (long long)FS.ns * NS) return;
+   if (b >= nb) return;
    const int k = inc[b];
-   if (k == 0) return;
+   unsigned* bk = list + off[b];
+   for (int a = 1; a < k; ++a) {
+      const unsigned t = bk[a];
+      const unsigned long long key = mv[t].key;
+      int c = a;
+      for (; c > 0 && mv[bk[c - 1]].key > key; --c) bk[c] = bk[c - 1];
+      bk[c] = t;
+   }
+   for (int a = 0; a < k; ++a) bkt[off[b] + a] = (unsigned)b;
+}
+
+// mover order[q] to slot q - off[bucket] after its bucket's stayers (bucket nb: not placed)
+__global__ void k_fast_mig_place(FastSpecies FS, long long NS, long long nb, const Mover* mv, const unsigned* order,
+                                 const unsigned* bkt, const long long* off, long long n) {
+   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (q >= n) return;
+   const long long b = bkt[q];
+   if (b >= nb) return;
    const int s = (int)(b / NS);
    const long long S = b % NS;
-   int* bk = bucket + off[b];
-   for (int a = 1; a < k; ++a)
-      for (int c = a; c > 0 && mv[bk[c - 1]].key > mv[bk[c]].key; --c) { const int t = bk[c]; bk[c] = bk[c - 1]; bk[c - 1] = t; }
    const SegSpecies& SS = FS.st[s];
-   const long long pos = SS.base[S] + SS.nxt.cnt[S];
-   if (pos + k > SS.base[S + 1]) { atomicOr((unsigned*)overflow, 1u); return; }
-   for (int a = 0; a < k; ++a) {
-      const Mover& M = mv[bk[a]];
-      for (int e = 0; e < 7; ++e) SS.nxt.a[e][pos + a] = M.s[e];
-      SS.nxt.lx[pos + a] = (unsigned char)(M.lx & 0xff);
-   }
-   SS.nxt.cnt[S] += k;
-   inc[b] = 0;
+   const long long pos = SS.base[S] + SS.nxt.cnt[S] + (q - off[b]);
+   const Mover& M = mv[order[q]];
+   for (int e = 0; e < 7; ++e) SS.nxt.a[e][pos] = M.s[e];
+   SS.nxt.lx[pos] = (unsigned char)(M.lx & 0xff);
 }
 
 // ---- upload / download / relayout support -----------------------------------------------------

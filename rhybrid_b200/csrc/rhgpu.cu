@@ -7,6 +7,7 @@
 // boundary conditions) and k_fields.cuh (propagateB).
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_reduce.cuh>
 
 #include <cmath>
 #include <cstdio>
@@ -193,8 +194,12 @@ struct rhgpu_ctx {
    SegHost seg[MAX_SPECIES];
    FastBufs fb = {};
    int* finc = nullptr;                 // arrivals per (species, segment)
-   int* ffill = nullptr;
-   int* fbucket = nullptr;
+   unsigned long long* mkey = nullptr;  // migration sort: 2 x mcap mover keys
+   unsigned* mval = nullptr;            // 2 x mcap mover indices
+   unsigned* mbkt = nullptr;            // 2 x mcap destination buckets
+   long long mcap = 0;
+   int* ffill = nullptr;                // ns*NS fill counters of the small-bucket placement
+   int* fmaxInc = nullptr;              // largest arrivals of a bucket
    int* fover = nullptr;                // 16 bytes
    int kR = 0, kJ = 0;
    void* sortTmp = nullptr;
@@ -625,6 +630,19 @@ int fastExponents(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+// sort buffers of the migration for up to `want` movers
+int ensureMigBuffers(rhgpu_ctx* c, long long want) {
+   if (want <= c->mcap) return RHGPU_OK;
+   cudaFree(c->mkey); cudaFree(c->mval); cudaFree(c->mbkt);
+   c->mkey = nullptr; c->mval = nullptr; c->mbkt = nullptr;
+   c->mcap = 0;
+   RH_CUDA(cudaMalloc(&c->mkey, sizeof(unsigned long long) * 2 * want));
+   RH_CUDA(cudaMalloc(&c->mval, sizeof(unsigned) * 2 * want));
+   RH_CUDA(cudaMalloc(&c->mbkt, sizeof(unsigned) * 2 * want));
+   c->mcap = want;
+   return RHGPU_OK;
+}
+
 // mover list: a quarter of all slots (at least 2^20)
 int fastMoverBuffers(rhgpu_ctx* c) {
    long long tot = 0;
@@ -632,15 +650,12 @@ int fastMoverBuffers(rhgpu_ctx* c) {
    const long long want = std::max(1LL << 20, tot / 4);
    if (want > c->fb.moverCap) {
       cudaFree(c->fb.movers);
-      cudaFree(c->fbucket);
       c->fb.movers = nullptr;
-      c->fbucket = nullptr;
       c->fb.moverCap = 0;
       RH_CUDA(cudaMalloc(&c->fb.movers, sizeof(Mover) * want));
-      RH_CUDA(cudaMalloc(&c->fbucket, sizeof(int) * want));
       c->fb.moverCap = want;
    }
-   return RHGPU_OK;
+   return ensureMigBuffers(c, want);
 }
 
 __global__ void k_iota(unsigned* v, long long n) {
@@ -651,6 +666,90 @@ __global__ void k_int_to64(const int* in, long long n, long long* out) {
    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (t < n) out[t] = in[t];
    if (t == n) out[n] = 0;
+}
+
+__global__ void k_fill_u32(unsigned* a, long long n, unsigned v) {
+   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (p < n) a[p] = v;
+}
+__global__ void k_gather_u32(const unsigned* src, const unsigned* idx, long long n, unsigned* dst) {
+   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (p < n) dst[p] = src[idx[p]];
+}
+
+int bitsFor(long long x) {
+   int b = 1;
+   while (b < 63 && (x >> b) != 0) ++b;
+   return b;
+}
+
+// the arrivals of the nm movers: per destination (species, segment) bucket the
+// count (c->finc) and first position (c->foffInc), the movers sorted by bucket
+// and within it by key (*order, *bucket; bucket ns*NS = not placed), and
+// whether some bucket lacks room (*over). Buckets of at most MIG_SMALL arrivals
+// (the usual case) are ordered one thread per bucket; otherwise two stable
+// radix sorts over all movers (by key, then by bucket) give the same order.
+const int MIG_SMALL = 64;
+template <class MV, class SET>
+int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** order, unsigned** bucket, int* over) {
+   const long long NS = c->fg.NS, nb = (long long)c->ns * NS;
+   if (nm > c->mcap) return fail(RHGPU_ERR_CAPACITY, "mover list larger than its sort buffers");
+   RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+   k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(mv, nm, NS, c->finc);
+   RH_LAUNCHED(c);
+   k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
+   RH_LAUNCHED(c);
+   size_t bytes = c->scanTmpBytes;
+   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
+   unsigned long long *kA = c->mkey, *kB = c->mkey + c->mcap;
+   unsigned *vA = c->mval, *vB = c->mval + c->mcap, *bA = c->mbkt, *bB = c->mbkt + c->mcap;
+   size_t mb = 0;
+   cub::DeviceReduce::Max(nullptr, mb, c->finc, c->fmaxInc, (int)nb, c->stream);
+   int rc = ensureSortTmp(c, mb);
+   if (rc) return rc;
+   mb = c->sortTmpBytes;
+   RH_CUDA(cub::DeviceReduce::Max(c->sortTmp, mb, c->finc, c->fmaxInc, (int)nb, c->stream));
+   int maxInc = 0;
+   RH_CUDA(cudaMemcpyAsync(&maxInc, c->fmaxInc, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   if (maxInc <= MIG_SMALL) {
+      // buckets past the placed movers stay at nb (not placed)
+      RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
+      k_fill_u32<<<blocks1d(nm, 256), 256, 0, c->stream>>>(bA, nm, (unsigned)nb);
+      k_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(mv, nm, NS, c->foffInc, c->ffill, vA);
+      RH_LAUNCHED(c);
+      k_mig_order_small<<<blocks1d(nb, 256), 256, 0, c->stream>>>(mv, nb, c->finc, c->foffInc, vA, bA);
+      RH_LAUNCHED(c);
+      k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(FS, NS, c->finc, c->fover);
+      RH_LAUNCHED(c);
+      RH_CUDA(cudaMemcpyAsync(over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+      *order = vA;
+      *bucket = bA;
+      return RHGPU_OK;
+   }
+   k_mig_sort_keys<<<blocks1d(nm, 256), 256, 0, c->stream>>>(mv, nm, NS, nb, kA, vA, bA);
+   RH_LAUNCHED(c);
+   const int kbits = 32 + bitsFor(NS > 1 ? NS - 1 : 1), bbits = bitsFor(nb);
+   size_t s1 = 0, s2 = 0;
+   cub::DeviceRadixSort::SortPairs(nullptr, s1, kA, kB, vA, vB, (int)nm, 0, kbits, c->stream);
+   cub::DeviceRadixSort::SortPairs(nullptr, s2, bB, bA, vB, vA, (int)nm, 0, bbits, c->stream);
+   rc = ensureSortTmp(c, std::max(s1, s2));
+   if (rc) return rc;
+   size_t sb = c->sortTmpBytes;
+   RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, kA, kB, vA, vB, (int)nm, 0, kbits, c->stream));
+   k_gather_u32<<<blocks1d(nm, 256), 256, 0, c->stream>>>(bA, vB, nm, bB);
+   RH_LAUNCHED(c);
+   sb = c->sortTmpBytes;
+   RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, bB, bA, vB, vA, (int)nm, 0, bbits, c->stream));
+   k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(FS, NS, c->finc, c->fover);
+   RH_LAUNCHED(c);
+   RH_CUDA(cudaMemcpyAsync(over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   *order = vA;
+   *bucket = bA;
+   return RHGPU_OK;
 }
 
 // exclusive prefix of a per-segment count array (NS+1 entries into c->ffirst); returns the total
@@ -836,36 +935,25 @@ int fastPush(rhgpu_ctx* c) {
       int over = 0;
       {
          RH_TIME(c, "fast_migrate");
-         RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
-         RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
-         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-         k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, NS, c->finc);
-         RH_LAUNCHED(c);
-         k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
-         RH_LAUNCHED(c);
-         size_t bytes = c->scanTmpBytes;
-         RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
-         k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->fb.movers, nm, NS, c->foffInc, c->ffill,
-                                                                     c->fbucket);
-         RH_LAUNCHED(c);
-         k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->fb.movers, c->finc,
-                                                                    c->foffInc, c->fbucket, c->fover);
-         RH_LAUNCHED(c);
-         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-      }
-      RH_CUDA(cudaStreamSynchronize(c->stream));
-      if (over) {
-         // some segments lack room for their arrivals: relayout with room, place the rest
-         RH_TIME(c, "fast_relayout");
-         int rc = fastRelayoutNext(c);
+         unsigned *order = nullptr, *bkt = nullptr;
+         int rc = migSort(c, c->fb.movers, (long long)nm, fastSpecies(c), &order, &bkt, &over);
          if (rc) return rc;
-         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-         k_fast_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->fb.movers, c->finc,
-                                                                    c->foffInc, c->fbucket, c->fover);
+         if (over) {
+            // some segments lack room for their arrivals: relayout with room for them
+            rc = fastRelayoutNext(c);
+            if (rc) return rc;
+            RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+            k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->finc, c->fover);
+            RH_LAUNCHED(c);
+            RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            RH_CUDA(cudaStreamSynchronize(c->stream));
+            if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+         }
+         k_fast_mig_place<<<blocks1d(nm, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, nb, c->fb.movers, order, bkt, c->foffInc,
+                                                                 (long long)nm);
          RH_LAUNCHED(c);
-         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-         RH_CUDA(cudaStreamSynchronize(c->stream));
-         if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+         k_mig_counts<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->finc);
+         RH_LAUNCHED(c);
       }
    }
    for (int s = 0; s < c->ns; ++s) c->seg[s].cur ^= 1;
@@ -1005,16 +1093,12 @@ int f32MoverBuffers(rhgpu_ctx* c) {
    const long long want = std::max(1LL << 20, tot / 4);
    if (want > c->f32b.moverCap) {
       cudaFree(c->f32b.movers);
-      cudaFree(c->fbucket);
       c->f32b.movers = nullptr;
-      c->fbucket = nullptr;
       c->f32b.moverCap = 0;
-      c->fb.moverCap = 0;
       RH_CUDA(cudaMalloc(&c->f32b.movers, sizeof(Mover32) * want));
-      RH_CUDA(cudaMalloc(&c->fbucket, sizeof(int) * want));
       c->f32b.moverCap = want;
    }
-   return RHGPU_OK;
+   return ensureMigBuffers(c, want);
 }
 
 int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n) {
@@ -1200,35 +1284,25 @@ int f32Push(rhgpu_ctx* c) {
       int over = 0;
       {
          RH_TIME(c, "f32_migrate");
-         RH_CUDA(cudaMemsetAsync(c->finc, 0, sizeof(int) * nb, c->stream));
-         RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
-         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-         k_fast_mig_count<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->f32b.movers, nm, NS, c->finc);
-         RH_LAUNCHED(c);
-         k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
-         RH_LAUNCHED(c);
-         size_t bytes = c->scanTmpBytes;
-         RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
-         k_fast_mig_bucket<<<blocks1d(nm, 256), 256, 0, c->stream>>>(c->f32b.movers, nm, NS, c->foffInc, c->ffill,
-                                                                     c->fbucket);
-         RH_LAUNCHED(c);
-         k_f32_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->f32b.movers, c->finc, c->foffInc,
-                                                                   c->fbucket, c->fover);
-         RH_LAUNCHED(c);
-         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-      }
-      RH_CUDA(cudaStreamSynchronize(c->stream));
-      if (over) {
-         RH_TIME(c, "f32_relayout");
-         rc = f32RelayoutNext(c);
+         unsigned *order = nullptr, *bkt = nullptr;
+         int rc = migSort(c, c->f32b.movers, (long long)nm, f32Set(c), &order, &bkt, &over);
          if (rc) return rc;
-         RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
-         k_f32_mig_place<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->f32b.movers, c->finc, c->foffInc,
-                                                                   c->fbucket, c->fover);
+         if (over) {
+            // some segments lack room for their arrivals: relayout with room for them
+            rc = f32RelayoutNext(c);
+            if (rc) return rc;
+            RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
+            k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->finc, c->fover);
+            RH_LAUNCHED(c);
+            RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            RH_CUDA(cudaStreamSynchronize(c->stream));
+            if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+         }
+         k_f32_mig_place<<<blocks1d(nm, 256), 256, 0, c->stream>>>(f32Set(c), NS, nb, c->f32b.movers, order, bkt, c->foffInc,
+                                                                 (long long)nm);
          RH_LAUNCHED(c);
-         RH_CUDA(cudaMemcpyAsync(&over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-         RH_CUDA(cudaStreamSynchronize(c->stream));
-         if (over) return fail(RHGPU_ERR_CAPACITY, "segment relayout did not make room");
+         k_mig_counts<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->finc);
+         RH_LAUNCHED(c);
       }
    }
    for (int s = 0; s < c->ns; ++s) c->f32[s].cur ^= 1;
@@ -1447,6 +1521,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->fb.nmovers, sizeof(unsigned long long));
    alloc((void**)&c->finc, sizeof(int) * nb);
    alloc((void**)&c->ffill, sizeof(int) * nb);
+   alloc((void**)&c->fmaxInc, sizeof(int));
    alloc((void**)&c->fcap, sizeof(long long) * (NS + 1));
    alloc((void**)&c->ffirst, sizeof(long long) * (NS + 1));
    alloc((void**)&c->ftmp64, sizeof(long long) * (NS + 1));
@@ -1529,7 +1604,8 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    }
    cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
    cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
-   cudaFree(c->finc); cudaFree(c->ffill); cudaFree(c->fbucket); cudaFree(c->fover);
+   cudaFree(c->finc); cudaFree(c->fover); cudaFree(c->ffill); cudaFree(c->fmaxInc);
+   cudaFree(c->mkey); cudaFree(c->mval); cudaFree(c->mbkt);
    cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
    cudaFree(c->ftmpInc64); cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots); cudaFree(c->flxTmp);
    cudaFree(c->diagPart);
