@@ -351,7 +351,9 @@ k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F
       __syncthreads();
       if (stay) {
          const int stayIdx = s_wcnt[warp] + __popc(bs & below);
-         const int firstIdx = stayersIn(s_bs, 0, max(s_prefix[s], c0) - c0);
+         // (zero unless the species starts inside this chunk)
+         const int p0 = s_prefix[s] - c0;
+         const int firstIdx = p0 > 0 ? stayersIn(s_bs, 0, p0) : 0;
          const F32Species& SS = FS.st[s];
          const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
          SS.nxt.cell[slot] = (int)cidx(g, ti, tj, tk);

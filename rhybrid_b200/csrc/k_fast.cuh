@@ -580,7 +580,9 @@ k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParam
       if (stay) {
          const int stayIdx = s_wcnt[warp] + __popc(bs & below);
          // stayers of the chunk before the first particle of this thread's species
-         const int firstIdx = stayersIn(s_bs, 0, max(s_prefix[s], c0) - c0);
+         // (zero unless the species starts inside this chunk)
+         const int p0 = s_prefix[s] - c0;
+         const int firstIdx = p0 > 0 ? stayersIn(s_bs, 0, p0) : 0;
          slot = FS.st[s].base[S] + s_stay[s] + (stayIdx - firstIdx);
       }
       // stayers of species tid in this chunk
