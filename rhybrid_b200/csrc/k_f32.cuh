@@ -175,9 +175,16 @@ __device__ inline void cicWeightsF(const float o[3], float wq, float w8[8]) {
 
 constexpr int REC32 = 11;   // floats per deposit record: w8[8], v[3]
 
+// PER: the periodic axes (bit a = axis a), fixed at compile time; the host
+// launches the instantiation that matches the grid
+template <int PER>
 __global__ void __launch_bounds__(FT, 4)
-k_f32_push_deposit(GridInfo g, Fields f, FastGeom fg, F32Set FS, F32Params pp, F32Bufs fb, double* cntd,
+k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp, F32Bufs fb, double* cntd,
                    unsigned long long* cntu, unsigned* err) {
+   GridInfo g = gIn;
+   g.per[0] = PER & 1;
+   g.per[1] = (PER >> 1) & 1;
+   g.per[2] = (PER >> 2) & 1;
    __shared__ float s_rec[FT * REC32];            // deposit records of a chunk; at the end acc[SEG][32]
    __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
    __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell

@@ -398,9 +398,16 @@ __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const Species
    return clamp;
 }
 
+// PER: the periodic axes (bit a = axis a), fixed at compile time; the host
+// launches the instantiation that matches the grid
+template <int PER>
 __global__ void __launch_bounds__(FT, 4)
-k_fast_push_deposit(GridInfo g, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
+k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
+   GridInfo g = gIn;
+   g.per[0] = PER & 1;
+   g.per[1] = (PER >> 1) & 1;
+   g.per[2] = (PER >> 2) & 1;
    __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
    __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
    __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell

@@ -630,6 +630,9 @@ int fastExponents(rhgpu_ctx* c) {
    return RHGPU_OK;
 }
 
+// the periodic axes of a grid as a 3-bit mask (bit a = axis a)
+int perMask(const GridInfo& g) { return (g.per[0] ? 1 : 0) | (g.per[1] ? 2 : 0) | (g.per[2] ? 4 : 0); }
+
 // sort buffers of the migration for up to `want` movers
 int ensureMigBuffers(rhgpu_ctx* c, long long want) {
    if (want <= c->mcap) return RHGPU_OK;
@@ -917,8 +920,16 @@ int fastPush(rhgpu_ctx* c) {
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "fast_push_deposit");
-      k_fast_push_deposit<<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, fastSpecies(c), pp, c->fb, c->cntD,
-                                                             c->cntU, c->err);
+      const FastSpecies FS = fastSpecies(c);
+      switch (perMask(c->g)) {
+#define RH_FAST_PD(M)                                                                                           \
+   case M:                                                                                                        \
+      k_fast_push_deposit<M><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, c->cntU, \
+                                                                 c->err);                                        \
+      break;
+         RH_FAST_PD(0) RH_FAST_PD(1) RH_FAST_PD(2) RH_FAST_PD(3) RH_FAST_PD(4) RH_FAST_PD(5) RH_FAST_PD(6) RH_FAST_PD(7)
+#undef RH_FAST_PD
+      }
       RH_LAUNCHED(c);
    }
    unsigned long long nm = 0;
@@ -1266,8 +1277,17 @@ int f32Push(rhgpu_ctx* c) {
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "f32_push_deposit");
-      k_f32_push_deposit<<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, f32Set(c), f32Params(c), c->f32b, c->cntD,
-                                                            c->cntU, c->err);
+      const F32Set FS = f32Set(c);
+      const F32Params FP = f32Params(c);
+      switch (perMask(c->g)) {
+#define RH_F32_PD(M)                                                                                            \
+   case M:                                                                                                        \
+      k_f32_push_deposit<M><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, FP, c->f32b, c->cntD, c->cntU, \
+                                                                c->err);                                         \
+      break;
+         RH_F32_PD(0) RH_F32_PD(1) RH_F32_PD(2) RH_F32_PD(3) RH_F32_PD(4) RH_F32_PD(5) RH_F32_PD(6) RH_F32_PD(7)
+#undef RH_F32_PD
+      }
       RH_LAUNCHED(c);
    }
    unsigned long long nm = 0;
