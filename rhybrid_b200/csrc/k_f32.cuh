@@ -230,7 +230,6 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       long long p = 0;
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0, vx = 0, vy = 0, vz = 0, ti = 0, tj = 0, tk = 0;
-      float w8[8];
       if (active) {
          const F32Species& SS = FS.st[s];
          p = i - s_prefix[s];
@@ -264,8 +263,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
             const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.accumulate[s]) {
                if (inSeg) {
-                  cicWeightsF(o, FS.wqRel[s], w8);
-                  rec = true;
+                  rec = true;   // its CIC weights are formed just before the record is written
                } else {
                   mflags |= MOVER_DEPOSIT;
                }
@@ -368,6 +366,8 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       }
       const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
       if (rec) {
+         float w8[8];
+         cicWeightsF(o, FS.wqRel[s], w8);
          float* r = s_rec + (s_wd[warp][rd] + rrank) * REC32;
          for (int q = 0; q < 8; ++q) r[q] = w8[q];
          r[8] = v[0]; r[9] = v[1]; r[10] = v[2];

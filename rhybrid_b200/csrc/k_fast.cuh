@@ -452,7 +452,6 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0;
       int vx = 0, vy = 0, vz = 0;
-      double w8[8];
       long long p = 0;
       if (active) {
          const SegSpecies& SS = FS.st[s];
@@ -486,8 +485,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
             const bool inSeg = vy == uy && vz == uz && vx >= u0 && vx < u1;
             if (FS.sp[s].accumulate) {
                if (inSeg) {
-                  cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
-                  rec = true;
+                  rec = true;   // its CIC weights are formed just before the record is written
                } else {
                   mflags |= MOVER_DEPOSIT;   // deposited by k_fast_mover_deposit
                }
@@ -595,6 +593,8 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       // stayers of species tid in this chunk
       const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
       if (rec) {
+         double w8[8];
+         cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
          double* r = s_rec + (s_wd[warp][rd] + rrank) * REC;
          for (int o = 0; o < 8; ++o) r[o] = w8[o];
          r[8] = st[3]; r[9] = st[4]; r[10] = st[5];
