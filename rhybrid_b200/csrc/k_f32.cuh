@@ -376,6 +376,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       if (tid < ns) s_stay[tid] += stayAdd;
       {
          const int r1 = s_bin[myDual + 1];
+#pragma unroll 2
          for (int r = s_bin[myDual]; r < r1; ++r) {
             const float* rr = s_rec + r * REC32;
             const float w = rr[myCorner];

@@ -610,6 +610,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       // ---- sums of this thread's (dual cell, corner), records in list order ----------------
       {
          const int r1 = s_bin[myDual + 1];
+#pragma unroll 2
          for (int r = s_bin[myDual]; r < r1; ++r) {
             const double* rr = s_rec + r * REC;
             const double w = rr[myCorner];
