@@ -409,9 +409,8 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
    g.per[1] = (PER >> 1) & 1;
    g.per[2] = (PER >> 2) & 1;
    __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
-   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
-   __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell
-   __shared__ int s_wcnt[FW];                     // stayers per warp, then the stayers of the warps before
+   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell)
+   __shared__ int s_wcnt[FW];                     // stayers per warp
    __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
    __shared__ int s_stay[FAST_MAX_SPECIES];
    __shared__ unsigned s_bs[FW];                  // stayer ballot of each warp
@@ -533,30 +532,32 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
          if (rrank == 0) s_wd[warp][rd] = __popc(mm);
       }
       __syncthreads();
-      if (warp == 0) {
-         // per dual cell (lane): first sorted record of the dual cell and of each
-         // warp's records for it; stayers of the warps before each warp
-         int t = 0;
-         int c[FW];
-         for (int w = 0; w < FW; ++w) { c[w] = s_wd[w][lane]; t += c[w]; }
+      // every warp, per dual cell (lane): the first sorted record of the dual cell
+      // (bin) and of this warp's records for it (off)
+      int binD, offD, total;
+      {
+         int t = 0, before = 0;
+#pragma unroll
+         for (int w = 0; w < FW; ++w) {
+            const int cw = s_wd[w][lane];
+            t += cw;
+            if (w < warp) before += cw;
+         }
          int x = t;
          for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
          }
-         int b = x - t;
-         s_bin[lane] = b;
-         if (lane == 31) s_bin[SEG] = x;
-         for (int w = 0; w < FW; ++w) { s_wd[w][lane] = b; b += c[w]; }
-         const int sw = lane < FW ? s_wcnt[lane] : 0;
-         int xs = sw;
-         for (int o = 1; o < FW; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, xs, o);
-            if (lane >= o) xs += y;
-         }
-         __syncwarp();
-         if (lane < FW) s_wcnt[lane] = xs - sw;
+         binD = x - t;
+         offD = binD + before;
+         total = __shfl_sync(0xffffffffu, x, 31);
       }
+      const int recPos = __shfl_sync(0xffffffffu, offD, rd) + rrank;
+      const int sumLo = __shfl_sync(0xffffffffu, binD, myDual);
+      const int sumHiN = __shfl_sync(0xffffffffu, binD, (myDual + 1) & 31);
+      const int sumHi = myDual == SEG - 1 ? total : sumHiN;
+      // stayers of the warps before this one
+      const int stayBefore = (int)__reduce_add_sync(0xffffffffu, (unsigned)(lane < warp ? s_wcnt[lane] : 0));
       {
          const unsigned lm = __ballot_sync(0xffffffffu, leave);
          if (lm) {
@@ -580,10 +581,9 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
             }
          }
       }
-      __syncthreads();
       long long slot = 0;   // next-buffer slot of a stayer (stored after the barrier)
       if (stay) {
-         const int stayIdx = s_wcnt[warp] + __popc(bs & below);
+         const int stayIdx = stayBefore + __popc(bs & below);
          // stayers of the chunk before the first particle of this thread's species
          // (zero unless the species starts inside this chunk)
          const int p0 = s_prefix[s] - c0;
@@ -595,7 +595,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       if (rec) {
          double w8[8];
          cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
-         double* r = s_rec + (s_wd[warp][rd] + rrank) * REC;
+         double* r = s_rec + recPos * REC;
          for (int o = 0; o < 8; ++o) r[o] = w8[o];
          r[8] = st[3]; r[9] = st[4]; r[10] = st[5];
       }
@@ -608,17 +608,14 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
          SS.nxt.lx[slot] = (unsigned char)(vx - u0);
       }
       // ---- sums of this thread's (dual cell, corner), records in list order ----------------
-      {
-         const int r1 = s_bin[myDual + 1];
 #pragma unroll 2
-         for (int r = s_bin[myDual]; r < r1; ++r) {
-            const double* rr = s_rec + r * REC;
-            const double w = rr[myCorner];
-            a0 += w;
-            a1 += w * rr[8];
-            a2 += w * rr[9];
-            a3 += w * rr[10];
-         }
+      for (int r = sumLo; r < sumHi; ++r) {
+         const double* rr = s_rec + r * REC;
+         const double w = rr[myCorner];
+         a0 += w;
+         a1 += w * rr[8];
+         a2 += w * rr[9];
+         a3 += w * rr[10];
       }
       // no barrier here: the next chunk's first barrier orders these reads before
       // its record writes
