@@ -222,8 +222,8 @@ KERNEL_BYTES = {
 # proportion with the number of particles and cells.
 KERNEL_TRAFFIC = {
     # kernel: (traffic bytes, particles, cells) of the captured launch
-    "fast_push_deposit": (262.132736e6 + 222.141952e6, 4080025, 44 * 59 * 59),
-    "f32_push_deposit": (142.863360e6 + 88.712704e6, 4080025, 44 * 59 * 59),
+    "fast_push_deposit": (261.331456e6 + 215.268096e6, 4080025, 44 * 59 * 59),
+    "f32_push_deposit": (142.888704e6 + 89.759744e6, 4080025, 44 * 59 * 59),
 }
 
 
