@@ -74,7 +74,7 @@ def step_time(lib, cfg: cf.Config, steps: int, dn=None, path: int = abi.PATH_FAS
         ctx.close()
 
 
-def run(scale: float = 0.05, train_steps: int = 8, iters: int = 80, lr: float = 2e-3, timed_steps: int = 5,
+def run(scale: float = 0.05, train_steps: int = 8, iters: int = 160, lr: float = 2e-3, timed_steps: int = 5,
         judge_ppc: int = 256):
     lib = abi.gpu_library()
     judge = mars_at(float(judge_ppc), scale)
@@ -157,7 +157,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--scale", type=float, default=0.05)
     ap.add_argument("--judge-ppc", type=int, default=256)
-    ap.add_argument("--iters", type=int, default=80, help="Adam steps per training step")
+    ap.add_argument("--iters", type=int, default=160, help="Adam steps per training step")
     ap.add_argument("--json", default=None)
     a = ap.parse_args(argv)
     out = run(scale=a.scale, judge_ppc=a.judge_ppc, iters=a.iters)
