@@ -61,6 +61,7 @@ extern "C" {
 #define RHGPU_DEVERR_NAN_PARTICLE   1u  /* non-finite particle coordinate after the push */
 #define RHGPU_DEVERR_FAST_PARTICLE  2u  /* particle moved more than one cell in a step */
 #define RHGPU_DEVERR_CAPACITY       4u  /* particle buffer overflow during migration */
+#define RHGPU_DEVERR_INJECT         8u  /* a particle source's rejection sampling ran out of tries */
 
 /* per-cell flag bits of the cell_flags array (user.cpp:1883-1941) */
 #define RHGPU_FLAG_INNER_FIELD     1u  /* innerFlagField: cell centre inside R_fieldObstacle */
@@ -286,6 +287,43 @@ int rhgpu_set_denoiser(rhgpu_ctx* ctx, rhgpu_dn* dn, int32_t enabled);
 int rhgpu_dn_pair_error(rhgpu_dn* dn, int32_t pair, double* out4);
 /* pairs stored and the index of the newest */
 int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
+
+/* Particle sources, the reference's injectors (src/particle_injector.cpp), on
+ * the GPU: after the boundary conditions of every step (src/user.cpp:119-122)
+ * each injection cell draws probRound(N) new macroparticles from a
+ * counter-based stream (Philox-4x32-10 keyed by `seed`, the step and the
+ * cell), so a run is reproducible and independent of thread order; they are
+ * stored like particles arriving from another segment and deposit from the
+ * next step on, as in the reference. Fast and FP32 paths only.
+ *   RHGPU_INJECT_SOLARWIND (InjectorSolarWind, :517-730): `velocity` has one
+ *     non-zero component U; the cells of the upstream outer wall that have
+ *     both neighbours along the other axes get N = ppc |U| dt / dx per step
+ *     at the wall face, the normal velocity from the flux of a drifting
+ *     Maxwellian (sampleDerivGaussian) and Gaussian tangential velocities.
+ *   RHGPU_INJECT_FLOW (InjectorFlow, :734-945): every cell of the walls in
+ *     `inflow_walls` (bit 0 +x, 1 -x, 2 +y, 3 -y, 4 +z, 5 -z) gets N = ppc
+ *     per step, uniform in the cell, velocity + Gaussian thermal velocity.
+ * Weight n dx^3 / ppc, thermal speed sqrt(k_B T / m) with the species' mass.
+ * n == 0 removes all sources. */
+#define RHGPU_INJECT_SOLARWIND 1
+#define RHGPU_INJECT_FLOW      2
+typedef struct rhgpu_injector {
+   int32_t  species;                  /* population index */
+   int32_t  type;                     /* RHGPU_INJECT_* */
+   double   velocity[3];              /* bulk velocity [m/s] */
+   double   density;                  /* number density [m^-3] */
+   double   temperature;              /* [K] */
+   double   macroparticles_per_cell;
+   int32_t  inflow_walls;             /* flow: walls (bit mask above) */
+   int32_t  reserved;
+   uint64_t seed;
+} rhgpu_injector;
+int rhgpu_set_injectors(rhgpu_ctx* ctx, int32_t n, const rhgpu_injector* injectors);
+/* injected per species: weight, macroparticles, weight * v^2
+ * (logCounterParticleInject*, particle_injector.cpp:569-571); 3 * n_species doubles */
+int rhgpu_get_injection_counters(rhgpu_ctx* ctx, double* out, int32_t n);
+/* Philox-4x32-10 of the particle sources, host side (for checks): out = philox(ctr, key) */
+void rhgpu_philox4x32(const uint32_t* ctr, const uint32_t* key, uint32_t* out);
 
 /* Counters: RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES*n_species doubles. */
 int rhgpu_get_counters(rhgpu_ctx* ctx, double* out, int32_t n);

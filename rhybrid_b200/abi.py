@@ -158,8 +158,23 @@ _OPTIONAL = {
     "dn_num_pairs": [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
     "set_denoiser": [_P, _P, C.c_int32],
     "set_threads": [_P, C.c_int32],
+    "set_injectors": [_P, C.c_int32, C.c_void_p],
+    "get_injection_counters": [_P, _D, C.c_int32],
+    "philox4x32": [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
 }
-_RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p}
+_RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p, "philox4x32": None}
+
+INJECT_SOLARWIND = 1
+INJECT_FLOW = 2
+# flow injector walls (rhgpu_injector.inflow_walls)
+WALLS = {"+x": 1, "-x": 2, "+y": 4, "-y": 8, "+z": 16, "-z": 32}
+
+
+class Injector(C.Structure):
+    """rhgpu_injector: one particle source (the reference's solar wind or flow injector)."""
+    _fields_ = [("species", C.c_int32), ("type", C.c_int32), ("velocity", C.c_double * 3),
+                ("density", C.c_double), ("temperature", C.c_double), ("macroparticles_per_cell", C.c_double),
+                ("inflow_walls", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_uint64)]
 
 
 def _ptr(a: np.ndarray, ct):
@@ -343,6 +358,19 @@ class Context:
         """rhgpu_accumulate_noalloc: the exact-path deposit without any device allocation."""
         self.lib.call("accumulate_noalloc", self.h)
 
+    def set_injectors(self, injectors):
+        """rhgpu_set_injectors: the particle sources (a list of Injector; empty: none)."""
+        arr = (Injector * max(len(injectors), 1))(*injectors)
+        self.lib.call("set_injectors", self.h, len(injectors), C.cast(arr, C.c_void_p))
+
+    def injection_counters(self) -> list:
+        """rhgpu_get_injection_counters: per species the injected weight,
+        macroparticles and weight * v^2."""
+        out = np.zeros(3 * self.nspecies, dtype=np.float64)
+        self.lib.call("get_injection_counters", self.h, _ptr(out, C.c_double), out.size)
+        return [{"weight": out[3 * s], "macroparticles": out[3 * s + 1], "weight_v2": out[3 * s + 2]}
+                for s in range(self.nspecies)]
+
     def set_denoiser(self, dn, enabled: bool = True):
         """rhgpu_set_denoiser: apply `dn` to the moments in every step (None: none)."""
         self.lib.call("set_denoiser", self.h, dn.h if dn is not None else None, 1 if enabled else 0)
@@ -365,6 +393,15 @@ class Context:
 
 
 _GPU_LIB: Optional[Library] = None
+
+
+def philox4x32(lib: "Library", ctr, key) -> list:
+    """The library's Philox-4x32-10 (host side) of a 4-word counter and 2-word key."""
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib.fn["philox4x32"](c, k, o)
+    return list(o)
 
 
 def gpu_library_path() -> str:

@@ -120,6 +120,25 @@ class Config:
 # ---------------------------------------------------------------------------
 # named configurations (workloads)
 
+C_DOUBLE3 = abi.C.c_double * 3
+
+
+def solar_wind_injectors(cfg: "Config", seed: int = 1) -> list:
+    """One InjectorSolarWind per upstream population with a velocity along one
+    axis, as the reference's .cfg files set the solar wind sources: density,
+    temperature and macroparticles per cell of the population (weight
+    n dx^3 / ppc, the uniform fill's weight)."""
+    out = []
+    for s, p in enumerate(cfg.populations):
+        v = tuple(float(x) for x in p.velocity)
+        if not p.upstream or sum(1 for x in v if x != 0.0) != 1 or p.temperature <= 0 or p.ppc <= 0:
+            continue
+        out.append(abi.Injector(species=s, type=abi.INJECT_SOLARWIND, velocity=(C_DOUBLE3)(*v), density=p.density,
+                                temperature=p.temperature, macroparticles_per_cell=p.ppc, inflow_walls=0,
+                                reserved=0, seed=seed * 1000003 + s))
+    return out
+
+
 def config_empty_box(nx=32, ny=32, nz=32, ppc=20.0) -> Config:
     """Plain FP64 periodic empty box: cell 100 km, one H+ species, n=5e6 m^-3,
     drift Vx=-400 km/s, Maxwellian T=1e5 K, B=(0,5,0) nT uniform, 20

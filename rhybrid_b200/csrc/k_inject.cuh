@@ -1,0 +1,203 @@
+// Particle sources (sm_100a): the reference's solar wind and flow injectors
+// (particle_injector.cpp:517-730 InjectorSolarWind, :734-945 InjectorFlow),
+// run after the boundary conditions of every step (user.cpp:119-122), on the
+// GPU. One thread per injection cell draws its particles from a counter-based
+// stream (Philox, keyed by the injector's seed, the step and the cell), so the
+// result does not depend on thread order. New particles enter the step's mover
+// list as placement-only movers (no deposit in this step, as in the reference)
+// with keys after every real mover, and the migration stores them.
+#pragma once
+
+#include "rh_device.cuh"
+#include "rh_rng.cuh"
+#include "k_fast.cuh"
+#include "k_f32.cuh"
+
+namespace rh {
+
+constexpr int INJ_SOLARWIND = 1;   // RHGPU_INJECT_SOLARWIND
+constexpr int INJ_FLOW = 2;        // RHGPU_INJECT_FLOW
+constexpr int INJ_MAX_TRIES = 1000;   // bound of every rejection loop (failures raise a device error)
+
+struct InjDev {
+   int species;
+   int type;
+   int wall;             // solar wind: axis * 2 + (1 if it enters at the positive wall)
+   int ncells;           // injection cells
+   const int* cells;     // their cell indices
+   double U;             // solar wind speed |U|
+   double vel[3];        // flow bulk velocity
+   double vth;           // thermal speed sqrt(k T / m)
+   double perCellPerDt;  // macroparticles per injection cell per step
+   double w;             // macroparticle weight
+   unsigned long long seed;
+   long long keyBase;    // first mover key source id (above every real segment)
+};
+
+// a Gaussian deviate pair by the polar method (G. Marsaglia, T. A. Bray, SIAM Rev. 6, 1964),
+// the reference's sampleGaussian; false if no pair is accepted in INJ_MAX_TRIES
+__device__ inline bool gaussianPair(RngStream& r, double& a, double& b) {
+   for (int t = 0; t < INJ_MAX_TRIES; ++t) {
+      const double x = 2.0 * r.uniform() - 1.0, y = 2.0 * r.uniform() - 1.0;
+      const double r2 = x * x + y * y;
+      if (r2 < 1.0 && r2 > 0.0) {
+         const double fac = sqrt(-2.0 * log(r2) / r2);
+         a = x * fac;
+         b = y * fac;
+         return true;
+      }
+   }
+   a = b = 0.0;
+   return false;
+}
+
+struct GaussSource {
+   double saved;
+   bool has;
+   bool ok;
+   __device__ double next(RngStream& r) {
+      if (has) { has = false; return saved; }
+      double a, b;
+      ok = gaussianPair(r, a, b) && ok;
+      saved = b;
+      has = true;
+      return a;
+   }
+};
+
+// f(x) = c max(0, x) exp(-(x - x0)^2 / 2): the reference's sampleDerivGaussian
+// (particle_injector.cpp:83-106), rejection from the unit Gaussian around the
+// maximum xm = (x0 + sqrt(x0^2 + 4)) / 2; the normal speed of a drifting
+// Maxwellian's flux through a wall, in thermal units
+__device__ inline double derivGaussian(double x0, RngStream& r, GaussSource& g) {
+   const double xm = 0.5 * (x0 + sqrt(x0 * x0 + 4.0));
+   const double d = (x0 - xm) * (x0 - xm);
+   for (int t = 0; t < INJ_MAX_TRIES; ++t) {
+      const double x = xm + g.next(r);
+      if (x < 0) continue;
+      // pdf / majorant = x exp(-(x - x0)^2 / 2) / (xm exp(-((x - xm)^2 + d) / 2))
+      const double ratio = (x / xm) * exp(-0.5 * ((x - x0) * (x - x0)) + 0.5 * ((x - xm) * (x - xm) + d));
+      if (r.uniform() <= ratio) return x;
+   }
+   g.ok = false;
+   return xm;
+}
+
+// the new particle's cell-local state (x, y, z, vx, vy, vz) in a cell of side dx
+__device__ inline void injState(const InjDev& J, double dx, RngStream& r, GaussSource& g, double st[6]) {
+   if (J.type == INJ_SOLARWIND) {
+      const int ax = J.wall >> 1;
+      const bool pos = J.wall & 1;   // enters through the positive wall, moving to -ax
+      for (int a = 0; a < 3; ++a) st[a] = a == ax ? (pos ? 0.0 : dx) : r.uniform() * dx;
+      for (int a = 0; a < 3; ++a) {
+         if (a == ax) {
+            const double s = J.vth * derivGaussian(J.U / J.vth, r, g);
+            st[3 + a] = pos ? -s : s;
+         } else {
+            st[3 + a] = J.vth * g.next(r);
+         }
+      }
+   } else {
+      for (int a = 0; a < 3; ++a) st[a] = r.uniform() * dx;
+      for (int a = 0; a < 3; ++a) st[3 + a] = J.vel[a] + J.vth * g.next(r);
+   }
+}
+
+// migration of an injected position that sits on the far face of its cell
+// (x == dx): to the next cell, as the push's migration does
+__device__ inline void injCell(const GridInfo& g, int& i, int& j, int& k, double st[3]) {
+   int c[3] = {i, j, k};
+   const int n[3] = {g.nx, g.ny, g.nz};
+   for (int a = 0; a < 3; ++a) {
+      if (st[a] >= g.dx) {
+         st[a] -= g.dx;
+         if (++c[a] >= n[a]) c[a] = g.per[a] ? 0 : n[a] - 1;
+      }
+   }
+   i = c[0]; j = c[1]; k = c[2];
+}
+
+// one thread per injection cell: probRound(perCellPerDt) particles (particle_injector.cpp:41-47)
+template <class MV>
+__global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* movers,
+                         unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err);
+
+__device__ inline void writeMover(Mover& M, const GridInfo& g, const FastGeom& fg, const double st[7], int i, int j,
+                                  int k, int species, unsigned long long key) {
+   const int ux = dualU(i + halfS(st[0], g.dx) - 1, g.nx, g.per[0]);
+   const int uy = dualU(j + halfS(st[1], g.dx) - 1, g.ny, g.per[1]);
+   const int uz = dualU(k + halfS(st[2], g.dx) - 1, g.nz, g.per[2]);
+   for (int a = 0; a < 7; ++a) M.s[a] = st[a];
+   M.key = key;
+   const int gd = ux / SEG;
+   M.dest = ((long long)uy + (long long)fg.nd[1] * uz) * fg.nseg + gd;
+   M.species = species;
+   M.lx = (ux - gd * SEG) | MOVER_PLACE;
+}
+
+// FP32 form: offsets in cell units (as k_f32_seg_of stores an uploaded particle)
+__device__ inline void writeMover(Mover32& M, const GridInfo& g, const FastGeom& fg, const double st[7], int i, int j,
+                                  int k, int species, unsigned long long key) {
+   const float below1 = 0x1.fffffep-1f;
+   float o[3];
+   for (int a = 0; a < 3; ++a) {
+      o[a] = (float)(st[a] / g.dx);
+      if (o[a] >= 1.0f) o[a] = below1;
+   }
+   const int ux = dualU(i + halfSf(o[0]) - 1, g.nx, g.per[0]);
+   const int uy = dualU(j + halfSf(o[1]) - 1, g.ny, g.per[1]);
+   const int uz = dualU(k + halfSf(o[2]) - 1, g.nz, g.per[2]);
+   for (int a = 0; a < 3; ++a) { M.o[a] = o[a]; M.v[a] = (float)st[3 + a]; }
+   M.cell = (int)cidx(g, i, j, k);
+   M.species = species;
+   M.key = key;
+   const int gd = ux / SEG;
+   M.dest = ((long long)uy + (long long)fg.nd[1] * uz) * fg.nseg + gd;
+   M.lx = (ux - gd * SEG) | MOVER_PLACE;
+}
+
+template <class MV>
+__global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* movers,
+                         unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err) {
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= J.ncells) return;
+   RngStream r;
+   r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
+   // probRound: floor(x) + 1 with probability x - floor(x)
+   const double x = J.perCellPerDt;
+   int n = 0;
+   if (x > 0) {
+      n = (int)floor(x);
+      if (r.uniform() < x - n) ++n;
+   }
+   if (n == 0) return;
+   const unsigned long long m0 = atomicAdd(nmovers, (unsigned long long)n);
+   const int cell = J.cells[t];
+   const int ci = cell % g.nx, cj = (cell / g.nx) % g.ny, ck = cell / (g.nx * g.ny);
+   GaussSource gs;
+   gs.has = false;
+   gs.ok = true;
+   double sw = 0.0, ske = 0.0;
+   for (int p = 0; p < n; ++p) {
+      double st[7];
+      injState(J, g.dx, r, gs, st);
+      st[6] = J.w;
+      int i = ci, j = cj, k = ck;
+      injCell(g, i, j, k, st);
+      sw += J.w;
+      ske += J.w * (st[3] * st[3] + st[4] * st[4] + st[5] * st[5]);
+      const unsigned long long m = m0 + p;
+      if ((long long)m >= moverCap) {
+         raiseError(err, RHGPU_DEVERR_CAPACITY);
+         continue;
+      }
+      const unsigned long long key = ((unsigned long long)(J.keyBase + t) << 32) | (unsigned long long)p;
+      writeMover(movers[m], g, fg, st, i, j, k, J.species, key);
+   }
+   if (!gs.ok) raiseError(err, RHGPU_DEVERR_INJECT);
+   atomicAdd(&injCnt[3 * J.species + 0], sw);
+   atomicAdd(&injCnt[3 * J.species + 1], (double)n);
+   atomicAdd(&injCnt[3 * J.species + 2], ske);
+}
+
+}  // namespace rh

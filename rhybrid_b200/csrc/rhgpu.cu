@@ -22,6 +22,7 @@
 #include "k_diag.cuh"
 #include "k_f32.cuh"
 #include "k_denoise.cuh"
+#include "k_inject.cuh"
 
 using namespace rh;
 
@@ -144,10 +145,18 @@ struct SegHost {
 
 }  // namespace
 
+struct InjHost {
+   InjDev d;
+   int* cells = nullptr;   // device copy of d.cells
+};
+
 struct rhgpu_ctx {
    rhgpu_params P;
    GridInfo g;
    int device = 0;
+   std::vector<InjHost> inj;      // particle sources
+   double* injCnt = nullptr;      // 3 x ns: injected weight, macroparticles, weight v^2
+   long long injKeyMax = 0;       // largest mover key source id of the sources
    cudaStream_t stream = nullptr;
    int ns = 0;
    rhgpu_species sp[MAX_SPECIES];
@@ -734,7 +743,7 @@ int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** 
    }
    k_mig_sort_keys<<<blocks1d(nm, 256), 256, 0, c->stream>>>(mv, nm, NS, nb, kA, vA, bA);
    RH_LAUNCHED(c);
-   const int kbits = 32 + bitsFor(NS > 1 ? NS - 1 : 1), bbits = bitsFor(nb);
+   const int kbits = 32 + bitsFor(std::max(NS > 1 ? NS - 1 : 1, c->injKeyMax)), bbits = bitsFor(nb);
    size_t s1 = 0, s2 = 0;
    cub::DeviceRadixSort::SortPairs(nullptr, s1, kA, kB, vA, vB, (int)nm, 0, kbits, c->stream);
    cub::DeviceRadixSort::SortPairs(nullptr, s2, bB, bA, vB, vA, (int)nm, 0, bbits, c->stream);
@@ -906,6 +915,19 @@ int fastDownload(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long 
 }
 
 // fused push + deposit, then placement of the particles that left their segment
+// the particle sources of this step, appended to the mover list
+template <class MV>
+int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
+   for (const InjHost& h : c->inj) {
+      if (h.d.ncells == 0) continue;
+      RH_TIME(c, "inject");
+      k_inject<MV><<<blocks1d(h.d.ncells, 128), 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers,
+                                                                     c->fb.nmovers, moverCap, c->injCnt, c->err);
+      RH_LAUNCHED(c);
+   }
+   return RHGPU_OK;
+}
+
 int fastPush(rhgpu_ctx* c) {
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
@@ -931,6 +953,10 @@ int fastPush(rhgpu_ctx* c) {
 #undef RH_FAST_PD
       }
       RH_LAUNCHED(c);
+   }
+   {
+      const int rc = injectAll(c, c->fb.movers, c->fb.moverCap);
+      if (rc) return rc;
    }
    unsigned long long nm = 0;
    RH_CUDA(cudaMemcpyAsync(&nm, c->fb.nmovers, sizeof nm, cudaMemcpyDeviceToHost, c->stream));
@@ -1290,6 +1316,10 @@ int f32Push(rhgpu_ctx* c) {
       }
       RH_LAUNCHED(c);
    }
+   {
+      const int rc = injectAll(c, c->f32b.movers, c->f32b.moverCap);
+      if (rc) return rc;
+   }
    unsigned long long nm = 0;
    RH_CUDA(cudaMemcpyAsync(&nm, c->fb.nmovers, sizeof nm, cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -1624,6 +1654,8 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    }
    cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
    cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
+   for (auto& h : c->inj) cudaFree(h.cells);
+   cudaFree(c->injCnt);
    cudaFree(c->finc); cudaFree(c->fover); cudaFree(c->ffill); cudaFree(c->fmaxInc);
    cudaFree(c->mkey); cudaFree(c->mval); cudaFree(c->mbkt);
    cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
@@ -1742,8 +1774,8 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
    if (c->path == RHGPU_PATH_FP32) return f32Upload(c, s, counts, particles, n);
    const long long N = c->g.N;
    PStore& P = c->ps[s];
-   if (n > P.cap) {
-      // bit-exact path storage, allocated on first use
+   if (n > P.cap || !P.start) {
+      // bit-exact path storage, allocated on first use (also for an empty upload)
       const long long cap = std::max<long long>(c->capHint[s], (long long)n + n / 8 + 1024);
       freeStore(c->ps[s]);
       freeStore(c->alt[s]);
@@ -1838,6 +1870,21 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
 
 namespace {
 int phasePush(rhgpu_ctx* c) {
+   if (!c->inj.empty() && c->path == RHGPU_PATH_EXACT)
+      return fail(RHGPU_ERR_STATE, "particle sources run on the fast and FP32 paths, not the exact path");
+   if (!c->inj.empty() && c->path == RHGPU_PATH_FP32) {
+      // the FP32 form stores one weight per species: a source must inject that weight
+      for (const InjHost& h : c->inj) {
+         if (h.d.ncells == 0 || !(h.d.perCellPerDt > 0)) continue;
+         double& ws = c->f32[h.d.species].w;
+         if (ws == 0.0) {   // a species uploaded without particles takes its source's weight
+            ws = h.d.w;
+            f32Exponents(c);
+         } else if (std::fabs(h.d.w - ws) > 1e-12 * ws) {
+            return fail(RHGPU_ERR_STATE, "FP32 form: a particle source's weight differs from its species' weight");
+         }
+      }
+   }
    return c->path == RHGPU_PATH_FAST ? fastPush(c) : c->path == RHGPU_PATH_FP32 ? f32Push(c) : pushAll(c);
 }
 int phaseAccumulate(rhgpu_ctx* c) {
@@ -1936,6 +1983,107 @@ int rhgpu_device_errors(rhgpu_ctx* c, uint32_t* word_out) {
    RH_CUDA(cudaMemcpyAsync(word_out, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
    return RHGPU_OK;
+}
+
+int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
+   if (!c || n < 0 || (n > 0 && !inj)) return fail(RHGPU_ERR_ARG, "set_injectors: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   for (auto& h : c->inj) cudaFree(h.cells);
+   c->inj.clear();
+   c->injKeyMax = 0;
+   if (!c->injCnt) {
+      RH_CUDA(cudaMalloc(&c->injCnt, sizeof(double) * 3 * MAX_SPECIES));
+      RH_CUDA(cudaMemset(c->injCnt, 0, sizeof(double) * 3 * MAX_SPECIES));
+   }
+   const GridInfo& g = c->g;
+   const int nn[3] = {g.nx, g.ny, g.nz};
+   long long keyBase = c->fg.NS > 0 ? c->fg.NS : 1;
+   for (int q = 0; q < n; ++q) {
+      const rhgpu_injector& J = inj[q];
+      if (J.species < 0 || J.species >= c->ns) return fail(RHGPU_ERR_ARG, "set_injectors: bad species");
+      if (!(J.density >= 0) || !(J.temperature >= 0) || !(J.macroparticles_per_cell >= 0))
+         return fail(RHGPU_ERR_ARG, "set_injectors: density, temperature and macroparticles_per_cell must be >= 0");
+      InjHost h;
+      std::memset(&h.d, 0, sizeof h.d);
+      h.d.species = J.species;
+      h.d.type = J.type;
+      h.d.seed = J.seed;
+      const double m = c->sp[J.species].m;
+      h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
+      const double ppc = J.macroparticles_per_cell;
+      h.d.w = (ppc > 0 && J.density > 0) ? J.density * g.dV / ppc : 0.0;
+      std::vector<int> cells;
+      // (i, j, k) has its neighbour along axis a on the side sgn
+      auto hasNb = [&](const int p[3], int a, int sgn) {
+         if (g.per[a]) return true;
+         return sgn > 0 ? p[a] < nn[a] - 1 : p[a] > 0;
+      };
+      if (J.type == RHGPU_INJECT_SOLARWIND) {
+         int ax = -1;
+         for (int a = 0; a < 3; ++a)
+            if (J.velocity[a] != 0.0) { if (ax >= 0) ax = 3; else ax = a; }
+         if (ax < 0 || ax > 2)
+            return fail(RHGPU_ERR_ARG, "set_injectors: solar wind velocity must have exactly one non-zero component");
+         const bool pos = J.velocity[ax] < 0;   // flows toward -ax: enters through the +ax wall
+         h.d.wall = 2 * ax + (pos ? 1 : 0);
+         h.d.U = std::fabs(J.velocity[ax]);
+         h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc * h.d.U * g.dt / g.dx : 0.0;
+         if (h.d.vth <= 0) return fail(RHGPU_ERR_ARG, "set_injectors: solar wind needs a temperature > 0");
+         // InjectorSolarWind::checkIfInjectionCell{X,Y,Z}{Pos,Neg} (particle_injector.cpp:392-446)
+         for (int k = 0; k < g.nz; ++k)
+            for (int j = 0; j < g.ny; ++j)
+               for (int i = 0; i < g.nx; ++i) {
+                  const int p[3] = {i, j, k};
+                  if (hasNb(p, ax, pos ? 1 : -1)) continue;
+                  bool edge = false;
+                  for (int a = 0; a < 3; ++a)
+                     if (a != ax && (!hasNb(p, a, 1) || !hasNb(p, a, -1))) edge = true;
+                  if (!edge) cells.push_back(i + g.nx * (j + g.ny * k));
+               }
+      } else if (J.type == RHGPU_INJECT_FLOW) {
+         for (int a = 0; a < 3; ++a) h.d.vel[a] = J.velocity[a];
+         h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc : 0.0;
+         // ghost cells of the selected inflow walls (InjectorFlow::inject, particle_injector.cpp:749-760)
+         for (int k = 0; k < g.nz; ++k)
+            for (int j = 0; j < g.ny; ++j)
+               for (int i = 0; i < g.nx; ++i) {
+                  const int p[3] = {i, j, k};
+                  bool in = false;
+                  for (int b = 0; b < 6; ++b)
+                     if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
+                  if (in) cells.push_back(i + g.nx * (j + g.ny * k));
+               }
+      } else {
+         return fail(RHGPU_ERR_ARG, "set_injectors: unknown type");
+      }
+      h.d.ncells = (int)cells.size();
+      h.d.keyBase = keyBase;
+      keyBase += (long long)cells.size();
+      if (!cells.empty()) {
+         RH_CUDA(cudaMalloc(&h.cells, sizeof(int) * cells.size()));
+         RH_CUDA(cudaMemcpy(h.cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+      }
+      h.d.cells = h.cells;
+      c->inj.push_back(h);
+   }
+   c->injKeyMax = keyBase;
+   return RHGPU_OK;
+}
+
+int rhgpu_get_injection_counters(rhgpu_ctx* c, double* out, int32_t n) {
+   if (!c || !out || n < 3 * c->ns) return fail(RHGPU_ERR_ARG, "get_injection_counters: bad arguments");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   std::vector<double> v(3 * (size_t)c->ns, 0.0);
+   if (c->injCnt) RH_CUDA(cudaMemcpy(v.data(), c->injCnt, sizeof(double) * v.size(), cudaMemcpyDeviceToHost));
+   std::memcpy(out, v.data(), sizeof(double) * v.size());
+   return RHGPU_OK;
+}
+
+void rhgpu_philox4x32(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+   const Philox4 r = philox4x32(ctr, key);
+   for (int a = 0; a < 4; ++a) out[a] = r.v[a];
 }
 
 int rhgpu_get_counters(rhgpu_ctx* c, double* out, int32_t n) {

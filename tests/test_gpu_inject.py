@@ -1,0 +1,128 @@
+"""Particle sources on the GPU (the reference's InjectorSolarWind and
+InjectorFlow, src/particle_injector.cpp): counts, placement and velocity
+statistics of the injected macroparticles. The reference draws from one
+sequential random stream, so the comparison is statistical, as its own
+tests/run_tests.py checks populations; the counter-based stream makes every
+run reproducible."""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+
+from rhybrid_b200 import abi
+from rhybrid_b200 import config as cf
+
+pytestmark = pytest.mark.gpu
+
+U, T, N0, PPC = 400e3, 1e5, 5e6, 50.0
+
+
+def box(periodic=(0, 1, 1), accelerate=False, nx=12, ny=8, nz=8):
+    pop = cf.Population(name="H+", density=N0, velocity=(-U, 0.0, 0.0), temperature=T, ppc=PPC,
+                        accelerate=accelerate)
+    return cf.Config(nx=nx, ny=ny, nz=nz, x_min=-0.5 * nx * 100e3, y_min=-0.5 * ny * 100e3,
+                     z_min=-0.5 * nz * 100e3, dx=100e3, periodic=periodic, dt=0.05, populations=[pop],
+                     name="inject_box")
+
+
+def empty_context(lib, cfg, path=abi.PATH_FAST, seed=1, cap=400000):
+    grid, _ = cf.initial_state(cfg.replace(populations=[dataclasses.replace(cfg.populations[0], ppc=1.0)]))
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[cap])
+    ctx.set_path(path)
+    ctx.upload_array("faceB", grid["faceB"])
+    ctx.upload_array("cellB", grid["cellB"])
+    ctx.upload_array("nodeEta", grid["nodeEta"])
+    ctx.upload_cell_flags(grid["flags"])
+    ctx.upload_particles(0, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+    ctx.set_injectors(cf.solar_wind_injectors(cfg, seed=seed))
+    return ctx
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return abi.gpu_library()
+
+
+def test_solar_wind_one_step(lib):
+    """ppc U dt / dx = 10 macroparticles per wall cell per step (an integer, so
+    probRound is exact), at the +x wall face, moving inward."""
+    cfg = box()
+    ctx = empty_context(lib, cfg)
+    try:
+        ctx.step(1)
+        cnt, p = ctx.download_particles(0)
+        ncell_wall = cfg.ny * cfg.nz
+        assert p.shape[0] == 10 * ncell_wall
+        cell = np.repeat(np.arange(cfg.ncells), cnt.astype(np.int64))
+        assert np.all(cell % cfg.nx == cfg.nx - 1)
+        assert np.all(p[:, 0] == 0.0) and np.all((p[:, 1] >= 0) & (p[:, 1] < cfg.dx))
+        assert np.all(p[:, 3] < 0)
+        w = N0 * cfg.dx ** 3 / PPC
+        assert np.allclose(p[:, 6], w, rtol=1e-12)
+        ic = ctx.injection_counters()[0]
+        assert ic["macroparticles"] == p.shape[0]
+        assert math.isclose(ic["weight"], p.shape[0] * w, rel_tol=1e-12)
+        assert math.isclose(ic["weight_v2"], float(np.sum(w * np.sum(p[:, 3:6] ** 2, axis=1))), rel_tol=1e-9)
+    finally:
+        ctx.close()
+
+
+def test_solar_wind_fills_box_at_density(lib):
+    """Drift only, 30 steps: the injected plasma fills the box behind its front
+    with the upstream density (ppc per cell), bulk velocity -U and thermal
+    spread sqrt(kT/m) across the flow."""
+    cfg = box()
+    ctx = empty_context(lib, cfg)
+    try:
+        ctx.step(30)
+        cnt, p = ctx.download_particles(0)
+    finally:
+        ctx.close()
+    per_cell = cnt.reshape(cfg.nz, cfg.ny, cfg.nx).mean(axis=(0, 1))
+    # each step's 10 particles per wall cell enter at the wall face (x = 11 cells)
+    # and drift 0.2 cells per step: the front is at 11 - 29 * 0.2 = 5.2 cells,
+    # cells 6..9 hold 5 injection groups each (ppc), cell 10 holds 4.5 (the last
+    # group is still on the face, in the injection layer 11)
+    filled = per_cell[6:10]
+    assert np.all(np.abs(filled / PPC - 1.0) < 0.05), filled
+    assert abs(per_cell[10] / (0.9 * PPC) - 1.0) < 0.05, per_cell[10]
+    vth = math.sqrt(abi.BOLTZMANN * T / abi.MASS_PROTON)
+    assert abs(p[:, 3].mean() / -U - 1.0) < 0.02
+    for a in (4, 5):
+        assert abs(p[:, a].std() / vth - 1.0) < 0.05
+        assert abs(p[:, a].mean()) < 0.05 * vth
+
+
+def test_reproducible_by_seed(lib):
+    cfg = box()
+    out = []
+    for seed in (1, 1, 2):
+        ctx = empty_context(lib, cfg, seed=seed)
+        try:
+            ctx.step(3)
+            out.append(ctx.download_particles(0)[1])
+        finally:
+            ctx.close()
+    assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
+    assert out[0].shape != out[2].shape or not np.array_equal(out[0], out[2])
+
+
+def test_fp32_form_injects_the_same_count(lib):
+    cfg = box()
+    ctx = empty_context(lib, cfg, path=abi.PATH_FP32)
+    try:
+        ctx.step(1)
+        assert ctx.num_particles(0) == 10 * cfg.ny * cfg.nz
+    finally:
+        ctx.close()
+
+
+def test_exact_path_refuses_sources(lib):
+    cfg = box()
+    ctx = empty_context(lib, cfg, path=abi.PATH_EXACT)
+    try:
+        with pytest.raises(abi.RhError):
+            ctx.step(1)
+    finally:
+        ctx.close()
