@@ -303,10 +303,26 @@ int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
  *   RHGPU_INJECT_FLOW (InjectorFlow, :734-945): every cell of the walls in
  *     `inflow_walls` (bit 0 +x, 1 -x, 2 +y, 3 -y, 4 +z, 5 -z) gets N = ppc
  *     per step, uniform in the cell, velocity + Gaussian thermal velocity.
- * Weight n dx^3 / ppc, thermal speed sqrt(k_B T / m) with the species' mass.
- * n == 0 removes all sources. */
+ *   RHGPU_INJECT_EXOSPHERE (InjectorExosphere, :1491-1840): a neutral
+ *     density profile (`profile`, below; n0/H0/T0/k0 per component, r0) is
+ *     averaged over each cell by Monte Carlo (1000 points, zero below the
+ *     exobase) at set-up; with the ionization rate (or the total production
+ *     rate) and the shadow factor (x < 0, y^2 + z^2 < shadow_radius^2) it
+ *     gives each cell's expected macroparticles per step, the whole box
+ *     N = macroparticles_per_cell_relative * upstream_macro_ratio per step,
+ *     weight total_rate dt / N. New particles are uniform in the cell and
+ *     above the exobase, with Gaussian velocities of the temperature.
+ * Solar wind and flow: weight n dx^3 / ppc. Thermal speed sqrt(k_B T / m)
+ * with the species' mass. n == 0 removes all sources. */
 #define RHGPU_INJECT_SOLARWIND 1
 #define RHGPU_INJECT_FLOW      2
+#define RHGPU_INJECT_EXOSPHERE 3
+/* neutral profiles (src/neutral_profiles.h) */
+#define RHGPU_NEUTRAL_CHAMBERLAIN_H 1   /* sum n0 exp(-H0 (1/r0 - 1/r)) */
+#define RHGPU_NEUTRAL_CHAMBERLAIN_T 2   /* sum n0 exp(-(G M m / k_B T0) (1/r0 - 1/r)) */
+#define RHGPU_NEUTRAL_EXPONENTIAL   3   /* sum n0 exp(-(r - r0) / H0) */
+#define RHGPU_NEUTRAL_POWER_LAW     4   /* sum n0 (r0 / r)^k0 */
+#define RHGPU_NEUTRAL_MAX_COMPONENTS 4
 typedef struct rhgpu_injector {
    int32_t  species;                  /* population index */
    int32_t  type;                     /* RHGPU_INJECT_* */
@@ -317,6 +333,18 @@ typedef struct rhgpu_injector {
    int32_t  inflow_walls;             /* flow: walls (bit mask above) */
    int32_t  reserved;
    uint64_t seed;
+   /* exosphere */
+   int32_t  profile;                  /* RHGPU_NEUTRAL_* */
+   int32_t  n_components;             /* 1 .. RHGPU_NEUTRAL_MAX_COMPONENTS */
+   double   r0;                       /* profile reference radius [m] */
+   double   n0[4], H0[4], T0[4], k0[4];
+   double   gm_object;                /* G M_object [m^3 s^-2] (Chamberlain T) */
+   double   exobase_radius, shadow_radius;
+   double   ionization_rate;          /* [1/s], or < 0: use total_production_rate */
+   double   ionization_factor_shadow;
+   double   total_production_rate;    /* [1/s], or < 0: use ionization_rate */
+   double   macroparticles_per_cell_relative;
+   double   upstream_macro_ratio;     /* Hybrid::upstreamMacroPleRatio (> 0) */
 } rhgpu_injector;
 int rhgpu_set_injectors(rhgpu_ctx* ctx, int32_t n, const rhgpu_injector* injectors);
 /* injected per species: weight, macroparticles, weight * v^2

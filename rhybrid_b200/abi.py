@@ -166,6 +166,8 @@ _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void
 
 INJECT_SOLARWIND = 1
 INJECT_FLOW = 2
+INJECT_EXOSPHERE = 3
+NEUTRAL_PROFILES = {"ChamberlainH": 1, "ChamberlainT": 2, "Exponential": 3, "PowerLaw": 4}
 # flow injector walls (rhgpu_injector.inflow_walls)
 WALLS = {"+x": 1, "-x": 2, "+y": 4, "-y": 8, "+z": 16, "-z": 32}
 
@@ -174,7 +176,13 @@ class Injector(C.Structure):
     """rhgpu_injector: one particle source (the reference's solar wind or flow injector)."""
     _fields_ = [("species", C.c_int32), ("type", C.c_int32), ("velocity", C.c_double * 3),
                 ("density", C.c_double), ("temperature", C.c_double), ("macroparticles_per_cell", C.c_double),
-                ("inflow_walls", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_uint64)]
+                ("inflow_walls", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_uint64),
+                ("profile", C.c_int32), ("n_components", C.c_int32), ("r0", C.c_double),
+                ("n0", C.c_double * 4), ("H0", C.c_double * 4), ("T0", C.c_double * 4), ("k0", C.c_double * 4),
+                ("gm_object", C.c_double), ("exobase_radius", C.c_double), ("shadow_radius", C.c_double),
+                ("ionization_rate", C.c_double), ("ionization_factor_shadow", C.c_double),
+                ("total_production_rate", C.c_double), ("macroparticles_per_cell_relative", C.c_double),
+                ("upstream_macro_ratio", C.c_double)]
 
 
 def _ptr(a: np.ndarray, ct):

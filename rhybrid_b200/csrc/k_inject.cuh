@@ -1,5 +1,6 @@
-// Particle sources (sm_100a): the reference's solar wind and flow injectors
-// (particle_injector.cpp:517-730 InjectorSolarWind, :734-945 InjectorFlow),
+// Particle sources (sm_100a): the reference's solar wind, flow and exosphere
+// injectors (particle_injector.cpp:517-730 InjectorSolarWind, :734-945
+// InjectorFlow, :1491-1840 InjectorExosphere),
 // run after the boundary conditions of every step (user.cpp:119-122), on the
 // GPU. One thread per injection cell draws its particles from a counter-based
 // stream (Philox, keyed by the injector's seed, the step and the cell), so the
@@ -17,6 +18,9 @@ namespace rh {
 
 constexpr int INJ_SOLARWIND = 1;   // RHGPU_INJECT_SOLARWIND
 constexpr int INJ_FLOW = 2;        // RHGPU_INJECT_FLOW
+constexpr int INJ_EXOSPHERE = 3;   // RHGPU_INJECT_EXOSPHERE
+constexpr double INJ_EPS_CELL = 1.0e-4;   // margin of a cell's random points (particle_injector.cpp:31)
+constexpr int INJ_MC_POINTS = 1000;       // Monte Carlo points per cell (particle_injector.cpp:33)
 constexpr int INJ_MAX_TRIES = 1000;   // bound of every rejection loop (failures raise a device error)
 
 struct InjDev {
@@ -32,7 +36,47 @@ struct InjDev {
    double w;             // macroparticle weight
    unsigned long long seed;
    long long keyBase;    // first mover key source id (above every real segment)
+   const double* rates;  // exosphere: expected macroparticles per step of each injection cell
+   double R2exo;         // exosphere: squared exobase radius
 };
+
+// neutral density of an exospheric profile at radius r (neutral_profiles.h:36-87):
+// 1 ChamberlainH, 2 ChamberlainT (a[i] = G M m / (k_B T0[i])), 3 Exponential, 4 PowerLaw
+struct NeutralProfile {
+   int type, n;
+   double r0;
+   double n0[4], b[4];   // b: H0, a, H0 or k0 per component
+};
+__device__ inline double neutralDensity(const NeutralProfile& P, double r) {
+   double d = 0.0;
+   for (int i = 0; i < P.n; ++i) {
+      if (P.type == 1 || P.type == 2) d += P.n0[i] * exp(-P.b[i] * (1.0 / P.r0 - 1.0 / r));
+      else if (P.type == 3) d += P.n0[i] * exp(-(r - P.r0) / P.b[i]);
+      else d += P.n0[i] * pow(P.r0 / r, P.b[i]);
+   }
+   return d;
+}
+
+// each cell's mean neutral density times its volume by Monte Carlo over
+// INJ_MC_POINTS points (zero below the exobase), particle_injector.cpp:1718-1736
+__global__ void k_exo_density(GridInfo g, NeutralProfile P, double R2exo, unsigned long long seed, double* out) {
+   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (n >= g.N) return;
+   const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((long long)g.nx * g.ny));
+   const double xc = g.x_min + (i + 0.5) * g.dx, yc = g.y_min + (j + 0.5) * g.dx, zc = g.z_min + (k + 0.5) * g.dx;
+   RngStream r;
+   r.init(seed, 0xE705u, (uint32_t)n, (uint32_t)(n >> 32));
+   double sum = 0.0;
+   for (int s = 0; s < INJ_MC_POINTS; ++s) {
+      const double x = xc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double y = yc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double z = zc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double r2 = x * x + y * y + z * z;
+      if (r2 < R2exo) continue;
+      sum += neutralDensity(P, sqrt(r2));
+   }
+   out[n] = sum / INJ_MC_POINTS * g.dV;
+}
 
 // a Gaussian deviate pair by the polar method (G. Marsaglia, T. A. Bray, SIAM Rev. 6, 1964),
 // the reference's sampleGaussian; false if no pair is accepted in INJ_MAX_TRIES
@@ -97,9 +141,12 @@ __device__ inline void injState(const InjDev& J, double dx, RngStream& r, GaussS
             st[3 + a] = J.vth * g.next(r);
          }
       }
-   } else {
+   } else if (J.type == INJ_FLOW) {
       for (int a = 0; a < 3; ++a) st[a] = r.uniform() * dx;
       for (int a = 0; a < 3; ++a) st[3 + a] = J.vel[a] + J.vth * g.next(r);
+   } else {   // exosphere (particle_injector.cpp:1538-1564)
+      for (int a = 0; a < 3; ++a) st[a] = 0.5 * dx + (1.0 - INJ_EPS_CELL) * dx * (r.uniform() - 0.5);
+      for (int a = 0; a < 3; ++a) st[3 + a] = J.vth * g.next(r);
    }
 }
 
@@ -164,7 +211,7 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
    RngStream r;
    r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
    // probRound: floor(x) + 1 with probability x - floor(x)
-   const double x = J.perCellPerDt;
+   const double x = J.type == INJ_EXOSPHERE ? J.rates[t] : J.perCellPerDt;
    int n = 0;
    if (x > 0) {
       n = (int)floor(x);
@@ -178,25 +225,39 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
    gs.has = false;
    gs.ok = true;
    double sw = 0.0, ske = 0.0;
+   int placed = 0;
    for (int p = 0; p < n; ++p) {
       double st[7];
       injState(J, g.dx, r, gs, st);
       st[6] = J.w;
       int i = ci, j = cj, k = ck;
-      injCell(g, i, j, k, st);
-      sw += J.w;
-      ske += J.w * (st[3] * st[3] + st[4] * st[4] + st[5] * st[5]);
+      // exosphere: only above the exobase, no redraw (particle_injector.cpp:1547-1549)
+      bool keep = true;
+      if (J.type == INJ_EXOSPHERE) {
+         const double xg = g.x_min + ci * g.dx + st[0], yg = g.y_min + cj * g.dx + st[1], zg = g.z_min + ck * g.dx + st[2];
+         keep = xg * xg + yg * yg + zg * zg >= J.R2exo;
+      }
+      if (keep) injCell(g, i, j, k, st);
       const unsigned long long m = m0 + p;
       if ((long long)m >= moverCap) {
          raiseError(err, RHGPU_DEVERR_CAPACITY);
          continue;
       }
+      if (!keep) {   // the reserved slot carries no flags: neither placed nor deposited
+         movers[m].lx = 0;
+         movers[m].species = J.species;
+         movers[m].key = ~0ull;
+         continue;
+      }
+      ++placed;
+      sw += J.w;
+      ske += J.w * (st[3] * st[3] + st[4] * st[4] + st[5] * st[5]);
       const unsigned long long key = ((unsigned long long)(J.keyBase + t) << 32) | (unsigned long long)p;
       writeMover(movers[m], g, fg, st, i, j, k, J.species, key);
    }
    if (!gs.ok) raiseError(err, RHGPU_DEVERR_INJECT);
    atomicAdd(&injCnt[3 * J.species + 0], sw);
-   atomicAdd(&injCnt[3 * J.species + 1], (double)n);
+   atomicAdd(&injCnt[3 * J.species + 1], (double)placed);
    atomicAdd(&injCnt[3 * J.species + 2], ske);
 }
 

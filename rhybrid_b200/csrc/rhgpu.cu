@@ -147,7 +147,8 @@ struct SegHost {
 
 struct InjHost {
    InjDev d;
-   int* cells = nullptr;   // device copy of d.cells
+   int* cells = nullptr;     // device copy of d.cells
+   double* rates = nullptr;  // device copy of d.rates (exosphere)
 };
 
 struct rhgpu_ctx {
@@ -1479,6 +1480,70 @@ int dnApplyCtx(rhgpu_ctx* c) {
 
 }  // namespace
 
+namespace {
+// InjectorExosphere::initialize (particle_injector.cpp:1610-1797): each cell's
+// expected exospheric ion macroparticles per step, the weight and the cells
+// that get any
+int exoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>& cells, std::vector<double>& rates) {
+   const GridInfo& g = c->g;
+   if (J.profile < 1 || J.profile > 4 || J.n_components < 1 || J.n_components > RHGPU_NEUTRAL_MAX_COMPONENTS)
+      return fail(RHGPU_ERR_ARG, "set_injectors: exosphere profile or its number of components");
+   if (!(J.upstream_macro_ratio > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs upstream_macro_ratio > 0");
+   const bool ionGiven = J.ionization_rate >= 0, totalGiven = J.total_production_rate >= 0;
+   if (ionGiven == totalGiven)
+      return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs exactly one of ionization_rate, total_production_rate");
+   const double m = c->sp[J.species].m;
+   NeutralProfile P;
+   std::memset(&P, 0, sizeof P);
+   P.type = J.profile;
+   P.n = J.n_components;
+   P.r0 = J.r0;
+   for (int i = 0; i < P.n; ++i) {
+      P.n0[i] = J.n0[i];
+      P.b[i] = J.profile == RHGPU_NEUTRAL_CHAMBERLAIN_H || J.profile == RHGPU_NEUTRAL_EXPONENTIAL ? J.H0[i]
+               : J.profile == RHGPU_NEUTRAL_CHAMBERLAIN_T ? J.gm_object * m / (1.380649e-23 * J.T0[i])
+                                                          : J.k0[i];
+   }
+   const double Rexo = std::max(J.exobase_radius, 0.0), Rsh = std::max(J.shadow_radius, 0.0);
+   h.d.R2exo = Rexo * Rexo;
+   double* dens = nullptr;
+   RH_CUDA(cudaMalloc(&dens, sizeof(double) * g.N));
+   k_exo_density<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, P, h.d.R2exo, J.seed, dens);
+   std::vector<double> cellExo(g.N);
+   cudaError_t e = cudaGetLastError();
+   if (e == cudaSuccess) e = cudaMemcpyAsync(cellExo.data(), dens, sizeof(double) * g.N, cudaMemcpyDeviceToHost, c->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+   cudaFree(dens);
+   if (e != cudaSuccess) return fail(RHGPU_ERR_CUDA, std::string("set_injectors: exosphere density: ") + cudaGetErrorString(e));
+   double total = 0.0;
+   for (double v : cellExo) {
+      if (v < 0) return fail(RHGPU_ERR_ARG, "set_injectors: negative neutral density");
+      total += v;
+   }
+   if (!(total > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: no neutrals in the box");
+   const double rel = J.macroparticles_per_cell_relative >= 0 ? J.macroparticles_per_cell_relative : 1.0;
+   const double perDt = rel * J.upstream_macro_ratio;
+   if (!(perDt > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: exosphere macroparticles per step must be positive");
+   const double ionRate = ionGiven ? J.ionization_rate : J.total_production_rate / total;
+   const double totalRate = ionGiven ? total * J.ionization_rate : J.total_production_rate;
+   if (!(totalRate > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: exosphere total production rate must be positive");
+   const double shadow = std::max(J.ionization_factor_shadow, 0.0);
+   for (long long n = 0; n < g.N; ++n) {
+      const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((long long)g.nx * g.ny));
+      const double xc = g.x_min + (i + 0.5) * g.dx, yc = g.y_min + (j + 0.5) * g.dx, zc = g.z_min + (k + 0.5) * g.dx;
+      const double f = (xc < 0 && yc * yc + zc * zc < Rsh * Rsh) ? shadow : 1.0;
+      const double r = perDt * cellExo[n] * f * ionRate / totalRate;
+      if (r > 0) {
+         cells.push_back((int)n);
+         rates.push_back(r);
+      }
+   }
+   h.d.w = totalRate * g.dt / perDt;
+   h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
+   return RHGPU_OK;
+}
+}  // namespace
+
 extern "C" {
 
 const char* rhgpu_last_error(void) { return g_err.c_str(); }
@@ -1654,7 +1719,7 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    }
    cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
    cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
-   for (auto& h : c->inj) cudaFree(h.cells);
+   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); }
    cudaFree(c->injCnt);
    cudaFree(c->finc); cudaFree(c->fover); cudaFree(c->ffill); cudaFree(c->fmaxInc);
    cudaFree(c->mkey); cudaFree(c->mval); cudaFree(c->mbkt);
@@ -1875,7 +1940,7 @@ int phasePush(rhgpu_ctx* c) {
    if (!c->inj.empty() && c->path == RHGPU_PATH_FP32) {
       // the FP32 form stores one weight per species: a source must inject that weight
       for (const InjHost& h : c->inj) {
-         if (h.d.ncells == 0 || !(h.d.perCellPerDt > 0)) continue;
+         if (h.d.ncells == 0 || !(h.d.w > 0)) continue;
          double& ws = c->f32[h.d.species].w;
          if (ws == 0.0) {   // a species uploaded without particles takes its source's weight
             ws = h.d.w;
@@ -1989,7 +2054,7 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
    if (!c || n < 0 || (n > 0 && !inj)) return fail(RHGPU_ERR_ARG, "set_injectors: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   for (auto& h : c->inj) cudaFree(h.cells);
+   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); }
    c->inj.clear();
    c->injKeyMax = 0;
    if (!c->injCnt) {
@@ -2054,6 +2119,15 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
                      if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
                   if (in) cells.push_back(i + g.nx * (j + g.ny * k));
                }
+      } else if (J.type == RHGPU_INJECT_EXOSPHERE) {
+         std::vector<double> rates;
+         int rc = exoRates(c, J, h, cells, rates);
+         if (rc) return rc;
+         if (!rates.empty()) {
+            RH_CUDA(cudaMalloc(&h.rates, sizeof(double) * rates.size()));
+            RH_CUDA(cudaMemcpy(h.rates, rates.data(), sizeof(double) * rates.size(), cudaMemcpyHostToDevice));
+         }
+         h.d.rates = h.rates;
       } else {
          return fail(RHGPU_ERR_ARG, "set_injectors: unknown type");
       }

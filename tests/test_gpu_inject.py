@@ -126,3 +126,68 @@ def test_exact_path_refuses_sources(lib):
             ctx.step(1)
     finally:
         ctx.close()
+
+
+def exo_box():
+    """A planet of 500 km radius at the centre of a closed box of 24^3 cells of
+    100 km, an O+ species, an exponential neutral profile from 600 km."""
+    pop = cf.Population(name="O+", mass=16.0, charge=1.0, density=0.0, velocity=(0.0, 0.0, 0.0),
+                        temperature=1e3, ppc=1.0, accelerate=False, upstream=False)
+    return cf.Config(nx=24, ny=24, nz=24, x_min=-1.2e6, y_min=-1.2e6, z_min=-1.2e6, dx=100e3,
+                     periodic=(0, 0, 0), dt=0.05, populations=[pop], name="exo_box")
+
+
+def exo_injector(shadow=1.0, seed=5):
+    j = abi.Injector(species=0, type=abi.INJECT_EXOSPHERE, temperature=1e3, seed=seed,
+                     profile=abi.NEUTRAL_PROFILES["Exponential"], n_components=1, r0=600e3,
+                     exobase_radius=600e3, shadow_radius=600e3, ionization_rate=1e-6,
+                     ionization_factor_shadow=shadow, total_production_rate=-1.0,
+                     macroparticles_per_cell_relative=1.0, upstream_macro_ratio=400.0)
+    j.n0[0] = 1e12
+    j.H0[0] = 200e3
+    return j
+
+
+def test_exosphere_source(lib):
+    """InjectorExosphere: about macroparticles_per_cell_relative *
+    upstream_macro_ratio = 400 new ions per step (fewer: those drawn below the
+    exobase in cells that straddle it are dropped, as in the reference), all
+    above the exobase, concentrated within a few scale heights, none in
+    the shadow when its factor is zero, weight total rate * dt / 400."""
+    cfg = exo_box()
+    grid, _ = cf.initial_state(cfg)
+    for shadow in (1.0, 0.0):
+        ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[100000])
+        try:
+            ctx.set_path(abi.PATH_FAST)
+            ctx.upload_array("faceB", grid["faceB"])
+            ctx.upload_array("cellB", grid["cellB"])
+            ctx.upload_array("nodeEta", grid["nodeEta"])
+            ctx.upload_cell_flags(grid["flags"])
+            ctx.upload_particles(0, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+            ctx.set_injectors([exo_injector(shadow)])
+            ctx.step(1)
+            cnt, p = ctx.download_particles(0)
+            ic = ctx.injection_counters()[0]
+        finally:
+            ctx.close()
+        cell = np.repeat(np.arange(cfg.ncells), cnt.astype(np.int64))
+        i, j, k = cell % 24, (cell // 24) % 24, cell // 576
+        xg = -1.2e6 + i * 100e3 + p[:, 0]
+        yg = -1.2e6 + j * 100e3 + p[:, 1]
+        zg = -1.2e6 + k * 100e3 + p[:, 2]
+        r = np.sqrt(xg ** 2 + yg ** 2 + zg ** 2)
+        assert np.all(r >= 600e3)
+        assert ic["macroparticles"] == p.shape[0]
+        if shadow == 1.0:
+            assert 300 <= p.shape[0] <= 440, p.shape[0]
+            assert np.mean(r < 1.2e6) > 0.8
+            w = p[0, 6]
+            assert math.isclose(ic["weight"], p.shape[0] * w, rel_tol=1e-12)
+            vth = math.sqrt(abi.BOLTZMANN * 1e3 / (16 * abi.MASS_PROTON))
+            assert abs(p[:, 3:6].std() / vth - 1.0) < 0.15
+        else:
+            xc = -1.2e6 + (i + 0.5) * 100e3
+            rc2 = (-1.2e6 + (j + 0.5) * 100e3) ** 2 + (-1.2e6 + (k + 0.5) * 100e3) ** 2
+            assert not np.any((xc < 0) & (rc2 < 600e3 ** 2))
+            assert p.shape[0] > 0
