@@ -468,22 +468,39 @@ __global__ void k_f32_gather(GridInfo g, Fields f, FastGeom fg, F32Bufs fb, doub
    RH_CELL_PROLOGUE
    const bool bnd = g.per[0] ? (fg.nseg > 1 && i % SEG == 0) : ((i + 1) % SEG == 0);
    const int gb = g.per[0] ? i / SEG : (i + 1) / SEG;
-   double v[4];
+   // every load first (one wait for memory), the same sums in the same order
+   float4 rp[4];
+   float rb[4][4];
+#pragma unroll
    for (int qq = 0; qq < 4; ++qq) {
       const int uyy = dualU(j - (qq & 1), g.ny, g.per[1]);
       const int uzz = dualU(k - (qq >> 1), g.nz, g.per[2]);
       const long long row = (long long)uyy + (long long)fg.nd[1] * uzz;
-      const float* rp = fb.RP + (((long long)qq * fg.nrows + row) * g.nx + i) * 4;
-      const float* rb = fb.RPB + (((long long)qq * fg.nrows + row) * fg.nseg + gb) * 4;
+      rp[qq] = *reinterpret_cast<const float4*>(fb.RP + (((long long)qq * fg.nrows + row) * g.nx + i) * 4);
+      if (bnd) {
+         const float* pb = fb.RPB + (((long long)qq * fg.nrows + row) * fg.nseg + gb) * 4;
+#pragma unroll
+         for (int l = 0; l < 4; ++l) rb[qq][l] = pb[l];
+      }
+   }
+   const unsigned tw = fb.touched[n >> 5];
+   unsigned long long mlo[4], mhi[4];
+#pragma unroll
+   for (int l = 0; l < 4; ++l) { mlo[l] = fb.MMlo[l * N + n]; mhi[l] = fb.MMhi[l * N + n]; }
+   double v[4];
+#pragma unroll
+   for (int qq = 0; qq < 4; ++qq) {
+      const float rv[4] = {rp[qq].x, rp[qq].y, rp[qq].z, rp[qq].w};
+#pragma unroll
       for (int l = 0; l < 4; ++l) {
-         float r = rp[l];
-         if (bnd) r = r + rb[l];
+         float r = rv[l];
+         if (bnd) r = r + rb[qq][l];
          v[l] = qq == 0 ? (double)r : v[l] + (double)r;
       }
    }
-   if (fb.touched[n >> 5] & (1u << (n & 31))) {
-      v[0] += fixedToDouble(fb.MMlo[n], fb.MMhi[n], hiR, loR);
-      for (int l = 0; l < 3; ++l) v[1 + l] += fixedToDouble(fb.MMlo[(1 + l) * N + n], fb.MMhi[(1 + l) * N + n], hiJ, loJ);
+   if (tw & (1u << (n & 31))) {
+      v[0] += fixedToDouble(mlo[0], mhi[0], hiR, loR);
+      for (int l = 0; l < 3; ++l) v[1 + l] += fixedToDouble(mlo[1 + l], mhi[1 + l], hiJ, loJ);
       for (int l = 0; l < 4; ++l) { fb.MMlo[l * N + n] = 0ull; fb.MMhi[l * N + n] = 0ull; }
    }
    double rho = v[0] * scale;
