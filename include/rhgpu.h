@@ -47,6 +47,10 @@ extern "C" {
 #define RHGPU_MASS_PROTON        1.67262192369e-27
 #define RHGPU_BOLTZMANN          1.380649e-23
 #define RHGPU_GRAVITY            6.67430e-11
+/* used by the field log's scales and energies (src/diagnostics.h:375-395, 691-704) */
+#define RHGPU_MASS_ELECTRON      9.1093837015e-31
+#define RHGPU_PERMITTIVITY       8.8541878128e-12
+#define RHGPU_SPEED_OF_LIGHT     299792458.0
 
 /* status codes */
 #define RHGPU_OK              0
@@ -364,14 +368,56 @@ int rhgpu_get_time(rhgpu_ctx* ctx, double* t_out, int64_t* timestep_out);
  * out[8*s + 0..7] per species s: N macroparticles, sum w, sum w*vx, sum w*vy,
  *   sum w*vz, sum w*|v|, sum w*v^2, max |v|;
  * then 30 field values over the cells with all neighbours outside the inner
- * field boundary (the reference's default, includeInnerCellsInFieldLog = false):
+ * field boundary (the reference's default, includeInnerCellsInFieldLog = false;
+ * rhgpu_log_open can include them):
  *   N cells, sum Bx, By, Bz, |B|, max |B|, sum |divB|, max |divB|, max |divB|/|B|,
  *   sum B^2 (cell B = mean of its two faces); sum Jix, Jiy, Jiz, |Ji|, max |Ji|;
  *   sum Epx, Epy, Epz, |Ep|, max |Ep|, sum Ep^2; sum nodeEx, Ey, Ez, |E|, max |E|,
  *   sum E^2; sum |Ue x B|^2; max |Ue|; sum cellRhoQi.
+ * With n >= 8*n_species + 36, six more: the spatial, temporal and velocity
+ * scales of the field log over the same cells (diagnostics.h:375-395): min and
+ * max electron inertial length (from cellRhoQi > 0), min and max proton
+ * inertial length and max Alfven speed (from the total ion mass density: every
+ * species' w*m in the particle's cell, /dV, floored at
+ * min_ion_charge_density*m_p/e), min ion Larmor period (from |B| > 0); where no
+ * cell qualifies, the reference's starting values (DBL_MAX for minima,
+ * -DBL_MAX for inertial-length maxima, 0 for the Alfven speed).
  * Sums are formed per block in a fixed tree and added on the host in block
- * order: deterministic, equal to the reference's sequential sums to round-off. */
+ * order: deterministic, equal to the reference's sequential sums to round-off.
+ * The mass density is the reference's sequential sum on the exact path and an
+ * exact fixed-point sum on the fast and FP32 paths. */
 int rhgpu_reduce_diagnostics(rhgpu_ctx* ctx, double* out, int32_t n);
+
+/* Population and field log files (Hybrid.log_interval logging of
+ * logWriteParticleField, src/diagnostics.h:405-818, with the files and headers
+ * of src/user.cpp:2147-2231): pop001_<name>.log per species and field.log in
+ * `directory`, numbers in scientific notation with a sign and `precision`
+ * digits (Hybrid.log_precision, 10 by default). */
+typedef struct rhgpu_log_config {
+   const char* directory;
+   const char* const* species_names;  /* n_species names (ParticleSpecies name) */
+   int32_t precision;
+   int32_t include_inner_cells;       /* Hybrid.includeInnerCellsInFieldLog */
+   double max_B_stop_run;             /* Constraints.max_magnetic_field_stop_run [T] */
+} rhgpu_log_config;
+
+/* Opens (truncates) the log files, writes their headers, zeroes the log
+ * counters and starts the rate interval at the current simulation time. */
+int rhgpu_log_open(rhgpu_ctx* ctx, const rhgpu_log_config* cfg);
+
+/* One log step (the caller's Hybrid.log_interval): appends one line to every
+ * log file with the current state and the counter rates since the previous log
+ * step, then zeroes the log counters (rhgpu_get_counters and
+ * rhgpu_get_injection_counters read zero afterwards) as the reference does.
+ * *stop_run is set to 1 when max |faceB| exceeds max_B_stop_run (the reference
+ * stops the run), else 0. The reference's main-log text (warnings, the stop
+ * message and, with main_log_diagnostics != 0, the diagnostics block) is
+ * copied to `messages` (up to messages_cap bytes, NUL-terminated; may be NULL). */
+int rhgpu_log_write(rhgpu_ctx* ctx, int32_t main_log_diagnostics, int32_t* stop_run, char* messages,
+                    int32_t messages_cap);
+
+/* Flushes and closes the log files (also done by rhgpu_destroy). */
+int rhgpu_log_close(rhgpu_ctx* ctx);
 
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void* rhgpu_stream(rhgpu_ctx* ctx);

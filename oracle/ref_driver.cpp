@@ -17,6 +17,10 @@
  *   addRemoteUpdates (finalize /dV, rho clamp) particle_accumulator.cpp:260-335
  *   applyBoundaryConditions                    user.cpp:128
  *   propagateB                                 user.cpp:134
+ * rhref_log_open / rhref_log_write run the reference's own log writer
+ * (diagnostics::logWriteParticleField, src/diagnostics.h:405-818) on the
+ * current state into files opened here without headers (the headers come
+ * from src/user.cpp, which is not built).
  * Only one rhref context may exist at a time: the reference keeps its state
  * in the static struct Hybrid (src/hybrid.h:161).
  */
@@ -33,6 +37,9 @@
 #include "particle_accumulator.h"
 #include "particle_propagator_boris_buneman.h"
 #include "particle_boundary_cond_hybrid.h"
+#include "diagnostics.h"
+
+#include <fstream>
 
 #include "oracle_common.h"
 
@@ -120,6 +127,9 @@ void setHybridStatics(RefCtx& c) {
    Hybrid::logCounterParticleEscapeKineticEnergy.assign(MAX_SPECIES,0.0);
    Hybrid::logCounterParticleImpact.assign(MAX_SPECIES,0.0);
    Hybrid::logCounterParticleImpactKineticEnergy.assign(MAX_SPECIES,0.0);
+   Hybrid::logCounterParticleInject.assign(MAX_SPECIES,0.0);
+   Hybrid::logCounterParticleInjectMacroparticles.assign(MAX_SPECIES,0.0);
+   Hybrid::logCounterParticleInjectKineticEnergy.assign(MAX_SPECIES,0.0);
    Hybrid::logCounterFieldMaxCellUe = 0;
    Hybrid::logCounterFieldMaxNodeUe = 0;
    Hybrid::logCounterFieldMaxVw = 0;
@@ -269,6 +279,7 @@ int rhref_create(const rhgpu_params* params,int32_t n_species,const rhgpu_specie
       S.accumulate = sp[s].accumulate != 0;
       S.accelerate = sp[s].accelerate != 0;
       c->particleIDs.push_back(pg.addUserDataDynamic<PARTICLE>());
+      c->plists[s].particleDataID = c->particleIDs[s];
    }
    setHybridStatics(*c);
    Accumulator* pool = accumulatorPool();
@@ -440,6 +451,66 @@ int rhref_get_counters(void* h,double* out,int32_t n) {
       q[4] = Hybrid::logCounterParticleImpactKineticEnergy[s];
    }
    for (int i=0;i<n && i<(int)v.size();++i) out[i] = v[i];
+   return RHGPU_OK;
+}
+
+/* the log files of logWriteParticleField: pop<NNN>_<name>.log and field.log in
+ * cfg->directory, number format as src/user.cpp:2158-2187 sets it, no headers */
+int rhref_log_open(void* h,const rhgpu_log_config* cfg) {
+   RefCtx* c = (RefCtx*)h;
+   if (!cfg || !cfg->directory || !cfg->species_names) return fail(RHGPU_ERR_ARG,"rhref_log_open: bad arguments");
+   for (std::ofstream* o: Hybrid::logParticle) delete o;
+   Hybrid::logParticle.clear();
+   if (Hybrid::logField.is_open()) Hybrid::logField.close();
+   const int prec = cfg->precision > 0 ? cfg->precision : 10;
+   for (int s=0;s<c->nspecies;++s) {
+      const std::string zero = s < 10 ? "00" : (s < 100 ? "0" : "");
+      const std::string fn = std::string(cfg->directory) + "/pop" + zero + std::to_string(s+1) + "_" + cfg->species_names[s] + ".log";
+      Hybrid::logParticle.push_back(new std::ofstream(fn.c_str(),std::ios_base::out));
+      Hybrid::logParticle.back()->precision(prec);
+      (*Hybrid::logParticle.back()) << std::scientific << std::showpos;
+   }
+   Hybrid::logField.open((std::string(cfg->directory) + "/field.log").c_str(),std::ios_base::out);
+   Hybrid::logField.precision(prec);
+   Hybrid::logField << std::scientific << std::showpos;
+   Hybrid::includeInnerCellsInFieldLog = cfg->include_inner_cells != 0;
+   Hybrid::maxBStopRun = cfg->max_B_stop_run;
+   Hybrid::writeMainLogDiagnosticsAfterLogStep = false;
+   Hybrid::logCounterTimeStart = c->sim.t;
+   for (int s=0;s<MAX_SPECIES;++s) {
+      Hybrid::logCounterParticleEscape[s] = 0; Hybrid::logCounterParticleImpact[s] = 0;
+      Hybrid::logCounterParticleInject[s] = 0; Hybrid::logCounterParticleInjectMacroparticles[s] = 0;
+      Hybrid::logCounterParticleEscapeKineticEnergy[s] = 0; Hybrid::logCounterParticleImpactKineticEnergy[s] = 0;
+      Hybrid::logCounterParticleInjectKineticEnergy[s] = 0; Hybrid::logCounterParticleMaxVi[s] = 0;
+   }
+   Hybrid::logCounterFieldMaxCellUe = 0; Hybrid::logCounterFieldMaxNodeUe = 0; Hybrid::logCounterFieldMaxVw = 0;
+   Hybrid::logCounterFieldMaxE = 0; Hybrid::logCounterFieldMinCellRhoQi = 0; Hybrid::logCounterFieldMinNodeRhoQi = 0;
+   return RHGPU_OK;
+}
+
+int rhref_log_write(void* h,int32_t main_log,int32_t* stop_run,char* messages,int32_t cap) {
+   RefCtx* c = (RefCtx*)h;
+   if (Hybrid::logParticle.size() != (size_t)c->nspecies) return fail(RHGPU_ERR_STATE,"rhref_log_write: rhref_log_open first");
+   /* the particle lists' sizes follow the per-cell counts the plugins keep */
+   std::vector<ParticleListBase*> lists;
+   for (int s=0;s<c->nspecies;++s) {
+      pargrid::DataWrapper<PARTICLE> w = c->sc.pargrid.getUserDataDynamic<PARTICLE>(c->particleIDs[s]);
+      for (size_t b=0;b<c->counts[s].size();++b) w.resize((pargrid::CellID)b,c->counts[s][b]);
+      lists.push_back(&c->plists[s]);
+   }
+   Hybrid::writeMainLogDiagnosticsAfterLogStep = main_log != 0;
+   const bool ok = diagnostics::logWriteParticleField(c->sim,c->sc,lists);
+   for (std::ofstream* o: Hybrid::logParticle) o->flush();
+   Hybrid::logField.flush();
+   if (stop_run) *stop_run = ok ? 0 : 1;
+   if (messages && cap > 0) messages[0] = 0;
+   return RHGPU_OK;
+}
+
+int rhref_log_close(void*) {
+   for (std::ofstream* o: Hybrid::logParticle) { o->close(); delete o; }
+   Hybrid::logParticle.clear();
+   if (Hybrid::logField.is_open()) Hybrid::logField.close();
    return RHGPU_OK;
 }
 

@@ -25,6 +25,9 @@ inline int MPI_Type_contiguous(int,MPI_Datatype,MPI_Datatype* t) { *t = 0; retur
 inline int MPI_Reduce(const void* in,void* out,int n,MPI_Datatype t,MPI_Op,int,MPI_Comm) {
    std::memcpy(out,in,(size_t)n*(t == MPI_DOUBLE ? 8 : 4)); return 0;
 }
+inline int MPI_Allreduce(const void* in,void* out,int n,MPI_Datatype t,MPI_Op,MPI_Comm) {
+   std::memcpy(out,in,(size_t)n*(t == MPI_DOUBLE ? 8 : 4)); return 0;
+}
 inline int MPI_Bcast(void*,int,MPI_Datatype,int,MPI_Comm) { return 0; }
 inline double MPI_Wtime() {
    using namespace std::chrono;

@@ -45,6 +45,9 @@ namespace constants {
    const Real BOLTZMANN         = RHGPU_BOLTZMANN;
    const Real GRAVITY           = RHGPU_GRAVITY;
    const Real EV_TO_KELVIN      = 11604.51812;
+   const Real MASS_ELECTRON     = RHGPU_MASS_ELECTRON;
+   const Real PERMITTIVITY      = RHGPU_PERMITTIVITY;
+   const Real SPEED_LIGHT       = RHGPU_SPEED_OF_LIGHT;
 }
 
 namespace profile {
@@ -74,6 +77,7 @@ namespace pargrid {
    typedef uint32_t CellID;
    typedef unsigned int DataID;
    typedef unsigned int StencilID;
+   typedef size_t ArraySizetype;
    const StencilID DEFAULT_STENCIL = 0;
    const StencilID INVALID_STENCILID = std::numeric_limits<StencilID>::max();
    const DataID INVALID_DATAID = std::numeric_limits<DataID>::max();
@@ -92,6 +96,7 @@ namespace pargrid {
       explicit DataWrapper(DynamicStore* s = nullptr): store(s) { }
       T** data() const { return reinterpret_cast<T**>(store->ptrs.data()); }
       const size_t* size() const { return store->sizes.data(); }
+      size_t size(CellID b) const { return store->sizes[b]; }
       bool resize(CellID b,size_t n) {
          store->cells[b].resize(n*sizeof(T) + 16);
          store->ptrs[b] = store->cells[b].data();
@@ -141,6 +146,7 @@ namespace pargrid {
       const std::vector<CellID>& getBoundaryCells(StencilID) const { return boundary; }
       const std::vector<CellID>& getExteriorCells() const { return exterior; }
       CellID getNumberOfLocalCells() const { return (CellID)flags.size(); }
+      int getRank() const { return 0; }
       CellID getNumberOfAllCells() const { return (CellID)flags.size(); }
       const std::vector<CellID>& getGlobalIDs() const { return globalIDs; }
       std::vector<double>& getCellWeights() { cellWeights.resize(flags.size()); return cellWeights; }
@@ -189,8 +195,18 @@ namespace pargrid {
    };
 }
 
+/* VLSV writer stand-in: the reduced-state writer in diagnostics.h compiles
+ * against it; the oracle never writes VLSV files (every call fails). */
+struct VlsvWriterStub {
+   bool open(const std::string&,MPI_Comm,int) { return false; }
+   template<class T> bool writeArray(const std::string&,const std::map<std::string,std::string>&,uint64_t,uint64_t,const T*) { return false; }
+   bool close() { return false; }
+   uint64_t getBytesWritten() const { return 0; }
+};
+
 struct SimulationClasses {
    pargrid::ParGrid pargrid;
+   VlsvWriterStub vlsv;
    Logger logger;
    Random random;
    std::vector<Real> blockCoordinates; /* 3 per cell: minimum corner */

@@ -59,11 +59,16 @@ DIAG_FIELD = ["N_cells", "sumBx", "sumBy", "sumBz", "sumB", "maxB", "sumDivB", "
               "sumCellEpx", "sumCellEpy", "sumCellEpz", "sumCellEp", "maxCellEp", "sumCellEp2",
               "sumNodeEx", "sumNodeEy", "sumNodeEz", "sumNodeE", "maxNodeE", "sumNodeE2",
               "sumCellE2", "maxUe", "sumCellRhoQi"]
+# the six scales that follow with n >= 8*n_species + 36 (LogDataField names)
+DIAG_SCALES = ["minInerLengthElectron", "maxInerLengthElectron", "minInerLengthProton", "maxInerLengthProton",
+               "minTLarmor", "maxVAlfven"]
 
 # rhgpu.h: physical constants
 PERMEABILITY = 1.2566370614359173e-06
 CHARGE_ELEMENTARY = 1.602176634e-19
 MASS_PROTON = 1.67262192369e-27
+MASS_ELECTRON = 9.1093837015e-31
+PERMITTIVITY = 8.8541878128e-12
 BOLTZMANN = 1.380649e-23
 GRAVITY = 6.67430e-11
 
@@ -161,6 +166,9 @@ _OPTIONAL = {
     "set_injectors": [_P, C.c_int32, C.c_void_p],
     "get_injection_counters": [_P, _D, C.c_int32],
     "philox4x32": [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+    "log_open": [_P, C.c_void_p],
+    "log_write": [_P, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_int32],
+    "log_close": [_P],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p, "philox4x32": None}
 
@@ -183,6 +191,12 @@ class Injector(C.Structure):
                 ("ionization_rate", C.c_double), ("ionization_factor_shadow", C.c_double),
                 ("total_production_rate", C.c_double), ("macroparticles_per_cell_relative", C.c_double),
                 ("upstream_macro_ratio", C.c_double)]
+
+
+class LogConfig(C.Structure):
+    """rhgpu_log_config: where and how the population and field logs are written."""
+    _fields_ = [("directory", C.c_char_p), ("species_names", C.POINTER(C.c_char_p)), ("precision", C.c_int32),
+                ("include_inner_cells", C.c_int32), ("max_B_stop_run", C.c_double)]
 
 
 def _ptr(a: np.ndarray, ct):
@@ -332,13 +346,33 @@ class Context:
         self.lib.call("device_errors", self.h, C.byref(w))
         return w.value
 
-    def reduce_diagnostics(self) -> dict:
-        """rhgpu_reduce_diagnostics: the population log per species and the field log."""
-        n = 8 * self.nspecies + 30
+    def reduce_diagnostics(self, scales: bool = False) -> dict:
+        """rhgpu_reduce_diagnostics: the population log per species and the field
+        log (with `scales`, also the field log's spatial, temporal and velocity scales)."""
+        n = 8 * self.nspecies + 30 + (6 if scales else 0)
         out = np.zeros(n, dtype=np.float64)
         self.lib.call("reduce_diagnostics", self.h, _ptr(out, C.c_double), n)
         pops = [dict(zip(DIAG_PARTICLE, out[8 * s:8 * s + 8])) for s in range(self.nspecies)]
-        return {"populations": pops, "field": dict(zip(DIAG_FIELD, out[8 * self.nspecies:]))}
+        return {"populations": pops, "field": dict(zip(DIAG_FIELD + DIAG_SCALES, out[8 * self.nspecies:]))}
+
+    def log_open(self, directory: str, species_names, precision: int = 10, include_inner_cells: bool = False,
+                 max_B_stop_run: float = float("inf")):
+        """rhgpu_log_open: pop<NNN>_<name>.log per species and field.log in `directory`."""
+        names = (C.c_char_p * self.nspecies)(*[n.encode() for n in species_names])
+        self._log_cfg = LogConfig(str(directory).encode(), names, precision, 1 if include_inner_cells else 0,
+                                  max_B_stop_run)
+        self._log_names = names
+        self.lib.call("log_open", self.h, C.cast(C.byref(self._log_cfg), C.c_void_p))
+
+    def log_write(self, main_log_diagnostics: bool = False):
+        """rhgpu_log_write: one line per log file; returns (stop_run, main-log text)."""
+        stop = C.c_int32()
+        buf = C.create_string_buffer(1 << 14)
+        self.lib.call("log_write", self.h, 1 if main_log_diagnostics else 0, C.byref(stop), buf, len(buf))
+        return bool(stop.value), buf.value.decode()
+
+    def log_close(self):
+        self.lib.call("log_close", self.h)
 
     def set_timing(self, on: bool):
         self.lib.call("set_timing", self.h, 1 if on else 0)

@@ -614,4 +614,15 @@ k_diag_particles_f32(F32Buf B, const long long* base, long long NS, double w, do
    blockReduce(v, DIAG_P_MAX, sm, part + (long long)blockIdx.x * DIAG_P);
 }
 
+// total ion mass density (logCalcParticle, diagnostics.h:223-238) on the FP32
+// form: every particle adds its species' w*m to its cell as an exact fixed-point sum
+__global__ void k_diag_rhom_f32(F32Buf B, const long long* base, long long NS, double wm, double scale,
+                                unsigned long long* lo, unsigned long long* hi) {
+   for (long long S = blockIdx.x; S < NS; S += gridDim.x)
+      for (int r = threadIdx.x; r < B.cnt[S]; r += blockDim.x) {
+         const long long n = B.cell[base[S] + r];
+         add128(lo + n, hi + n, wm, scale);
+      }
+}
+
 }  // namespace rh

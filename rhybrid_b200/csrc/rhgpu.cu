@@ -23,6 +23,7 @@
 #include "k_f32.cuh"
 #include "k_denoise.cuh"
 #include "k_inject.cuh"
+#include "rh_logs.h"
 
 using namespace rh;
 
@@ -227,7 +228,14 @@ struct rhgpu_ctx {
    unsigned char* flxTmp = nullptr;
    long long flxTmpCap = 0;
    long long capHint[MAX_SPECIES] = {};
-   double* diagPart = nullptr;          // DIAG_BLOCKS x DIAG_F partial rows of rhgpu_reduce_diagnostics
+   double* diagPart = nullptr;          // DIAG_BLOCKS x DIAG_FS partial rows of rhgpu_reduce_diagnostics
+   double* rhoM = nullptr;              // N: total ion mass density of the field log
+   unsigned long long* rhoMfix = nullptr;   // 2N: its fixed-point sums (lo, hi)
+   // log files (rhgpu_log_*)
+   LogFiles* logs = nullptr;
+   int logInner = 0;
+   double logTStart = 0.0;
+   double logMaxB = 0.0;
    // FP32 precision form
    bool f32ready = false;
    F32Host f32[MAX_SPECIES];
@@ -1644,7 +1652,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->ftmpInc64, sizeof(long long) * (nb + 1));
    alloc((void**)&c->foffInc, sizeof(long long) * (nb + 1));
    alloc((void**)&c->fover, 2 * sizeof(unsigned long long));
-   alloc((void**)&c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_F);
+   alloc((void**)&c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_FS);
    if (!rc) {
       // MM starts at zero; k_fast_gather clears what a step touched
       if (cudaMemset(c->fb.MMlo, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
@@ -1726,6 +1734,9 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->sortTmp); cudaFree(c->fcap); cudaFree(c->ffirst); cudaFree(c->ftmp64); cudaFree(c->ftmpCellStart);
    cudaFree(c->ftmpInc64); cudaFree(c->foffInc); cudaFree(c->fsort); cudaFree(c->fsortSlots); cudaFree(c->flxTmp);
    cudaFree(c->diagPart);
+   cudaFree(c->rhoM);
+   cudaFree(c->rhoMfix);
+   if (c->logs) { c->logs->close(); delete c->logs; c->logs = nullptr; }
    for (int s = 0; s < c->ns; ++s) {
       F32Host& h = c->f32[s];
       for (int b = 0; b < 2; ++b) {
@@ -2226,23 +2237,87 @@ int rhgpu_last_launch_count(rhgpu_ctx* c, int64_t* out) {
 
 namespace {
 // adds the DIAG_BLOCKS partial rows of width w in block order (sums, or maxima where maxMask has the bit)
-void diagCombine(const std::vector<double>& h, int w, unsigned long long maxMask, double* out) {
+void diagCombine(const std::vector<double>& h, int w, unsigned long long maxMask, double* out,
+                 unsigned long long minMask = 0ull) {
    for (int q = 0; q < w; ++q) {
-      double a = 0.0;
+      double a = ((minMask >> q) & 1ull) ? INFINITY : 0.0;
       for (int b = 0; b < DIAG_BLOCKS; ++b) {
          const double x = h[(size_t)b * w + q];
-         a = ((maxMask >> q) & 1ull) ? std::max(a, x) : a + x;
+         a = ((maxMask >> q) & 1ull) ? std::max(a, x) : ((minMask >> q) & 1ull) ? std::min(a, x) : a + x;
       }
       out[q] = a;
    }
 }
-}  // namespace
 
-int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
-   if (!c || !out) return fail(RHGPU_ERR_ARG, "bad arguments");
-   if (n < DIAG_P * c->ns + DIAG_F) return fail(RHGPU_ERR_ARG, "reduce_diagnostics: out needs 8*n_species + 30 doubles");
+// total ion mass density per cell into c->rhoM (logCalcParticle, diagnostics.h:223-238)
+int massDensity(rhgpu_ctx* c) {
+   const long long N = c->g.N;
+   if (!c->rhoM) {
+      RH_CUDA(cudaMalloc(&c->rhoM, sizeof(double) * N));
+      RH_CUDA(cudaMalloc(&c->rhoMfix, sizeof(unsigned long long) * 2 * N));
+   }
+   const double minRhoM = c->P.min_ion_charge_density * RHGPU_MASS_PROTON / RHGPU_CHARGE_ELEMENTARY;
+   if (c->path == RHGPU_PATH_EXACT) {
+      MassSet M;
+      std::memset(&M, 0, sizeof M);
+      M.ns = c->ns;
+      for (int s = 0; s < c->ns; ++s) { M.P[s] = c->ps[s]; M.m[s] = c->sp[s].m; }
+      k_diag_rhom_cell<<<blocks1d(N, 256), 256, 0, c->stream>>>(M, N, c->g.dV, minRhoM, c->rhoM);
+      RH_CUDA(cudaGetLastError());
+      return RHGPU_OK;
+   }
+   // fixed-point scale from the largest w*m: every addend below 2^62
+   double wm[MAX_SPECIES] = {};
+   double big = 0.0;
+   for (int s = 0; s < c->ns; ++s) {
+      double w = 0.0;
+      if (c->path == RHGPU_PATH_FAST) {
+         const SegHost& h = c->seg[s];
+         if (!h.a[h.cur][0]) continue;
+         unsigned long long* mw = (unsigned long long*)c->fover;
+         RH_CUDA(cudaMemsetAsync(mw, 0, sizeof(unsigned long long), c->stream));
+         k_fast_max_abs_w<<<(unsigned)c->fg.NS, 128, 0, c->stream>>>(segView(h, h.cur), h.base, mw);
+         RH_CUDA(cudaGetLastError());
+         unsigned long long bits = 0;
+         RH_CUDA(cudaMemcpyAsync(&bits, mw, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+         RH_CUDA(cudaStreamSynchronize(c->stream));
+         std::memcpy(&w, &bits, sizeof w);
+      } else {
+         if (!c->f32ready || !c->f32[s].cell[c->f32[s].cur]) continue;
+         w = std::fabs(c->f32[s].w);
+      }
+      wm[s] = w * c->sp[s].m;
+      big = std::max(big, wm[s]);
+   }
+   int e;
+   std::frexp(big > 0 ? big : 1.0, &e);
+   const int k = 62 - e;
+   const double scale = std::ldexp(1.0, k);
+   unsigned long long *lo = c->rhoMfix, *hi = c->rhoMfix + N;
+   RH_CUDA(cudaMemsetAsync(c->rhoMfix, 0, sizeof(unsigned long long) * 2 * N, c->stream));
+   for (int s = 0; s < c->ns; ++s) {
+      if (wm[s] == 0.0) continue;
+      if (c->path == RHGPU_PATH_FAST) {
+         const SegHost& h = c->seg[s];
+         k_diag_rhom_seg<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(c->g, c->fg, segView(h, h.cur), h.base, c->sp[s].m,
+                                                                      scale, lo, hi);
+      } else {
+         const F32Host& h = c->f32[s];
+         k_diag_rhom_f32<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(f32View(h, h.cur), h.base, c->fg.NS,
+                                                                      h.w * c->sp[s].m, scale, lo, hi);
+      }
+      RH_CUDA(cudaGetLastError());
+   }
+   k_diag_rhom_finish<<<blocks1d(N, 256), 256, 0, c->stream>>>(lo, hi, N, std::ldexp(1.0, 64 - k), std::ldexp(1.0, -k),
+                                                                c->g.dV, minRhoM, c->rhoM);
+   RH_CUDA(cudaGetLastError());
+   return RHGPU_OK;
+}
+
+// the population and field reductions into out (8 ns + 30 values, + 6 scales when withScales)
+int diagnostics(rhgpu_ctx* c, double* out, bool withScales) {
    RH_CUDA(cudaSetDevice(c->device));
-   std::vector<double> h((size_t)DIAG_BLOCKS * DIAG_F);
+   std::vector<double> h((size_t)DIAG_BLOCKS * DIAG_FS);
    for (int s = 0; s < c->ns; ++s) {
       double* o = out + DIAG_P * s;
       bool launched = false;
@@ -2272,11 +2347,131 @@ int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
       RH_CUDA(cudaStreamSynchronize(c->stream));
       diagCombine(h, DIAG_P, DIAG_P_MAX, o);
    }
-   k_diag_field<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(c->g, c->f, c->diagPart);
+   if (withScales) {
+      const int rc = massDensity(c);
+      if (rc) return rc;
+   }
+   k_diag_field<<<DIAG_BLOCKS, DIAG_THREADS, 0, c->stream>>>(c->g, c->f, withScales ? c->rhoM : nullptr, c->logInner,
+                                                             c->diagPart);
    RH_CUDA(cudaGetLastError());
-   RH_CUDA(cudaMemcpyAsync(h.data(), c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_F, cudaMemcpyDeviceToHost, c->stream));
+   RH_CUDA(cudaMemcpyAsync(h.data(), c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_FS, cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   diagCombine(h, DIAG_F, DIAG_F_MAX, out + DIAG_P * c->ns);
+   double f[DIAG_FS];
+   diagCombine(h, DIAG_FS, DIAG_F_MAX, f, DIAG_F_MIN);
+   double* o = out + DIAG_P * c->ns;
+   for (int q = 0; q < DIAG_F; ++q) o[q] = f[q];
+   if (withScales) {
+      // min/max de, min/max di, min Larmor period, max Alfven speed
+      logScales(f[30], f[31], f[32], f[33], f[5], RHGPU_MASS_ELECTRON, RHGPU_MASS_PROTON, RHGPU_CHARGE_ELEMENTARY,
+                RHGPU_PERMEABILITY, o + DIAG_F);
+      o[DIAG_F + 5] = f[34];
+   }
+   return RHGPU_OK;
+}
+
+// the log counters back to zero (logWriteParticleField, diagnostics.h:777-800)
+int zeroLogCounters(rhgpu_ctx* c) {
+   RH_CUDA(cudaMemsetAsync(c->cntU, 0, sizeof(unsigned long long) * NCNT_U, c->stream));
+   RH_CUDA(cudaMemsetAsync(c->cntD, 0, sizeof(double) * 4 * MAX_SPECIES, c->stream));
+   if (c->injCnt) RH_CUDA(cudaMemsetAsync(c->injCnt, 0, sizeof(double) * 3 * MAX_SPECIES, c->stream));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   return RHGPU_OK;
+}
+}  // namespace
+
+int rhgpu_reduce_diagnostics(rhgpu_ctx* c, double* out, int32_t n) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "bad arguments");
+   if (n < DIAG_P * c->ns + DIAG_F) return fail(RHGPU_ERR_ARG, "reduce_diagnostics: out needs 8*n_species + 30 doubles");
+   return diagnostics(c, out, n >= DIAG_P * c->ns + DIAG_F + 6);
+}
+
+int rhgpu_log_open(rhgpu_ctx* c, const rhgpu_log_config* cfg) {
+   if (!c || !cfg || !cfg->directory || !cfg->species_names) return fail(RHGPU_ERR_ARG, "log_open: bad arguments");
+   std::vector<LogSpecies> sp(c->ns);
+   for (int s = 0; s < c->ns; ++s) {
+      if (!cfg->species_names[s]) return fail(RHGPU_ERR_ARG, "log_open: a species name is NULL");
+      sp[s].name = cfg->species_names[s];
+      sp[s].m = c->sp[s].m;
+      sp[s].q = c->sp[s].q;
+   }
+   if (!c->logs) c->logs = new LogFiles();
+   std::string err;
+   if (!c->logs->open(cfg->directory, sp, cfg->precision > 0 ? cfg->precision : 10, err)) return fail(RHGPU_ERR_ARG, "log_open: " + err);
+   c->logInner = cfg->include_inner_cells ? 1 : 0;
+   c->logMaxB = cfg->max_B_stop_run;
+   c->logTStart = c->t;
+   RH_CUDA(cudaSetDevice(c->device));
+   return zeroLogCounters(c);
+}
+
+int rhgpu_log_write(rhgpu_ctx* c, int32_t main_log_diagnostics, int32_t* stop_run, char* messages, int32_t messages_cap) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   if (!c->logs || !c->logs->isOpen()) return fail(RHGPU_ERR_STATE, "log_write: rhgpu_log_open first");
+   const int ns = c->ns;
+   std::vector<double> d(DIAG_P * ns + DIAG_F + 6);
+   int rc = diagnostics(c, d.data(), true);
+   if (rc) return rc;
+   std::vector<double> cnt(RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES * ns);
+   rc = rhgpu_get_counters(c, cnt.data(), (int32_t)cnt.size());
+   if (rc) return rc;
+   std::vector<double> inj(3 * ns, 0.0);
+   if (c->injCnt) RH_CUDA(cudaMemcpy(inj.data(), c->injCnt, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost));
+   LogStep L;
+   L.t = c->t;
+   L.dt = c->P.dt;
+   L.dx = c->P.dx;
+   L.dV = c->g.dV;
+   L.tStart = c->logTStart;
+   L.timestep = c->timestep;
+   L.permeability = RHGPU_PERMEABILITY;
+   L.permittivity = RHGPU_PERMITTIVITY;
+   L.pop.resize(ns);
+   L.pc.assign(ns, std::vector<double>(LPC_COUNT, 0.0));
+   for (int s = 0; s < ns; ++s) {
+      const double* p = &d[DIAG_P * s];
+      L.pop[s] = LogPopulation{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7]};
+      const double* q = &cnt[RHGPU_NUM_FIELD_COUNTERS + RHGPU_CNT_PER_SPECIES * s];
+      std::vector<double>& pc = L.pc[s];
+      pc[LPC_MAXVI] = q[0];
+      pc[LPC_ESCAPE] = q[1];
+      pc[LPC_ESCAPE_KE] = q[2];
+      pc[LPC_IMPACT] = q[3];
+      pc[LPC_IMPACT_KE] = q[4];
+      pc[LPC_INJECT] = inj[3 * s + 0];
+      pc[LPC_INJECT_MACRO] = inj[3 * s + 1];
+      pc[LPC_INJECT_KE] = inj[3 * s + 2];
+   }
+   const double* f = &d[DIAG_P * ns];
+   LogField& F = L.f;
+   F.nCells = f[0];
+   F.sumBx = f[1]; F.sumBy = f[2]; F.sumBz = f[3]; F.sumB = f[4]; F.maxB = f[5];
+   F.sumDivB = f[6]; F.maxDivB = f[7]; F.maxDivBPerB = f[8]; F.sumB2 = f[9];
+   F.sumJx = f[10]; F.sumJy = f[11]; F.sumJz = f[12]; F.sumJ = f[13]; F.maxJ = f[14];
+   F.sumEpx = f[15]; F.sumEpy = f[16]; F.sumEpz = f[17]; F.sumEp = f[18]; F.maxEp = f[19]; F.sumEp2 = f[20];
+   F.sumEx = f[21]; F.sumEy = f[22]; F.sumEz = f[23]; F.sumE = f[24]; F.maxE = f[25]; F.sumE2 = f[26];
+   F.sumCellE2 = f[27]; F.maxUe = f[28];
+   F.minDe = f[30]; F.maxDe = f[31]; F.minDi = f[32]; F.maxDi = f[33]; F.minTLarmor = f[34]; F.maxVA = f[35];
+   L.fc[LFC_MAX_CELL_UE] = cnt[RHGPU_CNT_FIELD_MAX_CELL_UE];
+   L.fc[LFC_MAX_NODE_UE] = cnt[RHGPU_CNT_FIELD_MAX_NODE_UE];
+   L.fc[LFC_MAX_VW] = cnt[RHGPU_CNT_FIELD_MAX_NODE_UE];   // the reference's writer reports this counter here
+   L.fc[LFC_MAX_E] = cnt[RHGPU_CNT_FIELD_MAX_E];
+   L.fc[LFC_MIN_CELL_RHOQI] = cnt[RHGPU_CNT_FIELD_MIN_CELL_RHOQI];
+   L.fc[LFC_MIN_NODE_RHOQI] = cnt[RHGPU_CNT_FIELD_MIN_NODE_RHOQI];
+   std::string msg;
+   const bool ok = c->logs->write(L, c->logMaxB, main_log_diagnostics != 0, msg);
+   if (stop_run) *stop_run = ok ? 0 : 1;
+   if (messages && messages_cap > 0) {
+      const size_t k = std::min(msg.size(), (size_t)messages_cap - 1);
+      std::memcpy(messages, msg.data(), k);
+      messages[k] = 0;
+   }
+   c->logTStart = c->t;
+   return zeroLogCounters(c);
+}
+
+int rhgpu_log_close(rhgpu_ctx* c) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   if (c->logs) c->logs->close();
    return RHGPU_OK;
 }
 
