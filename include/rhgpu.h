@@ -419,6 +419,25 @@ int rhgpu_log_write(rhgpu_ctx* ctx, int32_t main_log_diagnostics, int32_t* stop_
 /* Flushes and closes the log files (also done by rhgpu_destroy). */
 int rhgpu_log_close(rhgpu_ctx* ctx);
 
+/* Temporal averages of the output populations (WRITE_GRID_TEMPORAL_AVERAGES,
+ * on in the reference's default build). group_of_species[s] is the output
+ * population of species s (Hybrid::outputPopVarId: species with the same
+ * output string share one; -1: none), n_groups the number of output
+ * populations. From the next step on, every accumulating species adds its CIC
+ * charge and current sums to its population's sums
+ * (particle_accumulator.cpp:148-150). Fast and exact paths; n_groups = 0
+ * switches them off. Allocates 16 * (n_groups + 1) bytes per cell. */
+int rhgpu_set_population_averages(rhgpu_ctx* ctx, int32_t n_groups, const int32_t* group_of_species);
+
+/* The output step's averages (operator_userdata.cpp:155-223), each argument
+ * NULL to skip it: cellB_average (3 per cell, interleaved) = cellAverageB /
+ * count; per output population g, n_average[g*N + n] = charge sum /
+ * (q dV) / count with q the charge of the population's first species, and
+ * v_average[(g*N + n)*3 + l] = current sum / charge sum where the charge sum
+ * is positive, else 0. The sums of what is returned restart from zero, and
+ * the average counter always does (as the reference's writer). */
+int rhgpu_output_averages(rhgpu_ctx* ctx, double* cellB_average, double* n_average, double* v_average);
+
 /* The CUDA stream (cudaStream_t) the context enqueues on. */
 void* rhgpu_stream(rhgpu_ctx* ctx);
 

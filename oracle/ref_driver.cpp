@@ -514,6 +514,59 @@ int rhref_log_close(void*) {
    return RHGPU_OK;
 }
 
+/* output populations of the temporal averages: the reference's own
+ * accumulateCell adds into their sums (particle_accumulator.cpp:148-150) */
+int rhref_set_population_averages(void* h,int32_t n_groups,const int32_t* group) {
+   RefCtx* c = (RefCtx*)h;
+   pargrid::ParGrid& pg = c->sc.pargrid;
+   Hybrid::outputPopVarId.assign(MAX_SPECIES,-1);
+   Hybrid::outputPopVarIdVector.assign(n_groups,std::vector<unsigned int>());
+   Hybrid::dataCellAverageDensityID.clear();
+   Hybrid::dataCellAverageVelocityID.clear();
+   for (int m=0;m<n_groups;++m) {
+      Hybrid::dataCellAverageDensityID.push_back(pg.addUserDataStatic<Real>(1));
+      Hybrid::dataCellAverageVelocityID.push_back(pg.addUserDataStatic<Real>(3));
+   }
+   for (int s=0;s<c->nspecies;++s) {
+      if (group[s] < -1 || group[s] >= n_groups) return fail(RHGPU_ERR_ARG,"group index out of range");
+      Hybrid::outputPopVarId[s] = group[s];
+      if (group[s] >= 0) Hybrid::outputPopVarIdVector[group[s]].push_back(s);
+   }
+   Hybrid::N_outputPopVars = n_groups;
+   return RHGPU_OK;
+}
+
+/* the output step's averages, restated from UserDataOP::writeData
+ * (operator_userdata.cpp:155-223) over the reference's sums */
+int rhref_output_averages(void* h,double* cellB,double* nOut,double* vOut) {
+   RefCtx* c = (RefCtx*)h;
+   pargrid::ParGrid& pg = c->sc.pargrid;
+   const size_t N = pg.getNumberOfLocalCells();
+   Real inv = 0.0;
+   if (Hybrid::gridTemporalAverageCounter > 0) inv = 1.0/static_cast<Real>(Hybrid::gridTemporalAverageCounter);
+   if (cellB) {
+      Real* a = pg.getUserDataStatic<Real>(Hybrid::dataCellAverageBID);
+      for (size_t n=0;n<N;++n) for (int l=0;l<3;++l) { cellB[3*n+l] = a[3*n+l]*inv; a[3*n+l] = 0.0; }
+   }
+   if (nOut || vOut) {
+      for (unsigned int m=0;m<Hybrid::N_outputPopVars;++m) {
+         Real* nA = pg.getUserDataStatic<Real>(Hybrid::dataCellAverageDensityID[m]);
+         Real* vA = pg.getUserDataStatic<Real>(Hybrid::dataCellAverageVelocityID[m]);
+         const Real q = c->species[Hybrid::outputPopVarIdVector[m][0]].q;
+         for (size_t n=0;n<N;++n) {
+            if (nOut) nOut[m*N + n] = nA[n]/(q*Hybrid::dV)*inv;
+            for (int l=0;l<3;++l) {
+               if (vOut) vOut[(m*N + n)*3 + l] = nA[n] > 0 ? vA[3*n+l]/nA[n] : 0.0;
+               vA[3*n+l] = 0.0;
+            }
+            nA[n] = 0.0;
+         }
+      }
+   }
+   Hybrid::gridTemporalAverageCounter = 0;
+   return RHGPU_OK;
+}
+
 int rhref_get_time(void* h,double* t,int64_t* ts) {
    RefCtx* c = (RefCtx*)h;
    *t = c->sim.t; *ts = c->sim.timestep;

@@ -169,6 +169,8 @@ _OPTIONAL = {
     "log_open": [_P, C.c_void_p],
     "log_write": [_P, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_int32],
     "log_close": [_P],
+    "set_population_averages": [_P, C.c_int32, C.POINTER(C.c_int32)],
+    "output_averages": [_P, _D, _D, _D],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p, "philox4x32": None}
 
@@ -373,6 +375,31 @@ class Context:
 
     def log_close(self):
         self.lib.call("log_close", self.h)
+
+    def set_population_averages(self, group_of_species):
+        """rhgpu_set_population_averages: output population of each species (-1: none)."""
+        g = np.ascontiguousarray(group_of_species, dtype=np.int32)
+        self._avg_groups = int(g.max()) + 1 if g.size and g.max() >= 0 else 0
+        self.lib.call("set_population_averages", self.h, self._avg_groups, _ptr(g, C.c_int32))
+
+    def output_averages(self, cellB: bool = True, populations: bool = True) -> dict:
+        """rhgpu_output_averages: cellBAverage (N x 3) and per output population
+        n_ave (N) and v_ave (N x 3); the returned sums and the counter restart."""
+        N = self.ncells
+        out = {}
+        b = np.zeros(3 * N) if cellB else None
+        G = getattr(self, "_avg_groups", 0) if populations else 0
+        n = np.zeros(G * N) if G else None
+        v = np.zeros(3 * G * N) if G else None
+        nul = C.POINTER(C.c_double)()
+        self.lib.call("output_averages", self.h, _ptr(b, C.c_double) if b is not None else nul,
+                      _ptr(n, C.c_double) if n is not None else nul, _ptr(v, C.c_double) if v is not None else nul)
+        if b is not None:
+            out["cellBAverage"] = b.reshape(N, 3)
+        if G:
+            out["n_ave"] = n.reshape(G, N)
+            out["v_ave"] = v.reshape(G, N, 3)
+        return out
 
     def set_timing(self, on: bool):
         self.lib.call("set_timing", self.h, 1 if on else 0)

@@ -79,6 +79,7 @@ struct Mover {
 };
 constexpr int MOVER_DEPOSIT = 1 << 8;   // deposits its CIC contributions (fixed point)
 constexpr int MOVER_PLACE = 1 << 9;     // is stored in the destination segment
+constexpr int MOVER_AVG = 1 << 10;      // removed after its in-segment deposit: population averages only
 
 struct FastBufs {
    double* RP;                 // row partials: 4 planes x nrows x nx x 4
@@ -400,7 +401,45 @@ __device__ inline bool pushOne(const GridInfo& g, const Fields& f, const Species
 
 // PER: the periodic axes (bit a = axis a), fixed at compile time; the host
 // launches the instantiation that matches the grid
-template <int PER>
+// the block's sums per (dual cell, corner) -> the segment's row partials (corner
+// ox = 1 of each dual cell plus ox = 0 of the next) and, where the first dual
+// cell's partner is in another segment, its boundary partial. s_rec is free.
+__device__ __forceinline__ void segPartialsOut(const GridInfo& g, const FastGeom& fg, const FastBufs& fb, double* s_rec,
+                                               long long row, int gseg, int u0, int u1, double a0, double a1,
+                                               double a2, double a3) {
+   const int tid = threadIdx.x, myDual = tid >> 3, myCorner = tid & 7;
+   {
+      double* q = s_rec + myDual * 32 + myCorner * 4;
+      q[0] = a0; q[1] = a1; q[2] = a2; q[3] = a3;
+   }
+   __syncthreads();
+   const int nx = g.nx;
+   const long long nrows = fg.nrows;
+   for (int e = tid; e < SEG * 16; e += FT) {
+      const int dl = e >> 4, qq = (e >> 2) & 3, m = e & 3;
+      const int lo = u0 + dl;   // the dual cell giving corner ox = 1 to cell x
+      if (lo >= u1) continue;
+      int x, hi;
+      if (g.per[0]) {
+         x = lo + 1 == nx ? 0 : lo + 1;
+         hi = lo + 1 < u1 ? dl + 1 : (fg.nseg == 1 ? 0 : -1);
+      } else {
+         x = lo;
+         if (x >= nx) continue;
+         hi = lo + 1 < u1 ? dl + 1 : -1;
+      }
+      double v = s_rec[dl * 32 + ((1 + 2 * qq) << 2) + m];
+      if (hi >= 0) v = v + s_rec[hi * 32 + ((2 * qq) << 2) + m];
+      fb.RP[(((long long)qq * nrows + row) * nx + x) * 4 + m] = v;
+   }
+   // corner ox = 0 of the first dual cell, when the cell's other dual cell is in another segment
+   if (tid < 16 && (g.per[0] ? fg.nseg > 1 : gseg >= 1)) {
+      const int qq = tid >> 2, m = tid & 3;
+      fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = s_rec[((2 * qq) << 2) + m];
+   }
+}
+
+template <int PER, bool AVG>
 __global__ void __launch_bounds__(FT, 4)
 k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
@@ -509,6 +548,8 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
             if (!removed) {
                stay = inSeg;
                if (!inSeg) mflags |= MOVER_PLACE;
+            } else if (AVG && rec) {
+               mflags |= MOVER_AVG;   // population averages: its in-segment deposit is listed
             }
             leave = mflags != 0;
          }
@@ -624,43 +665,16 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
    // ---- outputs: stayer counts, row partials, segment-boundary partial ---------------------
    __syncthreads();
    if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
-   {
-      double* q = s_rec + myDual * 32 + myCorner * 4;
-      q[0] = a0; q[1] = a1; q[2] = a2; q[3] = a3;
-   }
-   __syncthreads();
-   const int nx = g.nx;
-   const long long nrows = fg.nrows;
-   for (int e = tid; e < SEG * 16; e += FT) {
-      const int dl = e >> 4, qq = (e >> 2) & 3, m = e & 3;
-      const int lo = u0 + dl;   // the dual cell giving corner ox = 1 to cell x
-      if (lo >= u1) continue;
-      int x, hi;
-      if (g.per[0]) {
-         x = lo + 1 == nx ? 0 : lo + 1;
-         hi = lo + 1 < u1 ? dl + 1 : (fg.nseg == 1 ? 0 : -1);
-      } else {
-         x = lo;
-         if (x >= nx) continue;
-         hi = lo + 1 < u1 ? dl + 1 : -1;
-      }
-      double v = s_rec[dl * 32 + ((1 + 2 * qq) << 2) + m];
-      if (hi >= 0) v = v + s_rec[hi * 32 + ((2 * qq) << 2) + m];
-      fb.RP[(((long long)qq * nrows + row) * nx + x) * 4 + m] = v;
-   }
-   // corner ox = 0 of the first dual cell, when the cell's other dual cell is in another segment
-   if (tid < 16 && (g.per[0] ? fg.nseg > 1 : gseg >= 1)) {
-      const int qq = tid >> 2, m = tid & 3;
-      fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = s_rec[((2 * qq) << 2) + m];
-   }
+   segPartialsOut(g, fg, fb, s_rec, row, gseg, u0, u1, a0, a1, a2, a3);
 }
 
 // CIC contributions of the particles that left their segment, as exact fixed-point sums (MM)
-__global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, FastBufs fb, long long n) {
-   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= n) return;
-   const Mover& M = fb.movers[t];
-   if (!(M.lx & MOVER_DEPOSIT)) return;
+// one mover's CIC contributions as exact fixed-point sums into lo/hi (4 x N),
+// marking the touched cells (TOUCH)
+template <bool TOUCH>
+__device__ __forceinline__ void moverAdd128(const GridInfo& g, const FastGeom& fg, const FastSpecies& FS, const Mover& M,
+                                            unsigned long long* lo, unsigned long long* hi, double scaleR, double scaleJ,
+                                            unsigned* touched) {
    const int s = M.species;
    const long long row = M.dest / fg.nseg;
    const int vx = (int)(M.dest % fg.nseg) * SEG + (M.lx & 0xff);
@@ -675,11 +689,18 @@ __global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, Fa
       int dxc = bx + (o & 1), dyc = by + ((o >> 1) & 1), dzc = bz + ((o >> 2) & 1);
       if (!wrapc(dxc, g.nx, g.per[0]) || !wrapc(dyc, g.ny, g.per[1]) || !wrapc(dzc, g.nz, g.per[2])) continue;
       const long long dc = cidx(g, dxc, dyc, dzc);
-      add128(&fb.MMlo[dc], &fb.MMhi[dc], w8[o], fb.scaleR);
-      for (int l = 0; l < 3; ++l)
-         add128(&fb.MMlo[(1 + l) * N + dc], &fb.MMhi[(1 + l) * N + dc], w8[o] * st[3 + l], fb.scaleJ);
-      atomicOr(&fb.touched[dc >> 5], 1u << (dc & 31));
+      add128(&lo[dc], &hi[dc], w8[o], scaleR);
+      for (int l = 0; l < 3; ++l) add128(&lo[(1 + l) * N + dc], &hi[(1 + l) * N + dc], w8[o] * st[3 + l], scaleJ);
+      if (TOUCH) atomicOr(&touched[dc >> 5], 1u << (dc & 31));
    }
+}
+
+__global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, FastBufs fb, long long n) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= n) return;
+   const Mover& M = fb.movers[t];
+   if (!(M.lx & MOVER_DEPOSIT)) return;
+   moverAdd128<true>(g, fg, FS, M, fb.MMlo, fb.MMhi, fb.scaleR, fb.scaleJ, fb.touched);
 }
 
 // destination moments: four row partials (+ boundary partials) + fixed-point part, then finalize

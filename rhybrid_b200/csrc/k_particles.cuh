@@ -272,39 +272,57 @@ __global__ void __launch_bounds__(32 * DEP_WARPS) k_deposit_cell(GridInfo g, PSt
 }
 
 // destination sums over the 27 source cells in increasing source index
+// The up to 3 source coordinates per axis of the 27-neighbourhood of cell
+// (i,j,k), each with its offset source - destination, in increasing coordinate:
+// looping z, y, x over them visits the sources in increasing cell ID, the order
+// in which addValues3D reaches the destination when cells are accumulated in ID
+// order.
+struct Sources3 {
+   int c[3][3], o[3][3], n[3];
+};
+__device__ inline Sources3 sortedSources(const GridInfo& g, int i, int j, int k) {
+   Sources3 Q;
+   const int at[3] = {i, j, k}, nn[3] = {g.nx, g.ny, g.nz};
+   for (int a = 0; a < 3; ++a) {
+      Q.n[a] = 0;
+      for (int d = -1; d <= 1; ++d) {
+         int x = at[a] + d;
+         if (wrapc(x, nn[a], g.per[a])) { Q.c[a][Q.n[a]] = x; Q.o[a][Q.n[a]] = d; ++Q.n[a]; }
+      }
+      for (int u = 1; u < Q.n[a]; ++u)
+         for (int w = u; w > 0 && Q.c[a][w - 1] > Q.c[a][w]; --w) {
+            const int t1 = Q.c[a][w]; Q.c[a][w] = Q.c[a][w - 1]; Q.c[a][w - 1] = t1;
+            const int t2 = Q.o[a][w]; Q.o[a][w] = Q.o[a][w - 1]; Q.o[a][w - 1] = t2;
+         }
+   }
+   return Q;
+}
+
+// adds the 27 per-source contributions of one species' sums S to cell n, in
+// the sources' ID order, onto v[0..3] (rho, Ji)
+__device__ inline void addSources(const GridInfo& g, const Sources3& Q, const double* S, long long N, double v[4]) {
+   for (int c3 = 0; c3 < Q.n[2]; ++c3)
+      for (int b3 = 0; b3 < Q.n[1]; ++b3)
+         for (int a3 = 0; a3 < Q.n[0]; ++a3) {
+            const long long s = cidx(g, Q.c[0][a3], Q.c[1][b3], Q.c[2][c3]);
+            // destination seen from the source: offset -o, array index -o+1
+            const int e = (1 - Q.o[0][a3]) + 3 * ((1 - Q.o[1][b3]) + 3 * (1 - Q.o[2][c3]));
+            v[0] += S[(long long)e * N + s];
+            v[1] += S[(long long)(27 + 3 * e + 0) * N + s];
+            v[2] += S[(long long)(27 + 3 * e + 1) * N + s];
+            v[3] += S[(long long)(27 + 3 * e + 2) * N + s];
+         }
+}
+
 __global__ void k_deposit_gather(GridInfo g, Fields f, const double* S, int first, int last, double minRho,
                                  unsigned long long* cnt) {
    RH_CELL_PROLOGUE
-   // per axis: (coordinate, offset source-dest) of the up to 3 sources, sorted by coordinate
-   int cx[3], ox[3], nxs = 0, cy[3], oy[3], nys = 0, cz[3], oz[3], nzs = 0;
-   for (int d = -1; d <= 1; ++d) {
-      int a = i + d; if (wrapc(a, g.nx, g.per[0])) { cx[nxs] = a; ox[nxs] = d; ++nxs; }
-      int b = j + d; if (wrapc(b, g.ny, g.per[1])) { cy[nys] = b; oy[nys] = d; ++nys; }
-      int c = k + d; if (wrapc(c, g.nz, g.per[2])) { cz[nzs] = c; oz[nzs] = d; ++nzs; }
-   }
-#define RH_SORT3(cc, oo, nn)                                                           \
-   for (int u = 1; u < nn; ++u)                                                         \
-      for (int w = u; w > 0 && cc[w - 1] > cc[w]; --w) {                               \
-         int t1 = cc[w]; cc[w] = cc[w - 1]; cc[w - 1] = t1;                             \
-         int t2 = oo[w]; oo[w] = oo[w - 1]; oo[w - 1] = t2;                             \
-      }
-   RH_SORT3(cx, ox, nxs) RH_SORT3(cy, oy, nys) RH_SORT3(cz, oz, nzs)
-#undef RH_SORT3
-   double rho = first ? 0.0 : f.cellRho[n];
-   double J0 = first ? 0.0 : f.cellJi[0 * N + n];
-   double J1 = first ? 0.0 : f.cellJi[1 * N + n];
-   double J2 = first ? 0.0 : f.cellJi[2 * N + n];
-   for (int c3 = 0; c3 < nzs; ++c3)
-      for (int b3 = 0; b3 < nys; ++b3)
-         for (int a3 = 0; a3 < nxs; ++a3) {
-            const long long s = cidx(g, cx[a3], cy[b3], cz[c3]);
-            // destination seen from the source: offset -o, array index -o+1
-            const int e = (1 - ox[a3]) + 3 * ((1 - oy[b3]) + 3 * (1 - oz[c3]));
-            rho += S[(long long)e * N + s];
-            J0 += S[(long long)(27 + 3 * e + 0) * N + s];
-            J1 += S[(long long)(27 + 3 * e + 1) * N + s];
-            J2 += S[(long long)(27 + 3 * e + 2) * N + s];
-         }
+   const Sources3 Q = sortedSources(g, i, j, k);
+   double v[4];
+   v[0] = first ? 0.0 : f.cellRho[n];
+   for (int l = 0; l < 3; ++l) v[1 + l] = first ? 0.0 : f.cellJi[l * N + n];
+   addSources(g, Q, S, N, v);
+   double rho = v[0], J0 = v[1], J1 = v[2], J2 = v[3];
    bool clamp = false;
    if (last) {
       rho /= g.dV;

@@ -23,6 +23,7 @@
 #include "k_f32.cuh"
 #include "k_denoise.cuh"
 #include "k_inject.cuh"
+#include "k_avg.cuh"
 #include "rh_logs.h"
 
 using namespace rh;
@@ -231,6 +232,13 @@ struct rhgpu_ctx {
    double* diagPart = nullptr;          // DIAG_BLOCKS x DIAG_FS partial rows of rhgpu_reduce_diagnostics
    double* rhoM = nullptr;              // N: total ion mass density of the field log
    unsigned long long* rhoMfix = nullptr;   // 2N: its fixed-point sums (lo, hi)
+   // temporal averages of the output populations (rhgpu_set_population_averages)
+   int avgGroups = 0;
+   int avgGroupOf[MAX_SPECIES] = {};
+   double* avgN = nullptr;              // avgGroups x N charge sums
+   double* avgV = nullptr;              // avgGroups x 3N current sums (component planes)
+   double* avgOut = nullptr;            // 4N output staging
+   FastBufs avgFB = {};                 // fast path: row partials and fixed-point sums of one population
    // log files (rhgpu_log_*)
    LogFiles* logs = nullptr;
    int logInner = 0;
@@ -455,6 +463,13 @@ int depositExact(rhgpu_ctx* c, double* S) {
          RH_TIME(c, "deposit_gather");
          k_deposit_gather<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, c->f, S, s == first, s == last,
                                                                       c->P.min_ion_charge_density, c->cntU);
+         RH_LAUNCHED(c);
+      }
+      const int grp = c->avgGroups ? c->avgGroupOf[s] : -1;
+      if (grp >= 0) {
+         RH_TIME(c, "population_averages");
+         k_deposit_gather_avg<<<cellGrid(g), cellBlock(), 0, c->stream>>>(g, S, c->avgN + (long long)grp * g.N,
+                                                                          c->avgV + 3LL * grp * g.N);
          RH_LAUNCHED(c);
       }
    }
@@ -937,6 +952,56 @@ int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
    return RHGPU_OK;
 }
 
+// fast path: each output population's share of this step's deposit added to
+// its averages: the stayers (the next buffer before the arrivals are placed)
+// by segment, then every deposited mover (left its segment, or deposited in it
+// and removed by a boundary)
+int fastAverages(rhgpu_ctx* c, long long nm) {
+   const long long N = c->g.N;
+   FastBufs& A = c->avgFB;
+   if (!A.RP) {
+      RH_CUDA(cudaMalloc(&A.RP, sizeof(double) * 16 * c->fg.nrows * c->g.nx));
+      RH_CUDA(cudaMalloc(&A.RPB, sizeof(double) * 16 * c->fg.nrows * c->fg.nseg));
+      RH_CUDA(cudaMalloc(&A.MMlo, sizeof(unsigned long long) * 4 * N));
+      RH_CUDA(cudaMalloc(&A.MMhi, sizeof(unsigned long long) * 4 * N));
+      RH_CUDA(cudaMemset(A.RPB, 0, sizeof(double) * 16 * c->fg.nrows * c->fg.nseg));
+      RH_CUDA(cudaMemset(A.MMlo, 0, sizeof(unsigned long long) * 4 * N));
+      RH_CUDA(cudaMemset(A.MMhi, 0, sizeof(unsigned long long) * 4 * N));
+   }
+   A.scaleR = c->fb.scaleR;
+   A.scaleJ = c->fb.scaleJ;
+   const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
+   const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
+   FastSpecies FS = fastSpecies(c);
+   FastSpecies stay = FS;
+   for (int s = 0; s < c->ns; ++s) stay.st[s].cur = FS.st[s].nxt;
+   for (int grp = 0; grp < c->avgGroups; ++grp) {
+      unsigned mask = 0;
+      for (int s = 0; s < c->ns; ++s)
+         if (c->avgGroupOf[s] == grp && c->sp[s].accumulate && c->seg[s].a[c->seg[s].cur][0]) mask |= 1u << s;
+      if (!mask) continue;
+      RH_TIME(c, "population_averages");
+      switch (perMask(c->g)) {
+#define RH_FAST_AVG(M)                                                                                         \
+   case M:                                                                                                      \
+      k_fast_avg_deposit<M><<<(unsigned)c->fg.NS, FT, 0, c->stream>>>(c->g, c->fg, stay, mask, A);              \
+      break;
+         RH_FAST_AVG(0) RH_FAST_AVG(1) RH_FAST_AVG(2) RH_FAST_AVG(3) RH_FAST_AVG(4) RH_FAST_AVG(5) RH_FAST_AVG(6)
+         RH_FAST_AVG(7)
+#undef RH_FAST_AVG
+      }
+      RH_LAUNCHED(c);
+      if (nm > 0) {
+         k_fast_avg_movers<<<blocks1d(nm, 128), 128, 0, c->stream>>>(c->g, c->fg, FS, c->fb.movers, nm, mask, A);
+         RH_LAUNCHED(c);
+      }
+      k_fast_avg_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->fg, A, hiR, loR, hiJ, loJ,
+                                                                      c->avgN + (long long)grp * N, c->avgV + 3LL * grp * N);
+      RH_LAUNCHED(c);
+   }
+   return RHGPU_OK;
+}
+
 int fastPush(rhgpu_ctx* c) {
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
@@ -955,8 +1020,12 @@ int fastPush(rhgpu_ctx* c) {
       switch (perMask(c->g)) {
 #define RH_FAST_PD(M)                                                                                           \
    case M:                                                                                                        \
-      k_fast_push_deposit<M><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, c->cntU, \
-                                                                 c->err);                                        \
+      if (c->avgGroups)                                                                                           \
+         k_fast_push_deposit<M, true><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, \
+                                                                          c->cntU, c->err);                        \
+      else                                                                                                        \
+         k_fast_push_deposit<M, false><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb,         \
+                                                                           c->cntD, c->cntU, c->err);              \
       break;
          RH_FAST_PD(0) RH_FAST_PD(1) RH_FAST_PD(2) RH_FAST_PD(3) RH_FAST_PD(4) RH_FAST_PD(5) RH_FAST_PD(6) RH_FAST_PD(7)
 #undef RH_FAST_PD
@@ -975,6 +1044,10 @@ int fastPush(rhgpu_ctx* c) {
       RH_TIME(c, "fast_mover_deposit");
       k_fast_mover_deposit<<<blocks1d(nm, 128), 128, 0, c->stream>>>(c->g, c->fg, fastSpecies(c), c->fb, nm);
       RH_LAUNCHED(c);
+   }
+   if (c->avgGroups) {
+      const int rc = fastAverages(c, (long long)nm);
+      if (rc) return rc;
    }
    if (nm > 0) {
       const long long nb = (long long)c->ns * NS;
@@ -1736,6 +1809,8 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->diagPart);
    cudaFree(c->rhoM);
    cudaFree(c->rhoMfix);
+   cudaFree(c->avgN); cudaFree(c->avgV); cudaFree(c->avgOut);
+   cudaFree(c->avgFB.RP); cudaFree(c->avgFB.RPB); cudaFree(c->avgFB.MMlo); cudaFree(c->avgFB.MMhi);
    if (c->logs) { c->logs->close(); delete c->logs; c->logs = nullptr; }
    for (int s = 0; s < c->ns; ++s) {
       F32Host& h = c->f32[s];
@@ -1964,7 +2039,12 @@ int phasePush(rhgpu_ctx* c) {
    return c->path == RHGPU_PATH_FAST ? fastPush(c) : c->path == RHGPU_PATH_FP32 ? f32Push(c) : pushAll(c);
 }
 int phaseAccumulate(rhgpu_ctx* c) {
-   return c->path == RHGPU_PATH_FAST ? fastGather(c) : c->path == RHGPU_PATH_FP32 ? f32Gather(c) : accumulateAll(c);
+   if (c->path == RHGPU_PATH_FAST) return fastGather(c);
+   if (c->path == RHGPU_PATH_FP32) {
+      if (c->avgGroups) return fail(RHGPU_ERR_STATE, "population averages run on the fast and exact paths");
+      return f32Gather(c);
+   }
+   return accumulateAll(c);
 }
 // the fast path removes boundary particles inside its push kernel
 int phaseBoundaries(rhgpu_ctx* c) { return c->path == RHGPU_PATH_EXACT ? boundariesAll(c) : RHGPU_OK; }
@@ -2467,6 +2547,70 @@ int rhgpu_log_write(rhgpu_ctx* c, int32_t main_log_diagnostics, int32_t* stop_ru
    }
    c->logTStart = c->t;
    return zeroLogCounters(c);
+}
+
+int rhgpu_set_population_averages(rhgpu_ctx* c, int32_t n_groups, const int32_t* group_of_species) {
+   if (!c || n_groups < 0 || (n_groups > 0 && !group_of_species)) return fail(RHGPU_ERR_ARG, "set_population_averages: bad arguments");
+   if (n_groups > 0 && c->path == RHGPU_PATH_FP32)
+      return fail(RHGPU_ERR_STATE, "population averages run on the fast and exact paths");
+   for (int s = 0; s < c->ns && n_groups > 0; ++s)
+      if (group_of_species[s] < -1 || group_of_species[s] >= n_groups)
+         return fail(RHGPU_ERR_ARG, "set_population_averages: group index out of range");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   cudaFree(c->avgN); cudaFree(c->avgV); cudaFree(c->avgOut);
+   c->avgN = c->avgV = c->avgOut = nullptr;
+   c->avgGroups = 0;
+   if (n_groups == 0) return RHGPU_OK;
+   const long long N = c->g.N;
+   RH_CUDA(cudaMalloc(&c->avgN, sizeof(double) * n_groups * N));
+   RH_CUDA(cudaMalloc(&c->avgV, sizeof(double) * 3 * n_groups * N));
+   RH_CUDA(cudaMalloc(&c->avgOut, sizeof(double) * 4 * N));
+   RH_CUDA(cudaMemset(c->avgN, 0, sizeof(double) * n_groups * N));
+   RH_CUDA(cudaMemset(c->avgV, 0, sizeof(double) * 3 * n_groups * N));
+   for (int s = 0; s < c->ns; ++s) c->avgGroupOf[s] = group_of_species[s];
+   c->avgGroups = n_groups;
+   return RHGPU_OK;
+}
+
+int rhgpu_output_averages(rhgpu_ctx* c, double* cellB_average, double* n_average, double* v_average) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   if ((n_average || v_average) && !c->avgGroups)
+      return fail(RHGPU_ERR_STATE, "output_averages: no population averages (rhgpu_set_population_averages)");
+   RH_CUDA(cudaSetDevice(c->device));
+   const long long N = c->g.N;
+   const double inv = c->gridAvgCounter > 0 ? 1.0 / c->gridAvgCounter : 0.0;
+   if (!c->avgOut && cellB_average) {
+      RH_CUDA(cudaMalloc(&c->avgOut, sizeof(double) * 4 * N));
+   }
+   if (cellB_average) {
+      k_avgB_output<<<blocks1d(N, 256), 256, 0, c->stream>>>(N, c->arr[RHGPU_CELL_AVERAGE_B], inv, c->avgOut);
+      RH_CUDA(cudaGetLastError());
+      RH_CUDA(cudaMemcpyAsync(cellB_average, c->avgOut, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c->stream));
+      RH_CUDA(cudaStreamSynchronize(c->stream));
+   }
+   if (n_average || v_average) {
+      for (int grp = 0; grp < c->avgGroups; ++grp) {
+         // the charge of the population's first species (operator_userdata.cpp:186-187)
+         int first = -1;
+         for (int s = 0; s < c->ns && first < 0; ++s)
+            if (c->avgGroupOf[s] == grp) first = s;
+         const double q = first >= 0 ? c->sp[first].q : 1.0;
+         k_avg_output<<<blocks1d(N, 256), 256, 0, c->stream>>>(N, c->avgN + (long long)grp * N, c->avgV + 3LL * grp * N, q,
+                                                               c->g.dV, inv, n_average ? c->avgOut : nullptr,
+                                                               v_average ? c->avgOut + N : nullptr);
+         RH_CUDA(cudaGetLastError());
+         if (n_average)
+            RH_CUDA(cudaMemcpyAsync(n_average + (long long)grp * N, c->avgOut, sizeof(double) * N, cudaMemcpyDeviceToHost,
+                                    c->stream));
+         if (v_average)
+            RH_CUDA(cudaMemcpyAsync(v_average + 3LL * grp * N, c->avgOut + N, sizeof(double) * 3 * N,
+                                    cudaMemcpyDeviceToHost, c->stream));
+         RH_CUDA(cudaStreamSynchronize(c->stream));
+      }
+   }
+   c->gridAvgCounter = 0;
+   return RHGPU_OK;
 }
 
 int rhgpu_log_close(rhgpu_ctx* c) {
