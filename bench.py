@@ -54,10 +54,10 @@ def workload(name, scale=1.0):
     from rhybrid_b200 import config as cf
     if name == "mars":
         if scale == 1.0:
-            return cf.config_mars()
+            return cf.config_mars(exosphere=True)
         f = scale ** (1.0 / 3.0)
         return cf.config_mars(nx=max(8, int(round(120 * f))), ny=max(8, int(round(160 * f))),
-                              nz=max(8, int(round(160 * f))))
+                              nz=max(8, int(round(160 * f))), exosphere=True)
     if name == "empty_box":
         return cf.config_empty_box(32, 32, 32, ppc=20.0)
     raise ValueError(name)
@@ -264,7 +264,7 @@ def run_gpu(args, rank, world, local_rank):
     gen_s = time.time() - t0
     lib = abi.gpu_library()
     nps = [p[1].shape[0] for p in pops]
-    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + 1024 for n in nps], device=local_rank)
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + n // 20 + (1 << 20) for n in nps], device=local_rank)
     ctx.set_path({"fast": abi.PATH_FAST, "exact": abi.PATH_EXACT, "fp32": abi.PATH_FP32}[args.path])
     ctx.upload_array("faceB", grid["faceB"])
     ctx.upload_array("cellB", grid["cellB"])
@@ -272,6 +272,10 @@ def run_gpu(args, rank, world, local_rank):
     ctx.upload_cell_flags(grid["flags"])
     for s, (c, p) in enumerate(pops):
         ctx.upload_particles(s, c, p)
+    # the configuration's particle sources (solar wind inflow, O+ exosphere) on
+    # the GPU; the exact path (the reference's particle order) takes none
+    sources = cf.source_injectors(cfg, seed=cfg.seed) if args.path != "exact" else []
+    ctx.set_injectors(sources)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local_rank)
     for _ in range(args.warmup):
         ctx.step(1)
@@ -379,9 +383,11 @@ def run_gpu(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_all / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.path == "fp32" else "f64",
-            "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform)",
+            "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform; sources on the GPU)",
             "config": {"workload": cfg.name, "cells": [cfg.nx, cfg.ny, cfg.nz], "dx_m": cfg.dx, "dt_s": cfg.dt,
                        "ions": int(0.5 * (n0 + n1)), "species": [p.name for p in cfg.populations],
+                       "sources": [("exosphere " if j.type == abi.INJECT_EXOSPHERE else "solar wind ")
+                                   + cfg.populations[j.species].name for j in sources],
                        "parallelism": f"replicas x{world}", "particle_path": args.path, "l2": "state 10+ GB > 126 MB L2, no flush needed",
                        "sim_s_per_wall_s": round(args.steps * cfg.dt / (ms_all / 1e3), 4),
                        "step_roofline": {"achieved_gbs": round(step_ach, 1), "alg_bytes_per_step": int(step_alg),
@@ -407,7 +413,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "particle-steps/s", "value": round(value, 1), "unit": "particle-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform-in-cell Maxwellian fill)",
-        "config": {"workload": workload(args.workload).name, "sample": f"slabs 120x160x{m['nz_sub']}"},
+        "config": {"workload": workload(args.workload).name, "sample": f"slabs 120x160x{m['nz_sub']}",
+                   "sources": "none: the reference's injectors are not part of its built hot path"},
         "cpu_baseline": {"value": round(value, 1), "unit": "particle-steps/s", "cores": m["cores"], "kind": m["kind"],
                          "sample": f"{m['cores']} processes of the reference hot path, each on a 120x160x{m['nz_sub']} "
                                    f"slab ({m['particles_per_core']} ions), median of {len(rates)} steps"},

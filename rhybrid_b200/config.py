@@ -42,6 +42,7 @@ class Population:
     temperature: float = 1e5     # [K]
     ppc: float = 20.0            # macroparticles_per_cell
     upstream: bool = True        # counts towards the upstream plasma parameters
+    exosphere: Optional[dict] = None   # ExosphereInjector parameters of a planetary source
 
     @property
     def q(self) -> float:
@@ -139,6 +140,48 @@ def solar_wind_injectors(cfg: "Config", seed: int = 1) -> list:
     return out
 
 
+def upstream_macro_ratio(cfg: "Config") -> float:
+    """Hybrid::upstreamMacroPleRatio: the solar wind macroparticles injected per
+    step over the macroparticles per cell, of the first solar wind population
+    (particle_injector.cpp:690-712): |U| dt / dx times the wall cells."""
+    for p in cfg.populations:
+        v = [float(x) for x in p.velocity]
+        if not p.upstream or sum(1 for x in v if x != 0.0) != 1 or p.ppc <= 0:
+            continue
+        ax = next(a for a in range(3) if v[a] != 0.0)
+        dims, per = (cfg.nx, cfg.ny, cfg.nz), cfg.periodic
+        wall = 1
+        for a in range(3):
+            if a != ax:
+                wall *= dims[a] if per[a] else dims[a] - 2
+        return abs(v[ax]) * cfg.dt / cfg.dx * wall
+    return 0.0
+
+
+def source_injectors(cfg: "Config", seed: int = 1) -> list:
+    """Every particle source of the configuration: the solar wind injectors
+    and one InjectorExosphere per population with exosphere parameters."""
+    out = solar_wind_injectors(cfg, seed)
+    ratio = upstream_macro_ratio(cfg)
+    for s, p in enumerate(cfg.populations):
+        e = p.exosphere
+        if not e:
+            continue
+        j = abi.Injector(species=s, type=abi.INJECT_EXOSPHERE, temperature=p.temperature, seed=seed * 1000003 + s,
+                         profile=abi.NEUTRAL_PROFILES[e["profile"]], n_components=len(e["n0"]), r0=e["r0"],
+                         exobase_radius=e["exobase_radius"], shadow_radius=e["shadow_radius"],
+                         ionization_rate=e.get("ionization_rate", -1.0),
+                         ionization_factor_shadow=e.get("ionization_factor_shadow", 1.0),
+                         total_production_rate=e.get("total_production_rate", -1.0),
+                         macroparticles_per_cell_relative=e.get("macroparticles_per_cell_relative", 1.0),
+                         upstream_macro_ratio=ratio)
+        for k, (n0, H0) in enumerate(zip(e["n0"], e.get("H0", [0.0] * len(e["n0"])))):
+            j.n0[k] = n0
+            j.H0[k] = H0
+        out.append(j)
+    return out
+
+
 def config_empty_box(nx=32, ny=32, nz=32, ppc=20.0) -> Config:
     """Plain FP64 periodic empty box: cell 100 km, one H+ species, n=5e6 m^-3,
     drift Vx=-400 km/s, Maxwellian T=1e5 K, B=(0,5,0) nT uniform, 20
@@ -152,11 +195,14 @@ def config_empty_box(nx=32, ny=32, nz=32, ppc=20.0) -> Config:
                   name=f"empty_box_{nx}x{ny}x{nz}_ppc{ppc:g}")
 
 
-def config_mars(nx=120, ny=160, nz=160, ppc=30.0, dx=300e3) -> Config:
+def config_mars(nx=120, ny=160, nz=160, ppc=30.0, dx=300e3, exosphere=False) -> Config:
     """Plain FP64 Mars-like obstacle: cell 300 km, absorbing sphere r=3390 km,
     solar wind H+ (n=2e6 m^-3, 30 ppc) + He++ (4% of n, 1.5 ppc), V=-450 km/s,
     T=1e5 K, IMF (0,3,0) nT, closed walls with IMF on the +x wall, dt=0.05 s,
-    superconducting-sphere resistivity, electron pressure on."""
+    superconducting-sphere resistivity, electron pressure on. With exosphere,
+    a third population exoO+ starts empty and is fed by the exponential O+
+    exosphere source of examples/mars.cfg ([exoO+], [injector_exoO+]);
+    `source_injectors` gives it and the solar wind inflow."""
     R = 3390e3
     Lx, Ly, Lz = nx * dx, ny * dx, nz * dx
     pops = [
@@ -165,6 +211,14 @@ def config_mars(nx=120, ny=160, nz=160, ppc=30.0, dx=300e3) -> Config:
         Population(name="swHe++", mass=3.9737, charge=2.0, obstacle=R, density=0.04 * 2e6,
                    velocity=(-450e3, 0, 0), temperature=1e5, ppc=ppc / 20.0),
     ]
+    if exosphere:
+        pops.append(Population(name="exoO+", mass=15.883821896403, charge=1.0, obstacle=3590e3, density=0.0,
+                               velocity=(0.0, 0.0, 0.0), temperature=6500.0, ppc=0.0, upstream=False,
+                               exosphere={"profile": "Exponential", "r0": 3393.5e3,
+                                          "n0": [5.23e9, 9.76e8, 3.71e10], "H0": [626.2e3, 2790e3, 88.47e3],
+                                          "exobase_radius": 3790e3, "shadow_radius": 3390e3,
+                                          "ionization_factor_shadow": 0.0, "total_production_rate": 0.156e24,
+                                          "macroparticles_per_cell_relative": 1.0}))
     return Config(nx=nx, ny=ny, nz=nz, x_min=-0.5 * Lx, y_min=-0.5 * Ly, z_min=-0.5 * Lz, dx=dx,
                   periodic=(0, 0, 0), dt=0.05, R_fieldObstacle=R, R_particleObstacle=R,
                   imf=(0.0, 3e-9, 0.0), imf_boundary_cellB=(1, 0, 0, 0, 0, 0),
@@ -175,7 +229,7 @@ def config_mars(nx=120, ny=160, nz=160, ppc=30.0, dx=300e3) -> Config:
                   resistivity_value=6.0, resistivity_R=R,
                   max_ion_velocity=1500e3, max_electron_velocity=1500e3,
                   min_ion_charge_density_relative=0.05, max_whistler_velocity=1500e3,
-                  populations=pops, name=f"mars_{nx}x{ny}x{nz}_ppc{ppc:g}")
+                  populations=pops, name=f"mars_{nx}x{ny}x{nz}_ppc{ppc:g}" + ("_exoO+" if exosphere else ""))
 
 
 # ---------------------------------------------------------------------------

@@ -207,25 +207,36 @@ template <class MV>
 __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* movers,
                          unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err) {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-   if (t >= J.ncells) return;
+   const int lane = threadIdx.x & 31;
    RngStream r;
-   r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
-   // probRound: floor(x) + 1 with probability x - floor(x)
-   const double x = J.type == INJ_EXOSPHERE ? J.rates[t] : J.perCellPerDt;
    int n = 0;
-   if (x > 0) {
-      n = (int)floor(x);
-      if (r.uniform() < x - n) ++n;
+   if (t < J.ncells) {
+      r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
+      // probRound: floor(x) + 1 with probability x - floor(x)
+      const double x = J.type == INJ_EXOSPHERE ? J.rates[t] : J.perCellPerDt;
+      if (x > 0) {
+         n = (int)floor(x);
+         if (r.uniform() < x - n) ++n;
+      }
    }
-   if (n == 0) return;
-   const unsigned long long m0 = atomicAdd(nmovers, (unsigned long long)n);
-   const int cell = J.cells[t];
-   const int ci = cell % g.nx, cj = (cell / g.nx) % g.ny, ck = cell / (g.nx * g.ny);
+   // mover slots: one reservation per warp (inclusive scan of the counts)
+   int incl = n;
+   for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+   }
+   const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
+   unsigned long long base = 0;
+   if (lane == 31 && wtotal > 0) base = atomicAdd(nmovers, (unsigned long long)wtotal);
+   base = __shfl_sync(0xffffffffu, base, 31);
+   const unsigned long long m0 = base + (unsigned long long)(incl - n);
+   double sw = 0.0, ske = 0.0;
+   int placed = 0;
    GaussSource gs;
    gs.has = false;
    gs.ok = true;
-   double sw = 0.0, ske = 0.0;
-   int placed = 0;
+   const int cell = n > 0 ? J.cells[t] : 0;
+   const int ci = cell % g.nx, cj = (cell / g.nx) % g.ny, ck = cell / (g.nx * g.ny);
    for (int p = 0; p < n; ++p) {
       double st[7];
       injState(J, g.dx, r, gs, st);
@@ -256,9 +267,17 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
       writeMover(movers[m], g, fg, st, i, j, k, J.species, key);
    }
    if (!gs.ok) raiseError(err, RHGPU_DEVERR_INJECT);
-   atomicAdd(&injCnt[3 * J.species + 0], sw);
-   atomicAdd(&injCnt[3 * J.species + 1], (double)placed);
-   atomicAdd(&injCnt[3 * J.species + 2], ske);
+   // the injection counters: one atomic per warp
+   for (int o = 16; o > 0; o >>= 1) {
+      sw += __shfl_xor_sync(0xffffffffu, sw, o);
+      ske += __shfl_xor_sync(0xffffffffu, ske, o);
+      placed += __shfl_xor_sync(0xffffffffu, placed, o);
+   }
+   if (lane == 0 && placed > 0) {
+      atomicAdd(&injCnt[3 * J.species + 0], sw);
+      atomicAdd(&injCnt[3 * J.species + 1], (double)placed);
+      atomicAdd(&injCnt[3 * J.species + 2], ske);
+   }
 }
 
 }  // namespace rh

@@ -944,7 +944,7 @@ template <class MV>
 int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
    for (const InjHost& h : c->inj) {
       if (h.d.ncells == 0) continue;
-      RH_TIME(c, "inject");
+      RH_TIME(c, h.d.type == INJ_EXOSPHERE ? "inject_exosphere" : "inject_inflow");
       k_inject<MV><<<blocks1d(h.d.ncells, 128), 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers,
                                                                      c->fb.nmovers, moverCap, c->injCnt, c->err);
       RH_LAUNCHED(c);

@@ -117,3 +117,19 @@ def test_oracle_gyration_preserves_speed(port_lib):
         assert np.max(np.abs(v1 - v0) / v0) < 1e-14
     finally:
         ctx.close()
+
+
+def test_mars_sources():
+    """The Mars workload's particle sources: solar wind inflow of both upstream
+    populations and the O+ exosphere of examples/mars.cfg, its macroparticle
+    count tied to the solar wind's (upstreamMacroPleRatio,
+    particle_injector.cpp:690-712: |U| dt / dx times the upstream wall cells)."""
+    cfg = cf.config_mars(exosphere=True)
+    assert cf.upstream_macro_ratio(cfg) == pytest.approx(450e3 * 0.05 / 300e3 * 158 * 158)
+    src = cf.source_injectors(cfg, seed=7)
+    assert [j.type for j in src] == [abi.INJECT_SOLARWIND, abi.INJECT_SOLARWIND, abi.INJECT_EXOSPHERE]
+    exo = src[2]
+    assert exo.species == 2 and exo.n_components == 3 and exo.total_production_rate == 0.156e24
+    assert list(exo.H0)[:3] == [626.2e3, 2790e3, 88.47e3] and exo.temperature == 6500.0
+    grid, pops = cf.initial_state(cfg.replace(nx=12, ny=16, nz=16))
+    assert pops[2][1].shape[0] == 0 and pops[0][1].shape[0] > 0
