@@ -703,26 +703,50 @@ __global__ void k_fast_mover_deposit(GridInfo g, FastGeom fg, FastSpecies FS, Fa
    moverAdd128<true>(g, fg, FS, M, fb.MMlo, fb.MMhi, fb.scaleR, fb.scaleJ, fb.touched);
 }
 
-// destination moments: four row partials (+ boundary partials) + fixed-point part, then finalize
+// the segment-boundary partials folded into the row partials of their cells
+// (RP += RPB, the addition the gather would make): the gather then reads four
+// row partials per cell and nothing else
+__global__ void k_fast_fold_boundary(GridInfo g, FastGeom fg, FastBufs fb) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   const long long nrows = fg.nrows;
+   if (t >= 16 * nrows * fg.nseg) return;
+   const int m = (int)(t & 3);
+   const long long e = t >> 2;                    // (qq, row, gseg)
+   const int gseg = (int)(e % fg.nseg);
+   const long long qr = e / fg.nseg;              // qq * nrows + row
+   if (!(g.per[0] ? fg.nseg > 1 : gseg >= 1)) return;
+   const int x = g.per[0] ? gseg * SEG : gseg * SEG - 1;
+   if (x >= g.nx) return;
+   double* rp = fb.RP + (qr * g.nx + x) * 4 + m;
+   *rp = *rp + fb.RPB[e * 4 + m];
+}
+
+// destination moments: four row partials (boundary partials folded in) +
+// fixed-point part, then finalize. The touched word and the four row
+// partials (16-byte loads) are all requested before any sum.
 __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, double hiR, double loR, double hiJ,
                               double loJ, double minRho, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
-   const bool bnd = g.per[0] ? (fg.nseg > 1 && i % SEG == 0) : ((i + 1) % SEG == 0);
-   const int gb = g.per[0] ? i / SEG : (i + 1) / SEG;
-   double v[4];
+   const unsigned tw = fb.touched[n >> 5];
+   double2 rp[4][2];
+#pragma unroll
    for (int qq = 0; qq < 4; ++qq) {
       const int uyy = dualU(j - (qq & 1), g.ny, g.per[1]);
       const int uzz = dualU(k - (qq >> 1), g.nz, g.per[2]);
       const long long row = (long long)uyy + (long long)fg.nd[1] * uzz;
-      const double* rp = fb.RP + (((long long)qq * fg.nrows + row) * g.nx + i) * 4;
-      const double* rb = fb.RPB + (((long long)qq * fg.nrows + row) * fg.nseg + gb) * 4;
-      for (int l = 0; l < 4; ++l) {
-         double r = rp[l];
-         if (bnd) r = r + rb[l];
-         v[l] = qq == 0 ? r : v[l] + r;
-      }
+      const double2* p2 = reinterpret_cast<const double2*>(fb.RP + (((long long)qq * fg.nrows + row) * g.nx + i) * 4);
+      rp[qq][0] = p2[0];
+      rp[qq][1] = p2[1];
    }
-   if (fb.touched[n >> 5] & (1u << (n & 31))) {
+   double v[4] = {rp[0][0].x, rp[0][0].y, rp[0][1].x, rp[0][1].y};
+#pragma unroll
+   for (int qq = 1; qq < 4; ++qq) {
+      v[0] = v[0] + rp[qq][0].x;
+      v[1] = v[1] + rp[qq][0].y;
+      v[2] = v[2] + rp[qq][1].x;
+      v[3] = v[3] + rp[qq][1].y;
+   }
+   if (tw & (1u << (n & 31))) {
       v[0] += fixedToDouble(fb.MMlo[n], fb.MMhi[n], hiR, loR);
       for (int l = 0; l < 3; ++l) v[1 + l] += fixedToDouble(fb.MMlo[(1 + l) * N + n], fb.MMhi[(1 + l) * N + n], hiJ, loJ);
       for (int l = 0; l < 4; ++l) { fb.MMlo[l * N + n] = 0ull; fb.MMhi[l * N + n] = 0ull; }

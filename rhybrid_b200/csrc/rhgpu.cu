@@ -1081,6 +1081,8 @@ int fastPush(rhgpu_ctx* c) {
 
 int fastGather(rhgpu_ctx* c) {
    RH_TIME(c, "fast_gather");
+   k_fast_fold_boundary<<<blocks1d(16 * c->fg.nrows * c->fg.nseg, 256), 256, 0, c->stream>>>(c->g, c->fg, c->fb);
+   RH_LAUNCHED(c);
    const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
    const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
    k_fast_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->fb, hiR, loR, hiJ, loJ,
