@@ -316,16 +316,33 @@ int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
  *     N = macroparticles_per_cell_relative * upstream_macro_ratio per step,
  *     weight total_rate dt / N. New particles are uniform in the cell and
  *     above the exobase, with Gaussian velocities of the temperature.
+ *   RHGPU_INJECT_IONOSPHERE (InjectorIonosphere, :947-1240): each cell's
+ *     share of a spherical emission shell of `emission_radius` (1000 Monte
+ *     Carlo points per cell projected on the shell) times the emission
+ *     profile at the cell centre gives its expected macroparticles per step,
+ *     N = macroparticles_per_cell_relative * upstream_macro_ratio per step in
+ *     the box, weight total_production_rate dt / N. New particles are uniform
+ *     in the cell with Gaussian velocities of the temperature, turned outward.
  * Solar wind and flow: weight n dx^3 / ppc. Thermal speed sqrt(k_B T / m)
  * with the species' mass. n == 0 removes all sources. */
 #define RHGPU_INJECT_SOLARWIND 1
 #define RHGPU_INJECT_FLOW      2
 #define RHGPU_INJECT_EXOSPHERE 3
+#define RHGPU_INJECT_IONOSPHERE 4
+/* ionospheric emission profiles (InjectorIonosphere, particle_injector.cpp:1160-1210) */
+#define RHGPU_IONO_COS_SZA_DAY_CONSTANT_NIGHT 1   /* ionoCosSzaDayConstantNight */
+#define RHGPU_IONO_CONSTANT_DAY_CONSTANT_NIGHT 2  /* ionoConstantDayConstantNight */
+#define RHGPU_IONO_CONSTANT 3                     /* ionoConstant */
+#define RHGPU_IONO_POLAR_CAP 4                    /* ionoPolarCap */
 /* neutral profiles (src/neutral_profiles.h) */
 #define RHGPU_NEUTRAL_CHAMBERLAIN_H 1   /* sum n0 exp(-H0 (1/r0 - 1/r)) */
 #define RHGPU_NEUTRAL_CHAMBERLAIN_T 2   /* sum n0 exp(-(G M m / k_B T0) (1/r0 - 1/r)) */
 #define RHGPU_NEUTRAL_EXPONENTIAL   3   /* sum n0 exp(-(r - r0) / H0) */
 #define RHGPU_NEUTRAL_POWER_LAW     4   /* sum n0 (r0 / r)^k0 */
+/* planetary models (no parameters; the Sun on +x): */
+#define RHGPU_NEUTRAL_VENUS_HYDROGEN 5  /* VenusHydrogen: thermal day/night + hot corona */
+#define RHGPU_NEUTRAL_VENUS_OXYGEN   6  /* VenusOxygen: day/night Chamberlain-like */
+#define RHGPU_NEUTRAL_MERCURY_SODIUM_EXNER20 7  /* MercurySodiumExner20: Exner et al. (2020) Na */
 #define RHGPU_NEUTRAL_MAX_COMPONENTS 4
 typedef struct rhgpu_injector {
    int32_t  species;                  /* population index */
@@ -349,11 +366,25 @@ typedef struct rhgpu_injector {
    double   total_production_rate;    /* [1/s], or < 0: use ionization_rate */
    double   macroparticles_per_cell_relative;
    double   upstream_macro_ratio;     /* Hybrid::upstreamMacroPleRatio (> 0) */
+   /* ionosphere (also uses temperature, total_production_rate,
+    * macroparticles_per_cell_relative, upstream_macro_ratio) */
+   double   emission_radius;          /* radius of the emission shell [m] */
+   double   noon_factor, night_factor;   /* `noon`, `night` (ionoPolarCap: tilt and cap half angle [deg]) */
+   int32_t  iono_profile;             /* RHGPU_IONO_* */
+   int32_t  reserved2;
 } rhgpu_injector;
 int rhgpu_set_injectors(rhgpu_ctx* ctx, int32_t n, const rhgpu_injector* injectors);
 /* injected per species: weight, macroparticles, weight * v^2
  * (logCounterParticleInject*, particle_injector.cpp:569-571); 3 * n_species doubles */
 int rhgpu_get_injection_counters(rhgpu_ctx* ctx, double* out, int32_t n);
+
+/* The neutral density [m^-3] of an exosphere source's profile (its profile,
+ * n_components, r0, n0, H0, T0, k0, gm_object; `mass` is the ion mass the
+ * Chamberlain T profile uses) at n points xyz (x, y, z interleaved, metres
+ * from the planet's centre), evaluated on `device` as the source's set-up
+ * does (getNeutralDensity, src/neutral_profiles.h:215-241). */
+int rhgpu_neutral_density(const rhgpu_injector* profile, double mass, int64_t n, const double* xyz, double* out,
+                          int32_t device);
 /* Philox-4x32-10 of the particle sources, host side (for checks): out = philox(ctr, key) */
 void rhgpu_philox4x32(const uint32_t* ctr, const uint32_t* key, uint32_t* out);
 

@@ -166,6 +166,7 @@ _OPTIONAL = {
     "set_injectors": [_P, C.c_int32, C.c_void_p],
     "get_injection_counters": [_P, _D, C.c_int32],
     "philox4x32": [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+    "neutral_density": [C.c_void_p, C.c_double, C.c_int64, _D, _D, C.c_int32],
     "log_open": [_P, C.c_void_p],
     "log_write": [_P, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_int32],
     "log_close": [_P],
@@ -177,7 +178,11 @@ _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void
 INJECT_SOLARWIND = 1
 INJECT_FLOW = 2
 INJECT_EXOSPHERE = 3
-NEUTRAL_PROFILES = {"ChamberlainH": 1, "ChamberlainT": 2, "Exponential": 3, "PowerLaw": 4}
+INJECT_IONOSPHERE = 4
+IONO_PROFILES = {"ionoCosSzaDayConstantNight": 1, "ionoConstantDayConstantNight": 2, "ionoConstant": 3,
+                 "ionoPolarCap": 4}
+NEUTRAL_PROFILES = {"ChamberlainH": 1, "ChamberlainT": 2, "Exponential": 3, "PowerLaw": 4, "VenusHydrogen": 5,
+                    "VenusOxygen": 6, "MercurySodiumExner20": 7}
 # flow injector walls (rhgpu_injector.inflow_walls)
 WALLS = {"+x": 1, "-x": 2, "+y": 4, "-y": 8, "+z": 16, "-z": 32}
 
@@ -192,7 +197,9 @@ class Injector(C.Structure):
                 ("gm_object", C.c_double), ("exobase_radius", C.c_double), ("shadow_radius", C.c_double),
                 ("ionization_rate", C.c_double), ("ionization_factor_shadow", C.c_double),
                 ("total_production_rate", C.c_double), ("macroparticles_per_cell_relative", C.c_double),
-                ("upstream_macro_ratio", C.c_double)]
+                ("upstream_macro_ratio", C.c_double), ("emission_radius", C.c_double),
+                ("noon_factor", C.c_double), ("night_factor", C.c_double), ("iono_profile", C.c_int32),
+                ("reserved2", C.c_int32)]
 
 
 class LogConfig(C.Structure):
@@ -471,6 +478,15 @@ def philox4x32(lib: "Library", ctr, key) -> list:
     o = (C.c_uint32 * 4)()
     lib.fn["philox4x32"](c, k, o)
     return list(o)
+
+
+def neutral_density(lib: "Library", injector, mass: float, xyz: np.ndarray, device: int = 0) -> np.ndarray:
+    """rhgpu_neutral_density: an exosphere source's neutral density at points (n x 3, metres)."""
+    p = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(p.shape[0], dtype=np.float64)
+    lib.call("neutral_density", C.cast(C.byref(injector), C.c_void_p), mass, p.shape[0], _ptr(p, C.c_double),
+             _ptr(out, C.c_double), device)
+    return out
 
 
 def gpu_library_path() -> str:

@@ -43,6 +43,7 @@ class Population:
     ppc: float = 20.0            # macroparticles_per_cell
     upstream: bool = True        # counts towards the upstream plasma parameters
     exosphere: Optional[dict] = None   # ExosphereInjector parameters of a planetary source
+    ionosphere: Optional[dict] = None  # IonosphereInjector parameters of a planetary source
 
     @property
     def q(self) -> float:
@@ -159,8 +160,9 @@ def upstream_macro_ratio(cfg: "Config") -> float:
 
 
 def source_injectors(cfg: "Config", seed: int = 1) -> list:
-    """Every particle source of the configuration: the solar wind injectors
-    and one InjectorExosphere per population with exosphere parameters."""
+    """Every particle source of the configuration: the solar wind injectors,
+    one InjectorExosphere per population with exosphere parameters and one
+    InjectorIonosphere per population with ionosphere parameters."""
     out = solar_wind_injectors(cfg, seed)
     ratio = upstream_macro_ratio(cfg)
     for s, p in enumerate(cfg.populations):
@@ -179,6 +181,17 @@ def source_injectors(cfg: "Config", seed: int = 1) -> list:
             j.n0[k] = n0
             j.H0[k] = H0
         out.append(j)
+    for s, p in enumerate(cfg.populations):
+        o = p.ionosphere
+        if not o:
+            continue
+        out.append(abi.Injector(species=s, type=abi.INJECT_IONOSPHERE, temperature=p.temperature,
+                                seed=seed * 1000003 + 500 + s, emission_radius=o["emission_radius"],
+                                noon_factor=o["noon"], night_factor=o["night"],
+                                iono_profile=abi.IONO_PROFILES[o["profile"]],
+                                total_production_rate=o["total_production_rate"],
+                                macroparticles_per_cell_relative=o.get("macroparticles_per_cell_relative", 1.0),
+                                upstream_macro_ratio=ratio))
     return out
 
 

@@ -19,6 +19,7 @@ namespace rh {
 constexpr int INJ_SOLARWIND = 1;   // RHGPU_INJECT_SOLARWIND
 constexpr int INJ_FLOW = 2;        // RHGPU_INJECT_FLOW
 constexpr int INJ_EXOSPHERE = 3;   // RHGPU_INJECT_EXOSPHERE
+constexpr int INJ_IONOSPHERE = 4;  // RHGPU_INJECT_IONOSPHERE
 constexpr double INJ_EPS_CELL = 1.0e-4;   // margin of a cell's random points (particle_injector.cpp:31)
 constexpr int INJ_MC_POINTS = 1000;       // Monte Carlo points per cell (particle_injector.cpp:33)
 constexpr int INJ_MAX_TRIES = 1000;   // bound of every rejection loop (failures raise a device error)
@@ -57,6 +58,101 @@ __device__ inline double neutralDensity(const NeutralProfile& P, double r) {
    return d;
 }
 
+// Planetary neutral models of neutral_profiles.h:79-214. Corsair's planetary
+// constants are not vendored with the reference; these are the IAU nominal
+// radii and masses and 15.999 u for oxygen.
+constexpr double NP_VENUS_RADIUS = 6051.8e3;
+constexpr double NP_VENUS_MASS = 4.8675e24;
+constexpr double NP_MASS_OXYGEN = 15.999 * 1.66053906660e-27;
+constexpr double NP_MERCURY_RADIUS = 2439.7e3;
+
+// solar zenith angle (the Sun on +x)
+__device__ inline double sza(double x, double r) { return acos(x / r); }
+
+// Venus hydrogen: thermal day/night Chamberlain-like terms blended by the solar
+// zenith angle, plus the hot corona (exp(a1 r + a2 + a3 / r)) at noon, the
+// terminator and midnight (neutral_profiles.h:79-112)
+__device__ inline double venusHydrogen(double x, double y, double z) {
+   const double r = sqrt(x * x + y * y + z * z);
+   const double chi = sza(x, r);
+   const double exoR = NP_VENUS_RADIUS + 170e3;
+   const double GM = RHGPU_GRAVITY * NP_VENUS_MASS;
+   const double bDay = GM * RHGPU_MASS_PROTON / (RHGPU_BOLTZMANN * 285);
+   const double bNight = GM * RHGPU_MASS_PROTON / (RHGPU_BOLTZMANN * 110);
+   const double nDay = 1.32e11 * exp(-bDay * (1 / exoR - 1.0 / r));
+   const double nNight = 2.59e12 * exp(-bNight * (1.0 / exoR - 1.0 / r));
+   const double thermal = (1.0 - (chi / M_PI)) * nDay + (chi / M_PI) * nNight;
+   // hot corona fits: (a1 [1/m], a2, a3 [m]) at noon, terminator, midnight
+   const double hot[3][3] = {{-6.2625e-5 / 1e3, 15.4817, 3.6414e4 * 1e3},
+                             {-8.4607e-5 / 1e3, 15.9944, 2.9743e4 * 1e3},
+                             {-6.2309e-5 / 1e3, 15.2723, 4.3781e4 * 1e3}};
+   double h[3];
+   for (int q = 0; q < 3; ++q) h[q] = exp(hot[q][0] * r + hot[q][1] + hot[q][2] / r);
+   const double u = chi / (M_PI / 2);
+   const double hotN = chi <= M_PI / 2 ? (1.0 - u) * h[0] + u * h[1] : (1.0 - (u - 1)) * h[1] + (u - 1) * h[2];
+   return thermal + hotN;
+}
+
+// Venus oxygen: day and night Chamberlain-like profiles from their base radii,
+// blended by the solar zenith angle (neutral_profiles.h:114-138)
+__device__ inline double venusOxygen(double x, double y, double z) {
+   const double r = sqrt(x * x + y * y + z * z);
+   const double chi = sza(x, r);
+   const double GMm = RHGPU_GRAVITY * NP_VENUS_MASS * NP_MASS_OXYGEN;
+   const double r0Day = NP_VENUS_RADIUS + 200e3, r0Night = NP_VENUS_RADIUS + 300e3;
+   const double bDay = GMm / (RHGPU_BOLTZMANN * 6400), bNight = GMm / (RHGPU_BOLTZMANN * 4847);
+   const double nDay = r < r0Day ? 0.0 : 7.5e10 * exp(-bDay * (1.0 / r0Day - 1.0 / r));
+   const double nNight = r < r0Night ? 0.0 : 2e9 * exp(-bNight * (1.0 / r0Night - 1.0 / r));
+   return (1.0 - (chi / M_PI)) * nDay + (chi / M_PI) * nNight;
+}
+
+// one component of the Mercury sodium model: exponential in altitude times a
+// Gaussian in the great-circle angle from its maximum (neutral_profiles.h:141-147)
+__device__ inline double expexpNa(double x, double y, double z, double r, double Rp, double n0, double Hr, double Ht,
+                                  double latMax, double lonMax) {
+   const double lat = atan2(z, sqrt(x * x + y * y));
+   const double lon = atan2(y, x);
+   const double dth = acos(sin(lat) * sin(latMax) + cos(lat) * cos(latMax) * cos(lonMax - lon));
+   return n0 * exp(-(r - Rp) / Hr) * exp(-((dth / Ht) * (dth / Ht)));
+}
+
+// Mercury sodium, Exner et al. (2020, J. Geophys. Res. 125, e2019JA027691):
+// micro-meteoroid vaporisation, thermal desorption, two photon-stimulated
+// desorption lobes and four sputtering lobes, times (Rp / r)^2
+// (neutral_profiles.h:150-213)
+__device__ inline double mercurySodium(double x, double y, double z) {
+   const double Rp = NP_MERCURY_RADIUS;
+   const double r = sqrt(x * x + y * y + z * z);
+   const double d = M_PI / 180.0;
+   // {n0 [m^-3], Hr [m], angular width, latitude, longitude of the maximum}
+   const double lobes[7][5] = {{8.86e9, 100e3, 15 * d, 0 * d, 0 * d},        // thermal desorption
+                               {5.67e6, 748e3, 15 * d, 80 * d, 0 * d},       // sputtering, day
+                               {5.67e6, 748e3, 15 * d, -80 * d, 0 * d},
+                               {5.67e6, 748e3, 10 * d, 15 * d, 180 * d},     // sputtering, night
+                               {5.67e6, 748e3, 10 * d, -15 * d, 180 * d},
+                               {4.06e10, 232e3, 20 * d, 50 * d, 0 * d},      // photon-stimulated desorption
+                               {4.06e10, 232e3, 20 * d, -50 * d, 0 * d}};
+   double sum = 7.84e6 * exp(-(r - Rp) / 431e3);   // micro-meteoroid vaporisation
+   for (int q = 0; q < 7; ++q)
+      sum = sum + expexpNa(x, y, z, r, Rp, lobes[q][0], lobes[q][1], lobes[q][2], lobes[q][3], lobes[q][4]);
+   return ((Rp / r) * (Rp / r)) * sum;
+}
+
+// neutral density at (x, y, z): the planetary models (types 5-7) or a radial profile
+__device__ inline double neutralDensityAt(const NeutralProfile& P, double x, double y, double z) {
+   if (P.type == 5) return venusHydrogen(x, y, z);
+   if (P.type == 6) return venusOxygen(x, y, z);
+   if (P.type == 7) return mercurySodium(x, y, z);
+   return neutralDensity(P, sqrt(x * x + y * y + z * z));
+}
+
+// the neutral density at n points (x, y, z interleaved)
+__global__ void k_np_eval(NeutralProfile P, long long n, const double* xyz, double* out) {
+   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (t >= n) return;
+   out[t] = neutralDensityAt(P, xyz[3 * t], xyz[3 * t + 1], xyz[3 * t + 2]);
+}
+
 // each cell's mean neutral density times its volume by Monte Carlo over
 // INJ_MC_POINTS points (zero below the exobase), particle_injector.cpp:1718-1736
 __global__ void k_exo_density(GridInfo g, NeutralProfile P, double R2exo, unsigned long long seed, double* out) {
@@ -73,7 +169,7 @@ __global__ void k_exo_density(GridInfo g, NeutralProfile P, double R2exo, unsign
       const double z = zc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
       const double r2 = x * x + y * y + z * z;
       if (r2 < R2exo) continue;
-      sum += neutralDensity(P, sqrt(r2));
+      sum += neutralDensityAt(P, x, y, z);
    }
    out[n] = sum / INJ_MC_POINTS * g.dV;
 }
@@ -144,10 +240,56 @@ __device__ inline void injState(const InjDev& J, double dx, RngStream& r, GaussS
    } else if (J.type == INJ_FLOW) {
       for (int a = 0; a < 3; ++a) st[a] = r.uniform() * dx;
       for (int a = 0; a < 3; ++a) st[3 + a] = J.vel[a] + J.vth * g.next(r);
-   } else {   // exosphere (particle_injector.cpp:1538-1564)
+   } else {   // exosphere, ionosphere (particle_injector.cpp:1538-1564, 985-1018)
       for (int a = 0; a < 3; ++a) st[a] = 0.5 * dx + (1.0 - INJ_EPS_CELL) * dx * (r.uniform() - 0.5);
       for (int a = 0; a < 3; ++a) st[3 + a] = J.vth * g.next(r);
    }
+}
+
+// ionosphere: each cell's share of the emission shell r = R, by Monte Carlo
+// over INJ_MC_POINTS points of the cell projected on the shell, times the
+// emission profile at the cell centre (InjectorIonosphere::initialize,
+// particle_injector.cpp:1114-1210); profile 1..4 as RHGPU_IONO_*
+__device__ inline double ionoFactor(int profile, double noon, double night, double xc, double yc, double zc) {
+   if (profile == 3) return 1.0;
+   if (profile == 4) {   // polar caps: rotated toward noon by `noon` degrees, half angle `night` degrees
+      const double t = fabs(noon) * M_PI / 180.0, cap = fabs(night) * M_PI / 180.0;
+      const double s = zc > 0.0 ? -t : t;
+      const double x = xc * cos(s) + zc * sin(s), z = xc * sin(s) + zc * cos(s);
+      const double rr = sqrt(x * x + yc * yc + z * z);
+      const double colat = fabs(M_PI / 2.0 - acos(x / rr));
+      return colat <= cap ? 1.0 : 0.0;
+   }
+   const double rr = sqrt(xc * xc + yc * yc + zc * zc);
+   const double chi = acos(xc / rr);
+   if (profile == 1) return chi < M_PI / 2 ? noon + (night - noon) * (1 - cos(chi)) : night;
+   return chi < M_PI / 2 ? noon : night;   // 2: constant day, constant night
+}
+__global__ void k_iono_shell(GridInfo g, double R, int profile, double noon, double night, unsigned long long seed,
+                             double* out) {
+   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (n >= g.N) return;
+   const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((long long)g.nx * g.ny));
+   const double xc = g.x_min + (i + 0.5) * g.dx, yc = g.y_min + (j + 0.5) * g.dx, zc = g.z_min + (k + 0.5) * g.dx;
+   const double lo[3] = {xc - 0.5 * g.dx, yc - 0.5 * g.dx, zc - 0.5 * g.dx};
+   const double hi[3] = {xc + 0.5 * g.dx, yc + 0.5 * g.dx, zc + 0.5 * g.dx};
+   RngStream r;
+   r.init(seed, 0x10705u, (uint32_t)n, (uint32_t)(n >> 32));
+   double inside = 0.0;
+   for (int s = 0; s < INJ_MC_POINTS; ++s) {
+      double p[3];
+      p[0] = xc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      p[1] = yc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      p[2] = zc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double norm = R / sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+      bool in = true;
+      for (int a = 0; a < 3; ++a) {
+         p[a] *= norm;
+         in = in && p[a] > lo[a] && p[a] < hi[a];
+      }
+      if (in) inside += 1.0;
+   }
+   out[n] = inside * ionoFactor(profile, noon, night, xc, yc, zc);
 }
 
 // migration of an injected position that sits on the far face of its cell
@@ -213,7 +355,7 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
    if (t < J.ncells) {
       r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
       // probRound: floor(x) + 1 with probability x - floor(x)
-      const double x = J.type == INJ_EXOSPHERE ? J.rates[t] : J.perCellPerDt;
+      const double x = (J.type == INJ_EXOSPHERE || J.type == INJ_IONOSPHERE) ? J.rates[t] : J.perCellPerDt;
       if (x > 0) {
          n = (int)floor(x);
          if (r.uniform() < x - n) ++n;
@@ -242,6 +384,11 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
       injState(J, g.dx, r, gs, st);
       st[6] = J.w;
       int i = ci, j = cj, k = ck;
+      if (J.type == INJ_IONOSPHERE) {   // upward (particle_injector.cpp:1008-1013)
+         const double xg = g.x_min + ci * g.dx + st[0], yg = g.y_min + cj * g.dx + st[1], zg = g.z_min + ck * g.dx + st[2];
+         if (st[3] * xg + st[4] * yg + st[5] * zg < 0)
+            for (int a = 3; a < 6; ++a) st[a] = -st[a];
+      }
       // exosphere: only above the exobase, no redraw (particle_injector.cpp:1547-1549)
       bool keep = true;
       if (J.type == INJ_EXOSPHERE) {

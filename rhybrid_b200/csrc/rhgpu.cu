@@ -944,7 +944,9 @@ template <class MV>
 int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
    for (const InjHost& h : c->inj) {
       if (h.d.ncells == 0) continue;
-      RH_TIME(c, h.d.type == INJ_EXOSPHERE ? "inject_exosphere" : "inject_inflow");
+      RH_TIME(c, h.d.type == INJ_EXOSPHERE    ? "inject_exosphere"
+                 : h.d.type == INJ_IONOSPHERE ? "inject_ionosphere"
+                                              : "inject_inflow");
       k_inject<MV><<<blocks1d(h.d.ncells, 128), 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers,
                                                                      c->fb.nmovers, moverCap, c->injCnt, c->err);
       RH_LAUNCHED(c);
@@ -1567,25 +1569,35 @@ namespace {
 // InjectorExosphere::initialize (particle_injector.cpp:1610-1797): each cell's
 // expected exospheric ion macroparticles per step, the weight and the cells
 // that get any
-int exoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>& cells, std::vector<double>& rates) {
-   const GridInfo& g = c->g;
-   if (J.profile < 1 || J.profile > 4 || J.n_components < 1 || J.n_components > RHGPU_NEUTRAL_MAX_COMPONENTS)
-      return fail(RHGPU_ERR_ARG, "set_injectors: exosphere profile or its number of components");
-   if (!(J.upstream_macro_ratio > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs upstream_macro_ratio > 0");
-   const bool ionGiven = J.ionization_rate >= 0, totalGiven = J.total_production_rate >= 0;
-   if (ionGiven == totalGiven)
-      return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs exactly one of ionization_rate, total_production_rate");
-   const double m = c->sp[J.species].m;
-   NeutralProfile P;
+// the device form of a neutral profile (per-component parameters of the radial profiles)
+int neutralProfile(const rhgpu_injector& J, double m, NeutralProfile& P) {
    std::memset(&P, 0, sizeof P);
+   const bool planet = J.profile >= RHGPU_NEUTRAL_VENUS_HYDROGEN && J.profile <= RHGPU_NEUTRAL_MERCURY_SODIUM_EXNER20;
+   if (!planet && (J.profile < 1 || J.profile > 4 || J.n_components < 1 || J.n_components > RHGPU_NEUTRAL_MAX_COMPONENTS))
+      return fail(RHGPU_ERR_ARG, "neutral profile type or its number of components");
    P.type = J.profile;
-   P.n = J.n_components;
+   P.n = planet ? 0 : J.n_components;
    P.r0 = J.r0;
    for (int i = 0; i < P.n; ++i) {
       P.n0[i] = J.n0[i];
       P.b[i] = J.profile == RHGPU_NEUTRAL_CHAMBERLAIN_H || J.profile == RHGPU_NEUTRAL_EXPONENTIAL ? J.H0[i]
                : J.profile == RHGPU_NEUTRAL_CHAMBERLAIN_T ? J.gm_object * m / (1.380649e-23 * J.T0[i])
                                                           : J.k0[i];
+   }
+   return RHGPU_OK;
+}
+
+int exoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>& cells, std::vector<double>& rates) {
+   const GridInfo& g = c->g;
+   if (!(J.upstream_macro_ratio > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs upstream_macro_ratio > 0");
+   const bool ionGiven = J.ionization_rate >= 0, totalGiven = J.total_production_rate >= 0;
+   if (ionGiven == totalGiven)
+      return fail(RHGPU_ERR_ARG, "set_injectors: exosphere needs exactly one of ionization_rate, total_production_rate");
+   const double m = c->sp[J.species].m;
+   NeutralProfile P;
+   {
+      const int rc = neutralProfile(J, m, P);
+      if (rc) return rc;
    }
    const double Rexo = std::max(J.exobase_radius, 0.0), Rsh = std::max(J.shadow_radius, 0.0);
    h.d.R2exo = Rexo * Rexo;
@@ -1623,6 +1635,42 @@ int exoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>
    }
    h.d.w = totalRate * g.dt / perDt;
    h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
+   return RHGPU_OK;
+}
+// ionosphere: expected macroparticles per step of every cell on the emission
+// shell (InjectorIonosphere::initialize, particle_injector.cpp:1059-1229)
+int ionoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>& cells, std::vector<double>& rates) {
+   const GridInfo& g = c->g;
+   if (J.iono_profile < RHGPU_IONO_COS_SZA_DAY_CONSTANT_NIGHT || J.iono_profile > RHGPU_IONO_POLAR_CAP)
+      return fail(RHGPU_ERR_ARG, "set_injectors: unknown ionospheric emission profile");
+   if (!(J.emission_radius > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: ionosphere needs emission_radius > 0");
+   const double rel = J.macroparticles_per_cell_relative >= 0 ? J.macroparticles_per_cell_relative : 1.0;
+   const double perDt = rel * (J.upstream_macro_ratio > 0 ? J.upstream_macro_ratio : 100.0);
+   const double totalRate = J.total_production_rate;
+   const double m = c->sp[J.species].m;
+   h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
+   if (!(perDt > 0 && totalRate > 0)) { h.d.w = 0.0; return RHGPU_OK; }   // no emission
+   double* shell = nullptr;
+   RH_CUDA(cudaMalloc(&shell, sizeof(double) * g.N));
+   k_iono_shell<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, J.emission_radius, J.iono_profile, J.noon_factor,
+                                                            J.night_factor, J.seed, shell);
+   std::vector<double> inside(g.N);
+   cudaError_t e = cudaGetLastError();
+   if (e == cudaSuccess) e = cudaMemcpyAsync(inside.data(), shell, sizeof(double) * g.N, cudaMemcpyDeviceToHost, c->stream);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+   cudaFree(shell);
+   if (e != cudaSuccess) return fail(RHGPU_ERR_CUDA, std::string("set_injectors: ionosphere shell: ") + cudaGetErrorString(e));
+   double total = 0.0;
+   for (double v : inside) total += v;
+   if (total > 0.0)
+      for (long long n = 0; n < g.N; ++n) {
+         const double r = perDt * inside[n] / total;
+         if (r > 0) {
+            cells.push_back((int)n);
+            rates.push_back(r);
+         }
+      }
+   h.d.w = totalRate * g.dt / perDt;
    return RHGPU_OK;
 }
 }  // namespace
@@ -2212,9 +2260,9 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
                      if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
                   if (in) cells.push_back(i + g.nx * (j + g.ny * k));
                }
-      } else if (J.type == RHGPU_INJECT_EXOSPHERE) {
+      } else if (J.type == RHGPU_INJECT_EXOSPHERE || J.type == RHGPU_INJECT_IONOSPHERE) {
          std::vector<double> rates;
-         int rc = exoRates(c, J, h, cells, rates);
+         int rc = J.type == RHGPU_INJECT_EXOSPHERE ? exoRates(c, J, h, cells, rates) : ionoRates(c, J, h, cells, rates);
          if (rc) return rc;
          if (!rates.empty()) {
             RH_CUDA(cudaMalloc(&h.rates, sizeof(double) * rates.size()));
@@ -2235,6 +2283,29 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
       c->inj.push_back(h);
    }
    c->injKeyMax = keyBase;
+   return RHGPU_OK;
+}
+
+int rhgpu_neutral_density(const rhgpu_injector* profile, double mass, int64_t n, const double* xyz, double* out,
+                          int32_t device) {
+   if (!profile || n < 0 || (n > 0 && (!xyz || !out))) return fail(RHGPU_ERR_ARG, "neutral_density: bad arguments");
+   NeutralProfile P;
+   int rc = neutralProfile(*profile, mass, P);
+   if (rc) return rc;
+   if (n == 0) return RHGPU_OK;
+   RH_CUDA(cudaSetDevice(device));
+   double *dx = nullptr, *dout = nullptr;
+   RH_CUDA(cudaMalloc(&dx, sizeof(double) * 3 * n));
+   cudaError_t e = cudaMalloc(&dout, sizeof(double) * n);
+   if (e == cudaSuccess) e = cudaMemcpy(dx, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice);
+   if (e == cudaSuccess) {
+      k_np_eval<<<blocks1d(n, 128), 128>>>(P, n, dx, dout);
+      e = cudaGetLastError();
+   }
+   if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+   cudaFree(dx);
+   cudaFree(dout);
+   if (e != cudaSuccess) return fail(RHGPU_ERR_CUDA, std::string("neutral_density: ") + cudaGetErrorString(e));
    return RHGPU_OK;
 }
 

@@ -191,3 +191,116 @@ def test_exosphere_source(lib):
             rc2 = (-1.2e6 + (j + 0.5) * 100e3) ** 2 + (-1.2e6 + (k + 0.5) * 100e3) ** 2
             assert not np.any((xc < 0) & (rc2 < 600e3 ** 2))
             assert p.shape[0] > 0
+
+
+# the planetary neutral models of neutral_profiles.h:79-214 restated in numpy
+# (constants as the library states them: IAU radii and masses, 15.999 u oxygen)
+VENUS_R, VENUS_M, M_O, MERCURY_R = 6051.8e3, 4.8675e24, 15.999 * 1.66053906660e-27, 2439.7e3
+
+
+def np_venus_h(x, y, z):
+    r = np.sqrt(x * x + y * y + z * z)
+    chi = np.arccos(x / r)
+    exoR = VENUS_R + 170e3
+    GM = abi.GRAVITY * VENUS_M
+    bd, bn = GM * abi.MASS_PROTON / (abi.BOLTZMANN * 285), GM * abi.MASS_PROTON / (abi.BOLTZMANN * 110)
+    th = (1 - chi / np.pi) * 1.32e11 * np.exp(-bd * (1 / exoR - 1 / r)) + (chi / np.pi) * 2.59e12 * np.exp(-bn * (1 / exoR - 1 / r))
+    h = [np.exp(a1 * r + a2 + a3 / r) for a1, a2, a3 in ((-6.2625e-5 / 1e3, 15.4817, 3.6414e7),
+                                                         (-8.4607e-5 / 1e3, 15.9944, 2.9743e7),
+                                                         (-6.2309e-5 / 1e3, 15.2723, 4.3781e7))]
+    u = chi / (np.pi / 2)
+    hot = np.where(chi <= np.pi / 2, (1 - u) * h[0] + u * h[1], (2 - u) * h[1] + (u - 1) * h[2])
+    return th + hot
+
+
+def np_venus_o(x, y, z):
+    r = np.sqrt(x * x + y * y + z * z)
+    chi = np.arccos(x / r)
+    GMm = abi.GRAVITY * VENUS_M * M_O
+    r0d, r0n = VENUS_R + 200e3, VENUS_R + 300e3
+    nd = np.where(r < r0d, 0.0, 7.5e10 * np.exp(-GMm / (abi.BOLTZMANN * 6400) * (1 / r0d - 1 / r)))
+    nn = np.where(r < r0n, 0.0, 2e9 * np.exp(-GMm / (abi.BOLTZMANN * 4847) * (1 / r0n - 1 / r)))
+    return (1 - chi / np.pi) * nd + (chi / np.pi) * nn
+
+
+def np_mercury_na(x, y, z):
+    r = np.sqrt(x * x + y * y + z * z)
+    d = np.pi / 180
+    lat, lon = np.arctan2(z, np.sqrt(x * x + y * y)), np.arctan2(y, x)
+
+    def lobe(n0, hr, ht, la, lo):
+        dth = np.arccos(np.sin(lat) * np.sin(la) + np.cos(lat) * np.cos(la) * np.cos(lo - lon))
+        return n0 * np.exp(-(r - MERCURY_R) / hr) * np.exp(-(dth / ht) ** 2)
+    s = 7.84e6 * np.exp(-(r - MERCURY_R) / 431e3)
+    for args in ((8.86e9, 100e3, 15 * d, 0, 0), (5.67e6, 748e3, 15 * d, 80 * d, 0), (5.67e6, 748e3, 15 * d, -80 * d, 0),
+                 (5.67e6, 748e3, 10 * d, 15 * d, np.pi), (5.67e6, 748e3, 10 * d, -15 * d, np.pi),
+                 (4.06e10, 232e3, 20 * d, 50 * d, 0), (4.06e10, 232e3, 20 * d, -50 * d, 0)):
+        s = s + lobe(*args)
+    return (MERCURY_R / r) ** 2 * s
+
+
+@pytest.mark.parametrize("name,fn,R", [("VenusHydrogen", np_venus_h, VENUS_R), ("VenusOxygen", np_venus_o, VENUS_R),
+                                       ("MercurySodiumExner20", np_mercury_na, MERCURY_R)])
+def test_planetary_neutral_models(lib, name, fn, R):
+    """getNeutralDensity's planetary models (neutral_profiles.h:79-214) on the
+    GPU against numpy at points from the surface to 5 planet radii, all
+    directions."""
+    rng = np.random.default_rng(11)
+    n = 20000
+    u = rng.normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    xyz = u * rng.uniform(1.0, 5.0, size=(n, 1)) * R
+    j = abi.Injector(type=abi.INJECT_EXOSPHERE, profile=abi.NEUTRAL_PROFILES[name])
+    got = abi.neutral_density(lib, j, 16 * abi.MASS_PROTON, xyz)
+    want = fn(xyz[:, 0], xyz[:, 1], xyz[:, 2])
+    assert np.all(want >= 0) and want.max() > 0
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-10 * want.max())
+
+
+def iono_injector(profile, noon=1.0, night=0.1, seed=9):
+    return abi.Injector(species=0, type=abi.INJECT_IONOSPHERE, temperature=1e3, seed=seed,
+                        emission_radius=650e3, noon_factor=noon, night_factor=night,
+                        iono_profile=abi.IONO_PROFILES[profile], total_production_rate=1e24,
+                        macroparticles_per_cell_relative=1.0, upstream_macro_ratio=400.0)
+
+
+@pytest.mark.parametrize("profile", ["ionoCosSzaDayConstantNight", "ionoConstant"])
+def test_ionosphere_source(lib, profile):
+    """InjectorIonosphere: about macroparticles_per_cell_relative *
+    upstream_macro_ratio = 400 new ions per step, in the cells the emission
+    shell r = 650 km crosses, moving outward, weight total rate * dt / 400; the
+    cos(SZA)-day / constant-night profile (noon 1, night 0.1) puts most of them
+    on the dayside, the constant one about half."""
+    cfg = exo_box()
+    grid, _ = cf.initial_state(cfg)
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[100000])
+    try:
+        ctx.set_path(abi.PATH_FAST)
+        ctx.upload_array("faceB", grid["faceB"])
+        ctx.upload_array("cellB", grid["cellB"])
+        ctx.upload_array("nodeEta", grid["nodeEta"])
+        ctx.upload_cell_flags(grid["flags"])
+        ctx.upload_particles(0, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+        ctx.set_injectors([iono_injector(profile)])
+        ctx.step(1)
+        cnt, p = ctx.download_particles(0)
+        ic = ctx.injection_counters()[0]
+    finally:
+        ctx.close()
+    cell = np.repeat(np.arange(cfg.ncells), cnt.astype(np.int64))
+    i, j, k = cell % 24, (cell // 24) % 24, cell // 576
+    xg = -1.2e6 + i * 100e3 + p[:, 0]
+    yg = -1.2e6 + j * 100e3 + p[:, 1]
+    zg = -1.2e6 + k * 100e3 + p[:, 2]
+    r = np.sqrt(xg ** 2 + yg ** 2 + zg ** 2)
+    assert 320 <= p.shape[0] <= 480, p.shape[0]
+    assert ic["macroparticles"] == p.shape[0]
+    assert np.all(np.abs(r - 650e3) < math.sqrt(3) * 100e3 + 0.05 * 3.0 * 900e3 * 0.05)
+    # outward at injection; one push of 0.05 s at thermal speeds keeps it so for nearly all
+    assert np.mean(p[:, 3] * xg + p[:, 4] * yg + p[:, 5] * zg > 0) > 0.95
+    assert math.isclose(p[0, 6], 1e24 * cfg.dt / 400.0, rel_tol=1e-12)
+    day = np.mean(xg > 0)
+    if profile == "ionoConstant":
+        assert 0.4 < day < 0.6
+    else:
+        assert day > 0.75
