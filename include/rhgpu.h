@@ -323,12 +323,20 @@ int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
  *     N = macroparticles_per_cell_relative * upstream_macro_ratio per step in
  *     the box, weight total_production_rate dt / N. New particles are uniform
  *     in the cell with Gaussian velocities of the temperature, turned outward.
+ *   RHGPU_INJECT_CHAPMAN_IONOSPHERE (InjectorChapmanIonosphere, :1242-1482):
+ *     as the ionosphere, but each point is kept with the Chapman probability
+ *     a exp(1 - h - exp(-h)), h = (r - R)/H - log(1/a), a the cos(SZA)-day /
+ *     constant-night factor (noon_factor, night_factor), H the scale height
+ *     k_B T / (m g_Mars) (150 K for the cells' shares, `temperature` for the
+ *     new particles); cells with fewer than 10 of 1000 Monte Carlo points
+ *     kept emit nothing.
  * Solar wind and flow: weight n dx^3 / ppc. Thermal speed sqrt(k_B T / m)
  * with the species' mass. n == 0 removes all sources. */
 #define RHGPU_INJECT_SOLARWIND 1
 #define RHGPU_INJECT_FLOW      2
 #define RHGPU_INJECT_EXOSPHERE 3
 #define RHGPU_INJECT_IONOSPHERE 4
+#define RHGPU_INJECT_CHAPMAN_IONOSPHERE 5
 /* ionospheric emission profiles (InjectorIonosphere, particle_injector.cpp:1160-1210) */
 #define RHGPU_IONO_COS_SZA_DAY_CONSTANT_NIGHT 1   /* ionoCosSzaDayConstantNight */
 #define RHGPU_IONO_CONSTANT_DAY_CONSTANT_NIGHT 2  /* ionoConstantDayConstantNight */

@@ -179,6 +179,7 @@ INJECT_SOLARWIND = 1
 INJECT_FLOW = 2
 INJECT_EXOSPHERE = 3
 INJECT_IONOSPHERE = 4
+INJECT_CHAPMAN_IONOSPHERE = 5
 IONO_PROFILES = {"ionoCosSzaDayConstantNight": 1, "ionoConstantDayConstantNight": 2, "ionoConstant": 3,
                  "ionoPolarCap": 4}
 NEUTRAL_PROFILES = {"ChamberlainH": 1, "ChamberlainT": 2, "Exponential": 3, "PowerLaw": 4, "VenusHydrogen": 5,

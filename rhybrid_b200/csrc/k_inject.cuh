@@ -20,6 +20,7 @@ constexpr int INJ_SOLARWIND = 1;   // RHGPU_INJECT_SOLARWIND
 constexpr int INJ_FLOW = 2;        // RHGPU_INJECT_FLOW
 constexpr int INJ_EXOSPHERE = 3;   // RHGPU_INJECT_EXOSPHERE
 constexpr int INJ_IONOSPHERE = 4;  // RHGPU_INJECT_IONOSPHERE
+constexpr int INJ_CHAPMAN = 5;     // RHGPU_INJECT_CHAPMAN_IONOSPHERE
 constexpr double INJ_EPS_CELL = 1.0e-4;   // margin of a cell's random points (particle_injector.cpp:31)
 constexpr int INJ_MC_POINTS = 1000;       // Monte Carlo points per cell (particle_injector.cpp:33)
 constexpr int INJ_MAX_TRIES = 1000;   // bound of every rejection loop (failures raise a device error)
@@ -39,6 +40,7 @@ struct InjDev {
    long long keyBase;    // first mover key source id (above every real segment)
    const double* rates;  // exosphere: expected macroparticles per step of each injection cell
    double R2exo;         // exosphere: squared exobase radius
+   double R, noon, night, H;   // Chapman ionosphere: emission radius, day/night factors, scale height
 };
 
 // neutral density of an exospheric profile at radius r (neutral_profiles.h:36-87):
@@ -240,7 +242,7 @@ __device__ inline void injState(const InjDev& J, double dx, RngStream& r, GaussS
    } else if (J.type == INJ_FLOW) {
       for (int a = 0; a < 3; ++a) st[a] = r.uniform() * dx;
       for (int a = 0; a < 3; ++a) st[3 + a] = J.vel[a] + J.vth * g.next(r);
-   } else {   // exosphere, ionosphere (particle_injector.cpp:1538-1564, 985-1018)
+   } else {   // exosphere, ionospheres (particle_injector.cpp:1538-1564, 985-1018, 1285-1318)
       for (int a = 0; a < 3; ++a) st[a] = 0.5 * dx + (1.0 - INJ_EPS_CELL) * dx * (r.uniform() - 0.5);
       for (int a = 0; a < 3; ++a) st[3 + a] = J.vth * g.next(r);
    }
@@ -265,6 +267,39 @@ __device__ inline double ionoFactor(int profile, double noon, double night, doub
    if (profile == 1) return chi < M_PI / 2 ? noon + (night - noon) * (1 - cos(chi)) : night;
    return chi < M_PI / 2 ? noon : night;   // 2: constant day, constant night
 }
+// Chapman ionosphere: acceptance a0 = a exp(1 - h - exp(-h)) of a point at
+// (x, y, z) with h = (r - R) / H - log(1 / a), a the cos(SZA)-day / constant-night
+// factor there (particle_injector.cpp:1299-1312, 1444-1456). The scale height
+// uses Mars' surface gravity (Corsair's constants are not vendored: IAU
+// nominal mass 6.4171e23 kg and radius 3389.5 km).
+constexpr double NP_MARS_MASS = 6.4171e23;
+constexpr double NP_MARS_RADIUS = 3389.5e3;
+__device__ inline double chapmanAccept(double x, double y, double z, double R, double noon, double night, double H) {
+   const double r = sqrt(x * x + y * y + z * z);
+   const double chi = acos(x / r);
+   const double a = chi < M_PI / 2 ? noon + (night - noon) * (1 - cos(chi)) : night;
+   const double h = (r - R) / H - log(1.0 / a);
+   return a * exp(1 - h - exp(-1 * h));
+}
+__global__ void k_chapman_shell(GridInfo g, double R, double noon, double night, double H, unsigned long long seed,
+                                double* out) {
+   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (n >= g.N) return;
+   const int i = (int)(n % g.nx), j = (int)((n / g.nx) % g.ny), k = (int)(n / ((long long)g.nx * g.ny));
+   const double xc = g.x_min + (i + 0.5) * g.dx, yc = g.y_min + (j + 0.5) * g.dx, zc = g.z_min + (k + 0.5) * g.dx;
+   RngStream r;
+   r.init(seed, 0xC4A9u, (uint32_t)n, (uint32_t)(n >> 32));
+   double inside = 0.0;
+   for (int s = 0; s < INJ_MC_POINTS; ++s) {
+      const double x = xc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double y = yc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double z = zc + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+      const double a0 = chapmanAccept(x, y, z, R, noon, night, H);
+      if (r.uniform() < a0) inside += 1.0;
+   }
+   out[n] = inside < 10 ? 0.0 : inside;   // cells with fewer than 10 kept points emit nothing
+}
+
 __global__ void k_iono_shell(GridInfo g, double R, int profile, double noon, double night, unsigned long long seed,
                              double* out) {
    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -355,7 +390,8 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
    if (t < J.ncells) {
       r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
       // probRound: floor(x) + 1 with probability x - floor(x)
-      const double x = (J.type == INJ_EXOSPHERE || J.type == INJ_IONOSPHERE) ? J.rates[t] : J.perCellPerDt;
+      const double x = (J.type == INJ_EXOSPHERE || J.type == INJ_IONOSPHERE || J.type == INJ_CHAPMAN) ? J.rates[t]
+                                                                                                    : J.perCellPerDt;
       if (x > 0) {
          n = (int)floor(x);
          if (r.uniform() < x - n) ++n;
@@ -384,7 +420,18 @@ __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* 
       injState(J, g.dx, r, gs, st);
       st[6] = J.w;
       int i = ci, j = cj, k = ck;
-      if (J.type == INJ_IONOSPHERE) {   // upward (particle_injector.cpp:1008-1013)
+      if (J.type == INJ_CHAPMAN) {   // positions redrawn until accepted (particle_injector.cpp:1285-1318)
+         bool acc = false;
+         for (int tr = 0; tr < INJ_MAX_TRIES && !acc; ++tr) {
+            if (tr > 0)
+               for (int a = 0; a < 3; ++a) st[a] = 0.5 * g.dx + (1.0 - INJ_EPS_CELL) * g.dx * (r.uniform() - 0.5);
+            const double a0 = chapmanAccept(g.x_min + ci * g.dx + st[0], g.y_min + cj * g.dx + st[1],
+                                            g.z_min + ck * g.dx + st[2], J.R, J.noon, J.night, J.H);
+            acc = r.uniform() < a0;
+         }
+         if (!acc) gs.ok = false;
+      }
+      if (J.type == INJ_IONOSPHERE || J.type == INJ_CHAPMAN) {   // upward (particle_injector.cpp:1008-1013)
          const double xg = g.x_min + ci * g.dx + st[0], yg = g.y_min + cj * g.dx + st[1], zg = g.z_min + ck * g.dx + st[2];
          if (st[3] * xg + st[4] * yg + st[5] * zg < 0)
             for (int a = 3; a < 6; ++a) st[a] = -st[a];

@@ -944,9 +944,9 @@ template <class MV>
 int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
    for (const InjHost& h : c->inj) {
       if (h.d.ncells == 0) continue;
-      RH_TIME(c, h.d.type == INJ_EXOSPHERE    ? "inject_exosphere"
-                 : h.d.type == INJ_IONOSPHERE ? "inject_ionosphere"
-                                              : "inject_inflow");
+      RH_TIME(c, h.d.type == INJ_EXOSPHERE                                  ? "inject_exosphere"
+                 : (h.d.type == INJ_IONOSPHERE || h.d.type == INJ_CHAPMAN) ? "inject_ionosphere"
+                                                                            : "inject_inflow");
       k_inject<MV><<<blocks1d(h.d.ncells, 128), 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers,
                                                                      c->fb.nmovers, moverCap, c->injCnt, c->err);
       RH_LAUNCHED(c);
@@ -1641,7 +1641,8 @@ int exoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>
 // shell (InjectorIonosphere::initialize, particle_injector.cpp:1059-1229)
 int ionoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int>& cells, std::vector<double>& rates) {
    const GridInfo& g = c->g;
-   if (J.iono_profile < RHGPU_IONO_COS_SZA_DAY_CONSTANT_NIGHT || J.iono_profile > RHGPU_IONO_POLAR_CAP)
+   const bool chapman = J.type == RHGPU_INJECT_CHAPMAN_IONOSPHERE;
+   if (!chapman && (J.iono_profile < RHGPU_IONO_COS_SZA_DAY_CONSTANT_NIGHT || J.iono_profile > RHGPU_IONO_POLAR_CAP))
       return fail(RHGPU_ERR_ARG, "set_injectors: unknown ionospheric emission profile");
    if (!(J.emission_radius > 0)) return fail(RHGPU_ERR_ARG, "set_injectors: ionosphere needs emission_radius > 0");
    const double rel = J.macroparticles_per_cell_relative >= 0 ? J.macroparticles_per_cell_relative : 1.0;
@@ -1652,8 +1653,20 @@ int ionoRates(rhgpu_ctx* c, const rhgpu_injector& J, InjHost& h, std::vector<int
    if (!(perDt > 0 && totalRate > 0)) { h.d.w = 0.0; return RHGPU_OK; }   // no emission
    double* shell = nullptr;
    RH_CUDA(cudaMalloc(&shell, sizeof(double) * g.N));
-   k_iono_shell<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, J.emission_radius, J.iono_profile, J.noon_factor,
-                                                            J.night_factor, J.seed, shell);
+   if (chapman) {
+      // scale heights with Mars' surface gravity: 150 K for the cells' shares,
+      // the source's temperature for the new particles (particle_injector.cpp:1306-1307, 1450-1451)
+      const double gs = RHGPU_GRAVITY * NP_MARS_MASS / (NP_MARS_RADIUS * NP_MARS_RADIUS);
+      h.d.R = J.emission_radius;
+      h.d.noon = J.noon_factor;
+      h.d.night = J.night_factor;
+      h.d.H = (1.380649e-23 * J.temperature) / (m * gs);
+      k_chapman_shell<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, J.emission_radius, J.noon_factor, J.night_factor,
+                                                                 (1.380649e-23 * 150) / (m * gs), J.seed, shell);
+   } else {
+      k_iono_shell<<<blocks1d(g.N, 128), 128, 0, c->stream>>>(g, J.emission_radius, J.iono_profile, J.noon_factor,
+                                                               J.night_factor, J.seed, shell);
+   }
    std::vector<double> inside(g.N);
    cudaError_t e = cudaGetLastError();
    if (e == cudaSuccess) e = cudaMemcpyAsync(inside.data(), shell, sizeof(double) * g.N, cudaMemcpyDeviceToHost, c->stream);
@@ -2260,7 +2273,8 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
                      if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
                   if (in) cells.push_back(i + g.nx * (j + g.ny * k));
                }
-      } else if (J.type == RHGPU_INJECT_EXOSPHERE || J.type == RHGPU_INJECT_IONOSPHERE) {
+      } else if (J.type == RHGPU_INJECT_EXOSPHERE || J.type == RHGPU_INJECT_IONOSPHERE ||
+                 J.type == RHGPU_INJECT_CHAPMAN_IONOSPHERE) {
          std::vector<double> rates;
          int rc = J.type == RHGPU_INJECT_EXOSPHERE ? exoRates(c, J, h, cells, rates) : ionoRates(c, J, h, cells, rates);
          if (rc) return rc;

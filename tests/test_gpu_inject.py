@@ -304,3 +304,44 @@ def test_ionosphere_source(lib, profile):
         assert 0.4 < day < 0.6
     else:
         assert day > 0.75
+
+
+def test_chapman_ionosphere_source(lib):
+    """InjectorChapmanIonosphere: about 400 new ions per step in a thin
+    Chapman layer around the emission radius (scale height k_B T / (m g_Mars),
+    here about 21 km for O+ at 150 K), moving outward, mostly on the dayside
+    (noon 1, night 0.1), weight total rate * dt / 400, and no device error
+    from the position redraws."""
+    cfg = exo_box()
+    grid, _ = cf.initial_state(cfg)
+    j = abi.Injector(species=0, type=abi.INJECT_CHAPMAN_IONOSPHERE, temperature=150.0, seed=13,
+                     emission_radius=650e3, noon_factor=1.0, night_factor=0.1, total_production_rate=1e24,
+                     macroparticles_per_cell_relative=1.0, upstream_macro_ratio=400.0)
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[100000])
+    try:
+        ctx.set_path(abi.PATH_FAST)
+        ctx.upload_array("faceB", grid["faceB"])
+        ctx.upload_array("cellB", grid["cellB"])
+        ctx.upload_array("nodeEta", grid["nodeEta"])
+        ctx.upload_cell_flags(grid["flags"])
+        ctx.upload_particles(0, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+        ctx.set_injectors([j])
+        ctx.step(1)
+        assert ctx.device_errors() == 0
+        cnt, p = ctx.download_particles(0)
+        ic = ctx.injection_counters()[0]
+    finally:
+        ctx.close()
+    cell = np.repeat(np.arange(cfg.ncells), cnt.astype(np.int64))
+    i, jj, k = cell % 24, (cell // 24) % 24, cell // 576
+    xg = -1.2e6 + i * 100e3 + p[:, 0]
+    yg = -1.2e6 + jj * 100e3 + p[:, 1]
+    zg = -1.2e6 + k * 100e3 + p[:, 2]
+    r = np.sqrt(xg ** 2 + yg ** 2 + zg ** 2)
+    assert 320 <= p.shape[0] <= 480, p.shape[0]
+    assert ic["macroparticles"] == p.shape[0]
+    assert np.all(np.abs(r - 650e3) < 250e3), (r.min(), r.max())
+    assert np.mean(np.abs(r - 650e3) < 120e3) > 0.9
+    assert np.all(p[:, 3] * xg + p[:, 4] * yg + p[:, 5] * zg >= 0)
+    assert math.isclose(p[0, 6], 1e24 * cfg.dt / 400.0, rel_tol=1e-12)
+    assert np.mean(xg > 0) > 0.8
