@@ -458,6 +458,20 @@ int rhgpu_log_write(rhgpu_ctx* ctx, int32_t main_log_diagnostics, int32_t* stop_
 /* Flushes and closes the log files (also done by rhgpu_destroy). */
 int rhgpu_log_close(rhgpu_ctx* ctx);
 
+/* Per-cell grid constraint counters (USE_GRID_CONSTRAINT_COUNTERS, off in the
+ * reference's default build; hybrid_propagator.cpp:64-116, 1382, 1440, 1513,
+ * 1579, boris.h:153-155, particle_accumulator.cpp:327): how many times each
+ * cell or node hit a limit since the counters were switched on or last
+ * zeroed. rhgpu_set_grid_counters(ctx, 1) allocates 40 bytes per cell and
+ * zeroes them (a later call zeroes them again, as the reference does after a
+ * save step); 0 frees them. rhgpu_download_grid_counters writes 5 planes of
+ * N doubles: cellMaxUe (cell and node Ue limits, as the reference counts the
+ * node one in the cell array), cellMaxVi (ion speed limit, the particle's
+ * cell before it moves), cellMinRhoQi, nodeMaxE, nodeMaxVw. Every path. */
+#define RHGPU_GRID_COUNTER_PLANES 5
+int rhgpu_set_grid_counters(rhgpu_ctx* ctx, int32_t enable);
+int rhgpu_download_grid_counters(rhgpu_ctx* ctx, double* out);
+
 /* Temporal averages of the output populations (WRITE_GRID_TEMPORAL_AVERAGES,
  * on in the reference's default build). group_of_species[s] is the output
  * population of species s (Hybrid::outputPopVarId: species with the same

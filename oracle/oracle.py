@@ -5,6 +5,8 @@ package).
   port()       the C restatement, oracle/librhoracle.so (prefix rho_)
   reference()  RHybrid's own hot-path sources built against oracle/shim,
                oracle/_ref/librhref.so (prefix rhref_); None if not built
+  reference_gc()  the same with USE_GRID_CONSTRAINT_COUNTERS compiled in,
+               oracle/_ref/librhref_gc.so; None if not built
 """
 import os
 import subprocess
@@ -14,10 +16,12 @@ from rhybrid_b200.abi import Library
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "librhoracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "librhref.so")
+REF_GC_PATH = os.path.join(HERE, "_ref", "librhref_gc.so")
 REF_DIR = os.environ.get("RH_REFERENCE_DIR", "/root/reference")
 
 _port = None
 _ref = None
+_ref_gc = None
 
 
 def build(reference: bool = True):
@@ -44,3 +48,12 @@ def reference():
             return None
         _ref = Library(REF_PATH, "rhref_")
     return _ref
+
+
+def reference_gc():
+    global _ref_gc
+    if _ref_gc is None:
+        if not os.path.exists(REF_GC_PATH):
+            return None
+        _ref_gc = Library(REF_GC_PATH, "rhref_")
+    return _ref_gc

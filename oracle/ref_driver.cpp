@@ -249,6 +249,13 @@ int rhref_create(const rhgpu_params* params,int32_t n_species,const rhgpu_specie
    Hybrid::dataInnerFlagParticleID = pg.addUserDataStatic<bool>(1);
    Hybrid::dataInnerFlagCellEpID   = pg.addUserDataStatic<bool>(1);
    Hybrid::dataCellAverageBID      = pg.addUserDataStatic<Real>(3);
+#ifdef USE_GRID_CONSTRAINT_COUNTERS
+   Hybrid::dataGridCounterCellMaxUeID    = pg.addUserDataStatic<Real>(1);
+   Hybrid::dataGridCounterCellMaxViID    = pg.addUserDataStatic<Real>(1);
+   Hybrid::dataGridCounterCellMinRhoQiID = pg.addUserDataStatic<Real>(1);
+   Hybrid::dataGridCounterNodeMaxEID     = pg.addUserDataStatic<Real>(1);
+   Hybrid::dataGridCounterNodeMaxVwID    = pg.addUserDataStatic<Real>(1);
+#endif
    c->arrayIDs[RHGPU_FACE_B] = Hybrid::dataFaceBID;
    c->arrayIDs[RHGPU_CELL_B] = Hybrid::dataCellBID;
    c->arrayIDs[RHGPU_CELL_UE] = Hybrid::dataCellUeID;
@@ -566,6 +573,35 @@ int rhref_output_averages(void* h,double* cellB,double* nOut,double* vOut) {
    Hybrid::gridTemporalAverageCounter = 0;
    return RHGPU_OK;
 }
+
+#ifdef USE_GRID_CONSTRAINT_COUNTERS
+/* the reference's per-cell constraint counters (built with
+ * USE_GRID_CONSTRAINT_COUNTERS): zeroed here, read in the planes order of
+ * rhgpu_download_grid_counters */
+int rhref_set_grid_counters(void* h,int32_t) {
+   RefCtx* c = (RefCtx*)h;
+   pargrid::ParGrid& pg = c->sc.pargrid;
+   const pargrid::DataID ids[5] = {Hybrid::dataGridCounterCellMaxUeID,Hybrid::dataGridCounterCellMaxViID,
+                                   Hybrid::dataGridCounterCellMinRhoQiID,Hybrid::dataGridCounterNodeMaxEID,
+                                   Hybrid::dataGridCounterNodeMaxVwID};
+   for (int q=0;q<5;++q) {
+      Real* a = pg.getUserDataStatic<Real>(ids[q]);
+      for (size_t n=0;n<pg.getNumberOfAllCells();++n) a[n] = 0.0;
+   }
+   return RHGPU_OK;
+}
+
+int rhref_download_grid_counters(void* h,double* out) {
+   RefCtx* c = (RefCtx*)h;
+   pargrid::ParGrid& pg = c->sc.pargrid;
+   const pargrid::DataID ids[5] = {Hybrid::dataGridCounterCellMaxUeID,Hybrid::dataGridCounterCellMaxViID,
+                                   Hybrid::dataGridCounterCellMinRhoQiID,Hybrid::dataGridCounterNodeMaxEID,
+                                   Hybrid::dataGridCounterNodeMaxVwID};
+   const size_t N = pg.getNumberOfAllCells();
+   for (int q=0;q<5;++q) std::memcpy(out + q*N,pg.getUserDataStatic<Real>(ids[q]),N*sizeof(Real));
+   return RHGPU_OK;
+}
+#endif
 
 int rhref_get_time(void* h,double* t,int64_t* ts) {
    RefCtx* c = (RefCtx*)h;

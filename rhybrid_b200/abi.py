@@ -59,6 +59,8 @@ DIAG_FIELD = ["N_cells", "sumBx", "sumBy", "sumBz", "sumB", "maxB", "sumDivB", "
               "sumCellEpx", "sumCellEpy", "sumCellEpz", "sumCellEp", "maxCellEp", "sumCellEp2",
               "sumNodeEx", "sumNodeEy", "sumNodeEz", "sumNodeE", "maxNodeE", "sumNodeE2",
               "sumCellE2", "maxUe", "sumCellRhoQi"]
+# rhgpu_download_grid_counters planes (the reference's gridCounter* arrays)
+GRID_COUNTERS = ["cellMaxUe", "cellMaxVi", "cellMinRhoQi", "nodeMaxE", "nodeMaxVw"]
 # the six scales that follow with n >= 8*n_species + 36 (LogDataField names)
 DIAG_SCALES = ["minInerLengthElectron", "maxInerLengthElectron", "minInerLengthProton", "maxInerLengthProton",
                "minTLarmor", "maxVAlfven"]
@@ -171,6 +173,8 @@ _OPTIONAL = {
     "log_write": [_P, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_int32],
     "log_close": [_P],
     "set_population_averages": [_P, C.c_int32, C.POINTER(C.c_int32)],
+    "set_grid_counters": [_P, C.c_int32],
+    "download_grid_counters": [_P, _D],
     "output_averages": [_P, _D, _D, _D],
 }
 _RESTYPES = {"last_error": C.c_char_p, "version": C.c_char_p, "stream": C.c_void_p, "philox4x32": None}
@@ -389,6 +393,16 @@ class Context:
         g = np.ascontiguousarray(group_of_species, dtype=np.int32)
         self._avg_groups = int(g.max()) + 1 if g.size and g.max() >= 0 else 0
         self.lib.call("set_population_averages", self.h, self._avg_groups, _ptr(g, C.c_int32))
+
+    def set_grid_counters(self, enable: bool = True):
+        """rhgpu_set_grid_counters: per-cell constraint counters on (zeroed) or off."""
+        self.lib.call("set_grid_counters", self.h, 1 if enable else 0)
+
+    def grid_counters(self) -> dict:
+        """rhgpu_download_grid_counters: the five per-cell counter planes by name."""
+        out = np.zeros(len(GRID_COUNTERS) * self.ncells, dtype=np.float64)
+        self.lib.call("download_grid_counters", self.h, _ptr(out, C.c_double))
+        return {k: out[i * self.ncells:(i + 1) * self.ncells] for i, k in enumerate(GRID_COUNTERS)}
 
     def output_averages(self, cellB: bool = True, populations: bool = True) -> dict:
         """rhgpu_output_averages: cellBAverage (N x 3) and per output population

@@ -177,7 +177,8 @@ constexpr int REC32 = 11;   // floats per deposit record: w8[8], v[3]
 
 // PER: the periodic axes (bit a = axis a), fixed at compile time; the host
 // launches the instantiation that matches the grid
-template <int PER>
+// GC: the variant that also counts the per-cell maxVi constraint (grid counters on)
+template <int PER, bool GC>
 __global__ void __launch_bounds__(FT, 4)
 k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp, F32Bufs fb, double* cntd,
                    unsigned long long* cntu, unsigned* err) {
@@ -291,6 +292,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
          }
       }
       if (clamp) atomicAdd(&cntu[CNT_SPECIES_MAXVI + s], 1ull);
+      if (GC) gridCountAtomic(f, GC_CELL_MAX_VI, g.N, cell, clamp);
 
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
       if (lane == 0) {
@@ -463,6 +465,7 @@ __global__ void k_f32_mover_deposit(GridInfo g, FastGeom fg, F32Set FS, F32Bufs 
 }
 
 // cell moments: four row partials (+ boundary partials) + fixed-point part, times (w q)_0 / dV
+template <bool GC>   // GC: also count the rho clamp per cell (grid counters on)
 __global__ void k_f32_gather(GridInfo g, Fields f, FastGeom fg, F32Bufs fb, double hiR, double loR, double hiJ,
                              double loJ, double scale, double minRho, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
@@ -507,6 +510,7 @@ __global__ void k_f32_gather(GridInfo g, Fields f, FastGeom fg, F32Bufs fb, doub
    bool clamp = false;
    if (rho < minRho) { rho = minRho; clamp = true; }
    countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   if (GC) gridCount(f, GC_CELL_MIN_RHOQI, N, n, clamp);
    f.cellRho[n] = rho;
    for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = v[1 + l] * scale;
 }

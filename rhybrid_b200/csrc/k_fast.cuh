@@ -439,7 +439,10 @@ __device__ __forceinline__ void segPartialsOut(const GridInfo& g, const FastGeom
    }
 }
 
-template <int PER, bool AVG>
+// EXTRA: the variant with the optional outputs (the removed in-segment deposits
+// listed for the population averages, the per-cell maxVi constraint counter);
+// the default instantiation carries neither
+template <int PER, bool EXTRA>
 __global__ void __launch_bounds__(FT, 4)
 k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
@@ -505,6 +508,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
          if (cj >= g.ny) cj -= g.ny;
          if (ck >= g.nz) ck -= g.nz;
          clamp = pushStaged(g, s_f, FS.sp[s], pp, ci, cj, ck, lc, ly, lz, st);
+         if (EXTRA) gridCountAtomic(f, GC_CELL_MAX_VI, g.N, cidx(g, ci, cj, ck), clamp);
          if (isnan(st[0]) || isnan(st[1]) || isnan(st[2])) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
          int ox, oy, oz;
          int bad = migrateAxis(st[0], ox, dx, g.dx_below);
@@ -548,7 +552,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
             if (!removed) {
                stay = inSeg;
                if (!inSeg) mflags |= MOVER_PLACE;
-            } else if (AVG && rec) {
+            } else if (EXTRA && rec && pp.avgList) {
                mflags |= MOVER_AVG;   // population averages: its in-segment deposit is listed
             }
             leave = mflags != 0;
@@ -724,6 +728,7 @@ __global__ void k_fast_fold_boundary(GridInfo g, FastGeom fg, FastBufs fb) {
 // destination moments: four row partials (boundary partials folded in) +
 // fixed-point part, then finalize. The touched word and the four row
 // partials (16-byte loads) are all requested before any sum.
+template <bool GC>   // GC: also count the rho clamp per cell (grid counters on)
 __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, double hiR, double loR, double hiJ,
                               double loJ, double minRho, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
@@ -755,6 +760,7 @@ __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, do
    bool clamp = false;
    if (rho < minRho) { rho = minRho; clamp = true; }
    countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   if (GC) gridCount(f, GC_CELL_MIN_RHOQI, N, n, clamp);
    f.cellRho[n] = rho;
    for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = v[1 + l] / g.dV;
 }

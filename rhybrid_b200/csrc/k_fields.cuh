@@ -31,7 +31,19 @@ struct Fields {
    double* nodeE;   double* nodeEta; double* cellAvgB;
    double* tmp3;    // scratch 3-vector (Gaussian smoothing)
    const uint8_t* flags;
+   double* gc;      // per-cell grid constraint counters, GC_PLANES planes of N, or null (off)
 };
+
+// per-cell grid constraint counters (USE_GRID_CONSTRAINT_COUNTERS): how often
+// each cell (node) hit a limit; the node Ue limit counts in the cell plane, as
+// the reference does (hybrid_propagator.cpp:1579)
+enum GridCounterPlane { GC_CELL_MAX_UE = 0, GC_CELL_MAX_VI, GC_CELL_MIN_RHOQI, GC_NODE_MAX_E, GC_NODE_MAX_VW, GC_PLANES };
+__device__ inline void gridCount(const Fields& f, int plane, long long N, long long n, bool hit) {
+   if (hit && f.gc) f.gc[plane * N + n] += 1.0;
+}
+__device__ inline void gridCountAtomic(const Fields& f, int plane, long long N, long long n, bool hit) {
+   if (hit && f.gc) atomicAdd(&f.gc[plane * N + n], 1.0);
+}
 
 struct FieldParams {
    int use_hall, use_ep, isothermal;
@@ -233,6 +245,7 @@ __global__ void k_node_j(GridInfo g, Fields f, FieldParams fp, unsigned long lon
    const bool lim = vw > fp.maxVw && fp.maxVw > 0.0;
    if (lim) d = vw / fp.maxVw;
    countIf(lim, &cnt[CNT_MAX_VW]);
+   gridCount(f, GC_NODE_MAX_VW, N, n, lim);
    const double a = 0.5 / (g.dx * RHGPU_PERMEABILITY * d);
    f.nodeJ[0 * N + n] = (edgeJx1 + edgeJx2) * a;
    f.nodeJ[1 * N + n] = (edgeJy1 + edgeJy2) * a;
@@ -275,6 +288,7 @@ __global__ void k_cell_j_ue(GridInfo g, Fields f, FieldParams fp, unsigned long 
       }
    }
    countIf(clamp, &cnt[CNT_MAX_CELL_UE]);
+   gridCount(f, GC_CELL_MAX_UE, N, n, clamp);
    for (int l = 0; l < 3; ++l) f.cellUe[l * N + n] = Ue[l];
 }
 
@@ -311,6 +325,7 @@ __global__ void k_node_ue_b_e(GridInfo g, Fields f, FieldParams fp, unsigned lon
    }
    countIf(rhoClamp, &cnt[CNT_MIN_NODE_RHO]);
    countIf(ueClamp, &cnt[CNT_MAX_NODE_UE]);
+   gridCount(f, GC_CELL_MAX_UE, N, n, ueClamp);
    for (int l = 0; l < 3; ++l) f.nodeUe[l * N + n] = Ue[l];
    // upwindNodeB
    double xU = -0.5, yU = 0, zU = 0;
@@ -362,6 +377,7 @@ __global__ void k_node_ue_b_e(GridInfo g, Fields f, FieldParams fp, unsigned lon
       }
    }
    countIf(eClamp, &cnt[CNT_MAX_E]);
+   gridCount(f, GC_NODE_MAX_E, N, n, eClamp);
    for (int l = 0; l < 3; ++l) f.nodeE[l * N + n] = E[l];
 }
 

@@ -34,6 +34,7 @@ struct SpeciesDev {
 struct PushParams {
    int useIFT, use_ep, use_gravity;
    double GMdt, maxVi2;
+   int avgList;   // fast path, EXTRA variant: list the removed in-segment deposits for the population averages
 };
 
 // device error word bits
@@ -100,6 +101,7 @@ __global__ void k_push(GridInfo g, Fields f, PStore P, SpeciesDev sp, PushParams
       }
    }
    countIf(clamp, &cnt[CNT_SPECIES_MAXVI + sidx]);
+   gridCountAtomic(f, GC_CELL_MAX_VI, g.N, c, clamp);
    x += g.dt * vx;
    y += g.dt * vy;
    z += g.dt * vz;
@@ -330,6 +332,7 @@ __global__ void k_deposit_gather(GridInfo g, Fields f, const double* S, int firs
       J0 /= g.dV; J1 /= g.dV; J2 /= g.dV;
    }
    countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   gridCount(f, GC_CELL_MIN_RHOQI, N, n, clamp);
    f.cellRho[n] = rho;
    f.cellJi[0 * N + n] = J0;
    f.cellJi[1 * N + n] = J1;
@@ -343,6 +346,7 @@ __global__ void k_deposit_finalize_only(GridInfo g, Fields f, double minRho, uns
    bool clamp = false;
    if (rho < minRho) { rho = minRho; clamp = true; }
    countIf(clamp, &cnt[CNT_MIN_CELL_RHO]);
+   gridCount(f, GC_CELL_MIN_RHOQI, N, n, clamp);
    f.cellRho[n] = rho;
    for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = 0.0 / g.dV;
 }

@@ -239,6 +239,7 @@ struct rhgpu_ctx {
    double* avgV = nullptr;              // avgGroups x 3N current sums (component planes)
    double* avgOut = nullptr;            // 4N output staging
    FastBufs avgFB = {};                 // fast path: row partials and fixed-point sums of one population
+   double* gridCnt = nullptr;           // GC_PLANES x N grid constraint counters (c->f.gc when on)
    // log files (rhgpu_log_*)
    LogFiles* logs = nullptr;
    int logInner = 0;
@@ -421,6 +422,7 @@ int pushAll(rhgpu_ctx* c) {
    pp.use_gravity = c->P.use_gravity;
    pp.GMdt = c->P.GMdt;
    pp.maxVi2 = c->P.max_ion_speed2;
+   pp.avgList = c->avgGroups > 0;
    for (int s = 0; s < c->ns; ++s) {
       PStore& P = c->ps[s];
       if (!P.start) continue;   // species without uploaded particles
@@ -1013,6 +1015,7 @@ int fastPush(rhgpu_ctx* c) {
    pp.use_gravity = c->P.use_gravity;
    pp.GMdt = c->P.GMdt;
    pp.maxVi2 = c->P.max_ion_speed2;
+   pp.avgList = c->avgGroups > 0;
    const long long N = c->g.N, NS = c->fg.NS;
    RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
@@ -1022,7 +1025,7 @@ int fastPush(rhgpu_ctx* c) {
       switch (perMask(c->g)) {
 #define RH_FAST_PD(M)                                                                                           \
    case M:                                                                                                        \
-      if (c->avgGroups)                                                                                           \
+      if (c->avgGroups || c->f.gc)                                                                                \
          k_fast_push_deposit<M, true><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, \
                                                                           c->cntU, c->err);                        \
       else                                                                                                        \
@@ -1087,8 +1090,12 @@ int fastGather(rhgpu_ctx* c) {
    RH_LAUNCHED(c);
    const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
    const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
-   k_fast_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->fb, hiR, loR, hiJ, loJ,
-                                                               c->P.min_ion_charge_density, c->cntU);
+   if (c->f.gc)
+      k_fast_gather<true><<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->fb, hiR, loR, hiJ, loJ,
+                                                                        c->P.min_ion_charge_density, c->cntU);
+   else
+      k_fast_gather<false><<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->fb, hiR, loR, hiJ, loJ,
+                                                                         c->P.min_ion_charge_density, c->cntU);
    RH_LAUNCHED(c);
    return RHGPU_OK;
 }
@@ -1394,8 +1401,12 @@ int f32Push(rhgpu_ctx* c) {
       switch (perMask(c->g)) {
 #define RH_F32_PD(M)                                                                                            \
    case M:                                                                                                        \
-      k_f32_push_deposit<M><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, FP, c->f32b, c->cntD, c->cntU, \
-                                                                c->err);                                         \
+      if (c->f.gc)                                                                                                \
+         k_f32_push_deposit<M, true><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, FP, c->f32b, c->cntD,  \
+                                                                         c->cntU, c->err);                         \
+      else                                                                                                        \
+         k_f32_push_deposit<M, false><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, FP, c->f32b,          \
+                                                                          c->cntD, c->cntU, c->err);               \
       break;
          RH_F32_PD(0) RH_F32_PD(1) RH_F32_PD(2) RH_F32_PD(3) RH_F32_PD(4) RH_F32_PD(5) RH_F32_PD(6) RH_F32_PD(7)
 #undef RH_F32_PD
@@ -1452,8 +1463,12 @@ int f32Gather(rhgpu_ctx* c) {
    const double hiR = std::ldexp(1.0, 64 - c->kR), loR = std::ldexp(1.0, -c->kR);
    const double hiJ = std::ldexp(1.0, 64 - c->kJ), loJ = std::ldexp(1.0, -c->kJ);
    const double scale = f32WqRef(c) / c->g.dV;
-   k_f32_gather<<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->f32b, hiR, loR, hiJ, loJ, scale,
-                                                              c->P.min_ion_charge_density, c->cntU);
+   if (c->f.gc)
+      k_f32_gather<true><<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->f32b, hiR, loR, hiJ, loJ,
+                                                                       scale, c->P.min_ion_charge_density, c->cntU);
+   else
+      k_f32_gather<false><<<cellGrid(c->g), cellBlock(), 0, c->stream>>>(c->g, c->f, c->fg, c->f32b, hiR, loR, hiJ,
+                                                                        loJ, scale, c->P.min_ion_charge_density, c->cntU);
    RH_LAUNCHED(c);
    return RHGPU_OK;
 }
@@ -1832,6 +1847,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
       f.nodeE = c->arr[RHGPU_NODE_E]; f.nodeEta = c->arr[RHGPU_NODE_ETA]; f.cellAvgB = c->arr[RHGPU_CELL_AVERAGE_B];
       f.tmp3 = c->tmp3;
       f.flags = c->flags;
+      f.gc = nullptr;   // grid constraint counters off until rhgpu_set_grid_counters
    }
    if (rc) {
       rhgpu_destroy(c);
@@ -1874,6 +1890,7 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    cudaFree(c->rhoMfix);
    cudaFree(c->avgN); cudaFree(c->avgV); cudaFree(c->avgOut);
    cudaFree(c->avgFB.RP); cudaFree(c->avgFB.RPB); cudaFree(c->avgFB.MMlo); cudaFree(c->avgFB.MMhi);
+   cudaFree(c->gridCnt);
    if (c->logs) { c->logs->close(); delete c->logs; c->logs = nullptr; }
    for (int s = 0; s < c->ns; ++s) {
       F32Host& h = c->f32[s];
@@ -2697,6 +2714,32 @@ int rhgpu_output_averages(rhgpu_ctx* c, double* cellB_average, double* n_average
       }
    }
    c->gridAvgCounter = 0;
+   return RHGPU_OK;
+}
+
+int rhgpu_set_grid_counters(rhgpu_ctx* c, int32_t enable) {
+   if (!c) return fail(RHGPU_ERR_ARG, "null context");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   const long long N = c->g.N;
+   if (!enable) {
+      cudaFree(c->gridCnt);
+      c->gridCnt = nullptr;
+      c->f.gc = nullptr;
+      return RHGPU_OK;
+   }
+   if (!c->gridCnt) RH_CUDA(cudaMalloc(&c->gridCnt, sizeof(double) * GC_PLANES * N));
+   RH_CUDA(cudaMemset(c->gridCnt, 0, sizeof(double) * GC_PLANES * N));
+   c->f.gc = c->gridCnt;
+   return RHGPU_OK;
+}
+
+int rhgpu_download_grid_counters(rhgpu_ctx* c, double* out) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "download_grid_counters: bad arguments");
+   if (!c->gridCnt) return fail(RHGPU_ERR_STATE, "download_grid_counters: grid counters are off (rhgpu_set_grid_counters)");
+   RH_CUDA(cudaSetDevice(c->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   RH_CUDA(cudaMemcpy(out, c->gridCnt, sizeof(double) * GC_PLANES * c->g.N, cudaMemcpyDeviceToHost));
    return RHGPU_OK;
 }
 

@@ -26,3 +26,12 @@ def ref_lib():
     if lib is None:
         pytest.skip("reference build oracle/_ref/librhref.so not present")
     return lib
+
+
+@pytest.fixture(scope="session")
+def ref_gc_lib():
+    from oracle import oracle
+    lib = oracle.reference_gc()
+    if lib is None:
+        pytest.skip("reference build oracle/_ref/librhref_gc.so not present")
+    return lib
