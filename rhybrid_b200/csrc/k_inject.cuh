@@ -41,7 +41,33 @@ struct InjDev {
    const double* rates;  // exosphere: expected macroparticles per step of each injection cell
    double R2exo;         // exosphere: squared exobase radius
    double R, noon, night, H;   // Chapman ionosphere: emission radius, day/night factors, scale height
+   const int* list;            // rate-based sources: the cells that draw particles this step (k_inject_select), or null
+   const int* listCount;
 };
+
+// rate-based sources (exosphere, ionospheres): draw every injection cell's
+// count as k_inject does and list the cells that get at least one particle,
+// so that k_inject runs over those only (most cells draw none)
+__global__ void k_inject_select(InjDev J, long long step, int* list, int* count) {
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   const int lane = threadIdx.x & 31;
+   bool any = false;
+   if (t < J.ncells) {
+      RngStream r;
+      r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
+      const double x = J.rates[t];
+      if (x > 0) {
+         int n = (int)floor(x);
+         if (r.uniform() < x - n) ++n;
+         any = n > 0;
+      }
+   }
+   const unsigned m = __ballot_sync(0xffffffffu, any);
+   int base = 0;
+   if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+   base = __shfl_sync(0xffffffffu, base, 0);
+   if (any) list[base + __popc(m & ((1u << lane) - 1u))] = t;
+}
 
 // neutral density of an exospheric profile at radius r (neutral_profiles.h:36-87):
 // 1 ChamberlainH, 2 ChamberlainT (a[i] = G M m / (k_B T0[i])), 3 Exponential, 4 PowerLaw
@@ -380,14 +406,30 @@ __device__ inline void writeMover(Mover32& M, const GridInfo& g, const FastGeom&
    M.lx = (ux - gd * SEG) | MOVER_PLACE;
 }
 
+// one injection cell t (or none, t < 0) per thread of a full warp
+template <class MV>
+__device__ void injectCell(const GridInfo& g, const FastGeom& fg, const InjDev& J, long long step, int t, MV* movers,
+                           unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err);
+
+// grid-stride over the injection cells (or over the listed ones), whole blocks per round
 template <class MV>
 __global__ void k_inject(GridInfo g, FastGeom fg, InjDev J, long long step, MV* movers,
                          unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err) {
-   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   const int total = J.list ? *J.listCount : J.ncells;
+   for (int b0 = blockIdx.x * blockDim.x; b0 < total; b0 += gridDim.x * blockDim.x) {
+      const int idx = b0 + threadIdx.x;
+      const int t = idx < total ? (J.list ? J.list[idx] : idx) : -1;
+      injectCell(g, fg, J, step, t, movers, nmovers, moverCap, injCnt, err);
+   }
+}
+
+template <class MV>
+__device__ void injectCell(const GridInfo& g, const FastGeom& fg, const InjDev& J, long long step, int t, MV* movers,
+                           unsigned long long* nmovers, long long moverCap, double* injCnt, unsigned* err) {
    const int lane = threadIdx.x & 31;
    RngStream r;
    int n = 0;
-   if (t < J.ncells) {
+   if (t >= 0) {
       r.init(J.seed, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)t);
       // probRound: floor(x) + 1 with probability x - floor(x)
       const double x = (J.type == INJ_EXOSPHERE || J.type == INJ_IONOSPHERE || J.type == INJ_CHAPMAN) ? J.rates[t]

@@ -150,7 +150,8 @@ struct SegHost {
 struct InjHost {
    InjDev d;
    int* cells = nullptr;     // device copy of d.cells
-   double* rates = nullptr;  // device copy of d.rates (exosphere)
+   double* rates = nullptr;  // device copy of d.rates (exosphere, ionospheres)
+   int* list = nullptr;      // rate-based sources: cells drawing particles this step, then their count
 };
 
 struct rhgpu_ctx {
@@ -949,8 +950,15 @@ int injectAll(rhgpu_ctx* c, MV* movers, long long moverCap) {
       RH_TIME(c, h.d.type == INJ_EXOSPHERE                                  ? "inject_exosphere"
                  : (h.d.type == INJ_IONOSPHERE || h.d.type == INJ_CHAPMAN) ? "inject_ionosphere"
                                                                             : "inject_inflow");
-      k_inject<MV><<<blocks1d(h.d.ncells, 128), 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers,
-                                                                     c->fb.nmovers, moverCap, c->injCnt, c->err);
+      unsigned grid = blocks1d(h.d.ncells, 128);
+      if (h.d.list) {   // most cells of a rate-based source draw nothing: list the others first
+         RH_CUDA(cudaMemsetAsync(h.list + h.d.ncells, 0, sizeof(int), c->stream));
+         k_inject_select<<<grid, 128, 0, c->stream>>>(h.d, c->timestep, h.list, h.list + h.d.ncells);
+         RH_LAUNCHED(c);
+         grid = std::min(grid, 2u * 148u);
+      }
+      k_inject<MV><<<grid, 128, 0, c->stream>>>(c->g, c->fg, h.d, c->timestep, movers, c->fb.nmovers, moverCap,
+                                                c->injCnt, c->err);
       RH_LAUNCHED(c);
    }
    return RHGPU_OK;
@@ -1879,7 +1887,7 @@ int rhgpu_destroy(rhgpu_ctx* c) {
    }
    cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
    cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
-   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); }
+   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); cudaFree(h.list); }
    cudaFree(c->injCnt);
    cudaFree(c->finc); cudaFree(c->fover); cudaFree(c->ffill); cudaFree(c->fmaxInc);
    cudaFree(c->mkey); cudaFree(c->mval); cudaFree(c->mbkt);
@@ -2225,7 +2233,7 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
    if (!c || n < 0 || (n > 0 && !inj)) return fail(RHGPU_ERR_ARG, "set_injectors: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); }
+   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); cudaFree(h.list); }
    c->inj.clear();
    c->injKeyMax = 0;
    if (!c->injCnt) {
@@ -2300,6 +2308,12 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
             RH_CUDA(cudaMemcpy(h.rates, rates.data(), sizeof(double) * rates.size(), cudaMemcpyHostToDevice));
          }
          h.d.rates = h.rates;
+         if (!cells.empty()) {
+            // the selected cells (ncells ints) and their count (one int after them)
+            RH_CUDA(cudaMalloc(&h.list, sizeof(int) * (cells.size() + 1)));
+            h.d.list = h.list;
+            h.d.listCount = h.list + cells.size();
+         }
       } else {
          return fail(RHGPU_ERR_ARG, "set_injectors: unknown type");
       }
