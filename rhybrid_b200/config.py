@@ -44,6 +44,8 @@ class Population:
     upstream: bool = True        # counts towards the upstream plasma parameters
     exosphere: Optional[dict] = None   # ExosphereInjector parameters of a planetary source
     ionosphere: Optional[dict] = None  # IonosphereInjector parameters of a planetary source
+    flow_walls: Sequence[str] = ()     # FlowInjector inflow walls ("+x", "-x", ...)
+    fill: bool = True                  # filled uniformly at the start (UniformInjector); sources fill the rest
 
     @property
     def q(self) -> float:
@@ -161,8 +163,9 @@ def upstream_macro_ratio(cfg: "Config") -> float:
 
 def source_injectors(cfg: "Config", seed: int = 1) -> list:
     """Every particle source of the configuration: the solar wind injectors,
-    one InjectorExosphere per population with exosphere parameters and one
-    InjectorIonosphere per population with ionosphere parameters."""
+    one InjectorExosphere per population with exosphere parameters, one
+    InjectorFlow per population with inflow walls and one InjectorIonosphere
+    (or InjectorChapmanIonosphere) per population with ionosphere parameters."""
     out = solar_wind_injectors(cfg, seed)
     ratio = upstream_macro_ratio(cfg)
     for s, p in enumerate(cfg.populations):
@@ -177,18 +180,31 @@ def source_injectors(cfg: "Config", seed: int = 1) -> list:
                          total_production_rate=e.get("total_production_rate", -1.0),
                          macroparticles_per_cell_relative=e.get("macroparticles_per_cell_relative", 1.0),
                          upstream_macro_ratio=ratio)
-        for k, (n0, H0) in enumerate(zip(e["n0"], e.get("H0", [0.0] * len(e["n0"])))):
+        j.gm_object = abi.GRAVITY * cfg.M_object
+        for k, n0 in enumerate(e["n0"]):
             j.n0[k] = n0
-            j.H0[k] = H0
+            for key in ("H0", "T0", "k0"):
+                vals = e.get(key) or []
+                if k < len(vals):
+                    getattr(j, key)[k] = vals[k]
         out.append(j)
+    for s, p in enumerate(cfg.populations):
+        if not p.flow_walls or p.ppc <= 0 or p.density <= 0:
+            continue
+        mask = sum(abi.WALLS[w] for w in p.flow_walls)
+        out.append(abi.Injector(species=s, type=abi.INJECT_FLOW, velocity=(C_DOUBLE3)(*[float(x) for x in p.velocity]),
+                                density=p.density, temperature=p.temperature, macroparticles_per_cell=p.ppc,
+                                inflow_walls=mask, reserved=0, seed=seed * 1000003 + 700 + s))
     for s, p in enumerate(cfg.populations):
         o = p.ionosphere
         if not o:
             continue
-        out.append(abi.Injector(species=s, type=abi.INJECT_IONOSPHERE, temperature=p.temperature,
+        chapman = o["profile"] == "Chapman"
+        out.append(abi.Injector(species=s, type=abi.INJECT_CHAPMAN_IONOSPHERE if chapman else abi.INJECT_IONOSPHERE,
+                                temperature=p.temperature,
                                 seed=seed * 1000003 + 500 + s, emission_radius=o["emission_radius"],
                                 noon_factor=o["noon"], night_factor=o["night"],
-                                iono_profile=abi.IONO_PROFILES[o["profile"]],
+                                iono_profile=0 if chapman else abi.IONO_PROFILES[o["profile"]],
                                 total_production_rate=o["total_production_rate"],
                                 macroparticles_per_cell_relative=o.get("macroparticles_per_cell_relative", 1.0),
                                 upstream_macro_ratio=ratio))
@@ -387,18 +403,23 @@ def _eta_at(cfg: Config, x, y, z):
 
 
 def _initial_B(cfg: Config, x, y, z):
-    """setInitialB (src/magnetic_field.h:257-260) for constantB,
-    translateDipoleB (:98-111) and laminarFlowAroundSphereBx (:44-54)."""
+    """setInitialB (src/magnetic_field.h:257-260) for constantB, constantBx,
+    translateDipoleB (:98-111), laminarFlowAroundSphereBx (:44-54) and their
+    sum translateDipoleBAndLaminarFlowAroundSphereBx (:182-185)."""
     Bx = np.zeros_like(x)
     By = np.zeros_like(x)
     Bz = np.zeros_like(x)
     prof = cfg.b_profile
+    known = ("constantB", "constantBx", "translateDipoleB", "laminarFlowAroundSphereBx",
+             "translateDipoleBAndLaminarFlowAroundSphereBx")
+    if prof not in known:
+        raise ValueError(f"IntrinsicB profile {prof} not supported")
     if prof in ("constantB", "constantBx"):
         Bx = Bx + cfg.imf[0]
         if prof == "constantB":
             By = By + cfg.imf[1]
             Bz = Bz + cfg.imf[2]
-    elif prof == "translateDipoleB":
+    if prof in ("translateDipoleB", "translateDipoleBAndLaminarFlowAroundSphereBx"):
         x1, y1, z1 = x - cfg.dipole_origin[0], y - cfg.dipole_origin[1], z - cfg.dipole_origin[2]
         r2 = x1 * x1 + y1 * y1 + z1 * z1
         rr = np.sqrt(r2)
@@ -410,8 +431,17 @@ def _initial_B(cfg: Config, x, y, z):
             Bx = np.where(ok, Bx + coeff * x1 * z1, Bx)
             By = np.where(ok, By + coeff * y1 * z1, By)
             Bz = np.where(ok, Bz + coeff * (z1 * z1 - r2 / 3.0), Bz)
-    else:
-        raise ValueError(f"IntrinsicB profile {prof} not supported")
+    if prof in ("laminarFlowAroundSphereBx", "translateDipoleBAndLaminarFlowAroundSphereBx"):
+        # IMF Bx draped around a sphere, nothing added inside it (magnetic_field.h:44-54)
+        r2 = x * x + y * y + z * z
+        R3 = cfg.laminar_R ** 3
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = np.sqrt(r2)
+            coeff = -1.5 * cfg.imf[0] * R3 * x / r ** 5
+            ok = r2 >= cfg.laminar_R ** 2
+            Bx = np.where(ok, Bx + (coeff * x + cfg.imf[0] * (1 + 0.5 * (R3 / r ** 3))), Bx)
+            By = np.where(ok, By + coeff * y, By)
+            Bz = np.where(ok, Bz + coeff * z, Bz)
     return Bx, By, Bz
 
 
@@ -490,6 +520,8 @@ def uniform_population(cfg: Config, s: int, seed: Optional[int] = None, cell_mas
     p = cfg.populations[s]
     seed = cfg.seed if seed is None else seed
     N = cfg.ncells
+    if not p.fill:
+        return np.zeros(N, dtype=np.uint32), np.zeros((0, 7), dtype=np.float64)
     dx = cfg.dx
     dV = dx * dx * dx
     ppc = p.ppc
