@@ -1,0 +1,103 @@
+"""Run a simulation from a RHybrid .cfg file on the GPU, as Corsair's time
+loop drives the reference (src/user.cpp:49-158): particle sources every step,
+the population and field logs every log_interval steps (before the step, with
+the max-B stop), and at every data save step the grid arrays and the temporal
+averages written as a NumPy archive (state_<timestep>.npz; this library does
+not write VLSV files).
+
+    python -m rhybrid_b200.run mars.cfg --steps 1000 --out run1
+
+The state is device-resident: particles cross PCIe only when uploaded at the
+start.
+"""
+import argparse
+import os
+import sys
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from . import cfg as C
+from . import config as cf
+
+ARRAYS = ["faceB", "cellB", "cellUe", "cellEp", "cellRhoQi", "cellJi", "nodeE", "nodeB", "nodeUe"]
+
+
+def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: str = "fast", device: int = 0,
+        lib: Optional[abi.Library] = None, quiet: bool = False) -> dict:
+    """Runs `steps` time steps (the file's maximum_timesteps by default).
+    Returns {"steps": steps run, "stopped": max-B stop, "saved": [npz files]}."""
+    config, rs = C.load(cfg_path)
+    os.makedirs(out_dir, exist_ok=True)
+    nsteps = rs.maximum_timesteps if steps is None else steps
+    lib = lib or abi.gpu_library()
+    grid, pops = cf.initial_state(config)
+    sources = cf.source_injectors(config, seed=config.seed)
+    if sources and not lib.has("set_injectors"):
+        raise RuntimeError(f"{lib.path}: this library has no particle sources")
+    cap = [p[1].shape[0] + p[1].shape[0] // 4 + (1 << 16) for p in pops]
+    ctx = abi.Context(lib, cf.params(config), cf.species(config), capacity=cap, device=device)
+    saved, stopped, done = [], False, 0
+    try:
+        if lib.has("set_path"):
+            ctx.set_path({"fast": abi.PATH_FAST, "fp32": abi.PATH_FP32, "exact": abi.PATH_EXACT}[path])
+        ctx.upload_array("faceB", grid["faceB"])
+        ctx.upload_array("cellB", grid["cellB"])
+        ctx.upload_array("nodeEta", grid["nodeEta"])
+        ctx.upload_cell_flags(grid["flags"])
+        for s, (cnt, p) in enumerate(pops):
+            ctx.upload_particles(s, cnt, p)
+        if sources:
+            ctx.set_injectors(sources)
+        averages = any(g >= 0 for g in rs.output_groups) and lib.has("set_population_averages")
+        if averages:
+            ctx.set_population_averages(rs.output_groups)
+        logging = rs.log_interval > 0 and lib.has("log_open")
+        if logging:
+            ctx.log_open(out_dir, rs.species_names, precision=rs.log_precision,
+                         include_inner_cells=rs.include_inner_cells_in_field_log,
+                         max_B_stop_run=rs.max_magnetic_field_stop_run)
+        for _ in range(nsteps):
+            ts = ctx.time()[1]
+            if logging and ts % rs.log_interval == 0:
+                main = rs.main_log_diagnostics_interval > 0 and ts % rs.main_log_diagnostics_interval == 0
+                stopped, msg = ctx.log_write(main_log_diagnostics=main)
+                if msg and not quiet:
+                    sys.stdout.write(msg)
+                if stopped:
+                    break
+            ctx.step(1)
+            done += 1
+            ts = ctx.time()[1]
+            if rs.data_save_interval > 0 and ts % rs.data_save_interval == 0:
+                out = {name: ctx.download_array(name) for name in ARRAYS}
+                out["time"] = np.array(ctx.time()[0])
+                out["timestep"] = np.array(ts)
+                if averages:
+                    for k, v in ctx.output_averages().items():
+                        out[k] = v
+                fn = os.path.join(out_dir, f"state_{ts:07d}.npz")
+                np.savez(fn, **out)
+                saved.append(fn)
+        if logging:
+            ctx.log_close()
+    finally:
+        ctx.close()
+    return {"steps": done, "stopped": stopped, "saved": saved}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("cfg")
+    ap.add_argument("--steps", type=int, default=None, help="time steps (default: the file's maximum_timesteps)")
+    ap.add_argument("--out", default=".", help="directory of the log files and saved states")
+    ap.add_argument("--path", default="fast", choices=["fast", "fp32", "exact"])
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    r = run(a.cfg, a.steps, a.out, a.path, a.device)
+    print(f"{r['steps']} steps{' (stopped: max |B|)' if r['stopped'] else ''}, {len(r['saved'])} states saved")
+
+
+if __name__ == "__main__":
+    main()
