@@ -50,7 +50,9 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
             ctx.upload_particles(s, cnt, p)
         if sources:
             ctx.set_injectors(sources)
-        averages = any(g >= 0 for g in rs.output_groups) and lib.has("set_population_averages")
+        # the population averages run on the fast and exact paths (the FP32 form has none)
+        averages = (any(g >= 0 for g in rs.output_groups) and lib.has("set_population_averages")
+                    and not (path == "fp32" and lib.has("set_path")))
         if averages:
             ctx.set_population_averages(rs.output_groups)
         logging = rs.log_interval > 0 and lib.has("log_open")
