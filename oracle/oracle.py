@@ -57,3 +57,36 @@ def reference_gc():
             return None
         _ref_gc = Library(REF_GC_PATH, "rhref_")
     return _ref_gc
+
+
+def reference_write_data(ctx, params, group_names=()):
+    """Runs the reference's own output operator (UserDataOP::writeData,
+    src/operator_userdata.cpp:55-312) on a context of a reference library and
+    returns the arrays it hands to its VLSV writer, in write order, as
+    {name: array}: (N,) for vector size 1, else (N, vector size)."""
+    import ctypes as C
+
+    import numpy as np
+
+    lib = ctx.lib
+    dll = lib.dll
+    f = dll.rhref_write_data
+    f.argtypes, f.restype = [C.c_void_p, C.c_char_p, C.c_char_p], C.c_int32
+    if f(ctx.h, " ".join(params).encode(), " ".join(group_names).encode()) != 0:
+        raise RuntimeError(lib.last_error())
+    dll.rhref_data_count.argtypes, dll.rhref_data_count.restype = [C.c_void_p], C.c_int32
+    info = dll.rhref_data_info
+    info.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    get = dll.rhref_data_get
+    get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]
+    out = {}
+    for i in range(dll.rhref_data_count(ctx.h)):
+        name = C.create_string_buffer(256)
+        n, v = C.c_int64(), C.c_int64()
+        if info(ctx.h, i, name, 256, C.byref(n), C.byref(v)) != 0:
+            raise RuntimeError(lib.last_error())
+        a = np.empty(n.value * v.value, dtype=np.float64)
+        if get(ctx.h, i, a.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+            raise RuntimeError(lib.last_error())
+        out[name.value.decode()] = a if v.value == 1 else a.reshape(n.value, v.value)
+    return out

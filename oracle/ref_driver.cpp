@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -38,6 +39,7 @@
 #include "particle_propagator_boris_buneman.h"
 #include "particle_boundary_cond_hybrid.h"
 #include "diagnostics.h"
+#include "operator_userdata.h"
 
 #include <fstream>
 
@@ -602,6 +604,59 @@ int rhref_download_grid_counters(void* h,double* out) {
    return RHGPU_OK;
 }
 #endif
+
+/* The reference's own output operator, UserDataOP::writeData
+ * (src/operator_userdata.cpp:55-312), run on the current state; the VLSV
+ * stub of the shim keeps the arrays it writes. `params`: space-separated
+ * output parameter names (Hybrid.output_parameters, user.cpp:2302-2343);
+ * `group_names`: space-separated names of the output populations
+ * (outputPopVarStr) of rhref_set_population_averages. The arrays are read
+ * back with rhref_data_count / rhref_data_info / rhref_data_get. */
+int rhref_write_data(void* h,const char* params,const char* group_names) {
+   RefCtx* c = (RefCtx*)h;
+   Hybrid::outputCellParams.clear();
+   std::istringstream ps(params ? params : "");
+   for (std::string w; ps >> w; ) Hybrid::outputCellParams[w] = true;
+   Hybrid::outputPopVarStr.clear();
+   std::istringstream gs(group_names ? group_names : "");
+   for (std::string w; gs >> w; ) Hybrid::outputPopVarStr.push_back(w);
+   if (Hybrid::outputPopVarStr.size() != Hybrid::N_outputPopVars)
+      return fail(RHGPU_ERR_ARG,"rhref_write_data: one name per output population");
+   std::vector<ParticleListBase*> lists;
+   for (int s=0;s<c->nspecies;++s) {
+      pargrid::DataWrapper<PARTICLE> w = c->sc.pargrid.getUserDataDynamic<PARTICLE>(c->particleIDs[s]);
+      for (size_t b=0;b<c->counts[s].size();++b) w.resize((pargrid::CellID)b,c->counts[s][b]);
+      lists.push_back(&c->plists[s]);
+   }
+   UserDataOP op;
+   op.initialize(c->cr,c->sim,c->sc);
+   c->sc.vlsv.arrays.clear();
+   c->sc.vlsv.capture = true;
+   const bool ok = op.writeData("SpatialGrid",lists);
+   c->sc.vlsv.capture = false;
+   return ok ? RHGPU_OK : fail(RHGPU_ERR_STATE,"rhref_write_data: writeData failed");
+}
+
+int rhref_data_count(void* h) { return (int)((RefCtx*)h)->sc.vlsv.arrays.size(); }
+
+int rhref_data_info(void* h,int32_t i,char* name,int32_t cap,int64_t* arraySize,int64_t* vectorSize) {
+   RefCtx* c = (RefCtx*)h;
+   if (i < 0 || (size_t)i >= c->sc.vlsv.arrays.size() || cap < 1) return fail(RHGPU_ERR_ARG,"rhref_data_info: bad index");
+   const VlsvArray& a = c->sc.vlsv.arrays[i];
+   auto it = a.attribs.find("name");
+   std::snprintf(name,cap,"%s",it == a.attribs.end() ? "" : it->second.c_str());
+   *arraySize = (int64_t)a.arraySize;
+   *vectorSize = (int64_t)a.vectorSize;
+   return RHGPU_OK;
+}
+
+int rhref_data_get(void* h,int32_t i,double* out) {
+   RefCtx* c = (RefCtx*)h;
+   if (i < 0 || (size_t)i >= c->sc.vlsv.arrays.size()) return fail(RHGPU_ERR_ARG,"rhref_data_get: bad index");
+   const VlsvArray& a = c->sc.vlsv.arrays[i];
+   std::memcpy(out,a.data.data(),a.data.size()*sizeof(double));
+   return RHGPU_OK;
+}
 
 int rhref_get_time(void* h,double* t,int64_t* ts) {
    RefCtx* c = (RefCtx*)h;

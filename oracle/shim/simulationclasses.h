@@ -195,11 +195,31 @@ namespace pargrid {
    };
 }
 
-/* VLSV writer stand-in: the reduced-state writer in diagnostics.h compiles
- * against it; the oracle never writes VLSV files (every call fails). */
+/* VLSV writer stand-in. open() fails, so the oracle never writes a VLSV
+ * file (the reduced-state writer in diagnostics.h stops there). While
+ * `capture` is on, writeArray() keeps each array in memory instead, as
+ * doubles, with its tag, attributes and sizes: the arrays UserDataOP::writeData
+ * hands to the writer, read back by the oracle driver. */
+struct VlsvArray {
+   std::string tag;
+   std::map<std::string,std::string> attribs;
+   uint64_t arraySize = 0,vectorSize = 0;
+   std::vector<double> data;
+};
 struct VlsvWriterStub {
+   bool capture = false;
+   std::vector<VlsvArray> arrays;
    bool open(const std::string&,MPI_Comm,int) { return false; }
-   template<class T> bool writeArray(const std::string&,const std::map<std::string,std::string>&,uint64_t,uint64_t,const T*) { return false; }
+   template<class T> bool writeArray(const std::string& tag,const std::map<std::string,std::string>& attribs,
+                                     uint64_t arraySize,uint64_t vectorSize,const T* d) {
+      if (!capture) return false;
+      VlsvArray a;
+      a.tag = tag; a.attribs = attribs; a.arraySize = arraySize; a.vectorSize = vectorSize;
+      a.data.resize(arraySize*vectorSize);
+      for (size_t i=0;i<a.data.size();++i) a.data[i] = static_cast<double>(d[i]);
+      arrays.push_back(a);
+      return true;
+   }
    bool close() { return false; }
    uint64_t getBytesWritten() const { return 0; }
 };

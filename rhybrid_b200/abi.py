@@ -258,6 +258,8 @@ class Context:
     def __init__(self, lib: Library, params: Params, species: list, capacity=None, device: int = 0):
         self.lib = lib
         self.params = params
+        self.species = list(species)
+        self.cell_flags = None           # the flags last given to upload_cell_flags
         self.nspecies = len(species)
         self.ncells = params.nx * params.ny * params.nz
         arr = (Species * len(species))(*species)
@@ -301,6 +303,7 @@ class Context:
         f = np.ascontiguousarray(flags, dtype=np.uint8).reshape(-1)
         assert f.size == self.ncells
         self.lib.call("upload_cell_flags", self.h, _ptr(f, C.c_uint8))
+        self.cell_flags = f.copy()
 
     # particles -------------------------------------------------------
     def upload_particles(self, s: int, counts: np.ndarray, particles: np.ndarray):

@@ -28,6 +28,9 @@ class RunSettings:
     max_magnetic_field_stop_run: float = float("inf")
     output_parameters: List[str] = field(default_factory=list)
     output_groups: List[int] = field(default_factory=list)   # output population of each species (-1: none)
+    output_group_names: List[str] = field(default_factory=list)   # output_str of each output population
+    save_particles: bool = False            # Hybrid.save_particles (user.cpp:396)
+    save_particles_nstride: int = 10        # Hybrid.save_particles_Nstride (user.cpp:397)
     species_names: List[str] = field(default_factory=list)
     extra: Dict[str, Dict[str, List[str]]] = field(default_factory=dict)
 
@@ -225,7 +228,8 @@ def load_text(text: str) -> Tuple[cf.Config, RunSettings]:
         main_log_diagnostics_interval=hy.int("main_log_diagnostics_interval", 100),
         max_magnetic_field_stop_run=con.float("max_magnetic_field_stop_run", float("inf")),
         output_parameters=(hy.str("output_parameters", "") or "").split(), output_groups=groups,
-        species_names=names,
+        output_group_names=seen, save_particles=hy.bool("save_particles"),
+        save_particles_nstride=hy.int("save_particles_Nstride", 10), species_names=names,
         extra={k: v for k, v in P.items() if k in ("Restart", "LoadBalance", "DetectorParticle",
                                                     "DetectorBulkParameter", "DataOperatorExcludes")})
     return cfgobj, rs

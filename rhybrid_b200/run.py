@@ -1,9 +1,11 @@
 """Run a simulation from a RHybrid .cfg file on the GPU, as Corsair's time
 loop drives the reference (src/user.cpp:49-158): particle sources every step,
 the population and field logs every log_interval steps (before the step, with
-the max-B stop), and at every data save step the grid arrays and the temporal
-averages written as a NumPy archive (state_<timestep>.npz; this library does
-not write VLSV files).
+the max-B stop), and at every data save step the variables of
+Hybrid.output_parameters (the arrays the reference's output operator hands to
+its VLSV writer, output.cell_variables) and, with Hybrid.save_particles, the
+particle points (output.particle_points), written as a NumPy archive
+(state_<timestep>.npz; this library does not write the VLSV container).
 
     python -m rhybrid_b200.run mars.cfg --steps 1000 --out run1
 
@@ -20,8 +22,7 @@ import numpy as np
 from . import abi
 from . import cfg as C
 from . import config as cf
-
-ARRAYS = ["faceB", "cellB", "cellUe", "cellEp", "cellRhoQi", "cellJi", "nodeE", "nodeB", "nodeUe"]
+from . import output as O
 
 
 def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: str = "fast", device: int = 0,
@@ -73,12 +74,11 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
             done += 1
             ts = ctx.time()[1]
             if rs.data_save_interval > 0 and ts % rs.data_save_interval == 0:
-                out = {name: ctx.download_array(name) for name in ARRAYS}
+                out = O.cell_variables(ctx, rs.output_parameters, rs.output_groups, rs.output_group_names)
+                if rs.save_particles:
+                    out.update(O.particle_points(ctx, rs.species_names, rs.save_particles_nstride))
                 out["time"] = np.array(ctx.time()[0])
                 out["timestep"] = np.array(ts)
-                if averages:
-                    for k, v in ctx.output_averages().items():
-                        out[k] = v
                 fn = os.path.join(out_dir, f"state_{ts:07d}.npz")
                 np.savez(fn, **out)
                 saved.append(fn)

@@ -22,4 +22,6 @@ def test_run_loop(tmp_path, ref_lib):
     assert len(field) == 3   # time steps 0, 2, 4
     st = np.load(r["saved"][1])
     assert int(st["timestep"]) == 6 and st["cellB"].shape == (24 * 16 * 12, 3)
-    assert st["n_ave"].shape == (1, 24 * 16 * 12) and np.any(st["n_ave"] > 0)
+    # Hybrid.output_parameters = cellB n_ave v_ave: ne comes with the averages (operator_userdata.cpp:104-116)
+    assert sorted(st.files) == sorted(["cellB", "ne", "n_H+_ave", "v_H+_ave", "time", "timestep"])
+    assert st["n_H+_ave"].shape == (24 * 16 * 12,) and np.any(st["n_H+_ave"] > 0)
