@@ -11,6 +11,7 @@ import pytest
 from rhybrid_b200 import abi
 from rhybrid_b200 import cfg as C
 from rhybrid_b200 import config as cf
+from rhybrid_b200 import output as O
 
 TEXT = """
 gridbuilder = LogicallyCartesian
@@ -116,6 +117,7 @@ def test_cfg_reader():
     assert iono.ionosphere["profile"] == "ionoCosSzaDayConstantNight" and iono.ionosphere["night"] == 0.2
     assert rs.log_interval == 5 and rs.log_precision == 8 and rs.max_magnetic_field_stop_run == 500e-9
     assert rs.output_groups == [0, 1, 1] and rs.output_parameters == ["cellB", "n_ave", "v_ave"]
+    assert rs.output_group_names == ["H+", "O+"] and not rs.save_particles and rs.save_particles_nstride == 10
     src = cf.source_injectors(c)
     assert [(j.species, j.type) for j in src] == [(0, abi.INJECT_SOLARWIND), (1, abi.INJECT_EXOSPHERE),
                                                  (2, abi.INJECT_IONOSPHERE)]
@@ -165,5 +167,8 @@ def test_reference_examples_load():
             continue
         cf.source_injectors(c)
         assert len(rs.output_groups) == len(c.populations)
+        assert len(rs.output_group_names) == max(rs.output_groups, default=-1) + 1
+        # every output parameter an example asks for is one the output step knows
+        assert set(rs.output_parameters) <= set(O.PARAMETERS), (f, set(rs.output_parameters) - set(O.PARAMETERS))
         loaded += 1
     assert loaded >= 10
