@@ -204,5 +204,5 @@ def particle_points(ctx, species_names: Sequence[str], nstride: int = 10) -> Dic
         keep = sel[cell]
         out[f"ParticlePointMesh_{name}"] = q[keep, 0:3] + corner[cell[keep]]
         out[f"v_{name}"] = q[keep, 3:6].copy()
-        out[f"CellID_{name}"] = cell[keep].astype(np.float64)
+        out[f"CellID_{name}"] = cell[keep].astype(np.uint64)   # pargrid::CellID, unsigned
     return out
