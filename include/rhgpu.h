@@ -382,6 +382,14 @@ typedef struct rhgpu_injector {
    int32_t  reserved2;
 } rhgpu_injector;
 int rhgpu_set_injectors(rhgpu_ctx* ctx, int32_t n, const rhgpu_injector* injectors);
+/* expected macroparticles per step in every cell (N doubles, linear cell
+ * order) of source `injector` (index into the last rhgpu_set_injectors
+ * array). Filled for the rate-based sources: exosphere (cellExosphere,
+ * particle_injector.cpp:1780-1792) and ionospheres (cellIonosphere,
+ * :1205-1226). Zeros for the other types. These are the arrays the
+ * reference's output step writes as prod_rate_exo<k> / prod_rate_iono<k>
+ * (operator_userdata.cpp:123-154). Host memory only; no device work. */
+int rhgpu_source_rates(rhgpu_ctx* ctx, int32_t injector, double* out);
 /* injected per species: weight, macroparticles, weight * v^2
  * (logCounterParticleInject*, particle_injector.cpp:569-571); 3 * n_species doubles */
 int rhgpu_get_injection_counters(rhgpu_ctx* ctx, double* out, int32_t n);

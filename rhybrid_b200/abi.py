@@ -167,6 +167,7 @@ _OPTIONAL = {
     "set_threads": [_P, C.c_int32],
     "set_injectors": [_P, C.c_int32, C.c_void_p],
     "get_injection_counters": [_P, _D, C.c_int32],
+    "source_rates": [_P, C.c_int32, _D],
     "philox4x32": [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
     "neutral_density": [C.c_void_p, C.c_double, C.c_int64, _D, _D, C.c_int32],
     "log_open": [_P, C.c_void_p],
@@ -260,6 +261,7 @@ class Context:
         self.params = params
         self.species = list(species)
         self.cell_flags = None           # the flags last given to upload_cell_flags
+        self.injectors = []              # the sources last given to set_injectors
         self.nspecies = len(species)
         self.ncells = params.nx * params.ny * params.nz
         arr = (Species * len(species))(*species)
@@ -456,6 +458,14 @@ class Context:
         """rhgpu_set_injectors: the particle sources (a list of Injector; empty: none)."""
         arr = (Injector * max(len(injectors), 1))(*injectors)
         self.lib.call("set_injectors", self.h, len(injectors), C.cast(arr, C.c_void_p))
+        self.injectors = list(injectors)
+
+    def source_rates(self, injector: int) -> np.ndarray:
+        """rhgpu_source_rates: expected macroparticles per step in every cell
+        of a rate-based source (exosphere, ionospheres); zeros otherwise."""
+        out = np.zeros(self.ncells, dtype=np.float64)
+        self.lib.call("source_rates", self.h, injector, _ptr(out, C.c_double))
+        return out
 
     def injection_counters(self) -> list:
         """rhgpu_get_injection_counters: per species the injected weight,

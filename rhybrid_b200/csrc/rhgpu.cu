@@ -9,6 +9,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_reduce.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -152,6 +153,10 @@ struct InjHost {
    int* cells = nullptr;     // device copy of d.cells
    double* rates = nullptr;  // device copy of d.rates (exosphere, ionospheres)
    int* list = nullptr;      // rate-based sources: cells drawing particles this step, then their count
+   // rate-based sources, host copy: the cells with a positive expected
+   // number of macroparticles per step, and that number
+   std::vector<int> rateCells;
+   std::vector<double> rateValues;
 };
 
 struct rhgpu_ctx {
@@ -2307,6 +2312,8 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
             RH_CUDA(cudaMalloc(&h.rates, sizeof(double) * rates.size()));
             RH_CUDA(cudaMemcpy(h.rates, rates.data(), sizeof(double) * rates.size(), cudaMemcpyHostToDevice));
          }
+         h.rateCells = cells;
+         h.rateValues = rates;
          h.d.rates = h.rates;
          if (!cells.empty()) {
             // the selected cells (ncells ints) and their count (one int after them)
@@ -2328,6 +2335,15 @@ int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
       c->inj.push_back(h);
    }
    c->injKeyMax = keyBase;
+   return RHGPU_OK;
+}
+
+int rhgpu_source_rates(rhgpu_ctx* c, int32_t injector, double* out) {
+   if (!c || !out) return fail(RHGPU_ERR_ARG, "source_rates: bad arguments");
+   if (injector < 0 || injector >= (int)c->inj.size()) return fail(RHGPU_ERR_ARG, "source_rates: no such source");
+   const InjHost& h = c->inj[injector];
+   std::fill(out, out + c->g.N, 0.0);
+   for (size_t q = 0; q < h.rateCells.size(); ++q) out[h.rateCells[q]] = h.rateValues[q];
    return RHGPU_OK;
 }
 

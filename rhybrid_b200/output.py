@@ -21,9 +21,9 @@ cell: output populations in species order, particles in list order), so the
 values are the reference's bit for bit on the same state. This library keeps
 the arrays as a NumPy archive (run.py); it does not write the VLSV container.
 
-Not written: prod_rate_iono / prod_rate_exo (the per-cell production rates are
-kept inside the particle sources), cellB0 (USE_B_CONSTANT is off in the
-reference's default build). faceJ is written as zeros: in the default build
+prod_rate_iono<k> / prod_rate_exo<k> are the rate-based sources' expected
+macroparticles per step in each cell (rhgpu_source_rates). Not written: cellB0
+(USE_B_CONSTANT is off in the reference's default build). faceJ is written as zeros: in the default build
 (USE_EDGE_J) the reference computes J on edges and faceJ keeps its initial
 zeros (user.cpp:1855).
 """
@@ -110,6 +110,35 @@ def bulk_parameters(ctx, species: Sequence[int], particles: Optional[dict] = Non
     return dens / (dx * dx * dx), T, U
 
 
+def production_rates(ctx, iono: bool = True, exo: bool = True) -> Dict[str, np.ndarray]:
+    """prod_rate_iono<k> and prod_rate_exo<k> (operator_userdata.cpp:123-154)
+    from the context's sources, in species order. The reference numbers its
+    ionosphere slots with one counter per injector class
+    (particle_injector.cpp:1112-1114 for IonosphereInjector, :1415-1417 for
+    ChapmanIonosphereInjector), and both classes write cellIonosphere. So the
+    k-th source of each class fills slot k, and the later one in species
+    order is the one that stays. There is one slot per ionosphere population;
+    a slot no source writes is zeros."""
+    srcs = list(getattr(ctx, "injectors", []))
+    out: Dict[str, np.ndarray] = {}
+    if iono:
+        kinds = (abi.INJECT_IONOSPHERE, abi.INJECT_CHAPMAN_IONOSPHERE)
+        members = [q for q, j in enumerate(srcs) if j.type in kinds]
+        slots = [np.zeros(ctx.ncells) for _ in members]
+        seen = {t: 0 for t in kinds}
+        for q in sorted(members, key=lambda q: srcs[q].species):
+            t = srcs[q].type
+            slots[seen[t]] = ctx.source_rates(q)
+            seen[t] += 1
+        for k, a in enumerate(slots):
+            out[f"prod_rate_iono{k}"] = a
+    if exo:
+        members = sorted((q for q, j in enumerate(srcs) if j.type == abi.INJECT_EXOSPHERE), key=lambda q: srcs[q].species)
+        for k, q in enumerate(members):
+            out[f"prod_rate_exo{k}"] = ctx.source_rates(q)
+    return out
+
+
 def cell_variables(ctx, params: Iterable[str], groups: Sequence[int] = (), group_names: Sequence[str] = (),
                    grid_counters: bool = False) -> Dict[str, np.ndarray]:
     """The cell variables UserDataOP::writeData writes for the output
@@ -125,8 +154,6 @@ def cell_variables(ctx, params: Iterable[str], groups: Sequence[int] = (), group
     # configuration step does (user.cpp:2405-2410)
     for name in sorted(want - set(PARAMETERS)):
         warnings.warn(f"parameter requested for output does not exist: {name}")
-    for name in sorted(want & {"prod_rate_iono", "prod_rate_exo"}):
-        warnings.warn(f"{name}: the production rates are not written by this library")
     N = ctx.ncells
     out: Dict[str, np.ndarray] = {}
     for name, dim in GRID_ARRAYS:
@@ -145,6 +172,8 @@ def cell_variables(ctx, params: Iterable[str], groups: Sequence[int] = (), group
             out[name] = ((ctx.cell_flags & bit) != 0).astype(np.float64)
     if "n_ave" in want or "v_ave" in want:
         out["ne"] = ctx.download_array("cellRhoQi") / abi.CHARGE_ELEMENTARY
+    if "prod_rate_iono" in want or "prod_rate_exo" in want:
+        out.update(production_rates(ctx, "prod_rate_iono" in want, "prod_rate_exo" in want))
     ngroups = max(groups, default=-1) + 1
     if len(group_names) != ngroups or (len(groups) and len(groups) != ctx.nspecies):
         raise ValueError(f"{len(groups)} groups and {len(group_names)} names for {ctx.nspecies} species")

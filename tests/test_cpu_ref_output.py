@@ -115,3 +115,30 @@ def test_unknown_parameter_and_group_checks(ref_lib):
         assert list(out) == ["cellB"]
         with pytest.raises(ValueError):
             O.cell_variables(ctx, ["n"], GROUPS, ["H+"])
+
+
+class _SourcesOnly:
+    """Stand-in context with sources only: source_rates(q) is q+1 everywhere."""
+    ncells = 5
+
+    def __init__(self, injectors):
+        self.injectors = injectors
+
+    def source_rates(self, q):
+        return np.full(self.ncells, q + 1.0)
+
+
+def test_production_rate_slots():
+    """prod_rate_iono<k>: one counter per ionosphere injector class, both
+    writing cellIonosphere (particle_injector.cpp:1112-1114, :1415-1417), the
+    later source in species order staying; prod_rate_exo<k> in species order."""
+    J = lambda t, s: abi.Injector(type=t, species=s)   # noqa: E731
+    srcs = [J(abi.INJECT_IONOSPHERE, 1), J(abi.INJECT_CHAPMAN_IONOSPHERE, 2), J(abi.INJECT_IONOSPHERE, 3),
+            J(abi.INJECT_EXOSPHERE, 4), J(abi.INJECT_EXOSPHERE, 0), J(abi.INJECT_SOLARWIND, 5)]
+    out = O.production_rates(_SourcesOnly(srcs))
+    assert list(out) == ["prod_rate_iono0", "prod_rate_iono1", "prod_rate_iono2", "prod_rate_exo0", "prod_rate_exo1"]
+    assert out["prod_rate_iono0"][0] == 2.0     # the Chapman source (species 2) after species 1
+    assert out["prod_rate_iono1"][0] == 3.0     # the second IonosphereInjector (species 3)
+    assert not out["prod_rate_iono2"].any()     # no third writer
+    assert out["prod_rate_exo0"][0] == 5.0 and out["prod_rate_exo1"][0] == 4.0
+    assert O.production_rates(_SourcesOnly([])) == {}
