@@ -1,5 +1,6 @@
 """The .cfg-driven time loop (rhybrid_b200/run.py) on the GPU with solar wind,
-exosphere and ionosphere sources, log files and the temporal averages."""
+exosphere and ionosphere sources, log files, and saved states holding the
+temporal averages and the sources' production rates."""
 import numpy as np
 import pytest
 
