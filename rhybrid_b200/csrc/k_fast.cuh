@@ -18,6 +18,9 @@
 //   k_fast_push_deposit  one block per segment, one thread per particle:
 //                        push + migration + CIC weights of the new position +
 //                        boundary removal (particle_boundary_cond_hybrid.h:112-185).
+//                        The field stencil and each chunk of particles are
+//                        copied to shared memory with per-thread cp.async, the
+//                        next chunk while the current one is processed.
 //                        Particles that stay in the segment are written to the
 //                        next buffer in order; their deposit records go to
 //                        shared memory counting-sorted by target dual cell
@@ -439,47 +442,156 @@ __device__ __forceinline__ void segPartialsOut(const GridInfo& g, const FastGeom
    }
 }
 
+// ---- per-thread asynchronous global -> shared copies (cp.async) ----------------------------------
+// bytes = 0 copies nothing and writes zeros (the source address is not read)
+__device__ __forceinline__ void cpAsync8(void* sdst, const void* gsrc, int bytes) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// one species' arrays offset to the block's segment: current x..w (0-6), next
+// x..w (7-13), current lx (14), next lx (15)
+constexpr int SEG_PTRS = 16;
+
+// shared memory of k_fast_push_deposit (dynamic: more than the 48 KB static limit)
+struct PushDepositShared {
+   double rec[FT * REC];                  // deposit records of a chunk; at the end acc[SEG][32]
+   double pf[7][FT];                      // the next chunk's particles, one plane per component
+   SegFields f;                           // field stencil of the segment
+   void* ptr[FAST_MAX_SPECIES][SEG_PTRS];
+   StencilRow rows[SF_MAX_ROWS];
+   alignas(8) unsigned char wd[SEG][FW];  // records per (dual cell, warp)
+   int rank[FT];                          // stayers of the chunk before each chunk position
+   int wcnt[FW];                          // stayers per warp
+   int prefix[FAST_MAX_SPECIES + 1];      // first particle of each species in the segment
+   int stay[FAST_MAX_SPECIES];            // stayers of each species so far
+};
+constexpr size_t PUSH_DEPOSIT_SMEM = sizeof(PushDepositShared);
+
+// the segment's first chunk and the field stencil requested with cp.async: the
+// stencil rows (see stageSegRows) with zeros outside a non-periodic box, the
+// particles of chunk positions tid into pf
+template <int PER>
+__device__ __forceinline__ void pdStage(const GridInfo& g, const Fields& f, bool useEp, PushDepositShared& sh,
+                                        int total, int ns, int& lxNext) {
+   const int tid = threadIdx.x;
+   if (tid < total) {
+      int s = 0;
+      while (s + 1 < ns && tid >= sh.prefix[s + 1]) ++s;
+      const int p = tid - sh.prefix[s];
+#pragma unroll
+      for (int a = 0; a < 7; ++a) cpAsync8(&sh.pf[a][tid], (const double*)sh.ptr[s][a] + p, 8);
+      lxNext = ((const unsigned char*)sh.ptr[s][14])[p];
+   }
+   const int nrows = SF_ROWS_B + SF_ROWS_C * (useEp ? 2 : 1);
+   double* const base = (double*)&sh.f;
+   for (int e = tid; e < nrows * SF_ROW_W; e += FT) {
+      const int ri = e / SF_ROW_W, c = e - ri * SF_ROW_W;
+      const StencilRow r = sh.rows[ri];
+      if (c >= r.len) continue;
+      int x = r.xs + c;
+      if (PER & 1) { if (x < 0) x += g.nx; else if (x >= g.nx) x -= g.nx; }
+      const bool ok = r.src != nullptr && x >= 0 && x < g.nx;
+      cpAsync8(base + r.dst + c, ok ? r.src + x : f.faceB, ok ? 8 : 0);
+   }
+   cpAsyncCommit();
+}
+
+// cicWeightsLocal with the dual cell's lower centre (i - 1 + 0.5) dx = -dx/2 or
+// +dx/2 selected (both exact), the same weights bit for bit
+__device__ __forceinline__ void cicWeightsHalf(double x, double y, double z, double wq, const GridInfo& g, double hdx,
+                                               double w8[8]) {
+   const double x0 = x < hdx ? -hdx : hdx, y0 = y < hdx ? -hdx : hdx, z0 = z < hdx ? -hdx : hdx;
+   const double w_x = divDx(x - x0, g), w_y = divDx(y - y0, g), w_z = divDx(z - z0, g);
+   w8[0] = (1 - w_x) * (1 - w_y) * (1 - w_z) * wq;
+   w8[1] = w_x * (1 - w_y) * (1 - w_z) * wq;
+   w8[2] = (1 - w_x) * w_y * (1 - w_z) * wq;
+   w8[3] = w_x * w_y * (1 - w_z) * wq;
+   w8[4] = (1 - w_x) * (1 - w_y) * w_z * wq;
+   w8[5] = w_x * (1 - w_y) * w_z * wq;
+   w8[6] = (1 - w_x) * w_y * w_z * wq;
+   w8[7] = w_x * w_y * w_z * wq;
+}
+
 // EXTRA: the variant with the optional outputs (the removed in-segment deposits
 // listed for the population averages, the per-cell maxVi constraint counter);
-// the default instantiation carries neither
+// the default instantiation carries neither.
+//
+// One block per segment, one thread per particle, chunks of FT particles in
+// storage order (species after species). The particles of chunk k+1 are copied
+// to shared memory (cp.async, each thread its own position) while chunk k is
+// processed; per chunk two barriers order the records and the stayers. A
+// particle leaving the segment reserves its mover slot before the second
+// barrier and is written after the deposit sums, so the reservation's round
+// trip overlaps the chunk's remaining work.
 template <int PER, bool EXTRA>
 __global__ void __launch_bounds__(FT, 4)
 k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushParams pp, FastBufs fb,
                     double* cntd, unsigned long long* cntu, unsigned* err) {
+   extern __shared__ __align__(16) unsigned char pdSmem[];
+   PushDepositShared& sh = *reinterpret_cast<PushDepositShared*>(pdSmem);
    GridInfo g = gIn;
    g.per[0] = PER & 1;
    g.per[1] = (PER >> 1) & 1;
    g.per[2] = (PER >> 2) & 1;
-   __shared__ double s_rec[FT * REC];             // deposit records of a chunk; at the end acc[SEG][32]
-   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell)
-   __shared__ int s_wcnt[FW];                     // stayers per warp
-   __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
-   __shared__ int s_stay[FAST_MAX_SPECIES];
-   __shared__ unsigned s_bs[FW];                  // stayer ballot of each warp
-   __shared__ SegFields s_f;
-   __shared__ StencilRow s_rows[SF_MAX_ROWS];
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
-   const long long S = blockIdx.x;
-   const long long row = S / fg.nseg;
-   const int gseg = (int)(S % fg.nseg);
-   const int uy = (int)(row % fg.nd[1]), uz = (int)(row / fg.nd[1]);
-   const int ndx = fg.nd[0];
-   const int u0 = gseg * SEG, u1 = min(u0 + SEG, ndx);
+   const int S = (int)blockIdx.x;
+   const int nseg = fg.nseg;
+   const int row = S / nseg, gseg = S - row * nseg;
+   const int uy = row % fg.nd[1], uz = row / fg.nd[1];
+   const int u0 = gseg * SEG, u1 = min(u0 + SEG, fg.nd[0]);
    const int ns = FS.ns;
-   const double dx = g.dx;
-   if (tid == 0) {
-      int a = 0;
-      for (int s = 0; s < ns; ++s) {
-         s_prefix[s] = a;
-         a += FS.st[s].cur.cnt[S];
+   const double dx = g.dx, hdx = 0.5 * dx;
+   const int xs0 = dualB(u0, g.per[0]), ys0 = dualB(uy, g.per[1]), zs0 = dualB(uz, g.per[2]);
+
+   // ---- set-up: species prefix (warp 0), segment pointers (warps 1-4), stencil rows (warps 5-6)
+   if (warp == 0) {
+      const int cnt = lane < ns ? FS.st[lane].cur.cnt[S] : 0;
+      int x = cnt;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+         const int y = __shfl_up_sync(0xffffffffu, x, o);
+         if (lane >= o) x += y;
       }
-      s_prefix[ns] = a;
+      if (lane <= ns) sh.prefix[lane] = x - cnt;
+      if (lane < FAST_MAX_SPECIES) sh.stay[lane] = 0;
+   } else if (tid < 32 + SEG_PTRS * ns) {
+      const int q = tid - 32, s = q / SEG_PTRS, k = q - s * SEG_PTRS;
+      const SegSpecies& SS = FS.st[s];
+      const long long b = SS.base[S];
+      void* v;
+      if (k < 7) v = SS.cur.a[k] + b;
+      else if (k < 14) v = SS.nxt.a[k - 7] + b;
+      else if (k == 14) v = SS.cur.lx + b;
+      else v = SS.nxt.lx + b;
+      sh.ptr[s][k] = v;
+   } else if (tid >= 160 && tid < 160 + SF_ROWS_B + SF_ROWS_C * (pp.use_ep ? 2 : 1)) {
+      const int r = tid - 160;
+      int len, dxs, l, dy, dz;
+      const double* arr;
+      double* dst = stencilRow(sh.f, f, r, len, dxs, arr, l, dy, dz);
+      int y = ys0 + dy, z = zs0 + dz;
+      if (PER & 2) { if (y < 0) y += g.ny; else if (y >= g.ny) y -= g.ny; }
+      if (PER & 4) { if (z < 0) z += g.nz; else if (z >= g.nz) z -= g.nz; }
+      StencilRow sr;
+      sr.src = (y >= 0 && y < g.ny && z >= 0 && z < g.nz)
+                   ? arr + (long long)l * g.N + (long long)g.nx * ((long long)y + (long long)g.ny * z)
+                   : nullptr;
+      sr.dst = (int)(dst - (double*)&sh.f);
+      sr.xs = xs0 + dxs;
+      sr.len = len;
+      sh.rows[r] = sr;
    }
-   if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
-   stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), dualB(uy, g.per[1]), dualB(uz, g.per[2]), s_f, s_rows);
    __syncthreads();
-   const int total = s_prefix[ns];
+   const int total = sh.prefix[ns];
+   int lxNext = 0;
+   pdStage<PER>(g, f, pp.use_ep, sh, total, ns, lxNext);
+   cpAsyncWaitAll();
+   __syncthreads();
+
    const int myDual = tid >> 3, myCorner = tid & 7;   // this thread's sums: (dual cell, corner) x 4 moments
    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 
@@ -488,26 +600,27 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       const bool active = i < total;
       int s = 0;
       if (active)
-         while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
+         while (s + 1 < ns && i >= sh.prefix[s + 1]) ++s;
       double st[7];
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0;
       int vx = 0, vy = 0, vz = 0;
-      long long p = 0;
+      int p = 0;
+      const int lu = lxNext;
+      if (c0 > 0) cpAsyncWaitAll();   // this thread's copies of the chunk
       if (active) {
-         const SegSpecies& SS = FS.st[s];
-         p = i - s_prefix[s];
-         const long long slot = SS.base[S] + p;
-         for (int a = 0; a < 7; ++a) st[a] = SS.cur.a[a][slot];
-         const int lu = SS.cur.lx[slot];
-         const int lc = lu + 1 - halfS(st[0], dx), ly = 1 - halfS(st[1], dx), lz = 1 - halfS(st[2], dx);
-         int ci = dualB(u0 + lu, g.per[0]) + 1 - halfS(st[0], dx);
-         int cj = dualB(uy, g.per[1]) + ly;
-         int ck = dualB(uz, g.per[2]) + lz;
+         p = i - sh.prefix[s];
+#pragma unroll
+         for (int a = 0; a < 7; ++a) st[a] = sh.pf[a][tid];
+         const int hx = halfS(st[0], dx), hy = halfS(st[1], dx), hz = halfS(st[2], dx);
+         const int lc = lu + 1 - hx, ly = 1 - hy, lz = 1 - hz;
+         int ci = xs0 + lu + 1 - hx;
+         int cj = ys0 + ly;
+         int ck = zs0 + lz;
          if (ci >= g.nx) ci -= g.nx;   // periodic axes: dual cell 0 holds the upper half of the last cell
          if (cj >= g.ny) cj -= g.ny;
          if (ck >= g.nz) ck -= g.nz;
-         clamp = pushStaged(g, s_f, FS.sp[s], pp, ci, cj, ck, lc, ly, lz, st);
+         clamp = pushStaged(g, sh.f, FS.sp[s], pp, ci, cj, ck, lc, ly, lz, st);
          if (EXTRA) gridCountAtomic(f, GC_CELL_MAX_VI, g.N, cidx(g, ci, cj, ck), clamp);
          if (isnan(st[0]) || isnan(st[1]) || isnan(st[2])) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
          int ox, oy, oz;
@@ -516,8 +629,8 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
          bad |= migrateAxis(st[2], oz, dx, g.dx_below);
          int ti = ci + ox, tj = cj + oy, tk = ck + oz;
          const bool inside = wrapc(ti, g.nx, g.per[0]) && wrapc(tj, g.ny, g.per[1]) && wrapc(tk, g.nz, g.per[2]);
-         const double ke = st[6] * (sq(st[3]) + sq(st[4]) + sq(st[5]));
          if (bad || !inside) {
+            const double ke = st[6] * (sq(st[3]) + sq(st[4]) + sq(st[5]));
             atomicAdd(&cntd[4 * s + 0], st[6]);
             atomicAdd(&cntd[4 * s + 1], ke);
          } else {
@@ -533,20 +646,24 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
                }
             }
             // boundary conditions of the step
-            const long long cn = cidx(g, ti, tj, tk);
             bool removed = false;
             if (!allNb(g, ti, tj, tk)) {
                removed = true;
+               const double ke = st[6] * (sq(st[3]) + sq(st[4]) + sq(st[5]));
                atomicAdd(&cntd[4 * s + 0], st[6]);
                atomicAdd(&cntd[4 * s + 1], ke);
-            } else if (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
-               const double xp = blockOrigin(g.x_min, ti, dx) + st[0];
-               const double yp = blockOrigin(g.y_min, tj, dx) + st[1];
-               const double zp = blockOrigin(g.z_min, tk, dx) + st[2];
-               if (sq(xp) + sq(yp) + sq(zp) < FS.sp[s].R2obs) {
-                  removed = true;
-                  atomicAdd(&cntd[4 * s + 2], st[6]);
-                  atomicAdd(&cntd[4 * s + 3], ke);
+            } else {
+               const unsigned cn = (unsigned)ti + (unsigned)g.nx * ((unsigned)tj + (unsigned)g.ny * (unsigned)tk);
+               if (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
+                  const double xp = blockOrigin(g.x_min, ti, dx) + st[0];
+                  const double yp = blockOrigin(g.y_min, tj, dx) + st[1];
+                  const double zp = blockOrigin(g.z_min, tk, dx) + st[2];
+                  if (sq(xp) + sq(yp) + sq(zp) < FS.sp[s].R2obs) {
+                     removed = true;
+                     const double ke = st[6] * (sq(st[3]) + sq(st[4]) + sq(st[5]));
+                     atomicAdd(&cntd[4 * s + 2], st[6]);
+                     atomicAdd(&cntd[4 * s + 3], ke);
+                  }
                }
             }
             if (!removed) {
@@ -563,31 +680,41 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
       // ---- order of the chunk's stayers and records --------------------------------------
       // warp-local first: stayer/record ballots and the records per (warp, dual cell)
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
-      if (lane == 0) {
-         s_wcnt[warp] = __popc(bs);
-         s_bs[warp] = bs;
-      }
-      s_wd[warp][lane] = 0;
+      if (lane == 0) sh.wcnt[warp] = __popc(bs);
+      sh.wd[lane][warp] = 0;
       __syncwarp();
       const int rd = rec ? vx - u0 : 0;
       int rrank = 0;
       if (rec) {
          const unsigned mm = __match_any_sync(br, rd);
          rrank = __popc(mm & below);
-         if (rrank == 0) s_wd[warp][rd] = __popc(mm);
+         if (rrank == 0) sh.wd[rd][warp] = (unsigned char)__popc(mm);
       }
       __syncthreads();
+      // every shared-memory read of this chunk's particles is done: request the next chunk's
+      {
+         const int i2 = i + FT;
+         if (i2 < total) {
+            int s2 = s;
+            while (s2 + 1 < ns && i2 >= sh.prefix[s2 + 1]) ++s2;
+            const int p2 = i2 - sh.prefix[s2];
+#pragma unroll
+            for (int a = 0; a < 7; ++a) cpAsync8(&sh.pf[a][tid], (const double*)sh.ptr[s2][a] + p2, 8);
+            lxNext = ((const unsigned char*)sh.ptr[s2][14])[p2];
+         }
+         cpAsyncCommit();
+      }
       // every warp, per dual cell (lane): the first sorted record of the dual cell
       // (bin) and of this warp's records for it (off)
-      int binD, offD, total;
+      int binD, offD, nrec;
       {
-         int t = 0, before = 0;
-#pragma unroll
-         for (int w = 0; w < FW; ++w) {
-            const int cw = s_wd[w][lane];
-            t += cw;
-            if (w < warp) before += cw;
-         }
+         // the eight per-warp counts of dual cell `lane` are bytes (each at most 32):
+         // byte sums by one multiply per 32-bit half
+         const uint2 c8 = *reinterpret_cast<const uint2*>(&sh.wd[lane][0]);
+         const int t = (int)(((c8.x * 0x01010101u) >> 24) + ((c8.y * 0x01010101u) >> 24));
+         const unsigned mlo = warp >= 4 ? 0xffffffffu : (1u << (8 * warp)) - 1u;
+         const unsigned mhi = warp <= 4 ? 0u : (1u << (8 * (warp - 4))) - 1u;
+         const int before = (int)((((c8.x & mlo) * 0x01010101u) >> 24) + (((c8.y & mhi) * 0x01010101u) >> 24));
          int x = t;
          for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -595,81 +722,83 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
          }
          binD = x - t;
          offD = binD + before;
-         total = __shfl_sync(0xffffffffu, x, 31);
+         nrec = __shfl_sync(0xffffffffu, x, 31);
       }
       const int recPos = __shfl_sync(0xffffffffu, offD, rd) + rrank;
       const int sumLo = __shfl_sync(0xffffffffu, binD, myDual);
       const int sumHiN = __shfl_sync(0xffffffffu, binD, (myDual + 1) & 31);
-      const int sumHi = myDual == SEG - 1 ? total : sumHiN;
-      // stayers of the warps before this one
-      const int stayBefore = (int)__reduce_add_sync(0xffffffffu, (unsigned)(lane < warp ? s_wcnt[lane] : 0));
-      {
-         const unsigned lm = __ballot_sync(0xffffffffu, leave);
-         if (lm) {
-            const int leader = __ffs(lm) - 1;
-            unsigned long long b0 = 0;
-            if (lane == leader) b0 = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
-            b0 = __shfl_sync(0xffffffffu, b0, leader);
-            if (leave) {
-               const unsigned long long m = b0 + __popc(lm & below);
-               if ((long long)m < fb.moverCap) {
-                  Mover& M = fb.movers[m];
-                  for (int a = 0; a < 7; ++a) M.s[a] = st[a];
-                  M.key = ((unsigned long long)S << 32) | (unsigned long long)p;
-                  const int gd = vx / SEG;
-                  M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * fg.nseg + gd;
-                  M.species = s;
-                  M.lx = (vx - gd * SEG) | mflags;
-               } else {
-                  raiseError(err, RHGPU_DEVERR_CAPACITY);
-               }
-            }
-         }
-      }
-      long long slot = 0;   // next-buffer slot of a stayer (stored after the barrier)
-      if (stay) {
-         const int stayIdx = stayBefore + __popc(bs & below);
-         // stayers of the chunk before the first particle of this thread's species
-         // (zero unless the species starts inside this chunk)
-         const int p0 = s_prefix[s] - c0;
-         const int firstIdx = p0 > 0 ? stayersIn(s_bs, 0, p0) : 0;
-         slot = FS.st[s].base[S] + s_stay[s] + (stayIdx - firstIdx);
-      }
-      // stayers of species tid in this chunk
-      const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
+      const int sumHi = myDual == SEG - 1 ? nrec : sumHiN;
+      // stayers of the chunk before this position (and in all), and this species' count so far
+      const int wc = lane < FW ? sh.wcnt[lane] : 0;
+      const int myRank = (int)__reduce_add_sync(0xffffffffu, (unsigned)(lane < warp ? wc : 0)) + __popc(bs & below);
+      const int chunkStay = (int)__reduce_add_sync(0xffffffffu, (unsigned)wc);
+      sh.rank[tid] = myRank;
+      const int stayBase = stay ? sh.stay[s] : 0;
+      // mover slots reserved now, written after the sums
+      const unsigned lm = __ballot_sync(0xffffffffu, leave);
+      const int leader = lm ? __ffs(lm) - 1 : 0;
+      unsigned long long mb = 0;
+      if (lm && lane == leader) mb = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
       if (rec) {
          double w8[8];
-         cicWeightsLocal(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, w8);
-         double* r = s_rec + recPos * REC;
+         cicWeightsHalf(st[0], st[1], st[2], st[6] * FS.sp[s].q, g, hdx, w8);
+         double* r = sh.rec + recPos * REC;
+#pragma unroll
          for (int o = 0; o < 8; ++o) r[o] = w8[o];
          r[8] = st[3]; r[9] = st[4]; r[10] = st[5];
       }
       __syncthreads();
-      // running stayer count of each species (all reads of s_stay for this chunk are done)
-      if (tid < ns) s_stay[tid] += stayAdd;
       if (stay) {
-         const SegSpecies& SS = FS.st[s];
-         for (int a = 0; a < 7; ++a) SS.nxt.a[a][slot] = st[a];
-         SS.nxt.lx[slot] = (unsigned char)(vx - u0);
+         const int p0 = sh.prefix[s] - c0;   // chunk position of the species' first particle
+         const int q = stayBase + myRank - (p0 > 0 ? sh.rank[p0] : 0);
+         double* const* nx = (double* const*)&sh.ptr[s][7];
+#pragma unroll
+         for (int a = 0; a < 7; ++a) nx[a][q] = st[a];
+         ((unsigned char*)sh.ptr[s][15])[q] = (unsigned char)(vx - u0);
+      }
+      // running stayer count of each species
+      if (tid < ns) {
+         const int lo = min(max(sh.prefix[tid] - c0, 0), FT), hi = min(max(sh.prefix[tid + 1] - c0, 0), FT);
+         const int rlo = lo < FT ? sh.rank[lo] : chunkStay, rhi = hi < FT ? sh.rank[hi] : chunkStay;
+         sh.stay[tid] += rhi - rlo;
       }
       // ---- sums of this thread's (dual cell, corner), records in list order ----------------
 #pragma unroll 2
       for (int r = sumLo; r < sumHi; ++r) {
-         const double* rr = s_rec + r * REC;
+         const double* rr = sh.rec + r * REC;
          const double w = rr[myCorner];
          a0 += w;
          a1 += w * rr[8];
          a2 += w * rr[9];
          a3 += w * rr[10];
       }
-      // no barrier here: the next chunk's first barrier orders these reads before
-      // its record writes
+      // ---- particles that left the segment -----------------------------------------------
+      if (lm) {
+         mb = __shfl_sync(0xffffffffu, mb, leader);
+         if (leave) {
+            const unsigned long long m = mb + __popc(lm & below);
+            if ((long long)m < fb.moverCap) {
+               Mover& M = fb.movers[m];
+#pragma unroll
+               for (int a = 0; a < 7; ++a) M.s[a] = st[a];
+               M.key = ((unsigned long long)S << 32) | (unsigned long long)p;
+               const int gd = vx / SEG;
+               M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * nseg + gd;
+               M.species = s;
+               M.lx = (vx - gd * SEG) | mflags;
+            } else {
+               raiseError(err, RHGPU_DEVERR_CAPACITY);
+            }
+         }
+      }
+      // no barrier here: the next chunk's first barrier orders the reads of rec,
+      // rank and stay before their next writes
    }
 
    // ---- outputs: stayer counts, row partials, segment-boundary partial ---------------------
    __syncthreads();
-   if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
-   segPartialsOut(g, fg, fb, s_rec, row, gseg, u0, u1, a0, a1, a2, a3);
+   if (tid < ns) FS.st[tid].nxt.cnt[S] = sh.stay[tid];
+   segPartialsOut(g, fg, fb, sh.rec, row, gseg, u0, u1, a0, a1, a2, a3);
 }
 
 // CIC contributions of the particles that left their segment, as exact fixed-point sums (MM)

@@ -1019,6 +1019,24 @@ int fastAverages(rhgpu_ctx* c, long long nm) {
    return RHGPU_OK;
 }
 
+// k_fast_push_deposit uses more than the 48 KB of static shared memory: its
+// limit is raised once per instantiation (and device) before the launch
+template <int PER, bool EXTRA>
+int launchPushDeposit(rhgpu_ctx* c, const FastSpecies& FS, const PushParams& pp) {
+   static bool raised[64] = {};
+   int dev = 0;
+   RH_CUDA(cudaGetDevice(&dev));
+   if (dev < 0 || dev >= 64) return fail(RHGPU_ERR_CUDA, "device index out of range");
+   if (!raised[dev]) {
+      RH_CUDA(cudaFuncSetAttribute(k_fast_push_deposit<PER, EXTRA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)PUSH_DEPOSIT_SMEM));
+      raised[dev] = true;
+   }
+   k_fast_push_deposit<PER, EXTRA><<<(unsigned)c->fg.NS, FT, PUSH_DEPOSIT_SMEM, c->stream>>>(
+       c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, c->cntU, c->err);
+   return RHGPU_OK;
+}
+
 int fastPush(rhgpu_ctx* c) {
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
@@ -1035,19 +1053,19 @@ int fastPush(rhgpu_ctx* c) {
    {
       RH_TIME(c, "fast_push_deposit");
       const FastSpecies FS = fastSpecies(c);
+      int rc = RHGPU_OK;
       switch (perMask(c->g)) {
 #define RH_FAST_PD(M)                                                                                           \
    case M:                                                                                                        \
       if (c->avgGroups || c->f.gc)                                                                                \
-         k_fast_push_deposit<M, true><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb, c->cntD, \
-                                                                          c->cntU, c->err);                        \
+         rc = launchPushDeposit<M, true>(c, FS, pp);                                                              \
       else                                                                                                        \
-         k_fast_push_deposit<M, false><<<(unsigned)NS, FT, 0, c->stream>>>(c->g, c->f, c->fg, FS, pp, c->fb,         \
-                                                                           c->cntD, c->cntU, c->err);              \
+         rc = launchPushDeposit<M, false>(c, FS, pp);                                                             \
       break;
          RH_FAST_PD(0) RH_FAST_PD(1) RH_FAST_PD(2) RH_FAST_PD(3) RH_FAST_PD(4) RH_FAST_PD(5) RH_FAST_PD(6) RH_FAST_PD(7)
 #undef RH_FAST_PD
       }
+      if (rc) return rc;
       RH_LAUNCHED(c);
    }
    {
