@@ -331,7 +331,8 @@ int rhgpu_dn_num_pairs(rhgpu_dn* dn, int32_t* n_out, int32_t* newest);
  *     new particles); cells with fewer than 10 of 1000 Monte Carlo points
  *     kept emit nothing.
  * Solar wind and flow: weight n dx^3 / ppc. Thermal speed sqrt(k_B T / m)
- * with the species' mass. n == 0 removes all sources. */
+ * with the species' mass. n == 0 removes all sources. The call replaces the
+ * whole source set; if any source is rejected, the previous set stays in force. */
 #define RHGPU_INJECT_SOLARWIND 1
 #define RHGPU_INJECT_FLOW      2
 #define RHGPU_INJECT_EXOSPHERE 3

@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "librhoracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "librhref.so")
 REF_GC_PATH = os.path.join(HERE, "_ref", "librhref_gc.so")
-REF_DIR = os.environ.get("RH_REFERENCE_DIR", "/root/reference")
+# the reference tree: RH_REFERENCE_DIR, else the checkout next to this repository
+REF_DIR = os.environ.get("RH_REFERENCE_DIR") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 _port = None
 _ref = None
@@ -28,8 +29,11 @@ def build(reference: bool = True):
     """Builds the restatement, and the reference library when the reference
     tree is present (it is not on GPU machines, which use the prebuilt file)."""
     subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
-    if reference and os.path.isdir(os.path.join(REF_DIR, "src")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={REF_DIR}"], check=True)
+    if reference:
+        if os.path.isdir(os.path.join(REF_DIR, "src")):
+            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={REF_DIR}"], check=True)
+        elif not os.path.exists(REF_PATH):
+            print(f"oracle: no reference tree at {REF_DIR} (set RH_REFERENCE_DIR); the reference build is skipped")
 
 
 def port() -> Library:

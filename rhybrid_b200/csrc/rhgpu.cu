@@ -15,6 +15,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <atomic>
 
 #include "../../include/rhgpu.h"
 #include "k_fields.cuh"
@@ -120,7 +121,9 @@ struct TimerRec { int cls; int ea, eb; };
 // per device.
 __device__ __align__(256) double g_noallocScratch[108 * (size_t)RHGPU_NOALLOC_MAX_CELLS];
 constexpr int NOALLOC_MAX_DEVICES = 64;
-double* g_noallocPtr[NOALLOC_MAX_DEVICES] = {};
+// host threads may make their first call on a device at the same time: each
+// looks the address up and stores the same value
+std::atomic<double*> g_noallocPtr[NOALLOC_MAX_DEVICES] = {};
 
 // one species' FP32-form storage: cell index, FP32 offsets and velocities
 struct F32Host {
@@ -2193,14 +2196,14 @@ int rhgpu_accumulate_noalloc(rhgpu_ctx* c) {
                                      std::to_string(RHGPU_NOALLOC_MAX_CELLS) + ")");
    if (c->device < 0 || c->device >= NOALLOC_MAX_DEVICES) return fail(RHGPU_ERR_ARG, "accumulate_noalloc: device index out of range");
    RH_CUDA(cudaSetDevice(c->device));
-   double* S = g_noallocPtr[c->device];
+   double* S = g_noallocPtr[c->device].load();
    if (!S) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
       if (e != cudaSuccess || !p)
          return fail(RHGPU_ERR_CUDA, std::string("accumulate_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       S = (double*)p;
-      g_noallocPtr[c->device] = S;
+      g_noallocPtr[c->device].store(S);
    }
    // the kernel timer creates events on demand: off for this call
    const bool timing = c->timing;
@@ -2252,106 +2255,129 @@ int rhgpu_device_errors(rhgpu_ctx* c, uint32_t* word_out) {
    return RHGPU_OK;
 }
 
+// the device form of one particle source (cells, rates and lists allocated on
+// the device); on failure h holds whatever was allocated, for freeInjector
+int buildInjector(rhgpu_ctx* c, const rhgpu_injector& J, long long& keyBase, InjHost& h) {
+   const GridInfo& g = c->g;
+   const int nn[3] = {g.nx, g.ny, g.nz};
+   if (J.species < 0 || J.species >= c->ns) return fail(RHGPU_ERR_ARG, "set_injectors: bad species");
+   if (!(J.density >= 0) || !(J.temperature >= 0) || !(J.macroparticles_per_cell >= 0))
+      return fail(RHGPU_ERR_ARG, "set_injectors: density, temperature and macroparticles_per_cell must be >= 0");
+   std::memset(&h.d, 0, sizeof h.d);
+   h.d.species = J.species;
+   h.d.type = J.type;
+   h.d.seed = J.seed;
+   const double m = c->sp[J.species].m;
+   h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
+   const double ppc = J.macroparticles_per_cell;
+   h.d.w = (ppc > 0 && J.density > 0) ? J.density * g.dV / ppc : 0.0;
+   std::vector<int> cells;
+   // (i, j, k) has its neighbour along axis a on the side sgn
+   auto hasNb = [&](const int p[3], int a, int sgn) {
+      if (g.per[a]) return true;
+      return sgn > 0 ? p[a] < nn[a] - 1 : p[a] > 0;
+   };
+   if (J.type == RHGPU_INJECT_SOLARWIND) {
+      int ax = -1;
+      for (int a = 0; a < 3; ++a)
+         if (J.velocity[a] != 0.0) { if (ax >= 0) ax = 3; else ax = a; }
+      if (ax < 0 || ax > 2)
+         return fail(RHGPU_ERR_ARG, "set_injectors: solar wind velocity must have exactly one non-zero component");
+      const bool pos = J.velocity[ax] < 0;   // flows toward -ax: enters through the +ax wall
+      h.d.wall = 2 * ax + (pos ? 1 : 0);
+      h.d.U = std::fabs(J.velocity[ax]);
+      h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc * h.d.U * g.dt / g.dx : 0.0;
+      if (h.d.vth <= 0) return fail(RHGPU_ERR_ARG, "set_injectors: solar wind needs a temperature > 0");
+      // InjectorSolarWind::checkIfInjectionCell{X,Y,Z}{Pos,Neg} (particle_injector.cpp:392-446)
+      for (int k = 0; k < g.nz; ++k)
+         for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i) {
+               const int p[3] = {i, j, k};
+               if (hasNb(p, ax, pos ? 1 : -1)) continue;
+               bool edge = false;
+               for (int a = 0; a < 3; ++a)
+                  if (a != ax && (!hasNb(p, a, 1) || !hasNb(p, a, -1))) edge = true;
+               if (!edge) cells.push_back(i + g.nx * (j + g.ny * k));
+            }
+   } else if (J.type == RHGPU_INJECT_FLOW) {
+      for (int a = 0; a < 3; ++a) h.d.vel[a] = J.velocity[a];
+      h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc : 0.0;
+      // ghost cells of the selected inflow walls (InjectorFlow::inject, particle_injector.cpp:749-760)
+      for (int k = 0; k < g.nz; ++k)
+         for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i) {
+               const int p[3] = {i, j, k};
+               bool in = false;
+               for (int b = 0; b < 6; ++b)
+                  if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
+               if (in) cells.push_back(i + g.nx * (j + g.ny * k));
+            }
+   } else if (J.type == RHGPU_INJECT_EXOSPHERE || J.type == RHGPU_INJECT_IONOSPHERE ||
+              J.type == RHGPU_INJECT_CHAPMAN_IONOSPHERE) {
+      std::vector<double> rates;
+      int rc = J.type == RHGPU_INJECT_EXOSPHERE ? exoRates(c, J, h, cells, rates) : ionoRates(c, J, h, cells, rates);
+      if (rc) return rc;
+      if (!rates.empty()) {
+         RH_CUDA(cudaMalloc(&h.rates, sizeof(double) * rates.size()));
+         RH_CUDA(cudaMemcpy(h.rates, rates.data(), sizeof(double) * rates.size(), cudaMemcpyHostToDevice));
+      }
+      h.rateCells = cells;
+      h.rateValues = rates;
+      h.d.rates = h.rates;
+      if (!cells.empty()) {
+         // the selected cells (ncells ints) and their count (one int after them)
+         RH_CUDA(cudaMalloc(&h.list, sizeof(int) * (cells.size() + 1)));
+         h.d.list = h.list;
+         h.d.listCount = h.list + cells.size();
+      }
+   } else {
+      return fail(RHGPU_ERR_ARG, "set_injectors: unknown type");
+   }
+   h.d.ncells = (int)cells.size();
+   h.d.keyBase = keyBase;
+   keyBase += (long long)cells.size();
+   if (!cells.empty()) {
+      RH_CUDA(cudaMalloc(&h.cells, sizeof(int) * cells.size()));
+      RH_CUDA(cudaMemcpy(h.cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+   }
+   h.d.cells = h.cells;
+   return RHGPU_OK;
+}
+
+void freeInjector(InjHost& h) {
+   cudaFree(h.cells);
+   cudaFree(h.rates);
+   cudaFree(h.list);
+   h.cells = nullptr;
+   h.rates = nullptr;
+   h.list = nullptr;
+}
+
+// the new source set is built aside and replaces the old one only when every
+// source was built; on failure the previous sources stay in force and what was
+// built is freed
 int rhgpu_set_injectors(rhgpu_ctx* c, int32_t n, const rhgpu_injector* inj) {
    if (!c || n < 0 || (n > 0 && !inj)) return fail(RHGPU_ERR_ARG, "set_injectors: bad arguments");
    RH_CUDA(cudaSetDevice(c->device));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); cudaFree(h.list); }
-   c->inj.clear();
-   c->injKeyMax = 0;
    if (!c->injCnt) {
       RH_CUDA(cudaMalloc(&c->injCnt, sizeof(double) * 3 * MAX_SPECIES));
       RH_CUDA(cudaMemset(c->injCnt, 0, sizeof(double) * 3 * MAX_SPECIES));
    }
-   const GridInfo& g = c->g;
-   const int nn[3] = {g.nx, g.ny, g.nz};
    long long keyBase = c->fg.NS > 0 ? c->fg.NS : 1;
+   std::vector<InjHost> built;
    for (int q = 0; q < n; ++q) {
-      const rhgpu_injector& J = inj[q];
-      if (J.species < 0 || J.species >= c->ns) return fail(RHGPU_ERR_ARG, "set_injectors: bad species");
-      if (!(J.density >= 0) || !(J.temperature >= 0) || !(J.macroparticles_per_cell >= 0))
-         return fail(RHGPU_ERR_ARG, "set_injectors: density, temperature and macroparticles_per_cell must be >= 0");
       InjHost h;
-      std::memset(&h.d, 0, sizeof h.d);
-      h.d.species = J.species;
-      h.d.type = J.type;
-      h.d.seed = J.seed;
-      const double m = c->sp[J.species].m;
-      h.d.vth = J.temperature > 0 ? std::sqrt(1.380649e-23 * J.temperature / m) : 0.0;
-      const double ppc = J.macroparticles_per_cell;
-      h.d.w = (ppc > 0 && J.density > 0) ? J.density * g.dV / ppc : 0.0;
-      std::vector<int> cells;
-      // (i, j, k) has its neighbour along axis a on the side sgn
-      auto hasNb = [&](const int p[3], int a, int sgn) {
-         if (g.per[a]) return true;
-         return sgn > 0 ? p[a] < nn[a] - 1 : p[a] > 0;
-      };
-      if (J.type == RHGPU_INJECT_SOLARWIND) {
-         int ax = -1;
-         for (int a = 0; a < 3; ++a)
-            if (J.velocity[a] != 0.0) { if (ax >= 0) ax = 3; else ax = a; }
-         if (ax < 0 || ax > 2)
-            return fail(RHGPU_ERR_ARG, "set_injectors: solar wind velocity must have exactly one non-zero component");
-         const bool pos = J.velocity[ax] < 0;   // flows toward -ax: enters through the +ax wall
-         h.d.wall = 2 * ax + (pos ? 1 : 0);
-         h.d.U = std::fabs(J.velocity[ax]);
-         h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc * h.d.U * g.dt / g.dx : 0.0;
-         if (h.d.vth <= 0) return fail(RHGPU_ERR_ARG, "set_injectors: solar wind needs a temperature > 0");
-         // InjectorSolarWind::checkIfInjectionCell{X,Y,Z}{Pos,Neg} (particle_injector.cpp:392-446)
-         for (int k = 0; k < g.nz; ++k)
-            for (int j = 0; j < g.ny; ++j)
-               for (int i = 0; i < g.nx; ++i) {
-                  const int p[3] = {i, j, k};
-                  if (hasNb(p, ax, pos ? 1 : -1)) continue;
-                  bool edge = false;
-                  for (int a = 0; a < 3; ++a)
-                     if (a != ax && (!hasNb(p, a, 1) || !hasNb(p, a, -1))) edge = true;
-                  if (!edge) cells.push_back(i + g.nx * (j + g.ny * k));
-               }
-      } else if (J.type == RHGPU_INJECT_FLOW) {
-         for (int a = 0; a < 3; ++a) h.d.vel[a] = J.velocity[a];
-         h.d.perCellPerDt = ppc > 0 && J.density > 0 ? ppc : 0.0;
-         // ghost cells of the selected inflow walls (InjectorFlow::inject, particle_injector.cpp:749-760)
-         for (int k = 0; k < g.nz; ++k)
-            for (int j = 0; j < g.ny; ++j)
-               for (int i = 0; i < g.nx; ++i) {
-                  const int p[3] = {i, j, k};
-                  bool in = false;
-                  for (int b = 0; b < 6; ++b)
-                     if ((J.inflow_walls >> b & 1) && !hasNb(p, b >> 1, (b & 1) ? -1 : 1)) in = true;
-                  if (in) cells.push_back(i + g.nx * (j + g.ny * k));
-               }
-      } else if (J.type == RHGPU_INJECT_EXOSPHERE || J.type == RHGPU_INJECT_IONOSPHERE ||
-                 J.type == RHGPU_INJECT_CHAPMAN_IONOSPHERE) {
-         std::vector<double> rates;
-         int rc = J.type == RHGPU_INJECT_EXOSPHERE ? exoRates(c, J, h, cells, rates) : ionoRates(c, J, h, cells, rates);
-         if (rc) return rc;
-         if (!rates.empty()) {
-            RH_CUDA(cudaMalloc(&h.rates, sizeof(double) * rates.size()));
-            RH_CUDA(cudaMemcpy(h.rates, rates.data(), sizeof(double) * rates.size(), cudaMemcpyHostToDevice));
-         }
-         h.rateCells = cells;
-         h.rateValues = rates;
-         h.d.rates = h.rates;
-         if (!cells.empty()) {
-            // the selected cells (ncells ints) and their count (one int after them)
-            RH_CUDA(cudaMalloc(&h.list, sizeof(int) * (cells.size() + 1)));
-            h.d.list = h.list;
-            h.d.listCount = h.list + cells.size();
-         }
-      } else {
-         return fail(RHGPU_ERR_ARG, "set_injectors: unknown type");
+      const int rc = buildInjector(c, inj[q], keyBase, h);
+      if (rc) {
+         freeInjector(h);
+         for (auto& b : built) freeInjector(b);
+         return rc;
       }
-      h.d.ncells = (int)cells.size();
-      h.d.keyBase = keyBase;
-      keyBase += (long long)cells.size();
-      if (!cells.empty()) {
-         RH_CUDA(cudaMalloc(&h.cells, sizeof(int) * cells.size()));
-         RH_CUDA(cudaMemcpy(h.cells, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
-      }
-      h.d.cells = h.cells;
-      c->inj.push_back(h);
+      built.push_back(h);
    }
+   for (auto& h : c->inj) freeInjector(h);
+   c->inj = std::move(built);
    c->injKeyMax = keyBase;
    return RHGPU_OK;
 }

@@ -233,5 +233,5 @@ def particle_points(ctx, species_names: Sequence[str], nstride: int = 10) -> Dic
         keep = sel[cell]
         out[f"ParticlePointMesh_{name}"] = q[keep, 0:3] + corner[cell[keep]]
         out[f"v_{name}"] = q[keep, 3:6].copy()
-        out[f"CellID_{name}"] = cell[keep].astype(np.uint64)   # pargrid::CellID, unsigned
+        out[f"CellID_{name}"] = cell[keep].astype(np.uint32)   # pargrid::CellID, unsigned int
     return out
