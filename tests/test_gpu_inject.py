@@ -137,6 +137,32 @@ def exo_box():
                      periodic=(0, 0, 0), dt=0.05, populations=[pop], name="exo_box")
 
 
+def test_rejected_source_set_keeps_the_previous_one(lib):
+    """rhgpu_set_injectors replaces the whole source set only when every
+    source is accepted: a set whose second source names no species is
+    refused, and the solar wind set before it keeps injecting the same
+    particles as an untouched context."""
+    cfg = box()
+    counts = []
+    for bad_call in (False, True):
+        ctx = empty_context(lib, cfg)
+        try:
+            if bad_call:
+                good = cf.solar_wind_injectors(cfg, seed=1)[0]
+                bad = abi.Injector(species=7, type=abi.INJECT_SOLARWIND, density=N0, temperature=T,
+                                   macroparticles_per_cell=PPC, seed=2)
+                with pytest.raises(abi.RhError):
+                    ctx.set_injectors([good, bad])
+            ctx.step(2)
+            cnt, p = ctx.download_particles(0)
+            counts.append((cnt, p))
+        finally:
+            ctx.close()
+    assert counts[0][1].shape[0] > 0
+    assert np.array_equal(counts[0][0], counts[1][0])
+    assert np.array_equal(counts[0][1], counts[1][1])
+
+
 def exo_injector(shadow=1.0, seed=5):
     j = abi.Injector(species=0, type=abi.INJECT_EXOSPHERE, temperature=1e3, seed=seed,
                      profile=abi.NEUTRAL_PROFILES["Exponential"], n_components=1, r0=600e3,
