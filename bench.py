@@ -60,7 +60,20 @@ def workload(name, scale=1.0):
                               nz=max(8, int(round(160 * f))), exosphere=True)
     if name == "empty_box":
         return cf.config_empty_box(32, 32, 32, ppc=20.0)
+    f = scale ** (1.0 / 3.0)
+    if name == "c3":
+        # the FP32 precision form's workload: the Mars-like run at 256^3 cells of
+        # 300 km, 100 ppc (H+ 100, He++ 5; about 1.76e9 ions) with its O+ exosphere
+        n = max(8, int(round(256 * f)))
+        return cf.config_mars(nx=n, ny=n, nz=n, ppc=100.0, exosphere=True)
+    if name == "mercury":
+        n = max(8, int(round(320 * f)))
+        return cf.config_mercury(nx=n, ny=n, nz=n)
     raise ValueError(name)
+
+
+# workloads too large for host-side particle records: filled on the GPU
+GPU_FILL = ("c3", "mercury")
 
 
 # ---------------------------------------------------------------------------
@@ -259,19 +272,36 @@ def run_gpu(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     cfg = workload(args.workload, args.scale)
+    gpu_fill = args.fill == "gpu" or (args.fill == "auto" and args.workload in GPU_FILL)
+    if gpu_fill and args.path == "exact":
+        raise SystemExit("the exact path takes host records: --fill host")
     t0 = time.time()
-    grid, pops = cf.initial_state(cfg)
-    gen_s = time.time() - t0
     lib = abi.gpu_library()
-    nps = [p[1].shape[0] for p in pops]
-    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + n // 20 + (1 << 20) for n in nps], device=local_rank)
+    if gpu_fill:
+        grid, pops = cf.init_grid(cfg), None
+        ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), device=local_rank)
+    else:
+        grid, pops = cf.initial_state(cfg)
+        nps = [p[1].shape[0] for p in pops]
+        ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=[n + n // 20 + (1 << 20) for n in nps],
+                          device=local_rank)
     ctx.set_path({"fast": abi.PATH_FAST, "exact": abi.PATH_EXACT, "fp32": abi.PATH_FP32}[args.path])
     ctx.upload_array("faceB", grid["faceB"])
     ctx.upload_array("cellB", grid["cellB"])
     ctx.upload_array("nodeEta", grid["nodeEta"])
     ctx.upload_cell_flags(grid["flags"])
-    for s, (c, p) in enumerate(pops):
-        ctx.upload_particles(s, c, p)
+    nspec = len(cfg.populations)
+    if gpu_fill:
+        for s, pop in enumerate(cfg.populations):
+            if pop.fill and pop.ppc > 0 and pop.density > 0:
+                ctx.fill_uniform(s, pop.density, pop.temperature, pop.velocity, pop.ppc, seed=cfg.seed + 101 * s)
+            else:
+                ctx.upload_particles(s, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+    else:
+        for s, (c, p) in enumerate(pops):
+            ctx.upload_particles(s, c, p)
+    torch.cuda.synchronize()
+    gen_s = time.time() - t0
     # the configuration's particle sources (solar wind inflow, O+ exosphere) on
     # the GPU; the exact path (the reference's particle order) takes none
     sources = cf.source_injectors(cfg, seed=cfg.seed) if args.path != "exact" else []
@@ -279,7 +309,7 @@ def run_gpu(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local_rank)
     for _ in range(args.warmup):
         ctx.step(1)
-    n0 = sum(ctx.num_particles(s) for s in range(len(pops)))
+    n0 = sum(ctx.num_particles(s) for s in range(nspec))
     ctx.set_timing(True)
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -296,10 +326,12 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
+    free_b, total_b = torch.cuda.mem_get_info(local_rank)
+    mem_used_gb = (total_b - free_b) / 1e9
     launches = ctx.last_launch_count()
     ktimes = ctx.timing()
     ctx.set_timing(False)
-    n1 = sum(ctx.num_particles(s) for s in range(len(pops)))
+    n1 = sum(ctx.num_particles(s) for s in range(nspec))
     psteps = 0.5 * (n0 + n1) * args.steps
     ms_all, psteps_all = reduce_over_ranks(dist, ms, psteps, "cuda")
     value = psteps_all / (ms_all / 1e3)
@@ -308,12 +340,12 @@ def run_gpu(args, rank, world, local_rank):
     peak, peak_kind = hbm_peak()
     top = max(ktimes.items(), key=lambda kv: kv[1]) if ktimes else ("none", 0.0)
     per_species = KERNEL_BYTES.get(top[0], (None, False))[1]
-    nlaunch_top = args.steps * (len(pops) if per_species else 1)
+    nlaunch_top = args.steps * (nspec if per_species else 1)
     per_launch_ms = top[1] / max(nlaunch_top, 1)
     roof = None
     if top[0] in KERNEL_BYTES and per_launch_ms > 0:
         # particles of one launch (per-species kernels: the mean over species)
-        pcount = 0.5 * (n0 + n1) / (len(pops) if per_species else 1)
+        pcount = 0.5 * (n0 + n1) / (nspec if per_species else 1)
         alg = KERNEL_BYTES[top[0]][0](pcount, cfg.ncells)
         ach = alg / (per_launch_ms / 1e3) / 1e9
         roof = {"kernel": top[0], "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
@@ -330,7 +362,7 @@ def run_gpu(args, rank, world, local_rank):
 
     # end to end through the C ABI with host-resident state (rank-local)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not gpu_fill:
         cnts, parts = [], []
         for s in range(len(pops)):
             c, p = ctx.download_particles(s)
@@ -347,12 +379,12 @@ def run_gpu(args, rank, world, local_rank):
         t1 = time.perf_counter()
         e2e_ps = 0
         for _ in range(ke):
-            for s in range(len(pops)):
+            for s in range(nspec):
                 ctx.upload_particles(s, cnts[s], parts[s])
                 e2e_ps += parts[s].shape[0]
             ctx.step(1)
             d2h = 0
-            for s in range(len(pops)):
+            for s in range(nspec):
                 n = ctx.num_particles(s)
                 if n > out_pin[s].shape[0]:
                     out_pin[s] = np.empty((n, 7))
@@ -370,12 +402,13 @@ def run_gpu(args, rank, world, local_rank):
                "d2h_bytes_per_step": int(d2h), "steps": ke,
                "host": "every step: all particles uploaded from pinned host memory, one step, particles and "
                        "rhoq, Ji, faceB downloaded (a host that owns the particle lists)"}
+    if not args.no_e2e:
         # a host that keeps the state on the device (Corsair with the GPU plugin):
         # per step it reads back the step's diagnostics (population and field log
         # sums) and nothing else; the particles and the grid come back at the output
         # step that closes the sample
         ko = max(1, args.steps)
-        ndiag = 8 * len(pops) + 30
+        ndiag = 8 * nspec + 30
         diag = torch.empty(ndiag, dtype=torch.float64, pin_memory=True).numpy()
         if dist:
             dist.barrier()
@@ -383,26 +416,35 @@ def run_gpu(args, rank, world, local_rank):
         t1 = time.perf_counter()
         out_ps = 0
         for _ in range(ko):
-            out_ps += sum(ctx.num_particles(s) for s in range(len(pops)))
+            out_ps += sum(ctx.num_particles(s) for s in range(nspec))
             ctx.step(1)
             lib.call("reduce_diagnostics", ctx.h, abi._ptr(diag, abi.C.c_double), ndiag)
         d2h_out = 0
-        for s in range(len(pops)):
-            c, p = ctx.download_particles(s)
-            d2h_out += p.nbytes + c.nbytes
+        if not gpu_fill:
+            for s in range(nspec):
+                c, p = ctx.download_particles(s)
+                d2h_out += p.nbytes + c.nbytes
         for name in ("cellRhoQi", "cellJi", "faceB"):
             d2h_out += ctx.download_array(name).nbytes
         torch.cuda.synchronize()
         out_s = time.perf_counter() - t1
         out_s, out_ps = reduce_over_ranks(dist, out_s, float(out_ps), "cuda")
-        e2e["output_step_host"] = {"value": out_ps / out_s, "unit": "particle-steps/s", "steps": ko,
+        out = {"value": out_ps / out_s, "unit": "particle-steps/s", "steps": ko,
                                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(diag.nbytes + d2h_out / ko),
                                    "host": f"state resident on the device; each step reads back its {ndiag} "
-                                           "diagnostic sums, and the particles and rhoq, Ji, faceB come back once "
-                                           f"at the output step closing the {ko}-step sample"}
+                                           "diagnostic sums, and " + ("" if gpu_fill else "the particles and ")
+                                           + f"rhoq, Ji, faceB come back once at the output step closing the "
+                                           f"{ko}-step sample" + (" (the particles, filled on the GPU, stay there: "
+                                           "the run's output saves grid arrays only, save_particles = 0 as in "
+                                           "the reference's examples)" if gpu_fill else "")}
+        if e2e is None:
+            e2e = dict(out, note="particles filled on the GPU: no host-owned particle lists for a per-step "
+                                 "round trip; this is the device-resident host")
+        else:
+            e2e["output_step_host"] = out
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "mars":
         m = cpu_measure(args.workload, steps=5, warm=1)
         cpu = {"value": round(float(np.median(m["rates"])), 1), "unit": "particle-steps/s", "cores": m["cores"],
                "kind": m["kind"],
@@ -416,12 +458,14 @@ def run_gpu(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_all / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.path == "fp32" else "f64",
-            "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform; sources on the GPU)",
+            "data": "synthetic (seeded uniform-in-cell Maxwellian fill, InjectorUniform" +
+                    (", generated on the GPU" if gpu_fill else "") + "; sources on the GPU)",
             "config": {"workload": cfg.name, "cells": [cfg.nx, cfg.ny, cfg.nz], "dx_m": cfg.dx, "dt_s": cfg.dt,
                        "ions": int(0.5 * (n0 + n1)), "species": [p.name for p in cfg.populations],
                        "sources": [("exosphere " if j.type == abi.INJECT_EXOSPHERE else "solar wind ")
                                    + cfg.populations[j.species].name for j in sources],
                        "parallelism": f"replicas x{world}", "particle_path": args.path, "l2": "state 10+ GB > 126 MB L2, no flush needed",
+                       "device_mem_gb": round(mem_used_gb, 1),
                        "sim_s_per_wall_s": round(args.steps * cfg.dt / (ms_all / 1e3), 4),
                        "step_roofline": {"achieved_gbs": round(step_ach, 1), "alg_bytes_per_step": int(step_alg),
                                          "frac": round(step_ach / peak, 4)},
@@ -462,7 +506,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--workload", default="mars", choices=["mars", "empty_box"])
+    ap.add_argument("--workload", default="mars", choices=["mars", "empty_box", "c3", "mercury"],
+                    help="mars: plain FP64 Mars-like run (default); c3: the FP32 form's 256^3 100-ppc Mars-like run; "
+                         "mercury: the Mercury-like dipole 320^3 40 ppc")
+    ap.add_argument("--fill", default="auto", choices=["auto", "host", "gpu"],
+                    help="initial particles from host records (host) or generated on the GPU (gpu); auto: gpu for "
+                         "c3 and mercury")
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's cells (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -383,6 +383,18 @@ typedef struct rhgpu_injector {
    int32_t  reserved2;
 } rhgpu_injector;
 int rhgpu_set_injectors(rhgpu_ctx* ctx, int32_t n, const rhgpu_injector* injectors);
+/* Replaces species s's particles by a uniform fill generated on the GPU, for
+ * the fast path and the FP32 form (no host records: runs of 1e9 ions and more).
+ * The reference's InjectorUniform::injectParticles (particle_injector.cpp:
+ * 188-255): every cell whose centre lies in `region` (x_lo, x_hi, y_lo, y_hi,
+ * z_lo, z_hi in metres; NULL: the whole box) draws probRound(ppc) macroparticles
+ * (ppc = injector->macroparticles_per_cell), uniform in the central (1 - 1e-4)
+ * of the cell, velocity injector->velocity + sqrt(k_B T / m) N(0,1) per
+ * component, weight density dx^3 / ppc. Uses density, temperature, velocity,
+ * macroparticles_per_cell and seed of the injector; particle k of cell c draws
+ * from a Philox stream keyed by (seed, c, k), so the fill is reproducible. */
+int rhgpu_fill_uniform(rhgpu_ctx* ctx, int32_t s, const rhgpu_injector* injector, const double* region);
+
 /* expected macroparticles per step in every cell (N doubles, linear cell
  * order) of source `injector` (index into the last rhgpu_set_injectors
  * array). Filled for the rate-based sources: exosphere (cellExosphere,

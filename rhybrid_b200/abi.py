@@ -144,6 +144,7 @@ _SIGNATURES = {
 _OPTIONAL = {
     "device_errors": [_P, _U32],
     "reduce_diagnostics": [_P, _D, C.c_int32],
+    "fill_uniform": [_P, C.c_int32, C.c_void_p, C.c_void_p],
     "set_timing": [_P, C.c_int32],
     "get_timing": [_P, C.c_char_p, C.c_int32, _D, C.c_int32, C.POINTER(C.c_int32)],
     "last_launch_count": [_P, _I64],
@@ -459,6 +460,22 @@ class Context:
         arr = (Injector * max(len(injectors), 1))(*injectors)
         self.lib.call("set_injectors", self.h, len(injectors), C.cast(arr, C.c_void_p))
         self.injectors = list(injectors)
+
+    def fill_uniform(self, s: int, density: float, temperature: float, velocity, ppc: float, seed: int = 1,
+                     region=None):
+        """rhgpu_fill_uniform: replaces species s by a uniform fill generated on
+        the GPU (InjectorUniform; fast path and FP32 form). region: (x_lo, x_hi,
+        y_lo, y_hi, z_lo, z_hi) of the cell centres, or None for the whole box."""
+        j = Injector(species=s, type=0, density=density, temperature=temperature, macroparticles_per_cell=ppc,
+                     seed=seed)
+        for a in range(3):
+            j.velocity[a] = velocity[a]
+        reg = None
+        if region is not None:
+            reg = np.ascontiguousarray(region, dtype=np.float64)
+            assert reg.size == 6
+        self.lib.call("fill_uniform", self.h, s, C.cast(C.byref(j), C.c_void_p),
+                      reg.ctypes.data_as(C.c_void_p) if reg is not None else None)
 
     def source_rates(self, injector: int) -> np.ndarray:
         """rhgpu_source_rates: expected macroparticles per step in every cell

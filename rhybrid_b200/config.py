@@ -261,6 +261,39 @@ def config_mars(nx=120, ny=160, nz=160, ppc=30.0, dx=300e3, exosphere=False) -> 
                   populations=pops, name=f"mars_{nx}x{ny}x{nz}_ppc{ppc:g}" + ("_exoO+" if exosphere else ""))
 
 
+def config_mercury(nx=320, ny=320, nz=320, ppc=40.0, dx=100e3) -> Config:
+    """Mercury-like dipole: cell 100 km, a dipole of 190 nT at r = 2440 km
+    (surface field, southward as in examples/mercury.cfg) plus the IMF Bx
+    draped around a 1800 km sphere (translateDipoleBAndLaminarFlowAroundSphereBx,
+    src/magnetic_field.h:182-185), absorbing sphere r = 2439.7 km, solar wind
+    H+ n = 3e7 m^-3 at 40 ppc, V = -400 km/s. The box puts the planet at 5/8 of
+    x (more room downstream), as the example does. The rest follows
+    examples/mercury.cfg: T = 1.7e5 K, IMF (2, 0, -10) nT on the +x wall,
+    electron pressure 2.26e5 K (gamma 2), superconducting-core resistivity
+    (Rm 6 within 1800 km, 10x on the +y outer cells), constraints 4000 km/s
+    and E 0.0906 V/m, dt = 0.02 s, no gravity."""
+    R = 2439.7e3
+    Lx, Ly, Lz = nx * dx, ny * dx, nz * dx
+    pops = [Population(name="swH+", mass=1.0, charge=1.0, obstacle=R, density=3e7,
+                       velocity=(-400e3, 0, 0), temperature=1.7e5, ppc=ppc)]
+    return Config(nx=nx, ny=ny, nz=nz, x_min=-0.625 * Lx, y_min=-0.5 * Ly, z_min=-0.5 * Lz, dx=dx,
+                  periodic=(0, 0, 0), dt=0.02, R_fieldObstacle=R, R_particleObstacle=R,
+                  imf=(2e-9, 0.0, -10e-9), imf_boundary_cellB=(1, 0, 0, 0, 0, 0),
+                  imf_boundary_faceB=(1, 0, 0, 0, 0, 0),
+                  b_profile="translateDipoleBAndLaminarFlowAroundSphereBx", laminar_R=1800e3,
+                  dipole_surface_B=-190e-9, dipole_surface_R=2440e3, dipole_min_R=1000e3,
+                  dipole_origin=(0.0, 0.0, 0.0),
+                  use_electron_pressure=True, electron_temperature=2.26e5, electron_gamma=2,
+                  R_zeroElectronPressure=-100.0,
+                  resistivity_profile="resistivitySuperConductingSphere", resistivity_unit="Rm",
+                  resistivity_value=6.0, resistivity_R=1800e3,
+                  resistivity_outer_cells=(0, 4, 0, 0, 0, 0), resistivity_outer_coeffs=(1, 10, 1, 1, 1, 1),
+                  max_ion_velocity=4000e3, max_electron_velocity=4000e3,
+                  min_ion_charge_density_relative=0.05, max_electric_field=0.0906,
+                  max_whistler_velocity=4000e3, populations=pops,
+                  name=f"mercury_{nx}x{ny}x{nz}_ppc{ppc:g}")
+
+
 # ---------------------------------------------------------------------------
 # parameter derivation (src/user.cpp:356-1807)
 

@@ -26,6 +26,7 @@
 #include "k_denoise.cuh"
 #include "k_inject.cuh"
 #include "k_avg.cuh"
+#include "k_fill.cuh"
 #include "rh_logs.h"
 
 using namespace rh;
@@ -690,11 +691,20 @@ int ensureMigBuffers(rhgpu_ctx* c, long long want) {
    return RHGPU_OK;
 }
 
-// mover list: a quarter of all slots (at least 2^20)
+// entries of the mover list for `slots` particle slots: a quarter of them (at
+// least 2^20); past 2^29 slots a sixteenth, but at least 2^27 (movers are
+// about 1-3 % of the particles per step in the workloads, more in hot plasmas
+// of small test boxes; a step whose movers exceed the list fails with
+// RHGPU_ERR_CAPACITY)
+long long moverListSize(long long slots) {
+   return std::max(1LL << 20, std::min(slots / 4, std::max(slots / 16, 1LL << 27)));
+}
+
+// mover list: moverListSize of all slots
 int fastMoverBuffers(rhgpu_ctx* c) {
    long long tot = 0;
    for (int s = 0; s < c->ns; ++s) tot += c->seg[s].capOf[c->seg[s].cur];
-   const long long want = std::max(1LL << 20, tot / 4);
+   const long long want = moverListSize(tot);
    if (want > c->fb.moverCap) {
       cudaFree(c->fb.movers);
       c->fb.movers = nullptr;
@@ -1254,7 +1264,7 @@ void f32Exponents(rhgpu_ctx* c) {
 int f32MoverBuffers(rhgpu_ctx* c) {
    long long tot = 0;
    for (int s = 0; s < c->ns; ++s) tot += c->f32[s].capOf[c->f32[s].cur];
-   const long long want = std::max(1LL << 20, tot / 4);
+   const long long want = moverListSize(tot);
    if (want > c->f32b.moverCap) {
       cudaFree(c->f32b.movers);
       c->f32b.movers = nullptr;
@@ -2071,6 +2081,81 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
    RH_CUDA(cudaStreamSynchronize(c->stream));
    P.nslots = n;
    return ensureKeyCapacity(c, n);
+}
+
+int rhgpu_fill_uniform(rhgpu_ctx* c, int32_t s, const rhgpu_injector* J, const double* region) {
+   if (!c || s < 0 || s >= c->ns || !J) return fail(RHGPU_ERR_ARG, "fill_uniform: bad arguments");
+   if (c->path != RHGPU_PATH_FAST && c->path != RHGPU_PATH_FP32)
+      return fail(RHGPU_ERR_STATE, "fill_uniform: the fast path or the FP32 form only (the exact path takes host records)");
+   if (!(J->density >= 0) || !(J->temperature >= 0) || !(J->macroparticles_per_cell >= 0) ||
+       !(J->macroparticles_per_cell < 2e9))
+      return fail(RHGPU_ERR_ARG, "fill_uniform: density, temperature and macroparticles_per_cell must be >= 0");
+   RH_CUDA(cudaSetDevice(c->device));
+   const GridInfo& g = c->g;
+   FillSpec F;
+   F.seed = J->seed;
+   F.ppc = J->density > 0 ? J->macroparticles_per_cell : 0.0;
+   F.w = (F.ppc > 0) ? J->density * g.dV / F.ppc : 0.0;
+   F.vth = J->temperature > 0 ? std::sqrt(1.380649e-23 * J->temperature / c->sp[s].m) : 0.0;
+   for (int a = 0; a < 3; ++a) {
+      F.U[a] = J->velocity[a];
+      F.lo[a] = region ? region[2 * a] : -HUGE_VAL;
+      F.hi[a] = region ? region[2 * a + 1] : HUGE_VAL;
+   }
+   F.species = s;
+   const long long NS = c->fg.NS;
+   const bool f32 = c->path == RHGPU_PATH_FP32;
+   const float below1 = std::nextafter(1.0f, 0.0f);
+   int rc = RHGPU_OK;
+   int* cnt;
+   long long* base;
+   if (f32) {
+      rc = f32Init(c);
+      if (rc) return rc;
+      cnt = c->f32[s].cnt[c->f32[s].cur];
+      base = c->f32[s].base;
+   } else {
+      cnt = c->seg[s].cnt[c->seg[s].cur];
+      base = c->seg[s].base;
+   }
+   if (f32)
+      k_fill_count<true><<<(unsigned)NS, FILL_THREADS, 0, c->stream>>>(g, c->fg, F, below1, cnt);
+   else
+      k_fill_count<false><<<(unsigned)NS, FILL_THREADS, 0, c->stream>>>(g, c->fg, F, below1, cnt);
+   RH_CUDA(cudaGetLastError());
+   long long n = 0;
+   rc = segPrefix(c, cnt, &n);
+   if (rc) return rc;
+   if (c->capHint[s] > 0 && n > c->capHint[s]) return fail(RHGPU_ERR_CAPACITY, "fill_uniform: more particles than capacity");
+   long long slots = 0;
+   rc = fastLayout(c, cnt, nullptr, base, &slots);
+   if (rc) return rc;
+   if (f32) {
+      F32Host& h = c->f32[s];
+      rc = f32Reserve(h, 0, slots);
+      if (!rc) rc = f32Reserve(h, 1, slots);
+      if (rc) return rc;
+      h.w = F.w;
+      SegBuf none{};
+      k_fill_write<true><<<(unsigned)NS, FILL_THREADS, 0, c->stream>>>(g, c->fg, F, below1, base, none, f32View(h, h.cur));
+   } else {
+      SegHost& h = c->seg[s];
+      rc = segReserve(h, 0, slots);
+      if (!rc) rc = segReserve(h, 1, slots);
+      if (rc) return rc;
+      F32Buf none{};
+      k_fill_write<false><<<(unsigned)NS, FILL_THREADS, 0, c->stream>>>(g, c->fg, F, below1, base, segView(h, h.cur), none);
+   }
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   c->uploaded = true;
+   if (f32) {
+      f32Exponents(c);
+      return f32MoverBuffers(c);
+   }
+   rc = fastExponents(c);
+   if (rc) return rc;
+   return fastMoverBuffers(c);
 }
 
 int rhgpu_num_particles(rhgpu_ctx* c, int32_t s, int64_t* n_out) {
