@@ -480,6 +480,35 @@ def run_gpu(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_learned(args, rank, world, local_rank):
+    """The learned form in closed loop (rhybrid_b200.learned.closed_loop): one
+    line with the learned form's simulated seconds per wall second, its error
+    against the check run, and its speed-up over the plain FP64 path at matched
+    error (measured plain points only). Replicas only: every rank runs it, rank
+    0 prints."""
+    import torch
+    from rhybrid_b200 import learned
+    torch.cuda.set_device(local_rank)
+    out = learned.closed_loop(scale=args.scale, log=lambda m: print(m, file=sys.stderr, flush=True))
+    lr = out["learned"]
+    if rank == 0:
+        line = {
+            "metric": "sim-s per wall-s (learned 8 ppc FP64 fast path + denoiser; plain FP64 at matched error)",
+            "value": round(lr["sim_s_per_wall_s"], 4), "unit": "sim-s/wall-s", "n_gpus": world,
+            "steps": out["window"]["last_step"], "warmup": 0, "ms_per_step": round(lr["ms_per_step"], 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network bf16, fp32 accum)",
+            "data": "synthetic (uniform fill generated on the GPU, solar wind sources)",
+            "config": {"workload": f"mars_{out['geometry'][0]}x{out['geometry'][1]}x{out['geometry'][2]}_learned",
+                       "check_run": out["check_run"], "training": out["training"], "window": out["window"],
+                       "threshold": out["threshold"],
+                       "learned": {k: v for k, v in lr.items() if k != "samples"},
+                       "plain": [{k: v for k, v in p.items() if k != "samples"} for p in out["plain"]],
+                       "matched_error": out["matched_error"], "seconds": out["seconds"]},
+            "samples": {"learned": lr["samples"], **{f"plain_{p['ppc']}": p["samples"] for p in out["plain"]}},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -509,6 +538,10 @@ def main():
     ap.add_argument("--workload", default="mars", choices=["mars", "empty_box", "c3", "mercury"],
                     help="mars: plain FP64 Mars-like run (default); c3: the FP32 form's 256^3 100-ppc Mars-like run; "
                          "mercury: the Mercury-like dipole 320^3 40 ppc")
+    ap.add_argument("--form", default="plain", choices=["plain", "learned"],
+                    help="plain: the hot path (default); learned: the learned form's closed-loop evaluation at the "
+                         "Mars-like geometry (8 ppc + denoiser against a 256-ppc FP64 check run, plain FP64 at "
+                         "8-128 ppc)")
     ap.add_argument("--fill", default="auto", choices=["auto", "host", "gpu"],
                     help="initial particles from host records (host) or generated on the GPU (gpu); auto: gpu for "
                          "c3 and mercury")
@@ -524,6 +557,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.form == "learned":
+        run_learned(args, rank, world, local_rank)
     else:
         run_gpu(args, rank, world, local_rank)
 

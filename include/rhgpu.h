@@ -283,6 +283,19 @@ int rhgpu_dn_apply(rhgpu_dn* dn, const double* rho_in, const double* ji_in, doub
 int rhgpu_dn_loss_grad(rhgpu_dn* dn, const double* rho_in, const double* ji_in, const double* rho_target,
                        const double* ji_target, double* loss, float* grad);
 int rhgpu_dn_add_pair(rhgpu_dn* dn, rhgpu_ctx* ctx, int32_t factor, int32_t offset);
+/* Training pairs from crops of a larger grid, for a denoiser created with the
+ * crop's dimensions (non-periodic): the context's moments are deposited as by
+ * rhgpu_dn_add_pair (one in `factor` particles, weights times factor; and all
+ * particles) on its whole grid, and each crop, corner origins[3q..3q+2] (cell
+ * indices, inside the context's grid), is stored as one pair. The network is
+ * convolutional: parameters trained on crops apply to the whole grid
+ * (rhgpu_dn_get_params / rhgpu_dn_set_params). */
+int rhgpu_dn_add_crops(rhgpu_dn* dn, rhgpu_ctx* ctx, int32_t factor, int32_t offset, int32_t ncrops,
+                       const int32_t* origins);
+/* leaves the voxels within `border` of a non-periodic face out of the training
+ * loss (crops: their outer voxels see zeros instead of their neighbours;
+ * three layers of 3x3x3 reach 3 voxels). Default 0. */
+int rhgpu_dn_set_loss_border(rhgpu_dn* dn, int32_t border);
 /* Adam steps, one random stored pair per step; mean loss over the steps */
 int rhgpu_dn_train(rhgpu_dn* dn, int32_t iterations, float lr, double* mean_loss);
 int rhgpu_set_denoiser(rhgpu_ctx* ctx, rhgpu_dn* dn, int32_t enabled);

@@ -145,6 +145,8 @@ _OPTIONAL = {
     "device_errors": [_P, _U32],
     "reduce_diagnostics": [_P, _D, C.c_int32],
     "fill_uniform": [_P, C.c_int32, C.c_void_p, C.c_void_p],
+    "dn_add_crops": [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_void_p],
+    "dn_set_loss_border": [_P, C.c_int32],
     "set_timing": [_P, C.c_int32],
     "get_timing": [_P, C.c_char_p, C.c_int32, _D, C.c_int32, C.POINTER(C.c_int32)],
     "last_launch_count": [_P, _I64],
@@ -602,6 +604,15 @@ class Denoiser:
 
     def add_pair(self, ctx, factor: int, offset: int):
         self.lib.call("dn_add_pair", self.h, ctx.h, factor, offset)
+
+    def add_crops(self, ctx, factor: int, offset: int, origins):
+        """rhgpu_dn_add_crops: one pair per crop of ctx's grid; origins (n x 3) cell
+        indices of the crops' corners, the crop size being this denoiser's grid."""
+        o = np.ascontiguousarray(origins, dtype=np.int32).reshape(-1, 3)
+        self.lib.call("dn_add_crops", self.h, ctx.h, factor, offset, o.shape[0], o.ctypes.data_as(C.c_void_p))
+
+    def set_loss_border(self, border: int):
+        self.lib.call("dn_set_loss_border", self.h, border)
 
     def train(self, iterations: int, lr: float) -> float:
         loss = C.c_double()

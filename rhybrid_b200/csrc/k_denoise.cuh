@@ -344,13 +344,20 @@ __global__ void k_dn_reduce_rows(const float* part, long long rows, int n, float
 }
 
 // MSE loss over the 4 real channels and its gradient (BF16, 16 channels)
-__global__ void k_dn_loss(DnGrid g, const float* pred, const float* target, double inv, unsigned* dY, double* part) {
+// border: voxels within `border` of a non-periodic face are left out of the
+// loss (zero gradient): for training on crops of a larger grid, whose outer
+// voxels see the zero halo of the crop instead of their neighbours
+__global__ void k_dn_loss(DnGrid g, const float* pred, const float* target, double inv, unsigned* dY, double* part,
+                          int border) {
    __shared__ double s[256];
    double l = 0.0;
    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < g.N; v += (long long)gridDim.x * blockDim.x) {
+      const int x = (int)(v % g.nx), y = (int)((v / g.nx) % g.ny), z = (int)(v / ((long long)g.nx * g.ny));
+      const bool in = (g.per[0] || (x >= border && x < g.nx - border)) && (g.per[1] || (y >= border && y < g.ny - border)) &&
+                      (g.per[2] || (z >= border && z < g.nz - border));
       float d[4];
       for (int c = 0; c < 4; ++c) {
-         d[c] = pred[v * 4 + c] - target[v * 4 + c];
+         d[c] = in ? pred[v * 4 + c] - target[v * 4 + c] : 0.0f;
          l += (double)d[c] * d[c];
       }
       const float k = (float)(2.0 * inv);
@@ -426,6 +433,17 @@ __global__ void k_dn_subsample_deposit(GridInfo g, FastGeom fg, SegBuf B, const 
    }
 }
 // the deposit's finalize on the subsample sums: /dV, rho clamp, then normalized FP32 (N x 4)
+// one crop of a normalized (N x 4) moment grid: the crop's voxel (x, y, z) is
+// the full grid's (x0 + x, y0 + y, z0 + z)
+__global__ void k_dn_crop(const float* full, int fnx, int fny, DnGrid c, int x0, int y0, int z0, float* out) {
+   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (v >= c.N) return;
+   const int x = (int)(v % c.nx), y = (int)((v / c.nx) % c.ny), z = (int)(v / ((long long)c.nx * c.ny));
+   const long long f = (long long)(x0 + x) + (long long)fnx * ((long long)(y0 + y) + (long long)fny * (z0 + z));
+   const float4 q = *reinterpret_cast<const float4*>(full + 4 * f);
+   *reinterpret_cast<float4*>(out + 4 * v) = q;
+}
+
 __global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double rsr, double rsj,
                                       float* out) {
    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;

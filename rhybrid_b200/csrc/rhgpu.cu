@@ -288,6 +288,11 @@ struct rhgpu_dn {
    float* pairOut = nullptr;             // targets
    int pairCap = 0, pairCount = 0, pairNext = 0;
    long long adamStep = 0;
+   int border = 0;                       // loss mask width at non-periodic faces (crop training)
+   long long fullN = 0;                  // crop pairs: the source grid's deposits (normalized, 4 x fullN)
+   double* fullAcc = nullptr;
+   float* fullIn = nullptr;
+   float* fullOut = nullptr;
    unsigned long long rng = 0x9e3779b97f4a7c15ull;
 };
 
@@ -1561,7 +1566,13 @@ int dnForward(rhgpu_dn* d) {
 // loss against target (normalized FP32, N x 4) and the gradient of all parameters into d->grad
 int dnBackward(rhgpu_dn* d, const float* target, double* loss) {
    const long long N = d->g.N;
-   k_dn_loss<<<DN_LOSS_BLOCKS, 256, 0, d->stream>>>(d->g, d->out32, target, 1.0 / (4.0 * (double)N), d->dY[2], d->lossPart);
+   // voxels in the loss: all but the masked border of the non-periodic faces
+   long long in = 1;
+   const int nn[3] = {d->g.nx, d->g.ny, d->g.nz};
+   for (int a = 0; a < 3; ++a) in *= d->g.per[a] ? nn[a] : std::max(0, nn[a] - 2 * d->border);
+   if (in < 1) return fail(RHGPU_ERR_STATE, "dn_train: the loss border leaves no voxel");
+   k_dn_loss<<<DN_LOSS_BLOCKS, 256, 0, d->stream>>>(d->g, d->out32, target, 1.0 / (4.0 * (double)in), d->dY[2], d->lossPart,
+                                                   d->border);
    const unsigned wb = (unsigned)((N + DN_WGRAD_VOX - 1) / DN_WGRAD_VOX);
    for (int l = 2; l >= 0; --l) {
       k_dn_wgrad<<<dim3(wb, DN_TAPS), 32 * DN_WARPS, 0, d->stream>>>(d->g, d->act[l], d->dY[l], d->part);
@@ -1580,7 +1591,7 @@ int dnBackward(rhgpu_dn* d, const float* target, double* loss) {
    RH_CUDA(cudaStreamSynchronize(d->stream));
    double a = 0.0;
    for (double x : lp) a += x;
-   if (loss) *loss = a / (4.0 * (double)N);
+   if (loss) *loss = a / (4.0 * (double)in);
    return RHGPU_OK;
 }
 
@@ -2976,6 +2987,7 @@ int rhgpu_dn_destroy(rhgpu_dn* d) {
    for (int l = 0; l < 3; ++l) { cudaFree(d->act[l]); cudaFree(d->dY[l]); }
    cudaFree(d->res); cudaFree(d->out32); cudaFree(d->part); cudaFree(d->lossPart); cudaFree(d->acc);
    cudaFree(d->pairIn); cudaFree(d->pairOut);
+   cudaFree(d->fullAcc); cudaFree(d->fullIn); cudaFree(d->fullOut);
    if (d->stream) cudaStreamDestroy(d->stream);
    delete d;
    return RHGPU_OK;
@@ -3059,6 +3071,73 @@ int rhgpu_dn_loss_grad(rhgpu_dn* d, const double* rho_in, const double* ji_in, c
    return RHGPU_OK;
 }
 
+// the normalized moments of a fast-path context (4 x N floats, voxel-major):
+// one in `factor` of its particles (from `offset`) with weights times factor,
+// or all (factor 1); acc is 4 x N doubles of scratch
+int dnDepositSample(rhgpu_dn* d, rhgpu_ctx* c, int factor, int offset, double* acc, float* out) {
+   const long long N = c->g.N;
+   RH_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 4 * N, d->stream));
+   for (int s = 0; s < c->ns; ++s) {
+      if (!c->sp[s].accumulate) continue;
+      const SegHost& h = c->seg[s];
+      if (!h.a[h.cur][0]) continue;
+      k_dn_subsample_deposit<<<(unsigned)c->fg.NS, 128, 0, d->stream>>>(c->g, c->fg, segView(h, h.cur), h.base,
+                                                                       c->sp[s].q, factor, offset, acc);
+   }
+   k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, acc, c->g.dV, c->P.min_ion_charge_density,
+                                                                 1.0 / d->sr, 1.0 / d->sj, out);
+   RH_CUDA(cudaGetLastError());
+   return RHGPU_OK;
+}
+
+int rhgpu_dn_add_crops(rhgpu_dn* d, rhgpu_ctx* c, int32_t factor, int32_t offset, int32_t ncrops, const int32_t* origins) {
+   if (!d || !c || factor < 1 || offset < 0 || offset >= factor || ncrops < 1 || !origins)
+      return fail(RHGPU_ERR_ARG, "dn_add_crops: bad arguments");
+   if (d->pairCap < 1) return fail(RHGPU_ERR_STATE, "dn_add_crops: created without pair capacity");
+   if (c->path != RHGPU_PATH_FAST) return fail(RHGPU_ERR_STATE, "dn_add_crops: the context must use RHGPU_PATH_FAST");
+   if (c->device != d->device) return fail(RHGPU_ERR_ARG, "dn_add_crops: the device differs");
+   for (int q = 0; q < ncrops; ++q) {
+      const int* o = origins + 3 * q;
+      if (o[0] < 0 || o[1] < 0 || o[2] < 0 || o[0] + d->g.nx > c->g.nx || o[1] + d->g.ny > c->g.ny ||
+          o[2] + d->g.nz > c->g.nz)
+         return fail(RHGPU_ERR_ARG, "dn_add_crops: a crop leaves the context's grid");
+   }
+   RH_CUDA(cudaSetDevice(d->device));
+   RH_CUDA(cudaStreamSynchronize(c->stream));
+   const long long NF = c->g.N;
+   if (d->fullN != NF) {
+      cudaFree(d->fullAcc); cudaFree(d->fullIn); cudaFree(d->fullOut);
+      d->fullAcc = nullptr; d->fullIn = nullptr; d->fullOut = nullptr;
+      d->fullN = 0;
+      RH_CUDA(cudaMalloc(&d->fullAcc, sizeof(double) * 4 * NF));
+      RH_CUDA(cudaMalloc(&d->fullIn, sizeof(float) * 4 * NF));
+      RH_CUDA(cudaMalloc(&d->fullOut, sizeof(float) * 4 * NF));
+      d->fullN = NF;
+   }
+   int rc = dnDepositSample(d, c, factor, offset, d->fullAcc, d->fullIn);
+   if (!rc) rc = dnDepositSample(d, c, 1, 0, d->fullAcc, d->fullOut);
+   if (rc) return rc;
+   const long long N = d->g.N;
+   for (int q = 0; q < ncrops; ++q) {
+      const int* o = origins + 3 * q;
+      float* in = d->pairIn + (size_t)d->pairNext * 4 * N;
+      float* tg = d->pairOut + (size_t)d->pairNext * 4 * N;
+      k_dn_crop<<<blocks1d(N, 256), 256, 0, d->stream>>>(d->fullIn, c->g.nx, c->g.ny, d->g, o[0], o[1], o[2], in);
+      k_dn_crop<<<blocks1d(N, 256), 256, 0, d->stream>>>(d->fullOut, c->g.nx, c->g.ny, d->g, o[0], o[1], o[2], tg);
+      d->pairNext = (d->pairNext + 1) % d->pairCap;
+      d->pairCount = std::min(d->pairCount + 1, d->pairCap);
+   }
+   RH_CUDA(cudaGetLastError());
+   RH_CUDA(cudaStreamSynchronize(d->stream));
+   return RHGPU_OK;
+}
+
+int rhgpu_dn_set_loss_border(rhgpu_dn* d, int32_t border) {
+   if (!d || border < 0) return fail(RHGPU_ERR_ARG, "dn_set_loss_border: bad arguments");
+   d->border = border;
+   return RHGPU_OK;
+}
+
 int rhgpu_dn_add_pair(rhgpu_dn* d, rhgpu_ctx* c, int32_t factor, int32_t offset) {
    if (!d || !c || factor < 1 || offset < 0 || offset >= factor) return fail(RHGPU_ERR_ARG, "dn_add_pair: bad arguments");
    if (d->pairCap < 1) return fail(RHGPU_ERR_STATE, "dn_add_pair: created without pair capacity");
@@ -3072,20 +3151,9 @@ int rhgpu_dn_add_pair(rhgpu_dn* d, rhgpu_ctx* c, int32_t factor, int32_t offset)
    float* tg = d->pairOut + (size_t)d->pairNext * 4 * N;
    // input: one in `factor` particles, weights times factor; target: all particles,
    // by the same deposit of the same state
-   for (int pass = 0; pass < 2; ++pass) {
-      const int k = pass == 0 ? factor : 1, off = pass == 0 ? offset : 0;
-      RH_CUDA(cudaMemsetAsync(d->acc, 0, sizeof(double) * 4 * N, d->stream));
-      for (int s = 0; s < c->ns; ++s) {
-         if (!c->sp[s].accumulate) continue;
-         const SegHost& h = c->seg[s];
-         if (!h.a[h.cur][0]) continue;
-         k_dn_subsample_deposit<<<(unsigned)c->fg.NS, 128, 0, d->stream>>>(c->g, c->fg, segView(h, h.cur), h.base,
-                                                                          c->sp[s].q, k, off, d->acc);
-      }
-      k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, c->g.dV, c->P.min_ion_charge_density,
-                                                                    1.0 / d->sr, 1.0 / d->sj, pass == 0 ? in : tg);
-   }
-   RH_CUDA(cudaGetLastError());
+   int rc = dnDepositSample(d, c, factor, offset, d->acc, in);
+   if (!rc) rc = dnDepositSample(d, c, 1, 0, d->acc, tg);
+   if (rc) return rc;
    RH_CUDA(cudaStreamSynchronize(d->stream));
    d->pairNext = (d->pairNext + 1) % d->pairCap;
    d->pairCount = std::min(d->pairCount + 1, d->pairCap);

@@ -16,6 +16,8 @@ denoiser is switched off and the run continues with the plain deposit.
 """
 from __future__ import annotations
 
+import time
+
 import numpy as np
 
 from . import abi
@@ -135,3 +137,223 @@ class LearnedForm:
     def close(self):
         self.low.close()
         self.check.close()
+
+
+# ---------------------------------------------------------------------------
+# closed-loop evaluation at the full Mars-like geometry
+
+def c4_config(ppc: float, scale: float = 1.0) -> cf.Config:
+    """The learned form's workload: the Mars-like geometry (120x160x160 cells of
+    300 km, absorbing sphere, closed walls with the IMF on the +x wall) with its
+    solar wind H+ at `ppc` and He++ at ppc/20 and their inflow sources."""
+    f = scale ** (1.0 / 3.0)
+    return cf.config_mars(nx=max(16, int(round(120 * f))), ny=max(16, int(round(160 * f))),
+                          nz=max(16, int(round(160 * f))), ppc=ppc)
+
+
+def filled_context(lib: abi.Library, cfg: cf.Config, seed: int, path: int = abi.PATH_FAST) -> abi.Context:
+    """A context of cfg with its populations filled on the GPU and its sources set."""
+    grid = cf.init_grid(cfg)
+    ctx = abi.Context(lib, cf.params(cfg), cf.species(cfg))
+    ctx.set_path(path)
+    for k in ("faceB", "cellB", "nodeEta"):
+        ctx.upload_array(k, grid[k])
+    ctx.upload_cell_flags(grid["flags"])
+    for s, pop in enumerate(cfg.populations):
+        if pop.fill and pop.ppc > 0 and pop.density > 0:
+            ctx.fill_uniform(s, pop.density, pop.temperature, pop.velocity, pop.ppc, seed=seed + 101 * s)
+        else:
+            ctx.upload_particles(s, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 7)))
+    ctx.set_injectors(cf.source_injectors(cfg, seed=seed))
+    return ctx
+
+
+def _timed_steps(ctx: abi.Context, n: int) -> float:
+    import torch
+    st = torch.cuda.ExternalStream(ctx.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    ctx.step(n)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plain_ppcs=(8, 16, 32, 64, 128),
+                train_steps: int = 100, crops_per_step: int = 20, crop: int = 64, adam_steps: int = 4000,
+                lr: float = 1e-3, eval_steps: int = 100, every: int = 10, threshold: float = 0.02,
+                enforce_gate: bool = False, seed: int = 6461674, log=print) -> dict:
+    """The learned form in closed loop against a high-ppc plain check run.
+
+    1. Check run (judge_ppc, FP64 fast path, filled on the GPU) steps
+       train_steps + eval_steps. During the first train_steps it yields the
+       training pairs: after each step, crops_per_step random crop^3 crops of
+       (one in judge_ppc/low_ppc of its particles, weights scaled; all of
+       them) (rhgpu_dn_add_crops). During the last eval_steps its moments are
+       stored at every `every` steps, together with its own sampling error
+       (split-half: half of its particles against all, rhgpu_dn_add_pair with
+       factor 2).
+    2. The network is trained on the crop pairs (Adam, adam_steps), with the
+       3-voxel crop border left out of the loss.
+    3. Each low-ppc run starts from its own fill of the same initial state and
+       steps train_steps + eval_steps with the same sources: the learned form
+       (low_ppc, the denoiser between deposit and field update, the gate on)
+       and the plain FP64 path at each of plain_ppcs. At every stored step its
+       rho and J are compared with the check run's (relative L2 over the
+       grid). The gate compares the error against the truth estimate,
+       sqrt(e^2 - e_check^2), with `threshold` (against the raw error a check
+       run of J ppc fails every run once its own sampling error k/sqrt(J)
+       approaches the threshold). With enforce_gate it switches the denoiser
+       off as LearnedForm does; otherwise (the evaluation) the denoiser stays
+       on and the first step where the gate would have switched it off is
+       recorded.
+    4. Simulated seconds per wall second of each run over the evaluation
+       window (CUDA events, state resident), and the speed-up of the learned
+       form over the measured plain run with the smallest ppc whose error is
+       at most the learned form's (no interpolation).
+    """
+    lib = abi.gpu_library()
+    t_start = time.time()
+    judge_cfg = c4_config(float(judge_ppc), scale)
+    factor = judge_ppc // low_ppc
+    dn = abi.Denoiser(lib, crop, crop, crop, (0, 0, 0), pair_capacity=train_steps * crops_per_step)
+    dn.set_scales(*moment_scales(judge_cfg))
+    dn.set_params(init_params(seed % 1000))
+    dn.set_loss_border(3)
+    half = abi.Denoiser(lib, judge_cfg.nx, judge_cfg.ny, judge_cfg.nz, judge_cfg.periodic, pair_capacity=1)
+    half.set_scales(*moment_scales(judge_cfg))
+    rng = np.random.default_rng(seed)
+    judge = filled_context(lib, judge_cfg, seed)
+    n_judge = sum(judge.num_particles(s) for s in range(len(judge_cfg.populations)))
+    ref = {}
+    judge_noise = {}
+    try:
+        for st in range(train_steps):
+            judge.step(1)
+            org = np.stack([rng.integers(0, n - crop + 1, crops_per_step)
+                            for n in (judge_cfg.nx, judge_cfg.ny, judge_cfg.nz)], axis=1)
+            dn.add_crops(judge, factor, st % factor, org)
+        t_judge = 0.0
+        for st in range(eval_steps // every):
+            t_judge += _timed_steps(judge, every)
+            k = train_steps + (st + 1) * every
+            ref[k] = (judge.download_array("cellRhoQi"), judge.download_array("cellJi"))
+            half.add_pair(judge, 2, 0)
+            e = half.pair_error(0)
+            judge_noise[k] = (e["raw_rho"], e["raw_J"])
+        judge_ms = t_judge / eval_steps
+    finally:
+        judge.close()
+        half.close()
+    log(f"check run: {n_judge} ions, {judge_ms:.2f} ms/step, split-half noise {judge_noise}")
+    t0 = time.time()
+    losses = [dn.train(adam_steps // 20, lr) for _ in range(20)]
+    train_s = time.time() - t0
+    params = dn.params()
+    dn.close()
+    log(f"training: {adam_steps} Adam steps on {train_steps * crops_per_step} crop pairs, {train_s:.1f} s, "
+        f"losses {losses[0]:.4g} -> {losses[-1]:.4g}")
+
+    def run_low(ppc: int, learned: bool) -> dict:
+        cfg = c4_config(float(ppc), scale)
+        ctx = filled_context(lib, cfg, seed + 7)
+        net = None
+        try:
+            if learned:
+                net = abi.Denoiser(lib, cfg.nx, cfg.ny, cfg.nz, cfg.periodic)
+                net.set_scales(*moment_scales(cfg))
+                net.set_params(params)
+                ctx.set_denoiser(net, True)
+            ctx.step(train_steps)
+            n_ions = sum(ctx.num_particles(s) for s in range(len(cfg.populations)))
+            on = learned
+            gate_step = None
+            rows, t = [], 0.0
+            for st in range(eval_steps // every):
+                t += _timed_steps(ctx, every)
+                k = train_steps + (st + 1) * every
+                r, j = ctx.download_array("cellRhoQi"), ctx.download_array("cellJi")
+                e_r, e_j = relative_l2(r, ref[k][0]), relative_l2(j, ref[k][1])
+                n_r, n_j = judge_noise[k]
+                t_r = float(np.sqrt(max(e_r * e_r - n_r * n_r, 0.0)))
+                t_j = float(np.sqrt(max(e_j * e_j - n_j * n_j, 0.0)))
+                if learned and gate_step is None and max(t_r, t_j) > threshold:
+                    gate_step = k
+                    if enforce_gate:
+                        ctx.set_denoiser(net, False)
+                        on = False
+                rows.append({"step": k, "rho": e_r, "J": e_j, "rho_vs_truth": t_r, "J_vs_truth": t_j,
+                             "denoiser_on": on if learned else None})
+            ms = t / eval_steps
+            out = {"ppc": ppc, "learned": learned, "ions": int(n_ions), "ms_per_step": ms,
+                   "sim_s_per_wall_s": cfg.dt / (ms / 1e3), "samples": rows,
+                   "max_error": max(max(x["rho"], x["J"]) for x in rows),
+                   "max_error_vs_truth": max(max(x["rho_vs_truth"], x["J_vs_truth"]) for x in rows),
+                   "gate_would_switch_off_at": gate_step if learned else None,
+                   "gate_enforced": enforce_gate if learned else None}
+            log(f"{'learned' if learned else 'plain'} {ppc} ppc: {ms:.3f} ms/step, max error "
+                f"{out['max_error']:.4f} (vs truth {out['max_error_vs_truth']:.4f})")
+            return out
+        finally:
+            ctx.close()
+            if net is not None:
+                net.close()
+
+    learned_run = run_low(low_ppc, True)
+    plain = [run_low(p, False) for p in plain_ppcs]
+    e_l = learned_run["max_error"]
+    match = [p for p in plain if p["max_error"] <= e_l]
+    above = [p for p in plain if p["max_error"] > e_l]
+    res = {
+        "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx, "dt_s": judge_cfg.dt,
+        "check_run": {"ppc": judge_ppc, "ions": int(n_judge), "ms_per_step": judge_ms,
+                      "split_half_noise": {str(k): {"rho": v[0], "J": v[1]} for k, v in judge_noise.items()}},
+        "training": {"pairs": train_steps * crops_per_step, "crop": crop, "factor": factor, "adam_steps": adam_steps,
+                     "lr": lr, "seconds": round(train_s, 1), "losses": [round(x, 6) for x in losses]},
+        "window": {"first_step": train_steps + 1, "last_step": train_steps + eval_steps, "every": every},
+        "threshold": threshold, "learned": learned_run, "plain": plain,
+        "matched_error": None,
+        "seconds": round(time.time() - t_start, 1),
+    }
+    # plain runs at least as accurate as the learned form bound its matched-error
+    # speed-up from above (the matching ppc is at most theirs), less accurate
+    # ones from below (the learned form is both more accurate and faster)
+    res["matched_error"] = {"learned_max_error": e_l}
+    if above:
+        a = max(above, key=lambda p: p["ppc"])
+        res["matched_error"].update({
+            "speedup_lower_bound": a["ms_per_step"] / learned_run["ms_per_step"],
+            "lower_bound_plain_ppc": a["ppc"], "lower_bound_plain_error": a["max_error"]})
+    if match:
+        m = min(match, key=lambda p: p["ppc"])
+        res["matched_error"].update({
+            "speedup_upper_bound": m["ms_per_step"] / learned_run["ms_per_step"],
+            "upper_bound_plain_ppc": m["ppc"], "upper_bound_plain_error": m["max_error"]})
+    res["matched_error"]["note"] = ("measured plain runs only: the plain ppc matching the learned form's error "
+                                    "lies between the two bounds' ppc")
+    return res
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="the learned form in closed loop against a high-ppc check run")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--judge-ppc", type=int, default=256)
+    ap.add_argument("--train-steps", type=int, default=100)
+    ap.add_argument("--eval-steps", type=int, default=100)
+    ap.add_argument("--adam-steps", type=int, default=4000)
+    ap.add_argument("--plain", default="8,16,32,64,128")
+    ap.add_argument("--json", default=None)
+    a = ap.parse_args(argv)
+    out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
+                      adam_steps=a.adam_steps, plain_ppcs=tuple(int(x) for x in a.plain.split(",")))
+    print(json.dumps(out))
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
