@@ -66,6 +66,7 @@ extern "C" {
 #define RHGPU_DEVERR_FAST_PARTICLE  2u  /* particle moved more than one cell in a step */
 #define RHGPU_DEVERR_CAPACITY       4u  /* particle buffer overflow during migration */
 #define RHGPU_DEVERR_INJECT         8u  /* a particle source's rejection sampling ran out of tries */
+#define RHGPU_DEVERR_DENOISER      16u  /* a denoiser convolution's wait on its tensor-core work ran out */
 
 /* per-cell flag bits of the cell_flags array (user.cpp:1883-1941) */
 #define RHGPU_FLAG_INNER_FIELD     1u  /* innerFlagField: cell centre inside R_fieldObstacle */

@@ -1,8 +1,9 @@
 // Learned denoiser of the charge/current moments (sm_100a): a 3-layer 3D
 // convolutional network, 3x3x3 kernels, 16 channels (4 in, 4 out, residual),
 // leaky ReLU between layers, on BF16 activations with FP32 accumulation on the
-// tensor cores (mma.sync m16n8k16 bf16, A fragments by ldmatrix from a
-// shared-memory brick), forward and backward written here.
+// tensor cores, forward and backward written here: the convolutions (forward
+// and data gradient) on tcgen05.mma with the accumulators in tensor memory
+// (k_dn_conv_tc), the weight gradient on mma.sync m16n8k16 (k_dn_wgrad).
 //
 // Activations are channels-last, 16 BF16 channels per voxel (32 B), voxel
 // index v = i + nx (j + ny k); padded channels are zero. A convolution is an
@@ -35,9 +36,6 @@ struct DnGrid {
    long long N;
 };
 
-// B fragments of one layer for mma.m16n8k16 (.col): [tap][ntile][lane][2] u32,
-// b0 = W[k = 2q, 2q+1][n = g], b1 = W[k = 2q+8, 2q+9][n = g] (g = lane/4, q = lane%4)
-constexpr int DN_FRAG = DN_TAPS * 2 * 32 * 2;   // u32 per layer
 
 __device__ inline unsigned packBf16(float lo, float hi) {
    const __nv_bfloat16 a = __float2bfloat16_rn(lo), b = __float2bfloat16_rn(hi);
@@ -75,54 +73,7 @@ __device__ inline int dnNb(const DnGrid& g, DnPos p, int t, int sgn) {
    return i + g.nx * (j + g.ny * k);
 }
 
-// B fragments from FP32 weights W[27][16][16] (cin, cout); transposed: use W[t][cout][cin]
-__global__ void k_dn_frags(const float* W, unsigned* frag, int transposed) {
-   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (t, nt, lane)
-   if (e >= DN_TAPS * 2 * 32) return;
-   const int lane = e & 31, nt = (e >> 5) & 1, t = e >> 6;
-   const int g = lane >> 2, q = lane & 3;
-   const int n = nt * 8 + g;
-   auto w = [&](int k) {
-      return transposed ? W[(t * DN_C + n) * DN_C + k] : W[(t * DN_C + k) * DN_C + n];
-   };
-   frag[e * 2 + 0] = packBf16(w(2 * q), w(2 * q + 1));
-   frag[e * 2 + 1] = packBf16(w(2 * q + 8), w(2 * q + 9));
-}
-
-// One convolution layer (transposed: the data-gradient convolution, taps
-// mirrored and W transposed, no bias). A block covers a brick of DN_BX x DN_BY
-// x DN_BZ output voxels: the input brick with a one-voxel halo (zero outside a
-// non-periodic box, wrapped on periodic axes) is staged in shared memory with
-// 16-byte copies, and each warp runs 4 x-rows of 16 voxels (M) x 16 output
-// channels (two n8 tiles) over the 27 taps (K = 16 input channels per tap),
-// the A fragments read with ldmatrix. Voxel lv = hx + DN_HX (hy + DN_HY hz) of
-// the brick keeps its two 16-byte channel halves h at 16-byte slots
-// 2 lv + (h ^ bit 2 of hx): the 8 rows of an ldmatrix phase (8 consecutive hx)
-// fall on 8 different bank groups, and a tap's y/z shift keeps each lane's
-// swizzle, so the taps' addresses are a per-lane x part plus constants.
-// mode 0: out = lrelu(conv + b) as BF16; mode 1: out = conv + b as BF16;
-// mode 2: out = conv * (mask > 0 ? 1 : 1/8) as BF16 (leaky ReLU backward, mask
-// = that layer's input activation); mode 3: FP32 out (4 channels) = conv + b +
-// residual (the first 4 channels of res, FP32); mode 4: the moments mom.rho,
-// mom.J (FP64, planar) overwritten in place by (conv + b + their normalized
-// FP32 values) times the scales, rho clamped at mom.minRho. With `in` null,
-// the input is read from the moments mom: channels 0-3 = BF16(FP32(rho rsr)),
-// BF16(FP32(J rsj)), the rest zero (rsr = 1 / sr, rsj = 1 / sj, as k_dn_norm).
-struct DnMoments {
-   double* rho;    // N
-   double* J;      // 3 x N
-   double sr, sj, rsr, rsj, minRho;
-   long long N;
-};
-constexpr int DN_BX = 16, DN_BY = 8, DN_BZ = 4;                 // output brick
-constexpr int DN_HX = DN_BX + 2, DN_HY = DN_BY + 2, DN_HZ = DN_BZ + 2;
-constexpr int DN_HV = DN_HX * DN_HY * DN_HZ;                    // staged voxels
-constexpr int DN_TWARPS = 8;                                    // warps of k_dn_conv
-constexpr int DN_ROWS = DN_BY * DN_BZ / DN_TWARPS;              // x-rows per warp
-constexpr int DN_STAGE = (2 * DN_HV + 32 * DN_TWARPS - 1) / (32 * DN_TWARPS);   // 16-byte copies per thread
-static_assert(DN_BX == 16 && DN_BY * DN_BZ % DN_TWARPS == 0, "one m16 tile per brick x-row");
-
-__device__ inline int dnSlot(int hx, int lv, int h) { return 2 * lv + (h ^ ((hx >> 2) & 1)); }
+// the brick staging of a periodic or closed axis: coordinate x wrapped, or -1 outside
 __device__ inline int dnWrap(int x, int n, int per) {
    if (x >= 0 && x < n) return x;
    if (!per) return -1;
@@ -130,139 +81,313 @@ __device__ inline int dnWrap(int x, int n, int per) {
    return x < 0 ? x + n : x;
 }
 
-template <bool TRANSPOSED>
-__global__ void __launch_bounds__(32 * DN_TWARPS)
-k_dn_conv(DnGrid g, const unsigned* in, const unsigned* frag, const float* bias, int mode, unsigned* out,
-          const unsigned* mask, float* out32, const float* res, DnMoments mom) {
-   constexpr bool transposed = TRANSPOSED;
-   __shared__ __align__(16) uint4 sin[2 * DN_HV];
-   __shared__ __align__(16) unsigned sfrag[DN_FRAG];
-   const int tid = threadIdx.x;
-   const int x0 = blockIdx.x * DN_BX, y0 = blockIdx.y * DN_BY, z0 = blockIdx.z * DN_BZ;
-   {
-      const uint4* f4 = reinterpret_cast<const uint4*>(frag);
-      uint4* s4 = reinterpret_cast<uint4*>(sfrag);
-      for (int e = tid; e < DN_FRAG / 4; e += blockDim.x) s4[e] = f4[e];
-      uint4 v[DN_STAGE];
-      int slot[DN_STAGE];
-#pragma unroll
-      for (int k = 0; k < DN_STAGE; ++k) {
-         const int e = tid + 32 * DN_TWARPS * k;
-         v[k] = make_uint4(0u, 0u, 0u, 0u);
-         slot[k] = -1;
-         if (e >= 2 * DN_HV) continue;
-         const int lv = e >> 1, h = e & 1;
-         const int hx = lv % DN_HX, r = lv / DN_HX, hy = r % DN_HY, hz = r / DN_HY;
-         slot[k] = dnSlot(hx, lv, h);
-         const int x = dnWrap(x0 - 1 + hx, g.nx, g.per[0]), y = dnWrap(y0 - 1 + hy, g.ny, g.per[1]),
-                   z = dnWrap(z0 - 1 + hz, g.nz, g.per[2]);
-         if (x < 0 || y < 0 || z < 0) continue;
-         const long long gv = (long long)x + (long long)g.nx * ((long long)y + (long long)g.ny * z);
-         if (!in) {
-            if (h == 0)
-               v[k] = make_uint4(packBf16((float)(mom.rho[gv] * mom.rsr), (float)(mom.J[gv] * mom.rsj)),
-                                 packBf16((float)(mom.J[mom.N + gv] * mom.rsj), (float)(mom.J[2 * mom.N + gv] * mom.rsj)),
-                                 0u, 0u);
-         } else {
-            v[k] = reinterpret_cast<const uint4*>(in)[gv * 2 + h];
-         }
-      }
-#pragma unroll
-      for (int k = 0; k < DN_STAGE; ++k)
-         if (slot[k] >= 0) sin[slot[k]] = v[k];
+// inputs of the convolution read from the FP64 moments instead of an
+// activation (the first layer inside a step), and written back in place (the
+// last layer): rho (N) and J (3 x N, planar), their normalization and the rho floor
+struct DnMoments {
+   double* rho;    // N
+   double* J;      // 3 x N
+   double sr, sj, rsr, rsj, minRho;
+   long long N;
+};
+
+// ---- the convolution on the 5th-generation tensor cores (tcgen05) ----------------------------
+// One convolution layer as an implicit GEMM on tcgen05.mma (kind::f16, BF16 x
+// BF16 -> FP32 in tensor memory), the same arithmetic and modes as k_dn_conv
+// (forward, or TRANSPOSED: the data gradient with mirrored taps and W
+// transposed, no bias).
+//
+// A block owns a column of 30 x 8 output voxels in (x, y) and TC_ZC of its
+// z-slices. Input z-slices of 32 x-positions x 10 y-rows (one voxel of halo
+// each side) stream through a ring of 4 slots in shared memory, one plane per
+// 8-channel half with 16 bytes per voxel: any run of positions is a K-major,
+// unswizzled UMMA operand (core matrices of 8 consecutive positions x 16 bytes,
+// 128 B apart; the two channel halves one plane apart). An M-tile is 128
+// consecutive positions = 4 x-rows of one slice; the tap (dx, dy, dz) takes
+// slice z + dz and shifts the start by dx + 32 dy positions, so each tap is
+// one tcgen05.mma (M 128, N 16 output channels, K 16 input channels) on a
+// shifted A descriptor, 27 accumulating in tensor memory. Positions 0 and 31
+// of a row are the x halo: their outputs are computed and dropped. The weights
+// are staged once per block as UMMA B images (per tap N 16 x K 16 BF16,
+// K-major core matrices).
+//
+// Per output slice z: one thread issues its 2 tiles x 27 MMAs into one of two
+// tensor-memory buffers and commits them to that buffer's mbarrier; the warps
+// then take the previous slice's accumulators (tcgen05.ld, warp w its 32
+// lanes = one x-row, one voxel per thread, 16 channels) through the epilogue,
+// and slice z + 2 is copied into the slot slice z - 2 held (cp.async), while
+// the tensor cores work. Every mbarrier wait is bounded: on expiry the kernel
+// raises RHGPU_DEVERR_DENOISER in `err`, stops, and still frees its tensor
+// memory.
+constexpr int TC_HX = 32, TC_BY = 8, TC_ZC = 16;
+constexpr int TC_HY = TC_BY + 2;
+constexpr int TC_BX = TC_HX - 2;                             // output voxels per x-row
+constexpr int TC_SPOS = TC_HX * TC_HY;                       // positions of one staged slice
+constexpr int TC_PAD = 1;                                    // zero positions before and after a slice
+constexpr int TC_SLOT = (TC_SPOS + 2 * TC_PAD) * 16;         // bytes of one slice in one plane
+constexpr int TC_RING = 4;                                   // slices in shared memory
+constexpr int TC_PLANE = TC_RING * TC_SLOT;                  // bytes per channel-half plane
+constexpr int TC_TILES = TC_BY / 4;                          // M-tiles of 128 positions per slice
+constexpr int TC_COLS = 64;                                  // tensor-memory columns: 2 buffers x TC_TILES x 16
+constexpr int TC_BIMG = DN_TAPS * 512;                       // bytes of one layer's B images
+constexpr int TC_THREADS = 128;
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;               // mbarrier polls before giving up
+static_assert(2 * TC_TILES * 16 <= TC_COLS && TC_BY % 4 == 0, "two buffers of tiles fit the tensor-memory allocation");
+// a tile starts at row 1 + 4j; taps reach one row and one position either side
+static_assert(TC_HX * 0 - 1 >= -TC_PAD && TC_HX * (TC_HY - 1) + TC_HX - 1 + 1 < TC_SPOS + TC_PAD,
+              "taps stay inside the slice and its padding");
+
+struct TcShared {
+   alignas(16) unsigned char plane[2][TC_PLANE];
+   alignas(16) unsigned char bimg[TC_BIMG];
+   alignas(8) unsigned long long bar[2];
+   unsigned tmemBase;
+};
+constexpr size_t TC_SMEM = sizeof(TcShared);
+static_assert(TC_SMEM < (1u << 18), "operand addresses fit the descriptors' 14-bit start field");
+
+// UMMA B images of one layer from FP32 W[27][16 cin][16 cout]: per tap, element
+// (n, k) at byte (k / 8) * 256 + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+// B(n, k) = W[t][k][n] (forward) or W[t][n][k] (transposed)
+__global__ void k_dn_bimage(const float* W, __nv_bfloat16* img, int transposed) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (t, n, k)
+   if (e >= DN_TAPS * DN_C * DN_C) return;
+   const int k = e % DN_C, n = (e / DN_C) % DN_C, t = e / (DN_C * DN_C);
+   const float w = transposed ? W[(t * DN_C + n) * DN_C + k] : W[(t * DN_C + k) * DN_C + n];
+   img[t * 256 + (k / 8) * 128 + (n / 8) * 64 + (n % 8) * 8 + (k % 8)] = __float2bfloat16_rn(w);
+}
+
+__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+   // start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46), version 1 [46,48), no swizzle
+   return (unsigned long long)((addr >> 4) & 0x3fffu) | ((unsigned long long)((lbo >> 4) & 0x3fffu) << 16) |
+          ((unsigned long long)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, N = 16, M = 128
+constexpr unsigned TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ bool tcWait(unsigned bar, unsigned parity) {
+   for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
+      unsigned ok;
+      asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                   "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                   : "=r"(ok)
+                   : "r"(bar), "r"(parity)
+                   : "memory");
+      if (ok) return true;
    }
+   return false;
+}
+
+// input slice zz into ring slot `slot`: 32 x 10 positions from (x0 - 1, y0 - 1),
+// zeros outside a non-periodic box, wrapped on periodic axes
+__device__ __forceinline__ void tcStageSlice(TcShared& sh, const DnGrid& g, const unsigned* in, const DnMoments& mom,
+                                             int x0, int y0, int zz, int slot) {
+   const int z = dnWrap(zz, g.nz, g.per[2]);
+   for (int e = threadIdx.x; e < 2 * TC_SPOS; e += TC_THREADS) {
+      const int p = e >> 1, h = e & 1;
+      const int hx = p % TC_HX, hy = p / TC_HX;
+      const int x = dnWrap(x0 - 1 + hx, g.nx, g.per[0]), y = dnWrap(y0 - 1 + hy, g.ny, g.per[1]);
+      unsigned char* dst = &sh.plane[h][slot * TC_SLOT + 16 * (TC_PAD + p)];
+      const bool ok = x >= 0 && y >= 0 && z >= 0;
+      const long long gv = ok ? (long long)x + (long long)g.nx * ((long long)y + (long long)g.ny * z) : 0;
+      if (in) {
+         cpAsync16(dst, reinterpret_cast<const uint4*>(in) + (gv * 2 + h), ok ? 16 : 0);
+      } else {
+         uint4 v = make_uint4(0u, 0u, 0u, 0u);
+         if (ok && h == 0)
+            v = make_uint4(packBf16((float)(mom.rho[gv] * mom.rsr), (float)(mom.J[gv] * mom.rsj)),
+                           packBf16((float)(mom.J[mom.N + gv] * mom.rsj), (float)(mom.J[2 * mom.N + gv] * mom.rsj)),
+                           0u, 0u);
+         *reinterpret_cast<uint4*>(dst) = v;
+      }
+   }
+   cpAsyncCommit();
+}
+
+// the staged data (generic-proxy and cp.async writes) made visible to the
+// tensor cores and to every thread; PENDING: cp.async groups of this thread
+// that may stay in flight (the newest ones)
+template <int PENDING>
+__device__ __forceinline__ void tcPublish() {
+   asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
    __syncthreads();
-   const int lane = tid & 31, warp = tid >> 5;
-   const int gq = lane >> 2, q = lane & 3;
-   const int lr = lane & 15, lh = lane >> 4;   // ldmatrix: this lane's row and channel half
-   const unsigned sbase = (unsigned)__cvta_generic_to_shared(sin);
+   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+template <bool TRANSPOSED>
+__device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int buf, int x0, int y0, int z,
+                                           const float* bias, int mode, unsigned* out, const unsigned* mask,
+                                           float* out32, const float* res, const DnMoments& mom) {
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   unsigned rr[TC_TILES][16];
+#pragma unroll
+   for (int j = 0; j < TC_TILES; ++j) {
+      unsigned* r = rr[j];
+      const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + 16u * (unsigned)(buf * TC_TILES + j);
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                     "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                   : "r"(taddr));
+   }
+   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+   for (int j = 0; j < TC_TILES; ++j) {
+      const unsigned* r = rr[j];
+      const int x = x0 - 1 + lane, y = y0 + 4 * j + warp;
+      if (lane < 1 || lane > TC_BX || x >= g.nx || y >= g.ny) continue;
+      const long long v = (long long)x + (long long)g.nx * ((long long)y + (long long)g.ny * z);
+      float c[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) c[k] = __uint_as_float(r[k]);
+      if (!TRANSPOSED && bias)
+#pragma unroll
+         for (int k = 0; k < 16; ++k) c[k] += bias[k];
+      if (mode == 0)
+#pragma unroll
+         for (int k = 0; k < 16; ++k) c[k] = c[k] > 0.f ? c[k] : DN_LEAK * c[k];
+      if (mode == 2) {
+         const uint4 m0 = reinterpret_cast<const uint4*>(mask)[v * 2], m1 = reinterpret_cast<const uint4*>(mask)[v * 2 + 1];
+         const unsigned mw[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+#pragma unroll
+         for (int k = 0; k < 8; ++k) {
+            if (!(bf16lo(mw[k]) > 0.f)) c[2 * k] *= DN_LEAK;
+            if (!(bf16hi(mw[k]) > 0.f)) c[2 * k + 1] *= DN_LEAK;
+         }
+      }
+      if (mode == 3) {
+#pragma unroll
+         for (int k = 0; k < 4; ++k) out32[v * 4 + k] = c[k] + res[v * 4 + k];
+         continue;
+      }
+      if (mode == 4) {
+         double r0 = (double)(c[0] + (float)(mom.rho[v] * mom.rsr)) * mom.sr;
+         if (r0 < mom.minRho) r0 = mom.minRho;
+         const double j0 = (double)(c[1] + (float)(mom.J[v] * mom.rsj)) * mom.sj;
+         const double j1 = (double)(c[2] + (float)(mom.J[mom.N + v] * mom.rsj)) * mom.sj;
+         const double j2 = (double)(c[3] + (float)(mom.J[2 * mom.N + v] * mom.rsj)) * mom.sj;
+         mom.rho[v] = r0;
+         mom.J[v] = j0;
+         mom.J[mom.N + v] = j1;
+         mom.J[2 * mom.N + v] = j2;
+         continue;
+      }
+      uint4* o = reinterpret_cast<uint4*>(out) + v * 2;
+      o[0] = make_uint4(packBf16(c[0], c[1]), packBf16(c[2], c[3]), packBf16(c[4], c[5]), packBf16(c[6], c[7]));
+      o[1] = make_uint4(packBf16(c[8], c[9]), packBf16(c[10], c[11]), packBf16(c[12], c[13]), packBf16(c[14], c[15]));
+   }
+}
+
+template <bool TRANSPOSED>
+__global__ void __launch_bounds__(TC_THREADS)
+k_dn_conv_tc(DnGrid g, const unsigned* in, const __nv_bfloat16* bimg, const float* bias, int mode, unsigned* out,
+             const unsigned* mask, float* out32, const float* res, DnMoments mom, unsigned* err) {
+   extern __shared__ __align__(16) unsigned char tcSmemRaw[];
+   TcShared& sh = *reinterpret_cast<TcShared*>(tcSmemRaw);
+   const int tid = threadIdx.x, warp = tid >> 5;
+   const int x0 = blockIdx.x * TC_BX, y0 = blockIdx.y * TC_BY, z0 = blockIdx.z * TC_ZC;
+   const int nzc = min(TC_ZC, g.nz - z0);
+   const unsigned planeBase = (unsigned)__cvta_generic_to_shared(&sh.plane[0][0]);
+   const unsigned bimgBase = (unsigned)__cvta_generic_to_shared(&sh.bimg[0]);
+   // tensor memory (one warp), mbarriers (one thread)
+   if (warp == 0) {
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(&sh.tmemBase);
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(TC_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+   }
+   if (tid == 0) {
+      for (int j = 0; j < 2; ++j) {
+         const unsigned b = (unsigned)__cvta_generic_to_shared(&sh.bar[j]);
+         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1));
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   // the weights, the slices' zero padding, and input slices z0 - 1 .. z0 + 1 (ring slots 0-2)
+   {
+      const uint4* src = reinterpret_cast<const uint4*>(bimg);
+      for (int e = tid; e < TC_BIMG / 16; e += TC_THREADS) cpAsync16(&sh.bimg[16 * e], src + e, 16);
+      for (int e = tid; e < 2 * TC_RING * 2 * TC_PAD; e += TC_THREADS) {
+         const int h = e / (TC_RING * 2 * TC_PAD), q = e % (TC_RING * 2 * TC_PAD);
+         const int slot = q / (2 * TC_PAD), k = q % (2 * TC_PAD);
+         const int pos = k < TC_PAD ? k : TC_PAD + TC_SPOS + (k - TC_PAD);
+         *reinterpret_cast<uint4*>(&sh.plane[h][slot * TC_SLOT + 16 * pos]) = make_uint4(0u, 0u, 0u, 0u);
+      }
+      for (int k = 0; k < 3; ++k) tcStageSlice(sh, g, in, mom, x0, y0, z0 - 1 + k, k);
+   }
+   tcPublish<0>();
+   const unsigned tmem = sh.tmemBase;
    constexpr int sgn = TRANSPOSED ? -1 : 1;
-   // byte offsets: x part of this lane at hx = lr + dx + 1 (dx = -1, 0, 1), and of each row
-   unsigned xo[3];
+   bool timedOut = false;
+   for (int i = 0; i < nzc && !timedOut; ++i) {
+      // slice zz is in slot (zz - z0 + 1) mod TC_RING: slices z - 1 .. z + 1 (z = z0 + i) are
+      // in slots i .. i + 2; slice z + 2 is requested below as soon as its slot is free
+      const int buf = i & 1;
+      if (tid == 0) {
+         // descriptors: the low word holds the start address >> 4 (14 bits, no carry into LBO
+         // for shared addresses below 256 KB), so a tap's descriptor is a base plus a constant
+         const unsigned long long a0 = umma_desc(planeBase, TC_PLANE, 128);
+         const unsigned long long b0 = umma_desc(bimgBase, 256, 128);
+         unsigned slotLo[3];
 #pragma unroll
-   for (int d = 0; d < 3; ++d) {
-      const int hx = lr + d;
-      xo[d] = sbase + 16u * (unsigned)(2 * hx + (lh ^ ((hx >> 2) & 1)));
+         for (int q = 0; q < 3; ++q) {
+            const int dzq = sgn * (q - 1);
+            slotLo[q] = (unsigned)a0 + (unsigned)(((i + 1 + dzq) % TC_RING) * (TC_SLOT >> 4));
+         }
+         const unsigned aHi = (unsigned)(a0 >> 32), bHi = (unsigned)(b0 >> 32), bLo = (unsigned)b0;
+#pragma unroll
+         for (int j = 0; j < TC_TILES; ++j) {
+            const unsigned d = tmem + 16u * (unsigned)(buf * TC_TILES + j);
+#pragma unroll
+            for (int t = 0; t < DN_TAPS; ++t) {
+               const int dx = sgn * (t % 3 - 1), dy = sgn * ((t / 3) % 3 - 1);
+               const int pos = TC_PAD + TC_HX * (1 + 4 * j + dy) + dx;   // compile-time
+               const unsigned aLo = slotLo[t / 9] + (unsigned)pos;       // 16-byte units
+               const unsigned long long ad = ((unsigned long long)aHi << 32) | aLo;
+               const unsigned long long bd = ((unsigned long long)bHi << 32) | (bLo + 32u * (unsigned)t);
+               asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                            :
+                            : "r"(d), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(t > 0 ? 1 : 0), "r"(0), "r"(0), "r"(0),
+                              "r"(0));
+            }
+         }
+         const unsigned b = (unsigned)__cvta_generic_to_shared(&sh.bar[buf]);
+         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b) : "memory");
+      }
+      if (i > 0) {
+         // the previous slice's MMAs done: its slot z - 2 takes slice z + 2 (requested now, so
+         // that the copy runs during the epilogue), its accumulators go through the epilogue
+         const int pb = (i - 1) & 1;
+         if (!tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[pb]), (unsigned)(((i - 1) >> 1) & 1))) {
+            timedOut = true;
+         } else {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (i + 2 <= nzc) tcStageSlice(sh, g, in, mom, x0, y0, z0 + i + 2, (i + 3) % TC_RING);
+            tcEpilogue<TRANSPOSED>(g, tmem, pb, x0, y0, z0 + i - 1, bias, mode, out, mask, out32, res, mom);
+         }
+      } else if (i + 2 <= nzc) {
+         tcStageSlice(sh, g, in, mom, x0, y0, z0 + 2, 3 % TC_RING);   // slot 3 is still free
+      }
+      timedOut = __syncthreads_or(timedOut);
+      tcPublish<0>();
    }
-   unsigned ro[DN_ROWS];
-#pragma unroll
-   for (int r = 0; r < DN_ROWS; ++r) {
-      const int row = warp * DN_ROWS + r, ry = row % DN_BY, rz = row / DN_BY;
-      ro[r] = 32u * (unsigned)(DN_HX * ((ry + 1) + DN_HY * (rz + 1)));
-   }
-   float c[DN_ROWS][2][4];
-#pragma unroll
-   for (int r = 0; r < DN_ROWS; ++r)
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) c[r][nt][0] = c[r][nt][1] = c[r][nt][2] = c[r][nt][3] = 0.f;
-#pragma unroll
-   for (int t = 0; t < DN_TAPS; ++t) {
-      const int dx = sgn * (t % 3 - 1), dy = sgn * ((t / 3) % 3 - 1), dz = sgn * (t / 9 - 1);
-      const int tyz = 32 * DN_HX * (dy + DN_HY * dz);   // byte offset of the tap's y/z shift
-      const unsigned* f = sfrag + (t * 2) * 64;
-      const uint2 bf0 = *reinterpret_cast<const uint2*>(f + lane * 2);
-      const uint2 bf1 = *reinterpret_cast<const uint2*>(f + 64 + lane * 2);
-#pragma unroll
-      for (int r = 0; r < DN_ROWS; ++r) {
-         const unsigned addr = xo[dx + 1] + ro[r] + (unsigned)tyz;
-         unsigned a[4];
-         asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                      : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
-                      : "r"(addr));
-         mma16816(c[r][0], a, bf0.x, bf0.y);
-         mma16816(c[r][1], a, bf1.x, bf1.y);
+   if (!timedOut) {
+      const int lb = (nzc - 1) & 1;
+      if (!tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[lb]), (unsigned)(((nzc - 1) >> 1) & 1))) {
+         timedOut = true;
+      } else {
+         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+         tcEpilogue<TRANSPOSED>(g, tmem, lb, x0, y0, z0 + nzc - 1, bias, mode, out, mask, out32, res, mom);
       }
    }
-   // c[r][nt][0,1]: voxel x = gq, channels nt*8 + 2q, +1; c[r][nt][2,3]: x = gq + 8
-#pragma unroll
-   for (int r = 0; r < DN_ROWS; ++r) {
-      const int row = warp * DN_ROWS + r, y = y0 + row % DN_BY, z = z0 + row / DN_BY;
-      if (y >= g.ny || z >= g.nz) continue;
-      const long long rowv = (long long)g.nx * ((long long)y + (long long)g.ny * z);
-      const bool oka = x0 + gq < g.nx, okb = x0 + gq + 8 < g.nx;
-      const long long va = rowv + x0 + gq, vb = va + 8;
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) {
-         const int ch = nt * 8 + 2 * q;
-         float x0v = c[r][nt][0], x1v = c[r][nt][1], x2v = c[r][nt][2], x3v = c[r][nt][3];
-         if (!transposed && bias) { x0v += bias[ch]; x1v += bias[ch + 1]; x2v += bias[ch]; x3v += bias[ch + 1]; }
-         if (mode == 0) {
-            x0v = x0v > 0.f ? x0v : DN_LEAK * x0v; x1v = x1v > 0.f ? x1v : DN_LEAK * x1v;
-            x2v = x2v > 0.f ? x2v : DN_LEAK * x2v; x3v = x3v > 0.f ? x3v : DN_LEAK * x3v;
-         }
-         if (mode == 2) {
-            // leaky ReLU backward: the activation's sign is its input's sign
-            if (oka) { const unsigned m = mask[va * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x0v *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x1v *= DN_LEAK; }
-            if (okb) { const unsigned m = mask[vb * 8 + nt * 4 + q]; if (!(bf16lo(m) > 0.f)) x2v *= DN_LEAK; if (!(bf16hi(m) > 0.f)) x3v *= DN_LEAK; }
-         }
-         if (mode == 3) {
-            if (nt == 0 && q < 2) {
-               if (oka) { out32[va * 4 + ch] = x0v + res[va * 4 + ch]; out32[va * 4 + ch + 1] = x1v + res[va * 4 + ch + 1]; }
-               if (okb) { out32[vb * 4 + ch] = x2v + res[vb * 4 + ch]; out32[vb * 4 + ch + 1] = x3v + res[vb * 4 + ch + 1]; }
-            }
-            continue;
-         }
-         if (mode == 4) {
-            // channels ch, ch + 1 of voxels va, vb: (rho, Jx) for q = 0, (Jy, Jz) for q = 1
-            if (nt == 0 && q < 2) {
-               double* p0 = q == 0 ? mom.rho : mom.J + mom.N;
-               double* p1 = q == 0 ? mom.J : mom.J + 2 * mom.N;
-               const double s0 = q == 0 ? mom.sr : mom.sj, rs0 = q == 0 ? mom.rsr : mom.rsj;
-               auto put = [&](long long v, float y0, float y1) {
-                  double r0 = (double)(y0 + (float)(p0[v] * rs0)) * s0;
-                  const double r1 = (double)(y1 + (float)(p1[v] * mom.rsj)) * mom.sj;
-                  if (q == 0 && r0 < mom.minRho) r0 = mom.minRho;
-                  p0[v] = r0;
-                  p1[v] = r1;
-               };
-               if (oka) put(va, x0v, x1v);
-               if (okb) put(vb, x2v, x3v);
-            }
-            continue;
-         }
-         if (oka) out[va * 8 + nt * 4 + q] = packBf16(x0v, x1v);
-         if (okb) out[vb * 8 + nt * 4 + q] = packBf16(x2v, x3v);
-      }
+   if (timedOut && tid == 0) raiseError(err, RHGPU_DEVERR_DENOISER);
+   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+   __syncthreads();
+   if (warp == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS));
    }
 }
 

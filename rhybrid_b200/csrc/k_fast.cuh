@@ -448,6 +448,11 @@ __device__ __forceinline__ void cpAsync8(void* sdst, const void* gsrc, int bytes
    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
 }
+// 16-byte form (both addresses 16-byte aligned)
+__device__ __forceinline__ void cpAsync16(void* sdst, const void* gsrc, int bytes) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 

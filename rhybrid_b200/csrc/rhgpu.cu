@@ -275,7 +275,8 @@ struct rhgpu_dn {
    float* m = nullptr;                   // Adam moments
    float* v = nullptr;
    unsigned char* mask = nullptr;        // trainable entries
-   unsigned* frag = nullptr;             // 3 layers forward + 3 transposed, DN_FRAG each
+   __nv_bfloat16* bimg = nullptr;        // UMMA B images: 3 layers forward + 3 transposed, TC_BIMG bytes each
+   unsigned* err = nullptr;              // device error word of the convolutions (RHGPU_DEVERR_DENOISER)
    unsigned* act[3] = {};                // BF16 inputs of layers 0..2 (16 channels)
    unsigned* dY[3] = {};                 // BF16 output gradients of layers 0..2
    float* res = nullptr;                 // normalized FP32 input (N x 4)
@@ -1531,20 +1532,48 @@ namespace {
 
 const int DN_LOSS_BLOCKS = 296;
 
-int dnRebuildFrags(rhgpu_dn* d) {
-   for (int l = 0; l < 3; ++l) {
-      k_dn_frags<<<(DN_TAPS * 64 + 255) / 256, 256, 0, d->stream>>>(d->params + (size_t)l * DN_LAYER, d->frag + (size_t)l * DN_FRAG, 0);
-      k_dn_frags<<<(DN_TAPS * 64 + 255) / 256, 256, 0, d->stream>>>(d->params + (size_t)l * DN_LAYER,
-                                                                   d->frag + (size_t)(3 + l) * DN_FRAG, 1);
-   }
+// the UMMA B images of every layer (forward and transposed) from the FP32 parameters
+int dnRebuildImages(rhgpu_dn* d) {
+   for (int l = 0; l < 3; ++l)
+      for (int tr = 0; tr < 2; ++tr)
+         k_dn_bimage<<<(DN_TAPS * DN_C * DN_C + 255) / 256, 256, 0, d->stream>>>(
+             d->params + (size_t)l * DN_LAYER, d->bimg + (size_t)(3 * tr + l) * (TC_BIMG / 2), tr);
    RH_CUDA(cudaGetLastError());
    return RHGPU_OK;
 }
 
-// convolution blocks: one per output brick
-dim3 dnConvBlocks(const rhgpu_dn* d) {
-   return dim3((unsigned)((d->g.nx + DN_BX - 1) / DN_BX), (unsigned)((d->g.ny + DN_BY - 1) / DN_BY),
-               (unsigned)((d->g.nz + DN_BZ - 1) / DN_BZ));
+// one convolution layer on the tensor cores (k_dn_conv_tc): layer l, forward or
+// transposed (the data gradient); `err` receives RHGPU_DEVERR_DENOISER
+int dnConv(rhgpu_dn* d, cudaStream_t st, bool transposed, int l, const unsigned* in, const float* bias, int mode,
+           unsigned* out, const unsigned* mask, float* out32, const float* res, const DnMoments& mom, unsigned* err) {
+   static bool raised[64][2] = {};
+   if (d->device < 0 || d->device >= 64) return fail(RHGPU_ERR_CUDA, "denoiser: device index out of range");
+   if (!raised[d->device][transposed]) {
+      RH_CUDA(cudaFuncSetAttribute(transposed ? k_dn_conv_tc<true> : k_dn_conv_tc<false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+      raised[d->device][transposed] = true;
+   }
+   const dim3 grid((unsigned)((d->g.nx + TC_BX - 1) / TC_BX), (unsigned)((d->g.ny + TC_BY - 1) / TC_BY),
+                   (unsigned)((d->g.nz + TC_ZC - 1) / TC_ZC));
+   const __nv_bfloat16* img = d->bimg + (size_t)((transposed ? 3 : 0) + l) * (TC_BIMG / 2);
+   if (transposed)
+      k_dn_conv_tc<true><<<grid, TC_THREADS, TC_SMEM, st>>>(d->g, in, img, bias, mode, out, mask, out32, res, mom, err);
+   else
+      k_dn_conv_tc<false><<<grid, TC_THREADS, TC_SMEM, st>>>(d->g, in, img, bias, mode, out, mask, out32, res, mom, err);
+   RH_CUDA(cudaGetLastError());
+   return RHGPU_OK;
+}
+
+// the convolutions' device error word, read and cleared (after a synchronisation of d->stream)
+int dnCheckError(rhgpu_dn* d) {
+   unsigned w = 0;
+   RH_CUDA(cudaMemcpyAsync(&w, d->err, sizeof w, cudaMemcpyDeviceToHost, d->stream));
+   RH_CUDA(cudaStreamSynchronize(d->stream));
+   if (w) {
+      RH_CUDA(cudaMemsetAsync(d->err, 0, sizeof w, d->stream));
+      return fail(RHGPU_ERR_DEVICE, "denoiser: a convolution's wait on its tensor-core work ran out");
+   }
+   return RHGPU_OK;
 }
 
 // forward of the network on d->res (normalized FP32 input) into d->out32
@@ -1554,13 +1583,10 @@ int dnForward(rhgpu_dn* d) {
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[0], d->frag, b0, 0, d->act[1], nullptr, nullptr, nullptr, DnMoments{});
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, d->act[2], nullptr,
-                                                              nullptr, nullptr, DnMoments{});
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 3, nullptr,
-                                                              nullptr, d->out32, d->res, DnMoments{});
-   RH_CUDA(cudaGetLastError());
-   return RHGPU_OK;
+   int rc = dnConv(d, d->stream, false, 0, d->act[0], b0, 0, d->act[1], nullptr, nullptr, nullptr, DnMoments{}, d->err);
+   if (!rc) rc = dnConv(d, d->stream, false, 1, d->act[1], b1, 0, d->act[2], nullptr, nullptr, nullptr, DnMoments{}, d->err);
+   if (!rc) rc = dnConv(d, d->stream, false, 2, d->act[2], b2, 3, nullptr, nullptr, d->out32, d->res, DnMoments{}, d->err);
+   return rc;
 }
 
 // loss against target (normalized FP32, N x 4) and the gradient of all parameters into d->grad
@@ -1581,9 +1607,9 @@ int dnBackward(rhgpu_dn* d, const float* target, double* loss) {
       k_dn_bgrad<<<wb, 256, 0, d->stream>>>(d->g, d->dY[l], d->part);
       k_dn_reduce_rows<<<1, DN_C, 0, d->stream>>>(d->part, wb, DN_C, d->grad + (size_t)l * DN_LAYER + DN_TAPS * DN_C * DN_C);
       if (l > 0)
-         k_dn_conv<true><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, d->stream>>>(d->g, d->dY[l], d->frag + (size_t)(3 + l) * DN_FRAG, nullptr,
-                                                                    2, d->dY[l - 1], d->act[l], nullptr, nullptr,
-                                                                    DnMoments{});
+         if (int rc = dnConv(d, d->stream, true, l, d->dY[l], nullptr, 2, d->dY[l - 1], d->act[l], nullptr, nullptr,
+                             DnMoments{}, d->err))
+            return rc;
    }
    RH_CUDA(cudaGetLastError());
    std::vector<double> lp(DN_LOSS_BLOCKS);
@@ -1612,25 +1638,22 @@ int dnUploadMoments(rhgpu_dn* d, const double* rho, const double* ji, double* pl
 // the network on planar device moments (rho N, J 3 x N), in place: the first layer
 // reads and normalizes them, the last adds its output to their normalized values
 // and scales back (rho clamped at minRho), in three launches
-int dnApplyMoments(rhgpu_dn* d, cudaStream_t st, double* rho, double* J, double minRho) {
+int dnApplyMoments(rhgpu_dn* d, cudaStream_t st, double* rho, double* J, double minRho, unsigned* err) {
    const long long N = d->g.N;
    const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N};
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, nullptr, d->frag, b0, 0, d->act[1], nullptr, nullptr,
-                                                        nullptr, mom);
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, d->act[1], d->frag + DN_FRAG, b1, 0, d->act[2], nullptr,
-                                                        nullptr, nullptr, DnMoments{});
-   k_dn_conv<false><<<dnConvBlocks(d), 32 * DN_TWARPS, 0, st>>>(d->g, d->act[2], d->frag + 2 * DN_FRAG, b2, 4, nullptr,
-                                                        nullptr, nullptr, nullptr, mom);
-   return cudaGetLastError() != cudaSuccess ? fail(RHGPU_ERR_CUDA, "dn_apply: launch") : RHGPU_OK;
+   int rc = dnConv(d, st, false, 0, nullptr, b0, 0, d->act[1], nullptr, nullptr, nullptr, mom, err);
+   if (!rc) rc = dnConv(d, st, false, 1, d->act[1], b1, 0, d->act[2], nullptr, nullptr, nullptr, DnMoments{}, err);
+   if (!rc) rc = dnConv(d, st, false, 2, d->act[2], b2, 4, nullptr, nullptr, nullptr, nullptr, mom, err);
+   return rc;
 }
 
 // the denoiser on the context's moments (device, on the context's stream), before the field update
 int dnApplyCtx(rhgpu_ctx* c) {
    RH_TIME(c, "dn_apply");
-   return dnApplyMoments(c->dn, c->stream, c->f.cellRho, c->f.cellJi, c->P.min_ion_charge_density);
+   return dnApplyMoments(c->dn, c->stream, c->f.cellRho, c->f.cellJi, c->P.min_ion_charge_density, c->err);
 }
 
 }  // namespace
@@ -2944,7 +2967,8 @@ int rhgpu_dn_create(int32_t nx, int32_t ny, int32_t nz, const int32_t* periodic,
    alloc((void**)&d->m, sizeof(float) * DN_PARAMS);
    alloc((void**)&d->v, sizeof(float) * DN_PARAMS);
    alloc((void**)&d->mask, DN_PARAMS);
-   alloc((void**)&d->frag, sizeof(unsigned) * 6 * DN_FRAG);
+   alloc((void**)&d->bimg, 6 * (size_t)TC_BIMG);
+   alloc((void**)&d->err, sizeof(unsigned));
    for (int l = 0; l < 3; ++l) {
       alloc((void**)&d->act[l], sizeof(unsigned) * 8 * N);
       alloc((void**)&d->dY[l], sizeof(unsigned) * 8 * N);
@@ -2983,7 +3007,7 @@ int rhgpu_dn_destroy(rhgpu_dn* d) {
    if (!d) return RHGPU_OK;
    cudaSetDevice(d->device);
    if (d->stream) cudaStreamSynchronize(d->stream);
-   cudaFree(d->params); cudaFree(d->grad); cudaFree(d->m); cudaFree(d->v); cudaFree(d->mask); cudaFree(d->frag);
+   cudaFree(d->params); cudaFree(d->grad); cudaFree(d->m); cudaFree(d->v); cudaFree(d->mask); cudaFree(d->bimg); cudaFree(d->err);
    for (int l = 0; l < 3; ++l) { cudaFree(d->act[l]); cudaFree(d->dY[l]); }
    cudaFree(d->res); cudaFree(d->out32); cudaFree(d->part); cudaFree(d->lossPart); cudaFree(d->acc);
    cudaFree(d->pairIn); cudaFree(d->pairOut);
@@ -3004,7 +3028,7 @@ int rhgpu_dn_set_params(rhgpu_dn* d, const float* p, int64_t n) {
    RH_CUDA(cudaMemsetAsync(d->m, 0, sizeof(float) * n, d->stream));
    RH_CUDA(cudaMemsetAsync(d->v, 0, sizeof(float) * n, d->stream));
    d->adamStep = 0;
-   int rc = dnRebuildFrags(d);
+   int rc = dnRebuildImages(d);
    if (rc) return rc;
    RH_CUDA(cudaStreamSynchronize(d->stream));
    return RHGPU_OK;
@@ -3031,7 +3055,8 @@ int rhgpu_dn_apply(rhgpu_dn* d, const double* rho_in, const double* ji_in, doubl
    const long long N = d->g.N;
    int rc = dnUploadMoments(d, rho_in, ji_in, d->acc);
    if (rc) return rc;
-   rc = dnApplyMoments(d, d->stream, d->acc, d->acc + N, min_rho);
+   rc = dnApplyMoments(d, d->stream, d->acc, d->acc + N, min_rho, d->err);
+   if (!rc) rc = dnCheckError(d);
    if (rc) return rc;
    std::vector<double> h(4 * (size_t)N);
    RH_CUDA(cudaMemcpyAsync(h.data(), d->acc, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, d->stream));
@@ -3063,6 +3088,7 @@ int rhgpu_dn_loss_grad(rhgpu_dn* d, const double* rho_in, const double* ji_in, c
    float* tcopy = reinterpret_cast<float*>(d->acc);
    RH_CUDA(cudaMemcpyAsync(tcopy, target, sizeof(float) * 4 * N, cudaMemcpyDeviceToDevice, d->stream));
    rc = dnBackward(d, tcopy, loss);
+   if (!rc) rc = dnCheckError(d);
    if (rc) return rc;
    if (grad) {
       RH_CUDA(cudaMemcpyAsync(grad, d->grad, sizeof(float) * DN_PARAMS, cudaMemcpyDeviceToHost, d->stream));
@@ -3181,10 +3207,11 @@ int rhgpu_dn_train(rhgpu_dn* d, int32_t iterations, float lr, double* mean_loss)
       const float c1 = 1.f - std::pow(b1, (float)d->adamStep), c2 = 1.f - std::pow(b2, (float)d->adamStep);
       k_dn_adam<<<(DN_PARAMS + 255) / 256, 256, 0, d->stream>>>(d->params, d->grad, d->m, d->v, d->mask, DN_PARAMS, lr, b1, b2,
                                                                eps, c1, c2);
-      rc = dnRebuildFrags(d);
+      rc = dnRebuildImages(d);
       if (rc) return rc;
    }
    RH_CUDA(cudaStreamSynchronize(d->stream));
+   if (int rc = dnCheckError(d)) return rc;
    if (mean_loss) *mean_loss = iterations ? tot / iterations : 0.0;
    return RHGPU_OK;
 }
