@@ -860,8 +860,10 @@ __global__ void k_fast_fold_boundary(GridInfo g, FastGeom fg, FastBufs fb) {
 }
 
 // destination moments: four row partials (boundary partials folded in) +
-// fixed-point part, then finalize. The touched word and the four row
-// partials (16-byte loads) are all requested before any sum.
+// fixed-point part, then finalize. The touched word, the four row partials
+// (16-byte loads) and the fixed-point sums are all requested before any sum:
+// most cells are touched by some mover, and waiting for the touched word
+// before loading the sums would add a second dependent round trip.
 template <bool GC>   // GC: also count the rho clamp per cell (grid counters on)
 __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, double hiR, double loR, double hiJ,
                               double loJ, double minRho, unsigned long long* cnt) {
@@ -885,9 +887,15 @@ __global__ void k_fast_gather(GridInfo g, Fields f, FastGeom fg, FastBufs fb, do
       v[2] = v[2] + rp[qq][1].x;
       v[3] = v[3] + rp[qq][1].y;
    }
+   unsigned long long mlo[4], mhi[4];
+#pragma unroll
+   for (int l = 0; l < 4; ++l) {
+      mlo[l] = fb.MMlo[l * N + n];
+      mhi[l] = fb.MMhi[l * N + n];
+   }
    if (tw & (1u << (n & 31))) {
-      v[0] += fixedToDouble(fb.MMlo[n], fb.MMhi[n], hiR, loR);
-      for (int l = 0; l < 3; ++l) v[1 + l] += fixedToDouble(fb.MMlo[(1 + l) * N + n], fb.MMhi[(1 + l) * N + n], hiJ, loJ);
+      v[0] += fixedToDouble(mlo[0], mhi[0], hiR, loR);
+      for (int l = 0; l < 3; ++l) v[1 + l] += fixedToDouble(mlo[1 + l], mhi[1 + l], hiJ, loJ);
       for (int l = 0; l < 4; ++l) { fb.MMlo[l * N + n] = 0ull; fb.MMhi[l * N + n] = 0ull; }
    }
    double rho = v[0] / g.dV;

@@ -1,18 +1,18 @@
 // Field update propagateB (RHybrid src/hybrid_propagator.cpp:42-440) as
-// per-cell FP64 stencil kernels for sm_100a. Each kernel restates one or
-// more of the reference's per-block routines with the reference's operation
-// order, so that with --fmad=false the results are bitwise identical:
+// FP64 stencil kernels for sm_100a. Each kernel restates one or more of the
+// reference's per-block routines with the reference's operation order, so
+// that with --fmad=false the results are bitwise identical:
 //   k_face2cell          face2Cell                        (:1043-1056)
-//   k_ext_cell_bc        neumannCell x3 + setIMFCell      (:443-655, :910-977)
-//   k_cell2node_avg      cell2Node of B, rhoq, Ji + cellAverageB (:1059-1089, :157-167)
-//   k_ext_face_bc        neumannFace + setIMFFace         (:659-908, :979-1040)
-//   k_node_j             calcNodeJ (USE_EDGE_J)           (:1449-1522)
-//   k_cell_j_ue          node2Cell(J) + calcCellUe        (:1092-1112, :1342-1387)
+//   k_ext_bc             neumannCell x3 + setIMFCell, neumannFace + setIMFFace
+//                        (:443-908, :910-1040)
+//   k_node_fused         cell2Node of B, rhoq, Ji + cellAverageB, calcNodeJ
+//                        (USE_EDGE_J), calcNodeUe, upwindNodeB, calcNodeE
+//                        (:1059-1089, :157-167, :1449-1522, :1524-1584, :1268-1339, :1392-1446)
+//   k_cell_fused         node2Cell(J) + calcCellUe, calcCellEp, faceCurl
+//                        (:1092-1112, :1342-1387, :1674-1737, :1587-1671)
 //   k_ext_cell_neumann3  neumannCell of one 3-vector      (:443-655)
-//   k_node_ue_b_e        calcNodeUe + upwindNodeB + calcNodeE (:1524-1584, :1268-1339, :1392-1446)
-//   k_node2cell3, k_cell2node3, k_node_avg   nodeE smoothing (:354-404, :1115-1265)
-//   k_faraday            faceCurl(doFaraday=true)         (:1587-1671)
-//   k_cell_ep            calcCellEp                       (:1674-1737)
+//   k_node2cell3, k_cell2node3, k_node_avg, k_faraday   nodeE smoothing and the
+//                        Faraday step after it (:354-404, :1115-1265, :1587-1671)
 // Exterior-cell kernels run over the list of cells missing a neighbour. In
 // the reference those loops are sequential, but every value an exterior cell
 // receives comes from a cell (or a component) that the same loop does not
@@ -107,30 +107,6 @@ __device__ inline void extCellIJK(const GridInfo& g, int c, int& i, int& j, int&
    k = c / (g.nx * g.ny);
 }
 
-// neumannCell(cellB,3), neumannCell(cellJi,3), neumannCell(cellRhoQi,1), setIMFCell
-__global__ void k_ext_cell_bc(GridInfo g, Fields f, FieldParams fp, const int* ext, int next) {
-   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-   if (e >= next) return;
-   const int c = ext[e];
-   int i, j, k;
-   extCellIJK(g, c, i, j, k);
-   const long long N = g.N, n = c;
-   const int m = missingMask(g, i, j, k);
-   const signed char* o = c_neu.cellSrc[m];
-   const long long s = nbr(g, i, j, k, o[0], o[1], o[2]);
-   if (s >= 0) {
-      for (int l = 0; l < 3; ++l) f.cellB[l * N + n] = f.cellB[l * N + s];
-      for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = f.cellJi[l * N + s];
-      f.cellRho[n] = f.cellRho[s];
-   }
-   const int wall[6] = {32, 1, 2, 4, 8, 16};  // +x -x +y -y +z -z
-   for (int w = 0; w < 6; ++w) {
-      if ((m & wall[w]) && fp.imfCell[w]) {
-         for (int l = 0; l < 3; ++l) f.cellB[l * N + n] = fp.imf[l];
-      }
-   }
-}
-
 // neumannCell of one 3-vector (cellUe, or cellJ during smoothing)
 __global__ void k_ext_cell_neumann3(GridInfo g, double* a, const int* ext, int next) {
    const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,51 +122,9 @@ __global__ void k_ext_cell_neumann3(GridInfo g, double* a, const int* ext, int n
    for (int l = 0; l < 3; ++l) a[l * N + n] = a[l * N + s];
 }
 
-// neumannFace(faceB) + setIMFFace(faceB)
-__global__ void k_ext_face_bc(GridInfo g, Fields f, FieldParams fp, const int* ext, int next) {
-   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-   if (e >= next) return;
-   const int c = ext[e];
-   int i, j, k;
-   extCellIJK(g, c, i, j, k);
-   const long long N = g.N, n = c;
-   const int m = missingMask(g, i, j, k);
-   double v[3];
-   bool set[3] = {false, false, false};
-   for (int l = 0; l < 3; ++l) {
-      if (!c_neu.faceUse[m][l]) continue;
-      const signed char* o = c_neu.faceSrc[m][l];
-      const long long s = nbr(g, i, j, k, o[0], o[1], o[2]);
-      if (s < 0) continue;
-      v[l] = f.faceB[l * N + s];
-      set[l] = true;
-   }
-   for (int l = 0; l < 3; ++l) if (set[l]) f.faceB[l * N + n] = v[l];
-   const int wall[6] = {32, 1, 2, 4, 8, 16};
-   for (int w = 0; w < 6; ++w) {
-      if ((m & wall[w]) && fp.imfFace[w]) {
-         const int axis = w / 2;
-         for (int l = 0; l < 3; ++l) if (l != axis) f.faceB[l * N + n] = fp.imf[l];
-      }
-   }
-}
-
-// cell2Node of cellB, cellRhoQi, cellJi, then cellAverageB += cellB
-__global__ void k_cell2node_avg(GridInfo g, Fields f) {
-   RH_CELL_PROLOGUE
-   for (int l = 0; l < 3; ++l) f.cellAvgB[l * N + n] += f.cellB[l * N + n];
-   if (!plusOk(g, i, j, k)) return;
-   const long long c000 = n, c001 = nbr(g, i, j, k, 0, 0, 1), c010 = nbr(g, i, j, k, 0, 1, 0),
-                   c100 = nbr(g, i, j, k, 1, 0, 0), c011 = nbr(g, i, j, k, 0, 1, 1),
-                   c110 = nbr(g, i, j, k, 1, 1, 0), c101 = nbr(g, i, j, k, 1, 0, 1),
-                   c111 = nbr(g, i, j, k, 1, 1, 1);
 #define RH_C2N(dst, src, off)                                                                  \
    dst[off + n] = 0.125 * (src[off + c000] + src[off + c001] + src[off + c010] + src[off + c100] + \
                            src[off + c011] + src[off + c110] + src[off + c101] + src[off + c111]);
-   for (int l = 0; l < 3; ++l) { RH_C2N(f.nodeB, f.cellB, l * N) }
-   RH_C2N(f.nodeRho, f.cellRho, 0)
-   for (int l = 0; l < 3; ++l) { RH_C2N(f.nodeJi, f.cellJi, l * N) }
-}
 
 // cell2Node of a 3-vector (smoothing: cellJ -> nodeE)
 __global__ void k_cell2node3(GridInfo g, const double* src, double* dst) {
@@ -217,168 +151,6 @@ __global__ void k_node2cell3(GridInfo g, const double* src, double* dst) {
       dst[o + n] = 0.125 * (src[o + a0] + src[o + a1] + src[o + a2] + src[o + a3] + src[o + a4] +
                             src[o + a5] + src[o + a6] + src[o + a7]);
    }
-}
-
-// calcNodeJ: nodeJ = (two edge curls of faceB)/(2 dx mu0 d), whistler limiter d
-__global__ void k_node_j(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
-   RH_CELL_PROLOGUE
-   if (!plusOk(g, i, j, k)) return;
-   const double* fb = f.faceB;
-   const long long a000 = n, a100 = nbr(g, i, j, k, 1, 0, 0), a010 = nbr(g, i, j, k, 0, 1, 0),
-                   a001 = nbr(g, i, j, k, 0, 0, 1), a110 = nbr(g, i, j, k, 1, 1, 0),
-                   a101 = nbr(g, i, j, k, 1, 0, 1), a011 = nbr(g, i, j, k, 0, 1, 1);
-#define FB(a, l) fb[(l) * N + (a)]
-   const double edgeJx1 = -FB(a000, 2) + FB(a000, 1) + FB(a010, 2) - FB(a001, 1);
-   const double edgeJx2 = -FB(a100, 2) + FB(a100, 1) + FB(a110, 2) - FB(a101, 1);
-   const double edgeJy1 = +FB(a000, 2) + FB(a001, 0) - FB(a100, 2) - FB(a000, 0);
-   const double edgeJy2 = +FB(a010, 2) + FB(a011, 0) - FB(a110, 2) - FB(a010, 0);
-   const double edgeJz1 = -FB(a000, 1) + FB(a000, 0) + FB(a100, 1) - FB(a010, 0);
-   const double edgeJz2 = -FB(a001, 1) + FB(a001, 0) + FB(a101, 1) - FB(a011, 0);
-#undef FB
-   double d = 1.0;
-   double vw = 0.0;
-   const double ne = f.nodeRho[n] / RHGPU_CHARGE_ELEMENTARY;
-   const double Btot = sqrt(sq(f.nodeB[0 * N + n]) + sq(f.nodeB[1 * N + n]) + sq(f.nodeB[2 * N + n]));
-   if (ne > 0.0 && g.dx > 0.0) {
-      vw = 2.0 * Btot * 3.14159265358979323846 / (RHGPU_PERMEABILITY * ne * RHGPU_CHARGE_ELEMENTARY * g.dx);
-   }
-   const bool lim = vw > fp.maxVw && fp.maxVw > 0.0;
-   if (lim) d = vw / fp.maxVw;
-   countIf(lim, &cnt[CNT_MAX_VW]);
-   gridCount(f, GC_NODE_MAX_VW, N, n, lim);
-   const double a = 0.5 / (g.dx * RHGPU_PERMEABILITY * d);
-   f.nodeJ[0 * N + n] = (edgeJx1 + edgeJx2) * a;
-   f.nodeJ[1 * N + n] = (edgeJy1 + edgeJy2) * a;
-   f.nodeJ[2 * N + n] = (edgeJz1 + edgeJz2) * a;
-}
-
-// node2Cell(nodeJ -> cellJ) then calcCellUe
-__global__ void k_cell_j_ue(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
-   RH_CELL_PROLOGUE
-   if (!allNb(g, i, j, k)) return;
-   const long long a0 = n, a1 = nbr(g, i, j, k, -1, 0, 0), a2 = nbr(g, i, j, k, -1, -1, 0),
-                   a3 = nbr(g, i, j, k, 0, -1, 0), a4 = nbr(g, i, j, k, 0, 0, -1),
-                   a5 = nbr(g, i, j, k, 0, -1, -1), a6 = nbr(g, i, j, k, -1, 0, -1),
-                   a7 = nbr(g, i, j, k, -1, -1, -1);
-   double J[3];
-   for (int l = 0; l < 3; ++l) {
-      const double* s = f.nodeJ + l * N;
-      J[l] = 0.125 * (s[a0] + s[a1] + s[a2] + s[a3] + s[a4] + s[a5] + s[a6] + s[a7]);
-      f.cellJ[l * N + n] = J[l];
-   }
-   double Ue[3];
-   bool clamp = false;
-   if (f.flags[n] & RHGPU_FLAG_INNER_FIELD) {
-      for (int l = 0; l < 3; ++l) Ue[l] = fp.obstacleUe[l];
-   } else {
-      const double rho = f.cellRho[n];
-      for (int l = 0; l < 3; ++l) {
-         if (fabs(rho) > 0) {
-            if (fp.use_hall) Ue[l] = -(J[l] - f.cellJi[l * N + n]) / rho;
-            else Ue[l] = f.cellJi[l * N + n] / rho;
-         } else {
-            Ue[l] = 0.0;
-         }
-      }
-      const double Ue2 = sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]);
-      if (Ue2 > fp.maxUe2) {
-         const double norm = sqrt(fp.maxUe2 / Ue2);
-         Ue[0] *= norm; Ue[1] *= norm; Ue[2] *= norm;
-         clamp = true;
-      }
-   }
-   countIf(clamp, &cnt[CNT_MAX_CELL_UE]);
-   gridCount(f, GC_CELL_MAX_UE, N, n, clamp);
-   for (int l = 0; l < 3; ++l) f.cellUe[l * N + n] = Ue[l];
-}
-
-// calcNodeUe, upwindNodeB, calcNodeE for the node at the (+,+,+) corner
-__global__ void k_node_ue_b_e(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
-   RH_CELL_PROLOGUE
-   if (!plusOk(g, i, j, k)) return;
-   // calcNodeUe
-   double Ue[3];
-   bool rhoClamp = false, ueClamp = false;
-   if (f.flags[n] & RHGPU_FLAG_INNER_NODE) {
-      for (int l = 0; l < 3; ++l) Ue[l] = fp.obstacleUe[l];
-   } else {
-      double rho = f.nodeRho[n];
-      if (rho < fp.minRho) {
-         rho = fp.minRho;
-         f.nodeRho[n] = rho;
-         rhoClamp = true;
-      }
-      for (int l = 0; l < 3; ++l) {
-         if (fabs(rho) > 0) {
-            if (fp.use_hall) Ue[l] = -(f.nodeJ[l * N + n] - f.nodeJi[l * N + n]) / rho;
-            else Ue[l] = f.nodeJi[l * N + n] / rho;
-         } else {
-            Ue[l] = 0.0;
-         }
-      }
-      const double Ue2 = sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]);
-      if (Ue2 > fp.maxUe2) {
-         const double norm = sqrt(fp.maxUe2 / Ue2);
-         Ue[0] *= norm; Ue[1] *= norm; Ue[2] *= norm;
-         ueClamp = true;
-      }
-   }
-   countIf(rhoClamp, &cnt[CNT_MIN_NODE_RHO]);
-   countIf(ueClamp, &cnt[CNT_MAX_NODE_UE]);
-   gridCount(f, GC_CELL_MAX_UE, N, n, ueClamp);
-   for (int l = 0; l < 3; ++l) f.nodeUe[l * N + n] = Ue[l];
-   // upwindNodeB
-   double xU = -0.5, yU = 0, zU = 0;
-   const double U = sqrt(sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]));
-   if (U > 0) {
-      const double a = -0.5 / U;
-      xU = Ue[0] * a; yU = Ue[1] * a; zU = Ue[2] * a;
-   }
-   const double w111 = 1 / sqrt(sq(-0.5 - xU) + sq(-0.5 - yU) + sq(-0.5 - zU));
-   const double w112 = 1 / sqrt(sq(-0.5 - xU) + sq(-0.5 - yU) + sq(+0.5 - zU));
-   const double w121 = 1 / sqrt(sq(-0.5 - xU) + sq(+0.5 - yU) + sq(-0.5 - zU));
-   const double w211 = 1 / sqrt(sq(+0.5 - xU) + sq(-0.5 - yU) + sq(-0.5 - zU));
-   const double w122 = 1 / sqrt(sq(-0.5 - xU) + sq(+0.5 - yU) + sq(+0.5 - zU));
-   const double w221 = 1 / sqrt(sq(+0.5 - xU) + sq(+0.5 - yU) + sq(-0.5 - zU));
-   const double w212 = 1 / sqrt(sq(+0.5 - xU) + sq(-0.5 - yU) + sq(+0.5 - zU));
-   const double w222 = 1 / sqrt(sq(+0.5 - xU) + sq(+0.5 - yU) + sq(+0.5 - zU));
-   const double wsum = w111 + w112 + w121 + w211 + w122 + w221 + w212 + w222;
-   double B[3];
-   if (wsum > 0) {
-      const long long c111 = n, c112 = nbr(g, i, j, k, 0, 0, 1), c121 = nbr(g, i, j, k, 0, 1, 0),
-                      c211 = nbr(g, i, j, k, 1, 0, 0), c122 = nbr(g, i, j, k, 0, 1, 1),
-                      c221 = nbr(g, i, j, k, 1, 1, 0), c212 = nbr(g, i, j, k, 1, 0, 1),
-                      c222 = nbr(g, i, j, k, 1, 1, 1);
-      for (int l = 0; l < 3; ++l) {
-         const double* cb = f.cellB + l * N;
-         B[l] = (w111 * cb[c111] + w112 * cb[c112] + w121 * cb[c121] + w211 * cb[c211] + w122 * cb[c122] +
-                 w221 * cb[c221] + w212 * cb[c212] + w222 * cb[c222]) / wsum;
-      }
-   } else {
-      B[0] = B[1] = B[2] = 0.0;
-   }
-   for (int l = 0; l < 3; ++l) f.nodeB[l * N + n] = B[l];
-   // calcNodeE: E = -Ue x B + eta J
-   double E[3];
-   E[0] = -(Ue[1] * B[2] - Ue[2] * B[1]);
-   E[1] = -(Ue[2] * B[0] - Ue[0] * B[2]);
-   E[2] = -(Ue[0] * B[1] - Ue[1] * B[0]);
-   const double eta = f.nodeEta[n];
-   E[0] += eta * f.nodeJ[0 * N + n];
-   E[1] += eta * f.nodeJ[1 * N + n];
-   E[2] += eta * f.nodeJ[2 * N + n];
-   bool eClamp = false;
-   if (fp.maxE2 > 0) {
-      const double E2 = sq(E[0]) + sq(E[1]) + sq(E[2]);
-      if (E2 > fp.maxE2) {
-         const double scaling = sqrt(fp.maxE2 / E2);
-         E[0] *= scaling; E[1] *= scaling; E[2] *= scaling;
-         eClamp = true;
-      }
-   }
-   countIf(eClamp, &cnt[CNT_MAX_E]);
-   gridCount(f, GC_NODE_MAX_E, N, n, eClamp);
-   for (int l = 0; l < 3; ++l) f.nodeE[l * N + n] = E[l];
 }
 
 // nodeAvg: 27-point Gaussian of nodeE. Neighbours that do not exist read 0,
@@ -452,33 +224,299 @@ __global__ void k_faraday(GridInfo g, Fields f) {
    }
 }
 
-// calcCellEp: electron pressure field from the gradient of face-averaged nodeRhoQi
-__global__ void k_cell_ep(GridInfo g, Fields f, FieldParams fp) {
-   RH_CELL_PROLOGUE
-   if (!allNb(g, i, j, k)) return;
-   double Ep[3] = {0.0, 0.0, 0.0};
-   if (!(f.flags[n] & RHGPU_FLAG_INNER_CELLEP)) {
-      const double* r = f.nodeRho;
-      const long long o000 = n, o00m = nbr(g, i, j, k, 0, 0, -1), o0mm = nbr(g, i, j, k, 0, -1, -1),
-                      o0m0 = nbr(g, i, j, k, 0, -1, 0), om00 = nbr(g, i, j, k, -1, 0, 0),
-                      om0m = nbr(g, i, j, k, -1, 0, -1), ommm = nbr(g, i, j, k, -1, -1, -1),
-                      omm0 = nbr(g, i, j, k, -1, -1, 0);
-      const double xPos = 0.25 * (r[o000] + r[o00m] + r[o0mm] + r[o0m0]);
-      const double xNeg = 0.25 * (r[om00] + r[om0m] + r[ommm] + r[omm0]);
-      const double yPos = 0.25 * (r[o000] + r[o00m] + r[om0m] + r[om00]);
-      const double yNeg = 0.25 * (r[o0m0] + r[o0mm] + r[ommm] + r[omm0]);
-      const double zPos = 0.25 * (r[o000] + r[o0m0] + r[omm0] + r[om00]);
-      const double zNeg = 0.25 * (r[o00m] + r[o0mm] + r[ommm] + r[om0m]);
-      const double gx = (xPos - xNeg) / g.dx, gy = (yPos - yNeg) / g.dx, gz = (zPos - zNeg) / g.dx;
-      const double C = fp.ep_coeff;
-      if (!fp.isothermal) {
-         Ep[0] = -C * gx; Ep[1] = -C * gy; Ep[2] = -C * gz;
-      } else if (fabs(f.cellRho[n]) > 0) {
-         const double rho = f.cellRho[n];
-         Ep[0] = -C * gx / rho; Ep[1] = -C * gy / rho; Ep[2] = -C * gz / rho;
+// ---- the field update in fewer passes ------------------------------------------------------
+// The reference's propagateB steps, fused where one pass can form the values
+// the next one reads, each expression in the reference's order (bit for bit):
+//   k_ext_bc      neumannCell(cellB, cellJi, cellRhoQi) / setIMFCell and
+//                 neumannFace / setIMFFace(faceB) of the exterior cells
+//                 (hybrid_propagator.cpp:443-908; disjoint arrays)
+//   k_node_fused  per node: cellAverageB += cellB, cell2Node (nodeB, nodeRhoQi,
+//                 nodeJi), calcNodeJ (edge curls of faceB / (2 dx mu0 d), the
+//                 whistler limiter d), then calcNodeUe, upwindNodeB and calcNodeE;
+//                 the averaged nodeB that the whistler limiter reads stays in
+//                 registers, the upwind weights re-read the same eight cells
+//   k_cell_fused  per cell: node2Cell of nodeJ and calcCellUe, calcCellEp (the
+//                 gradient of face-averaged nodeRhoQi), and (FARADAY: no E
+//                 smoothing) faceCurl, faceB += dt curl E; none of them reads
+//                 what another writes
+// The cellUe Neumann pass (k_ext_cell_neumann3) follows k_cell_fused; calcNodeUe
+// and calcNodeE do not read cellUe, so its place before them in the reference's
+// order does not matter.
+__global__ void k_ext_bc(GridInfo g, Fields f, FieldParams fp, const int* ext, int next) {
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;
+   if (e >= next) return;
+   const int c = ext[e];
+   int i, j, k;
+   extCellIJK(g, c, i, j, k);
+   const long long N = g.N, n = c;
+   const int m = missingMask(g, i, j, k);
+   const int wall[6] = {32, 1, 2, 4, 8, 16};  // +x -x +y -y +z -z
+   {  // neumannCell(cellB, 3), neumannCell(cellJi, 3), neumannCell(cellRhoQi, 1), setIMFCell
+      const signed char* o = c_neu.cellSrc[m];
+      const long long s = nbr(g, i, j, k, o[0], o[1], o[2]);
+      if (s >= 0) {
+         for (int l = 0; l < 3; ++l) f.cellB[l * N + n] = f.cellB[l * N + s];
+         for (int l = 0; l < 3; ++l) f.cellJi[l * N + n] = f.cellJi[l * N + s];
+         f.cellRho[n] = f.cellRho[s];
+      }
+      for (int w = 0; w < 6; ++w)
+         if ((m & wall[w]) && fp.imfCell[w])
+            for (int l = 0; l < 3; ++l) f.cellB[l * N + n] = fp.imf[l];
+   }
+   {  // neumannFace(faceB), setIMFFace(faceB)
+      double v[3];
+      bool set[3] = {false, false, false};
+      for (int l = 0; l < 3; ++l) {
+         if (!c_neu.faceUse[m][l]) continue;
+         const signed char* o = c_neu.faceSrc[m][l];
+         const long long s = nbr(g, i, j, k, o[0], o[1], o[2]);
+         if (s < 0) continue;
+         v[l] = f.faceB[l * N + s];
+         set[l] = true;
+      }
+      for (int l = 0; l < 3; ++l) if (set[l]) f.faceB[l * N + n] = v[l];
+      for (int w = 0; w < 6; ++w) {
+         if ((m & wall[w]) && fp.imfFace[w]) {
+            const int axis = w / 2;
+            for (int l = 0; l < 3; ++l) if (l != axis) f.faceB[l * N + n] = fp.imf[l];
+         }
       }
    }
-   for (int l = 0; l < 3; ++l) f.cellEp[l * N + n] = Ep[l];
+}
+
+__global__ void k_node_fused(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
+   RH_CELL_PROLOGUE
+   for (int l = 0; l < 3; ++l) f.cellAvgB[l * N + n] += f.cellB[l * N + n];
+   if (!plusOk(g, i, j, k)) return;
+   const long long c000 = n, c001 = nbr(g, i, j, k, 0, 0, 1), c010 = nbr(g, i, j, k, 0, 1, 0),
+                   c100 = nbr(g, i, j, k, 1, 0, 0), c011 = nbr(g, i, j, k, 0, 1, 1),
+                   c110 = nbr(g, i, j, k, 1, 1, 0), c101 = nbr(g, i, j, k, 1, 0, 1),
+                   c111 = nbr(g, i, j, k, 1, 1, 1);
+   // cell2Node
+   double nodeBavg[3];
+   for (int l = 0; l < 3; ++l) {
+      const double* s = f.cellB + l * N;
+      nodeBavg[l] = 0.125 * (s[c000] + s[c001] + s[c010] + s[c100] + s[c011] + s[c110] + s[c101] + s[c111]);
+   }
+   double rho;
+   {
+      const double* s = f.cellRho;
+      rho = 0.125 * (s[c000] + s[c001] + s[c010] + s[c100] + s[c011] + s[c110] + s[c101] + s[c111]);
+   }
+   double Ji[3];
+#pragma unroll
+   for (int l = 0; l < 3; ++l) {
+      const double* s = f.cellJi + l * N;
+      Ji[l] = 0.125 * (s[c000] + s[c001] + s[c010] + s[c100] + s[c011] + s[c110] + s[c101] + s[c111]);
+      f.nodeJi[l * N + n] = Ji[l];
+   }
+   // calcNodeJ (its whistler limiter reads the averaged nodeB and the unclamped nodeRhoQi)
+   double Jn[3];
+   {
+      const double* fb = f.faceB;
+      const long long a000 = n, a100 = c100, a010 = c010, a001 = c001, a110 = c110, a101 = c101, a011 = c011;
+#define FB(a, l) fb[(l) * N + (a)]
+      const double edgeJx1 = -FB(a000, 2) + FB(a000, 1) + FB(a010, 2) - FB(a001, 1);
+      const double edgeJx2 = -FB(a100, 2) + FB(a100, 1) + FB(a110, 2) - FB(a101, 1);
+      const double edgeJy1 = +FB(a000, 2) + FB(a001, 0) - FB(a100, 2) - FB(a000, 0);
+      const double edgeJy2 = +FB(a010, 2) + FB(a011, 0) - FB(a110, 2) - FB(a010, 0);
+      const double edgeJz1 = -FB(a000, 1) + FB(a000, 0) + FB(a100, 1) - FB(a010, 0);
+      const double edgeJz2 = -FB(a001, 1) + FB(a001, 0) + FB(a101, 1) - FB(a011, 0);
+#undef FB
+      double d = 1.0;
+      double vw = 0.0;
+      const double ne = rho / RHGPU_CHARGE_ELEMENTARY;
+      const double Btot = sqrt(sq(nodeBavg[0]) + sq(nodeBavg[1]) + sq(nodeBavg[2]));
+      if (ne > 0.0 && g.dx > 0.0) {
+         vw = 2.0 * Btot * 3.14159265358979323846 / (RHGPU_PERMEABILITY * ne * RHGPU_CHARGE_ELEMENTARY * g.dx);
+      }
+      const bool lim = vw > fp.maxVw && fp.maxVw > 0.0;
+      if (lim) d = vw / fp.maxVw;
+      countIf(lim, &cnt[CNT_MAX_VW]);
+      gridCount(f, GC_NODE_MAX_VW, N, n, lim);
+      const double a = 0.5 / (g.dx * RHGPU_PERMEABILITY * d);
+      Jn[0] = (edgeJx1 + edgeJx2) * a;
+      Jn[1] = (edgeJy1 + edgeJy2) * a;
+      Jn[2] = (edgeJz1 + edgeJz2) * a;
+      for (int l = 0; l < 3; ++l) f.nodeJ[l * N + n] = Jn[l];
+   }
+   // calcNodeUe
+   double Ue[3];
+   bool rhoClamp = false, ueClamp = false;
+   if (f.flags[n] & RHGPU_FLAG_INNER_NODE) {
+      for (int l = 0; l < 3; ++l) Ue[l] = fp.obstacleUe[l];
+   } else {
+      if (rho < fp.minRho) {
+         rho = fp.minRho;
+         rhoClamp = true;
+      }
+      for (int l = 0; l < 3; ++l) {
+         if (fabs(rho) > 0) {
+            if (fp.use_hall) Ue[l] = -(Jn[l] - Ji[l]) / rho;
+            else Ue[l] = Ji[l] / rho;
+         } else {
+            Ue[l] = 0.0;
+         }
+      }
+      const double Ue2 = sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]);
+      if (Ue2 > fp.maxUe2) {
+         const double norm = sqrt(fp.maxUe2 / Ue2);
+         Ue[0] *= norm; Ue[1] *= norm; Ue[2] *= norm;
+         ueClamp = true;
+      }
+   }
+   f.nodeRho[n] = rho;
+   countIf(rhoClamp, &cnt[CNT_MIN_NODE_RHO]);
+   countIf(ueClamp, &cnt[CNT_MAX_NODE_UE]);
+   gridCount(f, GC_CELL_MAX_UE, N, n, ueClamp);
+   for (int l = 0; l < 3; ++l) f.nodeUe[l * N + n] = Ue[l];
+   // upwindNodeB: the same eight cells as cell2Node (c111 ... c222 = c000 ... c111)
+   double xU = -0.5, yU = 0, zU = 0;
+   const double U = sqrt(sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]));
+   if (U > 0) {
+      const double a = -0.5 / U;
+      xU = Ue[0] * a; yU = Ue[1] * a; zU = Ue[2] * a;
+   }
+   const double w111 = 1 / sqrt(sq(-0.5 - xU) + sq(-0.5 - yU) + sq(-0.5 - zU));
+   const double w112 = 1 / sqrt(sq(-0.5 - xU) + sq(-0.5 - yU) + sq(+0.5 - zU));
+   const double w121 = 1 / sqrt(sq(-0.5 - xU) + sq(+0.5 - yU) + sq(-0.5 - zU));
+   const double w211 = 1 / sqrt(sq(+0.5 - xU) + sq(-0.5 - yU) + sq(-0.5 - zU));
+   const double w122 = 1 / sqrt(sq(-0.5 - xU) + sq(+0.5 - yU) + sq(+0.5 - zU));
+   const double w221 = 1 / sqrt(sq(+0.5 - xU) + sq(+0.5 - yU) + sq(-0.5 - zU));
+   const double w212 = 1 / sqrt(sq(+0.5 - xU) + sq(-0.5 - yU) + sq(+0.5 - zU));
+   const double w222 = 1 / sqrt(sq(+0.5 - xU) + sq(+0.5 - yU) + sq(+0.5 - zU));
+   const double wsum = w111 + w112 + w121 + w211 + w122 + w221 + w212 + w222;
+   double B[3];
+   if (wsum > 0) {
+      for (int l = 0; l < 3; ++l) {
+         const double* cbl = f.cellB + l * N;
+         B[l] = (w111 * cbl[c000] + w112 * cbl[c001] + w121 * cbl[c010] + w211 * cbl[c100] + w122 * cbl[c011] +
+                 w221 * cbl[c110] + w212 * cbl[c101] + w222 * cbl[c111]) / wsum;
+      }
+   } else {
+      B[0] = B[1] = B[2] = 0.0;
+   }
+   for (int l = 0; l < 3; ++l) f.nodeB[l * N + n] = B[l];
+   // calcNodeE: E = -Ue x B + eta J
+   double E[3];
+   E[0] = -(Ue[1] * B[2] - Ue[2] * B[1]);
+   E[1] = -(Ue[2] * B[0] - Ue[0] * B[2]);
+   E[2] = -(Ue[0] * B[1] - Ue[1] * B[0]);
+   const double eta = f.nodeEta[n];
+   E[0] += eta * Jn[0];
+   E[1] += eta * Jn[1];
+   E[2] += eta * Jn[2];
+   bool eClamp = false;
+   if (fp.maxE2 > 0) {
+      const double E2 = sq(E[0]) + sq(E[1]) + sq(E[2]);
+      if (E2 > fp.maxE2) {
+         const double scaling = sqrt(fp.maxE2 / E2);
+         E[0] *= scaling; E[1] *= scaling; E[2] *= scaling;
+         eClamp = true;
+      }
+   }
+   countIf(eClamp, &cnt[CNT_MAX_E]);
+   gridCount(f, GC_NODE_MAX_E, N, n, eClamp);
+   for (int l = 0; l < 3; ++l) f.nodeE[l * N + n] = E[l];
+}
+
+template <bool FARADAY>
+__global__ void k_cell_fused(GridInfo g, Fields f, FieldParams fp, int useEp, unsigned long long* cnt) {
+   RH_CELL_PROLOGUE
+   const bool inner = allNb(g, i, j, k);
+   bool clamp = false;
+   if (inner) {
+      const long long a0 = n, a1 = nbr(g, i, j, k, -1, 0, 0), a2 = nbr(g, i, j, k, -1, -1, 0),
+                      a3 = nbr(g, i, j, k, 0, -1, 0), a4 = nbr(g, i, j, k, 0, 0, -1),
+                      a5 = nbr(g, i, j, k, 0, -1, -1), a6 = nbr(g, i, j, k, -1, 0, -1),
+                      a7 = nbr(g, i, j, k, -1, -1, -1);
+      // node2Cell(nodeJ -> cellJ), calcCellUe
+      double J[3];
+      for (int l = 0; l < 3; ++l) {
+         const double* s = f.nodeJ + l * N;
+         J[l] = 0.125 * (s[a0] + s[a1] + s[a2] + s[a3] + s[a4] + s[a5] + s[a6] + s[a7]);
+         f.cellJ[l * N + n] = J[l];
+      }
+      double Ue[3];
+      const unsigned char fl = f.flags[n];
+      if (fl & RHGPU_FLAG_INNER_FIELD) {
+         for (int l = 0; l < 3; ++l) Ue[l] = fp.obstacleUe[l];
+      } else {
+         const double rho = f.cellRho[n];
+         for (int l = 0; l < 3; ++l) {
+            if (fabs(rho) > 0) {
+               if (fp.use_hall) Ue[l] = -(J[l] - f.cellJi[l * N + n]) / rho;
+               else Ue[l] = f.cellJi[l * N + n] / rho;
+            } else {
+               Ue[l] = 0.0;
+            }
+         }
+         const double Ue2 = sq(Ue[0]) + sq(Ue[1]) + sq(Ue[2]);
+         if (Ue2 > fp.maxUe2) {
+            const double norm = sqrt(fp.maxUe2 / Ue2);
+            Ue[0] *= norm; Ue[1] *= norm; Ue[2] *= norm;
+            clamp = true;
+         }
+      }
+      for (int l = 0; l < 3; ++l) f.cellUe[l * N + n] = Ue[l];
+      // calcCellEp (reads the clamped nodeRhoQi)
+      if (useEp) {
+         double Ep[3] = {0.0, 0.0, 0.0};
+         if (!(fl & RHGPU_FLAG_INNER_CELLEP)) {
+            const double* r = f.nodeRho;
+            const long long o000 = a0, o00m = a4, o0mm = a5, o0m0 = a3, om00 = a1, om0m = a6, ommm = a7, omm0 = a2;
+            const double xPos = 0.25 * (r[o000] + r[o00m] + r[o0mm] + r[o0m0]);
+            const double xNeg = 0.25 * (r[om00] + r[om0m] + r[ommm] + r[omm0]);
+            const double yPos = 0.25 * (r[o000] + r[o00m] + r[om0m] + r[om00]);
+            const double yNeg = 0.25 * (r[o0m0] + r[o0mm] + r[ommm] + r[omm0]);
+            const double zPos = 0.25 * (r[o000] + r[o0m0] + r[omm0] + r[om00]);
+            const double zNeg = 0.25 * (r[o00m] + r[o0mm] + r[ommm] + r[om0m]);
+            const double gx = (xPos - xNeg) / g.dx, gy = (yPos - yNeg) / g.dx, gz = (zPos - zNeg) / g.dx;
+            const double C = fp.ep_coeff;
+            if (!fp.isothermal) {
+               Ep[0] = -C * gx; Ep[1] = -C * gy; Ep[2] = -C * gz;
+            } else if (fabs(f.cellRho[n]) > 0) {
+               const double rho = f.cellRho[n];
+               Ep[0] = -C * gx / rho; Ep[1] = -C * gy / rho; Ep[2] = -C * gz / rho;
+            }
+         }
+         for (int l = 0; l < 3; ++l) f.cellEp[l * N + n] = Ep[l];
+      }
+   }
+   countIf(clamp, &cnt[CNT_MAX_CELL_UE]);
+   gridCount(f, GC_CELL_MAX_UE, N, n, clamp);
+   if (!FARADAY) return;
+   // faceCurl(nodeE -> faceB)
+   bool doX = true, doY = true, doZ = true;
+   if (!inner) {
+      if (!plusOk(g, i, j, k)) return;
+      if (!xNeg(g, i)) { doY = doZ = false; }
+      if (!yNeg(g, j)) { doX = doZ = false; }
+      if (!zNeg(g, k)) { doX = doY = false; }
+   }
+   const double* E = f.nodeE;
+   const double dx = g.dx, dt = g.dt;
+   if (doX) {
+      const long long s5 = nbr(g, i, j, k, 0, -1, 0), s6 = nbr(g, i, j, k, 0, -1, -1), s7 = nbr(g, i, j, k, 0, 0, -1);
+      const double n5y = E[1 * N + s5], n5z = E[2 * N + s5], n6y = E[1 * N + s6], n6z = E[2 * N + s6];
+      const double n7y = E[1 * N + s7], n7z = E[2 * N + s7], n8y = E[1 * N + n], n8z = E[2 * N + n];
+      const double curlX = 0.5 * (+n5z + n6z - n6y - n7y - n7z - n8z + n8y + n5y) / dx;
+      f.faceB[0 * N + n] += dt * curlX;
+   }
+   if (doY) {
+      const long long s3 = nbr(g, i, j, k, -1, 0, -1), s4 = nbr(g, i, j, k, -1, 0, 0), s7 = nbr(g, i, j, k, 0, 0, -1);
+      const double n3x = E[0 * N + s3], n3z = E[2 * N + s3], n4x = E[0 * N + s4], n4z = E[2 * N + s4];
+      const double n7x = E[0 * N + s7], n7z = E[2 * N + s7], n8x = E[0 * N + n], n8z = E[2 * N + n];
+      const double curlY = 0.5 * (-n4x - n8x + n8z + n7z + n7x + n3x - n3z - n4z) / dx;
+      f.faceB[1 * N + n] += dt * curlY;
+   }
+   if (doZ) {
+      const long long s1 = nbr(g, i, j, k, -1, -1, 0), s4 = nbr(g, i, j, k, -1, 0, 0), s5 = nbr(g, i, j, k, 0, -1, 0);
+      const double n1x = E[0 * N + s1], n1y = E[1 * N + s1], n4x = E[0 * N + s4], n4y = E[1 * N + s4];
+      const double n5x = E[0 * N + s5], n5y = E[1 * N + s5], n8x = E[0 * N + n], n8y = E[1 * N + n];
+      const double curlZ = 0.5 * (-n1x - n5x - n5y - n8y + n8x + n4x + n4y + n1y) / dx;
+      f.faceB[2 * N + n] += dt * curlZ;
+   }
 }
 
 }  // namespace rh

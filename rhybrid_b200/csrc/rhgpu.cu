@@ -524,31 +524,36 @@ int boundariesAll(rhgpu_ctx* c) {
       RH_LAUNCHED(c);                                        \
    } while (0)
 
+// propagateB (hybrid_propagator.cpp:42-440) in five passes when E is not
+// smoothed: face2Cell, the exterior boundary rules, the node pass, the cell
+// pass with Faraday, the cellUe Neumann rule (k_fields.cuh: the fused kernels)
 int fieldsAll(rhgpu_ctx* c) {
    const GridInfo& g = c->g;
    const dim3 G = cellGrid(g), B = cellBlock();
    const unsigned EB = blocks1d(c->next > 0 ? c->next : 1, 128);
+   const bool smooth = c->P.n_linear_smoothings_nodeE > 0 || c->P.use_gaussian_smoothing_nodeE;
    RH_FIELD_LAUNCH(k_face2cell, G, B, g, c->f);
-   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
-   RH_FIELD_LAUNCH(k_cell2node_avg, G, B, g, c->f);
+   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
+   RH_FIELD_LAUNCH(k_node_fused, G, B, g, c->f, c->fp, c->cntU);
    c->gridAvgCounter += 1;
-   if (c->next > 0) RH_FIELD_LAUNCH(k_ext_face_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
-   RH_FIELD_LAUNCH(k_node_j, G, B, g, c->f, c->fp, c->cntU);
-   RH_FIELD_LAUNCH(k_cell_j_ue, G, B, g, c->f, c->fp, c->cntU);
+   if (smooth)
+      RH_FIELD_LAUNCH(k_cell_fused<false>, G, B, g, c->f, c->fp, c->P.use_electron_pressure, c->cntU);
+   else
+      RH_FIELD_LAUNCH(k_cell_fused<true>, G, B, g, c->f, c->fp, c->P.use_electron_pressure, c->cntU);
    if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellUe, c->ext, c->next);
-   RH_FIELD_LAUNCH(k_node_ue_b_e, G, B, g, c->f, c->fp, c->cntU);
-   for (int it = 0; it < c->P.n_linear_smoothings_nodeE; ++it) {
-      RH_FIELD_LAUNCH(k_node2cell3, G, B, g, c->f.nodeE, c->f.cellJ);
-      if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellJ, c->ext, c->next);
-      RH_FIELD_LAUNCH(k_cell2node3, G, B, g, c->f.cellJ, c->f.nodeE);
-      RH_CUDA(cudaMemsetAsync(c->f.cellJ, 0, sizeof(double) * 3 * g.N, c->stream));
+   if (smooth) {
+      for (int it = 0; it < c->P.n_linear_smoothings_nodeE; ++it) {
+         RH_FIELD_LAUNCH(k_node2cell3, G, B, g, c->f.nodeE, c->f.cellJ);
+         if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellJ, c->ext, c->next);
+         RH_FIELD_LAUNCH(k_cell2node3, G, B, g, c->f.cellJ, c->f.nodeE);
+         RH_CUDA(cudaMemsetAsync(c->f.cellJ, 0, sizeof(double) * 3 * g.N, c->stream));
+      }
+      if (c->P.use_gaussian_smoothing_nodeE) {
+         RH_CUDA(cudaMemcpyAsync(c->tmp3, c->f.nodeE, sizeof(double) * 3 * g.N, cudaMemcpyDeviceToDevice, c->stream));
+         RH_FIELD_LAUNCH(k_node_avg, G, B, g, c->tmp3, c->f.nodeE, c->fp);
+      }
+      RH_FIELD_LAUNCH(k_faraday, G, B, g, c->f);
    }
-   if (c->P.use_gaussian_smoothing_nodeE) {
-      RH_CUDA(cudaMemcpyAsync(c->tmp3, c->f.nodeE, sizeof(double) * 3 * g.N, cudaMemcpyDeviceToDevice, c->stream));
-      RH_FIELD_LAUNCH(k_node_avg, G, B, g, c->tmp3, c->f.nodeE, c->fp);
-   }
-   RH_FIELD_LAUNCH(k_faraday, G, B, g, c->f);
-   if (c->P.use_electron_pressure) RH_FIELD_LAUNCH(k_cell_ep, G, B, g, c->f, c->fp);
    c->t += c->P.dt;
    return RHGPU_OK;
 }
