@@ -7,6 +7,8 @@ package).
                oracle/_ref/librhref.so (prefix rhref_); None if not built
   reference_gc()  the same with USE_GRID_CONSTRAINT_COUNTERS compiled in,
                oracle/_ref/librhref_gc.so; None if not built
+  reference_corsair()  the same driver with the GPU library's Corsair
+               adaptor compiled in, oracle/_ref/librhref_corsair.so
 """
 import os
 import subprocess
@@ -17,12 +19,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "librhoracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "librhref.so")
 REF_GC_PATH = os.path.join(HERE, "_ref", "librhref_gc.so")
+REF_CORSAIR_PATH = os.path.join(HERE, "_ref", "librhref_corsair.so")
+GPU_LIB_PATH = os.path.join(HERE, "..", "rhybrid_b200", "librhgpu.so")
 # the reference tree: RH_REFERENCE_DIR, else the checkout next to this repository
 REF_DIR = os.environ.get("RH_REFERENCE_DIR") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 _port = None
 _ref = None
 _ref_gc = None
+_ref_corsair = None
 
 
 def build(reference: bool = True):
@@ -32,6 +37,8 @@ def build(reference: bool = True):
     if reference:
         if os.path.isdir(os.path.join(REF_DIR, "src")):
             subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={REF_DIR}"], check=True)
+            if os.path.exists(GPU_LIB_PATH):
+                subprocess.run(["make", "-s", "-C", HERE, "corsair", f"REF_DIR={REF_DIR}"], check=True)
         elif not os.path.exists(REF_PATH):
             print(f"oracle: no reference tree at {REF_DIR} (set RH_REFERENCE_DIR); the reference build is skipped")
 
@@ -61,6 +68,31 @@ def reference_gc():
             return None
         _ref_gc = Library(REF_GC_PATH, "rhref_")
     return _ref_gc
+
+
+def reference_corsair():
+    """The reference driver with the Corsair-side adaptor of the GPU library
+    compiled in (oracle/_ref/librhref_corsair.so, prefix rhref_, plus
+    rhcorsair_run); None if not built."""
+    global _ref_corsair
+    if _ref_corsair is None:
+        if not os.path.exists(REF_CORSAIR_PATH):
+            return None
+        _ref_corsair = Library(REF_CORSAIR_PATH, "rhref_")
+    return _ref_corsair
+
+
+def corsair_run(ctx, nsteps: int, path: int, device: int = 0):
+    """rhcorsair_run on a context of reference_corsair(): nsteps steps through
+    the adaptor's plugins and propagate() hook on the GPU, the state brought
+    back into the reference's containers."""
+    import ctypes as C
+    f = ctx.lib.dll.rhcorsair_run
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]
+    f.restype = C.c_int32
+    err = C.create_string_buffer(512)
+    if f(ctx.h, nsteps, path, device, err, 512) != 0:
+        raise RuntimeError("rhcorsair_run: " + err.value.decode())
 
 
 def reference_write_data(ctx, params, group_names=()):

@@ -665,3 +665,71 @@ int rhref_get_time(void* h,double* t,int64_t* ts) {
 }
 
 }  // extern "C"
+
+#ifdef RH_CORSAIR_ADAPTOR
+/* The Corsair-side adaptor of the GPU library (rhybrid_b200/corsair/rhgpu_corsair.h)
+ * driven on this driver's Corsair/ParGrid state: the plugins are made through
+ * the object factories by the names a run's .cfg uses, initialized on the
+ * particle lists, and called the way propagate() calls them (their per-cell
+ * methods do nothing on the GPU); gpuPropagate runs each step, gpuDownload
+ * brings the state back into the ParGrid containers, which rhref_download_*
+ * then read. Built only into oracle/_ref/librhref_corsair.so (linked with
+ * librhgpu.so). */
+#include "object_factories.h"
+#include "corsair/rhgpu_corsair.h"
+
+extern "C" int rhcorsair_run(void* h, int32_t nsteps, int32_t path, int32_t device, char* err, int32_t err_cap) {
+   RefCtx* c = (RefCtx*)h;
+   if (!c || nsteps < 0) return fail(RHGPU_ERR_ARG, "rhcorsair_run: bad arguments");
+   auto report = [&](const std::string& m) {
+      if (err && err_cap > 0) { std::strncpy(err, m.c_str(), (size_t)err_cap - 1); err[err_cap - 1] = 0; }
+      return fail(RHGPU_ERR_STATE, m);
+   };
+   ObjectFactories of;
+   if (!rhgpu_corsair::registerObjectMakers<PARTICLE>(of)) return report("registerObjectMakers");
+   std::vector<ParticleListBase*> lists;
+   std::vector<ParticlePropagatorBase*> props;
+   std::vector<ParticleAccumulatorBase*> accs;
+   std::vector<ParticleBoundaryCondBase*> bcs;
+   int rc = RHGPU_OK;
+   for (int s = 0; s < c->nspecies; ++s) {
+      lists.push_back(&c->plists[s]);
+      props.push_back(of.particlePropagators.create("BorisBuneman"));
+      accs.push_back(of.particleAccumulators.create("HybridAccumulator"));
+      bcs.push_back(of.particleBoundaryConditions.create("HybridBoundaryCond"));
+      if (!props.back() || !accs.back() || !bcs.back()) { rc = report("a plugin is not registered"); break; }
+      props.back()->initialize(c->sim, c->sc, c->cr, "", &c->plists[s]);
+      accs.back()->initialize(c->sim, c->sc, c->cr, "", &c->plists[s]);
+      bcs.back()->initialize(c->sim, c->sc, c->cr, "", &c->plists[s]);
+   }
+   const int per[3] = {c->P.periodic[0], c->P.periodic[1], c->P.periodic[2]};
+   if (!rc && !rhgpu_corsair::gpuSetup<PARTICLE>(c->sim, c->sc, lists, per, device, path)) rc = report(rhgpu_corsair::run().error);
+   const std::vector<pargrid::CellID>& cells = c->sc.pargrid.getInnerCells(pargrid::DEFAULT_STENCIL);
+   const Real* crd = getBlockCoordinateArray(c->sim, c->sc);
+   for (int n = 0; n < nsteps && !rc; ++n) {
+      c->sim.timestep += 1;
+      for (int s = 0; s < c->nspecies; ++s) {
+         pargrid::DataWrapper<PARTICLE> w = c->sc.pargrid.getUserDataDynamic<PARTICLE>(c->particleIDs[s]);
+         for (pargrid::CellID b : cells)
+            if (w.size()[b] > 0) props[s]->propagateCell(b, c->particleIDs[s], crd, (unsigned int)w.size()[b]);
+         accs[s]->clearAccumulationArrays();
+         accs[s]->accumulateBoundaryCells(c->particleIDs[s], c->counts[s].data());
+         accs[s]->accumulateInnerCells(c->particleIDs[s], c->counts[s].data());
+         accs[s]->addRemoteUpdates();
+      }
+      if (!rhgpu_corsair::gpuPropagate(c->sim, c->sc, lists)) rc = report(rhgpu_corsair::run().error);
+      c->sim.t += c->sim.dt;
+   }
+   if (!rc && !rhgpu_corsair::gpuDownload<PARTICLE>(c->sim, c->sc, lists)) rc = report(rhgpu_corsair::run().error);
+   if (!rc)
+      for (int s = 0; s < c->nspecies; ++s) {
+         pargrid::DataWrapper<PARTICLE> w = c->sc.pargrid.getUserDataDynamic<PARTICLE>(c->particleIDs[s]);
+         for (size_t b = 0; b < c->counts[s].size(); ++b) c->counts[s][b] = (unsigned int)w.size()[b];
+      }
+   rhgpu_corsair::gpuFinalize();
+   for (auto* p : props) delete p;
+   for (auto* p : accs) delete p;
+   for (auto* p : bcs) delete p;
+   return rc;
+}
+#endif
