@@ -5,7 +5,11 @@ Workload (default): the plain FP64 Mars-like obstacle run, 120x160x160 cells of
 300 km, absorbing sphere r=3390 km, solar-wind H+ (n=2e6 m^-3, 30 ppc) and He++
 (4 %, 1.5 ppc), V=-450 km/s, T=1e5 K, IMF (0,3,0) nT, dt=0.05 s; about 9.7e7
 ions. Inputs are synthetic (seeded uniform-in-cell Maxwellian fill, the
-reference's InjectorUniform), generated on the host.
+reference's InjectorUniform), generated on the host. --workload c3 (the FP32
+form's Mars-like run at 256^3 cells, 100 ppc, 1.72e9 ions) and --workload
+mercury (320^3 cells, 40 ppc, 1.28e9 ions) are filled on the GPU
+(rhgpu_fill_uniform); --form learned runs the learned form's closed-loop
+evaluation instead of the plain step.
 
 A step is one propagate(): push + migration + deposit + particle boundary
 conditions + field update, for all populations.
@@ -14,7 +18,13 @@ conditions + field update, for all populations.
   e2e     the same metric through the C ABI with the state in pinned host memory
           each step: upload of all particles, one step, download of the
           particles and of rhoq, Ji, faceB (the round trip of a host that keeps
-          ownership of the particle lists, as Corsair/ParGrid does)
+          ownership of the particle lists, as Corsair/ParGrid does);
+          e2e.output_step_host is the host that keeps the state on the device
+          and reads back each step's diagnostic sums, with the particles and
+          the grid arrays downloaded at the output step closing the sample
+  cpu_baseline  the reference's hot-path sources (oracle/_ref) on every host
+          core, one process per core on a slab of the workload; one warm-up
+          step, then the median of 5 timed steps
 
 --impl reference times the reference's own hot-path sources (oracle/_ref,
 compiled from the reference tree) on the host cores, as independent
@@ -235,7 +245,7 @@ KERNEL_BYTES = {
 # proportion with the number of particles and cells.
 KERNEL_TRAFFIC = {
     # kernel: (traffic bytes, particles, cells) of the captured launch
-    "fast_push_deposit": (261.331456e6 + 215.268096e6, 4080025, 44 * 59 * 59),
+    "fast_push_deposit": (263.379712e6 + 216.007168e6, 4110000, 44 * 59 * 59),
     "f32_push_deposit": (142.888704e6 + 89.759744e6, 4080025, 44 * 59 * 59),
 }
 

@@ -93,9 +93,10 @@ struct DnMoments {
 
 // ---- the convolution on the 5th-generation tensor cores (tcgen05) ----------------------------
 // One convolution layer as an implicit GEMM on tcgen05.mma (kind::f16, BF16 x
-// BF16 -> FP32 in tensor memory), the same arithmetic and modes as k_dn_conv
-// (forward, or TRANSPOSED: the data gradient with mirrored taps and W
-// transposed, no bias).
+// BF16 -> FP32 in tensor memory): the forward layer (bias, leaky ReLU, the
+// residual or the moments written back in the epilogue, by `mode`), or
+// TRANSPOSED, the data gradient with mirrored taps and W transposed, no bias,
+// masked by the ReLU derivative.
 //
 // A block owns a column of 30 x 8 output voxels in (x, y) and TC_ZC of its
 // z-slices. Input z-slices of 32 x-positions x 10 y-rows (one voxel of halo
@@ -103,39 +104,54 @@ struct DnMoments {
 // 8-channel half with 16 bytes per voxel: any run of positions is a K-major,
 // unswizzled UMMA operand (core matrices of 8 consecutive positions x 16 bytes,
 // 128 B apart; the two channel halves one plane apart). An M-tile is 128
-// consecutive positions = 4 x-rows of one slice; the tap (dx, dy, dz) takes
-// slice z + dz and shifts the start by dx + 32 dy positions, so each tap is
-// one tcgen05.mma (M 128, N 16 output channels, K 16 input channels) on a
-// shifted A descriptor, 27 accumulating in tensor memory. Positions 0 and 31
-// of a row are the x halo: their outputs are computed and dropped. The weights
-// are staged once per block as UMMA B images (per tap N 16 x K 16 BF16,
-// K-major core matrices).
+// consecutive positions = 4 x-rows of one slice. Positions 0 and 31 of a row
+// are the x halo: their outputs are computed and dropped.
 //
-// Per output slice z: one thread issues its 2 tiles x 27 MMAs into one of two
-// tensor-memory buffers and commits them to that buffer's mbarrier; the warps
-// then take the previous slice's accumulators (tcgen05.ld, warp w its 32
-// lanes = one x-row, one voxel per thread, 16 channels) through the epilogue,
-// and slice z + 2 is copied into the slot slice z - 2 held (cp.async), while
-// the tensor cores work. Every mbarrier wait is bounded: on expiry the kernel
-// raises RHGPU_DEVERR_DENOISER in `err`, stops, and still frees its tensor
-// memory.
-constexpr int TC_HX = 32, TC_BY = 8, TC_ZC = 16;
+// The loop runs over input slices (input-stationary along z): input slice z'
+// feeds output slices z' - 1, z', z' + 1 through the taps dz = +1, 0, -1 (the
+// data gradient: -1, 0, +1). For each in-plane shift (sx, sy) one MMA of N = 48
+// takes the slice shifted by sx + 32 sy positions as A and, as B, the three
+// taps' 16 x 16 weights stacked along N (k_dn_bimage), so one read of A by the
+// tensor core serves three output slices: per tile and input slice 9 MMAs of N
+// 48 in place of 27 of N 16 per output slice, a third of the A operand reads
+// from shared memory, which bound the narrow MMAs. The accumulators of output
+// slice o live in column group (o + 2) mod 4 of the tile's 64 tensor-memory
+// columns; where an MMA's three groups wrap past the last one it is issued as
+// two (N 32 and N 16). A group is zeroed (tcgen05.st) after its slice's
+// epilogue, before the first MMA of the output slice that reuses it.
+//
+// Per input slice: one thread issues the MMAs of both tiles and commits them
+// to an mbarrier; the warps wait for the previous input slice's MMAs, which
+// complete output slice z' - 2, take its accumulators through the epilogue
+// (tcgen05.ld, warp w its 32 lanes = one x-row, one voxel per thread, 16
+// channels), zero them, and copy input slice z' + 3 (cp.async) into the slot
+// that slice z' - 1 held, while the tensor cores work on slice z'. Every
+// mbarrier wait is bounded: on expiry the kernel raises RHGPU_DEVERR_DENOISER
+// in `err`, stops issuing, waits (bounded again) for the last commit of the
+// MMAs it issued, and still frees its tensor memory.
+constexpr int TC_HX = 32, TC_BY = 8, TC_ZC = 8;
 constexpr int TC_HY = TC_BY + 2;
 constexpr int TC_BX = TC_HX - 2;                             // output voxels per x-row
 constexpr int TC_SPOS = TC_HX * TC_HY;                       // positions of one staged slice
 constexpr int TC_PAD = 1;                                    // zero positions before and after a slice
 constexpr int TC_SLOT = (TC_SPOS + 2 * TC_PAD) * 16;         // bytes of one slice in one plane
 constexpr int TC_RING = 4;                                   // slices in shared memory
-constexpr int TC_PLANE = TC_RING * TC_SLOT;                  // bytes per channel-half plane
+// bytes per channel-half plane; the extra 16 put a position's two halves on different banks
+constexpr int TC_PLANE = TC_RING * TC_SLOT + 16;
 constexpr int TC_TILES = TC_BY / 4;                          // M-tiles of 128 positions per slice
-constexpr int TC_COLS = 64;                                  // tensor-memory columns: 2 buffers x TC_TILES x 16
-constexpr int TC_BIMG = DN_TAPS * 512;                       // bytes of one layer's B images
+constexpr int TC_GROUPS = 4;                                 // accumulator groups (output slices) per tile
+constexpr int TC_TCOLS = TC_GROUPS * 16;                     // tensor-memory columns per tile
+constexpr int TC_COLS = TC_TILES * TC_TCOLS;                 // tensor-memory columns of a block
+constexpr int TC_NB = 3 * DN_C;                              // N of a stacked B image: 3 taps x 16 channels
+constexpr int TC_QIMG = TC_NB * DN_C * 2;                    // bytes of one shift's B image
+constexpr int TC_BIMG = 9 * TC_QIMG;                         // bytes of one layer's B images
 constexpr int TC_THREADS = 128;
 constexpr long long TC_WAIT_LIMIT = 1LL << 22;               // mbarrier polls before giving up
-static_assert(2 * TC_TILES * 16 <= TC_COLS && TC_BY % 4 == 0, "two buffers of tiles fit the tensor-memory allocation");
-// a tile starts at row 1 + 4j; taps reach one row and one position either side
+static_assert(TC_BIMG == DN_TAPS * DN_C * DN_C * 2, "the stacked images hold every tap once");
+static_assert(TC_COLS == 128 && TC_BY % 4 == 0, "the allocation is a power of two; 4 blocks fill the 512 columns");
+// a tile starts at row 1 + 4j; shifts reach one row and one position either side
 static_assert(TC_HX * 0 - 1 >= -TC_PAD && TC_HX * (TC_HY - 1) + TC_HX - 1 + 1 < TC_SPOS + TC_PAD,
-              "taps stay inside the slice and its padding");
+              "shifted operands stay inside the slice and its padding");
 
 struct TcShared {
    alignas(16) unsigned char plane[2][TC_PLANE];
@@ -145,16 +161,25 @@ struct TcShared {
 };
 constexpr size_t TC_SMEM = sizeof(TcShared);
 static_assert(TC_SMEM < (1u << 18), "operand addresses fit the descriptors' 14-bit start field");
+static_assert(TC_PLANE % 16 == 0 && TC_QIMG % 16 == 0, "descriptor strides are multiples of 16 bytes");
 
-// UMMA B images of one layer from FP32 W[27][16 cin][16 cout]: per tap, element
-// (n, k) at byte (k / 8) * 256 + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
-// B(n, k) = W[t][k][n] (forward) or W[t][n][k] (transposed)
+// UMMA B images of one layer from FP32 W[27][16 cin][16 cout]. For each
+// in-plane shift q = (sx + 1) + 3 (sy + 1), an N 48 x K 16 BF16 image, element
+// (n, k) at byte q * TC_QIMG + (k / 8) * 768 + (n / 8) * 128 + (n % 8) * 16 +
+// (k % 8) * 2 (K-major core matrices). N block b = n / 16 is the tap that takes
+// input slice z' to output slice z' - 1 + b: forward the tap (sx, sy, 1 - b)
+// with B(n, k) = W[t][k][n % 16]; the data gradient the tap (-sx, -sy, b - 1)
+// with B(n, k) = W[t][n % 16][k]. Tap t = (dx + 1) + 3 (dy + 1) + 9 (dz + 1).
 __global__ void k_dn_bimage(const float* W, __nv_bfloat16* img, int transposed) {
-   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (t, n, k)
-   if (e >= DN_TAPS * DN_C * DN_C) return;
-   const int k = e % DN_C, n = (e / DN_C) % DN_C, t = e / (DN_C * DN_C);
-   const float w = transposed ? W[(t * DN_C + n) * DN_C + k] : W[(t * DN_C + k) * DN_C + n];
-   img[t * 256 + (k / 8) * 128 + (n / 8) * 64 + (n % 8) * 8 + (k % 8)] = __float2bfloat16_rn(w);
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (q, n, k)
+   if (e >= 9 * TC_NB * DN_C) return;
+   const int k = e % DN_C, n = (e / DN_C) % TC_NB, q = e / (DN_C * TC_NB);
+   const int b = n / DN_C, c = n % DN_C;
+   const int sx = q % 3 - 1, sy = q / 3 - 1;
+   const int dx = transposed ? -sx : sx, dy = transposed ? -sy : sy, dz = transposed ? b - 1 : 1 - b;
+   const int t = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+   const float w = transposed ? W[(t * DN_C + c) * DN_C + k] : W[(t * DN_C + k) * DN_C + c];
+   img[q * (TC_QIMG / 2) + (k / 8) * (TC_NB * 8) + (n / 8) * 64 + (n % 8) * 8 + (k % 8)] = __float2bfloat16_rn(w);
 }
 
 __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
@@ -163,8 +188,8 @@ __device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned 
           ((unsigned long long)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
 }
 // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
-// K-major, N = 16, M = 128
-constexpr unsigned TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+// K-major, M = 128, N as given
+__host__ __device__ constexpr unsigned tcIdesc(unsigned n) { return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
 
 __device__ __forceinline__ bool tcWait(unsigned bar, unsigned parity) {
    for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
@@ -202,7 +227,6 @@ __device__ __forceinline__ void tcStageSlice(TcShared& sh, const DnGrid& g, cons
          *reinterpret_cast<uint4*>(dst) = v;
       }
    }
-   cpAsyncCommit();
 }
 
 // the staged data (generic-proxy and cp.async writes) made visible to the
@@ -218,7 +242,7 @@ __device__ __forceinline__ void tcPublish() {
 }
 
 template <bool TRANSPOSED>
-__device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int buf, int x0, int y0, int z,
+__device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int group, int x0, int y0, int z,
                                            const float* bias, int mode, unsigned* out, const unsigned* mask,
                                            float* out32, const float* res, const DnMoments& mom) {
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -226,7 +250,7 @@ __device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int b
 #pragma unroll
    for (int j = 0; j < TC_TILES; ++j) {
       unsigned* r = rr[j];
-      const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + 16u * (unsigned)(buf * TC_TILES + j);
+      const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(j * TC_TCOLS + 16 * group);
       asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
@@ -280,6 +304,48 @@ __device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int b
    }
 }
 
+// zeros into 16 tensor-memory columns of this warp's 32 lanes
+__device__ __forceinline__ void tcZero16(unsigned taddr) {
+   asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n"
+                ::"r"(taddr), "r"(0u)
+                : "memory");
+}
+
+__device__ __forceinline__ void tcMma(unsigned d, unsigned long long ad, unsigned long long bd, unsigned idesc) {
+   asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                :
+                : "r"(d), "l"(ad), "l"(bd), "r"(idesc), "r"(1), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// the MMAs of one input slice (both tiles, 9 shifts): A from the slice's slot
+// (descriptor words aHi:aLo), B from the stacked images (bHi:bLo), output
+// slices z' - 1, z', z' + 1 into groups A0, A0 + 1, A0 + 2 (mod 4) of each tile
+template <int A0>
+__device__ __forceinline__ void tcIssue(unsigned tmem, unsigned aHi, unsigned aLo, unsigned bHi, unsigned bLo) {
+#pragma unroll
+   for (int j = 0; j < TC_TILES; ++j) {
+      const unsigned dT = tmem + (unsigned)(j * TC_TCOLS);
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+         const int sx = q % 3 - 1, sy = q / 3 - 1;
+         const int pos = TC_PAD + TC_HX * (1 + 4 * j + sy) + sx;   // compile-time, 16-byte units
+         const unsigned long long ad = ((unsigned long long)aHi << 32) | (aLo + (unsigned)pos);
+         const unsigned bq = bLo + (unsigned)(q * (TC_QIMG >> 4));
+         const unsigned long long b0 = ((unsigned long long)bHi << 32) | bq;
+         if (A0 <= 1) {
+            tcMma(dT + 16u * A0, ad, b0, tcIdesc(48));
+         } else if (A0 == 2) {   // groups 2, 3 | 0
+            tcMma(dT + 32u, ad, b0, tcIdesc(32));
+            tcMma(dT, ad, ((unsigned long long)bHi << 32) | (bq + (512u >> 4)), tcIdesc(16));
+         } else {                // groups 3 | 0, 1
+            tcMma(dT + 48u, ad, b0, tcIdesc(16));
+            tcMma(dT, ad, ((unsigned long long)bHi << 32) | (bq + (256u >> 4)), tcIdesc(32));
+         }
+      }
+   }
+}
+
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(TC_THREADS)
 k_dn_conv_tc(DnGrid g, const unsigned* in, const __nv_bfloat16* bimg, const float* bias, int mode, unsigned* out,
@@ -289,6 +355,7 @@ k_dn_conv_tc(DnGrid g, const unsigned* in, const __nv_bfloat16* bimg, const floa
    const int tid = threadIdx.x, warp = tid >> 5;
    const int x0 = blockIdx.x * TC_BX, y0 = blockIdx.y * TC_BY, z0 = blockIdx.z * TC_ZC;
    const int nzc = min(TC_ZC, g.nz - z0);
+   const int nin = nzc + 2;   // input slices z0 - 1 .. z0 + nzc; input i is slice z0 - 1 + i, in slot i % 4
    const unsigned planeBase = (unsigned)__cvta_generic_to_shared(&sh.plane[0][0]);
    const unsigned bimgBase = (unsigned)__cvta_generic_to_shared(&sh.bimg[0]);
    // tensor memory (one warp), mbarriers (one thread)
@@ -304,7 +371,7 @@ k_dn_conv_tc(DnGrid g, const unsigned* in, const __nv_bfloat16* bimg, const floa
       }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
-   // the weights, the slices' zero padding, and input slices z0 - 1 .. z0 + 1 (ring slots 0-2)
+   // the weights, the slices' zero padding, and input slices 0-2 (slots 0-2)
    {
       const uint4* src = reinterpret_cast<const uint4*>(bimg);
       for (int e = tid; e < TC_BIMG / 16; e += TC_THREADS) cpAsync16(&sh.bimg[16 * e], src + e, 16);
@@ -315,74 +382,77 @@ k_dn_conv_tc(DnGrid g, const unsigned* in, const __nv_bfloat16* bimg, const floa
          *reinterpret_cast<uint4*>(&sh.plane[h][slot * TC_SLOT + 16 * pos]) = make_uint4(0u, 0u, 0u, 0u);
       }
       for (int k = 0; k < 3; ++k) tcStageSlice(sh, g, in, mom, x0, y0, z0 - 1 + k, k);
+      cpAsyncCommit();
    }
    tcPublish<0>();
    const unsigned tmem = sh.tmemBase;
-   constexpr int sgn = TRANSPOSED ? -1 : 1;
+   const unsigned lanes = (unsigned)(32 * warp) << 16;
+   // every accumulator group starts at zero
+#pragma unroll
+   for (int c = 0; c < TC_COLS; c += 16) tcZero16(tmem + lanes + (unsigned)c);
+   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+   tcPublish<0>();
+   // descriptors: the low word holds the start address >> 4 (14 bits, no carry into LBO for
+   // shared addresses below 256 KB), so an operand's descriptor is a base plus a constant
+   const unsigned long long a0 = umma_desc(planeBase, TC_PLANE, 128);
+   const unsigned long long b0 = umma_desc(bimgBase, TC_NB * 16, 128);
+   const unsigned aHi = (unsigned)(a0 >> 32), aLo0 = (unsigned)a0, bHi = (unsigned)(b0 >> 32), bLo = (unsigned)b0;
    bool timedOut = false;
-   for (int i = 0; i < nzc && !timedOut; ++i) {
-      // slice zz is in slot (zz - z0 + 1) mod TC_RING: slices z - 1 .. z + 1 (z = z0 + i) are
-      // in slots i .. i + 2; slice z + 2 is requested below as soon as its slot is free
-      const int buf = i & 1;
+   int lastCommit = -1;   // the input slice whose commit covers every MMA issued so far
+   for (int i = 0; i < nin && !timedOut; ++i) {
+      lastCommit = i;
       if (tid == 0) {
-         // descriptors: the low word holds the start address >> 4 (14 bits, no carry into LBO
-         // for shared addresses below 256 KB), so a tap's descriptor is a base plus a constant
-         const unsigned long long a0 = umma_desc(planeBase, TC_PLANE, 128);
-         const unsigned long long b0 = umma_desc(bimgBase, 256, 128);
-         unsigned slotLo[3];
-#pragma unroll
-         for (int q = 0; q < 3; ++q) {
-            const int dzq = sgn * (q - 1);
-            slotLo[q] = (unsigned)a0 + (unsigned)(((i + 1 + dzq) % TC_RING) * (TC_SLOT >> 4));
+         const unsigned aLo = aLo0 + (unsigned)((i % TC_RING) * (TC_SLOT >> 4));
+         switch (i & 3) {   // output slice o of input i's N block b is i - 2 + b, in group (o + 2) & 3
+         case 0: tcIssue<0>(tmem, aHi, aLo, bHi, bLo); break;
+         case 1: tcIssue<1>(tmem, aHi, aLo, bHi, bLo); break;
+         case 2: tcIssue<2>(tmem, aHi, aLo, bHi, bLo); break;
+         default: tcIssue<3>(tmem, aHi, aLo, bHi, bLo); break;
          }
-         const unsigned aHi = (unsigned)(a0 >> 32), bHi = (unsigned)(b0 >> 32), bLo = (unsigned)b0;
-#pragma unroll
-         for (int j = 0; j < TC_TILES; ++j) {
-            const unsigned d = tmem + 16u * (unsigned)(buf * TC_TILES + j);
-#pragma unroll
-            for (int t = 0; t < DN_TAPS; ++t) {
-               const int dx = sgn * (t % 3 - 1), dy = sgn * ((t / 3) % 3 - 1);
-               const int pos = TC_PAD + TC_HX * (1 + 4 * j + dy) + dx;   // compile-time
-               const unsigned aLo = slotLo[t / 9] + (unsigned)pos;       // 16-byte units
-               const unsigned long long ad = ((unsigned long long)aHi << 32) | aLo;
-               const unsigned long long bd = ((unsigned long long)bHi << 32) | (bLo + 32u * (unsigned)t);
-               asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-                            :
-                            : "r"(d), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(t > 0 ? 1 : 0), "r"(0), "r"(0), "r"(0),
-                              "r"(0));
-            }
-         }
-         const unsigned b = (unsigned)__cvta_generic_to_shared(&sh.bar[buf]);
+         const unsigned b = (unsigned)__cvta_generic_to_shared(&sh.bar[i & 1]);
          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(b) : "memory");
       }
       if (i > 0) {
-         // the previous slice's MMAs done: its slot z - 2 takes slice z + 2 (requested now, so
-         // that the copy runs during the epilogue), its accumulators go through the epilogue
+         // input i - 1's MMAs done: output slice i - 3 is complete, slot (i - 1) % 4 is free
          const int pb = (i - 1) & 1;
-         if (!tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[pb]), (unsigned)(((i - 1) >> 1) & 1))) {
+         // warp-uniform outcome: the epilogue's tcgen05.ld / .st are warp-collective
+         if (!__all_sync(0xffffffffu, tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[pb]), (unsigned)(((i - 1) >> 1) & 1)))) {
             timedOut = true;
          } else {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (i + 2 <= nzc) tcStageSlice(sh, g, in, mom, x0, y0, z0 + i + 2, (i + 3) % TC_RING);
-            tcEpilogue<TRANSPOSED>(g, tmem, pb, x0, y0, z0 + i - 1, bias, mode, out, mask, out32, res, mom);
+            if (i + 3 < nin) tcStageSlice(sh, g, in, mom, x0, y0, z0 + 2 + i, (i + 3) % TC_RING);
+            const int o = i - 3, grp = (i + 3) & 3;   // (o + 2) & 3
+            if (o >= 0) tcEpilogue<TRANSPOSED>(g, tmem, grp, x0, y0, z0 + o, bias, mode, out, mask, out32, res, mom);
+            if (i + 1 < nin) {   // the group's next output slice, o + 4, takes its first MMA from input i + 1
+#pragma unroll
+               for (int j = 0; j < TC_TILES; ++j) tcZero16(tmem + lanes + (unsigned)(j * TC_TCOLS + 16 * grp));
+               asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            }
          }
-      } else if (i + 2 <= nzc) {
-         tcStageSlice(sh, g, in, mom, x0, y0, z0 + 2, 3 % TC_RING);   // slot 3 is still free
+      } else if (3 < nin) {
+         tcStageSlice(sh, g, in, mom, x0, y0, z0 + 2, 3);   // slot 3 is still free
       }
+      cpAsyncCommit();   // one group per iteration, empty or not
       timedOut = __syncthreads_or(timedOut);
-      tcPublish<0>();
+      tcPublish<1>();    // the copies issued now may stay in flight: their slice is read 3 iterations on
    }
    if (!timedOut) {
-      const int lb = (nzc - 1) & 1;
-      if (!tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[lb]), (unsigned)(((nzc - 1) >> 1) & 1))) {
+      const int lb = (nin - 1) & 1;
+      if (!__all_sync(0xffffffffu, tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[lb]), (unsigned)(((nin - 1) >> 1) & 1)))) {
          timedOut = true;
       } else {
          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-         tcEpilogue<TRANSPOSED>(g, tmem, lb, x0, y0, z0 + nzc - 1, bias, mode, out, mask, out32, res, mom);
+         tcEpilogue<TRANSPOSED>(g, tmem, (nzc + 1) & 3, x0, y0, z0 + nzc - 1, bias, mode, out, mask, out32, res, mom);
       }
    }
-   if (timedOut && tid == 0) raiseError(err, RHGPU_DEVERR_DENOISER);
+   if (timedOut) {
+      // the MMAs issued so far may still run: wait (bounded again) for the last commit
+      // before the tensor memory is freed
+      if (tid == 0) raiseError(err, RHGPU_DEVERR_DENOISER);
+      if (lastCommit >= 0)
+         tcWait((unsigned)__cvta_generic_to_shared(&sh.bar[lastCommit & 1]), (unsigned)((lastCommit >> 1) & 1));
+   }
+   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
    __syncthreads();
    if (warp == 0) {

@@ -284,7 +284,7 @@ __global__ void k_ext_bc(GridInfo g, Fields f, FieldParams fp, const int* ext, i
    }
 }
 
-__global__ void k_node_fused(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
+__global__ void __launch_bounds__(128, 8) k_node_fused(GridInfo g, Fields f, FieldParams fp, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
    for (int l = 0; l < 3; ++l) f.cellAvgB[l * N + n] += f.cellB[l * N + n];
    if (!plusOk(g, i, j, k)) return;
@@ -421,7 +421,7 @@ __global__ void k_node_fused(GridInfo g, Fields f, FieldParams fp, unsigned long
 }
 
 template <bool FARADAY>
-__global__ void k_cell_fused(GridInfo g, Fields f, FieldParams fp, int useEp, unsigned long long* cnt) {
+__global__ void __launch_bounds__(128, 8) k_cell_fused(GridInfo g, Fields f, FieldParams fp, int useEp, unsigned long long* cnt) {
    RH_CELL_PROLOGUE
    const bool inner = allNb(g, i, j, k);
    bool clamp = false;

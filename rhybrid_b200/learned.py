@@ -335,10 +335,43 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     return res
 
 
+def apply_timing(scale: float = 1.0, ppc: float = 8.0, warmup: int = 3, steps: int = 10, seed: int = 5) -> dict:
+    """Cost of the denoiser inside the step: a C4 context at `ppc` with the
+    network applied between deposit and field update (untrained weights
+    slightly perturbed, so every layer computes), `warmup` untimed steps, then
+    `steps` steps with the library's per-kernel CUDA-event timer. The
+    convolutions execute 3 x 27 x 16 x 16 x 2 flop per voxel on the tensor
+    cores (layer 0 has 4 input and layer 2 4 output channels, padded to 16)."""
+    lib = abi.gpu_library()
+    cfg = c4_config(ppc, scale)
+    ctx = filled_context(lib, cfg, seed)
+    net = abi.Denoiser(lib, cfg.nx, cfg.ny, cfg.nz, cfg.periodic)
+    try:
+        net.set_scales(*moment_scales(cfg))
+        net.set_params(init_params(0) * 1.01)
+        ctx.set_denoiser(net, True)
+        ctx.step(warmup)
+        ctx.set_timing(True)
+        ctx.step(steps)
+        t = {k: v / steps for k, v in ctx.timing().items()}
+        ctx.set_timing(False)
+    finally:
+        ctx.close()
+        net.close()
+    voxels = cfg.nx * cfg.ny * cfg.nz
+    flop = 3 * TAPS * C * C * 2 * voxels
+    ms = t.get("dn_apply", 0.0)
+    return {"geometry": [cfg.nx, cfg.ny, cfg.nz], "ppc": ppc, "steps": steps, "dn_apply_ms_per_step": ms,
+            "step_ms": sum(t.values()), "executed_tflops": flop / (ms * 1e-3) / 1e12 if ms > 0 else None,
+            "kernel_ms": t}
+
+
 def main(argv=None):
     import argparse
     import json
     ap = argparse.ArgumentParser(description="the learned form in closed loop against a high-ppc check run")
+    ap.add_argument("--apply-only", action="store_true",
+                    help="only time the denoiser applied inside the step (apply_timing) at --scale")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--judge-ppc", type=int, default=256)
     ap.add_argument("--train-steps", type=int, default=100)
@@ -347,6 +380,10 @@ def main(argv=None):
     ap.add_argument("--plain", default="8,16,32,64,128")
     ap.add_argument("--json", default=None)
     a = ap.parse_args(argv)
+    if a.apply_only:
+        out = apply_timing(scale=a.scale)
+        print(json.dumps(out))
+        return
     out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
                       adam_steps=a.adam_steps, plain_ppcs=tuple(int(x) for x in a.plain.split(",")))
     print(json.dumps(out))
