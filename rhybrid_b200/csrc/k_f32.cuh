@@ -175,9 +175,44 @@ __device__ inline void cicWeightsF(const float o[3], float wq, float w8[8]) {
 
 constexpr int REC32 = 11;   // floats per deposit record: w8[8], v[3]
 
+// shared memory of k_f32_push_deposit
+constexpr int F32_PTRS = 14;   // one species' arrays offset to the segment: current cell, o, v (0-6), next (7-13)
+struct F32PushShared {
+   float rec[FT * REC32];                   // deposit records of a chunk; at the end acc[SEG][32]
+   float pf[7][FT];                         // the next chunk's particles: cell (int bits), o[3], v[3]
+   SegFields32 f;                           // field stencil of the segment
+   void* ptr[FAST_MAX_SPECIES][F32_PTRS];
+   StencilRow rows[SF_MAX_ROWS];
+   alignas(8) unsigned char wd[SEG][FW];    // records per (dual cell, warp)
+   int rank[FT];                            // stayers of the chunk before each chunk position
+   int wcnt[FW];                            // stayers per warp
+   int prefix[FAST_MAX_SPECIES + 1];        // first particle of each species in the segment
+   int stay[FAST_MAX_SPECIES];              // stayers of each species so far
+};
+
+// chunk position tid of the chunk starting at c0 requested into pf (cp.async)
+__device__ __forceinline__ void f32Prefetch(F32PushShared& sh, int i, int total, int ns, int s0) {
+   const int tid = threadIdx.x;
+   if (i < total) {
+      int s = s0;
+      while (s + 1 < ns && i >= sh.prefix[s + 1]) ++s;
+      const int p = i - sh.prefix[s];
+#pragma unroll
+      for (int a = 0; a < 7; ++a) cpAsync4(&sh.pf[a][tid], (const float*)sh.ptr[s][a] + p);
+   }
+   cpAsyncCommit();
+}
+
 // PER: the periodic axes (bit a = axis a), fixed at compile time; the host
 // launches the instantiation that matches the grid
 // GC: the variant that also counts the per-cell maxVi constraint (grid counters on)
+//
+// One block per segment, one thread per particle, chunks of FT particles in
+// storage order (species after species), as k_fast_push_deposit: the next
+// chunk's particles are copied to shared memory (cp.async) while the current
+// one is processed, two barriers per chunk, per-warp record counts packed in
+// bytes, a leaving particle's mover slot reserved before the second barrier
+// and written after the deposit sums.
 template <int PER, bool GC>
 __global__ void __launch_bounds__(FT, 4)
 k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp, F32Bufs fb, double* cntd,
@@ -186,15 +221,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
    g.per[0] = PER & 1;
    g.per[1] = (PER >> 1) & 1;
    g.per[2] = (PER >> 2) & 1;
-   __shared__ float s_rec[FT * REC32];            // deposit records of a chunk; at the end acc[SEG][32]
-   __shared__ int s_wd[FW][SEG];                  // records per (warp, dual cell), then their first sorted slot
-   __shared__ int s_bin[SEG + 1];                 // first sorted record of each dual cell
-   __shared__ int s_wcnt[FW];                     // stayers per warp, then the stayers of the warps before
-   __shared__ unsigned s_bs[FW];
-   __shared__ int s_prefix[FAST_MAX_SPECIES + 1];
-   __shared__ int s_stay[FAST_MAX_SPECIES];
-   __shared__ SegFields32 s_f;
-   __shared__ StencilRow s_rows[SF_MAX_ROWS];
+   __shared__ F32PushShared sh;
    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
    const unsigned below = (1u << lane) - 1u;
    const long long S = blockIdx.x;
@@ -204,19 +231,35 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
    const int ndx = fg.nd[0];
    const int u0 = gseg * SEG, u1 = min(u0 + SEG, ndx);
    const int ns = FS.ns;
-   if (tid == 0) {
-      int a = 0;
-      for (int s = 0; s < ns; ++s) {
-         s_prefix[s] = a;
-         a += FS.st[s].cur.cnt[S];
+   // set-up: species prefix (warp 0), segment pointers (warps 1-4)
+   if (warp == 0) {
+      const int cnt = lane < ns ? FS.st[lane].cur.cnt[S] : 0;
+      int x = cnt;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+         const int y = __shfl_up_sync(0xffffffffu, x, o);
+         if (lane >= o) x += y;
       }
-      s_prefix[ns] = a;
+      if (lane <= ns) sh.prefix[lane] = x - cnt;
+      if (lane < FAST_MAX_SPECIES) sh.stay[lane] = 0;
+   } else if (tid < 32 + F32_PTRS * ns) {
+      const int q = tid - 32, s = q / F32_PTRS, k = q - s * F32_PTRS;
+      const F32Species& SS = FS.st[s];
+      const long long b = SS.base[S];
+      const F32Buf& B = k < 7 ? SS.cur : SS.nxt;
+      const int kk = k < 7 ? k : k - 7;
+      void* v;
+      if (kk == 0) v = B.cell + b;
+      else if (kk < 4) v = B.o[kk - 1] + b;
+      else v = B.v[kk - 4] + b;
+      sh.ptr[s][k] = v;
    }
-   if (tid < FAST_MAX_SPECIES) s_stay[tid] = 0;
    const int by0 = dualB(uy, g.per[1]), bz0 = dualB(uz, g.per[2]);
-   stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, s_f, s_rows);
+   // (stageSegRows' own barrier publishes the prefix and the pointers)
+   stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, sh.f, sh.rows);
    __syncthreads();
-   const int total = s_prefix[ns];
+   const int total = sh.prefix[ns];
+   f32Prefetch(sh, tid, total, ns, 0);
    const int myDual = tid >> 3, myCorner = tid & 7;
    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
 
@@ -225,18 +268,16 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       const bool active = i < total;
       int s = 0;
       if (active)
-         while (s + 1 < ns && i >= s_prefix[s + 1]) ++s;
+         while (s + 1 < ns && i >= sh.prefix[s + 1]) ++s;
       float o[3], v[3];
-      int cell = 0;
-      long long p = 0;
+      int cell = 0, p = 0;
       bool stay = false, rec = false, leave = false, clamp = false;
       int mflags = 0, vx = 0, vy = 0, vz = 0, ti = 0, tj = 0, tk = 0;
+      cpAsyncWaitAll();   // this thread's copies of the chunk
       if (active) {
-         const F32Species& SS = FS.st[s];
-         p = i - s_prefix[s];
-         const long long slot = SS.base[S] + p;
-         cell = SS.cur.cell[slot];
-         for (int a = 0; a < 3; ++a) { o[a] = SS.cur.o[a][slot]; v[a] = SS.cur.v[a][slot]; }
+         p = i - sh.prefix[s];
+         cell = __float_as_int(sh.pf[0][tid]);
+         for (int a = 0; a < 3; ++a) { o[a] = sh.pf[1 + a][tid]; v[a] = sh.pf[4 + a][tid]; }
          const int sx = halfSf(o[0]), sy = halfSf(o[1]), sz = halfSf(o[2]);
          int cj = by0 + 1 - sy, ck = bz0 + 1 - sz;
          if (cj >= g.ny) cj -= g.ny;
@@ -244,7 +285,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
          const int ci = cell - g.nx * (cj + g.ny * ck);
          const int lu = dualU(ci + sx - 1, g.nx, g.per[0]) - u0;
          const int lc = lu + 1 - sx, ly = 1 - sy, lz = 1 - sz;
-         clamp = pushF32(g, s_f, FS, s, pp, ci, cj, ck, lc, ly, lz, o, v);
+         clamp = pushF32(g, sh.f, FS, s, pp, ci, cj, ck, lc, ly, lz, o, v);
          if (isnan(o[0]) || isnan(o[1]) || isnan(o[2])) raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
          int ox, oy, oz;
          int bad = migrateAxisF(o[0], ox, pp.below1);
@@ -294,106 +335,114 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       if (clamp) atomicAdd(&cntu[CNT_SPECIES_MAXVI + s], 1ull);
       if (GC) gridCountAtomic(f, GC_CELL_MAX_VI, g.N, cell, clamp);
 
+      // ---- order of the chunk's stayers and records (warp-local first) ---------------------
       const unsigned bs = __ballot_sync(0xffffffffu, stay), br = __ballot_sync(0xffffffffu, rec);
-      if (lane == 0) {
-         s_wcnt[warp] = __popc(bs);
-         s_bs[warp] = bs;
-      }
-      s_wd[warp][lane] = 0;
+      if (lane == 0) sh.wcnt[warp] = __popc(bs);
+      sh.wd[lane][warp] = 0;
       __syncwarp();
       const int rd = rec ? vx - u0 : 0;
       int rrank = 0;
       if (rec) {
          const unsigned mm = __match_any_sync(br, rd);
          rrank = __popc(mm & below);
-         if (rrank == 0) s_wd[warp][rd] = __popc(mm);
+         if (rrank == 0) sh.wd[rd][warp] = (unsigned char)__popc(mm);
       }
       __syncthreads();
-      if (warp == 0) {
-         int t = 0;
-         int c[FW];
-         for (int w = 0; w < FW; ++w) { c[w] = s_wd[w][lane]; t += c[w]; }
+      // every shared-memory read of this chunk's particles is done: request the next chunk's
+      f32Prefetch(sh, i + FT, total, ns, s);
+      // every warp, per dual cell (lane): the first sorted record of the dual cell
+      // (bin) and of this warp's records for it (off)
+      int binD, offD, nrec;
+      {
+         const uint2 c8 = *reinterpret_cast<const uint2*>(&sh.wd[lane][0]);
+         const int t = (int)(((c8.x * 0x01010101u) >> 24) + ((c8.y * 0x01010101u) >> 24));
+         const unsigned mlo = warp >= 4 ? 0xffffffffu : (1u << (8 * warp)) - 1u;
+         const unsigned mhi = warp <= 4 ? 0u : (1u << (8 * (warp - 4))) - 1u;
+         const int before = (int)((((c8.x & mlo) * 0x01010101u) >> 24) + (((c8.y & mhi) * 0x01010101u) >> 24));
          int x = t;
          for (int q = 1; q < 32; q <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, q);
             if (lane >= q) x += y;
          }
-         int b = x - t;
-         s_bin[lane] = b;
-         if (lane == 31) s_bin[SEG] = x;
-         for (int w = 0; w < FW; ++w) { s_wd[w][lane] = b; b += c[w]; }
-         const int sw = lane < FW ? s_wcnt[lane] : 0;
-         int xs = sw;
-         for (int q = 1; q < FW; q <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, xs, q);
-            if (lane >= q) xs += y;
-         }
-         __syncwarp();
-         if (lane < FW) s_wcnt[lane] = xs - sw;
+         binD = x - t;
+         offD = binD + before;
+         nrec = __shfl_sync(0xffffffffu, x, 31);
       }
-      {
-         const unsigned lm = __ballot_sync(0xffffffffu, leave);
-         if (lm) {
-            const int leader = __ffs(lm) - 1;
-            unsigned long long b0 = 0;
-            if (lane == leader) b0 = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
-            b0 = __shfl_sync(0xffffffffu, b0, leader);
-            if (leave) {
-               const unsigned long long m = b0 + __popc(lm & below);
-               if ((long long)m < fb.moverCap) {
-                  Mover32& M = fb.movers[m];
-                  for (int a = 0; a < 3; ++a) { M.o[a] = o[a]; M.v[a] = v[a]; }
-                  M.cell = (int)cidx(g, ti, tj, tk);
-                  M.species = s;
-                  M.key = ((unsigned long long)S << 32) | (unsigned long long)p;
-                  const int gd = vx / SEG;
-                  M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * fg.nseg + gd;
-                  M.lx = (vx - gd * SEG) | mflags;
-               } else {
-                  raiseError(err, RHGPU_DEVERR_CAPACITY);
-               }
-            }
-         }
-      }
-      __syncthreads();
-      if (stay) {
-         const int stayIdx = s_wcnt[warp] + __popc(bs & below);
-         // (zero unless the species starts inside this chunk)
-         const int p0 = s_prefix[s] - c0;
-         const int firstIdx = p0 > 0 ? stayersIn(s_bs, 0, p0) : 0;
-         const F32Species& SS = FS.st[s];
-         const long long slot = SS.base[S] + s_stay[s] + (stayIdx - firstIdx);
-         SS.nxt.cell[slot] = (int)cidx(g, ti, tj, tk);
-         for (int a = 0; a < 3; ++a) { SS.nxt.o[a][slot] = o[a]; SS.nxt.v[a][slot] = v[a]; }
-      }
-      const int stayAdd = tid < ns ? stayersIn(s_bs, max(s_prefix[tid], c0) - c0, min(s_prefix[tid + 1], c0 + FT) - c0) : 0;
+      const int recPos = __shfl_sync(0xffffffffu, offD, rd) + rrank;
+      const int sumLo = __shfl_sync(0xffffffffu, binD, myDual);
+      const int sumHiN = __shfl_sync(0xffffffffu, binD, (myDual + 1) & 31);
+      const int sumHi = myDual == SEG - 1 ? nrec : sumHiN;
+      // stayers of the chunk before this position (and in all), and this species' count so far
+      const int wc = lane < FW ? sh.wcnt[lane] : 0;
+      const int myRank = (int)__reduce_add_sync(0xffffffffu, (unsigned)(lane < warp ? wc : 0)) + __popc(bs & below);
+      const int chunkStay = (int)__reduce_add_sync(0xffffffffu, (unsigned)wc);
+      sh.rank[tid] = myRank;
+      const int stayBase = stay ? sh.stay[s] : 0;
+      // mover slots reserved now, written after the sums
+      const unsigned lm = __ballot_sync(0xffffffffu, leave);
+      const int leader = lm ? __ffs(lm) - 1 : 0;
+      unsigned long long mb = 0;
+      if (lm && lane == leader) mb = atomicAdd(fb.nmovers, (unsigned long long)__popc(lm));
       if (rec) {
          float w8[8];
          cicWeightsF(o, FS.wqRel[s], w8);
-         float* r = s_rec + (s_wd[warp][rd] + rrank) * REC32;
+         float* r = sh.rec + recPos * REC32;
          for (int q = 0; q < 8; ++q) r[q] = w8[q];
          r[8] = v[0]; r[9] = v[1]; r[10] = v[2];
       }
       __syncthreads();
-      if (tid < ns) s_stay[tid] += stayAdd;
-      {
-         const int r1 = s_bin[myDual + 1];
-#pragma unroll 2
-         for (int r = s_bin[myDual]; r < r1; ++r) {
-            const float* rr = s_rec + r * REC32;
-            const float w = rr[myCorner];
-            a0 += w;
-            a1 += w * rr[8];
-            a2 += w * rr[9];
-            a3 += w * rr[10];
+      if (stay) {
+         const int p0 = sh.prefix[s] - c0;   // chunk position of the species' first particle
+         const int q = stayBase + myRank - (p0 > 0 ? sh.rank[p0] : 0);
+         ((int*)sh.ptr[s][7])[q] = (int)cidx(g, ti, tj, tk);
+         for (int a = 0; a < 3; ++a) {
+            ((float*)sh.ptr[s][8 + a])[q] = o[a];
+            ((float*)sh.ptr[s][11 + a])[q] = v[a];
          }
       }
+      // running stayer count of each species
+      if (tid < ns) {
+         const int lo = min(max(sh.prefix[tid] - c0, 0), FT), hi = min(max(sh.prefix[tid + 1] - c0, 0), FT);
+         const int rlo = lo < FT ? sh.rank[lo] : chunkStay, rhi = hi < FT ? sh.rank[hi] : chunkStay;
+         sh.stay[tid] += rhi - rlo;
+      }
+      // ---- sums of this thread's (dual cell, corner), records in list order ----------------
+#pragma unroll 2
+      for (int r = sumLo; r < sumHi; ++r) {
+         const float* rr = sh.rec + r * REC32;
+         const float w = rr[myCorner];
+         a0 += w;
+         a1 += w * rr[8];
+         a2 += w * rr[9];
+         a3 += w * rr[10];
+      }
+      // ---- particles that left the segment -----------------------------------------------
+      if (lm) {
+         mb = __shfl_sync(0xffffffffu, mb, leader);
+         if (leave) {
+            const unsigned long long m = mb + __popc(lm & below);
+            if ((long long)m < fb.moverCap) {
+               Mover32& M = fb.movers[m];
+               for (int a = 0; a < 3; ++a) { M.o[a] = o[a]; M.v[a] = v[a]; }
+               M.cell = (int)cidx(g, ti, tj, tk);
+               M.species = s;
+               M.key = ((unsigned long long)S << 32) | (unsigned long long)p;
+               const int gd = vx / SEG;
+               M.dest = ((long long)vy + (long long)fg.nd[1] * vz) * fg.nseg + gd;
+               M.lx = (vx - gd * SEG) | mflags;
+            } else {
+               raiseError(err, RHGPU_DEVERR_CAPACITY);
+            }
+         }
+      }
+      // no barrier here: the next chunk's first barrier orders the reads of rec,
+      // rank and stay before their next writes
    }
 
    __syncthreads();
-   if (tid < ns) FS.st[tid].nxt.cnt[S] = s_stay[tid];
+   if (tid < ns) FS.st[tid].nxt.cnt[S] = sh.stay[tid];
    {
-      float* q = s_rec + myDual * 32 + myCorner * 4;
+      float* q = sh.rec + myDual * 32 + myCorner * 4;
       q[0] = a0; q[1] = a1; q[2] = a2; q[3] = a3;
    }
    __syncthreads();
@@ -412,13 +461,13 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
          if (x >= nx) continue;
          hi = lo + 1 < u1 ? dl + 1 : -1;
       }
-      float val = s_rec[dl * 32 + ((1 + 2 * qq) << 2) + m];
-      if (hi >= 0) val = val + s_rec[hi * 32 + ((2 * qq) << 2) + m];
+      float val = sh.rec[dl * 32 + ((1 + 2 * qq) << 2) + m];
+      if (hi >= 0) val = val + sh.rec[hi * 32 + ((2 * qq) << 2) + m];
       fb.RP[(((long long)qq * nrows + row) * nx + x) * 4 + m] = val;
    }
    if (tid < 16 && (g.per[0] ? fg.nseg > 1 : gseg >= 1)) {
       const int qq = tid >> 2, m = tid & 3;
-      fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = s_rec[((2 * qq) << 2) + m];
+      fb.RPB[(((long long)qq * nrows + row) * fg.nseg + gseg) * 4 + m] = sh.rec[((2 * qq) << 2) + m];
    }
 }
 

@@ -442,20 +442,6 @@ __device__ __forceinline__ void segPartialsOut(const GridInfo& g, const FastGeom
    }
 }
 
-// ---- per-thread asynchronous global -> shared copies (cp.async) ----------------------------------
-// bytes = 0 copies nothing and writes zeros (the source address is not read)
-__device__ __forceinline__ void cpAsync8(void* sdst, const void* gsrc, int bytes) {
-   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
-}
-// 16-byte form (both addresses 16-byte aligned)
-__device__ __forceinline__ void cpAsync16(void* sdst, const void* gsrc, int bytes) {
-   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // one species' arrays offset to the block's segment: current x..w (0-6), next
 // x..w (7-13), current lx (14), next lx (15)
 constexpr int SEG_PTRS = 16;

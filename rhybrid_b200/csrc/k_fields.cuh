@@ -8,7 +8,7 @@
 //   k_node_fused         cell2Node of B, rhoq, Ji + cellAverageB, calcNodeJ
 //                        (USE_EDGE_J), calcNodeUe, upwindNodeB, calcNodeE
 //                        (:1059-1089, :157-167, :1449-1522, :1524-1584, :1268-1339, :1392-1446)
-//   k_cell_fused         node2Cell(J) + calcCellUe, calcCellEp, faceCurl
+//   k_cell_tiled         node2Cell(J) + calcCellUe, calcCellEp, faceCurl
 //                        (:1092-1112, :1342-1387, :1674-1737, :1587-1671)
 //   k_ext_cell_neumann3  neumannCell of one 3-vector      (:443-655)
 //   k_node2cell3, k_cell2node3, k_node_avg, k_faraday   nodeE smoothing and the
@@ -235,11 +235,15 @@ __global__ void k_faraday(GridInfo g, Fields f) {
 //                 whistler limiter d), then calcNodeUe, upwindNodeB and calcNodeE;
 //                 the averaged nodeB that the whistler limiter reads stays in
 //                 registers, the upwind weights re-read the same eight cells
-//   k_cell_fused  per cell: node2Cell of nodeJ and calcCellUe, calcCellEp (the
+//   k_cell_tiled  per cell: node2Cell of nodeJ and calcCellUe, calcCellEp (the
 //                 gradient of face-averaged nodeRhoQi), and (FARADAY: no E
 //                 smoothing) faceCurl, faceB += dt curl E; none of them reads
 //                 what another writes
-// The cellUe Neumann pass (k_ext_cell_neumann3) follows k_cell_fused; calcNodeUe
+// k_cell_tiled reads its eight-point stencils from node layers staged in shared
+// memory. The node pass reads its cells directly: its FP64 work per node (eight
+// square roots and divisions) keeps it issue-bound, and a staged version with
+// fewer resident warps took 0.42 ms against 0.33 ms for this one.
+// The cellUe Neumann pass (k_ext_cell_neumann3) follows k_cell_tiled; calcNodeUe
 // and calcNodeE do not read cellUe, so its place before them in the reference's
 // order does not matter.
 __global__ void k_ext_bc(GridInfo g, Fields f, FieldParams fp, const int* ext, int next) {
@@ -420,21 +424,58 @@ __global__ void __launch_bounds__(128, 8) k_node_fused(GridInfo g, Fields f, Fie
    for (int l = 0; l < 3; ++l) f.nodeE[l * N + n] = E[l];
 }
 
+// ---- the cell pass, its node stencil in shared memory ------------------------------------------
+// A block of 32 x 4 cells marches NT_Z planes along z; the node layers k - 1
+// and k that a plane of cells reads (nodeJ, nodeRhoQi, nodeE over 33 x 5 nodes
+// from (i0 - 1, j0 - 1)) sit in a ring of three layer slots, the next one
+// copied in with cp.async while the current plane is computed, so every node
+// value is loaded once per block instead of once per cell reading it.
+constexpr int NT_X = 32, NT_Y = 4, NT_Z = 8;
+constexpr int NT_LX = NT_X + 1, NT_LY = NT_Y + 1;
+constexpr int CT_ARR = 7;    // nodeJ x 3, nodeRhoQi, nodeE x 3
+constexpr int CT_LAYER = CT_ARR * NT_LY * NT_LX;
+constexpr size_t CT_SMEM = 3 * CT_LAYER * sizeof(double);
+
+// node (dx, dy, dz) in {-1, 0}^3 of a cell's stencil, o = (dx + 1) + 2 (dy + 1) + 4 (dz + 1)
+struct CellStencil {
+   const double* L;   // node layer k - 1
+   const double* U;   // node layer k
+   int off;           // this cell's (x, y) in a layer
+   __device__ __forceinline__ double at(int a, int o) const {
+      return ((o & 4) ? U : L)[a * (NT_LY * NT_LX) + off + ((o >> 1) & 1) * NT_LX + (o & 1)];
+   }
+   __device__ __forceinline__ double nj(int l, int o) const { return at(l, o); }
+   __device__ __forceinline__ double nr(int o) const { return at(3, o); }
+   __device__ __forceinline__ double ne(int l, int o) const { return at(4 + l, o); }
+};
+
+__device__ __forceinline__ void ctStage(const GridInfo& g, const Fields& f, double* dst, int i0, int j0, int kz) {
+   int z = kz;
+   const bool zok = wrapc(z, g.nz, g.per[2]);
+   const long long N = g.N;
+   for (int e = threadIdx.x + NT_X * threadIdx.y; e < CT_LAYER; e += NT_X * NT_Y) {
+      const int a = e / (NT_LY * NT_LX), r = e - a * (NT_LY * NT_LX), jj = r / NT_LX, ii = r - jj * NT_LX;
+      int x = i0 - 1 + ii, y = j0 - 1 + jj;
+      const bool ok = zok && wrapc(x, g.nx, g.per[0]) && wrapc(y, g.ny, g.per[1]);
+      const double* arr = a < 3 ? f.nodeJ + a * N : a == 3 ? f.nodeRho : f.nodeE + (a - 4) * N;
+      cpAsync8(dst + e, ok ? arr + cidx(g, x, y, z) : f.faceB, ok ? 8 : 0);
+   }
+}
+
 template <bool FARADAY>
-__global__ void __launch_bounds__(128, 8) k_cell_fused(GridInfo g, Fields f, FieldParams fp, int useEp, unsigned long long* cnt) {
-   RH_CELL_PROLOGUE
+__device__ __forceinline__ void cellFromStencil(const GridInfo& g, const Fields& f, const FieldParams& fp, int useEp,
+                                                unsigned long long* cnt, int i, int j, int k, long long n,
+                                                const CellStencil& st) {
+   const long long N = g.N;
    const bool inner = allNb(g, i, j, k);
    bool clamp = false;
    if (inner) {
-      const long long a0 = n, a1 = nbr(g, i, j, k, -1, 0, 0), a2 = nbr(g, i, j, k, -1, -1, 0),
-                      a3 = nbr(g, i, j, k, 0, -1, 0), a4 = nbr(g, i, j, k, 0, 0, -1),
-                      a5 = nbr(g, i, j, k, 0, -1, -1), a6 = nbr(g, i, j, k, -1, 0, -1),
-                      a7 = nbr(g, i, j, k, -1, -1, -1);
+      constexpr int a0 = 7, a1 = 6, a2 = 4, a3 = 5, a4 = 3, a5 = 1, a6 = 2, a7 = 0;
       // node2Cell(nodeJ -> cellJ), calcCellUe
       double J[3];
       for (int l = 0; l < 3; ++l) {
-         const double* s = f.nodeJ + l * N;
-         J[l] = 0.125 * (s[a0] + s[a1] + s[a2] + s[a3] + s[a4] + s[a5] + s[a6] + s[a7]);
+         J[l] = 0.125 * (st.nj(l, a0) + st.nj(l, a1) + st.nj(l, a2) + st.nj(l, a3) + st.nj(l, a4) + st.nj(l, a5) +
+                         st.nj(l, a6) + st.nj(l, a7));
          f.cellJ[l * N + n] = J[l];
       }
       double Ue[3];
@@ -463,14 +504,13 @@ __global__ void __launch_bounds__(128, 8) k_cell_fused(GridInfo g, Fields f, Fie
       if (useEp) {
          double Ep[3] = {0.0, 0.0, 0.0};
          if (!(fl & RHGPU_FLAG_INNER_CELLEP)) {
-            const double* r = f.nodeRho;
-            const long long o000 = a0, o00m = a4, o0mm = a5, o0m0 = a3, om00 = a1, om0m = a6, ommm = a7, omm0 = a2;
-            const double xPos = 0.25 * (r[o000] + r[o00m] + r[o0mm] + r[o0m0]);
-            const double xNeg = 0.25 * (r[om00] + r[om0m] + r[ommm] + r[omm0]);
-            const double yPos = 0.25 * (r[o000] + r[o00m] + r[om0m] + r[om00]);
-            const double yNeg = 0.25 * (r[o0m0] + r[o0mm] + r[ommm] + r[omm0]);
-            const double zPos = 0.25 * (r[o000] + r[o0m0] + r[omm0] + r[om00]);
-            const double zNeg = 0.25 * (r[o00m] + r[o0mm] + r[ommm] + r[om0m]);
+            constexpr int o000 = a0, o00m = a4, o0mm = a5, o0m0 = a3, om00 = a1, om0m = a6, ommm = a7, omm0 = a2;
+            const double xPos = 0.25 * (st.nr(o000) + st.nr(o00m) + st.nr(o0mm) + st.nr(o0m0));
+            const double xNeg = 0.25 * (st.nr(om00) + st.nr(om0m) + st.nr(ommm) + st.nr(omm0));
+            const double yPos = 0.25 * (st.nr(o000) + st.nr(o00m) + st.nr(om0m) + st.nr(om00));
+            const double yNeg = 0.25 * (st.nr(o0m0) + st.nr(o0mm) + st.nr(ommm) + st.nr(omm0));
+            const double zPos = 0.25 * (st.nr(o000) + st.nr(o0m0) + st.nr(omm0) + st.nr(om00));
+            const double zNeg = 0.25 * (st.nr(o00m) + st.nr(o0mm) + st.nr(ommm) + st.nr(om0m));
             const double gx = (xPos - xNeg) / g.dx, gy = (yPos - yNeg) / g.dx, gz = (zPos - zNeg) / g.dx;
             const double C = fp.ep_coeff;
             if (!fp.isothermal) {
@@ -494,28 +534,56 @@ __global__ void __launch_bounds__(128, 8) k_cell_fused(GridInfo g, Fields f, Fie
       if (!yNeg(g, j)) { doX = doZ = false; }
       if (!zNeg(g, k)) { doX = doY = false; }
    }
-   const double* E = f.nodeE;
    const double dx = g.dx, dt = g.dt;
    if (doX) {
-      const long long s5 = nbr(g, i, j, k, 0, -1, 0), s6 = nbr(g, i, j, k, 0, -1, -1), s7 = nbr(g, i, j, k, 0, 0, -1);
-      const double n5y = E[1 * N + s5], n5z = E[2 * N + s5], n6y = E[1 * N + s6], n6z = E[2 * N + s6];
-      const double n7y = E[1 * N + s7], n7z = E[2 * N + s7], n8y = E[1 * N + n], n8z = E[2 * N + n];
+      constexpr int s5 = 5, s6 = 1, s7 = 3, s8 = 7;
+      const double n5y = st.ne(1, s5), n5z = st.ne(2, s5), n6y = st.ne(1, s6), n6z = st.ne(2, s6);
+      const double n7y = st.ne(1, s7), n7z = st.ne(2, s7), n8y = st.ne(1, s8), n8z = st.ne(2, s8);
       const double curlX = 0.5 * (+n5z + n6z - n6y - n7y - n7z - n8z + n8y + n5y) / dx;
       f.faceB[0 * N + n] += dt * curlX;
    }
    if (doY) {
-      const long long s3 = nbr(g, i, j, k, -1, 0, -1), s4 = nbr(g, i, j, k, -1, 0, 0), s7 = nbr(g, i, j, k, 0, 0, -1);
-      const double n3x = E[0 * N + s3], n3z = E[2 * N + s3], n4x = E[0 * N + s4], n4z = E[2 * N + s4];
-      const double n7x = E[0 * N + s7], n7z = E[2 * N + s7], n8x = E[0 * N + n], n8z = E[2 * N + n];
+      constexpr int s3 = 2, s4 = 6, s7 = 3, s8 = 7;
+      const double n3x = st.ne(0, s3), n3z = st.ne(2, s3), n4x = st.ne(0, s4), n4z = st.ne(2, s4);
+      const double n7x = st.ne(0, s7), n7z = st.ne(2, s7), n8x = st.ne(0, s8), n8z = st.ne(2, s8);
       const double curlY = 0.5 * (-n4x - n8x + n8z + n7z + n7x + n3x - n3z - n4z) / dx;
       f.faceB[1 * N + n] += dt * curlY;
    }
    if (doZ) {
-      const long long s1 = nbr(g, i, j, k, -1, -1, 0), s4 = nbr(g, i, j, k, -1, 0, 0), s5 = nbr(g, i, j, k, 0, -1, 0);
-      const double n1x = E[0 * N + s1], n1y = E[1 * N + s1], n4x = E[0 * N + s4], n4y = E[1 * N + s4];
-      const double n5x = E[0 * N + s5], n5y = E[1 * N + s5], n8x = E[0 * N + n], n8y = E[1 * N + n];
+      constexpr int s1 = 4, s4 = 6, s5 = 5, s8 = 7;
+      const double n1x = st.ne(0, s1), n1y = st.ne(1, s1), n4x = st.ne(0, s4), n4y = st.ne(1, s4);
+      const double n5x = st.ne(0, s5), n5y = st.ne(1, s5), n8x = st.ne(0, s8), n8y = st.ne(1, s8);
       const double curlZ = 0.5 * (-n1x - n5x - n5y - n8y + n8x + n4x + n4y + n1y) / dx;
       f.faceB[2 * N + n] += dt * curlZ;
+   }
+}
+
+template <bool FARADAY>
+__global__ void __launch_bounds__(NT_X * NT_Y) k_cell_tiled(GridInfo g, Fields f, FieldParams fp, int useEp,
+                                                            unsigned long long* cnt) {
+   extern __shared__ __align__(16) double ctLayers[];
+   const int tx = threadIdx.x, ty = threadIdx.y;
+   const int i0 = blockIdx.x * NT_X, j0 = blockIdx.y * NT_Y, k0 = blockIdx.z * NT_Z;
+   const int i = i0 + tx, j = j0 + ty;
+   const int nk = min(NT_Z, g.nz - k0);
+   const bool mine = i < g.nx && j < g.ny;
+   ctStage(g, f, ctLayers, i0, j0, k0 - 1);
+   ctStage(g, f, ctLayers + CT_LAYER, i0, j0, k0);
+   cpAsyncCommit();
+   if (nk > 1) ctStage(g, f, ctLayers + 2 * CT_LAYER, i0, j0, k0 + 1);
+   cpAsyncCommit();
+   for (int t = 0; t < nk; ++t) {
+      cpAsyncWaitGroup<1>();   // node layers k - 1 and k are in
+      __syncthreads();
+      CellStencil st;
+      st.L = ctLayers + (t % 3) * CT_LAYER;
+      st.U = ctLayers + ((t + 1) % 3) * CT_LAYER;
+      st.off = ty * NT_LX + tx;
+      const int k = k0 + t;
+      if (mine) cellFromStencil<FARADAY>(g, f, fp, useEp, cnt, i, j, k, cidx(g, i, j, k), st);
+      __syncthreads();         // layer k - 1 is read by every thread: its slot takes layer k + 2
+      if (t + 3 <= nk) ctStage(g, f, ctLayers + (t % 3) * CT_LAYER, i0, j0, k0 + t + 2);
+      cpAsyncCommit();
    }
 }
 

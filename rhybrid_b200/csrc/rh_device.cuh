@@ -97,4 +97,28 @@ __host__ __device__ inline int migrateAxis(double& x, int& off, double dx, doubl
    return st;
 }
 
+#ifdef __CUDACC__
+// ---- per-thread asynchronous global -> shared copies (cp.async) ----------------------------------
+// bytes = 0 copies nothing and writes zeros (the source address is not read)
+__device__ __forceinline__ void cpAsync8(void* sdst, const void* gsrc, int bytes) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
+}
+// 4-byte form (both addresses 4-byte aligned)
+__device__ __forceinline__ void cpAsync4(void* sdst, const void* gsrc) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+// 16-byte form (both addresses 16-byte aligned)
+__device__ __forceinline__ void cpAsync16(void* sdst, const void* gsrc, int bytes) {
+   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// every group but the newest N of this thread complete
+template <int N>
+__device__ __forceinline__ void cpAsyncWaitGroup() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+#endif
+
 }  // namespace rh

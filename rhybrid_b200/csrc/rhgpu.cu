@@ -536,10 +536,17 @@ int fieldsAll(rhgpu_ctx* c) {
    if (c->next > 0) RH_FIELD_LAUNCH(k_ext_bc, EB, 128, g, c->f, c->fp, c->ext, c->next);
    RH_FIELD_LAUNCH(k_node_fused, G, B, g, c->f, c->fp, c->cntU);
    c->gridAvgCounter += 1;
-   if (smooth)
-      RH_FIELD_LAUNCH(k_cell_fused<false>, G, B, g, c->f, c->fp, c->P.use_electron_pressure, c->cntU);
-   else
-      RH_FIELD_LAUNCH(k_cell_fused<true>, G, B, g, c->f, c->fp, c->P.use_electron_pressure, c->cntU);
+   {
+      RH_TIME(c, "k_cell_tiled");
+      const dim3 NG((g.nx + NT_X - 1) / NT_X, (g.ny + NT_Y - 1) / NT_Y, (g.nz + NT_Z - 1) / NT_Z);
+      if (smooth)
+         k_cell_tiled<false><<<NG, dim3(NT_X, NT_Y), CT_SMEM, c->stream>>>(g, c->f, c->fp, c->P.use_electron_pressure,
+                                                                          c->cntU);
+      else
+         k_cell_tiled<true><<<NG, dim3(NT_X, NT_Y), CT_SMEM, c->stream>>>(g, c->f, c->fp, c->P.use_electron_pressure,
+                                                                         c->cntU);
+      RH_LAUNCHED(c);
+   }
    if (c->next > 0) RH_FIELD_LAUNCH(k_ext_cell_neumann3, EB, 128, g, c->f.cellUe, c->ext, c->next);
    if (smooth) {
       for (int it = 0; it < c->P.n_linear_smoothings_nodeE; ++it) {
@@ -3241,7 +3248,6 @@ int rhgpu_dn_pair_error(rhgpu_dn* d, int32_t pair, double* out4) {
    RH_CUDA(cudaMemcpyAsync(d->res, in, sizeof(float) * 4 * N, cudaMemcpyDeviceToDevice, d->stream));
    int rc = dnForward(d);
    if (rc) return rc;
-   double* part = d->lossPart;   // DN_LOSS_BLOCKS doubles, 2 x 4 rows needed per call below
    std::vector<double> h(4 * 64);
    double r[2][4];
    for (int which = 0; which < 2; ++which) {
@@ -3254,7 +3260,6 @@ int rhgpu_dn_pair_error(rhgpu_dn* d, int32_t pair, double* out4) {
          for (int b = 0; b < 64; ++b) r[which][q] += h[b * 4 + q];
       }
    }
-   (void)part;
    out4[0] = std::sqrt(r[0][0] / r[0][1]);   // raw rho
    out4[1] = std::sqrt(r[0][2] / r[0][3]);   // raw J
    out4[2] = std::sqrt(r[1][0] / r[1][1]);   // denoised rho
