@@ -246,7 +246,7 @@ KERNEL_BYTES = {
 KERNEL_TRAFFIC = {
     # kernel: (traffic bytes, particles, cells) of the captured launch
     "fast_push_deposit": (263.379712e6 + 216.007168e6, 4110000, 44 * 59 * 59),
-    "f32_push_deposit": (142.888704e6 + 89.759744e6, 4080025, 44 * 59 * 59),
+    "f32_push_deposit": (144.102912e6 + 89.603840e6, 4110000, 44 * 59 * 59),
 }
 
 
@@ -495,20 +495,26 @@ def run_learned(args, rank, world, local_rank):
     line with the learned form's simulated seconds per wall second, its error
     against the check run, and its speed-up over the plain FP64 path at matched
     error (measured plain points only). Replicas only: every rank runs it, rank
-    0 prints."""
+    0 prints. --workload mercury takes the Mercury-like geometry (at --scale of its
+    cells: its 256-ppc check run fits one GPU up to about 0.064), --path fp32 runs
+    the learned form on the FP32 precision form."""
     import torch
-    from rhybrid_b200 import learned
+    from rhybrid_b200 import abi, learned
     torch.cuda.set_device(local_rank)
-    out = learned.closed_loop(scale=args.scale, log=lambda m: print(m, file=sys.stderr, flush=True))
+    workload = "mercury" if args.workload == "mercury" else "mars"
+    low_path = abi.PATH_FP32 if args.path == "fp32" else abi.PATH_FAST
+    out = learned.closed_loop(scale=args.scale, workload=workload, low_path=low_path,
+                              log=lambda m: print(m, file=sys.stderr, flush=True))
     lr = out["learned"]
     if rank == 0:
+        form = "FP32 form" if low_path == abi.PATH_FP32 else "FP64 fast path"
         line = {
-            "metric": "sim-s per wall-s (learned 8 ppc FP64 fast path + denoiser; plain FP64 at matched error)",
+            "metric": f"sim-s per wall-s (learned 8 ppc {form} + denoiser; plain FP64 at matched error)",
             "value": round(lr["sim_s_per_wall_s"], 4), "unit": "sim-s/wall-s", "n_gpus": world,
             "steps": out["window"]["last_step"], "warmup": 0, "ms_per_step": round(lr["ms_per_step"], 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network bf16, fp32 accum)",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("f32" if low_path == abi.PATH_FP32 else "f64") + " (network bf16, fp32 accum)",
             "data": "synthetic (uniform fill generated on the GPU, solar wind sources)",
-            "config": {"workload": f"mars_{out['geometry'][0]}x{out['geometry'][1]}x{out['geometry'][2]}_learned",
+            "config": {"workload": f"{workload}_{out['geometry'][0]}x{out['geometry'][1]}x{out['geometry'][2]}_learned",
                        "check_run": out["check_run"], "training": out["training"], "window": out["window"],
                        "threshold": out["threshold"],
                        "learned": {k: v for k, v in lr.items() if k != "samples"},

@@ -151,6 +151,17 @@ def c4_config(ppc: float, scale: float = 1.0) -> cf.Config:
                           nz=max(16, int(round(160 * f))), ppc=ppc)
 
 
+def c5_config(ppc: float, scale: float = 1.0) -> cf.Config:
+    """The Mercury-like dipole geometry (320^3 cells of 100 km at scale 1) with
+    its solar wind H+ at `ppc` and its inflow source; `scale` is the fraction
+    of the cells, at the same cell size."""
+    n = max(16, int(round(320 * scale ** (1.0 / 3.0))))
+    return cf.config_mercury(nx=n, ny=n, nz=n, ppc=ppc)
+
+
+GEOMETRIES = {"mars": c4_config, "mercury": c5_config}
+
+
 def filled_context(lib: abi.Library, cfg: cf.Config, seed: int, path: int = abi.PATH_FAST) -> abi.Context:
     """A context of cfg with its populations filled on the GPU and its sources set."""
     grid = cf.init_grid(cfg)
@@ -183,8 +194,14 @@ def _timed_steps(ctx: abi.Context, n: int) -> float:
 def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plain_ppcs=(8, 16, 32, 64, 128),
                 train_steps: int = 100, crops_per_step: int = 20, crop: int = 64, adam_steps: int = 4000,
                 lr: float = 1e-3, eval_steps: int = 100, every: int = 10, threshold: float = 0.02,
-                enforce_gate: bool = False, seed: int = 6461674, log=print) -> dict:
+                enforce_gate: bool = False, seed: int = 6461674, workload: str = "mars",
+                low_path: int = abi.PATH_FAST, log=print) -> dict:
     """The learned form in closed loop against a high-ppc plain check run.
+
+    workload: "mars" (c4_config) or "mercury" (c5_config), at `scale` of the
+    cells. low_path: the particle path of the learned run (PATH_FAST, FP64, or
+    PATH_FP32, the FP32 precision form); the check run and the plain runs are
+    always the FP64 fast path.
 
     1. Check run (judge_ppc, FP64 fast path, filled on the GPU) steps
        train_steps + eval_steps. During the first train_steps it yields the
@@ -215,7 +232,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     """
     lib = abi.gpu_library()
     t_start = time.time()
-    judge_cfg = c4_config(float(judge_ppc), scale)
+    geom = GEOMETRIES[workload]
+    judge_cfg = geom(float(judge_ppc), scale)
     factor = judge_ppc // low_ppc
     dn = abi.Denoiser(lib, crop, crop, crop, (0, 0, 0), pair_capacity=train_steps * crops_per_step)
     dn.set_scales(*moment_scales(judge_cfg))
@@ -256,8 +274,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
         f"losses {losses[0]:.4g} -> {losses[-1]:.4g}")
 
     def run_low(ppc: int, learned: bool) -> dict:
-        cfg = c4_config(float(ppc), scale)
-        ctx = filled_context(lib, cfg, seed + 7)
+        cfg = geom(float(ppc), scale)
+        ctx = filled_context(lib, cfg, seed + 7, path=low_path if learned else abi.PATH_FAST)
         net = None
         try:
             if learned:
@@ -306,7 +324,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     match = [p for p in plain if p["max_error"] <= e_l]
     above = [p for p in plain if p["max_error"] > e_l]
     res = {
-        "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx, "dt_s": judge_cfg.dt,
+        "workload": workload, "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx,
+        "dt_s": judge_cfg.dt, "learned_path": "fp32" if low_path == abi.PATH_FP32 else "fast",
         "check_run": {"ppc": judge_ppc, "ions": int(n_judge), "ms_per_step": judge_ms,
                       "split_half_noise": {str(k): {"rho": v[0], "J": v[1]} for k, v in judge_noise.items()}},
         "training": {"pairs": train_steps * crops_per_step, "crop": crop, "factor": factor, "adam_steps": adam_steps,
@@ -377,7 +396,11 @@ def main(argv=None):
     ap.add_argument("--train-steps", type=int, default=100)
     ap.add_argument("--eval-steps", type=int, default=100)
     ap.add_argument("--adam-steps", type=int, default=4000)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--plain", default="8,16,32,64,128")
+    ap.add_argument("--workload", default="mars", choices=sorted(GEOMETRIES))
+    ap.add_argument("--learned-path", default="fast", choices=["fast", "fp32"],
+                    help="particle path of the learned run (the check and plain runs are FP64)")
     ap.add_argument("--json", default=None)
     a = ap.parse_args(argv)
     if a.apply_only:
@@ -385,7 +408,9 @@ def main(argv=None):
         print(json.dumps(out))
         return
     out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
-                      adam_steps=a.adam_steps, plain_ppcs=tuple(int(x) for x in a.plain.split(",")))
+                      adam_steps=a.adam_steps, lr=a.lr, plain_ppcs=tuple(int(x) for x in a.plain.split(",")),
+                      workload=a.workload,
+                      low_path=abi.PATH_FP32 if a.learned_path == "fp32" else abi.PATH_FAST)
     print(json.dumps(out))
     if a.json:
         with open(a.json, "w") as f:
