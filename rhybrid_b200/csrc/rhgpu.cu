@@ -27,6 +27,7 @@
 #include "k_inject.cuh"
 #include "k_avg.cuh"
 #include "k_fill.cuh"
+#include "k_scan.cuh"
 #include "rh_logs.h"
 
 using namespace rh;
@@ -363,6 +364,42 @@ int checkLaunch(rhgpu_ctx* c) {
 }
 #define RH_LAUNCHED(c) do { int rc_ = checkLaunch(c); if (rc_) return rc_; } while (0)
 
+// ---- prefix sums (k_scan.cuh) ---------------------------------------------------------------
+// scratch of a scan of n values: the tile sums of every level
+long long scanScratchLongs(long long n) {
+   long long tot = 16;
+   for (long long m = n; m > SCAN_TILE;) {
+      m = (m + SCAN_TILE - 1) / SCAN_TILE;
+      tot += m;
+   }
+   return tot;
+}
+
+int scanLevel(rhgpu_ctx* c, const long long* in, long long* out, long long n, long long* scratch) {
+   const long long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+   if (nb <= 1) {
+      k_scan_tile<<<1, SCAN_THREADS, 0, c->stream>>>(in, out, n, nullptr);
+      RH_LAUNCHED(c);
+      return RHGPU_OK;
+   }
+   k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, c->stream>>>(in, out, n, scratch);
+   RH_LAUNCHED(c);
+   if (int rc = scanLevel(c, scratch, scratch, nb, scratch + nb)) return rc;
+   k_scan_add<<<blocks1d(n, 256), 256, 0, c->stream>>>(out, n, scratch);
+   RH_LAUNCHED(c);
+   return RHGPU_OK;
+}
+
+// exclusive prefix sum of n 64-bit values on the context's stream (in and out
+// may be the same array); the context's scan scratch holds the tile sums
+int scanExclusive64(rhgpu_ctx* c, const long long* in, long long* out, long long n) {
+   if (n <= 0) return RHGPU_OK;
+   if (sizeof(long long) * (size_t)scanScratchLongs(n) > c->scanTmpBytes)
+      return fail(RHGPU_ERR_CAPACITY, "prefix sum larger than its scratch");
+   return scanLevel(c, in, out, n, (long long*)c->scanTmp);
+}
+
+
 SpeciesDev speciesDev(const rhgpu_ctx* c, int s) {
    SpeciesDev d;
    d.q = c->sp[s].q;
@@ -403,10 +440,7 @@ int migrate(rhgpu_ctx* c, int s) {
    RH_CUDA(cudaMemsetAsync(c->newCount + g.N, 0, sizeof(long long), c->stream));
    {
       RH_TIME(c, "mig_scan");
-      size_t bytes = c->scanTmpBytes;
-      RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, Q.start, g.N + 1, c->stream));
-      c->launches += 2;
-      c->launchesStep += 2;
+      if (int rc_ = scanExclusive64(c, c->newCount, Q.start, g.N + 1)) return rc_;
    }
    long long total = 0;
    RH_CUDA(cudaMemcpyAsync(&total, Q.start + g.N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
@@ -645,8 +679,7 @@ int fastLayout(rhgpu_ctx* c, const int* cnt, const int* extra, long long* base, 
    const long long NS = c->fg.NS;
    k_fast_capacity<<<blocks1d(NS + 1, 256), 256, 0, c->stream>>>(NS, cnt, extra, c->fcap);
    RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->fcap, base, NS + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->fcap, base, NS + 1)) return rc_;
    RH_CUDA(cudaMemcpyAsync(total, base + NS, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
    return RHGPU_OK;
@@ -775,16 +808,13 @@ int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** 
    RH_LAUNCHED(c);
    k_int_to64<<<blocks1d(nb + 1, 256), 256, 0, c->stream>>>(c->finc, nb, c->ftmpInc64);
    RH_LAUNCHED(c);
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmpInc64, c->foffInc, nb + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->ftmpInc64, c->foffInc, nb + 1)) return rc_;
    unsigned long long *kA = c->mkey, *kB = c->mkey + c->mcap;
    unsigned *vA = c->mval, *vB = c->mval + c->mcap, *bA = c->mbkt, *bB = c->mbkt + c->mcap;
-   size_t mb = 0;
-   cub::DeviceReduce::Max(nullptr, mb, c->finc, c->fmaxInc, (int)nb, c->stream);
-   int rc = ensureSortTmp(c, mb);
-   if (rc) return rc;
-   mb = c->sortTmpBytes;
-   RH_CUDA(cub::DeviceReduce::Max(c->sortTmp, mb, c->finc, c->fmaxInc, (int)nb, c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fmaxInc, 0, sizeof(int), c->stream));
+   k_max_int<<<(unsigned)std::min<long long>(blocks1d(nb, 256), 4 * 148), 256, 0, c->stream>>>(c->finc, nb, c->fmaxInc);
+   RH_LAUNCHED(c);
+   int rc = RHGPU_OK;
    int maxInc = 0;
    RH_CUDA(cudaMemcpyAsync(&maxInc, c->fmaxInc, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -832,8 +862,7 @@ int segPrefix(rhgpu_ctx* c, const int* cnt, long long* total) {
    const long long NS = c->fg.NS;
    k_int_to64<<<blocks1d(NS + 1, 256), 256, 0, c->stream>>>(cnt, NS, c->ftmp64);
    RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->ftmp64, c->ffirst, NS + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->ftmp64, c->ffirst, NS + 1)) return rc_;
    RH_CUDA(cudaMemcpyAsync(total, c->ffirst + NS, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
    return RHGPU_OK;
@@ -876,8 +905,7 @@ int fastUpload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* partic
    long long* cstart = c->ftmpCellStart;
    k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, c->outCount);
    RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, cstart, N + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->newCount, cstart, N + 1)) return rc_;
    long long total = 0;
    RH_CUDA(cudaMemcpyAsync(&total, cstart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -1328,8 +1356,7 @@ int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particl
    long long* cstart = c->ftmpCellStart;
    k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, c->outCount);
    RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, cstart, N + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->newCount, cstart, N + 1)) return rc_;
    long long total = 0;
    RH_CUDA(cudaMemcpyAsync(&total, cstart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -1903,11 +1930,9 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    }
    if (!rc) {
       // scan scratch for the largest scan (cells, dual cells, species x dual cells)
-      size_t bytes = 0;
       const long long mx = std::max(N, nb) + 1;
-      cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->foffInc, c->foffInc, mx, c->stream);
-      c->scanTmpBytes = bytes;
-      alloc(&c->scanTmp, bytes + 16);
+      c->scanTmpBytes = sizeof(long long) * (size_t)scanScratchLongs(mx);
+      alloc(&c->scanTmp, c->scanTmpBytes);
    }
    // exterior cells (missing a neighbour) and obstacle-flagged cells are
    // listed after upload_cell_flags; exterior list now
@@ -2112,8 +2137,7 @@ int rhgpu_upload_particles(rhgpu_ctx* c, int32_t s, const uint32_t* counts, cons
    if (n) RH_CUDA(cudaMemcpyAsync(aos, particles, sizeof(double) * 7 * n, cudaMemcpyHostToDevice, c->stream));
    k_counts_in<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, dcounts, c->newCount, P.alive);
    RH_CUDA(cudaGetLastError());
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, P.start, N + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->newCount, P.start, N + 1)) return rc_;
    long long total = 0;
    RH_CUDA(cudaMemcpyAsync(&total, P.start + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -2245,8 +2269,7 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
    k_alive_to64<<<blocks1d(N + 1, 256), 256, 0, c->stream>>>(N, P.alive, c->newCount);
    RH_CUDA(cudaGetLastError());
    long long* outStart = c->alt[s].start;
-   size_t bytes = c->scanTmpBytes;
-   RH_CUDA(cub::DeviceScan::ExclusiveSum(c->scanTmp, bytes, c->newCount, outStart, N + 1, c->stream));
+   if (int rc_ = scanExclusive64(c, c->newCount, outStart, N + 1)) return rc_;
    long long tot = 0;
    RH_CUDA(cudaMemcpyAsync(&tot, outStart + N, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
