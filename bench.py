@@ -373,14 +373,22 @@ def run_gpu(args, rank, world, local_rank):
     # end to end through the C ABI with host-resident state (rank-local)
     e2e = None
     if not args.no_e2e and not gpu_fill:
-        cnts, parts = [], []
+        # the FP32 form moves its own 6-float records (rhgpu_*_particles_f32), the
+        # FP64 paths 7 doubles per particle
+        f32rec = args.path == "fp32"
+        rw, rdt, rct = (6, torch.float32, abi.C.c_float) if f32rec else (7, torch.float64, abi.C.c_double)
+        cnts, parts, weights = [], [], []
         for s in range(len(pops)):
-            c, p = ctx.download_particles(s)
-            pin = torch.empty((max(p.shape[0], 1), 7), dtype=torch.float64, pin_memory=True).numpy()[: p.shape[0]]
+            if f32rec:
+                c, p, w = ctx.download_particles_f32(s)
+            else:
+                (c, p), w = ctx.download_particles(s), None
+            pin = torch.empty((max(p.shape[0], 1), rw), dtype=rdt, pin_memory=True).numpy()[: p.shape[0]]
             pin[:] = p
             cnts.append(c)
             parts.append(pin)
-        out_pin = [torch.empty((max(p.shape[0], 1), 7), dtype=torch.float64, pin_memory=True).numpy() for p in parts]
+            weights.append(w)
+        out_pin = [torch.empty((max(p.shape[0], 1), rw), dtype=rdt, pin_memory=True).numpy() for p in parts]
         ke = max(1, min(8, args.steps))
         h2d = sum(p.nbytes + c.nbytes for p, c in zip(parts, cnts))
         if dist:
@@ -390,19 +398,28 @@ def run_gpu(args, rank, world, local_rank):
         e2e_ps = 0
         for _ in range(ke):
             for s in range(nspec):
-                ctx.upload_particles(s, cnts[s], parts[s])
+                if f32rec:
+                    ctx.upload_particles_f32(s, cnts[s], parts[s], weights[s])
+                else:
+                    ctx.upload_particles(s, cnts[s], parts[s])
                 e2e_ps += parts[s].shape[0]
             ctx.step(1)
             d2h = 0
             for s in range(nspec):
                 n = ctx.num_particles(s)
                 if n > out_pin[s].shape[0]:
-                    out_pin[s] = np.empty((n, 7))
+                    out_pin[s] = np.empty((n, rw), dtype=parts[s].dtype)
                 cnt = np.empty(cfg.ncells, dtype=np.uint32)
                 nout = abi.C.c_int64()
-                lib.call("download_particles", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
-                         abi._ptr(out_pin[s], abi.C.c_double), out_pin[s].shape[0], abi.C.byref(nout))
-                d2h += nout.value * 56 + cnt.nbytes
+                if f32rec:
+                    wout = np.zeros(1)
+                    lib.call("download_particles_f32", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
+                             abi._ptr(out_pin[s], rct), out_pin[s].shape[0], abi.C.byref(nout),
+                             abi._ptr(wout, abi.C.c_double))
+                else:
+                    lib.call("download_particles", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
+                             abi._ptr(out_pin[s], rct), out_pin[s].shape[0], abi.C.byref(nout))
+                d2h += nout.value * out_pin[s].itemsize * rw + cnt.nbytes
             for name in ("cellRhoQi", "cellJi", "faceB"):
                 d2h += ctx.download_array(name).nbytes
         torch.cuda.synchronize()
@@ -411,7 +428,9 @@ def run_gpu(args, rank, world, local_rank):
         e2e = {"value": e2e_ps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": ke,
                "host": "every step: all particles uploaded from pinned host memory, one step, particles and "
-                       "rhoq, Ji, faceB downloaded (a host that owns the particle lists)"}
+                       "rhoq, Ji, faceB downloaded (a host that owns the particle lists)" +
+                       ("; the FP32 form's own 24-byte records (rhgpu_upload/download_particles_f32)" if f32rec
+                        else "; 56-byte double records")}
     if not args.no_e2e:
         # a host that keeps the state on the device (Corsair with the GPU plugin):
         # per step it reads back the step's diagnostics (population and field log

@@ -217,6 +217,21 @@ int rhgpu_num_particles(rhgpu_ctx* ctx, int32_t s, int64_t* n_out);
 int rhgpu_download_particles(rhgpu_ctx* ctx, int32_t s, uint32_t* counts, double* particles,
                              int64_t capacity, int64_t* n_out);
 
+/* FP32 form only (RHGPU_PATH_FP32; RHGPU_ERR_ARG otherwise): species s in the
+ * form's own records, 6 floats per particle: the offsets in the cell in units
+ * of dx, in [0, 1), then the velocity [m/s]; grouped by cell in linear cell
+ * order with per-cell counts, as rhgpu_upload_particles; `weight` is the
+ * species' one macroparticle weight. 24 bytes per particle cross the bus
+ * instead of 56, for hosts that keep the FP32 form's particle lists
+ * themselves. The reference has no counterpart: its particles are doubles. */
+int rhgpu_upload_particles_f32(rhgpu_ctx* ctx, int32_t s, const uint32_t* counts,
+                               const float* particles, int64_t n_particles, double weight);
+
+/* The inverse of rhgpu_upload_particles_f32: species s as 6-float records
+ * (capacity in records; RHGPU_ERR_ARG if too small) and its weight. */
+int rhgpu_download_particles_f32(rhgpu_ctx* ctx, int32_t s, uint32_t* counts, float* particles,
+                                 int64_t capacity, int64_t* n_out, double* weight_out);
+
 /* Runs nsteps time steps of propagate() (src/user.cpp:118-134) on the
  * device: field gather + push, migration, deposit, particle boundary
  * conditions, propagateB. Host-resident nothing; returns after enqueueing and

@@ -142,6 +142,9 @@ _SIGNATURES = {
     "last_error": [],
 }
 _OPTIONAL = {
+    # the FP32 form's own particle records (GPU library only)
+    "upload_particles_f32": [_P, C.c_int32, _U32, C.POINTER(C.c_float), C.c_int64, C.c_double],
+    "download_particles_f32": [_P, C.c_int32, _U32, C.POINTER(C.c_float), C.c_int64, _I64, _D],
     "device_errors": [_P, _U32],
     "reduce_diagnostics": [_P, _D, C.c_int32],
     "fill_uniform": [_P, C.c_int32, C.c_void_p, C.c_void_p],
@@ -330,6 +333,27 @@ class Context:
         self.lib.call("download_particles", self.h, s, _ptr(cnt, C.c_uint32), _ptr(p, C.c_double), p.shape[0],
                       C.byref(nout))
         return cnt, p[: nout.value]
+
+    def upload_particles_f32(self, s: int, counts: np.ndarray, particles: np.ndarray, weight: float):
+        """FP32 form only: particles as 6 float32 per record (offsets in the
+        cell in units of dx, in [0, 1), then the velocity), the species' weight
+        apart (rhgpu_upload_particles_f32)."""
+        cnt = np.ascontiguousarray(counts, dtype=np.uint32)
+        p = np.ascontiguousarray(particles, dtype=np.float32).reshape(-1, 6)
+        assert cnt.size == self.ncells
+        self.lib.call("upload_particles_f32", self.h, s, _ptr(cnt, C.c_uint32), _ptr(p, C.c_float), p.shape[0],
+                      float(weight))
+
+    def download_particles_f32(self, s: int):
+        """FP32 form only: (counts, 6-float records, weight)."""
+        n = self.num_particles(s)
+        cnt = np.empty(self.ncells, dtype=np.uint32)
+        p = np.empty((max(n, 1), 6), dtype=np.float32)
+        nout = C.c_int64()
+        w = np.zeros(1)
+        self.lib.call("download_particles_f32", self.h, s, _ptr(cnt, C.c_uint32), _ptr(p, C.c_float), p.shape[0],
+                      C.byref(nout), _ptr(w, C.c_double))
+        return cnt, p[: nout.value], float(w[0])
 
     # stepping --------------------------------------------------------
     def step(self, n: int = 1):

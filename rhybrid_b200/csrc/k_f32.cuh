@@ -571,20 +571,39 @@ __device__ inline float offsetOf(double x, double rdx, float below1) {
    if (o < 0.0f) o = 0.0f;
    return o;
 }
+// uploaded records: 7 doubles (cell-local position [m], velocity, weight), or
+// the FP32 form's own 6 floats (offsets in the cell in units of dx, velocity)
+struct RecordsD {
+   const double* a;
+   __device__ float off(long long p, int k, double rdx, float below1) const { return offsetOf(a[7 * p + k], rdx, below1); }
+   __device__ float vel(long long p, int k) const { return (float)a[7 * p + 3 + k]; }
+};
+struct RecordsF {
+   const float* a;
+   __device__ float off(long long p, int k, double, float below1) const {
+      float o = a[6 * p + k];
+      if (o >= 1.0f) o = below1;
+      if (o < 0.0f) o = 0.0f;
+      return o;
+   }
+   __device__ float vel(long long p, int k) const { return a[6 * p + 3 + k]; }
+};
+
 // segment and dual x of each uploaded particle, from its FP32 offsets
-__global__ void k_f32_seg_of(GridInfo g, FastGeom fg, const double* aos, const int* pcell, long long n, float below1,
+template <class R>
+__global__ void k_f32_seg_of(GridInfo g, FastGeom fg, R rec, const int* pcell, long long n, float below1,
                              unsigned* key) {
    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (p >= n) return;
    const int c = pcell[p];
    const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
-   const double* st = aos + 7 * p;
-   const int ux = dualU(i + halfSf(offsetOf(st[0], g.rdx, below1)) - 1, g.nx, g.per[0]);
-   const int uy = dualU(j + halfSf(offsetOf(st[1], g.rdx, below1)) - 1, g.ny, g.per[1]);
-   const int uz = dualU(k + halfSf(offsetOf(st[2], g.rdx, below1)) - 1, g.nz, g.per[2]);
+   const int ux = dualU(i + halfSf(rec.off(p, 0, g.rdx, below1)) - 1, g.nx, g.per[0]);
+   const int uy = dualU(j + halfSf(rec.off(p, 1, g.rdx, below1)) - 1, g.ny, g.per[1]);
+   const int uz = dualU(k + halfSf(rec.off(p, 2, g.rdx, below1)) - 1, g.nz, g.per[2]);
    key[p] = (unsigned)(((long long)uy + (long long)fg.nd[1] * uz) * fg.nseg + ux / SEG);
 }
-__global__ void k_f32_scatter_sorted(GridInfo g, const double* aos, const int* pcell, const unsigned* key,
+template <class R>
+__global__ void k_f32_scatter_sorted(GridInfo g, R rec, const int* pcell, const unsigned* key,
                                      const unsigned* idx, long long n, const long long* first, F32Buf B,
                                      const long long* base, float below1) {
    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -592,11 +611,10 @@ __global__ void k_f32_scatter_sorted(GridInfo g, const double* aos, const int* p
    const unsigned S = key[j];
    const long long slot = base[S] + (j - first[S]);
    const unsigned src = idx[j];
-   const double* st = aos + 7LL * src;
    B.cell[slot] = pcell[src];
    for (int a = 0; a < 3; ++a) {
-      B.o[a][slot] = offsetOf(st[a], g.rdx, below1);
-      B.v[a][slot] = (float)st[3 + a];
+      B.o[a][slot] = rec.off(src, a, g.rdx, below1);
+      B.v[a][slot] = rec.vel(src, a);
    }
 }
 __global__ void k_f32_cell_keys(FastGeom fg, F32Buf B, const long long* base, const long long* first, unsigned* key,
@@ -619,6 +637,17 @@ __global__ void k_f32_gather_records(F32Buf B, const unsigned long long* slots, 
       aos[7 * j + 3 + a] = (double)B.v[a][slot];
    }
    aos[7 * j + 6] = w;
+}
+// the FP32 form's own records: 6 floats per particle, offsets and velocity as stored
+__global__ void k_f32_gather_records_f32(F32Buf B, const unsigned long long* slots, const unsigned* idx, long long n,
+                                         float* rec) {
+   const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (j >= n) return;
+   const unsigned long long slot = slots[idx[j]];
+   for (int a = 0; a < 3; ++a) {
+      rec[6 * j + a] = B.o[a][slot];
+      rec[6 * j + 3 + a] = B.v[a][slot];
+   }
 }
 __global__ void k_f32_relayout(F32Buf from, const long long* fromBase, F32Buf to, const long long* toBase) {
    const long long S = blockIdx.x;

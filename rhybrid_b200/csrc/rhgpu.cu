@@ -1321,21 +1321,30 @@ int f32MoverBuffers(rhgpu_ctx* c) {
    return ensureMigBuffers(c, want);
 }
 
-int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n) {
+// particles: 7 doubles per record, or (particles32, with weight32) the FP32
+// form's own 6-float records
+int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particles, long long n,
+              const float* particles32 = nullptr, double weight32 = 0.0) {
    int rc = f32Init(c);
    if (rc) return rc;
    const long long N = c->g.N, NS = c->fg.NS;
-   rc = ensureStaging(c, sizeof(double) * 7 * (size_t)(n > 0 ? n : 1) + sizeof(uint32_t) * (size_t)N + 64);
+   const size_t recBytes = particles32 ? sizeof(float) * 6 : sizeof(double) * 7;
+   const size_t recAll = recBytes * (size_t)(n > 0 ? n : 1);
+   rc = ensureStaging(c, recAll + sizeof(uint32_t) * (size_t)N + 64);
    if (rc) return rc;
    rc = ensureKeyCapacity(c, 2 * n + 2);
    if (rc) return rc;
    double* aos = (double*)c->staging;
-   uint32_t* dcounts = (uint32_t*)((char*)c->staging + sizeof(double) * 7 * (size_t)(n > 0 ? n : 1));
+   float* aos32 = (float*)c->staging;
+   uint32_t* dcounts = (uint32_t*)((char*)c->staging + ((recAll + 15) / 16) * 16);
    RH_CUDA(cudaMemcpyAsync(dcounts, counts, sizeof(uint32_t) * N, cudaMemcpyHostToDevice, c->stream));
-   if (n) RH_CUDA(cudaMemcpyAsync(aos, particles, sizeof(double) * 7 * n, cudaMemcpyHostToDevice, c->stream));
+   if (n) RH_CUDA(cudaMemcpyAsync(c->staging, particles32 ? (const void*)particles32 : (const void*)particles,
+                                  recBytes * n, cudaMemcpyHostToDevice, c->stream));
    F32Host& h = c->f32[s];
    // one weight per species
-   if (n) {
+   if (particles32) {
+      h.w = n ? weight32 : 0.0;
+   } else if (n) {
       unsigned long long* mm = (unsigned long long*)c->fover;   // [0] min, [1] max
       const unsigned long long init[2] = {~0ull, 0ull};
       RH_CUDA(cudaMemcpyAsync(mm, init, sizeof init, cudaMemcpyHostToDevice, c->stream));
@@ -1371,7 +1380,10 @@ int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particl
    unsigned* idxOut = idxIn + (n + 1);
    const float below1 = std::nextafter(1.0f, 0.0f);
    if (n) {
-      k_f32_seg_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, aos, pcell, n, below1, keyIn);
+      if (particles32)
+         k_f32_seg_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, RecordsF{aos32}, pcell, n, below1, keyIn);
+      else
+         k_f32_seg_of<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, c->fg, RecordsD{aos}, pcell, n, below1, keyIn);
       k_iota<<<blocks1d(n, 256), 256, 0, c->stream>>>(idxIn, n);
       RH_CUDA(cudaGetLastError());
       size_t sb = 0;
@@ -1392,8 +1404,12 @@ int f32Upload(rhgpu_ctx* c, int s, const uint32_t* counts, const double* particl
    rc = f32Reserve(h, 1, slots);
    if (rc) return rc;
    if (n) {
-      k_f32_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, aos, pcell, keyOut, idxOut, n, c->ffirst,
-                                                                    f32View(h, h.cur), h.base, below1);
+      if (particles32)
+         k_f32_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, RecordsF{aos32}, pcell, keyOut, idxOut, n,
+                                                                       c->ffirst, f32View(h, h.cur), h.base, below1);
+      else
+         k_f32_scatter_sorted<<<blocks1d(n, 256), 256, 0, c->stream>>>(c->g, RecordsD{aos}, pcell, keyOut, idxOut, n,
+                                                                       c->ffirst, f32View(h, h.cur), h.base, below1);
       RH_CUDA(cudaGetLastError());
    }
    RH_CUDA(cudaStreamSynchronize(c->stream));
@@ -1406,7 +1422,9 @@ int f32NumParticles(rhgpu_ctx* c, int s, long long* n) {
    return segPrefix(c, c->f32[s].cnt[c->f32[s].cur], n);
 }
 
-int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long long capacity, long long* n_out) {
+// particles: 7 doubles per record, or (particles32) the FP32 form's own 6-float records
+int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long long capacity, long long* n_out,
+                float* particles32 = nullptr) {
    const long long N = c->g.N, NS = c->fg.NS;
    int rc = f32Init(c);
    if (rc) return rc;
@@ -1441,14 +1459,21 @@ int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long l
       RH_CUDA(cub::DeviceRadixSort::SortPairs(c->sortTmp, sb, keyIn, keyOut, idxIn, idxOut, (int)tot, 0, 32, c->stream));
       k_sorted_bounds<<<blocks1d(tot + 1, 256), 256, 0, c->stream>>>(keyOut, tot, N, c->ftmpCellStart);
       k_bounds_counts<<<blocks1d(N, 256), 256, 0, c->stream>>>(c->ftmpCellStart, N, cellCnt);
-      k_f32_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(f32View(h, h.cur), c->fsortSlots, idxOut, tot,
-                                                                      c->P.dx, h.w, aos);
+      if (particles32)
+         k_f32_gather_records_f32<<<blocks1d(tot, 256), 256, 0, c->stream>>>(f32View(h, h.cur), c->fsortSlots, idxOut,
+                                                                              tot, (float*)aos);
+      else
+         k_f32_gather_records<<<blocks1d(tot, 256), 256, 0, c->stream>>>(f32View(h, h.cur), c->fsortSlots, idxOut, tot,
+                                                                         c->P.dx, h.w, aos);
       RH_CUDA(cudaGetLastError());
    } else {
       RH_CUDA(cudaMemsetAsync(cellCnt, 0, sizeof(int) * N, c->stream));
    }
    RH_CUDA(cudaMemcpyAsync(counts, cellCnt, sizeof(uint32_t) * N, cudaMemcpyDeviceToHost, c->stream));
-   if (tot && particles) RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
+   if (tot && particles32)
+      RH_CUDA(cudaMemcpyAsync(particles32, aos, sizeof(float) * 6 * tot, cudaMemcpyDeviceToHost, c->stream));
+   else if (tot && particles)
+      RH_CUDA(cudaMemcpyAsync(particles, aos, sizeof(double) * 7 * tot, cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
    *n_out = tot;
    return RHGPU_OK;
@@ -2285,6 +2310,30 @@ int rhgpu_download_particles(rhgpu_ctx* c, int32_t s, uint32_t* counts, double* 
    RH_CUDA(cudaStreamSynchronize(c->stream));
    *n_out = tot;
    return RHGPU_OK;
+}
+
+int rhgpu_upload_particles_f32(rhgpu_ctx* c, int32_t s, const uint32_t* counts, const float* particles, int64_t n,
+                               double weight) {
+   if (!c || s < 0 || s >= c->ns || !counts || (n > 0 && !particles) || n < 0 || !std::isfinite(weight))
+      return fail(RHGPU_ERR_ARG, "upload_particles_f32: bad arguments");
+   if (c->path != RHGPU_PATH_FP32) return fail(RHGPU_ERR_ARG, "upload_particles_f32: the context is not on the FP32 form");
+   RH_CUDA(cudaSetDevice(c->device));
+   if (c->capHint[s] > 0 && n > c->capHint[s])
+      return fail(RHGPU_ERR_CAPACITY, "upload_particles_f32: more particles than capacity");
+   c->uploaded = true;
+   return f32Upload(c, s, counts, nullptr, n, particles, weight);
+}
+
+int rhgpu_download_particles_f32(rhgpu_ctx* c, int32_t s, uint32_t* counts, float* particles, int64_t capacity,
+                                 int64_t* n_out, double* weight_out) {
+   if (!c || s < 0 || s >= c->ns || !counts || !n_out) return fail(RHGPU_ERR_ARG, "download_particles_f32: bad arguments");
+   if (c->path != RHGPU_PATH_FP32) return fail(RHGPU_ERR_ARG, "download_particles_f32: the context is not on the FP32 form");
+   RH_CUDA(cudaSetDevice(c->device));
+   long long t = 0;
+   const int rc = f32Download(c, s, counts, nullptr, capacity, &t, particles);
+   *n_out = t;
+   if (!rc && weight_out) *weight_out = c->f32ready ? c->f32[s].w : 0.0;
+   return rc;
 }
 
 namespace {

@@ -156,3 +156,57 @@ def test_fp32_diagnostics_in_fp64():
             assert abs(got["sumWV2"] - e) <= 1e-12 * e
     finally:
         ctx.close()
+
+
+def test_fp32_own_records_roundtrip_and_same_run():
+    """rhgpu_upload_particles_f32 / rhgpu_download_particles_f32: the form's own
+    6-float records (offsets in cell units, velocities) with the weight apart.
+    Records come back exactly as stored, and a context loaded from them steps
+    bit for bit like the context they were downloaded from."""
+    cfg = closed_box_config()
+    grid, pops = cf.initial_state(cfg)
+    lib = abi.gpu_library()
+    cap = [int(1.5 * p[1].shape[0]) + 1024 for p in pops]
+    a = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=cap)
+    b = abi.Context(lib, cf.params(cfg), cf.species(cfg), capacity=cap)
+    try:
+        a.set_path(abi.PATH_FP32)
+        b.set_path(abi.PATH_FP32)
+        load(a, cfg, grid, pops)
+        for k in ("faceB", "cellB", "nodeEta"):
+            b.upload_array(k, grid[k])
+        b.upload_cell_flags(grid["flags"])
+        for s, (cnt, p) in enumerate(pops):
+            c32, r32, w = a.download_particles_f32(s)
+            assert np.array_equal(c32, cnt) and r32.dtype == np.float32 and r32.shape == (p.shape[0], 6)
+            assert w == p[0, 6]
+            assert np.all((r32[:, :3] >= 0) & (r32[:, :3] < 1))
+            # the double records of the same particles: positions = offsets x dx
+            c64, p64 = a.download_particles(s)
+            assert np.array_equal(c64, c32)
+            assert np.array_equal(p64[:, :3], r32[:, :3].astype(np.float64) * cfg.dx)
+            assert np.array_equal(p64[:, 3:6], r32[:, 3:6].astype(np.float64))
+            b.upload_particles_f32(s, c32, r32, w)
+            c2, r2, w2 = b.download_particles_f32(s)
+            assert np.array_equal(c2, c32) and np.array_equal(r2.view(np.uint32), r32.view(np.uint32)) and w2 == w
+        a.step(5)
+        b.step(5)
+        sa, sb = snapshot(a), snapshot(b)
+        for n in sa["arrays"]:
+            assert np.array_equal(sa["arrays"][n].view(np.uint64), sb["arrays"][n].view(np.uint64)), n
+        for (ca, pa), (cb, pb) in zip(sa["particles"], sb["particles"]):
+            assert np.array_equal(ca, cb) and np.array_equal(pa.view(np.uint64), pb.view(np.uint64))
+    finally:
+        a.close()
+        b.close()
+
+
+def test_fp32_own_records_need_the_fp32_form():
+    cfg = closed_box_config()
+    ctx = abi.Context(abi.gpu_library(), cf.params(cfg), cf.species(cfg))
+    try:
+        ctx.set_path(abi.PATH_FAST)
+        with pytest.raises(abi.RhError):
+            ctx.upload_particles_f32(0, np.zeros(cfg.ncells, dtype=np.uint32), np.zeros((0, 6), np.float32), 1.0)
+    finally:
+        ctx.close()
