@@ -450,9 +450,22 @@ def run_gpu(args, rank, world, local_rank):
             lib.call("reduce_diagnostics", ctx.h, abi._ptr(diag, abi.C.c_double), ndiag)
         d2h_out = 0
         if not gpu_fill:
+            # into pinned buffers, as the per-step round trip above
             for s in range(nspec):
-                c, p = ctx.download_particles(s)
-                d2h_out += p.nbytes + c.nbytes
+                n = ctx.num_particles(s)
+                if n > out_pin[s].shape[0]:
+                    out_pin[s] = torch.empty((n, rw), dtype=rdt, pin_memory=True).numpy()
+                cnt = np.empty(cfg.ncells, dtype=np.uint32)
+                nout = abi.C.c_int64()
+                if f32rec:
+                    wout = np.zeros(1)
+                    lib.call("download_particles_f32", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
+                             abi._ptr(out_pin[s], rct), out_pin[s].shape[0], abi.C.byref(nout),
+                             abi._ptr(wout, abi.C.c_double))
+                else:
+                    lib.call("download_particles", ctx.h, s, abi._ptr(cnt, abi.C.c_uint32),
+                             abi._ptr(out_pin[s], rct), out_pin[s].shape[0], abi.C.byref(nout))
+                d2h_out += nout.value * out_pin[s].itemsize * rw + cnt.nbytes
         for name in ("cellRhoQi", "cellJi", "faceB"):
             d2h_out += ctx.download_array(name).nbytes
         torch.cuda.synchronize()
