@@ -1107,7 +1107,7 @@ int fastPush(rhgpu_ctx* c) {
    pp.maxVi2 = c->P.max_ion_speed2;
    pp.avgList = c->avgGroups > 0;
    const long long N = c->g.N, NS = c->fg.NS;
-   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, (size_t)N + 16, c->stream));
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "fast_push_deposit");
@@ -1506,7 +1506,7 @@ int f32Push(rhgpu_ctx* c) {
    c->timestep += 1;
    if (c->P.initial_flow_through_period < c->t && c->useIFT) c->useIFT = 0;
    const long long N = c->g.N, NS = c->fg.NS;
-   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, sizeof(unsigned) * (N / 32 + 1), c->stream));
+   RH_CUDA(cudaMemsetAsync(c->fb.touched, 0, (size_t)N + 16, c->stream));
    RH_CUDA(cudaMemsetAsync(c->fb.nmovers, 0, sizeof(unsigned long long), c->stream));
    {
       RH_TIME(c, "f32_push_deposit");
@@ -1933,7 +1933,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->fb.RPB, sizeof(double) * 16 * fg.nrows * fg.nseg);
    alloc((void**)&c->fb.MMlo, sizeof(unsigned long long) * 4 * N);
    alloc((void**)&c->fb.MMhi, sizeof(unsigned long long) * 4 * N);
-   alloc((void**)&c->fb.touched, sizeof(unsigned) * (N / 32 + 1));
+   alloc((void**)&c->fb.touched, (size_t)N + 16);
    alloc((void**)&c->fb.nmovers, sizeof(unsigned long long));
    alloc((void**)&c->finc, sizeof(int) * nb);
    alloc((void**)&c->ffill, sizeof(int) * nb);
@@ -1947,7 +1947,7 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->fover, 2 * sizeof(unsigned long long));
    alloc((void**)&c->diagPart, sizeof(double) * DIAG_BLOCKS * DIAG_FS);
    if (!rc) {
-      // MM starts at zero; k_fast_gather clears what a step touched
+      // MM starts at zero; the gather clears it after reading
       if (cudaMemset(c->fb.MMlo, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
           cudaMemset(c->fb.MMhi, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
           cudaMemset(c->fb.RPB, 0, sizeof(double) * 16 * fg.nrows * fg.nseg) != cudaSuccess)
