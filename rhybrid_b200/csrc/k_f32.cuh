@@ -94,27 +94,28 @@ __device__ inline bool pushF32(const GridInfo& g, const SegFields32& F, const F3
    if (accelerate) {
       float B[3], Ue[3], E[3];
       const float xs = o[0], ys = o[1], zs = o[2];
-      B[0] = xs * F.bx[lz][ly][lc + 1] + (1.0f - xs) * F.bx[lz][ly][lc];
-      B[1] = ys * F.by[lz][ly + 1][lc] + (1.0f - ys) * F.by[lz][ly][lc];
-      B[2] = zs * F.bz[lz + 1][ly][lc] + (1.0f - zs) * F.bz[lz][ly][lc];
+      // (fused multiply-adds: the FP32 form is not held to the FP64 operation order)
+      B[0] = fmaf(xs, F.bx[lz][ly][lc + 1], (1.0f - xs) * F.bx[lz][ly][lc]);
+      B[1] = fmaf(ys, F.by[lz][ly + 1][lc], (1.0f - ys) * F.by[lz][ly][lc]);
+      B[2] = fmaf(zs, F.bz[lz + 1][ly][lc], (1.0f - zs) * F.bz[lz][ly][lc]);
       for (int l = 0; l < 3; ++l) Ue[l] = F.ue[l][lz][ly][lc];
-      E[0] = B[1] * Ue[2] - B[2] * Ue[1];
-      E[1] = B[2] * Ue[0] - B[0] * Ue[2];
-      E[2] = B[0] * Ue[1] - B[1] * Ue[0];
+      E[0] = fmaf(B[1], Ue[2], -(B[2] * Ue[1]));
+      E[1] = fmaf(B[2], Ue[0], -(B[0] * Ue[2]));
+      E[2] = fmaf(B[0], Ue[1], -(B[1] * Ue[0]));
       if (pp.use_ep) for (int l = 0; l < 3; ++l) E[l] += F.ep[l][lz][ly][lc];
       const float qm = FS.qm[s];
       const float dvx = qm * E[0], dvy = qm * E[1], dvz = qm * E[2];
       const float tx = qm * B[0], ty = qm * B[1], tz = qm * B[2];
-      const float t2 = tx * tx + ty * ty + tz * tz;
+      const float t2 = fmaf(tx, tx, fmaf(ty, ty, tz * tz));
       const float b2 = 2.0f / (1.0f + t2);
       const float sx = b2 * tx, sy = b2 * ty, sz = b2 * tz;
       const float vmx = vx + dvx, vmy = vy + dvy, vmz = vz + dvz;
-      const float v0x = vmx + vmy * tz - vmz * ty;
-      const float v0y = vmy + vmz * tx - vmx * tz;
-      const float v0z = vmz + vmx * ty - vmy * tx;
-      const float vpx = vmx + v0y * sz - v0z * sy;
-      const float vpy = vmy + v0z * sx - v0x * sz;
-      const float vpz = vmz + v0x * sy - v0y * sx;
+      const float v0x = fmaf(-vmz, ty, fmaf(vmy, tz, vmx));
+      const float v0y = fmaf(-vmx, tz, fmaf(vmz, tx, vmy));
+      const float v0z = fmaf(-vmy, tx, fmaf(vmx, ty, vmz));
+      const float vpx = fmaf(-v0z, sy, fmaf(v0y, sz, vmx));
+      const float vpy = fmaf(-v0x, sz, fmaf(v0z, sx, vmy));
+      const float vpz = fmaf(-v0y, sx, fmaf(v0x, sy, vmz));
       vx = vpx + dvx; vy = vpy + dvy; vz = vpz + dvz;
       if (pp.use_gravity) {
          const float xg = (float)blockOrigin(g.x_min, i, g.dx) + o[0] * pp.dx;
@@ -127,7 +128,7 @@ __device__ inline bool pushF32(const GridInfo& g, const SegFields32& F, const F3
             vx += sg * xg; vy += sg * yg; vz += sg * zg;
          }
       }
-      const float v2 = vx * vx + vy * vy + vz * vz;
+      const float v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
       if (v2 > pp.maxVi2) {
          const float norm = sqrtf(pp.maxVi2 / v2);
          vx *= norm; vy *= norm; vz *= norm;
@@ -135,9 +136,9 @@ __device__ inline bool pushF32(const GridInfo& g, const SegFields32& F, const F3
       }
    }
    v[0] = vx; v[1] = vy; v[2] = vz;
-   o[0] += pp.dtdx * vx;
-   o[1] += pp.dtdx * vy;
-   o[2] += pp.dtdx * vz;
+   o[0] = fmaf(pp.dtdx, vx, o[0]);
+   o[1] = fmaf(pp.dtdx, vy, o[1]);
+   o[2] = fmaf(pp.dtdx, vz, o[2]);
    return clamp;
 }
 
@@ -412,9 +413,9 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
          const float* rr = sh.rec + r * REC32;
          const float w = rr[myCorner];
          a0 += w;
-         a1 += w * rr[8];
-         a2 += w * rr[9];
-         a3 += w * rr[10];
+         a1 = fmaf(w, rr[8], a1);
+         a2 = fmaf(w, rr[9], a2);
+         a3 = fmaf(w, rr[10], a3);
       }
       // ---- particles that left the segment -----------------------------------------------
       if (lm) {
