@@ -74,6 +74,7 @@ struct F32Bufs {
    unsigned long long* MMlo;   // 4 x N (shared with the FP64 fast path)
    unsigned long long* MMhi;
    unsigned char* touched;
+   const unsigned char* segInner;   // per segment: an obstacle cell within reach (shared with the fast path)
    Mover32* movers;
    unsigned long long* nmovers;
    long long moverCap;
@@ -256,6 +257,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
       sh.ptr[s][k] = v;
    }
    const int by0 = dualB(uy, g.per[1]), bz0 = dualB(uz, g.per[2]);
+   const bool segInner = fb.segInner[S] != 0;   // an obstacle cell within one step of the segment
    // (stageSegRows' own barrier publishes the prefix and the pointers)
    stageSegRows(g, f, pp.use_ep, dualB(u0, g.per[0]), by0, bz0, sh.f, sh.rows);
    __syncthreads();
@@ -316,7 +318,7 @@ k_f32_push_deposit(GridInfo gIn, Fields f, FastGeom fg, F32Set FS, F32Params pp,
                removed = true;
                atomicAdd(&cntd[4 * s + 0], w);
                atomicAdd(&cntd[4 * s + 1], ke);
-            } else if (f.flags[cidx(g, ti, tj, tk)] & RHGPU_FLAG_INNER_PARTICLE) {
+            } else if (segInner && (f.flags[cidx(g, ti, tj, tk)] & RHGPU_FLAG_INNER_PARTICLE)) {
                const float xp = (float)blockOrigin(g.x_min, ti, g.dx) + o[0] * pp.dx;
                const float yp = (float)blockOrigin(g.y_min, tj, g.dx) + o[1] * pp.dx;
                const float zp = (float)blockOrigin(g.z_min, tk, g.dx) + o[2] * pp.dx;

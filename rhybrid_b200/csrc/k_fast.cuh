@@ -90,6 +90,7 @@ struct FastBufs {
    unsigned long long* MMlo;   // 4 x N
    unsigned long long* MMhi;   // 4 x N
    unsigned char* touched;     // byte per cell: MM nonzero this step
+   const unsigned char* segInner;   // per segment: an obstacle (RHGPU_FLAG_INNER_PARTICLE) cell within reach
    Mover* movers;
    unsigned long long* nmovers;
    long long moverCap;
@@ -537,6 +538,8 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
    const int ns = FS.ns;
    const double dx = g.dx, hdx = 0.5 * dx;
    const int xs0 = dualB(u0, g.per[0]), ys0 = dualB(uy, g.per[1]), zs0 = dualB(uz, g.per[2]);
+   // no obstacle cell within one step of the segment: the obstacle test is skipped
+   const bool segInner = fb.segInner[S] != 0;
 
    // ---- set-up: species prefix (warp 0), segment pointers (warps 1-4), stencil rows (warps 5-6)
    if (warp == 0) {
@@ -645,7 +648,7 @@ k_fast_push_deposit(GridInfo gIn, Fields f, FastGeom fg, FastSpecies FS, PushPar
                atomicAdd(&cntd[4 * s + 1], ke);
             } else {
                const unsigned cn = (unsigned)ti + (unsigned)g.nx * ((unsigned)tj + (unsigned)g.ny * (unsigned)tk);
-               if (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE) {
+               if (segInner && (f.flags[cn] & RHGPU_FLAG_INNER_PARTICLE)) {
                   const double xp = blockOrigin(g.x_min, ti, dx) + st[0];
                   const double yp = blockOrigin(g.y_min, tj, dx) + st[1];
                   const double zp = blockOrigin(g.z_min, tk, dx) + st[2];

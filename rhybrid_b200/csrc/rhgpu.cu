@@ -216,6 +216,7 @@ struct rhgpu_ctx {
    FastGeom fg;
    SegHost seg[MAX_SPECIES];
    FastBufs fb = {};
+   unsigned char* segInnerDev = nullptr;   // fb.segInner: per segment, an obstacle cell within one step
    int* finc = nullptr;                 // arrivals per (species, segment)
    unsigned long long* mkey = nullptr;  // migration sort: 2 x mcap mover keys
    unsigned* mval = nullptr;            // 2 x mcap mover indices
@@ -1241,6 +1242,7 @@ int f32Init(rhgpu_ctx* c) {
    c->f32b.MMlo = c->fb.MMlo;
    c->f32b.MMhi = c->fb.MMhi;
    c->f32b.touched = c->fb.touched;
+   c->f32b.segInner = c->fb.segInner;
    c->f32b.nmovers = c->fb.nmovers;
    RH_CUDA(cudaDeviceSynchronize());   // the clears above run on the default stream
    c->f32ready = true;
@@ -1934,6 +1936,8 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
    alloc((void**)&c->fb.MMlo, sizeof(unsigned long long) * 4 * N);
    alloc((void**)&c->fb.MMhi, sizeof(unsigned long long) * 4 * N);
    alloc((void**)&c->fb.touched, (size_t)N + 16);
+   alloc((void**)&c->segInnerDev, (size_t)NS + 16);
+   c->fb.segInner = c->segInnerDev;
    alloc((void**)&c->fb.nmovers, sizeof(unsigned long long));
    alloc((void**)&c->finc, sizeof(int) * nb);
    alloc((void**)&c->ffill, sizeof(int) * nb);
@@ -1950,7 +1954,8 @@ int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_spec
       // MM starts at zero; the gather clears it after reading
       if (cudaMemset(c->fb.MMlo, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
           cudaMemset(c->fb.MMhi, 0, sizeof(unsigned long long) * 4 * N) != cudaSuccess ||
-          cudaMemset(c->fb.RPB, 0, sizeof(double) * 16 * fg.nrows * fg.nseg) != cudaSuccess)
+          cudaMemset(c->fb.RPB, 0, sizeof(double) * 16 * fg.nrows * fg.nseg) != cudaSuccess ||
+          cudaMemset(c->segInnerDev, 0, (size_t)NS + 16) != cudaSuccess)
          rc = fail(RHGPU_ERR_CUDA, "create: clear fast-path sums");
    }
    if (!rc) {
@@ -2017,7 +2022,7 @@ int rhgpu_destroy(rhgpu_ctx* c) {
       cudaFree(h.base);
       cudaFree(h.baseAlt);
    }
-   cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched);
+   cudaFree(c->fb.RP); cudaFree(c->fb.RPB); cudaFree(c->fb.MMlo); cudaFree(c->fb.MMhi); cudaFree(c->fb.touched); cudaFree(c->segInnerDev);
    cudaFree(c->fb.nmovers); cudaFree(c->fb.movers);
    for (auto& h : c->inj) { cudaFree(h.cells); cudaFree(h.rates); cudaFree(h.list); }
    cudaFree(c->injCnt);
@@ -2101,6 +2106,36 @@ int rhgpu_upload_cell_flags(rhgpu_ctx* c, const uint8_t* host) {
    std::vector<int> ob;
    for (long long n = 0; n < c->g.N; ++n)
       if (host[n] & RHGPU_FLAG_INNER_PARTICLE) ob.push_back((int)n);
+   {
+      // per row segment: can a particle of it land, within one step, in a cell
+      // flagged RHGPU_FLAG_INNER_PARTICLE? The cells it can reach are those of
+      // its dual cells one cell out on every side (x from xs0 - 1 to
+      // xs0 + SEG + 1, y and z from the base - 1 to the base + 2, wrapped on
+      // periodic axes); the push kernels test the obstacle only where one is
+      const FastGeom& fg = c->fg;
+      const GridInfo& g = c->g;
+      std::vector<unsigned char> si((size_t)fg.NS, 0);
+      if (!ob.empty()) {
+         for (long long S = 0; S < fg.NS; ++S) {
+            const long long row = S / fg.nseg;
+            const int gseg = (int)(S % fg.nseg);
+            const int uy = (int)(row % fg.nd[1]), uz = (int)(row / fg.nd[1]);
+            const int xs0 = dualB(gseg * SEG, g.per[0]), ys0 = dualB(uy, g.per[1]), zs0 = dualB(uz, g.per[2]);
+            bool hit = false;
+            for (int dz = -1; dz <= 2 && !hit; ++dz)
+               for (int dy = -1; dy <= 2 && !hit; ++dy) {
+                  int y = ys0 + dy, z = zs0 + dz;
+                  if (!wrapc(y, g.ny, g.per[1]) || !wrapc(z, g.nz, g.per[2])) continue;
+                  for (int dx = -1; dx <= SEG + 1 && !hit; ++dx) {
+                     int x = xs0 + dx;
+                     if (wrapc(x, g.nx, g.per[0])) hit = (host[cidx(g, x, y, z)] & RHGPU_FLAG_INNER_PARTICLE) != 0;
+                  }
+               }
+            si[(size_t)S] = hit ? 1 : 0;
+         }
+      }
+      RH_CUDA(cudaMemcpy(c->segInnerDev, si.data(), (size_t)fg.NS, cudaMemcpyHostToDevice));
+   }
    cudaFree(c->obst);
    c->obst = nullptr;
    c->nobst = (int)ob.size();
