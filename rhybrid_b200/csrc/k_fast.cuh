@@ -926,7 +926,8 @@ __global__ void k_mig_check(SET FS, long long NS, const int* inc, int* overflow)
    if (b >= (long long)FS.ns * NS || inc[b] == 0) return;
    const int s = (int)(b / NS);
    const long long S = b % NS;
-   if (FS.st[s].base[S] + FS.st[s].nxt.cnt[S] + inc[b] > FS.st[s].base[S + 1]) atomicOr((unsigned*)overflow, 1u);
+   // one bit per species whose arrivals do not fit (relaid alone)
+   if (FS.st[s].base[S] + FS.st[s].nxt.cnt[S] + inc[b] > FS.st[s].base[S + 1]) atomicOr((unsigned*)overflow, 1u << s);
 }
 template <class SET>
 __global__ void k_mig_counts(SET FS, long long NS, int* inc) {

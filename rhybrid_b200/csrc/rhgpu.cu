@@ -870,9 +870,12 @@ int segPrefix(rhgpu_ctx* c, const int* cnt, long long* total) {
 }
 
 // relayout of every species' next buffer with room for its pending arrivals (finc), order kept
-int fastRelayoutNext(rhgpu_ctx* c) {
+// relays out the "next" buffers of the species in `mask` (bit s: species s)
+// with room for their pending arrivals; the other species keep their layout
+int fastRelayoutNext(rhgpu_ctx* c, unsigned mask) {
    const long long NS = c->fg.NS;
    for (int s = 0; s < c->ns; ++s) {
+      if (!((mask >> s) & 1u)) continue;
       SegHost& h = c->seg[s];
       const int nx = h.cur ^ 1;   // holds the step's particles; h.cur is free
       long long total = 0;
@@ -1155,7 +1158,7 @@ int fastPush(rhgpu_ctx* c) {
          if (rc) return rc;
          if (over) {
             // some segments lack room for their arrivals: relayout with room for them
-            rc = fastRelayoutNext(c);
+            rc = fastRelayoutNext(c, (unsigned)over);
             if (rc) return rc;
             RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
             k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(fastSpecies(c), NS, c->finc, c->fover);
@@ -1481,9 +1484,12 @@ int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long l
    return RHGPU_OK;
 }
 
-int f32RelayoutNext(rhgpu_ctx* c) {
+// relays out the "next" buffers of the species in `mask` (bit s: species s)
+// with room for their pending arrivals; the other species keep their layout
+int f32RelayoutNext(rhgpu_ctx* c, unsigned mask) {
    const long long NS = c->fg.NS;
    for (int s = 0; s < c->ns; ++s) {
+      if (!((mask >> s) & 1u)) continue;
       F32Host& h = c->f32[s];
       const int nx = h.cur ^ 1;
       long long total = 0;
@@ -1552,7 +1558,7 @@ int f32Push(rhgpu_ctx* c) {
          if (rc) return rc;
          if (over) {
             // some segments lack room for their arrivals: relayout with room for them
-            rc = f32RelayoutNext(c);
+            rc = f32RelayoutNext(c, (unsigned)over);
             if (rc) return rc;
             RH_CUDA(cudaMemsetAsync(c->fover, 0, sizeof(int), c->stream));
             k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(f32Set(c), NS, c->finc, c->fover);

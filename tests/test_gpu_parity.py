@@ -286,3 +286,23 @@ def test_fast_segment_overflow_relayout(gpu_lib, port_lib):
     b = run(port_lib, cfg, 12, grid=grid, pops=pops, fast=True)
     assert_state_equal(a, b, "fast converging beams")
     assert a["particles"][0][0].max() > 1.5 * cnt.max()
+
+
+def test_fast_relayout_of_one_species(gpu_lib, port_lib):
+    """Only the species whose arrivals overflow their segments is relaid out:
+    converging cold beams of one species beside a second, slow population whose
+    segments keep their layout; bitwise with the oracle (which has no layout)."""
+    cfg = cf.config_empty_box(16, 16, 4, ppc=12.0).replace(dt=0.06)
+    beam = dataclasses.replace(cfg.populations[0], temperature=1e2)
+    slow = dataclasses.replace(cfg.populations[0], name="slow", ppc=4.0, temperature=1e3, velocity=(0.0, 0.0, 0.0))
+    cfg = cfg.replace(populations=[beam, slow])
+    grid, pops = cf.initial_state(cfg)
+    cnt, p = pops[0]
+    p = p.copy()
+    j = (np.repeat(np.arange(cnt.size), cnt.astype(np.int64)) // cfg.nx) % cfg.ny
+    p[:, 4] = np.where(j < cfg.ny // 2, 1.2e6, -1.2e6)
+    pops = [(cnt, p), pops[1]]
+    a = run(gpu_lib, cfg, 12, grid=grid, pops=pops, fast=True)
+    b = run(port_lib, cfg, 12, grid=grid, pops=pops, fast=True)
+    assert_state_equal(a, b, "fast converging beams beside a slow population")
+    assert a["particles"][0][0].max() > 1.5 * cnt.max()
