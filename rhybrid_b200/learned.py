@@ -195,13 +195,15 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
                 train_steps: int = 100, crops_per_step: int = 20, crop: int = 64, adam_steps: int = 4000,
                 lr: float = 1e-3, eval_steps: int = 100, every: int = 10, threshold: float = 0.02,
                 enforce_gate: bool = False, seed: int = 6461674, workload: str = "mars",
-                low_path: int = abi.PATH_FAST, log=print) -> dict:
+                low_path: int = abi.PATH_FAST, rho_only: bool = False, log=print) -> dict:
     """The learned form in closed loop against a high-ppc plain check run.
 
     workload: "mars" (c4_config) or "mercury" (c5_config), at `scale` of the
     cells. low_path: the particle path of the learned run (PATH_FAST, FP64, or
     PATH_FP32, the FP32 precision form); the check run and the plain runs are
-    always the FP64 fast path.
+    always the FP64 fast path. rho_only: after training, the last layer's
+    current outputs are zeroed, so the learned run denoises the charge density
+    and keeps its deposited current.
 
     1. Check run (judge_ppc, FP64 fast path, filled on the GPU) steps
        train_steps + eval_steps. During the first train_steps it yields the
@@ -269,6 +271,10 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     losses = [dn.train(adam_steps // 20, lr) for _ in range(20)]
     train_s = time.time() - t0
     params = dn.params()
+    if rho_only:
+        last = params[2 * LAYER:3 * LAYER]
+        last[:TAPS * C * C].reshape(TAPS, C, C)[:, :, 1:4] = 0.0
+        last[TAPS * C * C + 1:TAPS * C * C + 4] = 0.0
     dn.close()
     log(f"training: {adam_steps} Adam steps on {train_steps * crops_per_step} crop pairs, {train_s:.1f} s, "
         f"losses {losses[0]:.4g} -> {losses[-1]:.4g}")
@@ -326,6 +332,7 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     res = {
         "workload": workload, "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx,
         "dt_s": judge_cfg.dt, "learned_path": "fp32" if low_path == abi.PATH_FP32 else "fast",
+        "denoised": "rho" if rho_only else "rho, J",
         "check_run": {"ppc": judge_ppc, "ions": int(n_judge), "ms_per_step": judge_ms,
                       "split_half_noise": {str(k): {"rho": v[0], "J": v[1]} for k, v in judge_noise.items()}},
         "training": {"pairs": train_steps * crops_per_step, "crop": crop, "factor": factor, "adam_steps": adam_steps,
@@ -397,6 +404,7 @@ def main(argv=None):
     ap.add_argument("--eval-steps", type=int, default=100)
     ap.add_argument("--adam-steps", type=int, default=4000)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--rho-only", action="store_true", help="denoise the charge density only (keep the current)")
     ap.add_argument("--plain", default="8,16,32,64,128")
     ap.add_argument("--workload", default="mars", choices=sorted(GEOMETRIES))
     ap.add_argument("--learned-path", default="fast", choices=["fast", "fp32"],
@@ -409,7 +417,7 @@ def main(argv=None):
         return
     out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
                       adam_steps=a.adam_steps, lr=a.lr, plain_ppcs=tuple(int(x) for x in a.plain.split(",")),
-                      workload=a.workload,
+                      workload=a.workload, rho_only=a.rho_only,
                       low_path=abi.PATH_FP32 if a.learned_path == "fp32" else abi.PATH_FAST)
     print(json.dumps(out))
     if a.json:
