@@ -529,13 +529,14 @@ def run_learned(args, rank, world, local_rank):
     error (measured plain points only). Replicas only: every rank runs it, rank
     0 prints. --workload mercury takes the Mercury-like geometry (at --scale of its
     cells: its 256-ppc check run fits one GPU up to about 0.064), --path fp32 runs
-    the learned form on the FP32 precision form."""
+    the learned form on the FP32 precision form, --velocity denoises rho and the
+    bulk velocity J / rho in place of rho and J."""
     import torch
     from rhybrid_b200 import abi, learned
     torch.cuda.set_device(local_rank)
     workload = "mercury" if args.workload == "mercury" else "mars"
     low_path = abi.PATH_FP32 if args.path == "fp32" else abi.PATH_FAST
-    out = learned.closed_loop(scale=args.scale, workload=workload, low_path=low_path,
+    out = learned.closed_loop(scale=args.scale, workload=workload, low_path=low_path, velocity=args.velocity,
                               log=lambda m: print(m, file=sys.stderr, flush=True))
     lr = out["learned"]
     if rank == 0:
@@ -547,6 +548,7 @@ def run_learned(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("f32" if low_path == abi.PATH_FP32 else "f64") + " (network bf16, fp32 accum)",
             "data": "synthetic (uniform fill generated on the GPU, solar wind sources)",
             "config": {"workload": f"{workload}_{out['geometry'][0]}x{out['geometry'][1]}x{out['geometry'][2]}_learned",
+                       "denoised": out["denoised"],
                        "check_run": out["check_run"], "training": out["training"], "window": out["window"],
                        "threshold": out["threshold"],
                        "learned": {k: v for k, v in lr.items() if k != "samples"},
@@ -596,6 +598,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's cells (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--velocity", action="store_true",
+                    help="--form learned: the denoiser sees rho and J / rho (rhgpu_dn_set_velocity_form)")
     ap.add_argument("--path", default="fast", choices=["fast", "exact", "fp32"],
                     help="fast: FP64, segment storage and deposit order (default); exact: the reference's order; "
                          "fp32: the FP32 precision form")

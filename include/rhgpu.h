@@ -290,6 +290,13 @@ int rhgpu_dn_destroy(rhgpu_dn* dn);
 int rhgpu_dn_set_params(rhgpu_dn* dn, const float* params, int64_t n);
 int rhgpu_dn_get_params(rhgpu_dn* dn, float* params, int64_t n);
 int rhgpu_dn_set_scales(rhgpu_dn* dn, double rho_scale, double j_scale);
+/* velocity form (no counterpart in the reference; off by default): the network
+ * sees rho / rho_scale and the bulk velocity (J / rho) / j_scale in place of
+ * J / j_scale, in its training pairs and where it is applied, and hands back
+ * J = rho' u' from its denoised density and velocity. j_scale is then a speed.
+ * The deposit's rho and J carry the same particles' noise, which largely
+ * cancels in J / rho; this form keeps that ratio as one quantity. */
+int rhgpu_dn_set_velocity_form(rhgpu_dn* dn, int32_t enabled);
 /* host moments in the ABI layout (rho per cell, Ji interleaved) in and out;
  * rho_out is clamped at min_rho as the deposit's finalize does */
 int rhgpu_dn_apply(rhgpu_dn* dn, const double* rho_in, const double* ji_in, double* rho_out, double* ji_out,

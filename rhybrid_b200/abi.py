@@ -150,6 +150,7 @@ _OPTIONAL = {
     "fill_uniform": [_P, C.c_int32, C.c_void_p, C.c_void_p],
     "dn_add_crops": [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_void_p],
     "dn_set_loss_border": [_P, C.c_int32],
+    "dn_set_velocity_form": [_P, C.c_int32],
     "set_timing": [_P, C.c_int32],
     "get_timing": [_P, C.c_char_p, C.c_int32, _D, C.c_int32, C.POINTER(C.c_int32)],
     "last_launch_count": [_P, _I64],
@@ -610,6 +611,11 @@ class Denoiser:
 
     def set_scales(self, rho_scale: float, j_scale: float):
         self.lib.call("dn_set_scales", self.h, rho_scale, j_scale)
+
+    def set_velocity_form(self, enabled: bool):
+        """rhgpu_dn_set_velocity_form: the network sees rho and J/rho (j_scale a
+        speed) and hands back J = rho' u'."""
+        self.lib.call("dn_set_velocity_form", self.h, 1 if enabled else 0)
 
     def apply(self, rho: np.ndarray, ji: np.ndarray, min_rho: float = -np.inf):
         r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)

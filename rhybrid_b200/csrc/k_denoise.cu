@@ -124,11 +124,12 @@ __global__ void k_dn_adam(float* p, const float* gr, float* m, float* v, const u
    p[e] -= lr * (m[e] / c1) / (sqrtf(v[e] / c2) + eps);
 }
 
-__global__ void k_dn_norm(long long N, const double* rho, const double* J, double rsr, double rsj, float* out) {
+__global__ void k_dn_norm(long long N, const double* rho, const double* J, double rsr, double rsj, int vel, float* out) {
    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (v >= N) return;
+   const double fj = dnJFactor(vel, rsj, rho[v]);
    out[v * 4] = (float)(rho[v] * rsr);
-   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(J[l * N + v] * rsj);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(J[l * N + v] * fj);
 }
 
 __global__ void k_dn_res_to_act(long long N, const float* res, unsigned* act) {
@@ -175,13 +176,14 @@ __global__ void k_dn_crop(const float* full, int fnx, int fny, DnGrid c, int x0,
 }
 
 __global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double rsr, double rsj,
-                                      float* out) {
+                                      int vel, float* out) {
    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (v >= N) return;
    double r = acc[v] / dV;
    if (r < minRho) r = minRho;
+   const double fj = dnJFactor(vel, rsj, r);
    out[v * 4] = (float)(r * rsr);
-   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(acc[(1 + l) * N + v] / dV * rsj);
+   for (int l = 0; l < 3; ++l) out[v * 4 + 1 + l] = (float)(acc[(1 + l) * N + v] / dV * fj);
 }
 
 __global__ void k_dn_err(long long N, const float* a, const float* t, double* part) {

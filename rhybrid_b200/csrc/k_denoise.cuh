@@ -88,7 +88,15 @@ struct DnMoments {
    double* J;      // 3 x N
    double sr, sj, rsr, rsj, minRho;
    long long N;
+   int vel;        // velocity form: the network sees rho and J / rho (sj the velocity scale)
 };
+
+// the factor that takes a current component to the network's input: 1 / sj,
+// or in the velocity form 1 / (sj rho), the bulk velocity J / rho over its
+// scale (0 where rho is not positive)
+__host__ __device__ inline double dnJFactor(int vel, double rsj, double rho) {
+   return vel ? (rho > 0.0 ? rsj / rho : 0.0) : rsj;
+}
 
 // ---- the convolution on the 5th-generation tensor cores (tcgen05) ----------------------------
 // One convolution layer as an implicit GEMM on tcgen05.mma (kind::f16, BF16 x
@@ -209,10 +217,11 @@ __device__ __forceinline__ void tcStageSlice(TcShared& sh, const DnGrid& g, cons
          cpAsync16(dst, reinterpret_cast<const uint4*>(in) + (gv * 2 + h), ok ? 16 : 0);
       } else {
          uint4 v = make_uint4(0u, 0u, 0u, 0u);
-         if (ok && h == 0)
-            v = make_uint4(packBf16((float)(mom.rho[gv] * mom.rsr), (float)(mom.J[gv] * mom.rsj)),
-                           packBf16((float)(mom.J[mom.N + gv] * mom.rsj), (float)(mom.J[2 * mom.N + gv] * mom.rsj)),
-                           0u, 0u);
+         if (ok && h == 0) {
+            const double r = mom.rho[gv], fj = dnJFactor(mom.vel, mom.rsj, r);
+            v = make_uint4(packBf16((float)(r * mom.rsr), (float)(mom.J[gv] * fj)),
+                           packBf16((float)(mom.J[mom.N + gv] * fj), (float)(mom.J[2 * mom.N + gv] * fj)), 0u, 0u);
+         }
          *reinterpret_cast<uint4*>(dst) = v;
       }
    }
@@ -276,11 +285,14 @@ __device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int g
          continue;
       }
       if (mode == 4) {
-         double r0 = (double)(c[0] + (float)(mom.rho[v] * mom.rsr)) * mom.sr;
+         // the velocity form writes back J = rho' u' from the denoised density and velocity
+         const double rin = mom.rho[v], fj = dnJFactor(mom.vel, mom.rsj, rin);
+         double r0 = (double)(c[0] + (float)(rin * mom.rsr)) * mom.sr;
          if (r0 < mom.minRho) r0 = mom.minRho;
-         const double j0 = (double)(c[1] + (float)(mom.J[v] * mom.rsj)) * mom.sj;
-         const double j1 = (double)(c[2] + (float)(mom.J[mom.N + v] * mom.rsj)) * mom.sj;
-         const double j2 = (double)(c[3] + (float)(mom.J[2 * mom.N + v] * mom.rsj)) * mom.sj;
+         double j0 = (double)(c[1] + (float)(mom.J[v] * fj)) * mom.sj;
+         double j1 = (double)(c[2] + (float)(mom.J[mom.N + v] * fj)) * mom.sj;
+         double j2 = (double)(c[3] + (float)(mom.J[2 * mom.N + v] * fj)) * mom.sj;
+         if (mom.vel) { j0 *= r0; j1 *= r0; j2 *= r0; }
          mom.rho[v] = r0;
          mom.J[v] = j0;
          mom.J[mom.N + v] = j1;
@@ -474,10 +486,10 @@ __global__ void k_dn_loss(DnGrid g, const float* pred, const float* target, doub
 __global__ void k_dn_adam(float* p, const float* gr, float* m, float* v, const unsigned char* mask, int n, float lr,
                           float b1, float b2, float eps, float c1, float c2);
 
-// planar FP64 moments (rho N, J 3N) -> normalized FP32 residual copy (N x 4) + BF16 input (16 channels)
 // normalized FP32 copy (N x 4) of planar FP64 moments: rho / sr and J / sj as
-// products with the reciprocals rsr = 1 / sr, rsj = 1 / sj
-__global__ void k_dn_norm(long long N, const double* rho, const double* J, double rsr, double rsj, float* out);
+// products with the reciprocals rsr = 1 / sr, rsj = 1 / sj (velocity form:
+// J / (sj rho), dnJFactor)
+__global__ void k_dn_norm(long long N, const double* rho, const double* J, double rsr, double rsj, int vel, float* out);
 
 // FP32 normalized moments (N x 4) -> BF16 network input (16 channels)
 __global__ void k_dn_res_to_act(long long N, const float* res, unsigned* act);
@@ -487,13 +499,14 @@ __global__ void k_dn_res_to_act(long long N, const float* res, unsigned* act);
 // atomics: training data only). One block per segment.
 __global__ void k_dn_subsample_deposit(GridInfo g, FastGeom fg, SegBuf B, const long long* base, double q, int factor,
                                        int offset, double* acc);
-// the deposit's finalize on the subsample sums: /dV, rho clamp, then normalized FP32 (N x 4)
 // one crop of a normalized (N x 4) moment grid: the crop's voxel (x, y, z) is
 // the full grid's (x0 + x, y0 + y, z0 + z)
 __global__ void k_dn_crop(const float* full, int fnx, int fny, DnGrid c, int x0, int y0, int z0, float* out);
 
+// the deposit's finalize on the subsample sums: /dV, rho clamp, then normalized
+// FP32 (N x 4) as k_dn_norm
 __global__ void k_dn_subsample_finish(long long N, const double* acc, double dV, double minRho, double rsr, double rsj,
-                                      float* out);
+                                      int vel, float* out);
 
 // squared-error sums for the relative L2 errors of one pair: per block
 // {sum |a-t|^2 rho, sum |t|^2 rho, sum |a-t|^2 J, sum |t|^2 J}

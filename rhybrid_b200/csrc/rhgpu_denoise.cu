@@ -114,7 +114,7 @@ int dnUploadMoments(rhgpu_dn* d, const double* rho, const double* ji, double* pl
 // and scales back (rho clamped at minRho), in three launches
 int dnApplyMoments(rhgpu_dn* d, cudaStream_t st, double* rho, double* J, double minRho, unsigned* err) {
    const long long N = d->g.N;
-   const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N};
+   const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N, d->vel};
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
@@ -240,6 +240,12 @@ int rhgpu_dn_set_scales(rhgpu_dn* d, double rho_scale, double j_scale) {
    return RHGPU_OK;
 }
 
+int rhgpu_dn_set_velocity_form(rhgpu_dn* d, int32_t enabled) {
+   if (!d) return fail(RHGPU_ERR_ARG, "dn_set_velocity_form: null denoiser");
+   d->vel = enabled ? 1 : 0;
+   return RHGPU_OK;
+}
+
 int rhgpu_dn_apply(rhgpu_dn* d, const double* rho_in, const double* ji_in, double* rho_out, double* ji_out, double min_rho) {
    if (!d || !rho_in || !ji_in || !rho_out || !ji_out) return fail(RHGPU_ERR_ARG, "dn_apply: bad arguments");
    RH_CUDA(cudaSetDevice(d->device));
@@ -266,13 +272,13 @@ int rhgpu_dn_loss_grad(rhgpu_dn* d, const double* rho_in, const double* ji_in, c
    const long long N = d->g.N;
    int rc = dnUploadMoments(d, rho_t, ji_t, d->acc);
    if (rc) return rc;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->out32);
+   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->vel, d->out32);
    // target kept in dY[0]'s storage as FP32 (N x 4 floats fit in 8 u32 per voxel)
    float* target = reinterpret_cast<float*>(d->dY[0]);
    RH_CUDA(cudaMemcpyAsync(target, d->out32, sizeof(float) * 4 * N, cudaMemcpyDeviceToDevice, d->stream));
    rc = dnUploadMoments(d, rho_in, ji_in, d->acc);
    if (rc) return rc;
-   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->res);
+   k_dn_norm<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, d->acc, d->acc + N, 1.0 / d->sr, 1.0 / d->sj, d->vel, d->res);
    rc = dnForward(d);
    if (rc) return rc;
    // the loss kernel reads the target before the backward overwrites dY[0]
@@ -302,7 +308,7 @@ int dnDepositSample(rhgpu_dn* d, rhgpu_ctx* c, int factor, int offset, double* a
                                                                        c->sp[s].q, factor, offset, acc);
    }
    k_dn_subsample_finish<<<blocks1d(N, 256), 256, 0, d->stream>>>(N, acc, c->g.dV, c->P.min_ion_charge_density,
-                                                                 1.0 / d->sr, 1.0 / d->sj, out);
+                                                                 1.0 / d->sr, 1.0 / d->sj, d->vel, out);
    RH_CUDA(cudaGetLastError());
    return RHGPU_OK;
 }

@@ -228,6 +228,7 @@ struct rhgpu_dn {
    float* fullIn = nullptr;
    float* fullOut = nullptr;
    unsigned long long rng = 0x9e3779b97f4a7c15ull;
+   int vel = 0;                          // velocity form (rhgpu_dn_set_velocity_form)
 };
 
 namespace rhh {

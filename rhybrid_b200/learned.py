@@ -56,6 +56,13 @@ def moment_scales(cfg: cf.Config):
     return abs(rho), abs(rho) * speed
 
 
+def velocity_scales(cfg: cf.Config):
+    """Normalization of the velocity form: the upstream charge density and the
+    upstream speed."""
+    rho, j = moment_scales(cfg)
+    return rho, j / rho
+
+
 def relative_l2(a: np.ndarray, b: np.ndarray) -> float:
     a, b = np.asarray(a, float).reshape(-1), np.asarray(b, float).reshape(-1)
     d = np.linalg.norm(b)
@@ -195,7 +202,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
                 train_steps: int = 100, crops_per_step: int = 20, crop: int = 64, adam_steps: int = 4000,
                 lr: float = 1e-3, eval_steps: int = 100, every: int = 10, threshold: float = 0.02,
                 enforce_gate: bool = False, seed: int = 6461674, workload: str = "mars",
-                low_path: int = abi.PATH_FAST, rho_only: bool = False, log=print) -> dict:
+                low_path: int = abi.PATH_FAST, rho_only: bool = False, velocity: bool = False,
+                log=print) -> dict:
     """The learned form in closed loop against a high-ppc plain check run.
 
     workload: "mars" (c4_config) or "mercury" (c5_config), at `scale` of the
@@ -203,7 +211,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     PATH_FP32, the FP32 precision form); the check run and the plain runs are
     always the FP64 fast path. rho_only: after training, the last layer's
     current outputs are zeroed, so the learned run denoises the charge density
-    and keeps its deposited current.
+    and keeps its deposited current. velocity: the network denoises rho and
+    the bulk velocity J / rho (rhgpu_dn_set_velocity_form) instead of rho and J.
 
     1. Check run (judge_ppc, FP64 fast path, filled on the GPU) steps
        train_steps + eval_steps. During the first train_steps it yields the
@@ -238,7 +247,11 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     judge_cfg = geom(float(judge_ppc), scale)
     factor = judge_ppc // low_ppc
     dn = abi.Denoiser(lib, crop, crop, crop, (0, 0, 0), pair_capacity=train_steps * crops_per_step)
-    dn.set_scales(*moment_scales(judge_cfg))
+    if velocity:
+        dn.set_velocity_form(True)
+        dn.set_scales(*velocity_scales(judge_cfg))
+    else:
+        dn.set_scales(*moment_scales(judge_cfg))
     dn.set_params(init_params(seed % 1000))
     dn.set_loss_border(3)
     half = abi.Denoiser(lib, judge_cfg.nx, judge_cfg.ny, judge_cfg.nz, judge_cfg.periodic, pair_capacity=1)
@@ -286,7 +299,11 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
         try:
             if learned:
                 net = abi.Denoiser(lib, cfg.nx, cfg.ny, cfg.nz, cfg.periodic)
-                net.set_scales(*moment_scales(cfg))
+                if velocity:
+                    net.set_velocity_form(True)
+                    net.set_scales(*velocity_scales(cfg))
+                else:
+                    net.set_scales(*moment_scales(cfg))
                 net.set_params(params)
                 ctx.set_denoiser(net, True)
             ctx.step(train_steps)
@@ -332,7 +349,7 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     res = {
         "workload": workload, "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx,
         "dt_s": judge_cfg.dt, "learned_path": "fp32" if low_path == abi.PATH_FP32 else "fast",
-        "denoised": "rho" if rho_only else "rho, J",
+        "denoised": "rho" if rho_only else ("rho, J/rho" if velocity else "rho, J"),
         "check_run": {"ppc": judge_ppc, "ions": int(n_judge), "ms_per_step": judge_ms,
                       "split_half_noise": {str(k): {"rho": v[0], "J": v[1]} for k, v in judge_noise.items()}},
         "training": {"pairs": train_steps * crops_per_step, "crop": crop, "factor": factor, "adam_steps": adam_steps,
@@ -405,6 +422,7 @@ def main(argv=None):
     ap.add_argument("--adam-steps", type=int, default=4000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--rho-only", action="store_true", help="denoise the charge density only (keep the current)")
+    ap.add_argument("--velocity", action="store_true", help="denoise rho and the bulk velocity J/rho")
     ap.add_argument("--plain", default="8,16,32,64,128")
     ap.add_argument("--workload", default="mars", choices=sorted(GEOMETRIES))
     ap.add_argument("--learned-path", default="fast", choices=["fast", "fp32"],
@@ -417,7 +435,7 @@ def main(argv=None):
         return
     out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
                       adam_steps=a.adam_steps, lr=a.lr, plain_ppcs=tuple(int(x) for x in a.plain.split(",")),
-                      workload=a.workload, rho_only=a.rho_only,
+                      workload=a.workload, rho_only=a.rho_only, velocity=a.velocity,
                       low_path=abi.PATH_FP32 if a.learned_path == "fp32" else abi.PATH_FAST)
     print(json.dumps(out))
     if a.json:
