@@ -18,8 +18,8 @@ vectors, N cells in linear order n = i + nx*(j + ny*k). The grid arrays,
 particles and averages are read from the device through the context; the
 per-cell moments are then summed on the host in the reference's order (per
 cell: output populations in species order, particles in list order), so the
-values are the reference's bit for bit on the same state. This library keeps
-the arrays as a NumPy archive (run.py); it does not write the VLSV container.
+values are the reference's bit for bit on the same state. rhybrid_b200.vlsv
+writes them as the reference's VLSV state file (run.py).
 
 prod_rate_iono<k> / prod_rate_exo<k> are the rate-based sources' expected
 macroparticles per step in each cell (rhgpu_source_rates). Not written: cellB0

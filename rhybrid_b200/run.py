@@ -4,8 +4,8 @@ the population and field logs every log_interval steps (before the step, with
 the max-B stop), and at every data save step the variables of
 Hybrid.output_parameters (the arrays the reference's output operator hands to
 its VLSV writer, output.cell_variables) and, with Hybrid.save_particles, the
-particle points (output.particle_points), written as a NumPy archive
-(state_<timestep>.npz; this library does not write the VLSV container).
+particle points (output.particle_points), written as the reference's VLSV
+state file (state_<timestep>.vlsv, rhybrid_b200.vlsv).
 
     python -m rhybrid_b200.run mars.cfg --steps 1000 --out run1
 
@@ -23,12 +23,13 @@ from . import abi
 from . import cfg as C
 from . import config as cf
 from . import output as O
+from . import vlsv as V
 
 
 def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: str = "fast", device: int = 0,
         lib: Optional[abi.Library] = None, quiet: bool = False) -> dict:
     """Runs `steps` time steps (the file's maximum_timesteps by default).
-    Returns {"steps": steps run, "stopped": max-B stop, "saved": [npz files]}."""
+    Returns {"steps": steps run, "stopped": max-B stop, "saved": [state files]}."""
     config, rs = C.load(cfg_path)
     os.makedirs(out_dir, exist_ok=True)
     nsteps = rs.maximum_timesteps if steps is None else steps
@@ -75,12 +76,9 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
             ts = ctx.time()[1]
             if rs.data_save_interval > 0 and ts % rs.data_save_interval == 0:
                 out = O.cell_variables(ctx, rs.output_parameters, rs.output_groups, rs.output_group_names)
-                if rs.save_particles:
-                    out.update(O.particle_points(ctx, rs.species_names, rs.save_particles_nstride))
-                out["time"] = np.array(ctx.time()[0])
-                out["timestep"] = np.array(ts)
-                fn = os.path.join(out_dir, f"state_{ts:07d}.npz")
-                np.savez(fn, **out)
+                parts = O.particle_points(ctx, rs.species_names, rs.save_particles_nstride) if rs.save_particles else None
+                fn = os.path.join(out_dir, f"state_{ts:07d}.vlsv")
+                V.write_state(fn, V.grid_of(ctx), ctx.time()[0], ts, out, parts)
                 saved.append(fn)
         if logging:
             ctx.log_close()

@@ -4,6 +4,7 @@ step, states with the temporal averages at every data save step."""
 import numpy as np
 
 from rhybrid_b200 import run as R
+from rhybrid_b200 import vlsv as V
 
 from test_cpu_cfg import TEXT
 
@@ -20,8 +21,10 @@ def test_run_loop(tmp_path, ref_lib):
     assert r["steps"] == 6 and not r["stopped"] and len(r["saved"]) == 2
     field = [ln for ln in open(out / "field.log") if not ln.startswith("%")]
     assert len(field) == 3   # time steps 0, 2, 4
-    st = np.load(r["saved"][1])
+    st = V.load_state(r["saved"][1])
+    assert r["saved"][1].endswith("state_0000006.vlsv")
     assert int(st["timestep"]) == 6 and st["cellB"].shape == (24 * 16 * 12, 3)
+    assert np.array_equal(st["CellID"], np.arange(24 * 16 * 12))
     # Hybrid.output_parameters = cellB n_ave v_ave: ne comes with the averages (operator_userdata.cpp:104-116)
-    assert sorted(st.files) == sorted(["cellB", "ne", "n_H+_ave", "v_H+_ave", "time", "timestep"])
+    assert sorted(st) == sorted(["CellID", "cellB", "ne", "n_H+_ave", "v_H+_ave", "time", "timestep"])
     assert st["n_H+_ave"].shape == (24 * 16 * 12,) and np.any(st["n_H+_ave"] > 0)

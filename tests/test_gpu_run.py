@@ -8,6 +8,7 @@ from rhybrid_b200 import abi
 from rhybrid_b200 import cfg as C
 from rhybrid_b200 import config as cf
 from rhybrid_b200 import run as R
+from rhybrid_b200 import vlsv as V
 
 from test_cpu_cfg import TEXT
 
@@ -27,7 +28,7 @@ def test_run_loop_gpu(tmp_path, path):
     assert len([ln for ln in open(out / "field.log") if not ln.startswith("%")]) == 3
     pop = [ln.split() for ln in open(out / "pop001_swH+.log") if not ln.startswith("%")]
     assert float(pop[-1][2]) > 0 and float(pop[-1][11]) > 0   # macroparticles, inject rate
-    st = np.load(r["saved"][-1])
+    st = V.load_state(r["saved"][-1])
     assert np.all(np.isfinite(st["cellB"])) and np.all(np.isfinite(st["ne"]))
     # the sources' expected macroparticles per step: the ionosphere's add up to its
     # macroparticles per step, the exosphere's to at most that (shadow factor)
