@@ -31,6 +31,9 @@ class RunSettings:
     output_group_names: List[str] = field(default_factory=list)   # output_str of each output population
     save_particles: bool = False            # Hybrid.save_particles (user.cpp:396)
     save_particles_nstride: int = 10        # Hybrid.save_particles_Nstride (user.cpp:397)
+    save_reduced_state_interval: int = 0    # Hybrid.save_reduced_state_interval (user.cpp:420)
+    save_reduced_state_nstride: int = 10    # Hybrid.save_reduced_state_Nstride (user.cpp:421; <= 0 gives 10, :2452-2455)
+    save_reduced_state_particles: bool = False   # Hybrid.save_reduced_state_include_particles (user.cpp:422)
     species_names: List[str] = field(default_factory=list)
     extra: Dict[str, Dict[str, List[str]]] = field(default_factory=dict)
 
@@ -230,6 +233,10 @@ def load_text(text: str) -> Tuple[cf.Config, RunSettings]:
         output_parameters=(hy.str("output_parameters", "") or "").split(), output_groups=groups,
         output_group_names=seen, save_particles=hy.bool("save_particles"),
         save_particles_nstride=hy.int("save_particles_Nstride", 10), species_names=names,
+        save_reduced_state_interval=hy.int("save_reduced_state_interval", 0),
+        save_reduced_state_nstride=(hy.int("save_reduced_state_Nstride", 10)
+                                    if hy.int("save_reduced_state_Nstride", 10) > 0 else 10),
+        save_reduced_state_particles=hy.bool("save_reduced_state_include_particles"),
         extra={k: v for k, v in P.items() if k in ("Restart", "LoadBalance", "DetectorParticle",
                                                     "DetectorBulkParameter", "DataOperatorExcludes")})
     return cfgobj, rs

@@ -210,6 +210,31 @@ def cell_variables(ctx, params: Iterable[str], groups: Sequence[int] = (), group
     return out
 
 
+def _strided_cells(nx: int, ny: int, n: int, nstride: int) -> np.ndarray:
+    """The cells an Nstride output keeps: id c with c % Nstride == 0,
+    c % (Nstride nx) < nx and c % (Nstride nx ny) < nx ny (ids are the linear
+    cell index)."""
+    cid = np.arange(n, dtype=np.int64)
+    return (cid % nstride == 0) & (cid % (nstride * nx) < nx) & (cid % (nstride * nx * ny) < nx * ny)
+
+
+def reduced_state(ctx, species_names: Sequence[str], nstride: int = 10, particles: bool = False) -> Dict[str, np.ndarray]:
+    """diagnostics::saveStateReduced (diagnostics.h:819-960): cellB and the
+    cell id of every cell an Nstride output keeps, and with `particles` each
+    species' particles in those cells as CellID_<name> and v_<name>."""
+    nx, ny, nz = _grid(ctx)
+    sel = _strided_cells(nx, ny, ctx.ncells, nstride)
+    out = {"CellID": np.flatnonzero(sel).astype(np.uint32), "cellB": ctx.download_array("cellB")[sel]}
+    if particles:
+        for s, name in enumerate(species_names):
+            cnt, q = ctx.download_particles(s)
+            cell = _cell_index(cnt)
+            keep = sel[cell]
+            out[f"CellID_{name}"] = cell[keep].astype(np.uint32)
+            out[f"v_{name}"] = q[keep, 3:6].copy()
+    return out
+
+
 def particle_points(ctx, species_names: Sequence[str], nstride: int = 10) -> Dict[str, np.ndarray]:
     """ParticleListHybrid::writeParticles (particle_list_hybrid.h:41-159) for
     every species: the particles of the cells whose id c satisfies
@@ -222,7 +247,7 @@ def particle_points(ctx, species_names: Sequence[str], nstride: int = 10) -> Dic
     nx, ny, nz = _grid(ctx)
     p = ctx.params
     cid = np.arange(ctx.ncells, dtype=np.int64)
-    sel = (cid % nstride == 0) & (cid % (nstride * nx) < nx) & (cid % (nstride * nx * ny) < nx * ny)
+    sel = _strided_cells(nx, ny, ctx.ncells, nstride)
     i, j, k = cid % nx, (cid // nx) % ny, cid // (nx * ny)
     corner = np.stack([p.x_min + i.astype(np.float64) * p.dx, p.y_min + j.astype(np.float64) * p.dx,
                        p.z_min + k.astype(np.float64) * p.dx], axis=1)

@@ -5,7 +5,10 @@ the max-B stop), and at every data save step the variables of
 Hybrid.output_parameters (the arrays the reference's output operator hands to
 its VLSV writer, output.cell_variables) and, with Hybrid.save_particles, the
 particle points (output.particle_points), written as the reference's VLSV
-state file (state_<timestep>.vlsv, rhybrid_b200.vlsv).
+state file (state_<timestep>.vlsv, rhybrid_b200.vlsv); with
+Hybrid.save_reduced_state_interval, the reduced state every that many steps
+(reduced<timestep>.vlsv: cellB of every Nstride-th cell, optionally those
+cells' particles).
 
     python -m rhybrid_b200.run mars.cfg --steps 1000 --out run1
 
@@ -29,7 +32,8 @@ from . import vlsv as V
 def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: str = "fast", device: int = 0,
         lib: Optional[abi.Library] = None, quiet: bool = False) -> dict:
     """Runs `steps` time steps (the file's maximum_timesteps by default).
-    Returns {"steps": steps run, "stopped": max-B stop, "saved": [state files]}."""
+    Returns {"steps": steps run, "stopped": max-B stop, "saved": [state files],
+    "reduced": [reduced state files]}."""
     config, rs = C.load(cfg_path)
     os.makedirs(out_dir, exist_ok=True)
     nsteps = rs.maximum_timesteps if steps is None else steps
@@ -40,7 +44,7 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
         raise RuntimeError(f"{lib.path}: this library has no particle sources")
     cap = [p[1].shape[0] + p[1].shape[0] // 4 + (1 << 16) for p in pops]
     ctx = abi.Context(lib, cf.params(config), cf.species(config), capacity=cap, device=device)
-    saved, stopped, done = [], False, 0
+    saved, reduced, stopped, done = [], [], False, 0
     try:
         if lib.has("set_path"):
             ctx.set_path({"fast": abi.PATH_FAST, "fp32": abi.PATH_FP32, "exact": abi.PATH_EXACT}[path])
@@ -74,6 +78,13 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
             ctx.step(1)
             done += 1
             ts = ctx.time()[1]
+            # the reduced state, written at the end of propagate() (user.cpp:150-155)
+            if rs.save_reduced_state_interval > 0 and ts % rs.save_reduced_state_interval == 0:
+                red = O.reduced_state(ctx, rs.species_names, rs.save_reduced_state_nstride,
+                                      rs.save_reduced_state_particles)
+                fn = os.path.join(out_dir, f"reduced{ts:08d}.vlsv")
+                V.write_reduced_state(fn, ctx.time()[0], ts, rs.save_reduced_state_nstride, red, rs.species_names)
+                reduced.append(fn)
             if rs.data_save_interval > 0 and ts % rs.data_save_interval == 0:
                 out = O.cell_variables(ctx, rs.output_parameters, rs.output_groups, rs.output_group_names)
                 parts = O.particle_points(ctx, rs.species_names, rs.save_particles_nstride) if rs.save_particles else None
@@ -84,7 +95,7 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
             ctx.log_close()
     finally:
         ctx.close()
-    return {"steps": done, "stopped": stopped, "saved": saved}
+    return {"steps": done, "stopped": stopped, "saved": saved, "reduced": reduced}
 
 
 def main(argv=None):

@@ -143,6 +143,33 @@ def write_state(path: str, grid: Mapping, time: float, timestep: int, cell_varia
     return path
 
 
+def write_reduced_state(path: str, time: float, timestep: int, nstride: int, reduced: Mapping[str, np.ndarray],
+                        species_names=()) -> str:
+    """The reduced state file (diagnostics::saveStateReduced,
+    diagnostics.h:819-960): the time, time step and Nstride parameters, then
+    CellID and cellB of the kept cells as pointdata on ReducedPointMesh, and
+    for each species in `reduced` (output.reduced_state with particles) its
+    CellID_<name> and v_<name> as pointdata on ReducedParticlePointMesh_<name>.
+    No mesh element is written for these point meshes, as in the reference."""
+    with Writer(path) as w:
+        w.write("PARAMETER", np.float64(time), name="time")
+        w.write("PARAMETER", np.uint32(timestep), name="timestep")
+        w.write("PARAMETER", np.uint32(nstride), name="Nstride")
+        w.write("VARIABLE", np.asarray(reduced["CellID"], dtype=np.uint32), name="CellID", mesh="ReducedPointMesh",
+                type="pointdata")
+        w.write("VARIABLE", np.asarray(reduced["cellB"], dtype=np.float64).reshape(-1, 3), name="cellB",
+                mesh="ReducedPointMesh", type="pointdata")
+        for name in species_names:
+            if f"v_{name}" not in reduced:
+                continue
+            mesh = f"ReducedParticlePointMesh_{name}"
+            w.write("VARIABLE", np.asarray(reduced[f"CellID_{name}"], dtype=np.uint32), name=f"CellID_{name}",
+                    mesh=mesh, type="pointdata")
+            w.write("VARIABLE", np.asarray(reduced[f"v_{name}"], dtype=np.float64).reshape(-1, 3), name=f"v_{name}",
+                    mesh=mesh, type="pointdata")
+    return path
+
+
 def grid_of(ctx) -> dict:
     """The spatial grid of a context (abi.Context) as write_state takes it."""
     p = ctx.params

@@ -7,7 +7,9 @@ the reference tree) and freezes what they return, with the written file.
 
 The reference tree is RH_REFERENCE_DIR, else the checkout next to this
 repository. Writes vlsv_state_5x4x3.vlsv and vlsv_state_5x4x3.npz (the inputs
-under in_*, the reader's answers under ref_*).
+under in_*, the reader's answers under ref_*), and the reduced state of the
+same cells (every REDUCED_NSTRIDE-th) as vlsv_reduced_5x4x3.vlsv, its reader
+answers under red_*.
 """
 import hashlib
 import os
@@ -23,6 +25,8 @@ from rhybrid_b200 import vlsv as V  # noqa: E402
 REF_DIR = os.environ.get("RH_REFERENCE_DIR") or os.path.normpath(
     os.path.join(HERE, "..", "..", "..", "reference"))
 NAME = "vlsv_state_5x4x3"
+REDUCED = "vlsv_reduced_5x4x3"
+REDUCED_NSTRIDE = 2
 GRID = {"nx": 5, "ny": 4, "nz": 3, "x_min": -750e3, "y_min": -600e3, "z_min": -450e3, "dx": 300e3,
         "periodic": (False, True, False)}
 TIME, TIMESTEP = 12.5, 250
@@ -54,6 +58,21 @@ def inputs():
         parts[f"v_{pop}"] = rng.normal(0, 4e5, (m, 3))
         parts[f"CellID_{pop}"] = cid
     return cells, parts
+
+
+def reduced_inputs(cells, parts):
+    """The reduced state of the same cells: every REDUCED_NSTRIDE-th cell's
+    id and cellB, and those cells' particles."""
+    nx, ny, n = GRID["nx"], GRID["ny"], GRID["nx"] * GRID["ny"] * GRID["nz"]
+    cid = np.arange(n)
+    s = REDUCED_NSTRIDE
+    keep = (cid % s == 0) & (cid % (s * nx) < nx) & (cid % (s * nx * ny) < nx * ny)
+    red = {"CellID": cid[keep].astype(np.uint32), "cellB": cells["cellB"][keep]}
+    for pop in ("H+", "O+"):
+        k = keep[parts[f"CellID_{pop}"]]
+        red[f"CellID_{pop}"] = parts[f"CellID_{pop}"][k]
+        red[f"v_{pop}"] = parts[f"v_{pop}"][k]
+    return red
 
 
 def main():
@@ -89,6 +108,18 @@ def main():
         out[f"ref_pv_{pop}"] = vp.read_particle_variable(f"v_{pop}")
         out[f"ref_pcid_{pop}"] = vp.read_particle_variable(f"CellID_{pop}")
     out["sha256"] = np.array(hashlib.sha256(open(path, "rb").read()).hexdigest())
+    red = reduced_inputs(cells, parts)
+    rpath = os.path.join(HERE, REDUCED + ".vlsv")
+    V.write_reduced_state(rpath, TIME, TIMESTEP, REDUCED_NSTRIDE, red, ("H+", "O+"))
+    rr = rhb.vlsvfile.VlsvReader(rpath)
+    rp = rhb.vlsvfile.VlsvParticles(rpath)
+    out.update({f"red_in_{k}": np.asarray(v) for k, v in red.items()})
+    for par in ("time", "timestep", "Nstride"):
+        out[f"red_par_{par}"] = np.array(rr.read_parameter(par))
+    out["red_point_variables"] = np.array(rp.get_all_point_variables())
+    for name in ("CellID", "cellB", "CellID_H+", "v_H+", "CellID_O+", "v_O+"):
+        out[f"red_var_{name}"] = rp.read_particle_variable(name)
+    out["red_sha256"] = np.array(hashlib.sha256(open(rpath, "rb").read()).hexdigest())
     np.savez_compressed(os.path.join(HERE, NAME + ".npz"), **out)
     print(f"wrote {path} ({os.path.getsize(path)} bytes) and {NAME}.npz")
 

@@ -104,3 +104,20 @@ def test_writer_rejects_bad_arrays(tmp_path):
             w.write("VARIABLE", np.zeros((2, 2, 2)), name="cube")
     with pytest.raises(ValueError):
         V.write_state(str(tmp_path / "y.vlsv"), G.GRID, 0.0, 0, {"short": np.zeros(3)})
+
+
+def test_reduced_state_pinned(tmp_path, gold):
+    """The reduced state file: reproduced byte for byte, and the reference's
+    reader read its parameters and point data back as written."""
+    red = {k[len("red_in_"):]: gold[k] for k in gold.files if k.startswith("red_in_")}
+    path = str(tmp_path / "r.vlsv")
+    V.write_reduced_state(path, G.TIME, G.TIMESTEP, G.REDUCED_NSTRIDE, red, ("H+", "O+"))
+    assert hashlib.sha256(open(path, "rb").read()).hexdigest() == str(gold["red_sha256"])
+    assert open(path, "rb").read() == open(os.path.join(HERE, "golden", G.REDUCED + ".vlsv"), "rb").read()
+    assert float(gold["red_par_time"]) == G.TIME and int(gold["red_par_timestep"]) == G.TIMESTEP
+    assert int(gold["red_par_Nstride"]) == G.REDUCED_NSTRIDE
+    assert list(gold["red_point_variables"]) == ["CellID", "cellB", "CellID_H+", "v_H+", "CellID_O+", "v_O+"]
+    cells, parts = state(gold)
+    want = G.reduced_inputs(cells, parts)
+    for name, a in want.items():
+        assert np.array_equal(gold[f"red_var_{name}"].reshape(a.shape), a), name
