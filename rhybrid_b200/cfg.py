@@ -31,6 +31,8 @@ class RunSettings:
     output_group_names: List[str] = field(default_factory=list)   # output_str of each output population
     save_particles: bool = False            # Hybrid.save_particles (user.cpp:396)
     save_particles_nstride: int = 10        # Hybrid.save_particles_Nstride (user.cpp:397)
+    data_save_all_timesteps_t_start: float = -1.0   # Hybrid.data_save_all_timesteps_t_start (user.cpp:418)
+    data_save_all_timesteps_t_end: float = -1.0     # Hybrid.data_save_all_timesteps_t_end (user.cpp:419)
     save_reduced_state_interval: int = 0    # Hybrid.save_reduced_state_interval (user.cpp:420)
     save_reduced_state_nstride: int = 10    # Hybrid.save_reduced_state_Nstride (user.cpp:421; <= 0 gives 10, :2452-2455)
     save_reduced_state_particles: bool = False   # Hybrid.save_reduced_state_include_particles (user.cpp:422)
@@ -233,12 +235,20 @@ def load_text(text: str) -> Tuple[cf.Config, RunSettings]:
         output_parameters=(hy.str("output_parameters", "") or "").split(), output_groups=groups,
         output_group_names=seen, save_particles=hy.bool("save_particles"),
         save_particles_nstride=hy.int("save_particles_Nstride", 10), species_names=names,
+        data_save_all_timesteps_t_start=hy.float("data_save_all_timesteps_t_start", -1.0),
+        data_save_all_timesteps_t_end=hy.float("data_save_all_timesteps_t_end", -1.0),
         save_reduced_state_interval=hy.int("save_reduced_state_interval", 0),
         save_reduced_state_nstride=(hy.int("save_reduced_state_Nstride", 10)
                                     if hy.int("save_reduced_state_Nstride", 10) > 0 else 10),
         save_reduced_state_particles=hy.bool("save_reduced_state_include_particles"),
         extra={k: v for k, v in P.items() if k in ("Restart", "LoadBalance", "DetectorParticle",
                                                     "DetectorBulkParameter", "DataOperatorExcludes")})
+    # the window of saving at every step (user.cpp:2381-2388): start > end is an
+    # error, a negative start or a non-positive end switches it off
+    if rs.data_save_all_timesteps_t_start > rs.data_save_all_timesteps_t_end:
+        raise ValueError("Hybrid.data_save_all_timesteps_t_start must be below Hybrid.data_save_all_timesteps_t_end")
+    if rs.data_save_all_timesteps_t_start < 0 or rs.data_save_all_timesteps_t_end <= 0:
+        rs.data_save_all_timesteps_t_start = rs.data_save_all_timesteps_t_end = -1.0
     return cfgobj, rs
 
 

@@ -75,6 +75,13 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
                     sys.stdout.write(msg)
                 if stopped:
                     break
+            # inside the window of Hybrid.data_save_all_timesteps_t_*, a state at
+            # every step (user.cpp:66-71, decided on the time before the step)
+            interval = rs.data_save_interval
+            t0 = ctx.time()[0]
+            if rs.data_save_all_timesteps_t_start >= 0 and \
+                    rs.data_save_all_timesteps_t_start <= t0 <= rs.data_save_all_timesteps_t_end:
+                interval = 1
             ctx.step(1)
             done += 1
             ts = ctx.time()[1]
@@ -85,7 +92,7 @@ def run(cfg_path: str, steps: Optional[int] = None, out_dir: str = ".", path: st
                 fn = os.path.join(out_dir, f"reduced{ts:08d}.vlsv")
                 V.write_reduced_state(fn, ctx.time()[0], ts, rs.save_reduced_state_nstride, red, rs.species_names)
                 reduced.append(fn)
-            if rs.data_save_interval > 0 and ts % rs.data_save_interval == 0:
+            if interval > 0 and ts % interval == 0:
                 out = O.cell_variables(ctx, rs.output_parameters, rs.output_groups, rs.output_group_names)
                 parts = O.particle_points(ctx, rs.species_names, rs.save_particles_nstride) if rs.save_particles else None
                 fn = os.path.join(out_dir, f"state_{ts:07d}.vlsv")

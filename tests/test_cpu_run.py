@@ -4,6 +4,7 @@ step, states with the temporal averages at every data save step."""
 import os
 
 import numpy as np
+import pytest
 
 from rhybrid_b200 import run as R
 from rhybrid_b200 import vlsv as V
@@ -61,3 +62,24 @@ def test_run_reduced_state(tmp_path, ref_lib):
         mesh = f"ReducedParticlePointMesh_{name}"
         assert np.array_equal(raw[("VARIABLE", f"CellID_{name}", mesh)], st[f"ParticlePointMesh_{name}/CellID_{name}"])
         assert np.array_equal(raw[("VARIABLE", f"v_{name}", mesh)], st[f"ParticlePointMesh_{name}/v_{name}"])
+
+
+def test_run_save_window(tmp_path, ref_lib):
+    """Hybrid.data_save_all_timesteps_t_start/end: a state after every step
+    that starts inside the window (user.cpp:66-71), the regular interval
+    elsewhere; a window ending before it starts is refused (user.cpp:2381)."""
+    from rhybrid_b200 import cfg as C
+    text = TEXT.replace("injector.name = SolarWindInjector", "injector.name = UniformInjector")
+    text = text.replace("particle.population.exosphere = exoO+\n", "").replace("particle.population.ionosphere = ionoO+\n", "")
+    text = text.replace("maximum_timesteps = 200", "maximum_timesteps = 8\ndata_save_interval = 4")
+    win = text.replace("[Hybrid]", "[Hybrid]\ndata_save_all_timesteps_t_start = 0.09\ndata_save_all_timesteps_t_end = 0.17")
+    f = tmp_path / "run.cfg"
+    f.write_text(win)
+    r = R.run(str(f), out_dir=str(tmp_path), lib=ref_lib, quiet=True)
+    assert [os.path.basename(p) for p in r["saved"]] == ["state_0000004.vlsv", "state_0000005.vlsv",
+                                                         "state_0000008.vlsv"]
+    bad = text.replace("[Hybrid]", "[Hybrid]\ndata_save_all_timesteps_t_start = 0.2\ndata_save_all_timesteps_t_end = 0.1")
+    with pytest.raises(ValueError):
+        C.load_text(bad)
+    _, rs = C.load_text(text.replace("[Hybrid]", "[Hybrid]\ndata_save_all_timesteps_t_start = -1\ndata_save_all_timesteps_t_end = 0.3"))
+    assert rs.data_save_all_timesteps_t_start == -1.0 and rs.data_save_all_timesteps_t_end == -1.0
