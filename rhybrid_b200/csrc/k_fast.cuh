@@ -117,21 +117,6 @@ __device__ inline double fixedToDouble(unsigned long long lo, unsigned long long
    return __ll2double_rn((long long)hi) * hiScale + __ull2double_rn(lo) * loScale;
 }
 
-// x / dx, correctly rounded, without a division: Markstein's method (P. Markstein,
-// "Computation of elementary functions on the IBM RISC System/6000 processor",
-// IBM J. Res. Dev. 34(1), 1990). With r = RN(1/dx) and q = RN(x r), the residual
-// e = x - q dx is exact in one fused multiply-add and RN(q + e r) = RN(x / dx).
-// The method needs no overflow or underflow on the way: quotients outside
-// [2^-500, 2^500] in magnitude (zeros, NaN and infinities included) take the
-// IEEE division; rhgpu_create keeps dx within [2^-200, 2^200].
-__device__ inline double divDx(double x, const GridInfo& g) {
-   const double q = x * g.rdx;
-   const double aq = fabs(q);
-   if (!(aq >= 0x1p-500 && aq <= 0x1p+500)) return x / g.dx;
-   const double e = fma(-q, g.dx, x);
-   return fma(e, g.rdx, q);
-}
-
 // cicWeights (particle_accumulator.cpp:68-110) with the divisions by dx done by divDx
 __device__ inline void cicWeightsDx(double x, double y, double z, double wq, const GridInfo& g, double w8[8]) {
    const double dx = g.dx;

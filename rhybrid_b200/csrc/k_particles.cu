@@ -140,65 +140,87 @@ __global__ void k_set_alive_from_count(long long N, const long long* cnt, int* a
    if (c < N) alive[c] = (int)cnt[c];
 }
 
-__global__ void __launch_bounds__(32 * DEP_WARPS) k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err) {
-   __shared__ double sw[DEP_WARPS][32][11];   // w8[0..7], v[0..2] of the batch's particles
-   __shared__ int soct[DEP_WARPS][32];        // octant (i + 2j + 4k) of the corner-000 entry, -1 if invalid
+__global__ void __launch_bounds__(32 * DEP_WARPS, 4) k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err) {
+   __shared__ double sw[DEP_WARPS][32][11];                // w8[0..7], v[0..2] of a batch's particles
+   __shared__ int soct[DEP_WARPS][32];                     // octant (i + 2j + 4k) of the corner-000 entry, 8 if invalid
+   __shared__ double stage[DEP_WARPS][DEP_ENTRIES + 1];    // the group's sums, per cell
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   const long long c = (long long)blockIdx.x * DEP_WARPS + warp;
-   if (c >= g.N) return;
-   int ea[4], eb[4], ec[4], el[4];
-   double acc[4] = {0.0, 0.0, 0.0, 0.0};
+   // per entry t: its value (-1 charge, 0..2 current) and its corner map,
+   // nibble o = the corner of a particle of octant o landing on the entry, 8
+   // for none (nibble 8: a particle without a valid octant)
+   unsigned long long cmap[4];
+   int el[4];
    const int ne = lane < 12 ? 4 : 3;
 #pragma unroll
    for (int t = 0; t < 4; ++t) {
       const int e = lane + 32 * t;
       int ind, l;
       if (e < 27) { ind = e; l = -1; } else { ind = (e - 27) / 3; l = (e - 27) % 3; }
-      ea[t] = ind % 3; eb[t] = (ind / 3) % 3; ec[t] = ind / 9; el[t] = l;
-   }
-   const long long a0 = P.start[c];
-   const int na = P.alive[c];
-   for (int b0 = 0; b0 < na; b0 += 32) {
-      const int nb = min(32, na - b0);
-      if (lane < nb) {
-         const long long p = a0 + b0 + lane;
-         const double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
-         const double wq = P.a[6][p] * q;
-         double w8[8];
-         int ind[8];
-         cicWeights(x, y, z, wq, g.dx, w8, ind);
-         int oct = -1;
-         const int i0 = ind[0] % 3, j0 = (ind[0] / 3) % 3, k0 = ind[0] / 9;
-         if (ind[0] >= 0 && ind[0] < 27 && i0 <= 1 && j0 <= 1 && k0 <= 1) oct = i0 + 2 * j0 + 4 * k0;
-         else raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
-#pragma unroll
-         for (int o = 0; o < 8; ++o) sw[warp][lane][o] = w8[o];
-         sw[warp][lane][8] = P.a[3][p];
-         sw[warp][lane][9] = P.a[4][p];
-         sw[warp][lane][10] = P.a[5][p];
-         soct[warp][lane] = oct;
+      const int ea = ind % 3, eb = (ind / 3) % 3, ec = ind / 9;
+      unsigned long long m = 8ull << 32;
+      for (int o = 0; o < 8; ++o) {
+         const int ox = ea - (o & 1), oy = eb - ((o >> 1) & 1), oz = ec - (o >> 2);
+         const bool on = (unsigned)ox <= 1u && (unsigned)oy <= 1u && (unsigned)oz <= 1u;
+         m |= (unsigned long long)(on ? ox + 2 * oy + 4 * oz : 8) << (4 * o);
       }
-      __syncwarp();
-      for (int j = 0; j < nb; ++j) {
-         const int oct = soct[warp][j];
-         if (oct < 0) continue;
-         const int i0 = oct & 1, j0 = (oct >> 1) & 1, k0 = oct >> 2;
+      cmap[t] = m;
+      el[t] = l;
+   }
+   const long long groups = (g.N + DEP_WARPS - 1) / DEP_WARPS;
+   for (long long grp = blockIdx.x; grp < groups; grp += gridDim.x) {
+      const long long c = grp * DEP_WARPS + warp;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      if (c < g.N) {
+         const long long a0 = P.start[c];
+         const int na = P.alive[c];
+         for (int b0 = 0; b0 < na; b0 += 32) {
+            const int nb = min(32, na - b0);
+            if (lane < nb) {
+               const long long p = a0 + b0 + lane;
+               const double x = P.a[0][p], y = P.a[1][p], z = P.a[2][p];
+               const double wq = P.a[6][p] * q;
+               double w8[8];
+               int ind[8];
+               cicWeights(x, y, z, wq, g, w8, ind);
+               int oct = 8;
+               const int i0 = ind[0] % 3, j0 = (ind[0] / 3) % 3, k0 = ind[0] / 9;
+               if (ind[0] >= 0 && ind[0] < 27 && i0 <= 1 && j0 <= 1 && k0 <= 1) oct = i0 + 2 * j0 + 4 * k0;
+               else raiseError(err, RHGPU_DEVERR_NAN_PARTICLE);
 #pragma unroll
-         for (int t = 0; t < 4; ++t) {
-            if (t >= ne) break;
-            const int ox = ea[t] - i0, oy = eb[t] - j0, oz = ec[t] - k0;
-            if ((unsigned)ox <= 1u && (unsigned)oy <= 1u && (unsigned)oz <= 1u) {
-               const double w = sw[warp][j][ox + 2 * oy + 4 * oz];
-               if (el[t] < 0) acc[t] += w;
-               else acc[t] += w * sw[warp][j][8 + el[t]];
+               for (int o = 0; o < 8; ++o) sw[warp][lane][o] = w8[o];
+               sw[warp][lane][8] = P.a[3][p];
+               sw[warp][lane][9] = P.a[4][p];
+               sw[warp][lane][10] = P.a[5][p];
+               soct[warp][lane] = oct;
             }
+            __syncwarp();
+#pragma unroll 2
+            for (int j = 0; j < nb; ++j) {
+               const int sh = 4 * soct[warp][j];
+               const double* r = sw[warp][j];
+#pragma unroll
+               for (int t = 0; t < 4; ++t) {
+                  if (t >= ne) break;
+                  const unsigned corner = (unsigned)(cmap[t] >> sh) & 15u;
+                  const double w = r[corner & 7u];
+                  const double v = el[t] < 0 ? w : w * r[8 + (el[t] < 0 ? 0 : el[t])];
+                  acc[t] += corner < 8u ? v : 0.0;
+               }
+            }
+            __syncwarp();
          }
       }
-      __syncwarp();
-   }
 #pragma unroll
-   for (int t = 0; t < 4; ++t)
-      if (t < ne) S[(long long)(lane + 32 * t) * g.N + c] = acc[t];
+      for (int t = 0; t < 4; ++t)
+         if (t < ne) stage[warp][lane + 32 * t] = acc[t];
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < DEP_ENTRIES * DEP_WARPS; idx += 32 * DEP_WARPS) {
+         const int e = idx / DEP_WARPS, w = idx - e * DEP_WARPS;
+         const long long cc = grp * DEP_WARPS + w;
+         if (cc < g.N) S[(long long)e * g.N + cc] = stage[w][e];
+      }
+      __syncthreads();
+   }
 }
 
 __global__ void k_deposit_gather(GridInfo g, Fields f, const double* S, int first, int last, double minRho,

@@ -56,15 +56,18 @@ __global__ void k_mig_scatter(GridInfo g, PStore P, PStore Q, const int* key, co
 __global__ void k_set_alive_from_count(long long N, const long long* cnt, int* alive);
 
 // CIC weights of one particle (particle_accumulator.cpp:68-110), corners in
-// the order 000,100,010,110,001,101,011,111 with their 3x3x3 indices
-__device__ inline void cicWeights(double x, double y, double z, double wq, double dx, double w8[8], int ind[8]) {
-   int i = (int)floor(x / dx), j = (int)floor(y / dx), k = (int)floor(z / dx);
+// the order 000,100,010,110,001,101,011,111 with their 3x3x3 indices; the
+// divisions by dx are divDx, the same correctly rounded quotients
+__device__ inline void cicWeights(double x, double y, double z, double wq, const GridInfo& g, double w8[8],
+                                  int ind[8]) {
+   const double dx = g.dx;
+   int i = (int)floor(divDx(x, g)), j = (int)floor(divDx(y, g)), k = (int)floor(divDx(z, g));
    if (x < (i + 0.5) * dx) { --i; }
    if (y < (j + 0.5) * dx) { --j; }
    if (z < (k + 0.5) * dx) { --k; }
    ++i; ++j; ++k;
    const double x0 = (i - 1 + 0.5) * dx, y0 = (j - 1 + 0.5) * dx, z0 = (k - 1 + 0.5) * dx;
-   const double w_x = (x - x0) / dx, w_y = (y - y0) / dx, w_z = (z - z0) / dx;
+   const double w_x = divDx(x - x0, g), w_y = divDx(y - y0, g), w_z = divDx(z - z0, g);
    w8[0] = (1 - w_x) * (1 - w_y) * (1 - w_z) * wq;
    w8[1] = w_x * (1 - w_y) * (1 - w_z) * wq;
    w8[2] = (1 - w_x) * w_y * (1 - w_z) * wq;
@@ -85,10 +88,21 @@ __device__ inline void cicWeights(double x, double y, double z, double wq, doubl
 // particles of the cell are taken 32 at a time, each lane computing one
 // particle's CIC weights into shared memory; then every lane walks those
 // particles in order and adds the contribution that falls on its entries, so
-// each entry is the same sequential sum as in the reference.
-// S[e*N + c] receives the 108 sums of cell c.
-constexpr int DEP_WARPS = 4;
-__global__ void __launch_bounds__(32 * DEP_WARPS) k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err);
+// each entry is the same sequential sum as in the reference. Each entry keeps
+// a map from the particle's octant (the 3x3x3 index of its corner 000 is one
+// of the 8 of {0,1}^3) to the corner landing on the entry, or none; an entry
+// no corner lands on adds +0.0, which leaves every sum unchanged (a sum that
+// starts at +0.0 is never -0.0, so x + 0.0 == x for each of its values), so
+// the walk has no branches and each sum is still the reference's sequence.
+// S[e*N + c] receives the 108 sums of cell c. A block takes DEP_WARPS
+// consecutive cells at a time (one per warp) and writes their sums row by row
+// through shared memory, DEP_WARPS cells contiguous per row; the blocks, one
+// resident wave of DEP_GRID, stride over the groups of cells, so each warp
+// builds its corner maps once.
+constexpr int DEP_WARPS = 8;
+constexpr int DEP_ENTRIES = 108;
+constexpr int DEP_GRID = 148 * 4;   // 4 blocks of 256 threads at 64 registers per SM
+__global__ void __launch_bounds__(32 * DEP_WARPS, 4) k_deposit_cell(GridInfo g, PStore P, double q, double* S, unsigned* err);
 
 // destination sums over the 27 source cells in increasing source index
 // The up to 3 source coordinates per axis of the 27-neighbourhood of cell

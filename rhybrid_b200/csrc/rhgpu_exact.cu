@@ -120,7 +120,8 @@ int depositExact(rhgpu_ctx* c, double* S) {
       if (!deposits(c, s)) continue;
       {
          RH_TIME(c, "deposit_cell");
-         k_deposit_cell<<<blocks1d(g.N, DEP_WARPS), 32 * DEP_WARPS, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, S, c->err);
+         const unsigned nblk = (unsigned)std::min<long long>(blocks1d(g.N, DEP_WARPS), DEP_GRID);
+         k_deposit_cell<<<nblk, 32 * DEP_WARPS, 0, c->stream>>>(g, c->ps[s], c->sp[s].q, S, c->err);
          RH_LAUNCHED(c);
       }
       {
