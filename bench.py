@@ -537,7 +537,7 @@ def run_learned(args, rank, world, local_rank):
     workload = "mercury" if args.workload == "mercury" else "mars"
     low_path = abi.PATH_FP32 if args.path == "fp32" else abi.PATH_FAST
     out = learned.closed_loop(scale=args.scale, workload=workload, low_path=low_path, velocity=args.velocity,
-                              log=lambda m: print(m, file=sys.stderr, flush=True))
+                              keep_radius=args.keep_radius, log=lambda m: print(m, file=sys.stderr, flush=True))
     lr = out["learned"]
     if rank == 0:
         form = "FP32 form" if low_path == abi.PATH_FP32 else "FP64 fast path"
@@ -548,7 +548,7 @@ def run_learned(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("f32" if low_path == abi.PATH_FP32 else "f64") + " (network bf16, fp32 accum)",
             "data": "synthetic (uniform fill generated on the GPU, solar wind sources)",
             "config": {"workload": f"{workload}_{out['geometry'][0]}x{out['geometry'][1]}x{out['geometry'][2]}_learned",
-                       "denoised": out["denoised"],
+                       "denoised": out["denoised"], "keep_radius": out["keep_radius"],
                        "check_run": out["check_run"], "training": out["training"], "window": out["window"],
                        "threshold": out["threshold"],
                        "learned": {k: v for k, v in lr.items() if k != "samples"},
@@ -600,6 +600,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--velocity", action="store_true",
                     help="--form learned: the denoiser sees rho and J / rho (rhgpu_dn_set_velocity_form)")
+    ap.add_argument("--keep-radius", type=float, default=0.0,
+                    help="--form learned: moments within this many obstacle radii stay as deposited")
     ap.add_argument("--path", default="fast", choices=["fast", "exact", "fp32"],
                     help="fast: FP64, segment storage and deposit order (default); exact: the reference's order; "
                          "fp32: the FP32 precision form")

@@ -297,6 +297,10 @@ int rhgpu_dn_set_scales(rhgpu_dn* dn, double rho_scale, double j_scale);
  * The deposit's rho and J carry the same particles' noise, which largely
  * cancels in J / rho; this form keeps that ratio as one quantity. */
 int rhgpu_dn_set_velocity_form(rhgpu_dn* dn, int32_t enabled);
+/* per cell (nx*ny*nz bytes, x fastest), nonzero: the cell's moments are left
+ * as deposited where the network is applied (no counterpart in the
+ * reference); NULL clears the mask. Training is unaffected. */
+int rhgpu_dn_set_keep_mask(rhgpu_dn* dn, const uint8_t* keep);
 /* host moments in the ABI layout (rho per cell, Ji interleaved) in and out;
  * rho_out is clamped at min_rho as the deposit's finalize does */
 int rhgpu_dn_apply(rhgpu_dn* dn, const double* rho_in, const double* ji_in, double* rho_out, double* ji_out,

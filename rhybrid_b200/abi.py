@@ -151,6 +151,7 @@ _OPTIONAL = {
     "dn_add_crops": [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_void_p],
     "dn_set_loss_border": [_P, C.c_int32],
     "dn_set_velocity_form": [_P, C.c_int32],
+    "dn_set_keep_mask": [_P, C.c_void_p],
     "set_timing": [_P, C.c_int32],
     "get_timing": [_P, C.c_char_p, C.c_int32, _D, C.c_int32, C.POINTER(C.c_int32)],
     "last_launch_count": [_P, _I64],
@@ -616,6 +617,17 @@ class Denoiser:
         """rhgpu_dn_set_velocity_form: the network sees rho and J/rho (j_scale a
         speed) and hands back J = rho' u'."""
         self.lib.call("dn_set_velocity_form", self.h, 1 if enabled else 0)
+
+    def set_keep_mask(self, keep):
+        """rhgpu_dn_set_keep_mask: cells (nonzero) whose moments the network
+        leaves as deposited; None clears it."""
+        if keep is None:
+            self.lib.call("dn_set_keep_mask", self.h, None)
+            return
+        k = np.ascontiguousarray(keep, dtype=np.uint8).reshape(-1)
+        if k.size != self.ncells:
+            raise ValueError(f"keep mask of {k.size} cells for {self.ncells}")
+        self.lib.call("dn_set_keep_mask", self.h, k.ctypes.data_as(C.c_void_p))
 
     def apply(self, rho: np.ndarray, ji: np.ndarray, min_rho: float = -np.inf):
         r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)

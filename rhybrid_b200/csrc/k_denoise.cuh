@@ -89,6 +89,7 @@ struct DnMoments {
    double sr, sj, rsr, rsj, minRho;
    long long N;
    int vel;        // velocity form: the network sees rho and J / rho (sj the velocity scale)
+   const unsigned char* keep;   // per cell, nonzero: the moments stay the deposit's (null: none)
 };
 
 // the factor that takes a current component to the network's input: 1 / sj,
@@ -285,6 +286,7 @@ __device__ __forceinline__ void tcEpilogue(const DnGrid& g, unsigned tmem, int g
          continue;
       }
       if (mode == 4) {
+         if (mom.keep && mom.keep[v]) continue;
          // the velocity form writes back J = rho' u' from the denoised density and velocity
          const double rin = mom.rho[v], fj = dnJFactor(mom.vel, mom.rsj, rin);
          double r0 = (double)(c[0] + (float)(rin * mom.rsr)) * mom.sr;

@@ -114,7 +114,7 @@ int dnUploadMoments(rhgpu_dn* d, const double* rho, const double* ji, double* pl
 // and scales back (rho clamped at minRho), in three launches
 int dnApplyMoments(rhgpu_dn* d, cudaStream_t st, double* rho, double* J, double minRho, unsigned* err) {
    const long long N = d->g.N;
-   const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N, d->vel};
+   const DnMoments mom{rho, J, d->sr, d->sj, 1.0 / d->sr, 1.0 / d->sj, minRho, N, d->vel, d->keep};
    const float* b0 = d->params + DN_TAPS * DN_C * DN_C;
    const float* b1 = d->params + DN_LAYER + DN_TAPS * DN_C * DN_C;
    const float* b2 = d->params + 2 * DN_LAYER + DN_TAPS * DN_C * DN_C;
@@ -202,7 +202,7 @@ int rhgpu_dn_destroy(rhgpu_dn* d) {
    for (int l = 0; l < 3; ++l) { cudaFree(d->act[l]); cudaFree(d->dY[l]); }
    cudaFree(d->res); cudaFree(d->out32); cudaFree(d->part); cudaFree(d->lossPart); cudaFree(d->acc);
    cudaFree(d->pairIn); cudaFree(d->pairOut);
-   cudaFree(d->fullAcc); cudaFree(d->fullIn); cudaFree(d->fullOut);
+   cudaFree(d->fullAcc); cudaFree(d->fullIn); cudaFree(d->fullOut); cudaFree(d->keep);
    if (d->stream) cudaStreamDestroy(d->stream);
    delete d;
    return RHGPU_OK;
@@ -243,6 +243,21 @@ int rhgpu_dn_set_scales(rhgpu_dn* d, double rho_scale, double j_scale) {
 int rhgpu_dn_set_velocity_form(rhgpu_dn* d, int32_t enabled) {
    if (!d) return fail(RHGPU_ERR_ARG, "dn_set_velocity_form: null denoiser");
    d->vel = enabled ? 1 : 0;
+   return RHGPU_OK;
+}
+
+int rhgpu_dn_set_keep_mask(rhgpu_dn* d, const uint8_t* keep) {
+   if (!d) return fail(RHGPU_ERR_ARG, "dn_set_keep_mask: null denoiser");
+   RH_CUDA(cudaSetDevice(d->device));
+   if (!keep) {
+      RH_CUDA(cudaStreamSynchronize(d->stream));
+      cudaFree(d->keep);
+      d->keep = nullptr;
+      return RHGPU_OK;
+   }
+   if (!d->keep) RH_CUDA(cudaMalloc(&d->keep, (size_t)d->g.N));
+   RH_CUDA(cudaMemcpyAsync(d->keep, keep, (size_t)d->g.N, cudaMemcpyHostToDevice, d->stream));
+   RH_CUDA(cudaStreamSynchronize(d->stream));
    return RHGPU_OK;
 }
 

@@ -17,18 +17,36 @@ F32Buf f32View(const F32Host& h, int which) {
 
 int f32Reserve(F32Host& h, int which, long long slots) {
    if (slots <= h.capOf[which] && h.cell[which]) return RHGPU_OK;
-   cudaFree(h.cell[which]);
-   h.cell[which] = nullptr;
-   for (int a = 0; a < 3; ++a) {
-      cudaFree(h.o[which][a]); cudaFree(h.v[which][a]);
-      h.o[which][a] = nullptr; h.v[which][a] = nullptr;
+   const long long had = h.capOf[which];
+   auto release = [&]() {
+      cudaFree(h.cell[which]);
+      h.cell[which] = nullptr;
+      for (int a = 0; a < 3; ++a) {
+         cudaFree(h.o[which][a]); cudaFree(h.v[which][a]);
+         h.o[which][a] = nullptr; h.v[which][a] = nullptr;
+      }
+      h.capOf[which] = 0;
+   };
+   auto alloc = [&](long long n) {
+      cudaError_t e = cudaMalloc(&h.cell[which], sizeof(int) * n);
+      for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+         e = cudaMalloc(&h.o[which][a], sizeof(float) * n);
+         if (e == cudaSuccess) e = cudaMalloc(&h.v[which][a], sizeof(float) * n);
+      }
+      return e;
+   };
+   release();
+   long long n = growSlots(had, slots);
+   if (alloc(n) != cudaSuccess && had > 0) {   // no room for the growth margin: the slots alone
+      release();
+      cudaGetLastError();
+      n = growSlots(0, slots);
+      alloc(n);
    }
-   h.capOf[which] = 0;
-   const long long n = slots + slots / 16 + 1024;
-   RH_CUDA(cudaMalloc(&h.cell[which], sizeof(int) * n));
-   for (int a = 0; a < 3; ++a) {
-      RH_CUDA(cudaMalloc(&h.o[which][a], sizeof(float) * n));
-      RH_CUDA(cudaMalloc(&h.v[which][a], sizeof(float) * n));
+   const cudaError_t e = cudaGetLastError();
+   if (e != cudaSuccess || !h.v[which][2]) {
+      release();
+      return fail(RHGPU_ERR_CUDA, std::string("FP32 particle storage: ") + cudaGetErrorString(e));
    }
    h.capOf[which] = n;
    return RHGPU_OK;
@@ -296,6 +314,7 @@ int f32Download(rhgpu_ctx* c, int s, uint32_t* counts, double* particles, long l
 // relays out the "next" buffers of the species in `mask` (bit s: species s)
 // with room for their pending arrivals; the other species keep their layout
 int f32RelayoutNext(rhgpu_ctx* c, unsigned mask) {
+   RH_TIME(c, "f32_relayout");
    const long long NS = c->fg.NS;
    for (int s = 0; s < c->ns; ++s) {
       if (!((mask >> s) & 1u)) continue;

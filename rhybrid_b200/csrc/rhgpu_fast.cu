@@ -8,12 +8,17 @@
 
 namespace rhh {
 
+// sort scratch of at least `bytes`; it grows by at least a quarter at a time,
+// since the migration's radix sorts ask for more with every new largest mover
+// count and each reallocation synchronises inside the step
 int ensureSortTmp(rhgpu_ctx* c, size_t bytes) {
    if (bytes <= c->sortTmpBytes) return RHGPU_OK;
+   const size_t want = std::max(bytes, c->sortTmpBytes + c->sortTmpBytes / 4) + 256;
    cudaFree(c->sortTmp);
    c->sortTmp = nullptr;
-   RH_CUDA(cudaMalloc(&c->sortTmp, bytes + 256));
-   c->sortTmpBytes = bytes + 256;
+   c->sortTmpBytes = 0;
+   RH_CUDA(cudaMalloc(&c->sortTmp, want));
+   c->sortTmpBytes = want;
    return RHGPU_OK;
 }
 
@@ -28,13 +33,32 @@ SegBuf segView(const SegHost& h, int which) {
 // particle arrays of buffer `which` with room for `slots` slots
 int segReserve(SegHost& h, int which, long long slots) {
    if (slots <= h.capOf[which] && h.a[which][0]) return RHGPU_OK;
-   for (int a = 0; a < 7; ++a) { cudaFree(h.a[which][a]); h.a[which][a] = nullptr; }
-   cudaFree(h.lx[which]);
-   h.lx[which] = nullptr;
-   h.capOf[which] = 0;
-   const long long n = slots + slots / 16 + 1024;
-   for (int a = 0; a < 7; ++a) RH_CUDA(cudaMalloc(&h.a[which][a], sizeof(double) * n));
-   RH_CUDA(cudaMalloc(&h.lx[which], n));
+   const long long had = h.capOf[which];
+   auto release = [&]() {
+      for (int a = 0; a < 7; ++a) { cudaFree(h.a[which][a]); h.a[which][a] = nullptr; }
+      cudaFree(h.lx[which]);
+      h.lx[which] = nullptr;
+      h.capOf[which] = 0;
+   };
+   auto alloc = [&](long long n) {
+      cudaError_t e = cudaSuccess;
+      for (int a = 0; a < 7 && e == cudaSuccess; ++a) e = cudaMalloc(&h.a[which][a], sizeof(double) * n);
+      if (e == cudaSuccess) e = cudaMalloc(&h.lx[which], n);
+      return e;
+   };
+   release();
+   long long n = growSlots(had, slots);
+   if (alloc(n) != cudaSuccess && had > 0) {   // no room for the growth margin: the slots alone
+      release();
+      cudaGetLastError();
+      n = growSlots(0, slots);
+      alloc(n);
+   }
+   const cudaError_t e = cudaGetLastError();
+   if (e != cudaSuccess || !h.lx[which]) {
+      release();
+      return fail(RHGPU_ERR_CUDA, std::string("particle storage: ") + cudaGetErrorString(e));
+   }
    h.capOf[which] = n;
    return RHGPU_OK;
 }
@@ -177,6 +201,7 @@ int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** 
       *bucket = bA;
       return RHGPU_OK;
    }
+   RH_TIME(c, "mig_radix_order");   // the fallback: a bucket with more than MIG_SMALL arrivals
    k_mig_sort_keys<<<blocks1d(nm, 256), 256, 0, c->stream>>>(mv, nm, NS, nb, kA, vA, bA);
    RH_LAUNCHED(c);
    const int kbits = 32 + bitsFor(std::max(NS > 1 ? NS - 1 : 1, c->injKeyMax)), bbits = bitsFor(nb);
@@ -215,6 +240,7 @@ int segPrefix(rhgpu_ctx* c, const int* cnt, long long* total) {
 // relays out the "next" buffers of the species in `mask` (bit s: species s)
 // with room for their pending arrivals; the other species keep their layout
 int fastRelayoutNext(rhgpu_ctx* c, unsigned mask) {
+   RH_TIME(c, "fast_relayout");
    const long long NS = c->fg.NS;
    for (int s = 0; s < c->ns; ++s) {
       if (!((mask >> s) & 1u)) continue;

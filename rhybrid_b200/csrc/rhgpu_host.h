@@ -229,6 +229,7 @@ struct rhgpu_dn {
    float* fullOut = nullptr;
    unsigned long long rng = 0x9e3779b97f4a7c15ull;
    int vel = 0;                          // velocity form (rhgpu_dn_set_velocity_form)
+   unsigned char* keep = nullptr;        // per cell: moments left as deposited (rhgpu_dn_set_keep_mask)
 };
 
 namespace rhh {
@@ -260,6 +261,15 @@ inline int growBuffer(T*& p, long long& have, long long need) {
    RH_CUDA(cudaMalloc(&p, sizeof(T) * n));
    have = n;
    return RHGPU_OK;
+}
+
+// slots to allocate for `slots` particles in a buffer of `have` slots (0: a
+// first allocation): 1/16 more, and when a buffer grows again at least a
+// quarter more than it had, so that a run whose particle count keeps rising
+// reallocates (a synchronous free and allocation inside a step) rarely
+inline long long growSlots(long long have, long long slots) {
+   const long long n = slots + slots / 16 + 1024;
+   return have > 0 ? std::max(n, have + have / 4) : n;
 }
 
 // the periodic axes of a grid as a 3-bit mask (bit a = axis a)

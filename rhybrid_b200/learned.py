@@ -63,6 +63,18 @@ def velocity_scales(cfg: cf.Config):
     return rho, j / rho
 
 
+def keep_mask(cfg: cf.Config, radius: float) -> np.ndarray:
+    """Cells whose centre lies within `radius` field-obstacle radii of the
+    origin (the planet's centre): the denoiser leaves their moments as
+    deposited (rhgpu_dn_set_keep_mask)."""
+    k, j, i = np.meshgrid(np.arange(cfg.nz), np.arange(cfg.ny), np.arange(cfg.nx), indexing="ij")
+    x = cfg.x_min + (i + 0.5) * cfg.dx
+    y = cfg.y_min + (j + 0.5) * cfg.dx
+    z = cfg.z_min + (k + 0.5) * cfg.dx
+    R = radius * max(cfg.R_fieldObstacle, 0.0)
+    return ((x * x + y * y + z * z) < R * R).astype(np.uint8).reshape(-1)
+
+
 def relative_l2(a: np.ndarray, b: np.ndarray) -> float:
     a, b = np.asarray(a, float).reshape(-1), np.asarray(b, float).reshape(-1)
     d = np.linalg.norm(b)
@@ -203,7 +215,7 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
                 lr: float = 1e-3, eval_steps: int = 100, every: int = 10, threshold: float = 0.02,
                 enforce_gate: bool = False, seed: int = 6461674, workload: str = "mars",
                 low_path: int = abi.PATH_FAST, rho_only: bool = False, velocity: bool = False,
-                log=print) -> dict:
+                keep_radius: float = 0.0, log=print) -> dict:
     """The learned form in closed loop against a high-ppc plain check run.
 
     workload: "mars" (c4_config) or "mercury" (c5_config), at `scale` of the
@@ -213,6 +225,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
     current outputs are zeroed, so the learned run denoises the charge density
     and keeps its deposited current. velocity: the network denoises rho and
     the bulk velocity J / rho (rhgpu_dn_set_velocity_form) instead of rho and J.
+    keep_radius: in the learned run, the moments of cells within that many
+    field-obstacle radii of the planet's centre stay as deposited (keep_mask).
 
     1. Check run (judge_ppc, FP64 fast path, filled on the GPU) steps
        train_steps + eval_steps. During the first train_steps it yields the
@@ -305,6 +319,8 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
                 else:
                     net.set_scales(*moment_scales(cfg))
                 net.set_params(params)
+                if keep_radius > 0:
+                    net.set_keep_mask(keep_mask(cfg, keep_radius))
                 ctx.set_denoiser(net, True)
             ctx.step(train_steps)
             n_ions = sum(ctx.num_particles(s) for s in range(len(cfg.populations)))
@@ -350,6 +366,7 @@ def closed_loop(scale: float = 1.0, judge_ppc: int = 256, low_ppc: int = 8, plai
         "workload": workload, "geometry": [judge_cfg.nx, judge_cfg.ny, judge_cfg.nz], "dx_m": judge_cfg.dx,
         "dt_s": judge_cfg.dt, "learned_path": "fp32" if low_path == abi.PATH_FP32 else "fast",
         "denoised": "rho" if rho_only else ("rho, J/rho" if velocity else "rho, J"),
+        "keep_radius": keep_radius,
         "check_run": {"ppc": judge_ppc, "ions": int(n_judge), "ms_per_step": judge_ms,
                       "split_half_noise": {str(k): {"rho": v[0], "J": v[1]} for k, v in judge_noise.items()}},
         "training": {"pairs": train_steps * crops_per_step, "crop": crop, "factor": factor, "adam_steps": adam_steps,
@@ -423,6 +440,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--rho-only", action="store_true", help="denoise the charge density only (keep the current)")
     ap.add_argument("--velocity", action="store_true", help="denoise rho and the bulk velocity J/rho")
+    ap.add_argument("--keep-radius", type=float, default=0.0,
+                    help="leave the moments within this many obstacle radii of the planet as deposited")
     ap.add_argument("--plain", default="8,16,32,64,128")
     ap.add_argument("--workload", default="mars", choices=sorted(GEOMETRIES))
     ap.add_argument("--learned-path", default="fast", choices=["fast", "fp32"],
@@ -436,6 +455,7 @@ def main(argv=None):
     out = closed_loop(scale=a.scale, judge_ppc=a.judge_ppc, train_steps=a.train_steps, eval_steps=a.eval_steps,
                       adam_steps=a.adam_steps, lr=a.lr, plain_ppcs=tuple(int(x) for x in a.plain.split(",")),
                       workload=a.workload, rho_only=a.rho_only, velocity=a.velocity,
+                      keep_radius=a.keep_radius,
                       low_path=abi.PATH_FP32 if a.learned_path == "fp32" else abi.PATH_FAST)
     print(json.dumps(out))
     if a.json:
