@@ -42,6 +42,11 @@ __global__ void k_fast_mig_place(FastSpecies FS, long long NS, long long nb, con
    SS.nxt.lx[pos] = (unsigned char)(M.lx & 0xff);
 }
 
+__global__ void k_mig_large_list(const int* inc, long long nb, unsigned* large, int* nlarge) {
+   const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+   if (b < nb && inc[b] > MIG_SMALL) large[atomicAdd(nlarge, 1)] = (unsigned)b;
+}
+
 __global__ void k_fast_seg_of(GridInfo g, FastGeom fg, const double* aos, const int* pcell, long long n,
                               unsigned* key, unsigned char* lx) {
    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;

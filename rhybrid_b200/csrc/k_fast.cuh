@@ -914,12 +914,15 @@ __global__ void k_mig_bucket(const MV* mv, long long n, long long NS, const long
    const int k = atomicAdd(&fill[b], 1);
    list[off[b] + k] = (unsigned)t;
 }
+constexpr int MIG_SMALL = 64;     // arrivals a bucket's own thread orders
+constexpr int MIG_LARGE = 2048;   // arrivals one block orders in shared memory (k_mig_order_large)
 template <class MV>
 __global__ void k_mig_order_small(const MV* mv, long long nb, const int* inc, const long long* off, unsigned* list,
                                   unsigned* bkt) {
    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
    if (b >= nb) return;
    const int k = inc[b];
+   if (k > MIG_SMALL) return;   // k_mig_order_large
    unsigned* bk = list + off[b];
    for (int a = 1; a < k; ++a) {
       const unsigned t = bk[a];
@@ -929,6 +932,62 @@ __global__ void k_mig_order_small(const MV* mv, long long nb, const int* inc, co
       bk[c] = t;
    }
    for (int a = 0; a < k; ++a) bkt[off[b] + a] = (unsigned)b;
+}
+
+// the buckets with more than MIG_SMALL arrivals, appended to large[] (count in *nlarge)
+__global__ void k_mig_large_list(const int* inc, long long nb, unsigned* large, int* nlarge);
+
+// each bucket of large[] (at most MIG_LARGE arrivals) ordered by one block: its
+// arrivals' (key, mover index) sorted bitonically in shared memory, the order
+// the radix sorts give (by key; equal keys by mover index)
+constexpr int MIG_LARGE_THREADS = 256;
+template <class MV>
+__global__ void __launch_bounds__(MIG_LARGE_THREADS) k_mig_order_large(const MV* mv, const int* inc, const long long* off,
+                                                                        unsigned* list, unsigned* bkt,
+                                                                        const unsigned* large, const int* nlarge) {
+   __shared__ unsigned long long skey[MIG_LARGE];
+   __shared__ unsigned sval[MIG_LARGE];
+   const int n = *nlarge;
+   for (int q = blockIdx.x; q < n; q += gridDim.x) {
+      const unsigned b = large[q];
+      const int k = inc[b];
+      unsigned* bk = list + off[b];
+      int m = 1;
+      while (m < k) m <<= 1;
+      for (int i = threadIdx.x; i < m; i += MIG_LARGE_THREADS) {
+         if (i < k) {
+            skey[i] = mv[bk[i]].key;
+            sval[i] = bk[i];
+         } else {
+            skey[i] = ~0ull;
+            sval[i] = ~0u;
+         }
+      }
+      __syncthreads();
+      for (int size = 2; size <= m; size <<= 1) {
+         for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < m; i += MIG_LARGE_THREADS) {
+               const int j = i ^ stride;
+               if (j > i) {
+                  const bool up = (i & size) == 0;
+                  const unsigned long long ki = skey[i], kj = skey[j];
+                  const unsigned vi = sval[i], vj = sval[j];
+                  const bool gt = ki > kj || (ki == kj && vi > vj);
+                  if (gt == up) {
+                     skey[i] = kj; skey[j] = ki;
+                     sval[i] = vj; sval[j] = vi;
+                  }
+               }
+            }
+            __syncthreads();
+         }
+      }
+      for (int i = threadIdx.x; i < k; i += MIG_LARGE_THREADS) {
+         bk[i] = sval[i];
+         bkt[off[b] + i] = b;
+      }
+      __syncthreads();
+   }
 }
 
 // mover order[q] to slot q - off[bucket] after its bucket's stayers (bucket nb: not placed)

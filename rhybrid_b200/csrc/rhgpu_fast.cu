@@ -162,9 +162,9 @@ int bitsFor(long long x) {
 // count (c->finc) and first position (c->foffInc), the movers sorted by bucket
 // and within it by key (*order, *bucket; bucket ns*NS = not placed), and
 // whether some bucket lacks room (*over). Buckets of at most MIG_SMALL arrivals
-// (the usual case) are ordered one thread per bucket; otherwise two stable
-// radix sorts over all movers (by key, then by bucket) give the same order.
-const int MIG_SMALL = 64;
+// (the usual case) are ordered one thread per bucket, those of up to
+// MIG_LARGE one block per bucket; past that two stable radix sorts over all
+// movers (by key, then by bucket) give the same order.
 template <class MV, class SET>
 int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** order, unsigned** bucket, int* over) {
    const long long NS = c->fg.NS, nb = (long long)c->ns * NS;
@@ -185,7 +185,7 @@ int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** 
    int maxInc = 0;
    RH_CUDA(cudaMemcpyAsync(&maxInc, c->fmaxInc, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
    RH_CUDA(cudaStreamSynchronize(c->stream));
-   if (maxInc <= MIG_SMALL) {
+   if (maxInc <= MIG_LARGE) {
       // buckets past the placed movers stay at nb (not placed)
       RH_CUDA(cudaMemsetAsync(c->ffill, 0, sizeof(int) * nb, c->stream));
       k_fill_u32<<<blocks1d(nm, 256), 256, 0, c->stream>>>(bA, nm, (unsigned)nb);
@@ -193,6 +193,16 @@ int migSort(rhgpu_ctx* c, const MV* mv, long long nm, const SET& FS, unsigned** 
       RH_LAUNCHED(c);
       k_mig_order_small<<<blocks1d(nb, 256), 256, 0, c->stream>>>(mv, nb, c->finc, c->foffInc, vA, bA);
       RH_LAUNCHED(c);
+      if (maxInc > MIG_SMALL) {
+         // the large buckets (each holds more than MIG_SMALL movers, so fewer
+         // than nm / MIG_SMALL of them) listed in bB, their count in fmaxInc
+         RH_CUDA(cudaMemsetAsync(c->fmaxInc, 0, sizeof(int), c->stream));
+         k_mig_large_list<<<blocks1d(nb, 256), 256, 0, c->stream>>>(c->finc, nb, bB, c->fmaxInc);
+         RH_LAUNCHED(c);
+         const unsigned grid = (unsigned)std::min<long long>(nm / MIG_SMALL + 1, 4 * 148);
+         k_mig_order_large<<<grid, MIG_LARGE_THREADS, 0, c->stream>>>(mv, c->finc, c->foffInc, vA, bA, bB, c->fmaxInc);
+         RH_LAUNCHED(c);
+      }
       k_mig_check<<<blocks1d(nb, 256), 256, 0, c->stream>>>(FS, NS, c->finc, c->fover);
       RH_LAUNCHED(c);
       RH_CUDA(cudaMemcpyAsync(over, c->fover, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
