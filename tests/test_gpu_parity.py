@@ -263,11 +263,20 @@ def test_fast_closed_box_vs_reference_order(gpu_lib, port_lib):
 def test_fast_large_arrival_buckets_bitwise(gpu_lib, port_lib):
     """300 ppc of a hot plasma (1e7 K, 40 % of a cell per step) in a small
     periodic box: hundreds of particles arrive in each destination segment per
-    step, more than the per-bucket ordering takes, so the movers are placed
-    through the two radix sorts; bitwise with the oracle."""
+    step, more than one thread orders, so each destination's movers are ordered
+    by one block in shared memory; bitwise with the oracle."""
     cfg = cf.config_empty_box(8, 6, 5, ppc=300.0).replace(dt=0.1)
     cfg = cfg.replace(populations=[dataclasses.replace(cfg.populations[0], temperature=1e7)])
     assert_state_equal(run(gpu_lib, cfg, 4, fast=True), run(port_lib, cfg, 4, fast=True), "fast 300 ppc hot")
+
+
+def test_fast_huge_arrival_buckets_bitwise(gpu_lib, port_lib):
+    """3000 ppc of the same plasma: thousands of arrivals per destination
+    segment, more than one block orders, so the movers are placed through the
+    two radix sorts over all of them; bitwise with the oracle."""
+    cfg = cf.config_empty_box(8, 6, 5, ppc=3000.0).replace(dt=0.1)
+    cfg = cfg.replace(populations=[dataclasses.replace(cfg.populations[0], temperature=1e7)])
+    assert_state_equal(run(gpu_lib, cfg, 3, fast=True), run(port_lib, cfg, 3, fast=True), "fast 3000 ppc hot")
 
 
 def test_fast_segment_overflow_relayout(gpu_lib, port_lib):
