@@ -165,7 +165,8 @@ const char* rhgpu_version(void);
  * userLateInitialization (src/user.cpp:356) sets up: grid arrays are
  * allocated and zeroed (src/user.cpp:1853-1868); particle storage holds up
  * to capacity[s] particles of species s. The device is cudaSetDevice'd to
- * `device` first. */
+ * `device` first. Every axis needs at least 3 cells (the reference also runs
+ * periodic axes of 1 cell; RHGPU_ERR_ARG here) and 27 * cells below 2^31. */
 int rhgpu_create(const rhgpu_params* params, int32_t n_species, const rhgpu_species* species,
                  const int64_t* capacity, int32_t device, rhgpu_ctx** out);
 
