@@ -33,6 +33,23 @@ def test_library_exports_every_declared_symbol():
     assert "sm_100a" in lib.fn["version"]().decode()
 
 
+def test_entry_points_refuse_null_handles():
+    """Entry points given a null context or denoiser return RHGPU_ERR_ARG
+    before any CUDA call, so this runs without a GPU."""
+    path = abi.gpu_library_path()
+    if not os.path.exists(path):
+        pytest.skip("librhgpu.so not built")
+    import ctypes
+    dll = ctypes.CDLL(path)
+    dll.rhgpu_last_error.restype = ctypes.c_char_p
+    for name, args in [("rhgpu_dn_set_velocity_form", (None, 1)), ("rhgpu_dn_set_keep_mask", (None, None)),
+                       ("rhgpu_dn_set_scales", (None, ctypes.c_double(1.0), ctypes.c_double(1.0))),
+                       ("rhgpu_set_path", (None, 0)), ("rhgpu_step", (None, 1)),
+                       ("rhgpu_accumulate_noalloc", (None,))]:
+        assert getattr(dll, name)(*args) == abi.ERR_ARG, name
+        assert dll.rhgpu_last_error(), name
+
+
 def test_resistivity_units():
     cfg = cf.config_empty_box()
     # Rm: eta = mu0*dx*U/Rm (resistivity.h:86-93)
