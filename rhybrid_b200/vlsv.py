@@ -29,6 +29,7 @@ PARAMETERs.
 """
 import os
 import struct
+import xml.etree.ElementTree as ET
 from typing import Dict, Mapping, Optional
 from xml.sax.saxutils import quoteattr
 
@@ -199,7 +200,6 @@ def load_state(path: str) -> Dict[str, np.ndarray]:
 def read(path: str) -> Dict[tuple, np.ndarray]:
     """Every array of a VLSV file, keyed by (tag, name, mesh): the container's
     own reading, for tests and tools."""
-    import xml.etree.ElementTree as ET
     out = {}
     with open(path, "rb") as f:
         raw = f.read()
@@ -210,5 +210,5 @@ def read(path: str) -> Dict[tuple, np.ndarray]:
         dt = np.dtype({"float": "f", "int": "i", "uint": "u"}[a["datatype"]] + a["datasize"]).newbyteorder("<")
         n, v = int(a["arraysize"]), int(a["vectorsize"])
         data = np.frombuffer(raw, dtype=dt, count=n * v, offset=int(el.text))
-        out[(el.tag, a.get("name"), a.get("mesh"))] = data.reshape(n, v) if v > 1 else data.copy()
+        out[(el.tag, a.get("name"), a.get("mesh"))] = (data.reshape(n, v) if v > 1 else data).copy()
     return out
