@@ -13,6 +13,11 @@ The gate (LearnedForm.judge): at each output step the denoised moments of the
 low-ppc run are compared with those of the high-ppc check run; when the
 relative L2 error of rho or J exceeds the threshold (2 % by default), the
 denoiser is switched off and the run continues with the plain deposit.
+
+The network can denoise rho and J, or rho and the bulk velocity J / rho (the
+velocity form, velocity_scales; J is handed back as rho' u'), and can leave
+the cells near the planet as deposited (keep_mask). closed_loop measures the
+whole scheme against plain runs at matched error.
 """
 from __future__ import annotations
 
